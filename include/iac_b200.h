@@ -1,0 +1,171 @@
+/*
+ * iac_b200.h -- C ABI of libiac_b200.so, the B200 (sm_100a) implementation of
+ * IncohAutoCorrelate's pair-correlation path.
+ *
+ * Plain C: pointers, sizes, status codes.  Device pointers ("d_") are CUDA
+ * global-memory addresses on the context's device; host pointers ("h_") are
+ * ordinary (preferably pinned) host memory.  `stream` is a cudaStream_t passed
+ * as void* (NULL = the legacy default stream).  Every function returns an
+ * iac_status; a non-IAC_OK return leaves a message for iac_last_error().
+ *
+ * Each entry point names the reference interface it replaces
+ * (FabianTr/IncohAutoCorrelate, IncohAutoCorrelate/ abbreviated IAC/).
+ * Mesh layouts are the reference's: voxel (fs, ms, ss) at fs + ms*S + ss*S*S,
+ * fs running fastest, centre C = (S-1)/2 (IAC/ACMesh.cpp:84-105).
+ */
+#ifndef IAC_B200_H
+#define IAC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IAC_ABI_VERSION 1
+
+typedef enum {
+    IAC_OK = 0,
+    IAC_ERR_INVALID_ARG = 1,  /* bad size, even mesh edge, null pointer, ... */
+    IAC_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    IAC_ERR_NO_MEMORY = 3,    /* device or pinned allocation failed */
+    IAC_ERR_TIMEOUT = 4,      /* a bounded device-side wait ran out */
+    IAC_ERR_OUT_OF_MESH = 5,  /* writes fell outside the mesh and were skipped */
+    IAC_ERR_UNSUPPORTED = 6   /* no sm_100 device, or a mode not built */
+} iac_status;
+
+/* Settings::Interpolation, IAC/Settings.h:158 */
+typedef enum { IAC_NEAREST = 0, IAC_LINEAR = 1 } iac_interpolation;
+
+/* ACMesh::MeshShape, IAC/ACMesh.h:21-29 */
+typedef struct {
+    uint32_t k_a, k_b, k_c;    /* q axis on the fast / medium / slow mesh axis */
+    uint32_t size_ab, size_c;  /* edge lengths including the 2-voxel padding */
+    uint32_t center[3];
+    float dq_per_voxel;
+    uint32_t voxel_per_dq;
+    float max_q;
+} iac_mesh_shape;
+
+/* AC1D::Shape, IAC/AC1D.h */
+typedef struct {
+    uint32_t size;
+    float max_q;
+    float dq_per_step;
+} iac_ac1d_shape;
+
+typedef struct iac_ctx iac_ctx;
+
+/* ---------------------------------------------------------------------- */
+/* context, errors                                                          */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces Settings::SetUp_OpenCL + the OCL device pool
+ * (IAC/Settings.cpp:331-470).  One context per device; thread-safe; calls
+ * from several host threads may share it, each on its own stream. */
+iac_status iac_ctx_create(int device, iac_ctx **out);
+iac_status iac_ctx_destroy(iac_ctx *ctx);
+/* Synchronises `stream`, then reports and clears the context's device-side
+ * error counters: writes skipped because their voxel lay outside the mesh
+ * (the reference writes them out of bounds) and bounded waits that ran out. */
+iac_status iac_ctx_check(iac_ctx *ctx, void *stream, uint64_t *out_of_mesh);
+const char *iac_status_string(iac_status s);
+const char *iac_last_error(void); /* thread-local message of the last failure */
+int iac_abi_version(void);
+/* number of launches of this library's kernels since the context was made */
+uint64_t iac_ctx_launch_count(const iac_ctx *ctx);
+
+/* ---------------------------------------------------------------------- */
+/* geometry (host arithmetic, no device work)                               */
+/* ---------------------------------------------------------------------- */
+
+/* Detector::Calc_kMap, IAC/Detector.cpp:310-361 (k-map on the device:
+ * d_kmap = d_pixel_map / |d_pixel_map|; max_q[3] returned to the host). */
+iac_status iac_calc_kmap(iac_ctx *ctx, const float *d_pixel_map, uint64_t npix, float *d_kmap,
+                         float max_q[3], void *stream);
+/* ACMesh::CreateBigMeshForDetector, IAC/ACMesh.cpp:74-106 */
+iac_status iac_big_mesh_shape(const float max_q[3], int edge_size, float q_zoom,
+                              iac_mesh_shape *shape);
+/* ACMesh::CreateSmallMesh_CofQ_ForDetector, IAC/ACMesh.cpp:140-206 */
+iac_status iac_small_cq_mesh_shape(const float max_q[3], int perp_size, float q_zoom,
+                                   iac_mesh_shape *shape);
+/* AC1D::Initialize(Det, ArraySize, QZoom), IAC/AC1D.cpp:53-59 */
+iac_status iac_ac1d_shape_init(const float max_q[3], uint32_t array_size, float q_zoom,
+                               iac_ac1d_shape *shape);
+
+/* ---------------------------------------------------------------------- */
+/* (a) sparse photon pairs -> uint64 3D q-mesh                              */
+/* ---------------------------------------------------------------------- */
+
+/* Options of Detector::AutoCorrelateSparseList (IAC/Detector.h:93). */
+typedef struct {
+    iac_mesh_shape shape;   /* big cubic mesh, CreateBigMeshForDetector */
+    int32_t interp_first;   /* FlagsFirstMap.InterpolationMode  */
+    int32_t interp_second;  /* FlagsSecondMap.InterpolationMode */
+    int32_t double_map;     /* DoubleMapping                    */
+    double multiplicator;   /* round(1/F_I_Conversion.Step) = 1000, IAC/Detector.cpp:1055-1057 */
+} iac_sparse_params;
+
+/* Number of uint64 words of the half mesh S*S*((S+1)/2) and full mesh S^3. */
+uint64_t iac_half_mesh_words(uint32_t size_ab);
+uint64_t iac_full_mesh_words(uint32_t size_ab);
+
+/* Batched device route of Detector::AutoCorrelateSparseList
+ * (IAC/Detector.cpp:1053-1146 + kernel Autocor_sparseHL, IAC/kernel.cl:451-652)
+ * for nframes frames at once.
+ *   d_photons       float4 (kx, ky, kz, count) per photon, frames concatenated
+ *                   (the SparseHitList layout, IAC/Detector.h:120)
+ *   d_frame_offsets nframes+1 photon offsets (uint64)
+ *   d_rot9          9 floats per frame, row-major HitEvent::RotMatrix
+ *                   (IAC/Settings.h:107)
+ *   d_half_mesh     accumulates the half mesh (ss >= 0) of the reference
+ *                   kernel, uint64[iac_half_mesh_words(S)]; not cleared.
+ * The call is asynchronous on `stream`.  It uses the context's scratch
+ * (work-queue counters and the per-frame tile table). */
+iac_status iac_sparse_ac_batch(iac_ctx *ctx, const float *d_photons,
+                               const uint64_t *d_frame_offsets, const float *d_rot9,
+                               uint32_t nframes, const iac_sparse_params *params,
+                               uint64_t *d_half_mesh, void *stream);
+
+/* Point reflection of the half mesh into the full mesh, the fold of
+ * IAC/Detector.cpp:1147-1170 (d_full += mirror(d_half)).  The reference folds
+ * after every frame through FloatToInt(half/Multiplicator); that map is the
+ * identity while a frame adds less than 1.05e7 to one half-mesh voxel, so one
+ * fold per batch gives the same mesh (see iac_sparse_ac_frames_host). */
+iac_status iac_sparse_fold(iac_ctx *ctx, const uint64_t *d_half_mesh, uint32_t size_ab,
+                           uint64_t *d_full_mesh, void *stream);
+
+/* End-to-end replacement for a loop of Detector::AutoCorrelateSparseList
+ * calls on host data (RunIAC per-frame loop, IAC/RunIAC.cpp:524-550):
+ * host photon lists in, h_full_mesh (uint64[S^3], ACMesh::Mesh layout)
+ * accumulated (+=) on return.  Synchronous. */
+iac_status iac_sparse_ac_frames_host(iac_ctx *ctx, const float *h_photons,
+                                     const uint64_t *h_frame_offsets, const float *h_rot9,
+                                     uint32_t nframes, const iac_sparse_params *params,
+                                     uint64_t *h_full_mesh);
+
+/* Work-queue tuning of the persistent pair kernel (see DESIGN.md of the
+ * project for the autotuner); zeros select the built-in defaults. */
+typedef struct {
+    uint32_t tile_pairs;      /* pairs per queue tile           */
+    uint32_t block_threads;   /* threads per CTA                */
+    uint32_t ctas_per_sm;     /* persistent CTAs per SM         */
+} iac_sparse_tuning;
+iac_status iac_sparse_set_tuning(iac_ctx *ctx, const iac_sparse_tuning *t);
+iac_status iac_sparse_get_tuning(iac_ctx *ctx, iac_sparse_tuning *t);
+
+/* ---------------------------------------------------------------------- */
+/* micro-benchmarks (roofline denominators)                                 */
+/* ---------------------------------------------------------------------- */
+
+/* Scattered 64-bit (or 32-bit) atomic adds into a buffer of `words` words:
+ * `updates` adds at pseudo-random addresses.  Used to measure the L2 atomic
+ * rate the pair kernels are bound by.  Asynchronous. */
+iac_status iac_bench_scatter_add(iac_ctx *ctx, void *d_buffer, uint64_t words, int word_bits,
+                                 uint64_t updates, uint32_t seed, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IAC_B200_H */

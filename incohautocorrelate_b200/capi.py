@@ -1,0 +1,237 @@
+"""ctypes binding of libiac_b200.so (the C ABI declared in include/iac_b200.h).
+
+This is the thin Python view of the C ABI used by the tests and by bench.py.
+It loads the in-tree shared library and fails loudly when it is missing:
+there is no Python or CPU fallback for any kernel.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libiac_b200.so")
+
+IAC_OK = 0
+IAC_ERR_INVALID_ARG = 1
+IAC_ERR_CUDA = 2
+IAC_ERR_NO_MEMORY = 3
+IAC_ERR_TIMEOUT = 4
+IAC_ERR_OUT_OF_MESH = 5
+IAC_ERR_UNSUPPORTED = 6
+
+NEAREST = 0
+LINEAR = 1
+
+
+class IacError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"iac status {status}: {message}")
+        self.status = status
+
+
+class MeshShape(C.Structure):
+    """ACMesh::MeshShape (IAC/ACMesh.h:21-29)."""
+    _fields_ = [("k_a", C.c_uint32), ("k_b", C.c_uint32), ("k_c", C.c_uint32),
+                ("size_ab", C.c_uint32), ("size_c", C.c_uint32),
+                ("center", C.c_uint32 * 3), ("dq_per_voxel", C.c_float),
+                ("voxel_per_dq", C.c_uint32), ("max_q", C.c_float)]
+
+    def as_dict(self):
+        return {"k": (self.k_a, self.k_b, self.k_c), "size_ab": self.size_ab,
+                "size_c": self.size_c, "center": tuple(self.center),
+                "dq_per_voxel": self.dq_per_voxel, "voxel_per_dq": self.voxel_per_dq,
+                "max_q": self.max_q}
+
+
+class AC1DShape(C.Structure):
+    _fields_ = [("size", C.c_uint32), ("max_q", C.c_float), ("dq_per_step", C.c_float)]
+
+
+class SparseParams(C.Structure):
+    _fields_ = [("shape", MeshShape), ("interp_first", C.c_int32),
+                ("interp_second", C.c_int32), ("double_map", C.c_int32),
+                ("multiplicator", C.c_double)]
+
+
+class SparseTuning(C.Structure):
+    _fields_ = [("tile_pairs", C.c_uint32), ("block_threads", C.c_uint32),
+                ("ctas_per_sm", C.c_uint32)]
+
+
+_lib = None
+_VP = C.c_void_p
+_U64 = C.c_uint64
+_U32 = C.c_uint32
+
+
+def _declare(lib):
+    def fn(name, args, res=C.c_int):
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+        return f
+
+    fn("iac_ctx_create", [C.c_int, C.POINTER(_VP)])
+    fn("iac_ctx_destroy", [_VP])
+    fn("iac_ctx_check", [_VP, _VP, C.POINTER(_U64)])
+    fn("iac_status_string", [C.c_int], C.c_char_p)
+    fn("iac_last_error", [], C.c_char_p)
+    fn("iac_abi_version", [], C.c_int)
+    fn("iac_ctx_launch_count", [_VP], _U64)
+    fn("iac_calc_kmap", [_VP, _VP, _U64, _VP, C.POINTER(C.c_float), _VP])
+    fn("iac_big_mesh_shape", [C.POINTER(C.c_float), C.c_int, C.c_float, C.POINTER(MeshShape)])
+    fn("iac_small_cq_mesh_shape", [C.POINTER(C.c_float), C.c_int, C.c_float,
+                                   C.POINTER(MeshShape)])
+    fn("iac_ac1d_shape_init", [C.POINTER(C.c_float), _U32, C.c_float, C.POINTER(AC1DShape)])
+    fn("iac_half_mesh_words", [_U32], _U64)
+    fn("iac_full_mesh_words", [_U32], _U64)
+    fn("iac_sparse_ac_batch", [_VP, _VP, _VP, _VP, _U32, C.POINTER(SparseParams), _VP, _VP])
+    fn("iac_sparse_fold", [_VP, _VP, _U32, _VP, _VP])
+    fn("iac_sparse_ac_frames_host", [_VP, _VP, _VP, _VP, _U32, C.POINTER(SparseParams), _VP])
+    fn("iac_sparse_set_tuning", [_VP, C.POINTER(SparseTuning)])
+    fn("iac_sparse_get_tuning", [_VP, C.POINTER(SparseTuning)])
+    fn("iac_bench_scatter_add", [_VP, _VP, _U64, C.c_int, _U64, _U32, _VP])
+    return lib
+
+
+def lib():
+    """The loaded library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `make -C incohautocorrelate_b200` "
+                "(or __graft_entry__.build()); there is no fallback implementation")
+        _lib = _declare(C.CDLL(LIB_PATH))
+    return _lib
+
+
+def check(status: int):
+    if status != IAC_OK:
+        L = lib()
+        raise IacError(status, (L.iac_last_error() or b"").decode() or
+                       L.iac_status_string(status).decode())
+    return status
+
+
+def _f3(v):
+    return (C.c_float * 3)(*[float(x) for x in v])
+
+
+def big_mesh_shape(max_q, edge_size: int, q_zoom: float = 1.0) -> MeshShape:
+    s = MeshShape()
+    check(lib().iac_big_mesh_shape(_f3(max_q), int(edge_size), float(q_zoom), C.byref(s)))
+    return s
+
+
+def small_cq_mesh_shape(max_q, perp_size: int, q_zoom: float = 1.0) -> MeshShape:
+    s = MeshShape()
+    check(lib().iac_small_cq_mesh_shape(_f3(max_q), int(perp_size), float(q_zoom), C.byref(s)))
+    return s
+
+
+def ac1d_shape(max_q, size: int, q_zoom: float = 1.0) -> AC1DShape:
+    s = AC1DShape()
+    check(lib().iac_ac1d_shape_init(_f3(max_q), int(size), float(q_zoom), C.byref(s)))
+    return s
+
+
+def half_mesh_words(S: int) -> int:
+    return int(lib().iac_half_mesh_words(S))
+
+
+def full_mesh_words(S: int) -> int:
+    return int(lib().iac_full_mesh_words(S))
+
+
+def sparse_params(shape: MeshShape, interp_first=NEAREST, interp_second=NEAREST,
+                  double_map=True, multiplicator=1000.0) -> SparseParams:
+    p = SparseParams()
+    p.shape = shape
+    p.interp_first = int(interp_first)
+    p.interp_second = int(interp_second)
+    p.double_map = int(bool(double_map))
+    p.multiplicator = float(multiplicator)
+    return p
+
+
+def _ptr(x):
+    """Device or host address of a torch tensor / numpy array / int."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if hasattr(x, "ctypes"):
+        return x.ctypes.data
+    raise TypeError(type(x))
+
+
+class Context:
+    """An iac_ctx on one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self._h = _VP()
+        check(lib().iac_ctx_create(int(device), C.byref(self._h)))
+        self.device = device
+
+    def close(self):
+        if self._h:
+            lib().iac_ctx_destroy(self._h)
+            self._h = _VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def launches(self) -> int:
+        return int(lib().iac_ctx_launch_count(self._h))
+
+    def check(self, stream=None) -> int:
+        """Synchronise and return the number of skipped out-of-mesh writes."""
+        oob = _U64(0)
+        st = lib().iac_ctx_check(self._h, _ptr(stream), C.byref(oob))
+        if st not in (IAC_OK, IAC_ERR_OUT_OF_MESH):
+            check(st)
+        return int(oob.value)
+
+    def calc_kmap(self, d_pixel_map, npix, d_kmap, stream=None):
+        mq = (C.c_float * 3)()
+        check(lib().iac_calc_kmap(self._h, _ptr(d_pixel_map), int(npix), _ptr(d_kmap), mq,
+                                  _ptr(stream)))
+        return [mq[0], mq[1], mq[2]]
+
+    def sparse_ac_batch(self, d_photons, d_offsets, d_rot, nframes, params, d_half, stream=None):
+        check(lib().iac_sparse_ac_batch(self._h, _ptr(d_photons), _ptr(d_offsets), _ptr(d_rot),
+                                        int(nframes), C.byref(params), _ptr(d_half),
+                                        _ptr(stream)))
+
+    def sparse_fold(self, d_half, S, d_full, stream=None):
+        check(lib().iac_sparse_fold(self._h, _ptr(d_half), int(S), _ptr(d_full), _ptr(stream)))
+
+    def sparse_ac_frames_host(self, h_photons, h_offsets, h_rot, nframes, params, h_full):
+        check(lib().iac_sparse_ac_frames_host(self._h, _ptr(h_photons), _ptr(h_offsets),
+                                              _ptr(h_rot), int(nframes), C.byref(params),
+                                              _ptr(h_full)))
+
+    def set_sparse_tuning(self, tile_pairs=0, block_threads=0, ctas_per_sm=0):
+        t = SparseTuning(int(tile_pairs), int(block_threads), int(ctas_per_sm))
+        check(lib().iac_sparse_set_tuning(self._h, C.byref(t)))
+
+    def sparse_tuning(self):
+        t = SparseTuning()
+        check(lib().iac_sparse_get_tuning(self._h, C.byref(t)))
+        return {"tile_pairs": t.tile_pairs, "block_threads": t.block_threads,
+                "ctas_per_sm": t.ctas_per_sm}
+
+    def bench_scatter_add(self, d_buf, words, word_bits, updates, seed=1, stream=None):
+        check(lib().iac_bench_scatter_add(self._h, _ptr(d_buf), int(words), int(word_bits),
+                                          int(updates), int(seed), _ptr(stream)))

@@ -1,0 +1,321 @@
+// ctx.cu -- context, error reporting, mesh geometry, k-map and the
+// scatter-add micro-benchmark of libiac_b200.
+#include <cmath>
+#include <cstdarg>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "iac_internal.cuh"
+
+namespace iac {
+
+static thread_local char g_last_error[512] = "";
+
+void set_error(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_last_error, sizeof g_last_error, fmt, ap);
+    va_end(ap);
+}
+
+iac_status Scratch::ensure(size_t need)
+{
+    if (need <= bytes) return IAC_OK;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    size_t grow = need + need / 4 + 4096;
+    IAC_CUDA(cudaMalloc(&ptr, grow));
+    bytes = grow;
+    return IAC_OK;
+}
+
+void Scratch::release()
+{
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+}  // namespace iac
+
+using namespace iac;
+
+extern "C" {
+
+const char *iac_status_string(iac_status s)
+{
+    switch (s) {
+    case IAC_OK: return "ok";
+    case IAC_ERR_INVALID_ARG: return "invalid argument";
+    case IAC_ERR_CUDA: return "CUDA error";
+    case IAC_ERR_NO_MEMORY: return "out of memory";
+    case IAC_ERR_TIMEOUT: return "device wait timed out";
+    case IAC_ERR_OUT_OF_MESH: return "writes outside the mesh were skipped";
+    case IAC_ERR_UNSUPPORTED: return "unsupported";
+    }
+    return "unknown status";
+}
+
+const char *iac_last_error(void) { return g_last_error; }
+
+int iac_abi_version(void) { return IAC_ABI_VERSION; }
+
+iac_status iac_ctx_create(int device, iac_ctx **out)
+{
+    IAC_REQUIRE(out != nullptr, "iac_ctx_create: out is NULL");
+    *out = nullptr;
+    int n = 0;
+    IAC_CUDA(cudaGetDeviceCount(&n));
+    IAC_REQUIRE(device >= 0 && device < n, "iac_ctx_create: device %d of %d", device, n);
+    cudaDeviceProp prop;
+    IAC_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) {
+        set_error("iac_ctx_create: device %d is sm_%d%d; this library is built for sm_100a",
+                  device, prop.major, prop.minor);
+        return IAC_ERR_UNSUPPORTED;
+    }
+    DeviceGuard g(device);
+    iac_ctx *c = new iac_ctx();
+    c->device = device;
+    c->sm_count = prop.multiProcessorCount;
+    c->cc_major = prop.major;
+    c->cc_minor = prop.minor;
+    cudaError_t e = cudaMalloc(&c->d_counters, sizeof(DeviceCounters));
+    if (e != cudaSuccess) {
+        delete c;
+        set_error("iac_ctx_create: %s", cudaGetErrorString(e));
+        return IAC_ERR_NO_MEMORY;
+    }
+    cudaMemset(c->d_counters, 0, sizeof(DeviceCounters));
+    cudaDeviceSynchronize();
+    *out = c;
+    return IAC_OK;
+}
+
+iac_status iac_ctx_destroy(iac_ctx *ctx)
+{
+    if (!ctx) return IAC_OK;
+    {
+        DeviceGuard g(ctx->device);
+        cudaDeviceSynchronize();
+        ctx->sparse_scratch.release();
+        for (auto &kv : ctx->stream_scratch) {
+            for (auto &s : kv.second.bufs) s.release();
+        }
+        if (ctx->d_counters) cudaFree(ctx->d_counters);
+    }
+    delete ctx;
+    return IAC_OK;
+}
+
+iac_status iac_ctx_check(iac_ctx *ctx, void *stream, uint64_t *out_of_mesh)
+{
+    IAC_REQUIRE(ctx != nullptr, "iac_ctx_check: ctx is NULL");
+    DeviceGuard g(ctx->device);
+    IAC_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    DeviceCounters h;
+    IAC_CUDA(cudaMemcpy(&h, ctx->d_counters, sizeof h, cudaMemcpyDeviceToHost));
+    IAC_CUDA(cudaMemset(ctx->d_counters, 0, sizeof h));
+    if (out_of_mesh) *out_of_mesh = h.out_of_mesh;
+    if (h.timeouts) {
+        set_error("%llu bounded device waits ran out", (unsigned long long)h.timeouts);
+        return IAC_ERR_TIMEOUT;
+    }
+    if (h.out_of_mesh) {
+        set_error("%llu writes fell outside the mesh and were skipped",
+                  (unsigned long long)h.out_of_mesh);
+        return IAC_ERR_OUT_OF_MESH;
+    }
+    return IAC_OK;
+}
+
+uint64_t iac_ctx_launch_count(const iac_ctx *ctx)
+{
+    return ctx ? ctx->launches.load(std::memory_order_relaxed) : 0;
+}
+
+// ---------------------------------------------------------------------------
+// mesh geometry (host arithmetic in the reference's float order)
+// ---------------------------------------------------------------------------
+
+static void mesh_pitch(iac_mesh_shape *s, float maxq)
+{
+    s->max_q = maxq;
+    s->dq_per_voxel = maxq / (float)(((s->size_ab - 1) / 2) - 2);
+    s->voxel_per_dq = (uint32_t)std::floor(1.0f / s->dq_per_voxel);
+    s->dq_per_voxel = 1.0f / ((float)s->voxel_per_dq);
+}
+
+iac_status iac_big_mesh_shape(const float mq[3], int edge, float q_zoom, iac_mesh_shape *s)
+{
+    IAC_REQUIRE(mq && s, "iac_big_mesh_shape: NULL argument");
+    IAC_REQUIRE(edge % 2 != 0, "Meshsize must be odd for each dimension (got %d)", edge);
+    IAC_REQUIRE(edge >= 5, "mesh edge %d too small", edge);
+    s->k_a = 0;
+    s->k_b = 1;
+    s->k_c = 2;
+    s->size_ab = (uint32_t)edge + 2;
+    s->size_c = s->size_ab;
+    s->center[0] = s->center[1] = (s->size_ab - 1) / 2;
+    s->center[2] = (s->size_c - 1) / 2;
+    float m = std::max(std::max(mq[0], mq[1]), mq[2]);
+    mesh_pitch(s, m / q_zoom);
+    return IAC_OK;
+}
+
+iac_status iac_small_cq_mesh_shape(const float mq[3], int perp, float q_zoom, iac_mesh_shape *s)
+{
+    IAC_REQUIRE(mq && s, "iac_small_cq_mesh_shape: NULL argument");
+    IAC_REQUIRE(perp % 2 != 0, "Meshsize must be odd for each dimension (got %d)", perp);
+    IAC_REQUIRE(perp >= 5, "mesh edge %d too small", perp);
+    uint32_t a = 0, b = 1, c = 2;
+    if (mq[b] > mq[a]) std::swap(a, b);
+    if (mq[c] > mq[b]) std::swap(c, b);
+    if (mq[b] > mq[a]) std::swap(a, b);
+    s->k_a = a;
+    s->k_b = b;
+    s->k_c = c;
+    s->size_ab = (uint32_t)perp + 2;
+    if (q_zoom == 1.0f)
+        s->size_c = (uint32_t)(int)std::floor((double)((mq[c] / mq[a]) * (float)perp) + 2.5);
+    else
+        s->size_c = s->size_ab;
+    if (s->size_c % 2 == 0) s->size_c += 1;
+    s->center[0] = s->center[1] = (s->size_ab - 1) / 2;
+    s->center[2] = (s->size_c - 1) / 2;
+    mesh_pitch(s, mq[a] / q_zoom);
+    return IAC_OK;
+}
+
+iac_status iac_ac1d_shape_init(const float mq[3], uint32_t size, float q_zoom, iac_ac1d_shape *s)
+{
+    IAC_REQUIRE(mq && s, "iac_ac1d_shape_init: NULL argument");
+    IAC_REQUIRE(size >= 3, "AC1D array size %u too small", size);
+    s->size = size;
+    s->max_q = std::sqrt(mq[0] * mq[0] + mq[1] * mq[1] + mq[2] * mq[2]) / q_zoom;
+    s->dq_per_step = s->max_q / ((float)(size - 2));
+    return IAC_OK;
+}
+
+uint64_t iac_half_mesh_words(uint32_t S) { return (uint64_t)S * S * ((S + 1) / 2); }
+uint64_t iac_full_mesh_words(uint32_t S) { return (uint64_t)S * S * S; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// k-map: unit vectors and the per-block extent of each axis
+// ---------------------------------------------------------------------------
+__global__ void kmap_kernel(const float *__restrict__ pm, uint64_t npix, float *__restrict__ km,
+                            float *__restrict__ block_ext)
+{
+    float mx[3] = {-100.0f, -100.0f, -100.0f}, mn[3] = {100.0f, 100.0f, 100.0f};
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < npix;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        float x = pm[3 * i], y = pm[3 * i + 1], z = pm[3 * i + 2];
+        float r = norm3(x, y, z);
+        float k[3] = {__fdiv_rn(x, r), __fdiv_rn(y, r), __fdiv_rn(z, r)};
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            km[3 * i + d] = k[d];
+            mx[d] = fmaxf(mx[d], k[d]);
+            mn[d] = fminf(mn[d], k[d]);
+        }
+    }
+    __shared__ float s[6][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        for (int o = 16; o; o >>= 1) {
+            mx[d] = fmaxf(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+            mn[d] = fminf(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+        }
+    }
+    if (lane == 0)
+        for (int d = 0; d < 3; d++) {
+            s[d][w] = mx[d];
+            s[3 + d][w] = mn[d];
+        }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int nw = blockDim.x >> 5;
+        float v = s[threadIdx.x][0];
+        for (int j = 1; j < nw; j++)
+            v = threadIdx.x < 3 ? fmaxf(v, s[threadIdx.x][j]) : fminf(v, s[threadIdx.x][j]);
+        block_ext[6 * blockIdx.x + threadIdx.x] = v;
+    }
+}
+
+extern "C" iac_status iac_calc_kmap(iac_ctx *ctx, const float *d_pm, uint64_t npix, float *d_km,
+                                    float max_q[3], void *stream)
+{
+    IAC_REQUIRE(ctx && d_pm && d_km && max_q, "iac_calc_kmap: NULL argument");
+    IAC_REQUIRE(npix > 0, "iac_calc_kmap: empty pixel map");
+    DeviceGuard g(ctx->device);
+    const int threads = 256;
+    int blocks = (int)std::min<uint64_t>((npix + threads - 1) / threads, 4 * (uint64_t)ctx->sm_count);
+    float *d_ext = nullptr;
+    IAC_CUDA(cudaMallocAsync(&d_ext, sizeof(float) * 6 * blocks, as_stream(stream)));
+    kmap_kernel<<<blocks, threads, 0, as_stream(stream)>>>(d_pm, npix, d_km, d_ext);
+    IAC_LAUNCHED(ctx);
+    IAC_CUDA(cudaGetLastError());
+    std::vector<float> ext(6 * (size_t)blocks);
+    IAC_CUDA(cudaMemcpyAsync(ext.data(), d_ext, sizeof(float) * ext.size(), cudaMemcpyDeviceToHost,
+                             as_stream(stream)));
+    IAC_CUDA(cudaFreeAsync(d_ext, as_stream(stream)));
+    IAC_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    float mx[3] = {-100.0f, -100.0f, -100.0f}, mn[3] = {100.0f, 100.0f, 100.0f};
+    for (int b = 0; b < blocks; b++)
+        for (int d = 0; d < 3; d++) {
+            mx[d] = std::max(mx[d], ext[6 * b + d]);
+            mn[d] = std::min(mn[d], ext[6 * b + 3 + d]);
+        }
+    for (int d = 0; d < 3; d++) max_q[d] = std::fabs(mx[d] - mn[d]);
+    return IAC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// scatter-add micro-benchmark: the L2 atomic rate that bounds the binning
+// kernels (addresses from a 64-bit mix of the update index)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t mix64(uint64_t x)
+{
+    x ^= x >> 30;
+    x *= 0xbf58476d1ce4e5b9ull;
+    x ^= x >> 27;
+    x *= 0x94d049bb133111ebull;
+    x ^= x >> 31;
+    return x;
+}
+
+template <typename T>
+__global__ void scatter_add_kernel(T *__restrict__ buf, uint64_t words, uint64_t updates, uint32_t seed)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < updates; u += stride) {
+        uint64_t h = mix64(u ^ ((uint64_t)seed << 40));
+        atomicAdd(&buf[h % words], (T)1);
+    }
+}
+
+extern "C" iac_status iac_bench_scatter_add(iac_ctx *ctx, void *d_buffer, uint64_t words,
+                                            int word_bits, uint64_t updates, uint32_t seed,
+                                            void *stream)
+{
+    IAC_REQUIRE(ctx && d_buffer && words > 0, "iac_bench_scatter_add: bad argument");
+    IAC_REQUIRE(word_bits == 32 || word_bits == 64, "word_bits must be 32 or 64");
+    DeviceGuard g(ctx->device);
+    const int threads = 256;
+    const int blocks = ctx->sm_count * 8;
+    if (word_bits == 64)
+        scatter_add_kernel<unsigned long long><<<blocks, threads, 0, as_stream(stream)>>>(
+            (unsigned long long *)d_buffer, words, updates, seed);
+    else
+        scatter_add_kernel<unsigned int><<<blocks, threads, 0, as_stream(stream)>>>(
+            (unsigned int *)d_buffer, words, updates, seed);
+    IAC_LAUNCHED(ctx);
+    IAC_CUDA(cudaGetLastError());
+    return IAC_OK;
+}

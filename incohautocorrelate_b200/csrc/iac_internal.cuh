@@ -1,0 +1,148 @@
+// iac_internal.cuh -- shared internals of libiac_b200 (context, errors,
+// scratch memory, exact-arithmetic helpers).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+
+#include "../../include/iac_b200.h"
+
+namespace iac {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+void set_error(const char *fmt, ...);
+
+#define IAC_CUDA(call)                                                              \
+    do {                                                                            \
+        cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess) {                                                    \
+            ::iac::set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                             __FILE__, __LINE__);                                   \
+            return e_ == cudaErrorMemoryAllocation ? IAC_ERR_NO_MEMORY : IAC_ERR_CUDA; \
+        }                                                                           \
+    } while (0)
+
+#define IAC_REQUIRE(cond, ...)               \
+    do {                                     \
+        if (!(cond)) {                       \
+            ::iac::set_error(__VA_ARGS__);   \
+            return IAC_ERR_INVALID_ARG;      \
+        }                                    \
+    } while (0)
+
+#define IAC_LAUNCHED(ctx) ((ctx)->launches.fetch_add(1, std::memory_order_relaxed))
+
+// ---------------------------------------------------------------------------
+// device-side error counters, one block per context
+// ---------------------------------------------------------------------------
+struct DeviceCounters {
+    unsigned long long out_of_mesh;
+    unsigned long long timeouts;
+    unsigned long long pad[6];
+};
+
+// A growable device scratch buffer owned by the context.
+struct Scratch {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    iac_status ensure(size_t need);
+    void release();
+};
+
+// Per-stream scratch slots, so that host threads working on their own streams
+// never share a work queue or a staging buffer.
+enum ScratchSlot {
+    SLOT_TILES = 0,   // sparse: per-frame tile table + queue counter
+    SLOT_PHOTONS,     // host-buffer entry points: staged inputs / outputs
+    SLOT_OFFSETS,
+    SLOT_ROT,
+    SLOT_HALF,
+    SLOT_FULL,
+    SLOT_AUX0,
+    SLOT_AUX1,
+    SLOT_COUNT
+};
+struct StreamScratch {
+    Scratch bufs[SLOT_COUNT];
+};
+
+}  // namespace iac
+
+struct iac_ctx {
+    int device = 0;
+    int sm_count = 0;
+    int cc_major = 0, cc_minor = 0;
+    std::mutex mu;  // guards scratch growth and tuning
+    iac::DeviceCounters *d_counters = nullptr;
+    iac::Scratch sparse_scratch;
+    std::unordered_map<void *, iac::StreamScratch> stream_scratch;  // keyed by stream
+    iac_sparse_tuning tuning{};
+    cudaStream_t host_stream = nullptr;  // stream of the host-buffer entry points
+    std::atomic<uint64_t> launches{0};
+};
+
+namespace iac {
+
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Scratch slot `slot` of `stream`, grown to at least `bytes`.
+inline iac_status stream_scratch(iac_ctx *ctx, void *stream, int slot, size_t bytes, void **out)
+{
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    Scratch &s = ctx->stream_scratch[stream].bufs[slot];
+    iac_status st = s.ensure(bytes);
+    *out = s.ptr;
+    return st;
+}
+
+// RAII guard that makes the context's device current for the calling thread.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// exact arithmetic: every operation explicitly rounded, never contracted
+// into a fused multiply-add, in the reference's operation order.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+
+// |q| as sqrt(q0*q0 + q1*q1 + q2*q2), left to right, IEEE sqrt.
+__device__ __forceinline__ float norm3(float q0, float q1, float q2)
+{
+    return __fsqrt_rn(fadd(fadd(fmul(q0, q0), fmul(q1, q1)), fmul(q2, q2)));
+}
+
+// Row-major M*v as q0*R0 + q1*R1 + q2*R2 (ArrayOperators::Rotate order).
+__device__ __forceinline__ float rot_row(float a, float b, float c, float r0, float r1, float r2)
+{
+    return fadd(fadd(fmul(a, r0), fmul(b, r1)), fmul(c, r2));
+}
+
+// C cast (unsigned long)(double) for the non-negative values of the path.
+__device__ __forceinline__ unsigned long long d2u64(double x) { return __double2ull_rz(x); }
+
+}  // namespace iac

@@ -1,0 +1,514 @@
+// sparse_ac.cu -- (a) sparse photon pairs -> uint64 3D q-mesh.
+//
+// Replaces the device route of Detector::AutoCorrelateSparseList
+// (IAC/Detector.cpp:1053-1181) and its kernel Autocor_sparseHL with helpers
+// AddRotatedQToMesh / AddQToPositiveSS (IAC/kernel.cl:349-652), batched over
+// many frames.
+//
+// Work decomposition.  A frame of n photons has n(n-1)/2 distinct pairs plus
+// n self pairs.  The planner (one CTA) gives every frame
+// max(1, ceil(pairs / tile_pairs)) tiles and writes the exclusive prefix sum of
+// those counts: the device work queue.  The pair kernel is persistent: each
+// CTA pops the next tile index with one atomic, finds its frame by binary
+// search over the prefix table and walks the tile's pairs, one pair per thread
+// per step.  Frames of 5 or 2 500 photons therefore cost in proportion to their
+// pair count, and no CTA waits on another.
+//
+// Pair enumeration.  Local pair l of a frame maps to
+//   d = l / n + 1,  i = l % n,  j = (i + d) mod n
+// which lists every unordered pair {i, j}, i != j, exactly once for l in
+// [0, n(n-1)/2) (a circulant walk: offsets d = 1 .. floor((n-1)/2) for every
+// i, plus d = n/2 for i < n/2 when n is even).  Consecutive threads take
+// consecutive i at the same offset d, so their photon loads are contiguous.
+// The pair is then evaluated exactly as the reference's work item does for
+// ind = min(i, j) and i = max(i, j): q = k_lo - k_hi.
+//
+// Exactness.  All float operations are the reference's, in its order, as
+// explicitly rounded intrinsics (no contraction into FMA); sqrt is IEEE; the
+// value (double)v_lo * v_hi * Multiplicator is truncated to uint64 as the C
+// cast does.  Self pairs add (uint64)(v*v*Mult) at q = 0, which the reference
+// writes to half-mesh voxel (C, C, 0) without a mirror for every second-level
+// interpolation mode; they are summed per tile and added with one atomic.
+//
+// The half mesh accumulates with 64-bit atomic adds in L2 (the 201^3 half mesh
+// is 32.6 MB and stays L2-resident).  Writes whose voxel would fall outside the
+// mesh (possible only for non-orthonormal rotations; the reference writes them
+// out of bounds) are skipped and counted in the context's error block.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "iac_internal.cuh"
+
+namespace iac {
+
+struct SparseArgs {
+    const float4 *__restrict__ photons;
+    const uint64_t *__restrict__ offsets;
+    const float *__restrict__ rot;
+    const unsigned long long *__restrict__ tile_off;  // nframes + 1
+    unsigned long long *__restrict__ half;
+    unsigned long long *queue;
+    DeviceCounters *counters;
+    uint32_t nframes;
+    uint32_t tile_pairs;
+    int S, C, half_ss;
+    float maxq;
+    float vpdq;  // (float)Voxel_per_dq
+    double mult;
+};
+
+// ---------------------------------------------------------------------------
+// planner: tiles per frame, exclusive scan, queue reset (one CTA)
+// ---------------------------------------------------------------------------
+constexpr int PLAN_THREADS = 1024;
+
+__device__ __forceinline__ unsigned long long frame_tiles(const uint64_t *off, uint32_t f,
+                                                          uint32_t tile_pairs)
+{
+    const unsigned long long n = off[f + 1] - off[f];
+    if (n == 0) return 0;
+    const unsigned long long pairs = n * (n - 1) / 2;
+    const unsigned long long t = (pairs + tile_pairs - 1) / tile_pairs;
+    return t > 0 ? t : 1;
+}
+
+__global__ void __launch_bounds__(PLAN_THREADS)
+    sparse_plan_kernel(const uint64_t *__restrict__ off, uint32_t nframes, uint32_t tile_pairs,
+                       unsigned long long *__restrict__ tile_off, unsigned long long *queue)
+{
+    __shared__ unsigned long long warp_sums[PLAN_THREADS / 32];
+    const uint32_t tid = threadIdx.x;
+    const uint32_t chunk = (nframes + PLAN_THREADS - 1) / PLAN_THREADS;
+    const uint32_t f0 = min(nframes, tid * chunk), f1 = min(nframes, f0 + chunk);
+    unsigned long long local = 0;
+    for (uint32_t f = f0; f < f1; f++) local += frame_tiles(off, f, tile_pairs);
+    // block-wide exclusive scan of the per-thread sums
+    const int lane = tid & 31, w = tid >> 5;
+    unsigned long long incl = local;
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned long long v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) warp_sums[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        unsigned long long v = warp_sums[lane];
+        unsigned long long s = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned long long u = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += u;
+        }
+        warp_sums[lane] = s - v;  // exclusive warp prefix
+    }
+    __syncthreads();
+    unsigned long long run = warp_sums[w] + incl - local;
+    for (uint32_t f = f0; f < f1; f++) {
+        tile_off[f] = run;
+        run += frame_tiles(off, f, tile_pairs);
+    }
+    if (tid == PLAN_THREADS - 1) {
+        tile_off[nframes] = warp_sums[w] + incl;
+        *queue = 0ull;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// binning helpers (IAC/kernel.cl:349-448)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void hm_put(const SparseArgs &a, int fs, int ms, int ss,
+                                       unsigned long long v)
+{
+    if ((unsigned)fs >= (unsigned)a.S || (unsigned)ms >= (unsigned)a.S ||
+        (unsigned)ss >= (unsigned)a.half_ss) {
+        atomicAdd(&a.counters->out_of_mesh, 1ull);
+        return;
+    }
+    if (v == 0) return;
+    atomicAdd(&a.half[(size_t)fs + (size_t)ms * a.S + (size_t)ss * a.S * a.S], v);
+}
+
+// AddQToPositiveSS, IAC/kernel.cl:349-372 (q != 0 here; q = 0 is the self pair)
+__device__ __forceinline__ void add_positive_ss(const SparseArgs &a, int fs, int ms, int ss,
+                                                unsigned long long v)
+{
+    if (ss > 0) {
+        hm_put(a, fs, ms, ss, v);
+    } else {
+        if (ss == 0) hm_put(a, fs, ms, ss, v);
+        hm_put(a, 2 * a.C - fs, 2 * a.C - ms, -ss, v);
+    }
+}
+
+// AddRotatedQToMesh, IAC/kernel.cl:374-448
+template <int I2>
+__device__ __forceinline__ void add_rotated(const SparseArgs &a, double val, float q0, float q1,
+                                            float q2)
+{
+    const float Cf = (float)a.C;
+    if (I2 == 0) {
+        const unsigned long long v = d2u64(dmul(val, a.mult));
+        const int fs = (int)fadd(Cf, roundf(q0));
+        const int ms = (int)fadd(Cf, roundf(q1));
+        const int ss = (int)roundf(q2);
+        add_positive_ss(a, fs, ms, ss, v);
+    } else {
+        const float f0 = floorf(q0), f1 = floorf(q1), f2 = floorf(q2);
+        const double sf = dsub(1.0, (double)fsub(q0, f0));
+        const double sm = dsub(1.0, (double)fsub(q1, f1));
+        const double sz = dsub(1.0, (double)fsub(q2, f2));
+        const int fs = (int)fadd(Cf, f0), ms = (int)fadd(Cf, f1), ss = (int)f2;
+        const double tm = dmul(val, a.mult);
+        const double xf[2] = {sf, dsub(1.0, sf)}, yf[2] = {sm, dsub(1.0, sm)},
+                     zf[2] = {sz, dsub(1.0, sz)};
+#pragma unroll
+        for (int cz = 0; cz < 2; cz++)
+#pragma unroll
+            for (int cy = 0; cy < 2; cy++)
+#pragma unroll
+                for (int cx = 0; cx < 2; cx++) {
+                    const double w = dmul(dmul(xf[cx], yf[cy]), zf[cz]);
+                    add_positive_ss(a, fs + cx, ms + cy, ss + cz, d2u64(dmul(tm, w)));
+                }
+    }
+}
+
+// One distinct pair, the body of the reference's loop for i > ind
+// (IAC/kernel.cl:493-649).
+template <int DMAP, int I1, int I2>
+__device__ __forceinline__ void bin_pair(const SparseArgs &a, const float4 A, const float4 B,
+                                         const float *R)
+{
+    float q0 = fsub(A.x, B.x), q1 = fsub(A.y, B.y), q2 = fsub(A.z, B.z);
+    if (norm3(q0, q1, q2) > a.maxq) return;
+    q0 = fmul(q0, a.vpdq);
+    q1 = fmul(q1, a.vpdq);
+    q2 = fmul(q2, a.vpdq);
+    const double val = dmul((double)A.w, (double)B.w);
+    const int C = a.C;
+    const float Cf = (float)C;
+    if (DMAP) {
+        if (I1 == 0) {
+            const int fs = (int)fadd(roundf(q0), Cf);
+            const int ms = (int)fadd(roundf(q1), Cf);
+            const int ss = (int)fadd(roundf(q2), Cf);
+            const float r0 = (float)(fs - C), r1 = (float)(ms - C), r2 = (float)(ss - C);
+            add_rotated<I2>(a, val, rot_row(r0, r1, r2, R[0], R[1], R[2]),
+                            rot_row(r0, r1, r2, R[3], R[4], R[5]),
+                            rot_row(r0, r1, r2, R[6], R[7], R[8]));
+        } else {
+            const float f0 = floorf(q0), f1 = floorf(q1), f2 = floorf(q2);
+            const double sf = dsub(1.0, (double)fsub(q0, f0));
+            const double sm = dsub(1.0, (double)fsub(q1, f1));
+            const double sz = dsub(1.0, (double)fsub(q2, f2));
+            const int fs = (int)fadd(Cf, f0), ms = (int)fadd(Cf, f1), ss = (int)fadd(Cf, f2);
+            const float base = (float)val;
+            const double xf[2] = {sf, dsub(1.0, sf)}, yf[2] = {sm, dsub(1.0, sm)},
+                         zf[2] = {sz, dsub(1.0, sz)};
+#pragma unroll
+            for (int cz = 0; cz < 2; cz++)
+#pragma unroll
+                for (int cy = 0; cy < 2; cy++)
+#pragma unroll
+                    for (int cx = 0; cx < 2; cx++) {
+                        const float tv =
+                            (float)dmul((double)base, dmul(dmul(xf[cx], yf[cy]), zf[cz]));
+                        const float r0 = (float)((fs + cx) - C), r1 = (float)((ms + cy) - C),
+                                    r2 = (float)((ss + cz) - C);
+                        add_rotated<I2>(a, (double)tv, rot_row(r0, r1, r2, R[0], R[1], R[2]),
+                                        rot_row(r0, r1, r2, R[3], R[4], R[5]),
+                                        rot_row(r0, r1, r2, R[6], R[7], R[8]));
+                    }
+        }
+    } else {
+        add_rotated<I2>(a, val, rot_row(q0, q1, q2, R[0], R[1], R[2]),
+                        rot_row(q0, q1, q2, R[3], R[4], R[5]),
+                        rot_row(q0, q1, q2, R[6], R[7], R[8]));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// persistent pair kernel
+// ---------------------------------------------------------------------------
+template <int DMAP, int I1, int I2>
+__global__ void __launch_bounds__(256) sparse_pairs_kernel(const SparseArgs a)
+{
+    __shared__ unsigned long long s_tile;
+    __shared__ uint32_t s_frame;
+    __shared__ float s_rot[9];
+    __shared__ unsigned long long s_self[8];
+
+    const unsigned long long ntiles = a.tile_off[a.nframes];
+    const uint32_t nthr = blockDim.x;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const unsigned long long t = atomicAdd(a.queue, 1ull);
+            s_tile = t;
+            if (t < ntiles) {
+                // last frame f with tile_off[f] <= t
+                uint32_t lo = 0, hi = a.nframes;  // tile_off[lo] <= t < tile_off[hi]
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (a.tile_off[mid] <= t)
+                        lo = mid;
+                    else
+                        hi = mid;
+                }
+                s_frame = lo;
+#pragma unroll
+                for (int k = 0; k < 9; k++) s_rot[k] = a.rot[9 * (size_t)lo + k];
+            }
+        }
+        __syncthreads();
+        const unsigned long long t = s_tile;
+        if (t >= ntiles) break;
+        const uint32_t f = s_frame;
+        float R[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) R[k] = s_rot[k];
+        const uint64_t base = a.offsets[f];
+        const uint32_t n = (uint32_t)(a.offsets[f + 1] - base);
+        const unsigned long long chunk = t - a.tile_off[f];
+        const float4 *__restrict__ P = a.photons + base;
+
+        // self pairs (q = 0): once per frame, on its first tile
+        if (chunk == 0) {
+            unsigned long long s = 0;
+            for (uint32_t i = threadIdx.x; i < n; i += nthr) {
+                const double v = (double)P[i].w;
+                s += d2u64(dmul(dmul(v, v), a.mult));
+            }
+            for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if ((threadIdx.x & 31) == 0) s_self[threadIdx.x >> 5] = s;
+        }
+
+        // distinct pairs of this tile
+        const unsigned long long npairs = (unsigned long long)n * (n - 1) / 2;
+        const unsigned long long p0 = chunk * a.tile_pairs;
+        const unsigned long long p1 = min(npairs, p0 + a.tile_pairs);
+        if (p0 + threadIdx.x < p1) {
+            unsigned long long l = p0 + threadIdx.x;
+            uint32_t d = (uint32_t)(l / n) + 1;
+            uint32_t i = (uint32_t)(l - (unsigned long long)(d - 1) * n);
+            const uint32_t dq = nthr / n, dr = nthr % n;
+            for (; l < p1; l += nthr) {
+                uint32_t j = i + d;
+                if (j >= n) j -= n;
+                const uint32_t lo = min(i, j), hi = max(i, j);
+                bin_pair<DMAP, I1, I2>(a, P[lo], P[hi], R);
+                i += dr;
+                d += dq;
+                if (i >= n) {
+                    i -= n;
+                    d += 1;
+                }
+            }
+        }
+        __syncthreads();
+        if (chunk == 0 && threadIdx.x == 0) {
+            unsigned long long s = 0;
+            for (uint32_t w = 0; w < (nthr + 31) / 32; w++) s += s_self[w];
+            if (s) atomicAdd(&a.half[(size_t)a.C + (size_t)a.C * a.S], s);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// fold: full[fs, ms, ss + C] += half; full[2C - fs, 2C - ms, C - ss] += half
+// for ss > 0 (IAC/Detector.cpp:1147-1170).  Every full-mesh voxel receives
+// exactly one half-mesh voxel, so plain read-modify-write suffices.
+// ---------------------------------------------------------------------------
+__global__ void sparse_fold_kernel(const unsigned long long *__restrict__ half, uint32_t S,
+                                   unsigned long long *__restrict__ full)
+{
+    const uint32_t C = (S - 1) / 2;
+    const uint64_t plane = (uint64_t)S * S;
+    const uint64_t total = plane * ((S + 1) / 2);
+    for (uint64_t h = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; h < total;
+         h += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t ss = (uint32_t)(h / plane);
+        const uint32_t rem = (uint32_t)(h - (uint64_t)ss * plane);
+        const uint32_t ms = rem / S, fs = rem - ms * S;
+        const unsigned long long v = half[h];
+        if (v == 0) continue;
+        full[fs + (uint64_t)ms * S + (uint64_t)(ss + C) * plane] += v;
+        if (ss != 0) full[(2 * C - fs) + (uint64_t)(2 * C - ms) * S + (uint64_t)(C - ss) * plane] += v;
+    }
+}
+
+typedef void (*PairKernel)(const SparseArgs);
+
+static PairKernel pick_kernel(int dmap, int i1, int i2)
+{
+    if (!dmap) return i2 ? sparse_pairs_kernel<0, 0, 1> : sparse_pairs_kernel<0, 0, 0>;
+    if (i1 == 0) return i2 ? sparse_pairs_kernel<1, 0, 1> : sparse_pairs_kernel<1, 0, 0>;
+    return i2 ? sparse_pairs_kernel<1, 1, 1> : sparse_pairs_kernel<1, 1, 0>;
+}
+
+static iac_sparse_tuning effective_tuning(iac_ctx *ctx)
+{
+    iac_sparse_tuning t;
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        t = ctx->tuning;
+    }
+    if (t.tile_pairs == 0) t.tile_pairs = 4096;
+    if (t.block_threads == 0) t.block_threads = 256;
+    if (t.ctas_per_sm == 0) t.ctas_per_sm = 8;
+    return t;
+}
+
+static iac_status check_params(const iac_sparse_params *p)
+{
+    IAC_REQUIRE(p != nullptr, "sparse params are NULL");
+    const iac_mesh_shape &s = p->shape;
+    IAC_REQUIRE(s.size_ab >= 5 && (s.size_ab % 2) == 1 && s.size_c == s.size_ab,
+                "sparse pair mesh must be cubic with an odd edge (got %u x %u)", s.size_ab, s.size_c);
+    IAC_REQUIRE(s.size_ab <= 2047, "mesh edge %u too large", s.size_ab);
+    IAC_REQUIRE(s.voxel_per_dq > 0, "Voxel_per_dq is 0");
+    IAC_REQUIRE(p->interp_first == 0 || p->interp_first == 1, "interp_first must be 0 or 1");
+    IAC_REQUIRE(p->interp_second == 0 || p->interp_second == 1, "interp_second must be 0 or 1");
+    IAC_REQUIRE(p->multiplicator > 0, "multiplicator must be positive");
+    return IAC_OK;
+}
+
+}  // namespace iac
+
+using namespace iac;
+
+extern "C" {
+
+iac_status iac_sparse_set_tuning(iac_ctx *ctx, const iac_sparse_tuning *t)
+{
+    IAC_REQUIRE(ctx && t, "iac_sparse_set_tuning: NULL argument");
+    IAC_REQUIRE(t->block_threads == 0 || (t->block_threads % 32 == 0 && t->block_threads <= 256 &&
+                                          t->block_threads >= 64),
+                "block_threads must be a multiple of 32 in [64, 256]");
+    IAC_REQUIRE(t->tile_pairs == 0 || t->tile_pairs >= 64, "tile_pairs must be >= 64");
+    IAC_REQUIRE(t->ctas_per_sm <= 32, "ctas_per_sm must be <= 32");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->tuning = *t;
+    return IAC_OK;
+}
+
+iac_status iac_sparse_get_tuning(iac_ctx *ctx, iac_sparse_tuning *t)
+{
+    IAC_REQUIRE(ctx && t, "iac_sparse_get_tuning: NULL argument");
+    *t = effective_tuning(ctx);
+    return IAC_OK;
+}
+
+iac_status iac_sparse_ac_batch(iac_ctx *ctx, const float *d_photons, const uint64_t *d_off,
+                               const float *d_rot9, uint32_t nframes, const iac_sparse_params *p,
+                               uint64_t *d_half, void *stream)
+{
+    IAC_REQUIRE(ctx != nullptr, "iac_sparse_ac_batch: ctx is NULL");
+    iac_status st = check_params(p);
+    if (st != IAC_OK) return st;
+    if (nframes == 0) return IAC_OK;
+    IAC_REQUIRE(d_photons && d_off && d_rot9 && d_half, "iac_sparse_ac_batch: NULL pointer");
+    IAC_REQUIRE((reinterpret_cast<uintptr_t>(d_photons) & 15) == 0,
+                "photon array must be 16-byte aligned (float4 per photon)");
+    DeviceGuard g(ctx->device);
+    const iac_sparse_tuning tun = effective_tuning(ctx);
+
+    void *scratch = nullptr;
+    const size_t table_bytes = sizeof(unsigned long long) * ((size_t)nframes + 1);
+    st = stream_scratch(ctx, stream, SLOT_TILES, table_bytes + 256, &scratch);
+    if (st != IAC_OK) return st;
+    unsigned long long *tile_off = (unsigned long long *)scratch;
+    unsigned long long *queue =
+        (unsigned long long *)((char *)scratch + ((table_bytes + 127) / 128) * 128);
+
+    cudaStream_t s = as_stream(stream);
+    sparse_plan_kernel<<<1, PLAN_THREADS, 0, s>>>(d_off, nframes, tun.tile_pairs, tile_off, queue);
+    IAC_LAUNCHED(ctx);
+    IAC_CUDA(cudaGetLastError());
+
+    SparseArgs a;
+    a.photons = reinterpret_cast<const float4 *>(d_photons);
+    a.offsets = d_off;
+    a.rot = d_rot9;
+    a.tile_off = tile_off;
+    a.half = reinterpret_cast<unsigned long long *>(d_half);
+    a.queue = queue;
+    a.counters = ctx->d_counters;
+    a.nframes = nframes;
+    a.tile_pairs = tun.tile_pairs;
+    a.S = (int)p->shape.size_ab;
+    a.C = (a.S - 1) / 2;
+    a.half_ss = (a.S + 1) / 2;
+    a.maxq = p->shape.max_q;
+    a.vpdq = (float)p->shape.voxel_per_dq;
+    a.mult = p->multiplicator;
+
+    const PairKernel k = pick_kernel(p->double_map, p->interp_first, p->interp_second);
+    const int grid = ctx->sm_count * (int)tun.ctas_per_sm;
+    k<<<grid, tun.block_threads, 0, s>>>(a);
+    IAC_LAUNCHED(ctx);
+    IAC_CUDA(cudaGetLastError());
+    return IAC_OK;
+}
+
+iac_status iac_sparse_fold(iac_ctx *ctx, const uint64_t *d_half, uint32_t S, uint64_t *d_full,
+                           void *stream)
+{
+    IAC_REQUIRE(ctx && d_half && d_full, "iac_sparse_fold: NULL argument");
+    IAC_REQUIRE(S >= 3 && (S % 2) == 1 && S <= 2047, "iac_sparse_fold: bad mesh edge %u", S);
+    DeviceGuard g(ctx->device);
+    sparse_fold_kernel<<<ctx->sm_count * 4, 256, 0, as_stream(stream)>>>(
+        reinterpret_cast<const unsigned long long *>(d_half), S,
+        reinterpret_cast<unsigned long long *>(d_full));
+    IAC_LAUNCHED(ctx);
+    IAC_CUDA(cudaGetLastError());
+    return IAC_OK;
+}
+
+iac_status iac_sparse_ac_frames_host(iac_ctx *ctx, const float *h_photons,
+                                     const uint64_t *h_off, const float *h_rot9, uint32_t nframes,
+                                     const iac_sparse_params *p, uint64_t *h_full)
+{
+    IAC_REQUIRE(ctx != nullptr, "iac_sparse_ac_frames_host: ctx is NULL");
+    iac_status st = check_params(p);
+    if (st != IAC_OK) return st;
+    IAC_REQUIRE(h_off && h_full, "iac_sparse_ac_frames_host: NULL pointer");
+    if (nframes == 0) return IAC_OK;
+    IAC_REQUIRE(h_photons && h_rot9, "iac_sparse_ac_frames_host: NULL pointer");
+    DeviceGuard g(ctx->device);
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        if (!ctx->host_stream) IAC_CUDA(cudaStreamCreateWithFlags(&ctx->host_stream, cudaStreamNonBlocking));
+    }
+    cudaStream_t s = ctx->host_stream;
+    void *key = (void *)s;
+    const uint64_t nph = h_off[nframes] - h_off[0];
+    const uint32_t S = p->shape.size_ab;
+    const size_t half_b = sizeof(uint64_t) * iac_half_mesh_words(S);
+    const size_t full_b = sizeof(uint64_t) * iac_full_mesh_words(S);
+    void *d_ph, *d_off, *d_rot, *d_half, *d_full;
+    if ((st = stream_scratch(ctx, key, SLOT_PHOTONS, 16 * nph + 16, &d_ph)) != IAC_OK) return st;
+    if ((st = stream_scratch(ctx, key, SLOT_OFFSETS, 8 * ((size_t)nframes + 1), &d_off)) != IAC_OK) return st;
+    if ((st = stream_scratch(ctx, key, SLOT_ROT, 36 * (size_t)nframes, &d_rot)) != IAC_OK) return st;
+    if ((st = stream_scratch(ctx, key, SLOT_HALF, half_b, &d_half)) != IAC_OK) return st;
+    if ((st = stream_scratch(ctx, key, SLOT_FULL, full_b, &d_full)) != IAC_OK) return st;
+
+    // offsets are rebased so that the first frame starts at photon 0
+    std::vector<uint64_t> off(h_off, h_off + nframes + 1);
+    const uint64_t o0 = off[0];
+    for (auto &o : off) o -= o0;
+    IAC_CUDA(cudaMemcpyAsync(d_ph, h_photons + 4 * o0, 16 * nph, cudaMemcpyHostToDevice, s));
+    IAC_CUDA(cudaMemcpyAsync(d_off, off.data(), 8 * off.size(), cudaMemcpyHostToDevice, s));
+    IAC_CUDA(cudaMemcpyAsync(d_rot, h_rot9, 36 * (size_t)nframes, cudaMemcpyHostToDevice, s));
+    IAC_CUDA(cudaMemsetAsync(d_half, 0, half_b, s));
+    IAC_CUDA(cudaMemcpyAsync(d_full, h_full, full_b, cudaMemcpyHostToDevice, s));
+    st = iac_sparse_ac_batch(ctx, (const float *)d_ph, (const uint64_t *)d_off, (const float *)d_rot,
+                             nframes, p, (uint64_t *)d_half, key);
+    if (st != IAC_OK) return st;
+    st = iac_sparse_fold(ctx, (const uint64_t *)d_half, S, (uint64_t *)d_full, key);
+    if (st != IAC_OK) return st;
+    IAC_CUDA(cudaMemcpyAsync(h_full, d_full, full_b, cudaMemcpyDeviceToHost, s));
+    IAC_CUDA(cudaStreamSynchronize(s));
+    return IAC_OK;
+}
+
+}  // extern "C"

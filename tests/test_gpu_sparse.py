@@ -1,0 +1,170 @@
+"""(a) sparse photon pairs -> uint64 mesh on the GPU, through the C ABI,
+against the oracle.  Integer meshes must match bit for bit."""
+import numpy as np
+import pytest
+
+from helpers import random_frames, small_detector, to_capi_shape
+
+pytestmark = pytest.mark.gpu
+
+MODES = [(d, i1, i2) for d in (0, 1) for i1 in (0, 1) for i2 in (0, 1) if d or i1 == 0]
+
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def gpu_full_mesh(ctx, photons, offsets, rot, shape, dmap=1, i1=0, i2=0, tuning=None):
+    import torch
+    from incohautocorrelate_b200 import capi
+    S = shape.size_ab
+    p = capi.sparse_params(to_capi_shape(shape), i1, i2, dmap, 1000.0)
+    half = torch.zeros(capi.half_mesh_words(S), dtype=torch.int64, device="cuda")
+    full = torch.zeros(capi.full_mesh_words(S), dtype=torch.int64, device="cuda")
+    if tuning:
+        ctx.set_sparse_tuning(**tuning)
+    ph = _dev(photons if len(photons) else np.zeros((1, 4), np.float32))
+    off = _dev(offsets.astype(np.uint64).view(np.int64))
+    R = _dev(rot.astype(np.float32))
+    ctx.sparse_ac_batch(ph, off, R, len(offsets) - 1, p, half)
+    ctx.sparse_fold(half, S, full)
+    oob = ctx.check()
+    if tuning:
+        ctx.set_sparse_tuning()
+    return full.cpu().numpy().view(np.uint64), oob
+
+
+@pytest.mark.parametrize("dmap,i1,i2", MODES)
+def test_all_modes_bit_exact(ctx, oracle_lib, rng, dmap, i1, i2):
+    from incohautocorrelate_b200 import workloads as W
+    _, km, mq = small_detector()
+    shape = oracle_lib.big_mesh_shape(mq, 31)
+    sizes = [0, 1, 2, 3, 9, 31, 64, 65, 127, 200, 0, 5]
+    ph, off = random_frames(km, sizes, rng, integer=(i1 == 0 and i2 == 0))
+    rot = W.haar_rotations(len(sizes), seed=11)
+    want, o1 = oracle_lib.sparse_batch(ph, off, rot, shape, i1, i2, dmap, cpu_gpu=1)
+    got, o2 = gpu_full_mesh(ctx, ph, off, rot, shape, dmap, i1, i2)
+    assert o1 == 0 and o2 == 0
+    np.testing.assert_array_equal(got, want)
+
+
+def test_small_config_matches_reference_route(ctx, oracle_lib):
+    """128^2 detector, Poisson(0.01) frames, identity orientation, 65^3 mesh:
+    the reference takes its CPU route for these frames (hits < 1 %)."""
+    from incohautocorrelate_b200 import workloads as W
+    cfg = W.small_config(nframes=300, seed=1)
+    shape = oracle_lib.big_mesh_shape(cfg["max_q"], cfg["mesh_size"])
+    want, _ = oracle_lib.sparse_batch(cfg["photons"], cfg["offsets"], cfg["rot"], shape,
+                                      cpu_gpu=-1, det_pixels=cfg["npix"])
+    got, oob = gpu_full_mesh(ctx, cfg["photons"], cfg["offsets"], cfg["rot"], shape)
+    assert oob == 0
+    np.testing.assert_array_equal(got, want)
+
+
+def test_rotated_config_subset_matches(ctx, oracle_lib):
+    """1024x512 two-panel detector, log-normal photon counts, random SO(3)
+    orientations, 201^3 mesh: 400 frames against the oracle."""
+    from incohautocorrelate_b200 import workloads as W
+    cfg = W.rotated_config(nframes=400, seed=2)
+    shape = oracle_lib.big_mesh_shape(cfg["max_q"], cfg["mesh_size"])
+    want, _ = oracle_lib.sparse_batch(cfg["photons"], cfg["offsets"], cfg["rot"], shape,
+                                      cpu_gpu=-1, det_pixels=cfg["npix"])
+    got, oob = gpu_full_mesh(ctx, cfg["photons"], cfg["offsets"], cfg["rot"], shape)
+    assert oob == 0
+    np.testing.assert_array_equal(got, want)
+
+
+def test_one_large_frame(ctx, oracle_lib, rng):
+    """A 3000-photon frame (4.5 M pairs) spans many queue tiles."""
+    from incohautocorrelate_b200 import workloads as W
+    pm, km, mq, mask = W.rotated_detector()
+    shape = oracle_lib.big_mesh_shape(mq, 199)
+    ph, off = random_frames(km, [3000, 4, 1500], rng)
+    rot = W.haar_rotations(3, seed=4)
+    want, _ = oracle_lib.sparse_batch(ph, off, rot, shape)
+    got, oob = gpu_full_mesh(ctx, ph, off, rot, shape)
+    assert oob == 0
+    np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("tuning", [dict(tile_pairs=64, block_threads=64, ctas_per_sm=1),
+                                    dict(tile_pairs=1000, block_threads=96, ctas_per_sm=3),
+                                    dict(tile_pairs=65536, block_threads=256, ctas_per_sm=16)])
+def test_tuning_does_not_change_the_mesh(ctx, oracle_lib, rng, tuning):
+    from incohautocorrelate_b200 import workloads as W
+    _, km, mq = small_detector()
+    shape = oracle_lib.big_mesh_shape(mq, 31)
+    ph, off = random_frames(km, [1, 70, 300, 2, 45], rng)
+    rot = W.haar_rotations(5, seed=8)
+    want, _ = oracle_lib.sparse_batch(ph, off, rot, shape)
+    got, _ = gpu_full_mesh(ctx, ph, off, rot, shape, tuning=tuning)
+    np.testing.assert_array_equal(got, want)
+
+
+def test_empty_inputs(ctx, oracle_lib):
+    _, km, mq = small_detector()
+    shape = oracle_lib.big_mesh_shape(mq, 31)
+    off = np.zeros(4, np.uint64)  # three empty frames
+    got, oob = gpu_full_mesh(ctx, np.zeros((0, 4), np.float32), off,
+                             np.tile(np.eye(3, dtype=np.float32).reshape(1, 9), (3, 1)), shape)
+    assert oob == 0 and not got.any()
+
+
+def test_out_of_mesh_writes_are_counted(ctx, oracle_lib, rng):
+    _, km, mq = small_detector()
+    shape = oracle_lib.big_mesh_shape(mq, 31)
+    ph, off = random_frames(km, [60], rng)
+    R = np.array([[3, 0, 0, 0, 3, 0, 0, 0, 3]], np.float32)
+    want, o1 = oracle_lib.sparse_batch(ph, off, R, shape)
+    got, o2 = gpu_full_mesh(ctx, ph, off, R, shape)
+    assert o1 > 0 and o2 == o1
+    np.testing.assert_array_equal(got, want)
+
+
+def test_host_entry_point_accumulates(ctx, oracle_lib, rng):
+    """iac_sparse_ac_frames_host: host buffers in, ACMesh::Mesh += result."""
+    from incohautocorrelate_b200 import capi, workloads as W
+    _, km, mq = small_detector()
+    shape = oracle_lib.big_mesh_shape(mq, 31)
+    ph, off = random_frames(km, [10, 80, 33], rng)
+    rot = W.haar_rotations(3, seed=1)
+    want, _ = oracle_lib.sparse_batch(ph, off, rot, shape)
+    p = capi.sparse_params(to_capi_shape(shape))
+    mesh = np.zeros(capi.full_mesh_words(shape.size_ab), np.uint64)
+    ctx.sparse_ac_frames_host(ph, off, rot, 3, p, mesh)
+    np.testing.assert_array_equal(mesh, want)
+    ctx.sparse_ac_frames_host(ph, off, rot, 3, p, mesh)
+    np.testing.assert_array_equal(mesh, 2 * want)
+
+
+def test_full_size_properties(ctx):
+    """100 000 rotated frames at 201^3: point symmetry of the full mesh, the
+    batch is the sum of its halves (linearity), and the result does not depend
+    on the work-queue tiling."""
+    import torch
+    from incohautocorrelate_b200 import workloads as W
+    cfg = W.rotated_config(nframes=100_000, seed=2)
+    from incohautocorrelate_b200 import capi
+    shape = capi.big_mesh_shape(cfg["max_q"], cfg["mesh_size"])
+
+    class S:  # oracle-shaped shim for gpu_full_mesh
+        pass
+    s = S()
+    for f, _ in capi.MeshShape._fields_:
+        setattr(s, f, getattr(shape, f))
+    ph, off, rot = cfg["photons"], cfg["offsets"], cfg["rot"]
+    full, oob = gpu_full_mesh(ctx, ph, off, rot, s)
+    assert oob == 0
+    S_ = shape.size_ab
+    m = full.reshape(S_, S_, S_)
+    np.testing.assert_array_equal(m, m[::-1, ::-1, ::-1])
+    h = len(off) // 2
+    a, _ = gpu_full_mesh(ctx, ph[: off[h]], off[: h + 1], rot[:h], s)
+    b, _ = gpu_full_mesh(ctx, ph[off[h]:], off[h:] - off[h], rot[h:], s,
+                         tuning=dict(tile_pairs=777, block_threads=128, ctas_per_sm=2))
+    np.testing.assert_array_equal(a + b, full)
+    # every self pair lands on the centre voxel
+    w = ph[:, 3].astype(np.int64)
+    assert int(m[(S_ - 1) // 2, (S_ - 1) // 2, (S_ - 1) // 2]) >= 1000 * int((w * w).sum())
+    del torch
