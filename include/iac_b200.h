@@ -145,15 +145,156 @@ iac_status iac_sparse_ac_frames_host(iac_ctx *ctx, const float *h_photons,
                                      uint32_t nframes, const iac_sparse_params *params,
                                      uint64_t *h_full_mesh);
 
-/* Work-queue tuning of the persistent pair kernel (see DESIGN.md of the
- * project for the autotuner); zeros select the built-in defaults. */
+/* Work-queue tuning of the persistent pair kernel.  Fields left 0 come from
+ * the autotuner's table (tuning/sparse_tuning.tsv beside the library, or the
+ * file named by IAC_SPARSE_TUNING; the row of the nearest mesh edge), else
+ * from built-in defaults.  iac_sparse_get_tuning reports the setting a batch
+ * on a mesh of edge size_ab would use. */
 typedef struct {
     uint32_t tile_pairs;      /* pairs per queue tile           */
     uint32_t block_threads;   /* threads per CTA                */
     uint32_t ctas_per_sm;     /* persistent CTAs per SM         */
 } iac_sparse_tuning;
 iac_status iac_sparse_set_tuning(iac_ctx *ctx, const iac_sparse_tuning *t);
-iac_status iac_sparse_get_tuning(iac_ctx *ctx, iac_sparse_tuning *t);
+iac_status iac_sparse_get_tuning(iac_ctx *ctx, uint32_t size_ab, iac_sparse_tuning *t);
+
+/* ---------------------------------------------------------------------- */
+/* (b) dense mean-intensity C(q)                                            */
+/* ---------------------------------------------------------------------- */
+
+/* Multiplicator of Detector::AutoCorrelate_CofQ_SmallMesh
+ * (IAC/Detector.cpp:1211-1227): 10^k * 1e5 with Mean(I)^2 * 10^k >= 1.
+ * Host arithmetic on a host array. */
+iac_status iac_cq_small_multiplicator(const float *h_intensity, uint64_t npix, double *mult);
+
+/* Kernel AutoCorr_CQ_small (IAC/kernel.cl:27-184) of
+ * Detector::AutoCorrelate_CofQ_SmallMesh (IAC/Detector.cpp:1184-1315): every
+ * ordered pixel pair of the mean intensity, (uint64)(I_a*I_b*Mult) binned at
+ * q = k_a - k_b on the small mesh (nearest or 8-corner linear).
+ * d_mesh (uint64[size_ab^2 * size_c], CQMesh order) is accumulated, not
+ * cleared; CQMesh = d_mesh / Mult.  Asynchronous on `stream`. */
+iac_status iac_cq_small(iac_ctx *ctx, const float *d_intensity, const float *d_kmap,
+                        uint64_t npix, const iac_mesh_shape *small_shape, int interp,
+                        double multiplicator, uint64_t *d_mesh, void *stream);
+
+/* Rotation/weight table and Multiplicator of Detector::Merge_smallCofQ
+ * (IAC/Detector.cpp:1339-1427): h_rw10 gets 9 rotation floats + the rounded
+ * weight MeanIntensity^2 per frame.  Host arithmetic. */
+iac_status iac_cq_merge_weights(const float *h_rot9, const float *h_mean_intensity,
+                                uint32_t nframes, const double *h_small_cq, uint64_t small_words,
+                                float *h_rw10, double *mult);
+
+/* Kernel Merge_CQ (IAC/kernel.cl:189-344): every small-mesh voxel with
+ * C >= 1e-37 rotated by every frame's matrix and added, weighted, to the
+ * cubic mesh d_big (uint64[size_ab^3]), which is accumulated, not cleared;
+ * CQMesh(big) = d_big / Mult.  Asynchronous. */
+iac_status iac_cq_merge(iac_ctx *ctx, const double *d_small_cq, const float *d_rw10,
+                        uint32_t nframes, const iac_mesh_shape *small_shape, int interp,
+                        double multiplicator, uint64_t *d_big, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* (c) AC1D                                                                 */
+/* ---------------------------------------------------------------------- */
+
+/* Multiplicator of AC1D::Calculate_CQ (IAC/AC1D.cpp:78-91). Host. */
+iac_status iac_ac1d_cq_multiplicator(const float *h_intensity, uint64_t npix, double *mult);
+
+/* Kernel AutoCorr_CQ_AV (IAC/kernel.cl:656-764) of AC1D::Calculate_CQ
+ * (IAC/AC1D.cpp:61-195): |q| histogram of all ordered pixel pairs of the mean
+ * intensity into d_hist (uint64[shape.size], accumulated).  Equals the sum of
+ * the reference's 10000 sub-histograms; CQ = d_hist / Mult.  Asynchronous. */
+iac_status iac_ac1d_cq(iac_ctx *ctx, const float *d_intensity, const float *d_kmap,
+                       uint64_t npix, const iac_ac1d_shape *shape, int interp,
+                       double multiplicator, uint64_t *d_hist, void *stream);
+
+/* VecSize = ceil(MaxQ / dq) - 1 of Calculate_AC_UW_Mapped (IAC/AC1D.cpp:301). */
+uint32_t iac_ac1d_vecsize(float max_q, float dqdx);
+
+/* Kernel AutoCorr_sparseHL_AAV (IAC/kernel.cl:863-950) over a batch of
+ * photon lists (layout as iac_sparse_ac_batch), the device route of
+ * Calculate_AC_UW_Mapped (IAC/AC1D.cpp:295-379): every ordered pair of each
+ * frame, self pairs included, into d_hist (uint64[iac_ac1d_vecsize], bins
+ * taken modulo VecSize as the reference's fold does; accumulated).
+ * AC_UW = d_hist / Mult (Mult = 100 in the reference).  Asynchronous. */
+iac_status iac_ac1d_sparse_batch(iac_ctx *ctx, const float *d_photons,
+                                 const uint64_t *d_frame_offsets, uint32_t nframes, float max_q,
+                                 float dqdx, int interp, double multiplicator, uint64_t *d_hist,
+                                 void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* (d) simulator                                                            */
+/* ---------------------------------------------------------------------- */
+
+/* Crystal::EmittingCrystSettings (IAC/Crystal.h:37-44) */
+typedef struct {
+    int32_t incoherent;          /* random phase per emitter and mode       */
+    float fluorescence_yield;    /* 0 < FlYield <= 1                        */
+    int32_t random_orientation;  /* roll an orientation per frame           */
+    float isotropy;              /* 0 <= Isotropie <= 1                     */
+} iac_crystal_params;
+
+/* Crystal::GetEmitters for every (frame, mode) (IAC/Crystal.cpp:29-120, with
+ * the rotation stored inverted as IAC/Simulator.cpp:707-722 does).
+ *   d_atoms      3 doubles per atom (Crystal::AtomPositions)
+ *   d_emitters   float4 (x, y, z, phase), [frame][mode][atom]; the first
+ *                d_em_count[frame*nmodes + mode] entries of each block are used
+ *   d_rot_event  9 floats per frame (HitEvent::RotMatrix, the inverse)
+ *   d_rot_crystal optional, 9 floats per frame (the crystal rotation)
+ * Random numbers: Philox4x32-10 streams keyed by `seed`, a pure function of
+ * (frame, mode, atom).  Asynchronous. */
+iac_status iac_crystal_emitters(iac_ctx *ctx, const double *d_atoms, uint32_t natoms,
+                                uint32_t nframes, uint32_t nmodes, const iac_crystal_params *cp,
+                                uint64_t seed, float *d_emitters, uint32_t *d_em_count,
+                                float *d_rot_event, float *d_rot_crystal, void *stream);
+
+/* Parameters of kernel SimulateCrystal (IAC/Simulator.cpp:742-777). */
+typedef struct {
+    int32_t subsampling;        /* SuSa: (2 SuSa + 1)^2 sub-pixels          */
+    double u_step[3];           /* sub-pixel step along the fast axis       */
+    double v_step[3];           /* sub-pixel step along the slow axis       */
+    double wavelength;
+    int32_t intensity_squared;  /* 0: add |Psi| per sub-pixel as the reference
+                                   kernel does (IAC/kernel.cl:844); 1: |Psi|^2 */
+    int32_t accurate_sincos;    /* 0: explicit 2*pi reduction + SFU sin/cos;
+                                   1: sincosf                                */
+} iac_sim_params;
+
+/* Kernel SimulateCrystal per mode, summed over modes as SimulatePart does
+ * (IAC/Simulator.cpp:779-866), for nframes frames: d_intensity is
+ * float[nframes][npix].  Asynchronous. */
+iac_status iac_simulate_intensity(iac_ctx *ctx, const float *d_pixel_map, uint64_t npix,
+                                  const float *d_emitters, const uint32_t *d_em_count,
+                                  uint32_t natoms, uint32_t nmodes, uint32_t nframes,
+                                  const iac_sim_params *params, float *d_intensity, void *stream);
+
+/* Post-processing of SimulatePart (IAC/Simulator.cpp:870-894). */
+typedef struct {
+    double expected_photons;  /* AveragePhotonesPerEmitterOnDetector * FlYield * #atoms */
+    int32_t poisson;          /* PoissonSample                                     */
+    float adu_noise;          /* ADUNoise (uniform +-level), 0 = none              */
+    float value_per_photon;   /* ValuePerPhoton                                    */
+} iac_photon_params;
+
+/* Rescale each frame to the expected photon number, draw Poisson counts
+ * (inversion below a mean of 25, clipped Box-Muller above, as
+ * ArrayOperators::ScalarPoissonSampling), add noise, scale by the value per
+ * photon; in place.  Random streams are indexed by first_frame + frame and
+ * pixel.  Asynchronous. */
+iac_status iac_simulate_photons(iac_ctx *ctx, float *d_intensity, uint64_t npix, uint32_t nframes,
+                                uint64_t first_frame, const iac_photon_params *params,
+                                uint64_t seed, void *stream);
+
+/* Detector::CreateSparseHitList(Threshold, Step) on the device
+ * (IAC/Detector.cpp:926-977) after the pixel mask (IAC/RunIAC.cpp:534):
+ * frames float[nframes][npix] -> photon lists float4 (k, value) in pixel order
+ * with nframes+1 offsets, ready for iac_sparse_ac_batch.  d_mask may be NULL.
+ * If h_total is given the call synchronises, stores the photon count and
+ * fails when it exceeds `capacity` (entries beyond it are not written). */
+iac_status iac_sparsify_frames(iac_ctx *ctx, const float *d_intensity, const int *d_mask,
+                               const float *d_kmap, uint64_t npix, uint32_t nframes,
+                               float threshold, float step, int photonize, float *d_photons,
+                               uint64_t capacity, uint64_t *d_frame_offsets, uint64_t *h_total,
+                               void *stream);
 
 /* ---------------------------------------------------------------------- */
 /* micro-benchmarks (roofline denominators)                                 */

@@ -1,0 +1,116 @@
+"""Autotuner of the persistent photon-pair kernel's work queue.
+
+For each mesh edge it times the batched correlator over a grid of
+(tile_pairs, block_threads, ctas_per_sm) on a seeded workload of that mesh and
+records the fastest setting in tuning/sparse_tuning.tsv, a table that
+libiac_b200.so reads when a context is created (the row with the nearest mesh
+edge is applied unless iac_sparse_set_tuning overrides it).
+
+    python -m incohautocorrelate_b200.autotune [--edges 63,199] [--frames N]
+
+Needs a GPU.  The results depend on the GPU model and clocks; the committed
+table was measured on a B200.
+"""
+from __future__ import annotations
+
+import argparse
+import itertools
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+TABLE = os.path.join(HERE, "tuning", "sparse_tuning.tsv")
+
+GRID = dict(tile_pairs=[1024, 2048, 4096, 8192, 16384],
+            block_threads=[128, 256],
+            ctas_per_sm=[4, 8, 16])
+
+
+def workload_for_edge(edge: int, frames: int):
+    from . import workloads as W
+    if edge <= 101:
+        cfg = W.small_config(nframes=frames, seed=1)
+        cfg["rot"] = W.haar_rotations(frames, seed=5)
+    else:
+        cfg = W.rotated_config(nframes=frames, seed=2)
+    cfg["mesh_size"] = edge
+    return cfg
+
+
+def time_setting(ctx, bufs, params, nframes, setting, reps=3):
+    import torch
+    ph, off, rot, half = bufs
+    ctx.set_sparse_tuning(**setting)
+    s = torch.cuda.current_stream()
+    for _ in range(2):
+        ctx.sparse_ac_batch(ph, off, rot, nframes, params, half, s.cuda_stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s)
+    for _ in range(reps):
+        ctx.sparse_ac_batch(ph, off, rot, nframes, params, half, s.cuda_stream)
+    b.record(s)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def tune_edge(ctx, edge: int, frames: int):
+    import torch
+
+    from . import capi
+    cfg = workload_for_edge(edge, frames)
+    shape = capi.big_mesh_shape(cfg["max_q"], edge)
+    params = capi.sparse_params(shape)
+    ph = torch.from_numpy(cfg["photons"]).cuda()
+    off = torch.from_numpy(cfg["offsets"].view(np.int64)).cuda()
+    rot = torch.from_numpy(cfg["rot"]).cuda()
+    half = torch.zeros(capi.half_mesh_words(shape.size_ab), dtype=torch.int64, device="cuda")
+    n = np.diff(cfg["offsets"].astype(np.int64))
+    pairs = int((n * (n + 1) // 2).sum())
+    results = []
+    keys = list(GRID)
+    for vals in itertools.product(*(GRID[k] for k in keys)):
+        setting = dict(zip(keys, vals))
+        ms = time_setting(ctx, (ph, off, rot, half), params, len(n), setting)
+        results.append((ms, setting))
+    results.sort(key=lambda r: r[0])
+    ms, best = results[0]
+    return dict(edge=edge, frames=len(n), pairs=pairs, ms=ms, pairs_per_s=pairs / (ms * 1e-3),
+                **best), results
+
+
+def write_table(rows):
+    os.makedirs(os.path.dirname(TABLE), exist_ok=True)
+    with open(TABLE, "w") as fh:
+        fh.write("# mesh_edge\ttile_pairs\tblock_threads\tctas_per_sm\tpairs_per_s\tframes\n")
+        for r in sorted(rows, key=lambda r: r["edge"]):
+            fh.write(f"{r['edge']}\t{r['tile_pairs']}\t{r['block_threads']}\t"
+                     f"{r['ctas_per_sm']}\t{r['pairs_per_s']:.4g}\t{r['frames']}\n")
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--edges", default="63,199")
+    ap.add_argument("--frames", type=int, default=100_000)
+    ap.add_argument("--json", default=None, help="also write every timing here")
+    a = ap.parse_args(argv)
+    from . import capi
+    ctx = capi.Context(0)
+    rows, dump = [], {}
+    for e in [int(x) for x in a.edges.split(",")]:
+        best, allr = tune_edge(ctx, e, a.frames)
+        rows.append(best)
+        dump[e] = [dict(ms=m, **s) for m, s in allr]
+        print(json.dumps(best), flush=True)
+    write_table(rows)
+    if a.json:
+        with open(a.json, "w") as fh:
+            json.dump(dump, fh, indent=1)
+    ctx.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -90,8 +90,17 @@ def _declare(lib):
     fn("iac_sparse_fold", [_VP, _VP, _U32, _VP, _VP])
     fn("iac_sparse_ac_frames_host", [_VP, _VP, _VP, _VP, _U32, C.POINTER(SparseParams), _VP])
     fn("iac_sparse_set_tuning", [_VP, C.POINTER(SparseTuning)])
-    fn("iac_sparse_get_tuning", [_VP, C.POINTER(SparseTuning)])
+    fn("iac_sparse_get_tuning", [_VP, _U32, C.POINTER(SparseTuning)])
     fn("iac_bench_scatter_add", [_VP, _VP, _U64, C.c_int, _U64, _U32, _VP])
+    D = C.c_double
+    fn("iac_cq_small_multiplicator", [_VP, _U64, C.POINTER(D)])
+    fn("iac_cq_small", [_VP, _VP, _VP, _U64, C.POINTER(MeshShape), C.c_int, D, _VP, _VP])
+    fn("iac_cq_merge_weights", [_VP, _VP, _U32, _VP, _U64, _VP, C.POINTER(D)])
+    fn("iac_cq_merge", [_VP, _VP, _VP, _U32, C.POINTER(MeshShape), C.c_int, D, _VP, _VP])
+    fn("iac_ac1d_cq_multiplicator", [_VP, _U64, C.POINTER(D)])
+    fn("iac_ac1d_cq", [_VP, _VP, _VP, _U64, C.POINTER(AC1DShape), C.c_int, D, _VP, _VP])
+    fn("iac_ac1d_vecsize", [C.c_float, C.c_float], _U32)
+    fn("iac_ac1d_sparse_batch", [_VP, _VP, _VP, _U32, C.c_float, C.c_float, C.c_int, D, _VP, _VP])
     return lib
 
 
@@ -135,6 +144,33 @@ def ac1d_shape(max_q, size: int, q_zoom: float = 1.0) -> AC1DShape:
     s = AC1DShape()
     check(lib().iac_ac1d_shape_init(_f3(max_q), int(size), float(q_zoom), C.byref(s)))
     return s
+
+
+def cq_small_multiplicator(h_intensity) -> float:
+    m = C.c_double()
+    check(lib().iac_cq_small_multiplicator(_ptr(h_intensity), int(h_intensity.size), C.byref(m)))
+    return m.value
+
+
+def ac1d_cq_multiplicator(h_intensity) -> float:
+    m = C.c_double()
+    check(lib().iac_ac1d_cq_multiplicator(_ptr(h_intensity), int(h_intensity.size), C.byref(m)))
+    return m.value
+
+
+def cq_merge_weights(h_rot9, h_mean_intensity, h_small_cq):
+    """(rw10 table float32[n, 10], Multiplicator) of Detector::Merge_smallCofQ."""
+    import numpy as np
+    nf = int(len(h_mean_intensity))
+    rw = np.zeros((nf, 10), np.float32)
+    m = C.c_double()
+    check(lib().iac_cq_merge_weights(_ptr(h_rot9), _ptr(h_mean_intensity), nf, _ptr(h_small_cq),
+                                     int(h_small_cq.size), _ptr(rw), C.byref(m)))
+    return rw, m.value
+
+
+def ac1d_vecsize(max_q: float, dqdx: float) -> int:
+    return int(lib().iac_ac1d_vecsize(float(max_q), float(dqdx)))
 
 
 def half_mesh_words(S: int) -> int:
@@ -226,11 +262,29 @@ class Context:
         t = SparseTuning(int(tile_pairs), int(block_threads), int(ctas_per_sm))
         check(lib().iac_sparse_set_tuning(self._h, C.byref(t)))
 
-    def sparse_tuning(self):
+    def sparse_tuning(self, size_ab: int = 0):
         t = SparseTuning()
-        check(lib().iac_sparse_get_tuning(self._h, C.byref(t)))
+        check(lib().iac_sparse_get_tuning(self._h, int(size_ab), C.byref(t)))
         return {"tile_pairs": t.tile_pairs, "block_threads": t.block_threads,
                 "ctas_per_sm": t.ctas_per_sm}
+
+    def cq_small(self, d_I, d_kmap, npix, shape, interp, mult, d_mesh, stream=None):
+        check(lib().iac_cq_small(self._h, _ptr(d_I), _ptr(d_kmap), int(npix), C.byref(shape),
+                                 int(interp), float(mult), _ptr(d_mesh), _ptr(stream)))
+
+    def cq_merge(self, d_small, d_rw, nframes, shape, interp, mult, d_big, stream=None):
+        check(lib().iac_cq_merge(self._h, _ptr(d_small), _ptr(d_rw), int(nframes), C.byref(shape),
+                                 int(interp), float(mult), _ptr(d_big), _ptr(stream)))
+
+    def ac1d_cq(self, d_I, d_kmap, npix, shape, interp, mult, d_hist, stream=None):
+        check(lib().iac_ac1d_cq(self._h, _ptr(d_I), _ptr(d_kmap), int(npix), C.byref(shape),
+                                int(interp), float(mult), _ptr(d_hist), _ptr(stream)))
+
+    def ac1d_sparse_batch(self, d_photons, d_offsets, nframes, max_q, dqdx, interp, mult, d_hist,
+                          stream=None):
+        check(lib().iac_ac1d_sparse_batch(self._h, _ptr(d_photons), _ptr(d_offsets), int(nframes),
+                                          float(max_q), float(dqdx), int(interp), float(mult),
+                                          _ptr(d_hist), _ptr(stream)))
 
     def bench_scatter_add(self, d_buf, words, word_bits, updates, seed=1, stream=None):
         check(lib().iac_bench_scatter_add(self._h, _ptr(d_buf), int(words), int(word_bits),

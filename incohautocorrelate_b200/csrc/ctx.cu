@@ -1,5 +1,7 @@
 // ctx.cu -- context, error reporting, mesh geometry, k-map and the
 // scatter-add micro-benchmark of libiac_b200.
+#include <dlfcn.h>
+
 #include <cmath>
 #include <cstdarg>
 #include <cstdlib>
@@ -30,6 +32,36 @@ iac_status Scratch::ensure(size_t need)
     IAC_CUDA(cudaMalloc(&ptr, grow));
     bytes = grow;
     return IAC_OK;
+}
+
+// The autotuner's table: tuning/sparse_tuning.tsv next to this library (or the
+// file named by IAC_SPARSE_TUNING).  Rows: mesh_edge tile_pairs block_threads
+// ctas_per_sm [...]; '#' starts a comment.
+static void load_tuning_table(iac_ctx *c)
+{
+    std::string path;
+    if (const char *env = std::getenv("IAC_SPARSE_TUNING")) {
+        path = env;
+    } else {
+        Dl_info info;
+        if (dladdr((void *)&load_tuning_table, &info) && info.dli_fname) {
+            path = info.dli_fname;
+            const size_t slash = path.find_last_of('/');
+            path = (slash == std::string::npos ? std::string(".") : path.substr(0, slash)) +
+                   "/tuning/sparse_tuning.tsv";
+        }
+    }
+    FILE *fh = path.empty() ? nullptr : std::fopen(path.c_str(), "r");
+    if (!fh) return;
+    char line[512];
+    while (std::fgets(line, sizeof line, fh)) {
+        if (line[0] == '#') continue;
+        unsigned e, t, b, k;
+        if (std::sscanf(line, "%u %u %u %u", &e, &t, &b, &k) == 4 && t >= 64 && b >= 64 &&
+            b <= 256 && b % 32 == 0 && k >= 1 && k <= 32)
+            c->tuning_table.push_back({e, t, b, k});
+    }
+    std::fclose(fh);
 }
 
 void Scratch::release()
@@ -91,6 +123,7 @@ iac_status iac_ctx_create(int device, iac_ctx **out)
     }
     cudaMemset(c->d_counters, 0, sizeof(DeviceCounters));
     cudaDeviceSynchronize();
+    load_tuning_table(c);
     *out = c;
     return IAC_OK;
 }
@@ -200,6 +233,79 @@ iac_status iac_ac1d_shape_init(const float mq[3], uint32_t size, float q_zoom, i
     return IAC_OK;
 }
 
+// ---------------------------------------------------------------------------
+// host-side multiplicators and the merge weight table
+// ---------------------------------------------------------------------------
+
+// ArrayOperators::Min_Max_Mean_Value(float*) mean, IAC/ArrayOperators.h:160-175
+static float mean_of(const float *a, uint64_t n)
+{
+    double t = 0;
+    for (uint64_t i = 0; i < n; i++) t += a[i];
+    t = t / (double)(int)n;
+    return (float)t;
+}
+
+iac_status iac_cq_small_multiplicator(const float *h_I, uint64_t npix, double *mult)
+{
+    IAC_REQUIRE(h_I && mult && npix > 0, "iac_cq_small_multiplicator: bad argument");
+    const float m = mean_of(h_I, npix);
+    IAC_REQUIRE(m > 0, "No intensity > 0 found in averaged intensity");
+    double x = 1e-10;
+    for (; 1 > (double)(m * m) * x;) x *= 10;
+    *mult = x * 100000;
+    return IAC_OK;
+}
+
+iac_status iac_ac1d_cq_multiplicator(const float *h_I, uint64_t npix, double *mult)
+{
+    IAC_REQUIRE(h_I && mult && npix > 0, "iac_ac1d_cq_multiplicator: bad argument");
+    const float m = mean_of(h_I, npix);
+    IAC_REQUIRE(m > 0, "No intensity > 0 found in averaged intensity");
+    double x = 1e-10;
+    for (; 1 > (double)(m * m) * x;) x *= 10;
+    x = x * 1e5;
+    if (x > 1e18) x = 1e18;
+    *mult = x;
+    return IAC_OK;
+}
+
+iac_status iac_cq_merge_weights(const float *R, const float *MI, uint32_t nf, const double *cq,
+                                uint64_t small_n, float *rw, double *mult_out)
+{
+    IAC_REQUIRE(R && MI && cq && rw && mult_out && small_n > 0, "iac_cq_merge_weights: bad argument");
+    double maxw = 0.0;
+    for (uint32_t i = 0; i < nf; i++) {
+        for (int d = 0; d < 9; d++) rw[10 * (size_t)i + d] = R[9 * (size_t)i + d];
+        rw[10 * (size_t)i + 9] = (float)((double)MI[i] * (double)MI[i]);
+        if (MI[i] > maxw) maxw = MI[i];
+    }
+    double t = 0;
+    for (uint64_t i = 0; i < small_n; i++) t += cq[i];
+    const double mean_cq = t / (double)(int)small_n;
+    // the reference's search below never ends for an empty C(q) or zero weights
+    IAC_REQUIRE(mean_cq > 0 && maxw > 0, "C(q) mesh is empty or every frame weight is zero");
+    double m = 1e-12;
+    for (; 1 > maxw * maxw * mean_cq * m;) m *= 10;
+    uint64_t oom = 1;
+    for (; oom < nf;) oom *= 10;
+    m = m / (double)oom;
+    m *= 1e10;
+    if (m > 0.6) m = std::round(m);
+    if (m < 1 && m > 0.1) m = 1;
+    if (m < 1e-12) m = 1e-12;
+    for (uint32_t i = 0; i < nf; i++) {
+        float red = (float)m;
+        if (m > 0.6) red = std::round((float)m);
+        float w = rw[10 * (size_t)i + 9];
+        w *= red;
+        w = std::floor((float)((double)w + 0.5));
+        rw[10 * (size_t)i + 9] = w / red;
+    }
+    *mult_out = m;
+    return IAC_OK;
+}
+
 uint64_t iac_half_mesh_words(uint32_t S) { return (uint64_t)S * S * ((S + 1) / 2); }
 uint64_t iac_full_mesh_words(uint32_t S) { return (uint64_t)S * S * S; }
 
@@ -278,25 +384,20 @@ extern "C" iac_status iac_calc_kmap(iac_ctx *ctx, const float *d_pm, uint64_t np
 
 // ---------------------------------------------------------------------------
 // scatter-add micro-benchmark: the L2 atomic rate that bounds the binning
-// kernels (addresses from a 64-bit mix of the update index)
+// kernels.  Each update adds 1 at a pseudo-random word chosen by a 32-bit
+// multiplicative hash and a multiply-high range reduction, so the loop body
+// is a handful of integer instructions around one RED.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint64_t mix64(uint64_t x)
-{
-    x ^= x >> 30;
-    x *= 0xbf58476d1ce4e5b9ull;
-    x ^= x >> 27;
-    x *= 0x94d049bb133111ebull;
-    x ^= x >> 31;
-    return x;
-}
-
 template <typename T>
-__global__ void scatter_add_kernel(T *__restrict__ buf, uint64_t words, uint64_t updates, uint32_t seed)
+__global__ void scatter_add_kernel(T *__restrict__ buf, uint32_t words, uint64_t updates, uint32_t seed)
 {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < updates; u += stride) {
-        uint64_t h = mix64(u ^ ((uint64_t)seed << 40));
-        atomicAdd(&buf[h % words], (T)1);
+    uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint32_t h = (uint32_t)u * 2654435761u + seed * 97u;
+    for (; u < updates; u += stride) {
+        h = h * 1664525u + 1013904223u;
+        const uint32_t x = h ^ (h >> 15);
+        atomicAdd(&buf[__umulhi(x, words)], (T)1);
     }
 }
 
@@ -304,17 +405,18 @@ extern "C" iac_status iac_bench_scatter_add(iac_ctx *ctx, void *d_buffer, uint64
                                             int word_bits, uint64_t updates, uint32_t seed,
                                             void *stream)
 {
-    IAC_REQUIRE(ctx && d_buffer && words > 0, "iac_bench_scatter_add: bad argument");
+    IAC_REQUIRE(ctx && d_buffer && words > 0 && words <= 0xffffffffull,
+                "iac_bench_scatter_add: bad argument");
     IAC_REQUIRE(word_bits == 32 || word_bits == 64, "word_bits must be 32 or 64");
     DeviceGuard g(ctx->device);
     const int threads = 256;
     const int blocks = ctx->sm_count * 8;
     if (word_bits == 64)
         scatter_add_kernel<unsigned long long><<<blocks, threads, 0, as_stream(stream)>>>(
-            (unsigned long long *)d_buffer, words, updates, seed);
+            (unsigned long long *)d_buffer, (uint32_t)words, updates, seed);
     else
         scatter_add_kernel<unsigned int><<<blocks, threads, 0, as_stream(stream)>>>(
-            (unsigned int *)d_buffer, words, updates, seed);
+            (unsigned int *)d_buffer, (uint32_t)words, updates, seed);
     IAC_LAUNCHED(ctx);
     IAC_CUDA(cudaGetLastError());
     return IAC_OK;

@@ -1,0 +1,498 @@
+// dense_pairs.cu -- (b) dense mean-intensity C(q) on the small mesh and
+// (c) the AC1D |q| histogram of the mean intensity.
+//
+// Replaces AutoCorr_CQ_small (IAC/kernel.cl:27-184, host
+// Detector::AutoCorrelate_CofQ_SmallMesh, IAC/Detector.cpp:1184-1315) and
+// AutoCorr_CQ_AV (IAC/kernel.cl:656-764, host AC1D::Calculate_CQ,
+// IAC/AC1D.cpp:61-195).
+//
+// Both reference kernels visit every ordered pixel pair (ind, i), self pairs
+// included.  The pair (i, ind) is the point reflection of (ind, i): q changes
+// sign exactly, the value I_ind*I_i is the same float, and round()/floor()
+// based binning is reflected exactly (nearest: round(-x) = -round(x); linear:
+// the corner weights 1 - (x - floor x) of -x are the reflected weights of x,
+// bit for bit).  So each unordered pair is evaluated once and its mesh
+// contribution is added at the voxel and at its reflection through the mesh
+// centre; for |q| the two orders are identical and the bin gets twice the
+// value.  Self pairs (q = 0) are added once at the centre.
+//
+// Work decomposition.  Pixels are cut into tiles of TILE consecutive pixels.
+// A persistent CTA pops tile pairs (P <= Q) from a queue: thread t owns pixel
+// P*TILE + t and walks the TILE pixels of Q, staged in shared memory as float4
+// (k, I).  Tile pairs whose k bounding boxes are farther apart than MaxQ are
+// skipped whole.  Contributions are accumulated per thread while consecutive
+// pixels of Q fall into the same voxel (row-adjacent pixels move q by a
+// fraction of a voxel), then added to a shared-memory window covering the
+// tile pair's q range, which is flushed to the global mesh (voxel and
+// reflection) once per tile pair.  Tile pairs whose window would not fit fall
+// back to global atomics.  The AC1D histogram lives in shared memory for the
+// whole launch and is flushed once per CTA.
+//
+// All FP32 operations are the reference's, in its order, without FMA
+// contraction; values are (uint64)(double(I_a*I_b) * Mult) per pair as the
+// reference's casts do, so the integer meshes are bit-identical.
+#include <algorithm>
+#include <cmath>
+
+#include "iac_internal.cuh"
+
+namespace iac {
+
+constexpr int DTILE = 256;        // pixels per tile == threads per CTA
+constexpr int WINDOW_WORDS = 2048;  // shared-memory window (16 KB of uint64)
+
+struct DenseArgs {
+    const float *__restrict__ I;
+    const float *__restrict__ K;     // 3 floats per pixel
+    const float4 *__restrict__ box;  // per tile: min (x,y,z), max (x,y,z) as 2 float4
+    unsigned long long *__restrict__ out;
+    unsigned long long *queue;
+    DeviceCounters *counters;
+    uint64_t npix;
+    uint32_t ntiles;
+    unsigned long long npairs;  // tile pairs
+    float maxq, maxq2;
+    float vpdq;
+    double mult;
+    // C(q) small mesh
+    int ab, sc, cab, cc;  // sizes and centres
+    int ka, kb, kc;       // q axis on mesh fs / ms / ss
+    // AC1D
+    uint32_t hsize;
+    float dq;
+};
+
+// tile-pair index -> (P, Q): first the ntiles diagonal pairs, then the
+// circulant walk over distinct pairs (d = l / T + 1, P = l % T, Q = P + d mod T)
+__device__ __forceinline__ void decode_tile_pair(unsigned long long p, uint32_t T, uint32_t &P,
+                                                 uint32_t &Q)
+{
+    if (p < T) {
+        P = Q = (uint32_t)p;
+        return;
+    }
+    const unsigned long long l = p - T;
+    const uint32_t d = (uint32_t)(l / T) + 1;
+    P = (uint32_t)(l % T);
+    Q = P + d;
+    if (Q >= T) Q -= T;
+}
+
+__global__ void tile_box_kernel(const float *__restrict__ K, const float *__restrict__ I,
+                                uint64_t npix, uint32_t ntiles, float4 *__restrict__ box)
+{
+    const uint32_t t = blockIdx.x;
+    const uint64_t i = (uint64_t)t * DTILE + threadIdx.x;
+    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    if (i < npix && I[i] != 0.0f) {  // zero-intensity pixels never contribute
+#pragma unroll
+        for (int d = 0; d < 3; d++) mn[d] = mx[d] = K[3 * i + d];
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+        for (int o = 16; o; o >>= 1) {
+            mn[d] = fminf(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+            mx[d] = fmaxf(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+        }
+    __shared__ float s[6][DTILE / 32];
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0)
+        for (int d = 0; d < 3; d++) {
+            s[d][w] = mn[d];
+            s[3 + d][w] = mx[d];
+        }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float r[6];
+        for (int d = 0; d < 6; d++) {
+            r[d] = s[d][0];
+            for (int j = 1; j < DTILE / 32; j++) r[d] = d < 3 ? fminf(r[d], s[d][j]) : fmaxf(r[d], s[d][j]);
+        }
+        box[2 * t] = make_float4(r[0], r[1], r[2], 0.f);
+        box[2 * t + 1] = make_float4(r[3], r[4], r[5], 0.f);
+    }
+}
+
+// lower bound of |k_a - k_b| over two boxes, inflated by a relative margin
+__device__ __forceinline__ bool boxes_beyond(const float4 a0, const float4 a1, const float4 b0,
+                                             const float4 b1, float maxq)
+{
+    const float gx = fmaxf(0.f, fmaxf(a0.x - b1.x, b0.x - a1.x));
+    const float gy = fmaxf(0.f, fmaxf(a0.y - b1.y, b0.y - a1.y));
+    const float gz = fmaxf(0.f, fmaxf(a0.z - b1.z, b0.z - a1.z));
+    if (!(a0.x <= a1.x) || !(b0.x <= b1.x)) return true;  // an empty tile
+    return sqrtf(gx * gx + gy * gy + gz * gz) > maxq * 1.0001f + 1e-6f;
+}
+
+__device__ __forceinline__ float pick(float x, float y, float z, int axis)
+{
+    return axis == 0 ? x : (axis == 1 ? y : z);
+}
+
+// --------------------------------------------------------------------------
+// C(q) small mesh
+// --------------------------------------------------------------------------
+struct Window {
+    int lo[3];  // first voxel (fs, ms, ss) of the window
+    int dim[3];
+    bool on;
+};
+
+__device__ __forceinline__ void global_put_pair(const DenseArgs &a, int fs, int ms, int ss,
+                                                unsigned long long v)
+{
+    if (v == 0) return;
+    if ((unsigned)fs >= (unsigned)a.ab || (unsigned)ms >= (unsigned)a.ab ||
+        (unsigned)ss >= (unsigned)a.sc) {
+        atomicAdd(&a.counters->out_of_mesh, 1ull);
+    } else {
+        atomicAdd(&a.out[(uint64_t)fs + (uint64_t)ms * a.ab + (uint64_t)ss * a.ab * a.ab], v);
+    }
+    const int rf = 2 * a.cab - fs, rm = 2 * a.cab - ms, rs = 2 * a.cc - ss;
+    if ((unsigned)rf >= (unsigned)a.ab || (unsigned)rm >= (unsigned)a.ab ||
+        (unsigned)rs >= (unsigned)a.sc) {
+        atomicAdd(&a.counters->out_of_mesh, 1ull);
+    } else {
+        atomicAdd(&a.out[(uint64_t)rf + (uint64_t)rm * a.ab + (uint64_t)rs * a.ab * a.ab], v);
+    }
+}
+
+__device__ __forceinline__ void put(const DenseArgs &a, const Window &w, unsigned long long *win,
+                                    int fs, int ms, int ss, unsigned long long v)
+{
+    if (v == 0) return;
+    const int x = fs - w.lo[0], y = ms - w.lo[1], z = ss - w.lo[2];
+    if (w.on && (unsigned)x < (unsigned)w.dim[0] && (unsigned)y < (unsigned)w.dim[1] &&
+        (unsigned)z < (unsigned)w.dim[2])
+        atomicAdd(&win[x + w.dim[0] * (y + w.dim[1] * z)], v);
+    else
+        global_put_pair(a, fs, ms, ss, v);
+}
+
+template <int INTERP>
+__global__ void __launch_bounds__(DTILE) cq_small_kernel(const DenseArgs a)
+{
+    __shared__ float4 sq[DTILE];
+    __shared__ unsigned long long win[WINDOW_WORDS];
+    __shared__ unsigned long long s_pair;
+    __shared__ unsigned long long s_self[DTILE / 32];
+    const uint32_t T = a.ntiles;
+    const float cabf = (float)a.cab, ccf = (float)a.cc;
+    for (;;) {
+        if (threadIdx.x == 0) s_pair = atomicAdd(a.queue, 1ull);
+        __syncthreads();
+        const unsigned long long p = s_pair;
+        if (p >= a.npairs) break;
+        uint32_t P, Q;
+        decode_tile_pair(p, T, P, Q);
+        const float4 p0 = a.box[2 * P], p1 = a.box[2 * P + 1], q0 = a.box[2 * Q], q1 = a.box[2 * Q + 1];
+        if (boxes_beyond(p0, p1, q0, q1, a.maxq)) {
+            __syncthreads();
+            continue;
+        }
+        // window over the q range of the pair (P - Q), one voxel of margin
+        Window w;
+        {
+            const float lo3[3] = {p0.x - q1.x, p0.y - q1.y, p0.z - q1.z};
+            const float hi3[3] = {p1.x - q0.x, p1.y - q0.y, p1.z - q0.z};
+            const int ax[3] = {a.ka, a.kb, a.kc};
+            const int cen[3] = {a.cab, a.cab, a.cc};
+            int words = 1;
+            for (int d = 0; d < 3; d++) {
+                const float l = (ax[d] == 0 ? lo3[0] : ax[d] == 1 ? lo3[1] : lo3[2]) * a.vpdq;
+                const float h = (ax[d] == 0 ? hi3[0] : ax[d] == 1 ? hi3[1] : hi3[2]) * a.vpdq;
+                w.lo[d] = (int)floorf(l) - 1 + cen[d];
+                w.dim[d] = (int)ceilf(h) + 2 + cen[d] - w.lo[d] + (INTERP ? 1 : 0);
+                words *= max(1, w.dim[d]);
+            }
+            w.on = words <= WINDOW_WORDS;
+            if (w.on)
+                for (int i = threadIdx.x; i < words; i += DTILE) win[i] = 0ull;
+        }
+        // stage tile Q
+        {
+            const uint64_t j = (uint64_t)Q * DTILE + threadIdx.x;
+            sq[threadIdx.x] = j < a.npix ? make_float4(a.K[3 * j], a.K[3 * j + 1], a.K[3 * j + 2], a.I[j])
+                                         : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        __syncthreads();
+        const uint64_t ia = (uint64_t)P * DTILE + threadIdx.x;
+        unsigned long long self = 0;
+        if (ia < a.npix) {
+            const float k0 = a.K[3 * ia], k1 = a.K[3 * ia + 1], k2 = a.K[3 * ia + 2];
+            const float Ia = a.I[ia];
+            if (P == Q) {
+                const double sv = (double)fmul(Ia, Ia);
+                if (!(sv < 1e-37f)) self = d2u64(dmul(sv, a.mult));
+            }
+            const int j0 = (P == Q) ? threadIdx.x + 1 : 0;
+            int cur_f = 0, cur_m = 0, cur_s = 0;
+            unsigned long long acc[INTERP ? 8 : 1];
+#pragma unroll
+            for (int c = 0; c < (INTERP ? 8 : 1); c++) acc[c] = 0;
+            bool have = false;
+            for (int j = j0; j < DTILE; j++) {
+                const float4 b = sq[j];
+                const double val = (double)fmul(Ia, b.w);
+                if (val < 1e-37f) continue;
+                float qx = fsub(k0, b.x), qy = fsub(k1, b.y), qz = fsub(k2, b.z);
+                if (fadd(fadd(fmul(qx, qx), fmul(qy, qy)), fmul(qz, qz)) > a.maxq2) continue;
+                qx = fmul(qx, a.vpdq);
+                qy = fmul(qy, a.vpdq);
+                qz = fmul(qz, a.vpdq);
+                const float qa = pick(qx, qy, qz, a.ka), qb = pick(qx, qy, qz, a.kb),
+                            qc = pick(qx, qy, qz, a.kc);
+                const double vm = dmul(val, a.mult);
+                int f, m, s;
+                if (INTERP == 0) {
+                    f = (int)fadd(round_away_f(qa), cabf);
+                    m = (int)fadd(round_away_f(qb), cabf);
+                    s = (int)fadd(round_away_f(qc), ccf);
+                } else {
+                    f = (int)fadd(floorf(qa), cabf);
+                    m = (int)fadd(floorf(qb), cabf);
+                    s = (int)fadd(floorf(qc), ccf);
+                }
+                if (!have || f != cur_f || m != cur_m || s != cur_s) {
+                    if (have) {
+                        if (INTERP == 0) {
+                            put(a, w, win, cur_f, cur_m, cur_s, acc[0]);
+                        } else {
+#pragma unroll
+                            for (int c = 0; c < 8; c++)
+                                put(a, w, win, cur_f + (c >> 2), cur_m + ((c >> 1) & 1), cur_s + (c & 1), acc[c]);
+                        }
+                    }
+                    have = true;
+                    cur_f = f;
+                    cur_m = m;
+                    cur_s = s;
+#pragma unroll
+                    for (int c = 0; c < (INTERP ? 8 : 1); c++) acc[c] = 0;
+                }
+                if (INTERP == 0) {
+                    acc[0] += d2u64(vm);
+                } else {
+                    // IAC/kernel.cl:139-179: Sep = 1 - (q - floor q) in float
+                    const double sf = (double)fsub(1.0f, fsub(qa, floorf(qa)));
+                    const double sm = (double)fsub(1.0f, fsub(qb, floorf(qb)));
+                    const double sz = (double)fsub(1.0f, fsub(qc, floorf(qc)));
+                    const double xf[2] = {sf, dsub(1.0, sf)}, yf[2] = {sm, dsub(1.0, sm)},
+                                 zf[2] = {sz, dsub(1.0, sz)};
+#pragma unroll
+                    for (int c = 0; c < 8; c++)
+                        acc[c] += d2u64(dmul(vm, dmul(dmul(xf[c >> 2], yf[(c >> 1) & 1]), zf[c & 1])));
+                }
+            }
+            if (have) {
+                if (INTERP == 0) {
+                    put(a, w, win, cur_f, cur_m, cur_s, acc[0]);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 8; c++)
+                        put(a, w, win, cur_f + (c >> 2), cur_m + ((c >> 1) & 1), cur_s + (c & 1), acc[c]);
+                }
+            }
+        }
+        // self pairs of a diagonal tile: once, at the centre
+        for (int o = 16; o; o >>= 1) self += __shfl_xor_sync(0xffffffffu, self, o);
+        if ((threadIdx.x & 31) == 0) s_self[threadIdx.x >> 5] = self;
+        __syncthreads();
+        if (threadIdx.x == 0 && P == Q) {
+            unsigned long long t = 0;
+            for (int i = 0; i < DTILE / 32; i++) t += s_self[i];
+            if (t) atomicAdd(&a.out[(uint64_t)a.cab + (uint64_t)a.cab * a.ab + (uint64_t)a.cc * a.ab * a.ab], t);
+        }
+        if (w.on) {
+            const int words = w.dim[0] * w.dim[1] * w.dim[2];
+            for (int i = threadIdx.x; i < words; i += DTILE) {
+                const unsigned long long v = win[i];
+                if (!v) continue;
+                const int x = i % w.dim[0], y = (i / w.dim[0]) % w.dim[1], z = i / (w.dim[0] * w.dim[1]);
+                global_put_pair(a, x + w.lo[0], y + w.lo[1], z + w.lo[2], v);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// --------------------------------------------------------------------------
+// AC1D C(q): |q| histogram in shared memory for the whole launch
+// --------------------------------------------------------------------------
+template <int INTERP>
+__global__ void __launch_bounds__(DTILE) ac1d_cq_kernel(const DenseArgs a)
+{
+    extern __shared__ unsigned long long hist[];
+    __shared__ float4 sq[DTILE];
+    __shared__ unsigned long long s_pair;
+    for (uint32_t i = threadIdx.x; i < a.hsize; i += DTILE) hist[i] = 0;
+    const uint32_t T = a.ntiles;
+    for (;;) {
+        if (threadIdx.x == 0) s_pair = atomicAdd(a.queue, 1ull);
+        __syncthreads();
+        const unsigned long long p = s_pair;
+        if (p >= a.npairs) break;
+        uint32_t P, Q;
+        decode_tile_pair(p, T, P, Q);
+        const float4 p0 = a.box[2 * P], p1 = a.box[2 * P + 1], q0 = a.box[2 * Q], q1 = a.box[2 * Q + 1];
+        if (boxes_beyond(p0, p1, q0, q1, a.maxq)) {
+            __syncthreads();
+            continue;
+        }
+        {
+            const uint64_t j = (uint64_t)Q * DTILE + threadIdx.x;
+            sq[threadIdx.x] = j < a.npix ? make_float4(a.K[3 * j], a.K[3 * j + 1], a.K[3 * j + 2], a.I[j])
+                                         : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        __syncthreads();
+        const uint64_t ia = (uint64_t)P * DTILE + threadIdx.x;
+        if (ia < a.npix) {
+            const float k0 = a.K[3 * ia], k1 = a.K[3 * ia + 1], k2 = a.K[3 * ia + 2];
+            const float Ia = a.I[ia];
+            if (P == Q) {  // self pair: q = 0 -> bin 0, once
+                const double sv = (double)fmul(Ia, Ia);
+                if (!(sv < 1e-37f)) atomicAdd(&hist[0], (unsigned long long)(long long)dmul(sv, a.mult));
+            }
+            const int j0 = (P == Q) ? threadIdx.x + 1 : 0;
+            for (int j = j0; j < DTILE; j++) {
+                const float4 b = sq[j];
+                const double val = (double)fmul(Ia, b.w);
+                if (val < 1e-37f) continue;
+                const float dx = fsub(k0, b.x), dy = fsub(k1, b.y), dz = fsub(k2, b.z);
+                float q = __fsqrt_rn(fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz)));
+                if (q > a.maxq) continue;
+                q = __fdiv_rn(q, a.dq);
+                if (INTERP == 0) {
+                    // sc = (uint)floor(q + 0.5) with q + 0.5 in double
+                    const uint32_t sc = (uint32_t)floor(dadd((double)q, 0.5)) % a.hsize;
+                    const unsigned long long v = (unsigned long long)(long long)dmul(val, a.mult);
+                    atomicAdd(&hist[sc], 2ull * v);
+                } else {
+                    const float fq = floorf(q);
+                    const uint32_t sc1 = (uint32_t)fq % a.hsize, sc2 = ((uint32_t)fq + 1) % a.hsize;
+                    const double sep = (double)fsub(q, fq);
+                    const unsigned long long v1 =
+                        (unsigned long long)(long long)dmul(dmul(val, dsub(1.0, sep)), a.mult);
+                    const unsigned long long v2 = (unsigned long long)(long long)dmul(dmul(val, sep), a.mult);
+                    atomicAdd(&hist[sc1], 2ull * v1);
+                    atomicAdd(&hist[sc2], 2ull * v2);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < a.hsize; i += DTILE)
+        if (hist[i]) atomicAdd(&a.out[i], hist[i]);
+}
+
+static float sqrt_threshold(float m)
+{
+    if (!(m >= 0.0f) || std::isinf(m)) return m;
+    float s = m * m;
+    while (std::sqrt(s) > m) s = std::nextafter(s, 0.0f);
+    for (;;) {
+        const float n = std::nextafter(s, INFINITY);
+        if (std::isinf(n) || std::sqrt(n) > m) break;
+        s = n;
+    }
+    return s;
+}
+
+// tile boxes + queue counter in stream scratch; returns args with common fields
+static iac_status prepare(iac_ctx *ctx, void *stream, const float *d_I, const float *d_K,
+                          uint64_t npix, DenseArgs &a)
+{
+    a.I = d_I;
+    a.K = d_K;
+    a.npix = npix;
+    a.ntiles = (uint32_t)((npix + DTILE - 1) / DTILE);
+    a.npairs = (unsigned long long)a.ntiles * (a.ntiles + 1) / 2;
+    a.counters = ctx->d_counters;
+    void *scr = nullptr;
+    const size_t box_bytes = sizeof(float4) * 2 * (size_t)a.ntiles;
+    iac_status st = stream_scratch(ctx, stream, SLOT_AUX0, box_bytes + 256, &scr);
+    if (st != IAC_OK) return st;
+    a.box = (const float4 *)scr;
+    a.queue = (unsigned long long *)((char *)scr + ((box_bytes + 127) / 128) * 128);
+    cudaStream_t s = as_stream(stream);
+    IAC_CUDA(cudaMemsetAsync(a.queue, 0, sizeof(unsigned long long), s));
+    tile_box_kernel<<<a.ntiles, DTILE, 0, s>>>(d_K, d_I, npix, a.ntiles, (float4 *)scr);
+    IAC_LAUNCHED(ctx);
+    IAC_CUDA(cudaGetLastError());
+    return IAC_OK;
+}
+
+}  // namespace iac
+
+using namespace iac;
+
+extern "C" {
+
+iac_status iac_cq_small(iac_ctx *ctx, const float *d_I, const float *d_kmap, uint64_t npix,
+                        const iac_mesh_shape *sh, int interp, double mult, uint64_t *d_mesh,
+                        void *stream)
+{
+    IAC_REQUIRE(ctx && d_I && d_kmap && sh && d_mesh, "iac_cq_small: NULL argument");
+    IAC_REQUIRE(interp == 0 || interp == 1, "interpolation must be 0 or 1");
+    IAC_REQUIRE(npix > 0 && npix < (1ull << 32), "iac_cq_small: pixel count %llu out of range",
+                (unsigned long long)npix);
+    IAC_REQUIRE(sh->size_ab >= 5 && sh->size_ab % 2 == 1 && sh->size_c >= 1 && sh->size_c % 2 == 1,
+                "small mesh sizes must be odd");
+    IAC_REQUIRE(sh->k_a < 3 && sh->k_b < 3 && sh->k_c < 3, "bad axis alignment");
+    IAC_REQUIRE(mult > 0, "multiplicator must be positive");
+    DeviceGuard g(ctx->device);
+    DenseArgs a{};
+    iac_status st = prepare(ctx, stream, d_I, d_kmap, npix, a);
+    if (st != IAC_OK) return st;
+    a.out = (unsigned long long *)d_mesh;
+    a.maxq = sh->max_q;
+    a.maxq2 = sqrt_threshold(sh->max_q);
+    a.vpdq = (float)sh->voxel_per_dq;
+    a.mult = mult;
+    a.ab = (int)sh->size_ab;
+    a.sc = (int)sh->size_c;
+    a.cab = (a.ab - 1) / 2;
+    a.cc = (a.sc - 1) / 2;
+    a.ka = (int)sh->k_a;
+    a.kb = (int)sh->k_b;
+    a.kc = (int)sh->k_c;
+    const int grid = ctx->sm_count * 4;
+    if (interp == 0)
+        cq_small_kernel<0><<<grid, DTILE, 0, as_stream(stream)>>>(a);
+    else
+        cq_small_kernel<1><<<grid, DTILE, 0, as_stream(stream)>>>(a);
+    IAC_LAUNCHED(ctx);
+    IAC_CUDA(cudaGetLastError());
+    return IAC_OK;
+}
+
+iac_status iac_ac1d_cq(iac_ctx *ctx, const float *d_I, const float *d_kmap, uint64_t npix,
+                       const iac_ac1d_shape *sh, int interp, double mult, uint64_t *d_hist,
+                       void *stream)
+{
+    IAC_REQUIRE(ctx && d_I && d_kmap && sh && d_hist, "iac_ac1d_cq: NULL argument");
+    IAC_REQUIRE(interp == 0 || interp == 1, "interpolation must be 0 or 1");
+    IAC_REQUIRE(npix > 0 && npix < (1ull << 32), "iac_ac1d_cq: pixel count out of range");
+    IAC_REQUIRE(sh->size >= 3 && sh->size <= 24576, "AC1D size %u out of range [3, 24576]", sh->size);
+    IAC_REQUIRE(mult > 0, "multiplicator must be positive");
+    DeviceGuard g(ctx->device);
+    DenseArgs a{};
+    iac_status st = prepare(ctx, stream, d_I, d_kmap, npix, a);
+    if (st != IAC_OK) return st;
+    a.out = (unsigned long long *)d_hist;
+    a.maxq = sh->max_q;
+    a.maxq2 = sqrt_threshold(sh->max_q);
+    a.mult = mult;
+    a.hsize = sh->size;
+    a.dq = sh->dq_per_step;
+    const size_t smem = sizeof(unsigned long long) * sh->size;
+    auto k = interp == 0 ? ac1d_cq_kernel<0> : ac1d_cq_kernel<1>;
+    IAC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<ctx->sm_count * 4, DTILE, smem, as_stream(stream)>>>(a);
+    IAC_LAUNCHED(ctx);
+    IAC_CUDA(cudaGetLastError());
+    return IAC_OK;
+}
+
+}  // extern "C"

@@ -10,6 +10,7 @@
 #include <mutex>
 #include <string>
 #include <unordered_map>
+#include <vector>
 
 #include "../../include/iac_b200.h"
 
@@ -84,7 +85,11 @@ struct iac_ctx {
     iac::DeviceCounters *d_counters = nullptr;
     iac::Scratch sparse_scratch;
     std::unordered_map<void *, iac::StreamScratch> stream_scratch;  // keyed by stream
-    iac_sparse_tuning tuning{};
+    iac_sparse_tuning tuning{};  // explicit override (zeros: use the table)
+    struct TuningRow {
+        uint32_t edge, tile_pairs, block_threads, ctas_per_sm;
+    };
+    std::vector<TuningRow> tuning_table;  // autotuner results, tuning/sparse_tuning.tsv
     cudaStream_t host_stream = nullptr;  // stream of the host-buffer entry points
     std::atomic<uint64_t> launches{0};
 };
@@ -144,5 +149,35 @@ __device__ __forceinline__ float rot_row(float a, float b, float c, float r0, fl
 
 // C cast (unsigned long)(double) for the non-negative values of the path.
 __device__ __forceinline__ unsigned long long d2u64(double x) { return __double2ull_rz(x); }
+
+// ---------------------------------------------------------------------------
+// round half away from zero (C round / OpenCL round) with FP32 adds only.
+// (|x| + 1.5*2^23) - 1.5*2^23 rounds |x| to the nearest integer, ties to even;
+// a tie that went down is moved up.  Exact for |x| < 2^22; larger magnitudes
+// (which only non-orthonormal rotations produce) take roundf.
+// ---------------------------------------------------------------------------
+constexpr float ROUND_MAGIC = 12582912.0f;  // 1.5 * 2^23
+constexpr int ROUND_MAGIC_BITS = 0x4B400000;
+
+__device__ __forceinline__ float round_away_f(float x)
+{
+    const float a = fabsf(x);
+    if (!(a < 4194304.0f)) return roundf(x);
+    float r = fsub(fadd(a, ROUND_MAGIC), ROUND_MAGIC);
+    if (fsub(a, r) == 0.5f) r = fadd(r, 1.0f);
+    return copysignf(r, x);
+}
+
+// round_away_f(x) as int, for |x| < 2^22; larger magnitudes return a value far
+// outside every mesh (the caller's bounds check rejects it).
+__device__ __forceinline__ int round_away_i(float x)
+{
+    const float a = fabsf(x);
+    if (!(a < 4194304.0f)) return 1 << 30;
+    const float y = fadd(a, ROUND_MAGIC);
+    int r = __float_as_int(y) - ROUND_MAGIC_BITS;
+    if (fsub(a, fsub(y, ROUND_MAGIC)) == 0.5f) r += 1;
+    return x < 0.0f ? -r : r;
+}
 
 }  // namespace iac

@@ -35,6 +35,7 @@
 // mesh (possible only for non-orthonormal rotations; the reference writes them
 // out of bounds) are skipped and counted in the context's error block.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -53,9 +54,13 @@ struct SparseArgs {
     uint32_t nframes;
     uint32_t tile_pairs;
     int S, C, half_ss;
+    uint32_t plane;  // S * S (the half mesh has fewer than 2^32 words for S <= 1621)
     float maxq;
-    float vpdq;  // (float)Voxel_per_dq
+    float maxq2;  // largest float s with sqrtf(s) <= maxq: |q| > maxq  <=>  |q|^2 > maxq2
+    float vpdq;   // (float)Voxel_per_dq
     double mult;
+    float mult_f;                           // Multiplicator as float when it is an integer <= 1024
+    const unsigned char *__restrict__ small_counts;  // per frame: counts are integers in [0, 128]
 };
 
 // ---------------------------------------------------------------------------
@@ -114,6 +119,27 @@ __global__ void __launch_bounds__(PLAN_THREADS)
 }
 
 // ---------------------------------------------------------------------------
+// per-frame check: are all photon values integers in [0, 128]?  Then the pair
+// value v_lo * v_hi * Mult (Mult an integer <= 1024) is at most 2^24 and the
+// FP32 product is exact, equal to the reference's double product.
+// One warp per frame.
+// ---------------------------------------------------------------------------
+__global__ void sparse_count_check_kernel(const float4 *__restrict__ ph, const uint64_t *__restrict__ off,
+                                          uint32_t nframes, unsigned char *__restrict__ flags)
+{
+    const uint32_t f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (f >= nframes) return;
+    bool ok = true;
+    for (uint64_t i = off[f] + lane; i < off[f + 1]; i += 32) {
+        const float w = ph[i].w;
+        ok &= (w >= 0.0f) && (w <= 128.0f) && (w == truncf(w));
+    }
+    ok = __all_sync(0xffffffffu, ok);
+    if (lane == 0) flags[f] = ok ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------
 // binning helpers (IAC/kernel.cl:349-448)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void hm_put(const SparseArgs &a, int fs, int ms, int ss,
@@ -125,7 +151,7 @@ __device__ __forceinline__ void hm_put(const SparseArgs &a, int fs, int ms, int 
         return;
     }
     if (v == 0) return;
-    atomicAdd(&a.half[(size_t)fs + (size_t)ms * a.S + (size_t)ss * a.S * a.S], v);
+    atomicAdd(&a.half[(uint32_t)fs + (uint32_t)ms * (uint32_t)a.S + (uint32_t)ss * a.plane], v);
 }
 
 // AddQToPositiveSS, IAC/kernel.cl:349-372 (q != 0 here; q = 0 is the self pair)
@@ -140,6 +166,26 @@ __device__ __forceinline__ void add_positive_ss(const SparseArgs &a, int fs, int
     }
 }
 
+// Second-level nearest neighbour of AddRotatedQToMesh (IAC/kernel.cl:380-389)
+// followed by AddQToPositiveSS: fs = C + round(q0), ms = C + round(q1),
+// ss = round(q2); a negative ss goes to the point reflection, ss = 0 goes to
+// both.  (The reference adds the float centre to the rounded float, which is
+// exact for every in-mesh index.)
+__device__ __forceinline__ void add_nearest(const SparseArgs &a, float q0, float q1, float q2,
+                                            unsigned long long v)
+{
+    int fs = a.C + round_away_i(q0);
+    int ms = a.C + round_away_i(q1);
+    int ss = round_away_i(q2);
+    if (ss < 0) {
+        fs = 2 * a.C - fs;
+        ms = 2 * a.C - ms;
+        ss = -ss;
+    }
+    hm_put(a, fs, ms, ss, v);
+    if (ss == 0) hm_put(a, 2 * a.C - fs, 2 * a.C - ms, 0, v);
+}
+
 // AddRotatedQToMesh, IAC/kernel.cl:374-448
 template <int I2>
 __device__ __forceinline__ void add_rotated(const SparseArgs &a, double val, float q0, float q1,
@@ -148,10 +194,7 @@ __device__ __forceinline__ void add_rotated(const SparseArgs &a, double val, flo
     const float Cf = (float)a.C;
     if (I2 == 0) {
         const unsigned long long v = d2u64(dmul(val, a.mult));
-        const int fs = (int)fadd(Cf, roundf(q0));
-        const int ms = (int)fadd(Cf, roundf(q1));
-        const int ss = (int)roundf(q2);
-        add_positive_ss(a, fs, ms, ss, v);
+        add_nearest(a, q0, q1, q2, v);
     } else {
         const float f0 = floorf(q0), f1 = floorf(q1), f2 = floorf(q2);
         const double sf = dsub(1.0, (double)fsub(q0, f0));
@@ -177,22 +220,37 @@ __device__ __forceinline__ void add_rotated(const SparseArgs &a, double val, flo
 // (IAC/kernel.cl:493-649).
 template <int DMAP, int I1, int I2>
 __device__ __forceinline__ void bin_pair(const SparseArgs &a, const float4 A, const float4 B,
-                                         const float *R)
+                                         const float *R, const bool small_counts)
 {
     float q0 = fsub(A.x, B.x), q1 = fsub(A.y, B.y), q2 = fsub(A.z, B.z);
-    if (norm3(q0, q1, q2) > a.maxq) return;
+    // sqrt(|q|^2) > MaxQ, decided on |q|^2 against the exact float threshold
+    if (fadd(fadd(fmul(q0, q0), fmul(q1, q1)), fmul(q2, q2)) > a.maxq2) return;
     q0 = fmul(q0, a.vpdq);
     q1 = fmul(q1, a.vpdq);
     q2 = fmul(q2, a.vpdq);
-    const double val = dmul((double)A.w, (double)B.w);
     const int C = a.C;
     const float Cf = (float)C;
+    if (I2 == 0 && (DMAP == 0 || I1 == 0)) {
+        // nearest neighbour at the second level: value (ulong)(v_lo * v_hi * Mult)
+        unsigned long long v;
+        if (small_counts)  // integers <= 128 and Mult <= 1024: the float product is exact
+            v = (unsigned long long)__float2uint_rz(fmul(fmul(A.w, B.w), a.mult_f));
+        else
+            v = d2u64(dmul(dmul((double)A.w, (double)B.w), a.mult));
+        float t0 = q0, t1 = q1, t2 = q2;
+        if (DMAP) {  // first-level nearest neighbour: back to the voxel centre
+            t0 = round_away_f(q0);
+            t1 = round_away_f(q1);
+            t2 = round_away_f(q2);
+        }
+        add_nearest(a, rot_row(t0, t1, t2, R[0], R[1], R[2]), rot_row(t0, t1, t2, R[3], R[4], R[5]),
+                    rot_row(t0, t1, t2, R[6], R[7], R[8]), v);
+        return;
+    }
+    const double val = dmul((double)A.w, (double)B.w);
     if (DMAP) {
         if (I1 == 0) {
-            const int fs = (int)fadd(roundf(q0), Cf);
-            const int ms = (int)fadd(roundf(q1), Cf);
-            const int ss = (int)fadd(roundf(q2), Cf);
-            const float r0 = (float)(fs - C), r1 = (float)(ms - C), r2 = (float)(ss - C);
+            const float r0 = round_away_f(q0), r1 = round_away_f(q1), r2 = round_away_f(q2);
             add_rotated<I2>(a, val, rot_row(r0, r1, r2, R[0], R[1], R[2]),
                             rot_row(r0, r1, r2, R[3], R[4], R[5]),
                             rot_row(r0, r1, r2, R[6], R[7], R[8]));
@@ -236,6 +294,7 @@ __global__ void __launch_bounds__(256) sparse_pairs_kernel(const SparseArgs a)
     __shared__ unsigned long long s_tile;
     __shared__ uint32_t s_frame;
     __shared__ float s_rot[9];
+    __shared__ int s_small;
     __shared__ unsigned long long s_self[8];
 
     const unsigned long long ntiles = a.tile_off[a.nframes];
@@ -255,6 +314,7 @@ __global__ void __launch_bounds__(256) sparse_pairs_kernel(const SparseArgs a)
                         hi = mid;
                 }
                 s_frame = lo;
+                s_small = a.small_counts ? a.small_counts[lo] : 0;
 #pragma unroll
                 for (int k = 0; k < 9; k++) s_rot[k] = a.rot[9 * (size_t)lo + k];
             }
@@ -263,6 +323,7 @@ __global__ void __launch_bounds__(256) sparse_pairs_kernel(const SparseArgs a)
         const unsigned long long t = s_tile;
         if (t >= ntiles) break;
         const uint32_t f = s_frame;
+        const bool small = s_small != 0;
         float R[9];
 #pragma unroll
         for (int k = 0; k < 9; k++) R[k] = s_rot[k];
@@ -295,7 +356,7 @@ __global__ void __launch_bounds__(256) sparse_pairs_kernel(const SparseArgs a)
                 uint32_t j = i + d;
                 if (j >= n) j -= n;
                 const uint32_t lo = min(i, j), hi = max(i, j);
-                bin_pair<DMAP, I1, I2>(a, P[lo], P[hi], R);
+                bin_pair<DMAP, I1, I2>(a, P[lo], P[hi], R, small);
                 i += dr;
                 d += dq;
                 if (i >= n) {
@@ -336,6 +397,100 @@ __global__ void sparse_fold_kernel(const unsigned long long *__restrict__ half, 
     }
 }
 
+// ---------------------------------------------------------------------------
+// AC1D of sparse photon lists: AutoCorr_sparseHL_AAV (IAC/kernel.cl:863-950)
+// summed over frames.  Every ordered pair of a frame, self pairs included,
+// adds (uint64)(v_a * v_b * Mult) at bin floor(|q|/dq + 0.5) (nearest) or
+// splits it over floor(|q|/dq) and the next bin (linear).  The two orders of
+// a distinct pair give the same |q| and value, so each distinct pair adds
+// twice its value.  Bins are taken modulo VecSize, which is what the
+// reference's sub-histogram layout and index-modulo fold (IAC/AC1D.cpp:366-375)
+// do to bins at or beyond VecSize.  The histogram lives in shared memory for
+// the whole launch.  Work queue and pair enumeration are the pair kernel's.
+// ---------------------------------------------------------------------------
+template <int INTERP>
+__global__ void __launch_bounds__(256) ac1d_sparse_kernel(const SparseArgs a, float maxq, float dqdx,
+                                                          uint32_t vecsize,
+                                                          unsigned long long *__restrict__ out)
+{
+    extern __shared__ unsigned long long hist[];
+    __shared__ unsigned long long s_tile;
+    __shared__ uint32_t s_frame;
+    for (uint32_t i = threadIdx.x; i < vecsize; i += blockDim.x) hist[i] = 0;
+    const unsigned long long ntiles = a.tile_off[a.nframes];
+    const uint32_t nthr = blockDim.x;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const unsigned long long t = atomicAdd(a.queue, 1ull);
+            s_tile = t;
+            if (t < ntiles) {
+                uint32_t lo = 0, hi = a.nframes;
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (a.tile_off[mid] <= t) lo = mid; else hi = mid;
+                }
+                s_frame = lo;
+            }
+        }
+        __syncthreads();
+        const unsigned long long t = s_tile;
+        if (t >= ntiles) break;
+        const uint32_t f = s_frame;
+        const uint64_t base = a.offsets[f];
+        const uint32_t n = (uint32_t)(a.offsets[f + 1] - base);
+        const unsigned long long chunk = t - a.tile_off[f];
+        const float4 *__restrict__ P = a.photons + base;
+        if (chunk == 0)  // self pairs: q = 0, bin 0 (linear: bin 0 gets all of it, bin 1 nothing)
+            for (uint32_t i = threadIdx.x; i < n; i += nthr) {
+                const double v = (double)P[i].w;
+                const unsigned long long w = d2u64(dmul(dmul(v, v), a.mult));
+                if (w) atomicAdd(&hist[0], w);
+            }
+        const unsigned long long npairs = (unsigned long long)n * (n - 1) / 2;
+        const unsigned long long p0 = chunk * a.tile_pairs;
+        const unsigned long long p1 = min(npairs, p0 + a.tile_pairs);
+        if (p0 + threadIdx.x < p1) {
+            unsigned long long l = p0 + threadIdx.x;
+            uint32_t d = (uint32_t)(l / n) + 1;
+            uint32_t i = (uint32_t)(l - (unsigned long long)(d - 1) * n);
+            const uint32_t dq = nthr / n, dr = nthr % n;
+            for (; l < p1; l += nthr) {
+                uint32_t j = i + d;
+                if (j >= n) j -= n;
+                const float4 A = P[min(i, j)], B = P[max(i, j)];
+                const float dx = fsub(A.x, B.x), dy = fsub(A.y, B.y), dz = fsub(A.z, B.z);
+                float q = __fsqrt_rn(fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz)));
+                if (!(q > maxq)) {
+                    q = __fdiv_rn(q, dqdx);
+                    const double val = dmul((double)A.w, (double)B.w);
+                    if (INTERP == 0) {
+                        const uint32_t sc = (uint32_t)floor(dadd((double)q, 0.5)) % vecsize;
+                        const unsigned long long w = d2u64(dmul(val, a.mult));
+                        if (w) atomicAdd(&hist[sc], 2ull * w);
+                    } else {
+                        const float fq = floorf(q);
+                        const double sep = (double)fsub(q, fq);
+                        const unsigned long long w1 = d2u64(dmul(dmul(val, dsub(1.0, sep)), a.mult));
+                        const unsigned long long w2 = d2u64(dmul(dmul(val, sep), a.mult));
+                        if (w1) atomicAdd(&hist[(uint32_t)fq % vecsize], 2ull * w1);
+                        if (w2) atomicAdd(&hist[((uint32_t)fq + 1) % vecsize], 2ull * w2);
+                    }
+                }
+                i += dr;
+                d += dq;
+                if (i >= n) {
+                    i -= n;
+                    d += 1;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < vecsize; i += blockDim.x)
+        if (hist[i]) atomicAdd(&out[i], hist[i]);
+}
+
 typedef void (*PairKernel)(const SparseArgs);
 
 static PairKernel pick_kernel(int dmap, int i1, int i2)
@@ -345,17 +500,46 @@ static PairKernel pick_kernel(int dmap, int i1, int i2)
     return i2 ? sparse_pairs_kernel<1, 1, 1> : sparse_pairs_kernel<1, 1, 0>;
 }
 
-static iac_sparse_tuning effective_tuning(iac_ctx *ctx)
+// Explicit settings win; otherwise the autotuner row of the nearest mesh edge;
+// otherwise built-in defaults.
+static iac_sparse_tuning effective_tuning(iac_ctx *ctx, uint32_t size_ab)
 {
     iac_sparse_tuning t;
     {
         std::lock_guard<std::mutex> lk(ctx->mu);
         t = ctx->tuning;
+        if (!ctx->tuning_table.empty() && size_ab >= 2) {
+            const uint32_t edge = size_ab - 2;
+            const iac_ctx::TuningRow *best = nullptr;
+            for (const auto &r : ctx->tuning_table)
+                if (!best || (r.edge > edge ? r.edge - edge : edge - r.edge) <
+                                 (best->edge > edge ? best->edge - edge : edge - best->edge))
+                    best = &r;
+            if (t.tile_pairs == 0) t.tile_pairs = best->tile_pairs;
+            if (t.block_threads == 0) t.block_threads = best->block_threads;
+            if (t.ctas_per_sm == 0) t.ctas_per_sm = best->ctas_per_sm;
+        }
     }
     if (t.tile_pairs == 0) t.tile_pairs = 4096;
     if (t.block_threads == 0) t.block_threads = 256;
     if (t.ctas_per_sm == 0) t.ctas_per_sm = 8;
     return t;
+}
+
+// Largest float s with sqrtf(s) <= m: since IEEE sqrt is monotonic,
+// sqrtf(x) > m exactly when x > s (host sqrtf is correctly rounded like the
+// device's __fsqrt_rn).
+static float sqrt_threshold(float m)
+{
+    if (!(m >= 0.0f) || std::isinf(m)) return m;
+    float s = m * m;
+    while (std::sqrt(s) > m) s = std::nextafter(s, 0.0f);
+    for (;;) {
+        const float n = std::nextafter(s, INFINITY);
+        if (std::isinf(n) || std::sqrt(n) > m) break;
+        s = n;
+    }
+    return s;
 }
 
 static iac_status check_params(const iac_sparse_params *p)
@@ -364,7 +548,7 @@ static iac_status check_params(const iac_sparse_params *p)
     const iac_mesh_shape &s = p->shape;
     IAC_REQUIRE(s.size_ab >= 5 && (s.size_ab % 2) == 1 && s.size_c == s.size_ab,
                 "sparse pair mesh must be cubic with an odd edge (got %u x %u)", s.size_ab, s.size_c);
-    IAC_REQUIRE(s.size_ab <= 2047, "mesh edge %u too large", s.size_ab);
+    IAC_REQUIRE(s.size_ab <= 1621, "mesh edge %u too large (at most 1621)", s.size_ab);
     IAC_REQUIRE(s.voxel_per_dq > 0, "Voxel_per_dq is 0");
     IAC_REQUIRE(p->interp_first == 0 || p->interp_first == 1, "interp_first must be 0 or 1");
     IAC_REQUIRE(p->interp_second == 0 || p->interp_second == 1, "interp_second must be 0 or 1");
@@ -391,10 +575,10 @@ iac_status iac_sparse_set_tuning(iac_ctx *ctx, const iac_sparse_tuning *t)
     return IAC_OK;
 }
 
-iac_status iac_sparse_get_tuning(iac_ctx *ctx, iac_sparse_tuning *t)
+iac_status iac_sparse_get_tuning(iac_ctx *ctx, uint32_t size_ab, iac_sparse_tuning *t)
 {
     IAC_REQUIRE(ctx && t, "iac_sparse_get_tuning: NULL argument");
-    *t = effective_tuning(ctx);
+    *t = effective_tuning(ctx, size_ab);
     return IAC_OK;
 }
 
@@ -410,20 +594,31 @@ iac_status iac_sparse_ac_batch(iac_ctx *ctx, const float *d_photons, const uint6
     IAC_REQUIRE((reinterpret_cast<uintptr_t>(d_photons) & 15) == 0,
                 "photon array must be 16-byte aligned (float4 per photon)");
     DeviceGuard g(ctx->device);
-    const iac_sparse_tuning tun = effective_tuning(ctx);
+    const iac_sparse_tuning tun = effective_tuning(ctx, p->shape.size_ab);
 
     void *scratch = nullptr;
-    const size_t table_bytes = sizeof(unsigned long long) * ((size_t)nframes + 1);
-    st = stream_scratch(ctx, stream, SLOT_TILES, table_bytes + 256, &scratch);
+    const size_t table_bytes = ((sizeof(unsigned long long) * ((size_t)nframes + 1) + 127) / 128) * 128;
+    st = stream_scratch(ctx, stream, SLOT_TILES, table_bytes + 128 + nframes, &scratch);
     if (st != IAC_OK) return st;
     unsigned long long *tile_off = (unsigned long long *)scratch;
-    unsigned long long *queue =
-        (unsigned long long *)((char *)scratch + ((table_bytes + 127) / 128) * 128);
+    unsigned long long *queue = (unsigned long long *)((char *)scratch + table_bytes);
+    unsigned char *flags = (unsigned char *)scratch + table_bytes + 128;
 
     cudaStream_t s = as_stream(stream);
     sparse_plan_kernel<<<1, PLAN_THREADS, 0, s>>>(d_off, nframes, tun.tile_pairs, tile_off, queue);
     IAC_LAUNCHED(ctx);
     IAC_CUDA(cudaGetLastError());
+    const bool mult_small_int = p->multiplicator >= 1.0 && p->multiplicator <= 1024.0 &&
+                                p->multiplicator == std::floor(p->multiplicator);
+    if (mult_small_int && p->interp_second == 0 && !(p->double_map && p->interp_first == 1)) {
+        const uint32_t blocks = (uint32_t)(((uint64_t)nframes * 32 + 255) / 256);
+        sparse_count_check_kernel<<<blocks, 256, 0, s>>>(
+            reinterpret_cast<const float4 *>(d_photons), d_off, nframes, flags);
+        IAC_LAUNCHED(ctx);
+        IAC_CUDA(cudaGetLastError());
+    } else {
+        flags = nullptr;
+    }
 
     SparseArgs a;
     a.photons = reinterpret_cast<const float4 *>(d_photons);
@@ -438,9 +633,13 @@ iac_status iac_sparse_ac_batch(iac_ctx *ctx, const float *d_photons, const uint6
     a.S = (int)p->shape.size_ab;
     a.C = (a.S - 1) / 2;
     a.half_ss = (a.S + 1) / 2;
+    a.plane = (uint32_t)a.S * (uint32_t)a.S;
     a.maxq = p->shape.max_q;
+    a.maxq2 = sqrt_threshold(p->shape.max_q);
     a.vpdq = (float)p->shape.voxel_per_dq;
     a.mult = p->multiplicator;
+    a.mult_f = (float)p->multiplicator;
+    a.small_counts = flags;
 
     const PairKernel k = pick_kernel(p->double_map, p->interp_first, p->interp_second);
     const int grid = ctx->sm_count * (int)tun.ctas_per_sm;
@@ -448,6 +647,53 @@ iac_status iac_sparse_ac_batch(iac_ctx *ctx, const float *d_photons, const uint6
     IAC_LAUNCHED(ctx);
     IAC_CUDA(cudaGetLastError());
     return IAC_OK;
+}
+
+iac_status iac_ac1d_sparse_batch(iac_ctx *ctx, const float *d_photons, const uint64_t *d_off,
+                                 uint32_t nframes, float max_q, float dqdx, int interp,
+                                 double mult, uint64_t *d_hist, void *stream)
+{
+    IAC_REQUIRE(ctx != nullptr, "iac_ac1d_sparse_batch: ctx is NULL");
+    IAC_REQUIRE(interp == 0 || interp == 1, "interpolation must be 0 or 1");
+    IAC_REQUIRE(dqdx > 0 && max_q > 0, "iac_ac1d_sparse_batch: MaxQ and dq must be positive");
+    IAC_REQUIRE(mult > 0, "multiplicator must be positive");
+    const uint32_t vecsize = iac_ac1d_vecsize(max_q, dqdx);
+    IAC_REQUIRE(vecsize >= 1 && vecsize <= 24576, "VecSize %u out of range [1, 24576]", vecsize);
+    if (nframes == 0) return IAC_OK;
+    IAC_REQUIRE(d_photons && d_off && d_hist, "iac_ac1d_sparse_batch: NULL pointer");
+    DeviceGuard g(ctx->device);
+    const iac_sparse_tuning tun = effective_tuning(ctx, 0);
+    void *scratch = nullptr;
+    const size_t table_bytes = ((sizeof(unsigned long long) * ((size_t)nframes + 1) + 127) / 128) * 128;
+    iac_status st = stream_scratch(ctx, stream, SLOT_TILES, table_bytes + 128 + nframes, &scratch);
+    if (st != IAC_OK) return st;
+    unsigned long long *tile_off = (unsigned long long *)scratch;
+    unsigned long long *queue = (unsigned long long *)((char *)scratch + table_bytes);
+    cudaStream_t s = as_stream(stream);
+    sparse_plan_kernel<<<1, PLAN_THREADS, 0, s>>>(d_off, nframes, tun.tile_pairs, tile_off, queue);
+    IAC_LAUNCHED(ctx);
+    IAC_CUDA(cudaGetLastError());
+    SparseArgs a{};
+    a.photons = reinterpret_cast<const float4 *>(d_photons);
+    a.offsets = d_off;
+    a.tile_off = tile_off;
+    a.queue = queue;
+    a.counters = ctx->d_counters;
+    a.nframes = nframes;
+    a.tile_pairs = tun.tile_pairs;
+    a.mult = mult;
+    const size_t smem = sizeof(unsigned long long) * vecsize;
+    auto k = interp == 0 ? ac1d_sparse_kernel<0> : ac1d_sparse_kernel<1>;
+    IAC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<ctx->sm_count * 4, 256, smem, s>>>(a, max_q, dqdx, vecsize, (unsigned long long *)d_hist);
+    IAC_LAUNCHED(ctx);
+    IAC_CUDA(cudaGetLastError());
+    return IAC_OK;
+}
+
+uint32_t iac_ac1d_vecsize(float max_q, float dqdx)
+{
+    return (uint32_t)((int)std::ceil(max_q / dqdx) - 1);
 }
 
 iac_status iac_sparse_fold(iac_ctx *ctx, const uint64_t *d_half, uint32_t S, uint64_t *d_full,

@@ -629,6 +629,10 @@ void iaco_cq_merge_weights(const float *R, const float *MI, uint32_t nf, const d
     double t = 0;
     for (uint64_t i = 0; i < small_n; i++) t += cq[i];
     double mean_cq = t / (double)(int)small_n;
+    if (!(mean_cq > 0) || !(maxw > 0)) { /* the reference's search would not end */
+        *mult_out = 0;
+        return;
+    }
     double m = 1e-12;
     for (; 1 > maxw * maxw * mean_cq * m;) m *= 10;
     uint64_t oom = 1;
