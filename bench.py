@@ -20,6 +20,7 @@ and the per-rank meshes are summed on rank 0 with one NCCL reduce per step.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -48,6 +49,10 @@ def parse():
     ap.add_argument("--cpu-frames", type=int, default=1500,
                     help="frames per CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel", default="sparse",
+                    choices=["sparse", "cq_small", "ac1d_cq", "cq_merge", "ac1d_sparse", "simulate"],
+                    help="sparse is the headline; the others measure the remaining kernels "
+                         "of the path on their configurations")
     return ap.parse_args()
 
 
@@ -396,8 +401,277 @@ def run_ours(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# the other kernels of the path, each on its configuration (one JSON line)
+# ---------------------------------------------------------------------------
+def _fp32_peak_tflops(clock_mhz):
+    """FP32 FMA peak of 148 SMs x 128 lanes x 2 flop at the sampled clock (no
+    measured FP32 figure exists for this pool; derived, not measured)."""
+    return 148 * 128 * 2 * clock_mhz * 1e6 / 1e12
+
+
+def _time(fn, steps, warmup, stream):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps
+
+
+def _dense_inputs(ny, nx, gap=None):
+    from incohautocorrelate_b200 import workloads as W
+    I = W.radial_mean_intensity(ny, nx, 300.0, 0.02, 0.05, seed=3)
+    pm = W.flat_pixel_map(ny, nx, gap_x=2e-3 if gap else 0.0, gap_after=gap)
+    km, mq = W.kmap_numpy(pm)
+    return I, km, mq
+
+
+def run_kernel(args):
+    import torch
+    from incohautocorrelate_b200 import capi
+    from incohautocorrelate_b200 import workloads as W
+    torch.cuda.set_device(0)
+    ctx = capi.Context(0)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    nthreads = cores()
+    clocks = ClockSampler(0)
+    line = {"metric": None, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic",
+            "kernel": args.kernel}
+    import oracle
+    if args.kernel in ("cq_small", "ac1d_cq"):
+        I, km, mq = _dense_inputs(1024, 1024)
+        npix = I.size
+        dI, dk = torch.from_numpy(I).cuda(), torch.from_numpy(km).cuda()
+        pairs = npix * (npix + 1) // 2
+        if args.kernel == "cq_small":
+            sh = capi.small_cq_mesh_shape(mq, 253)
+            mult = capi.cq_small_multiplicator(I)
+            out = torch.zeros(sh.size_ab * sh.size_ab * sh.size_c, dtype=torch.int64, device="cuda")
+            fn = lambda: (out.zero_(), ctx.cq_small(dI, dk, npix, sh, 0, mult, out, sp))
+            shape_desc = f"small C(q) mesh {sh.size_ab}x{sh.size_ab}x{sh.size_c}"
+        else:
+            sh = capi.ac1d_shape(mq, 2048)
+            mult = capi.ac1d_cq_multiplicator(I)
+            out = torch.zeros(sh.size, dtype=torch.int64, device="cuda")
+            fn = lambda: (out.zero_(), ctx.ac1d_cq(dI, dk, npix, sh, 1, mult, out, sp))
+            shape_desc = "AC1D 2048 bins, linear"
+        clocks.start()
+        ms = _time(fn, args.steps, min(args.warmup, 1), stream)
+        clk = clocks.stop()
+        rate = pairs / (ms * 1e-3)
+        # FP32 work per unordered pair: diff 3, norm 5, product 1, scale 3 (3D) / div 1
+        flops = 12.0
+        mhz = clk["sm_mhz"] or 1965.0
+        line.update(metric=f"pixel pairs/s into {shape_desc}", value=rate, unit="pairs/s",
+                    ms_per_step=ms, dtype="fp32+u64",
+                    config={"workload": "1024x1024 radial mean intensity, 5% masked, "
+                                        "all 5.5e11 unordered pixel pairs", "pixels": npix},
+                    clocks=clk,
+                    roofline={"bound": "fp32", "achieved": rate * flops / 1e12,
+                              "peak": _fp32_peak_tflops(mhz), "unit": "TFLOP/s",
+                              "frac": rate * flops / 1e12 / _fp32_peak_tflops(mhz),
+                              "peak_source": "derived 148 SM x 128 FP32 lanes x 2 at the sampled "
+                                             "clock (no measured FP32 peak)",
+                              "flop_per_pair": flops})
+        if not args.no_cpu_baseline:
+            rows = 48
+            Ih = np.ascontiguousarray(I)
+            t0 = time.perf_counter()
+            if args.kernel == "cq_small":
+                so = oracle.small_cq_mesh_shape(mq, 253)
+                m = np.zeros(so.size_ab * so.size_ab * so.size_c, np.uint64)
+                oracle.lib().iaco_cq_small(oracle.p(Ih), oracle.p(km), npix, so, 0, mult,
+                                           npix // 2, npix // 2 + rows, oracle.p(m))
+            else:
+                so = oracle.ac1d_shape(mq, 2048)
+                m = np.zeros(so.size, np.uint64)
+                oracle.lib().iaco_ac1d_cq(oracle.p(Ih), oracle.p(km), npix, so, 1, mult,
+                                          npix // 2, npix // 2 + rows, oracle.p(m))
+            dt = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": rows * npix / 2 / dt, "unit": "pairs/s",
+                                    "cores": nthreads, "kind": "port",
+                                    "sample": f"{rows} rows x {npix} pixels of the reference's "
+                                              f"ordered-pair loop ({dt:.1f} s), counted as "
+                                              "unordered pairs (2 ordered = 1)"}
+    elif args.kernel == "cq_merge":
+        I, km, mq = _dense_inputs(512, 1024, gap=512)
+        npix = I.size
+        sh = capi.small_cq_mesh_shape(mq, 199)
+        mult = capi.cq_small_multiplicator(I)
+        small_u = torch.zeros(sh.size_ab * sh.size_ab * sh.size_c, dtype=torch.int64, device="cuda")
+        ctx.cq_small(torch.from_numpy(I).cuda(), torch.from_numpy(km).cuda(), npix, sh, 0, mult,
+                     small_u, sp)
+        small = (small_u.cpu().numpy().view(np.uint64).astype(np.float64) / mult)
+        nf = args.frames
+        R = W.haar_rotations(nf, seed=3)
+        MI = np.random.default_rng(4).uniform(0.5e-4, 4e-4, nf).astype(np.float32)
+        rw, m = capi.cq_merge_weights(R, MI, small)
+        d_small, d_rw = torch.from_numpy(small).cuda(), torch.from_numpy(rw).cuda()
+        big = torch.zeros(sh.size_ab ** 3, dtype=torch.int64, device="cuda")
+        nvox = int((small >= np.float32(1e-37)).sum())
+        fn = lambda: (big.zero_(), ctx.cq_merge(d_small, d_rw, nf, sh, 0, m, big, sp))
+        clocks.start()
+        ms = _time(fn, args.steps, min(args.warmup, 1), stream)
+        clk = clocks.stop()
+        rate = nvox * nf / (ms * 1e-3)
+        line.update(metric="voxel-frame scatters/s (C(q) merge)", value=rate, unit="scatters/s",
+                    ms_per_step=ms, dtype="fp32+u64",
+                    config={"workload": f"small C(q) {sh.size_ab}x{sh.size_ab}x{sh.size_c} "
+                                        f"({nvox} non-zero voxels) x {nf} SO(3) frames into "
+                                        f"{sh.size_ab}^3"},
+                    clocks=clk,
+                    roofline={"bound": "l2-atomic", "achieved": rate, "unit": "updates/s",
+                              "note": "one 64-bit L2 atomic per (voxel, frame)"})
+        if not args.no_cpu_baseline:
+            sub = min(nvox, 20000)
+            so = oracle.small_cq_mesh_shape(mq, 199)
+            out = np.zeros(sh.size_ab ** 3, np.uint64)
+            nz = np.nonzero(small >= np.float32(1e-37))[0]
+            v0 = int(nz[len(nz) // 2])
+            t0 = time.perf_counter()
+            oracle.lib().iaco_cq_merge(oracle.p(small), oracle.p(rw.reshape(-1)), min(nf, 2000), so,
+                                       0, m, v0, v0 + sub, oracle.p(out))
+            dt = time.perf_counter() - t0
+            done = int(((small[v0:v0 + sub]) >= np.float32(1e-37)).sum()) * min(nf, 2000)
+            line["cpu_baseline"] = {"value": done / dt, "unit": "scatters/s", "cores": nthreads,
+                                    "kind": "port", "sample": f"{sub} voxels x {min(nf, 2000)} frames"}
+    elif args.kernel == "ac1d_sparse":
+        cfg = W.rotated_config(nframes=args.frames, seed=2)
+        sh = capi.ac1d_shape(cfg["max_q"], 256)
+        vs = capi.ac1d_vecsize(sh.max_q, sh.dq_per_step)
+        ph = torch.from_numpy(cfg["photons"]).cuda()
+        off = torch.from_numpy(cfg["offsets"].view(np.int64)).cuda()
+        hist = torch.zeros(vs, dtype=torch.int64, device="cuda")
+        nf = len(cfg["offsets"]) - 1
+        fn = lambda: (hist.zero_(), ctx.ac1d_sparse_batch(ph, off, nf, sh.max_q, sh.dq_per_step, 1,
+                                                          100.0, hist, sp))
+        clocks.start()
+        ms = _time(fn, args.steps, args.warmup, stream)
+        clk = clocks.stop()
+        pairs = _pairs(cfg["offsets"])
+        line.update(metric="photon pairs/s into the AC1D histogram", value=pairs / (ms * 1e-3),
+                    unit="pairs/s", ms_per_step=ms, dtype="fp32+u64", clocks=clk,
+                    config={"workload": f"{nf} rotated-correlator frames, 256 bins, linear"})
+    elif args.kernel == "simulate":
+        line.update(simulate_pipeline(args, ctx, stream, clocks, nthreads))
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
+def simulate_pipeline(args, ctx, stream, clocks, nthreads):
+    """512x512 detector (75 um at 0.10 m), 5x5x8 simple-cubic crystal (a = 4 A,
+    200 emitters), 4 modes, SuSa 0, lambda 1.55 A, I = sum_modes |Psi|^2, mean
+    0.02 photons per pixel, random orientations: emitters -> intensity ->
+    Poisson -> photon lists -> 201^3 pair mesh, all on the device, in chunks
+    of frames."""
+    import torch
+    import oracle
+    from incohautocorrelate_b200 import capi
+    from incohautocorrelate_b200 import workloads as W
+    sp = stream.cuda_stream
+    n = 512
+    pm_m = W.flat_pixel_map(n, n)
+    pm = (pm_m * np.float32(1e10)).astype(np.float32)  # Angstrom
+    km, mq = W.kmap_numpy(pm_m)
+    cells = (5, 5, 8)
+    atoms = np.array([[(x - cells[0] / 2.0 + 0.5) * 4.0, (y - cells[1] / 2.0 + 0.5) * 4.0,
+                       (z - cells[2] / 2.0 + 0.5) * 4.0]
+                      for x in range(cells[0]) for y in range(cells[1]) for z in range(cells[2])],
+                     np.float64)
+    na, nmodes = len(atoms), 4
+    chunk = min(args.frames, 1000)
+    npix = n * n
+    d_pm, d_km = torch.from_numpy(pm).cuda(), torch.from_numpy(km).cuda()
+    d_atoms = torch.from_numpy(atoms.reshape(-1)).cuda()
+    em = torch.zeros((chunk, nmodes, na, 4), dtype=torch.float32, device="cuda")
+    cnt = torch.zeros(chunk * nmodes, dtype=torch.int32, device="cuda")
+    rot = torch.zeros((chunk, 9), dtype=torch.float32, device="cuda")
+    img = torch.zeros((chunk, npix), dtype=torch.float32, device="cuda")
+    cap = int(chunk * npix * 0.05) + 100000
+    phot = torch.zeros((cap, 4), dtype=torch.float32, device="cuda")
+    offs = torch.zeros(chunk + 1, dtype=torch.int64, device="cuda")
+    shape = capi.big_mesh_shape(mq, 199)
+    S = shape.size_ab
+    half = torch.zeros(capi.half_mesh_words(S), dtype=torch.int64, device="cuda")
+    cp = capi.CrystalParams(1, 1.0, 1, 1.0)
+    us = 75e-6 * 1e10
+    simp = capi.SimParams(0, (C.c_double * 3)(us, 0, 0), (C.c_double * 3)(0, us, 0), 1.55, 1, 0)
+    pp = capi.PhotonParams(0.02 * npix, 1, 0.0, 1.0)
+    params = capi.sparse_params(shape)
+    ev = {"intensity": []}
+
+    def step(k):
+        ctx.crystal_emitters(d_atoms, na, chunk, nmodes, cp, 1234 + k, em, cnt, rot, None, sp)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ctx.simulate_intensity(d_pm, npix, em, cnt, na, nmodes, chunk, simp, img, sp)
+        b.record(stream)
+        ev["intensity"].append((a, b))
+        ctx.simulate_photons(img, npix, chunk, k * chunk, pp, 99, sp)
+        ctx.sparsify_frames(img, None, d_km, npix, chunk, 0.0, 1.0, 1, phot, cap, offs, sp,
+                            want_total=False)
+        ctx.sparse_ac_batch(phot, offs, rot, chunk, params, half, sp)
+
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+    ev["intensity"].clear()
+    clocks.start()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for k in range(args.steps):
+        step(args.warmup + k)
+    b.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = a.elapsed_time(b) / args.steps
+    ms_int = sum(x.elapsed_time(y) for x, y in ev["intensity"]) / len(ev["intensity"])
+    terms = npix * na * nmodes * chunk
+    mufu_peak = 148 * 16 * (clk["sm_mhz"] or 1965.0) * 1e6 / 2  # two SFU ops per term
+    out = {"metric": "simulated frames/s into the 201^3 pair mesh", "value": chunk / (ms * 1e-3),
+           "unit": "frames/s", "ms_per_step": ms, "dtype": "fp32",
+           "config": {"workload": "512x512, 5x5x8 crystal (200 emitters), 4 modes, SuSa 0, "
+                                  "|Psi|^2, 0.02 photons/pixel, random orientation",
+                      "frames_per_step": chunk},
+           "clocks": clk,
+           "roofline": {"bound": "sfu", "kernel": "simulate_kernel", "kernel_ms": ms_int,
+                        "achieved": terms / (ms_int * 1e-3), "unit": "terms/s",
+                        "peak": mufu_peak, "frac": terms / (ms_int * 1e-3) / mufu_peak,
+                        "peak_source": "derived: 148 SM x 16 SFU results/clk / 2 (sin + cos) "
+                                       "at the sampled clock"}}
+    if not args.no_cpu_baseline:
+        em_h = em[0].cpu().numpy()
+        P = np.array([na, 1, 0, us, 0, 0, 0, us, 0, 1.55], np.float64)
+        rows = 4096
+        t = np.zeros(rows, np.float32)
+        t0 = time.perf_counter()
+        for m in range(nmodes):
+            e = np.ascontiguousarray(em_h[m])
+            oracle.lib().iaco_simulate_crystal(oracle.p(pm[: 3 * rows].copy()), rows, oracle.p(e),
+                                               na, oracle.p(P), 1, oracle.p(t))
+        dt = time.perf_counter() - t0
+        cpu_terms = rows * na * nmodes / dt
+        out["cpu_baseline"] = {"value": cpu_terms / (npix * na * nmodes), "unit": "frames/s",
+                               "cores": nthreads, "kind": "port",
+                               "sample": f"SimulateCrystal of {rows} pixels x 4 modes "
+                                         f"({dt:.2f} s), scaled to a 512x512 frame; intensity "
+                                         "only (no Poisson, no correlation)"}
+    return out
+
+
 def main():
     args = parse()
+    if args.kernel != "sparse":
+        return run_kernel(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

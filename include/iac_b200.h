@@ -68,7 +68,9 @@ iac_status iac_ctx_create(int device, iac_ctx **out);
 iac_status iac_ctx_destroy(iac_ctx *ctx);
 /* Synchronises `stream`, then reports and clears the context's device-side
  * error counters: writes skipped because their voxel lay outside the mesh
- * (the reference writes them out of bounds) and bounded waits that ran out. */
+ * (the reference writes them out of bounds; IAC_ERR_OUT_OF_MESH), photons
+ * dropped because a photon list was full (IAC_ERR_NO_MEMORY) and bounded
+ * waits that ran out (IAC_ERR_TIMEOUT). */
 iac_status iac_ctx_check(iac_ctx *ctx, void *stream, uint64_t *out_of_mesh);
 const char *iac_status_string(iac_status s);
 const char *iac_last_error(void); /* thread-local message of the last failure */
@@ -289,7 +291,8 @@ iac_status iac_simulate_photons(iac_ctx *ctx, float *d_intensity, uint64_t npix,
  * frames float[nframes][npix] -> photon lists float4 (k, value) in pixel order
  * with nframes+1 offsets, ready for iac_sparse_ac_batch.  d_mask may be NULL.
  * If h_total is given the call synchronises, stores the photon count and
- * fails when it exceeds `capacity` (entries beyond it are not written). */
+ * fails when it exceeds `capacity`.  Entries beyond the capacity are never
+ * written and the offsets are clamped to it (counted for iac_ctx_check). */
 iac_status iac_sparsify_frames(iac_ctx *ctx, const float *d_intensity, const int *d_mask,
                                const float *d_kmap, uint64_t npix, uint32_t nframes,
                                float threshold, float step, int photonize, float *d_photons,

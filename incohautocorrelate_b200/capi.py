@@ -59,6 +59,29 @@ class SparseTuning(C.Structure):
                 ("ctas_per_sm", C.c_uint32)]
 
 
+class CrystalParams(C.Structure):
+    _fields_ = [("incoherent", C.c_int32), ("fluorescence_yield", C.c_float),
+                ("random_orientation", C.c_int32), ("isotropy", C.c_float)]
+
+
+class SimParams(C.Structure):
+    _fields_ = [("subsampling", C.c_int32), ("u_step", C.c_double * 3),
+                ("v_step", C.c_double * 3), ("wavelength", C.c_double),
+                ("intensity_squared", C.c_int32), ("accurate_sincos", C.c_int32)]
+
+
+class PhotonParams(C.Structure):
+    _fields_ = [("expected_photons", C.c_double), ("poisson", C.c_int32),
+                ("adu_noise", C.c_float), ("value_per_photon", C.c_float)]
+
+
+# Philox stream tags of csrc/rng.cuh
+RNG_POISSON = 0x01 << 56
+RNG_ROTATION = 0x02 << 56
+RNG_PHASE = 0x03 << 56
+RNG_YIELD = 0x04 << 56
+RNG_NOISE = 0x05 << 56
+
 _lib = None
 _VP = C.c_void_p
 _U64 = C.c_uint64
@@ -101,6 +124,13 @@ def _declare(lib):
     fn("iac_ac1d_cq", [_VP, _VP, _VP, _U64, C.POINTER(AC1DShape), C.c_int, D, _VP, _VP])
     fn("iac_ac1d_vecsize", [C.c_float, C.c_float], _U32)
     fn("iac_ac1d_sparse_batch", [_VP, _VP, _VP, _U32, C.c_float, C.c_float, C.c_int, D, _VP, _VP])
+    fn("iac_crystal_emitters", [_VP, _VP, _U32, _U32, _U32, C.POINTER(CrystalParams), _U64, _VP,
+                                _VP, _VP, _VP, _VP])
+    fn("iac_simulate_intensity", [_VP, _VP, _U64, _VP, _VP, _U32, _U32, _U32,
+                                  C.POINTER(SimParams), _VP, _VP])
+    fn("iac_simulate_photons", [_VP, _VP, _U64, _U32, _U64, C.POINTER(PhotonParams), _U64, _VP])
+    fn("iac_sparsify_frames", [_VP, _VP, _VP, _VP, _U64, _U32, C.c_float, C.c_float, C.c_int,
+                               _VP, _U64, _VP, C.POINTER(_U64), _VP])
     return lib
 
 
@@ -285,6 +315,34 @@ class Context:
         check(lib().iac_ac1d_sparse_batch(self._h, _ptr(d_photons), _ptr(d_offsets), int(nframes),
                                           float(max_q), float(dqdx), int(interp), float(mult),
                                           _ptr(d_hist), _ptr(stream)))
+
+    def crystal_emitters(self, d_atoms, natoms, nframes, nmodes, cparams, seed, d_em, d_count,
+                         d_rot_event, d_rot_crystal=None, stream=None):
+        check(lib().iac_crystal_emitters(self._h, _ptr(d_atoms), int(natoms), int(nframes),
+                                         int(nmodes), C.byref(cparams), int(seed), _ptr(d_em),
+                                         _ptr(d_count), _ptr(d_rot_event), _ptr(d_rot_crystal),
+                                         _ptr(stream)))
+
+    def simulate_intensity(self, d_pm, npix, d_em, d_count, natoms, nmodes, nframes, sparams,
+                           d_out, stream=None):
+        check(lib().iac_simulate_intensity(self._h, _ptr(d_pm), int(npix), _ptr(d_em),
+                                           _ptr(d_count), int(natoms), int(nmodes), int(nframes),
+                                           C.byref(sparams), _ptr(d_out), _ptr(stream)))
+
+    def simulate_photons(self, d_I, npix, nframes, first_frame, pparams, seed, stream=None):
+        check(lib().iac_simulate_photons(self._h, _ptr(d_I), int(npix), int(nframes),
+                                         int(first_frame), C.byref(pparams), int(seed),
+                                         _ptr(stream)))
+
+    def sparsify_frames(self, d_I, d_mask, d_kmap, npix, nframes, threshold, step, photonize,
+                        d_photons, capacity, d_offsets, stream=None, want_total=True):
+        tot = _U64(0)
+        check(lib().iac_sparsify_frames(self._h, _ptr(d_I), _ptr(d_mask), _ptr(d_kmap), int(npix),
+                                        int(nframes), float(threshold), float(step),
+                                        int(photonize), _ptr(d_photons), int(capacity),
+                                        _ptr(d_offsets), C.byref(tot) if want_total else None,
+                                        _ptr(stream)))
+        return int(tot.value)
 
     def bench_scatter_add(self, d_buf, words, word_bits, updates, seed=1, stream=None):
         check(lib().iac_bench_scatter_add(self._h, _ptr(d_buf), int(words), int(word_bits),

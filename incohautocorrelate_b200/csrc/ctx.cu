@@ -157,6 +157,11 @@ iac_status iac_ctx_check(iac_ctx *ctx, void *stream, uint64_t *out_of_mesh)
         set_error("%llu bounded device waits ran out", (unsigned long long)h.timeouts);
         return IAC_ERR_TIMEOUT;
     }
+    if (h.photon_overflow) {
+        set_error("%llu photons did not fit the photon-list capacity and were dropped",
+                  (unsigned long long)h.photon_overflow);
+        return IAC_ERR_NO_MEMORY;
+    }
     if (h.out_of_mesh) {
         set_error("%llu writes fell outside the mesh and were skipped",
                   (unsigned long long)h.out_of_mesh);

@@ -198,14 +198,16 @@ __global__ void __launch_bounds__(DTILE) cq_small_kernel(const DenseArgs a)
             const int ax[3] = {a.ka, a.kb, a.kc};
             const int cen[3] = {a.cab, a.cab, a.cc};
             int words = 1;
+            bool ok = true;
             for (int d = 0; d < 3; d++) {
                 const float l = (ax[d] == 0 ? lo3[0] : ax[d] == 1 ? lo3[1] : lo3[2]) * a.vpdq;
                 const float h = (ax[d] == 0 ? hi3[0] : ax[d] == 1 ? hi3[1] : hi3[2]) * a.vpdq;
                 w.lo[d] = (int)floorf(l) - 1 + cen[d];
                 w.dim[d] = (int)ceilf(h) + 2 + cen[d] - w.lo[d] + (INTERP ? 1 : 0);
-                words *= max(1, w.dim[d]);
+                ok &= w.dim[d] >= 1 && w.dim[d] <= WINDOW_WORDS;
+                words *= max(1, min(w.dim[d], WINDOW_WORDS + 1));
             }
-            w.on = words <= WINDOW_WORDS;
+            w.on = ok && words <= WINDOW_WORDS;
             if (w.on)
                 for (int i = threadIdx.x; i < words; i += DTILE) win[i] = 0ull;
         }

@@ -47,7 +47,8 @@ void set_error(const char *fmt, ...);
 struct DeviceCounters {
     unsigned long long out_of_mesh;
     unsigned long long timeouts;
-    unsigned long long pad[6];
+    unsigned long long photon_overflow;  // photons beyond a photon-list capacity (dropped)
+    unsigned long long pad[5];
 };
 
 // A growable device scratch buffer owned by the context.

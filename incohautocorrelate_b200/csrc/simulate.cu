@@ -434,11 +434,17 @@ __global__ void sparsify_write_kernel(const float *__restrict__ I, const int *__
     }
 }
 
+// frame offsets, clamped to the capacity so that no consumer reads past the
+// photons actually written; a clamp is counted as an overflow
 __global__ void frame_offsets_kernel(const uint64_t *__restrict__ block_off, uint32_t blocks_per_frame,
-                                     uint32_t nframes, uint64_t *__restrict__ frame_off)
+                                     uint32_t nframes, uint64_t capacity,
+                                     uint64_t *__restrict__ frame_off, DeviceCounters *counters)
 {
     const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f <= nframes) frame_off[f] = block_off[(size_t)f * blocks_per_frame];
+    if (f > nframes) return;
+    const uint64_t o = block_off[(size_t)f * blocks_per_frame];
+    frame_off[f] = o < capacity ? o : capacity;
+    if (f == nframes && o > capacity) atomicAdd(&counters->photon_overflow, o - capacity);
 }
 
 }  // namespace iac
@@ -573,10 +579,11 @@ iac_status iac_sparsify_frames(iac_ctx *ctx, const float *d_intensity, const int
     const uint32_t bpf = (uint32_t)((npix + SPARSE_PIX - 1) / SPARSE_PIX);
     const uint64_t nb = (uint64_t)bpf * nframes;
     void *scr = nullptr;
-    iac_status st = stream_scratch(ctx, stream, SLOT_AUX1, sizeof(uint32_t) * nb + sizeof(uint64_t) * (nb + 2), &scr);
+    const size_t counts_bytes = ((sizeof(uint32_t) * nb + 15) / 16) * 16;
+    iac_status st = stream_scratch(ctx, stream, SLOT_AUX1, counts_bytes + sizeof(uint64_t) * (nb + 2), &scr);
     if (st != IAC_OK) return st;
     uint32_t *counts = (uint32_t *)scr;
-    uint64_t *boff = (uint64_t *)((char *)scr + ((sizeof(uint32_t) * nb + 15) / 16) * 16);
+    uint64_t *boff = (uint64_t *)((char *)scr + counts_bytes);
     dim3 grid(bpf, nframes);
     sparsify_count_kernel<<<grid, SPARSE_THREADS, 0, s>>>(d_intensity, d_mask, npix, threshold, counts);
     IAC_LAUNCHED(ctx);
@@ -585,7 +592,8 @@ iac_status iac_sparsify_frames(iac_ctx *ctx, const float *d_intensity, const int
     sparsify_write_kernel<<<grid, SPARSE_THREADS, 0, s>>>(d_intensity, d_mask, d_kmap, npix, threshold, step,
                                                           photonize, boff, (float4 *)d_photons, capacity);
     IAC_LAUNCHED(ctx);
-    frame_offsets_kernel<<<(nframes + 256) / 256, 256, 0, s>>>(boff, bpf, nframes, d_frame_offsets);
+    frame_offsets_kernel<<<(nframes + 256) / 256, 256, 0, s>>>(boff, bpf, nframes, capacity,
+                                                               d_frame_offsets, ctx->d_counters);
     IAC_LAUNCHED(ctx);
     IAC_CUDA(cudaGetLastError());
     if (h_total) {
