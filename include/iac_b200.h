@@ -147,6 +147,24 @@ iac_status iac_sparse_ac_frames_host(iac_ctx *ctx, const float *h_photons,
                                      uint32_t nframes, const iac_sparse_params *params,
                                      uint64_t *h_full_mesh);
 
+/* Allocation-free form of iac_sparse_ac_batch (no counterpart in the
+ * reference, which creates OpenCL buffers on every call).  For callers that
+ * may not allocate device memory while they run -- an acquisition loop that
+ * cannot take the synchronisation and latency of cudaMalloc/cudaFree, or a
+ * host framework that owns all device memory -- this call keeps its work
+ * queue in a fixed 1.8 MB array of device memory inside the library (present
+ * on every GPU that loads it, until the process exits) and calls no
+ * allocator.  Same arguments and result as iac_sparse_ac_batch, at most
+ * 200 000 frames per call (more is rejected with IAC_ERR_INVALID_ARG).
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  Calls share the array: two calls
+ * that run on the GPU at the same time (on different streams) race, so keep
+ * them on one stream or otherwise ordered. */
+iac_status iac_sparse_ac_batch_static(iac_ctx *ctx, const float *d_photons,
+                                      const uint64_t *d_frame_offsets, const float *d_rot9,
+                                      uint32_t nframes, const iac_sparse_params *params,
+                                      uint64_t *d_half_mesh, void *stream);
+
 /* Work-queue tuning of the persistent pair kernel.  Fields left 0 come from
  * the autotuner's table (tuning/sparse_tuning.tsv beside the library, or the
  * file named by IAC_SPARSE_TUNING; the row of the nearest mesh edge), else

@@ -111,6 +111,7 @@ def _declare(lib):
     fn("iac_full_mesh_words", [_U32], _U64)
     fn("iac_sparse_ac_batch", [_VP, _VP, _VP, _VP, _U32, C.POINTER(SparseParams), _VP, _VP])
     fn("iac_sparse_fold", [_VP, _VP, _U32, _VP, _VP])
+    fn("iac_sparse_ac_batch_static", [_VP, _VP, _VP, _VP, _U32, C.POINTER(SparseParams), _VP, _VP])
     fn("iac_sparse_ac_frames_host", [_VP, _VP, _VP, _VP, _U32, C.POINTER(SparseParams), _VP])
     fn("iac_sparse_set_tuning", [_VP, C.POINTER(SparseTuning)])
     fn("iac_sparse_get_tuning", [_VP, _U32, C.POINTER(SparseTuning)])
@@ -279,6 +280,14 @@ class Context:
         check(lib().iac_sparse_ac_batch(self._h, _ptr(d_photons), _ptr(d_offsets), _ptr(d_rot),
                                         int(nframes), C.byref(params), _ptr(d_half),
                                         _ptr(stream)))
+
+    def sparse_ac_batch_static(self, d_photons, d_offsets, d_rot, nframes, params, d_half,
+                               stream=None):
+        """iac_sparse_ac_batch_static: the batched pair correlator with its work queue in
+        a fixed device array of the library (no device allocation at all)."""
+        check(lib().iac_sparse_ac_batch_static(self._h, _ptr(d_photons), _ptr(d_offsets),
+                                               _ptr(d_rot), int(nframes), C.byref(params),
+                                               _ptr(d_half), _ptr(stream)))
 
     def sparse_fold(self, d_half, S, d_full, stream=None):
         check(lib().iac_sparse_fold(self._h, _ptr(d_half), int(S), _ptr(d_full), _ptr(stream)))

@@ -758,3 +758,126 @@ iac_status iac_sparse_ac_frames_host(iac_ctx *ctx, const float *h_photons,
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of iac_sparse_ac_batch.
+//
+// Some callers may not allocate device memory once they are running: a
+// detector acquisition loop that cannot absorb the device-wide
+// synchronisation and unbounded latency a cudaMalloc/cudaFree can cause, or a
+// host framework that hands out all device memory from its own pool and
+// forbids allocations behind its back.  iac_sparse_ac_batch grows a per-stream
+// scratch buffer on first use; this entry point instead keeps the same work
+// queue (tile table, queue counter, per-frame flags) in a fixed array of
+// device memory that is part of the loaded library, so it never allocates.
+//
+// The array's name in host code only stands in for the symbol; the kernels
+// need its device address, which cudaGetSymbolAddress gives once per device
+// (looked up on the first call made on that device, with the device current).
+// The array is shared by every call on the device and keeps the previous
+// call's contents: the planner kernel rewrites the whole tile table and
+// resets the queue counter before the pair kernel reads them, so nothing has
+// to be cleared from the host, but two calls running on the GPU at the same
+// time (e.g. on two streams) would overwrite each other's queue.
+// ---------------------------------------------------------------------------
+namespace iac {
+
+constexpr uint32_t STATIC_MAX_FRAMES = 200000;
+constexpr size_t STATIC_TABLE_BYTES =
+    ((sizeof(unsigned long long) * ((size_t)STATIC_MAX_FRAMES + 1) + 255) / 256) * 256;
+constexpr size_t STATIC_QUEUE_BYTES = 256;
+constexpr size_t STATIC_SCRATCH_BYTES = STATIC_TABLE_BYTES + STATIC_QUEUE_BYTES + STATIC_MAX_FRAMES;
+
+static __device__ __align__(256) unsigned char g_sparse_static_scratch[STATIC_SCRATCH_BYTES];
+
+constexpr int STATIC_MAX_DEVICES = 64;
+static std::mutex g_static_mu;
+static void *g_static_addr[STATIC_MAX_DEVICES];
+
+// Device address of g_sparse_static_scratch on `dev` (which must be current).
+static iac_status static_scratch_address(int dev, void **out)
+{
+    IAC_REQUIRE(dev >= 0 && dev < STATIC_MAX_DEVICES, "device %d beyond the %d supported", dev,
+                STATIC_MAX_DEVICES);
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    if (!g_static_addr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_sparse_static_scratch);
+        if (e != cudaSuccess || !p) {
+            set_error("cudaGetSymbolAddress of the fixed scratch failed on device %d: %s", dev,
+                      cudaGetErrorString(e));
+            return IAC_ERR_CUDA;
+        }
+        g_static_addr[dev] = p;
+    }
+    *out = g_static_addr[dev];
+    return IAC_OK;
+}
+
+}  // namespace iac
+
+extern "C" iac_status iac_sparse_ac_batch_static(iac_ctx *ctx, const float *d_photons,
+                                                 const uint64_t *d_off, const float *d_rot9,
+                                                 uint32_t nframes, const iac_sparse_params *p,
+                                                 uint64_t *d_half, void *stream)
+{
+    IAC_REQUIRE(ctx != nullptr, "iac_sparse_ac_batch_static: ctx is NULL");
+    iac_status st = check_params(p);
+    if (st != IAC_OK) return st;
+    IAC_REQUIRE(nframes <= STATIC_MAX_FRAMES,
+                "iac_sparse_ac_batch_static: %u frames requested; its fixed scratch holds the work "
+                "queue of at most %u frames per call (split the batch or use iac_sparse_ac_batch)",
+                nframes, STATIC_MAX_FRAMES);
+    if (nframes == 0) return IAC_OK;
+    IAC_REQUIRE(d_photons && d_off && d_rot9 && d_half, "iac_sparse_ac_batch_static: NULL pointer");
+    IAC_REQUIRE((reinterpret_cast<uintptr_t>(d_photons) & 15) == 0,
+                "photon array must be 16-byte aligned (float4 per photon)");
+    DeviceGuard g(ctx->device);
+    void *base = nullptr;
+    if ((st = static_scratch_address(ctx->device, &base)) != IAC_OK) return st;
+    const iac_sparse_tuning tun = effective_tuning(ctx, p->shape.size_ab);
+    unsigned long long *tile_off = (unsigned long long *)base;
+    unsigned long long *queue = (unsigned long long *)((char *)base + STATIC_TABLE_BYTES);
+    unsigned char *flags = (unsigned char *)base + STATIC_TABLE_BYTES + STATIC_QUEUE_BYTES;
+
+    cudaStream_t s = as_stream(stream);
+    sparse_plan_kernel<<<1, PLAN_THREADS, 0, s>>>(d_off, nframes, tun.tile_pairs, tile_off, queue);
+    IAC_LAUNCHED(ctx);
+    IAC_CUDA(cudaGetLastError());
+    const bool mult_small_int = p->multiplicator >= 1.0 && p->multiplicator <= 1024.0 &&
+                                p->multiplicator == std::floor(p->multiplicator);
+    if (mult_small_int && p->interp_second == 0 && !(p->double_map && p->interp_first == 1)) {
+        const uint32_t blocks = (uint32_t)(((uint64_t)nframes * 32 + 255) / 256);
+        sparse_count_check_kernel<<<blocks, 256, 0, s>>>(reinterpret_cast<const float4 *>(d_photons),
+                                                         d_off, nframes, flags);
+        IAC_LAUNCHED(ctx);
+        IAC_CUDA(cudaGetLastError());
+    } else {
+        flags = nullptr;
+    }
+    SparseArgs a;
+    a.photons = reinterpret_cast<const float4 *>(d_photons);
+    a.offsets = d_off;
+    a.rot = d_rot9;
+    a.tile_off = tile_off;
+    a.half = reinterpret_cast<unsigned long long *>(d_half);
+    a.queue = queue;
+    a.counters = ctx->d_counters;
+    a.nframes = nframes;
+    a.tile_pairs = tun.tile_pairs;
+    a.S = (int)p->shape.size_ab;
+    a.C = (a.S - 1) / 2;
+    a.half_ss = (a.S + 1) / 2;
+    a.plane = (uint32_t)a.S * (uint32_t)a.S;
+    a.maxq = p->shape.max_q;
+    a.maxq2 = sqrt_threshold(p->shape.max_q);
+    a.vpdq = (float)p->shape.voxel_per_dq;
+    a.mult = p->multiplicator;
+    a.mult_f = (float)p->multiplicator;
+    a.small_counts = flags;
+    const PairKernel k = pick_kernel(p->double_map, p->interp_first, p->interp_second);
+    k<<<ctx->sm_count * (int)tun.ctas_per_sm, tun.block_threads, 0, s>>>(a);
+    IAC_LAUNCHED(ctx);
+    IAC_CUDA(cudaGetLastError());
+    return IAC_OK;
+}
