@@ -79,6 +79,22 @@ int iac_abi_version(void);
 uint64_t iac_ctx_launch_count(const iac_ctx *ctx);
 
 /* ---------------------------------------------------------------------- */
+/* memory and streams (so that FFI callers need not link the CUDA runtime)  */
+/* ---------------------------------------------------------------------- */
+
+iac_status iac_device_alloc(iac_ctx *ctx, size_t bytes, void **d_ptr);
+iac_status iac_device_free(iac_ctx *ctx, void *d_ptr);
+iac_status iac_host_alloc_pinned(iac_ctx *ctx, size_t bytes, void **h_ptr);
+iac_status iac_host_free_pinned(iac_ctx *ctx, void *h_ptr);
+iac_status iac_memcpy_h2d(iac_ctx *ctx, void *d_dst, const void *h_src, size_t bytes, void *stream);
+iac_status iac_memcpy_d2h(iac_ctx *ctx, void *h_dst, const void *d_src, size_t bytes, void *stream);
+iac_status iac_memcpy_d2d(iac_ctx *ctx, void *d_dst, const void *d_src, size_t bytes, void *stream);
+iac_status iac_memset_device(iac_ctx *ctx, void *d_ptr, int value, size_t bytes, void *stream);
+iac_status iac_stream_create(iac_ctx *ctx, void **stream);
+iac_status iac_stream_destroy(iac_ctx *ctx, void *stream);
+iac_status iac_stream_synchronize(iac_ctx *ctx, void *stream);
+
+/* ---------------------------------------------------------------------- */
 /* geometry (host arithmetic, no device work)                               */
 /* ---------------------------------------------------------------------- */
 

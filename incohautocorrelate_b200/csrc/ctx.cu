@@ -170,6 +170,113 @@ iac_status iac_ctx_check(iac_ctx *ctx, void *stream, uint64_t *out_of_mesh)
     return IAC_OK;
 }
 
+iac_status iac_device_alloc(iac_ctx *ctx, size_t bytes, void **d_ptr)
+{
+    IAC_REQUIRE(ctx && d_ptr, "iac_device_alloc: NULL argument");
+    DeviceGuard g(ctx->device);
+    *d_ptr = nullptr;
+    if (bytes == 0) return IAC_OK;
+    IAC_CUDA(cudaMalloc(d_ptr, bytes));
+    return IAC_OK;
+}
+
+iac_status iac_device_free(iac_ctx *ctx, void *d_ptr)
+{
+    IAC_REQUIRE(ctx != nullptr, "iac_device_free: ctx is NULL");
+    if (!d_ptr) return IAC_OK;
+    DeviceGuard g(ctx->device);
+    IAC_CUDA(cudaFree(d_ptr));
+    return IAC_OK;
+}
+
+iac_status iac_host_alloc_pinned(iac_ctx *ctx, size_t bytes, void **h_ptr)
+{
+    IAC_REQUIRE(ctx && h_ptr, "iac_host_alloc_pinned: NULL argument");
+    DeviceGuard g(ctx->device);
+    *h_ptr = nullptr;
+    if (bytes == 0) return IAC_OK;
+    IAC_CUDA(cudaMallocHost(h_ptr, bytes));
+    return IAC_OK;
+}
+
+iac_status iac_host_free_pinned(iac_ctx *ctx, void *h_ptr)
+{
+    IAC_REQUIRE(ctx != nullptr, "iac_host_free_pinned: ctx is NULL");
+    if (!h_ptr) return IAC_OK;
+    IAC_CUDA(cudaFreeHost(h_ptr));
+    return IAC_OK;
+}
+
+static iac_status copy(iac_ctx *ctx, void *dst, const void *src, size_t bytes, cudaMemcpyKind k,
+                       void *stream)
+{
+    IAC_REQUIRE(ctx != nullptr, "copy: ctx is NULL");
+    if (bytes == 0) return IAC_OK;
+    IAC_REQUIRE(dst && src, "copy: NULL pointer");
+    DeviceGuard g(ctx->device);
+    IAC_CUDA(cudaMemcpyAsync(dst, src, bytes, k, as_stream(stream)));
+    return IAC_OK;
+}
+
+iac_status iac_memcpy_h2d(iac_ctx *ctx, void *d, const void *h, size_t n, void *stream)
+{
+    return copy(ctx, d, h, n, cudaMemcpyHostToDevice, stream);
+}
+iac_status iac_memcpy_d2h(iac_ctx *ctx, void *h, const void *d, size_t n, void *stream)
+{
+    return copy(ctx, h, d, n, cudaMemcpyDeviceToHost, stream);
+}
+iac_status iac_memcpy_d2d(iac_ctx *ctx, void *d, const void *s, size_t n, void *stream)
+{
+    return copy(ctx, d, s, n, cudaMemcpyDeviceToDevice, stream);
+}
+
+iac_status iac_memset_device(iac_ctx *ctx, void *d_ptr, int value, size_t bytes, void *stream)
+{
+    IAC_REQUIRE(ctx != nullptr, "iac_memset_device: ctx is NULL");
+    if (bytes == 0) return IAC_OK;
+    IAC_REQUIRE(d_ptr != nullptr, "iac_memset_device: NULL pointer");
+    DeviceGuard g(ctx->device);
+    IAC_CUDA(cudaMemsetAsync(d_ptr, value, bytes, as_stream(stream)));
+    return IAC_OK;
+}
+
+iac_status iac_stream_create(iac_ctx *ctx, void **stream)
+{
+    IAC_REQUIRE(ctx && stream, "iac_stream_create: NULL argument");
+    DeviceGuard g(ctx->device);
+    cudaStream_t s;
+    IAC_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    *stream = (void *)s;
+    return IAC_OK;
+}
+
+iac_status iac_stream_destroy(iac_ctx *ctx, void *stream)
+{
+    IAC_REQUIRE(ctx != nullptr, "iac_stream_destroy: ctx is NULL");
+    if (!stream) return IAC_OK;
+    DeviceGuard g(ctx->device);
+    IAC_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        auto it = ctx->stream_scratch.find(stream);
+        if (it != ctx->stream_scratch.end()) {
+            for (auto &b : it->second.bufs) b.release();
+            ctx->stream_scratch.erase(it);
+        }
+    }
+    IAC_CUDA(cudaStreamDestroy(as_stream(stream)));
+    return IAC_OK;
+}
+
+iac_status iac_stream_synchronize(iac_ctx *ctx, void *stream)
+{
+    IAC_REQUIRE(ctx != nullptr, "iac_stream_synchronize: ctx is NULL");
+    DeviceGuard g(ctx->device);
+    IAC_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    return IAC_OK;
+}
+
 uint64_t iac_ctx_launch_count(const iac_ctx *ctx)
 {
     return ctx ? ctx->launches.load(std::memory_order_relaxed) : 0;
