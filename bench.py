@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--cpu-frames", type=int, default=1500,
                     help="frames per CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--det", type=int, default=1024,
+                    help="edge of the square detector of the dense kernels (1024 = their config)")
     ap.add_argument("--kernel", default="sparse",
                     choices=["sparse", "cq_small", "ac1d_cq", "cq_merge", "ac1d_sparse", "simulate"],
                     help="sparse is the headline; the others measure the remaining kernels "
@@ -241,7 +243,7 @@ def run_ours(args):
     torch.cuda.set_device(dev)
     import torch.distributed as dist
 
-    from incohautocorrelate_b200 import capi
+    from incohautocorrelate_b200 import capi, shard
     from incohautocorrelate_b200 import workloads as W
 
     cfg = W.rotated_config(nframes=args.frames, seed=2 + 7919 * rank)
@@ -289,7 +291,7 @@ def run_ours(args):
             ev.append((a, b))
         ctx.sparse_fold(half, S, full, sptr)
         if distributed:
-            dist.reduce(full, dst=0)
+            shard.reduce_mesh(full, dst=0)
 
     for _ in range(args.warmup):
         step()
@@ -447,7 +449,7 @@ def run_kernel(args):
             "kernel": args.kernel}
     import oracle
     if args.kernel in ("cq_small", "ac1d_cq"):
-        I, km, mq = _dense_inputs(1024, 1024)
+        I, km, mq = _dense_inputs(args.det, args.det)
         npix = I.size
         dI, dk = torch.from_numpy(I).cuda(), torch.from_numpy(km).cuda()
         pairs = npix * (npix + 1) // 2
@@ -472,8 +474,8 @@ def run_kernel(args):
         mhz = clk["sm_mhz"] or 1965.0
         line.update(metric=f"pixel pairs/s into {shape_desc}", value=rate, unit="pairs/s",
                     ms_per_step=ms, dtype="fp32+u64",
-                    config={"workload": "1024x1024 radial mean intensity, 5% masked, "
-                                        "all 5.5e11 unordered pixel pairs", "pixels": npix},
+                    config={"workload": f"{args.det}x{args.det} radial mean intensity, 5% masked, "
+                                        f"all {pairs:.3g} unordered pixel pairs", "pixels": npix},
                     clocks=clk,
                     roofline={"bound": "fp32", "achieved": rate * flops / 1e12,
                               "peak": _fp32_peak_tflops(mhz), "unit": "TFLOP/s",

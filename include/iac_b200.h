@@ -190,6 +190,8 @@ typedef struct {
     uint32_t tile_pairs;      /* pairs per queue tile           */
     uint32_t block_threads;   /* threads per CTA                */
     uint32_t ctas_per_sm;     /* persistent CTAs per SM         */
+    uint32_t cache_hints;     /* L2 policy: 1 = keep the mesh resident (evict-last
+                                 atomics, evict-first photon loads), 2 = none  */
 } iac_sparse_tuning;
 iac_status iac_sparse_set_tuning(iac_ctx *ctx, const iac_sparse_tuning *t);
 iac_status iac_sparse_get_tuning(iac_ctx *ctx, uint32_t size_ab, iac_sparse_tuning *t);

@@ -56,7 +56,7 @@ class SparseParams(C.Structure):
 
 class SparseTuning(C.Structure):
     _fields_ = [("tile_pairs", C.c_uint32), ("block_threads", C.c_uint32),
-                ("ctas_per_sm", C.c_uint32)]
+                ("ctas_per_sm", C.c_uint32), ("cache_hints", C.c_uint32)]
 
 
 class CrystalParams(C.Structure):
@@ -297,15 +297,15 @@ class Context:
                                               _ptr(h_rot), int(nframes), C.byref(params),
                                               _ptr(h_full)))
 
-    def set_sparse_tuning(self, tile_pairs=0, block_threads=0, ctas_per_sm=0):
-        t = SparseTuning(int(tile_pairs), int(block_threads), int(ctas_per_sm))
+    def set_sparse_tuning(self, tile_pairs=0, block_threads=0, ctas_per_sm=0, cache_hints=0):
+        t = SparseTuning(int(tile_pairs), int(block_threads), int(ctas_per_sm), int(cache_hints))
         check(lib().iac_sparse_set_tuning(self._h, C.byref(t)))
 
     def sparse_tuning(self, size_ab: int = 0):
         t = SparseTuning()
         check(lib().iac_sparse_get_tuning(self._h, int(size_ab), C.byref(t)))
         return {"tile_pairs": t.tile_pairs, "block_threads": t.block_threads,
-                "ctas_per_sm": t.ctas_per_sm}
+                "ctas_per_sm": t.ctas_per_sm, "cache_hints": t.cache_hints}
 
     def cq_small(self, d_I, d_kmap, npix, shape, interp, mult, d_mesh, stream=None):
         check(lib().iac_cq_small(self._h, _ptr(d_I), _ptr(d_kmap), int(npix), C.byref(shape),

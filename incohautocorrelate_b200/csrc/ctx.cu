@@ -56,10 +56,16 @@ static void load_tuning_table(iac_ctx *c)
     char line[512];
     while (std::fgets(line, sizeof line, fh)) {
         if (line[0] == '#') continue;
-        unsigned e, t, b, k;
-        if (std::sscanf(line, "%u %u %u %u", &e, &t, &b, &k) == 4 && t >= 64 && b >= 64 &&
-            b <= 256 && b % 32 == 0 && k >= 1 && k <= 32)
-            c->tuning_table.push_back({e, t, b, k});
+        unsigned e, t, b, k, h = 2;
+        char rest[256] = "";
+        if (std::sscanf(line, "%u %u %u %u %255[^\n]", &e, &t, &b, &k, rest) >= 4 && t >= 64 && b >= 64 &&
+            b <= 256 && b % 32 == 0 && k >= 1 && k <= 32) {
+            // optional sixth column: cache_hints (the fifth is the measured rate)
+            double rate;
+            unsigned hh;
+            if (std::sscanf(rest, "%lf %*u %u", &rate, &hh) == 2 && (hh == 1 || hh == 2)) h = hh;
+            c->tuning_table.push_back({e, t, b, k, h});
+        }
     }
     std::fclose(fh);
 }
@@ -139,6 +145,10 @@ iac_status iac_ctx_destroy(iac_ctx *ctx)
             for (auto &s : kv.second.bufs) s.release();
         }
         if (ctx->d_counters) cudaFree(ctx->d_counters);
+        for (auto &e : ctx->copy_events)
+            if (e) cudaEventDestroy(e);
+        if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+        if (ctx->host_stream) cudaStreamDestroy(ctx->host_stream);
     }
     delete ctx;
     return IAC_OK;

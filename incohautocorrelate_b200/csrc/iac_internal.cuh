@@ -14,6 +14,8 @@
 
 #include "../../include/iac_b200.h"
 
+#define IAC_COPY_CHUNKS 8
+
 namespace iac {
 
 // ---------------------------------------------------------------------------
@@ -88,10 +90,12 @@ struct iac_ctx {
     std::unordered_map<void *, iac::StreamScratch> stream_scratch;  // keyed by stream
     iac_sparse_tuning tuning{};  // explicit override (zeros: use the table)
     struct TuningRow {
-        uint32_t edge, tile_pairs, block_threads, ctas_per_sm;
+        uint32_t edge, tile_pairs, block_threads, ctas_per_sm, cache_hints;
     };
     std::vector<TuningRow> tuning_table;  // autotuner results, tuning/sparse_tuning.tsv
     cudaStream_t host_stream = nullptr;  // stream of the host-buffer entry points
+    cudaStream_t copy_stream = nullptr;  // their host-to-device copies
+    cudaEvent_t copy_events[IAC_COPY_CHUNKS + 1] = {};
     std::atomic<uint64_t> launches{0};
 };
 

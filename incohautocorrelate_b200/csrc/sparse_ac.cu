@@ -61,7 +61,36 @@ struct SparseArgs {
     double mult;
     float mult_f;                           // Multiplicator as float when it is an integer <= 1024
     const unsigned char *__restrict__ small_counts;  // per frame: counts are integers in [0, 128]
+    int cache_hints;  // 1: mesh atomics evict-last, photon loads evict-first in L2
+    uint64_t mesh_policy;  // set inside the kernel when cache_hints is on
 };
+
+// L2 cache policies (PTX createpolicy) for the pair kernel: the half mesh is
+// kept resident while the photon stream passes through.
+__device__ __forceinline__ uint64_t l2_policy_evict_last()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_first()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ void red_add_hint(unsigned long long *addr, unsigned long long v, uint64_t pol)
+{
+    asm volatile("red.global.add.L2::cache_hint.u64 [%0], %1, %2;" ::"l"(addr), "l"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ float4 ld_photon_hint(const float4 *p, uint64_t pol)
+{
+    float4 r;
+    asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+                 : "l"(p), "l"(pol));
+    return r;
+}
 
 // ---------------------------------------------------------------------------
 // planner: tiles per frame, exclusive scan, queue reset (one CTA)
@@ -151,7 +180,11 @@ __device__ __forceinline__ void hm_put(const SparseArgs &a, int fs, int ms, int 
         return;
     }
     if (v == 0) return;
-    atomicAdd(&a.half[(uint32_t)fs + (uint32_t)ms * (uint32_t)a.S + (uint32_t)ss * a.plane], v);
+    unsigned long long *addr = &a.half[(uint32_t)fs + (uint32_t)ms * (uint32_t)a.S + (uint32_t)ss * a.plane];
+    if (a.cache_hints)
+        red_add_hint(addr, v, a.mesh_policy);
+    else
+        atomicAdd(addr, v);
 }
 
 // AddQToPositiveSS, IAC/kernel.cl:349-372 (q != 0 here; q = 0 is the self pair)
@@ -289,8 +322,13 @@ __device__ __forceinline__ void bin_pair(const SparseArgs &a, const float4 A, co
 // persistent pair kernel
 // ---------------------------------------------------------------------------
 template <int DMAP, int I1, int I2>
-__global__ void __launch_bounds__(256) sparse_pairs_kernel(const SparseArgs a)
+__global__ void __launch_bounds__(256) sparse_pairs_kernel(SparseArgs a)
 {
+    uint64_t photon_policy = 0;
+    if (a.cache_hints) {
+        a.mesh_policy = l2_policy_evict_last();
+        photon_policy = l2_policy_evict_first();
+    }
     __shared__ unsigned long long s_tile;
     __shared__ uint32_t s_frame;
     __shared__ float s_rot[9];
@@ -356,7 +394,11 @@ __global__ void __launch_bounds__(256) sparse_pairs_kernel(const SparseArgs a)
                 uint32_t j = i + d;
                 if (j >= n) j -= n;
                 const uint32_t lo = min(i, j), hi = max(i, j);
-                bin_pair<DMAP, I1, I2>(a, P[lo], P[hi], R, small);
+                if (a.cache_hints)
+                    bin_pair<DMAP, I1, I2>(a, ld_photon_hint(P + lo, photon_policy),
+                                           ld_photon_hint(P + hi, photon_policy), R, small);
+                else
+                    bin_pair<DMAP, I1, I2>(a, P[lo], P[hi], R, small);
                 i += dr;
                 d += dq;
                 if (i >= n) {
@@ -491,7 +533,7 @@ __global__ void __launch_bounds__(256) ac1d_sparse_kernel(const SparseArgs a, fl
         if (hist[i]) atomicAdd(&out[i], hist[i]);
 }
 
-typedef void (*PairKernel)(const SparseArgs);
+typedef void (*PairKernel)(SparseArgs);
 
 static PairKernel pick_kernel(int dmap, int i1, int i2)
 {
@@ -518,6 +560,7 @@ static iac_sparse_tuning effective_tuning(iac_ctx *ctx, uint32_t size_ab)
             if (t.tile_pairs == 0) t.tile_pairs = best->tile_pairs;
             if (t.block_threads == 0) t.block_threads = best->block_threads;
             if (t.ctas_per_sm == 0) t.ctas_per_sm = best->ctas_per_sm;
+            if (t.cache_hints == 0) t.cache_hints = best->cache_hints;
         }
     }
     if (t.tile_pairs == 0) t.tile_pairs = 4096;
@@ -570,6 +613,7 @@ iac_status iac_sparse_set_tuning(iac_ctx *ctx, const iac_sparse_tuning *t)
                 "block_threads must be a multiple of 32 in [64, 256]");
     IAC_REQUIRE(t->tile_pairs == 0 || t->tile_pairs >= 64, "tile_pairs must be >= 64");
     IAC_REQUIRE(t->ctas_per_sm <= 32, "ctas_per_sm must be <= 32");
+    IAC_REQUIRE(t->cache_hints <= 2, "cache_hints must be 0 (table), 1 (on) or 2 (off)");
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->tuning = *t;
     return IAC_OK;
@@ -640,6 +684,8 @@ iac_status iac_sparse_ac_batch(iac_ctx *ctx, const float *d_photons, const uint6
     a.mult = p->multiplicator;
     a.mult_f = (float)p->multiplicator;
     a.small_counts = flags;
+    a.cache_hints = tun.cache_hints == 1 ? 1 : 0;
+    a.mesh_policy = 0;
 
     const PairKernel k = pick_kernel(p->double_map, p->interp_first, p->interp_second);
     const int grid = ctx->sm_count * (int)tun.ctas_per_sm;
@@ -724,32 +770,73 @@ iac_status iac_sparse_ac_frames_host(iac_ctx *ctx, const float *h_photons,
     {
         std::lock_guard<std::mutex> lk(ctx->mu);
         if (!ctx->host_stream) IAC_CUDA(cudaStreamCreateWithFlags(&ctx->host_stream, cudaStreamNonBlocking));
+        if (!ctx->copy_stream) IAC_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+        if (!ctx->copy_events[0])
+            for (auto &e : ctx->copy_events) IAC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
-    cudaStream_t s = ctx->host_stream;
+    cudaStream_t s = ctx->host_stream, cs = ctx->copy_stream;
     void *key = (void *)s;
-    const uint64_t nph = h_off[nframes] - h_off[0];
+    const uint64_t o0 = h_off[0];
+    const uint64_t nph = h_off[nframes] - o0;
     const uint32_t S = p->shape.size_ab;
     const size_t half_b = sizeof(uint64_t) * iac_half_mesh_words(S);
     const size_t full_b = sizeof(uint64_t) * iac_full_mesh_words(S);
+    // Pipelining: the frames are cut into chunks of about equal photon count;
+    // chunk k+1 is copied on the copy stream while chunk k is binned.  Every
+    // chunk has its own rebased offsets so it is an independent batch.
+    const uint32_t nchunks = std::max<uint32_t>(1, std::min<uint32_t>(IAC_COPY_CHUNKS, nframes / 64));
+    std::vector<uint32_t> cut(nchunks + 1, 0);
+    cut[nchunks] = nframes;
+    for (uint32_t k = 1; k < nchunks; k++) {
+        const uint64_t target = o0 + nph * k / nchunks;
+        cut[k] = (uint32_t)(std::lower_bound(h_off, h_off + nframes + 1, target) - h_off);
+        cut[k] = std::max(cut[k], cut[k - 1]);
+    }
     void *d_ph, *d_off, *d_rot, *d_half, *d_full;
     if ((st = stream_scratch(ctx, key, SLOT_PHOTONS, 16 * nph + 16, &d_ph)) != IAC_OK) return st;
-    if ((st = stream_scratch(ctx, key, SLOT_OFFSETS, 8 * ((size_t)nframes + 1), &d_off)) != IAC_OK) return st;
+    if ((st = stream_scratch(ctx, key, SLOT_OFFSETS, 8 * ((size_t)nframes + nchunks + 1), &d_off)) != IAC_OK) return st;
     if ((st = stream_scratch(ctx, key, SLOT_ROT, 36 * (size_t)nframes, &d_rot)) != IAC_OK) return st;
     if ((st = stream_scratch(ctx, key, SLOT_HALF, half_b, &d_half)) != IAC_OK) return st;
     if ((st = stream_scratch(ctx, key, SLOT_FULL, full_b, &d_full)) != IAC_OK) return st;
-
-    // offsets are rebased so that the first frame starts at photon 0
-    std::vector<uint64_t> off(h_off, h_off + nframes + 1);
-    const uint64_t o0 = off[0];
-    for (auto &o : off) o -= o0;
-    IAC_CUDA(cudaMemcpyAsync(d_ph, h_photons + 4 * o0, 16 * nph, cudaMemcpyHostToDevice, s));
-    IAC_CUDA(cudaMemcpyAsync(d_off, off.data(), 8 * off.size(), cudaMemcpyHostToDevice, s));
-    IAC_CUDA(cudaMemcpyAsync(d_rot, h_rot9, 36 * (size_t)nframes, cudaMemcpyHostToDevice, s));
+    std::vector<uint64_t> off((size_t)nframes + nchunks);
+    size_t w = 0;
+    std::vector<size_t> off_pos(nchunks);
+    for (uint32_t k = 0; k < nchunks; k++) {
+        off_pos[k] = w;
+        for (uint32_t f = cut[k]; f <= cut[k + 1]; f++) off[w++] = h_off[f] - h_off[cut[k]];
+    }
+    {   // size the work-queue scratch for the largest chunk now: growing it
+        // between chunk launches would synchronise the device
+        void *t = nullptr;
+        const size_t tb = ((sizeof(unsigned long long) * ((size_t)nframes + 1) + 127) / 128) * 128;
+        if ((st = stream_scratch(ctx, key, SLOT_TILES, tb + 128 + nframes, &t)) != IAC_OK) return st;
+    }
+    // the previous call's chunk copies must be done before the staging is reused
+    IAC_CUDA(cudaStreamSynchronize(cs));
     IAC_CUDA(cudaMemsetAsync(d_half, 0, half_b, s));
-    IAC_CUDA(cudaMemcpyAsync(d_full, h_full, full_b, cudaMemcpyHostToDevice, s));
-    st = iac_sparse_ac_batch(ctx, (const float *)d_ph, (const uint64_t *)d_off, (const float *)d_rot,
-                             nframes, p, (uint64_t *)d_half, key);
-    if (st != IAC_OK) return st;
+    IAC_CUDA(cudaMemcpyAsync(d_off, off.data(), 8 * w, cudaMemcpyHostToDevice, cs));
+    for (uint32_t k = 0; k < nchunks; k++) {
+        const uint32_t f0 = cut[k], f1 = cut[k + 1];
+        const uint64_t p0 = h_off[f0] - o0, p1 = h_off[f1] - o0;
+        if (p1 > p0)
+            IAC_CUDA(cudaMemcpyAsync((char *)d_ph + 16 * p0, h_photons + 4 * (o0 + p0), 16 * (p1 - p0),
+                                     cudaMemcpyHostToDevice, cs));
+        if (f1 > f0)
+            IAC_CUDA(cudaMemcpyAsync((char *)d_rot + 36 * (size_t)f0, h_rot9 + 9 * (size_t)f0,
+                                     36 * (size_t)(f1 - f0), cudaMemcpyHostToDevice, cs));
+        IAC_CUDA(cudaEventRecord(ctx->copy_events[k], cs));
+        IAC_CUDA(cudaStreamWaitEvent(s, ctx->copy_events[k], 0));
+        if (f1 > f0) {
+            st = iac_sparse_ac_batch(ctx, (const float *)((char *)d_ph + 16 * p0),
+                                     (const uint64_t *)d_off + off_pos[k], (const float *)d_rot + 9 * (size_t)f0,
+                                     f1 - f0, p, (uint64_t *)d_half, key);
+            if (st != IAC_OK) return st;
+        }
+    }
+    // the mesh the caller holds, uploaded behind the photon stream
+    IAC_CUDA(cudaMemcpyAsync(d_full, h_full, full_b, cudaMemcpyHostToDevice, cs));
+    IAC_CUDA(cudaEventRecord(ctx->copy_events[nchunks], cs));
+    IAC_CUDA(cudaStreamWaitEvent(s, ctx->copy_events[nchunks], 0));
     st = iac_sparse_fold(ctx, (const uint64_t *)d_half, S, (uint64_t *)d_full, key);
     if (st != IAC_OK) return st;
     IAC_CUDA(cudaMemcpyAsync(h_full, d_full, full_b, cudaMemcpyDeviceToHost, s));
@@ -875,6 +962,8 @@ extern "C" iac_status iac_sparse_ac_batch_static(iac_ctx *ctx, const float *d_ph
     a.mult = p->multiplicator;
     a.mult_f = (float)p->multiplicator;
     a.small_counts = flags;
+    a.cache_hints = tun.cache_hints == 1 ? 1 : 0;
+    a.mesh_policy = 0;
     const PairKernel k = pick_kernel(p->double_map, p->interp_first, p->interp_second);
     k<<<ctx->sm_count * (int)tun.ctas_per_sm, tun.block_threads, 0, s>>>(a);
     IAC_LAUNCHED(ctx);

@@ -167,6 +167,43 @@ def test_host_entry_point_accumulates(ctx, oracle_lib, rng):
     np.testing.assert_array_equal(mesh, 2 * want)
 
 
+def test_host_entry_point_pipelined_chunks(ctx, oracle_lib):
+    """1 500 frames go through the host entry point in several copy/compute
+    chunks; the mesh equals the device entry point's and the oracle's."""
+    import torch
+    from incohautocorrelate_b200 import capi, workloads as W
+    cfg = W.rotated_config(nframes=1500, seed=31)
+    shape = oracle_lib.big_mesh_shape(cfg["max_q"], cfg["mesh_size"])
+    want, _ = oracle_lib.sparse_batch(cfg["photons"], cfg["offsets"], cfg["rot"], shape, cpu_gpu=-1,
+                                      det_pixels=cfg["npix"])
+    p = capi.sparse_params(to_capi_shape(shape))
+    ph = torch.from_numpy(cfg["photons"]).pin_memory()
+    off = torch.from_numpy(cfg["offsets"].view(np.int64)).pin_memory()
+    rot = torch.from_numpy(cfg["rot"]).pin_memory()
+    mesh = torch.zeros(capi.full_mesh_words(shape.size_ab), dtype=torch.int64).pin_memory()
+    ctx.sparse_ac_frames_host(ph, off, rot, 1500, p, mesh)
+    np.testing.assert_array_equal(mesh.numpy().view(np.uint64), want)
+    # a sub-range of frames: offsets that do not start at 0
+    mesh.zero_()
+    ctx.sparse_ac_frames_host(ph, off[700:].clone(), rot[700:].clone(), 800, p, mesh)
+    part, _ = oracle_lib.sparse_batch(cfg["photons"][int(cfg["offsets"][700]):],
+                                      cfg["offsets"][700:] - cfg["offsets"][700], cfg["rot"][700:], shape,
+                                      cpu_gpu=-1, det_pixels=cfg["npix"])
+    np.testing.assert_array_equal(mesh.numpy().view(np.uint64), part)
+
+
+def test_cache_hint_setting_does_not_change_the_mesh(ctx, oracle_lib, rng):
+    from incohautocorrelate_b200 import workloads as W
+    _, km, mq = small_detector()
+    shape = oracle_lib.big_mesh_shape(mq, 31)
+    ph, off = random_frames(km, [5, 90, 200, 1, 33], rng)
+    rot = W.haar_rotations(5, seed=18)
+    want, _ = oracle_lib.sparse_batch(ph, off, rot, shape)
+    for hints in (1, 2):
+        got, _ = gpu_full_mesh(ctx, ph, off, rot, shape, tuning=dict(cache_hints=hints))
+        np.testing.assert_array_equal(got, want)
+
+
 def test_full_size_properties(ctx):
     """100 000 rotated frames at 201^3: point symmetry of the full mesh, the
     batch is the sum of its halves (linearity), and the result does not depend
