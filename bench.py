@@ -280,8 +280,8 @@ def run_ours(args):
     ev = []
 
     def step(record=False):
+        full.zero_()  # clear the full mesh first so the half mesh is the L2-resident one
         half.zero_()
-        full.zero_()
         if record:
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
@@ -457,13 +457,13 @@ def run_kernel(args):
             sh = capi.small_cq_mesh_shape(mq, 253)
             mult = capi.cq_small_multiplicator(I)
             out = torch.zeros(sh.size_ab * sh.size_ab * sh.size_c, dtype=torch.int64, device="cuda")
-            fn = lambda: (out.zero_(), ctx.cq_small(dI, dk, npix, sh, 0, mult, out, sp))
+            fn = lambda: (out.zero_(), ctx.cq_small(dI, dk, npix, sh, 0, mult, out, sp, fast_size=args.det))
             shape_desc = f"small C(q) mesh {sh.size_ab}x{sh.size_ab}x{sh.size_c}"
         else:
             sh = capi.ac1d_shape(mq, 2048)
             mult = capi.ac1d_cq_multiplicator(I)
             out = torch.zeros(sh.size, dtype=torch.int64, device="cuda")
-            fn = lambda: (out.zero_(), ctx.ac1d_cq(dI, dk, npix, sh, 1, mult, out, sp))
+            fn = lambda: (out.zero_(), ctx.ac1d_cq(dI, dk, npix, sh, 1, mult, out, sp, fast_size=args.det))
             shape_desc = "AC1D 2048 bins, linear"
         clocks.start()
         ms = _time(fn, args.steps, min(args.warmup, 1), stream)
@@ -510,7 +510,7 @@ def run_kernel(args):
         mult = capi.cq_small_multiplicator(I)
         small_u = torch.zeros(sh.size_ab * sh.size_ab * sh.size_c, dtype=torch.int64, device="cuda")
         ctx.cq_small(torch.from_numpy(I).cuda(), torch.from_numpy(km).cuda(), npix, sh, 0, mult,
-                     small_u, sp)
+                     small_u, sp, fast_size=1024)
         small = (small_u.cpu().numpy().view(np.uint64).astype(np.float64) / mult)
         nf = args.frames
         R = W.haar_rotations(nf, seed=3)

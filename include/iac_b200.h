@@ -210,10 +210,13 @@ iac_status iac_cq_small_multiplicator(const float *h_intensity, uint64_t npix, d
  * ordered pixel pair of the mean intensity, (uint64)(I_a*I_b*Mult) binned at
  * q = k_a - k_b on the small mesh (nearest or 8-corner linear).
  * d_mesh (uint64[size_ab^2 * size_c], CQMesh order) is accumulated, not
- * cleared; CQMesh = d_mesh / Mult.  Asynchronous on `stream`. */
+ * cleared; CQMesh = d_mesh / Mult.  fast_size is the detector row length
+ * (DetectorSize[1]); given, the kernel works on 16 x 16 pixel patches whose
+ * pair differences stay within a small shared-memory window (0 = unknown
+ * pixel order).  Asynchronous on `stream`. */
 iac_status iac_cq_small(iac_ctx *ctx, const float *d_intensity, const float *d_kmap,
-                        uint64_t npix, const iac_mesh_shape *small_shape, int interp,
-                        double multiplicator, uint64_t *d_mesh, void *stream);
+                        uint64_t npix, uint32_t fast_size, const iac_mesh_shape *small_shape,
+                        int interp, double multiplicator, uint64_t *d_mesh, void *stream);
 
 /* Rotation/weight table and Multiplicator of Detector::Merge_smallCofQ
  * (IAC/Detector.cpp:1339-1427): h_rw10 gets 9 rotation floats + the rounded
@@ -240,9 +243,10 @@ iac_status iac_ac1d_cq_multiplicator(const float *h_intensity, uint64_t npix, do
 /* Kernel AutoCorr_CQ_AV (IAC/kernel.cl:656-764) of AC1D::Calculate_CQ
  * (IAC/AC1D.cpp:61-195): |q| histogram of all ordered pixel pairs of the mean
  * intensity into d_hist (uint64[shape.size], accumulated).  Equals the sum of
- * the reference's 10000 sub-histograms; CQ = d_hist / Mult.  Asynchronous. */
+ * the reference's 10000 sub-histograms; CQ = d_hist / Mult.  fast_size as for
+ * iac_cq_small.  Asynchronous. */
 iac_status iac_ac1d_cq(iac_ctx *ctx, const float *d_intensity, const float *d_kmap,
-                       uint64_t npix, const iac_ac1d_shape *shape, int interp,
+                       uint64_t npix, uint32_t fast_size, const iac_ac1d_shape *shape, int interp,
                        double multiplicator, uint64_t *d_hist, void *stream);
 
 /* VecSize = ceil(MaxQ / dq) - 1 of Calculate_AC_UW_Mapped (IAC/AC1D.cpp:301). */

@@ -282,7 +282,7 @@ void Detector::AutoCorrelate_CofQ_SmallMesh(ACMesh &SmallMesh, AutoCorrFlags Fla
     Check(iac_memcpy_h2d(ctx, dI.p, Intensity, n * 4, s), "copy intensity");
     Check(iac_memcpy_h2d(ctx, dK.p, kMap, n * 12, s), "copy k-map");
     Check(iac_memset_device(ctx, dM.p, 0, words * 8, s), "clear mesh");
-    Check(iac_cq_small(ctx, (const float *)dI.p, (const float *)dK.p, n, &sh, Flags.InterpolationMode, mult,
+    Check(iac_cq_small(ctx, (const float *)dI.p, (const float *)dK.p, n, DetectorSize[1], &sh, Flags.InterpolationMode, mult,
                        (uint64_t *)dM.p, s),
           "iac_cq_small");
     std::vector<uint64_t> h(words);

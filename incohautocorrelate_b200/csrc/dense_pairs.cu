@@ -16,9 +16,10 @@
 // centre; for |q| the two orders are identical and the bin gets twice the
 // value.  Self pairs (q = 0) are added once at the centre.
 //
-// Work decomposition.  Pixels are cut into tiles of TILE consecutive pixels.
+// Work decomposition.  Pixels are cut into tiles of 256: 16 x 16 patches of
+// the detector when its row length is given, else 256 consecutive pixels.
 // A persistent CTA pops tile pairs (P <= Q) from a queue: thread t owns pixel
-// P*TILE + t and walks the TILE pixels of Q, staged in shared memory as float4
+// t of tile P and walks the TILE pixels of Q, staged in shared memory as float4
 // (k, I).  Tile pairs whose k bounding boxes are farther apart than MaxQ are
 // skipped whole.  Contributions are accumulated per thread while consecutive
 // pixels of Q fall into the same voxel (row-adjacent pixels move q by a
@@ -51,6 +52,8 @@ struct DenseArgs {
     uint64_t npix;
     uint32_t ntiles;
     unsigned long long npairs;  // tile pairs
+    uint32_t nx, ny, ptx;       // 2D patch tiling: row length, rows, patches per row (nx = 0: linear)
+    uint32_t mult_int;          // Multiplicator as an integer below 2^29, else 0
     float maxq, maxq2;
     float vpdq;
     double mult;
@@ -78,13 +81,43 @@ __device__ __forceinline__ void decode_tile_pair(unsigned long long p, uint32_t 
     if (Q >= T) Q -= T;
 }
 
-__global__ void tile_box_kernel(const float *__restrict__ K, const float *__restrict__ I,
-                                uint64_t npix, uint32_t ntiles, float4 *__restrict__ box)
+// Pixel of slot j (0..255) of tile t.  With the row length known the tiles
+// are 16 x 16 pixel patches, whose pair differences cover a few voxels, so the
+// shared-memory window of a tile pair stays small; otherwise 256 consecutive
+// pixels.  Returns npix for a slot outside the detector.
+__device__ __forceinline__ uint64_t tile_pixel(const DenseArgs &a, uint32_t t, uint32_t j)
+{
+    if (a.nx) {
+        const uint32_t py = t / a.ptx, px = t - py * a.ptx;
+        const uint32_t y = py * 16 + (j >> 4), x = px * 16 + (j & 15);
+        return (y < a.ny && x < a.nx) ? (uint64_t)y * a.nx + x : a.npix;
+    }
+    const uint64_t i = (uint64_t)t * DTILE + j;
+    return i < a.npix ? i : a.npix;
+}
+
+// (uint64)((double)p * M) for finite p >= 0 and an integer M < 2^29: the double
+// product of a 24-bit mantissa and M is exact, so the cast is the floor of the
+// exact product, formed here in integers.
+__device__ __forceinline__ unsigned long long scaled_floor(float p, uint32_t M)
+{
+    const uint32_t b = __float_as_uint(p);
+    const int e = (int)((b >> 23) & 0xff);
+    const uint64_t m = (b & 0x7fffffu) | (e ? 0x800000u : 0u);
+    const int sh = (e ? e : 1) - 150;  // p = m * 2^sh
+    const uint64_t prod = m * (uint64_t)M;
+    if (sh >= 0) return prod << sh;
+    return sh <= -64 ? 0ull : (prod >> (-sh));
+}
+
+__global__ void tile_box_kernel(const DenseArgs a, float4 *__restrict__ box)
 {
     const uint32_t t = blockIdx.x;
-    const uint64_t i = (uint64_t)t * DTILE + threadIdx.x;
+    const uint64_t i = tile_pixel(a, t, threadIdx.x);
+    const float *__restrict__ K = a.K;
+    const float *__restrict__ I = a.I;
     float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-    if (i < npix && I[i] != 0.0f) {  // zero-intensity pixels never contribute
+    if (i < a.npix && I[i] != 0.0f) {  // zero-intensity pixels never contribute
 #pragma unroll
         for (int d = 0; d < 3; d++) mn[d] = mx[d] = K[3 * i + d];
     }
@@ -213,19 +246,20 @@ __global__ void __launch_bounds__(DTILE) cq_small_kernel(const DenseArgs a)
         }
         // stage tile Q
         {
-            const uint64_t j = (uint64_t)Q * DTILE + threadIdx.x;
+            const uint64_t j = tile_pixel(a, Q, threadIdx.x);
             sq[threadIdx.x] = j < a.npix ? make_float4(a.K[3 * j], a.K[3 * j + 1], a.K[3 * j + 2], a.I[j])
                                          : make_float4(0.f, 0.f, 0.f, 0.f);
         }
         __syncthreads();
-        const uint64_t ia = (uint64_t)P * DTILE + threadIdx.x;
+        const uint64_t ia = tile_pixel(a, P, threadIdx.x);
         unsigned long long self = 0;
         if (ia < a.npix) {
             const float k0 = a.K[3 * ia], k1 = a.K[3 * ia + 1], k2 = a.K[3 * ia + 2];
             const float Ia = a.I[ia];
             if (P == Q) {
-                const double sv = (double)fmul(Ia, Ia);
-                if (!(sv < 1e-37f)) self = d2u64(dmul(sv, a.mult));
+                const float sv = fmul(Ia, Ia);
+                if (!(sv < 1e-37f))
+                    self = a.mult_int ? scaled_floor(sv, a.mult_int) : d2u64(dmul((double)sv, a.mult));
             }
             const int j0 = (P == Q) ? threadIdx.x + 1 : 0;
             int cur_f = 0, cur_m = 0, cur_s = 0;
@@ -235,8 +269,8 @@ __global__ void __launch_bounds__(DTILE) cq_small_kernel(const DenseArgs a)
             bool have = false;
             for (int j = j0; j < DTILE; j++) {
                 const float4 b = sq[j];
-                const double val = (double)fmul(Ia, b.w);
-                if (val < 1e-37f) continue;
+                const float pv = fmul(Ia, b.w);  // (double)(I_a*I_b) < 1e-37f  <=>  pv < 1e-37f
+                if (pv < 1e-37f) continue;
                 float qx = fsub(k0, b.x), qy = fsub(k1, b.y), qz = fsub(k2, b.z);
                 if (fadd(fadd(fmul(qx, qx), fmul(qy, qy)), fmul(qz, qz)) > a.maxq2) continue;
                 qx = fmul(qx, a.vpdq);
@@ -244,7 +278,6 @@ __global__ void __launch_bounds__(DTILE) cq_small_kernel(const DenseArgs a)
                 qz = fmul(qz, a.vpdq);
                 const float qa = pick(qx, qy, qz, a.ka), qb = pick(qx, qy, qz, a.kb),
                             qc = pick(qx, qy, qz, a.kc);
-                const double vm = dmul(val, a.mult);
                 int f, m, s;
                 if (INTERP == 0) {
                     f = (int)fadd(round_away_f(qa), cabf);
@@ -273,8 +306,9 @@ __global__ void __launch_bounds__(DTILE) cq_small_kernel(const DenseArgs a)
                     for (int c = 0; c < (INTERP ? 8 : 1); c++) acc[c] = 0;
                 }
                 if (INTERP == 0) {
-                    acc[0] += d2u64(vm);
+                    acc[0] += a.mult_int ? scaled_floor(pv, a.mult_int) : d2u64(dmul((double)pv, a.mult));
                 } else {
+                    const double vm = dmul((double)pv, a.mult);
                     // IAC/kernel.cl:139-179: Sep = 1 - (q - floor q) in float
                     const double sf = (double)fsub(1.0f, fsub(qa, floorf(qa)));
                     const double sm = (double)fsub(1.0f, fsub(qb, floorf(qb)));
@@ -342,32 +376,37 @@ __global__ void __launch_bounds__(DTILE) ac1d_cq_kernel(const DenseArgs a)
             continue;
         }
         {
-            const uint64_t j = (uint64_t)Q * DTILE + threadIdx.x;
+            const uint64_t j = tile_pixel(a, Q, threadIdx.x);
             sq[threadIdx.x] = j < a.npix ? make_float4(a.K[3 * j], a.K[3 * j + 1], a.K[3 * j + 2], a.I[j])
                                          : make_float4(0.f, 0.f, 0.f, 0.f);
         }
         __syncthreads();
-        const uint64_t ia = (uint64_t)P * DTILE + threadIdx.x;
+        const uint64_t ia = tile_pixel(a, P, threadIdx.x);
         if (ia < a.npix) {
             const float k0 = a.K[3 * ia], k1 = a.K[3 * ia + 1], k2 = a.K[3 * ia + 2];
             const float Ia = a.I[ia];
             if (P == Q) {  // self pair: q = 0 -> bin 0, once
-                const double sv = (double)fmul(Ia, Ia);
-                if (!(sv < 1e-37f)) atomicAdd(&hist[0], (unsigned long long)(long long)dmul(sv, a.mult));
+                const float sv = fmul(Ia, Ia);
+                if (!(sv < 1e-37f))
+                    atomicAdd(&hist[0], a.mult_int ? scaled_floor(sv, a.mult_int)
+                                                   : (unsigned long long)(long long)dmul((double)sv, a.mult));
             }
             const int j0 = (P == Q) ? threadIdx.x + 1 : 0;
             for (int j = j0; j < DTILE; j++) {
                 const float4 b = sq[j];
-                const double val = (double)fmul(Ia, b.w);
-                if (val < 1e-37f) continue;
+                const float pv = fmul(Ia, b.w);
+                if (pv < 1e-37f) continue;
+                const double val = (double)pv;
                 const float dx = fsub(k0, b.x), dy = fsub(k1, b.y), dz = fsub(k2, b.z);
                 float q = __fsqrt_rn(fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz)));
                 if (q > a.maxq) continue;
                 q = __fdiv_rn(q, a.dq);
                 if (INTERP == 0) {
-                    // sc = (uint)floor(q + 0.5) with q + 0.5 in double
-                    const uint32_t sc = (uint32_t)floor(dadd((double)q, 0.5)) % a.hsize;
-                    const unsigned long long v = (unsigned long long)(long long)dmul(val, a.mult);
+                    // sc = (uint)floor(q + 0.5) with q + 0.5 in double; for q < 2^22
+                    // the float sum is exact and gives the same bin
+                    const uint32_t sc = (uint32_t)floorf(fadd(q, 0.5f)) % a.hsize;
+                    const unsigned long long v =
+                        a.mult_int ? scaled_floor(pv, a.mult_int) : (unsigned long long)(long long)dmul(val, a.mult);
                     atomicAdd(&hist[sc], 2ull * v);
                 } else {
                     const float fq = floorf(q);
@@ -403,12 +442,22 @@ static float sqrt_threshold(float m)
 
 // tile boxes + queue counter in stream scratch; returns args with common fields
 static iac_status prepare(iac_ctx *ctx, void *stream, const float *d_I, const float *d_K,
-                          uint64_t npix, DenseArgs &a)
+                          uint64_t npix, uint32_t fast_size, double mult, DenseArgs &a)
 {
     a.I = d_I;
     a.K = d_K;
     a.npix = npix;
-    a.ntiles = (uint32_t)((npix + DTILE - 1) / DTILE);
+    a.mult = mult;
+    a.mult_int = (mult >= 1.0 && mult < 536870912.0 && mult == std::floor(mult)) ? (uint32_t)mult : 0u;
+    if (fast_size >= 16 && npix % fast_size == 0) {
+        a.nx = fast_size;
+        a.ny = (uint32_t)(npix / fast_size);
+        a.ptx = (a.nx + 15) / 16;
+        a.ntiles = a.ptx * ((a.ny + 15) / 16);
+    } else {
+        a.nx = a.ny = a.ptx = 0;
+        a.ntiles = (uint32_t)((npix + DTILE - 1) / DTILE);
+    }
     a.npairs = (unsigned long long)a.ntiles * (a.ntiles + 1) / 2;
     a.counters = ctx->d_counters;
     void *scr = nullptr;
@@ -419,7 +468,7 @@ static iac_status prepare(iac_ctx *ctx, void *stream, const float *d_I, const fl
     a.queue = (unsigned long long *)((char *)scr + ((box_bytes + 127) / 128) * 128);
     cudaStream_t s = as_stream(stream);
     IAC_CUDA(cudaMemsetAsync(a.queue, 0, sizeof(unsigned long long), s));
-    tile_box_kernel<<<a.ntiles, DTILE, 0, s>>>(d_K, d_I, npix, a.ntiles, (float4 *)scr);
+    tile_box_kernel<<<a.ntiles, DTILE, 0, s>>>(a, (float4 *)scr);
     IAC_LAUNCHED(ctx);
     IAC_CUDA(cudaGetLastError());
     return IAC_OK;
@@ -432,8 +481,8 @@ using namespace iac;
 extern "C" {
 
 iac_status iac_cq_small(iac_ctx *ctx, const float *d_I, const float *d_kmap, uint64_t npix,
-                        const iac_mesh_shape *sh, int interp, double mult, uint64_t *d_mesh,
-                        void *stream)
+                        uint32_t fast_size, const iac_mesh_shape *sh, int interp, double mult,
+                        uint64_t *d_mesh, void *stream)
 {
     IAC_REQUIRE(ctx && d_I && d_kmap && sh && d_mesh, "iac_cq_small: NULL argument");
     IAC_REQUIRE(interp == 0 || interp == 1, "interpolation must be 0 or 1");
@@ -445,13 +494,12 @@ iac_status iac_cq_small(iac_ctx *ctx, const float *d_I, const float *d_kmap, uin
     IAC_REQUIRE(mult > 0, "multiplicator must be positive");
     DeviceGuard g(ctx->device);
     DenseArgs a{};
-    iac_status st = prepare(ctx, stream, d_I, d_kmap, npix, a);
+    iac_status st = prepare(ctx, stream, d_I, d_kmap, npix, fast_size, mult, a);
     if (st != IAC_OK) return st;
     a.out = (unsigned long long *)d_mesh;
     a.maxq = sh->max_q;
     a.maxq2 = sqrt_threshold(sh->max_q);
     a.vpdq = (float)sh->voxel_per_dq;
-    a.mult = mult;
     a.ab = (int)sh->size_ab;
     a.sc = (int)sh->size_c;
     a.cab = (a.ab - 1) / 2;
@@ -459,7 +507,7 @@ iac_status iac_cq_small(iac_ctx *ctx, const float *d_I, const float *d_kmap, uin
     a.ka = (int)sh->k_a;
     a.kb = (int)sh->k_b;
     a.kc = (int)sh->k_c;
-    const int grid = ctx->sm_count * 4;
+    const int grid = ctx->sm_count * 8;
     if (interp == 0)
         cq_small_kernel<0><<<grid, DTILE, 0, as_stream(stream)>>>(a);
     else
@@ -470,8 +518,8 @@ iac_status iac_cq_small(iac_ctx *ctx, const float *d_I, const float *d_kmap, uin
 }
 
 iac_status iac_ac1d_cq(iac_ctx *ctx, const float *d_I, const float *d_kmap, uint64_t npix,
-                       const iac_ac1d_shape *sh, int interp, double mult, uint64_t *d_hist,
-                       void *stream)
+                       uint32_t fast_size, const iac_ac1d_shape *sh, int interp, double mult,
+                       uint64_t *d_hist, void *stream)
 {
     IAC_REQUIRE(ctx && d_I && d_kmap && sh && d_hist, "iac_ac1d_cq: NULL argument");
     IAC_REQUIRE(interp == 0 || interp == 1, "interpolation must be 0 or 1");
@@ -480,18 +528,17 @@ iac_status iac_ac1d_cq(iac_ctx *ctx, const float *d_I, const float *d_kmap, uint
     IAC_REQUIRE(mult > 0, "multiplicator must be positive");
     DeviceGuard g(ctx->device);
     DenseArgs a{};
-    iac_status st = prepare(ctx, stream, d_I, d_kmap, npix, a);
+    iac_status st = prepare(ctx, stream, d_I, d_kmap, npix, fast_size, mult, a);
     if (st != IAC_OK) return st;
     a.out = (unsigned long long *)d_hist;
     a.maxq = sh->max_q;
     a.maxq2 = sqrt_threshold(sh->max_q);
-    a.mult = mult;
     a.hsize = sh->size;
     a.dq = sh->dq_per_step;
     const size_t smem = sizeof(unsigned long long) * sh->size;
     auto k = interp == 0 ? ac1d_cq_kernel<0> : ac1d_cq_kernel<1>;
     IAC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<ctx->sm_count * 4, DTILE, smem, as_stream(stream)>>>(a);
+    k<<<ctx->sm_count * 8, DTILE, smem, as_stream(stream)>>>(a);
     IAC_LAUNCHED(ctx);
     IAC_CUDA(cudaGetLastError());
     return IAC_OK;

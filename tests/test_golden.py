@@ -115,9 +115,10 @@ def test_gpu_dense_fixtures(ctx, oracle_lib):
     I, km = g["intensity"], g["kmap"]
     s = to_capi_shape(oracle_lib.small_cq_mesh_shape(g["max_q"], int(g["perp"])))
     for interp in (0, 1):
-        out = torch.zeros(g["cq_small_0"].size, dtype=torch.int64, device="cuda")
-        ctx.cq_small(_dev(I), _dev(km), I.size, s, interp, float(g["mult"]), out)
-        np.testing.assert_array_equal(out.cpu().numpy().view(np.uint64), g[f"cq_small_{interp}"])
+        for fast in (0, 22):  # linear tiles, 16 x 16 patches of the 18 x 22 detector
+            out = torch.zeros(g["cq_small_0"].size, dtype=torch.int64, device="cuda")
+            ctx.cq_small(_dev(I), _dev(km), I.size, s, interp, float(g["mult"]), out, fast_size=fast)
+            np.testing.assert_array_equal(out.cpu().numpy().view(np.uint64), g[f"cq_small_{interp}"])
     small = g["cq_small_0"].astype(np.float64) / float(g["mult"])
     nf = len(g["merge_mean_intensity"])
     for interp in (0, 1):
@@ -126,9 +127,10 @@ def test_gpu_dense_fixtures(ctx, oracle_lib):
         np.testing.assert_array_equal(big.cpu().numpy().view(np.uint64), g[f"merge_{interp}"])
     sh = capi.ac1d_shape(g["max_q"], 97)
     for interp in (0, 1):
-        h = torch.zeros(sh.size, dtype=torch.int64, device="cuda")
-        ctx.ac1d_cq(_dev(I), _dev(km), I.size, sh, interp, float(g["ac1d_mult"]), h)
-        np.testing.assert_array_equal(h.cpu().numpy().view(np.uint64), g[f"ac1d_cq_{interp}"])
+        for fast in (0, 22):
+            h = torch.zeros(sh.size, dtype=torch.int64, device="cuda")
+            ctx.ac1d_cq(_dev(I), _dev(km), I.size, sh, interp, float(g["ac1d_mult"]), h, fast_size=fast)
+            np.testing.assert_array_equal(h.cpu().numpy().view(np.uint64), g[f"ac1d_cq_{interp}"])
     assert ctx.check() == 0
 
 

@@ -40,8 +40,11 @@ def _oracle_cq_small(o, I, km, s, interp, mult, rows=None):
 
 
 @pytest.mark.parametrize("interp", [0, 1])
+@pytest.mark.parametrize("patches", [False, True])
 @pytest.mark.parametrize("ny,nx", [(40, 48), (33, 70), (1, 300)])
-def test_cq_small_bit_exact(ctx, oracle_lib, rng, interp, ny, nx):
+def test_cq_small_bit_exact(ctx, oracle_lib, rng, interp, patches, ny, nx):
+    """Linear tiles (row length unknown) and 16 x 16 patches, including
+    ragged patches at the detector edges and a single-row detector."""
     from incohautocorrelate_b200 import capi
     o = oracle_lib
     pm, km, mq = small_detector(ny, nx, 6e-4)
@@ -52,9 +55,27 @@ def test_cq_small_bit_exact(ctx, oracle_lib, rng, interp, ny, nx):
     assert mult == o.lib().iaco_cq_small_multiplicator(o.p(I), npix)
     want = _oracle_cq_small(o, I, km, s, interp, mult)
     out = _zeros(want.size)
-    ctx.cq_small(_dev(I), _dev(km), npix, to_capi_shape(s), interp, mult, out)
+    ctx.cq_small(_dev(I), _dev(km), npix, to_capi_shape(s), interp, mult, out,
+                 fast_size=nx if patches else 0)
     assert ctx.check() == 0
     np.testing.assert_array_equal(_u64(out), want)
+
+
+@pytest.mark.parametrize("mult", [1000.0, 1234.5, 3.0e9, 2.0 ** 29 - 1])
+def test_cq_small_value_paths(ctx, oracle_lib, rng, mult):
+    """Integer multiplicators below 2^29 take the exact integer product; the
+    others the double product.  Both reproduce the reference's cast."""
+    o = oracle_lib
+    pm, km, mq = small_detector(24, 40, 6e-4)
+    I = _intensity(km.size // 3, rng)
+    I[::7] *= np.float32(37.25)
+    s = o.small_cq_mesh_shape(mq, 31)
+    for fast in (0, 40):
+        want = _oracle_cq_small(o, I, km, s, 0, mult)
+        out = _zeros(want.size)
+        ctx.cq_small(_dev(I), _dev(km), I.size, to_capi_shape(s), 0, mult, out, fast_size=fast)
+        assert ctx.check() == 0
+        np.testing.assert_array_equal(_u64(out), want)
 
 
 def test_cq_small_dense_detector_region(ctx, oracle_lib):
@@ -68,10 +89,11 @@ def test_cq_small_dense_detector_region(ctx, oracle_lib):
     s = o.small_cq_mesh_shape(mq, 253)
     mult = capi.cq_small_multiplicator(I)
     want = _oracle_cq_small(o, I, km, s, 0, mult)
-    out = _zeros(want.size)
-    ctx.cq_small(_dev(I), _dev(km), I.size, to_capi_shape(s), 0, mult, out)
-    assert ctx.check() == 0
-    np.testing.assert_array_equal(_u64(out), want)
+    for fast in (0, 128):
+        out = _zeros(want.size)
+        ctx.cq_small(_dev(I), _dev(km), I.size, to_capi_shape(s), 0, mult, out, fast_size=fast)
+        assert ctx.check() == 0
+        np.testing.assert_array_equal(_u64(out), want)
 
 
 @pytest.mark.parametrize("interp", [0, 1])
@@ -103,7 +125,9 @@ def test_cq_merge_bit_exact(ctx, oracle_lib, rng, interp):
 
 
 @pytest.mark.parametrize("interp", [0, 1])
-def test_ac1d_cq_bit_exact(ctx, oracle_lib, rng, interp):
+@pytest.mark.parametrize("fast", [0, 48])
+@pytest.mark.parametrize("mult_of", ["reference", 1234.5])
+def test_ac1d_cq_bit_exact(ctx, oracle_lib, rng, interp, fast, mult_of):
     from incohautocorrelate_b200 import capi
     o = oracle_lib
     pm, km, mq = small_detector(40, 48, 6e-4)
@@ -113,10 +137,13 @@ def test_ac1d_cq_bit_exact(ctx, oracle_lib, rng, interp):
     sh = capi.ac1d_shape(mq, 257)
     mult = capi.ac1d_cq_multiplicator(I)
     assert mult == o.lib().iaco_ac1d_cq_multiplicator(o.p(I), npix)
+    if mult_of != "reference":
+        mult = mult_of
     want = np.zeros(sh.size, np.uint64)
     o.lib().iaco_ac1d_cq(o.p(I), o.p(km), npix, sh_o, interp, mult, 0, npix, o.p(want))
     out = _zeros(sh.size)
-    ctx.ac1d_cq(_dev(I), _dev(km), npix, sh, interp, mult, out)
+    ctx.ac1d_cq(_dev(I), _dev(km), npix, sh, interp, mult, out, fast_size=fast)
+    assert ctx.check() == 0
     np.testing.assert_array_equal(_u64(out), want)
 
 
