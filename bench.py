@@ -463,7 +463,7 @@ def run_kernel(args):
             sh = capi.ac1d_shape(mq, 2048)
             mult = capi.ac1d_cq_multiplicator(I)
             out = torch.zeros(sh.size, dtype=torch.int64, device="cuda")
-            fn = lambda: (out.zero_(), ctx.ac1d_cq(dI, dk, npix, sh, 1, mult, out, sp, fast_size=args.det))
+            fn = lambda: (out.zero_(), ctx.ac1d_cq(dI, dk, npix, sh, 1, mult, out, sp))
             shape_desc = "AC1D 2048 bins, linear"
         clocks.start()
         ms = _time(fn, args.steps, min(args.warmup, 1), stream)

@@ -243,10 +243,9 @@ iac_status iac_ac1d_cq_multiplicator(const float *h_intensity, uint64_t npix, do
 /* Kernel AutoCorr_CQ_AV (IAC/kernel.cl:656-764) of AC1D::Calculate_CQ
  * (IAC/AC1D.cpp:61-195): |q| histogram of all ordered pixel pairs of the mean
  * intensity into d_hist (uint64[shape.size], accumulated).  Equals the sum of
- * the reference's 10000 sub-histograms; CQ = d_hist / Mult.  fast_size as for
- * iac_cq_small.  Asynchronous. */
+ * the reference's 10000 sub-histograms; CQ = d_hist / Mult.  Asynchronous. */
 iac_status iac_ac1d_cq(iac_ctx *ctx, const float *d_intensity, const float *d_kmap,
-                       uint64_t npix, uint32_t fast_size, const iac_ac1d_shape *shape, int interp,
+                       uint64_t npix, const iac_ac1d_shape *shape, int interp,
                        double multiplicator, uint64_t *d_hist, void *stream);
 
 /* VecSize = ceil(MaxQ / dq) - 1 of Calculate_AC_UW_Mapped (IAC/AC1D.cpp:301). */

@@ -122,7 +122,7 @@ def _declare(lib):
     fn("iac_cq_merge_weights", [_VP, _VP, _U32, _VP, _U64, _VP, C.POINTER(D)])
     fn("iac_cq_merge", [_VP, _VP, _VP, _U32, C.POINTER(MeshShape), C.c_int, D, _VP, _VP])
     fn("iac_ac1d_cq_multiplicator", [_VP, _U64, C.POINTER(D)])
-    fn("iac_ac1d_cq", [_VP, _VP, _VP, _U64, _U32, C.POINTER(AC1DShape), C.c_int, D, _VP, _VP])
+    fn("iac_ac1d_cq", [_VP, _VP, _VP, _U64, C.POINTER(AC1DShape), C.c_int, D, _VP, _VP])
     fn("iac_ac1d_vecsize", [C.c_float, C.c_float], _U32)
     fn("iac_ac1d_sparse_batch", [_VP, _VP, _VP, _U32, C.c_float, C.c_float, C.c_int, D, _VP, _VP])
     fn("iac_crystal_emitters", [_VP, _VP, _U32, _U32, _U32, C.POINTER(CrystalParams), _U64, _VP,
@@ -316,10 +316,9 @@ class Context:
         check(lib().iac_cq_merge(self._h, _ptr(d_small), _ptr(d_rw), int(nframes), C.byref(shape),
                                  int(interp), float(mult), _ptr(d_big), _ptr(stream)))
 
-    def ac1d_cq(self, d_I, d_kmap, npix, shape, interp, mult, d_hist, stream=None, fast_size=0):
-        check(lib().iac_ac1d_cq(self._h, _ptr(d_I), _ptr(d_kmap), int(npix), int(fast_size),
-                                C.byref(shape), int(interp), float(mult), _ptr(d_hist),
-                                _ptr(stream)))
+    def ac1d_cq(self, d_I, d_kmap, npix, shape, interp, mult, d_hist, stream=None):
+        check(lib().iac_ac1d_cq(self._h, _ptr(d_I), _ptr(d_kmap), int(npix), C.byref(shape),
+                                int(interp), float(mult), _ptr(d_hist), _ptr(stream)))
 
     def ac1d_sparse_batch(self, d_photons, d_offsets, nframes, max_q, dqdx, interp, mult, d_hist,
                           stream=None):

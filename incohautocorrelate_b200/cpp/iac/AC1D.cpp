@@ -68,8 +68,7 @@ void AC1D::Calculate_CQ(Detector &Det, Settings &Options, Settings::Interpolatio
     Check(iac_memcpy_h2d(ctx, dI.p, Det.Intensity, n * 4, s), "copy intensity");
     Check(iac_memcpy_h2d(ctx, dK.p, Det.kMap, n * 12, s), "copy k-map");
     Check(iac_memset_device(ctx, dH.p, 0, 8 * (size_t)Shape.Size, s), "clear histogram");
-    Check(iac_ac1d_cq(ctx, (const float *)dI.p, (const float *)dK.p, n, Det.DetectorSize[1], &sh, Mode, mult,
-                      (uint64_t *)dH.p, s),
+    Check(iac_ac1d_cq(ctx, (const float *)dI.p, (const float *)dK.p, n, &sh, Mode, mult, (uint64_t *)dH.p, s),
           "iac_ac1d_cq");
     std::vector<uint64_t> h(Shape.Size);
     Check(iac_memcpy_d2h(ctx, h.data(), dH.p, 8 * h.size(), s), "copy histogram");

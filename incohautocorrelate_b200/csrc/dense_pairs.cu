@@ -518,8 +518,8 @@ iac_status iac_cq_small(iac_ctx *ctx, const float *d_I, const float *d_kmap, uin
 }
 
 iac_status iac_ac1d_cq(iac_ctx *ctx, const float *d_I, const float *d_kmap, uint64_t npix,
-                       uint32_t fast_size, const iac_ac1d_shape *sh, int interp, double mult,
-                       uint64_t *d_hist, void *stream)
+                       const iac_ac1d_shape *sh, int interp, double mult, uint64_t *d_hist,
+                       void *stream)
 {
     IAC_REQUIRE(ctx && d_I && d_kmap && sh && d_hist, "iac_ac1d_cq: NULL argument");
     IAC_REQUIRE(interp == 0 || interp == 1, "interpolation must be 0 or 1");
@@ -528,7 +528,9 @@ iac_status iac_ac1d_cq(iac_ctx *ctx, const float *d_I, const float *d_kmap, uint
     IAC_REQUIRE(mult > 0, "multiplicator must be positive");
     DeviceGuard g(ctx->device);
     DenseArgs a{};
-    iac_status st = prepare(ctx, stream, d_I, d_kmap, npix, fast_size, mult, a);
+    // linear tiles: the pixels of a 16 x 16 patch pair share few |q| bins, and
+    // a warp's shared-memory histogram atomics would collide on them
+    iac_status st = prepare(ctx, stream, d_I, d_kmap, npix, 0, mult, a);
     if (st != IAC_OK) return st;
     a.out = (unsigned long long *)d_hist;
     a.maxq = sh->max_q;

@@ -127,10 +127,9 @@ def test_gpu_dense_fixtures(ctx, oracle_lib):
         np.testing.assert_array_equal(big.cpu().numpy().view(np.uint64), g[f"merge_{interp}"])
     sh = capi.ac1d_shape(g["max_q"], 97)
     for interp in (0, 1):
-        for fast in (0, 22):
-            h = torch.zeros(sh.size, dtype=torch.int64, device="cuda")
-            ctx.ac1d_cq(_dev(I), _dev(km), I.size, sh, interp, float(g["ac1d_mult"]), h, fast_size=fast)
-            np.testing.assert_array_equal(h.cpu().numpy().view(np.uint64), g[f"ac1d_cq_{interp}"])
+        h = torch.zeros(sh.size, dtype=torch.int64, device="cuda")
+        ctx.ac1d_cq(_dev(I), _dev(km), I.size, sh, interp, float(g["ac1d_mult"]), h)
+        np.testing.assert_array_equal(h.cpu().numpy().view(np.uint64), g[f"ac1d_cq_{interp}"])
     assert ctx.check() == 0
 
 

@@ -125,9 +125,8 @@ def test_cq_merge_bit_exact(ctx, oracle_lib, rng, interp):
 
 
 @pytest.mark.parametrize("interp", [0, 1])
-@pytest.mark.parametrize("fast", [0, 48])
 @pytest.mark.parametrize("mult_of", ["reference", 1234.5])
-def test_ac1d_cq_bit_exact(ctx, oracle_lib, rng, interp, fast, mult_of):
+def test_ac1d_cq_bit_exact(ctx, oracle_lib, rng, interp, mult_of):
     from incohautocorrelate_b200 import capi
     o = oracle_lib
     pm, km, mq = small_detector(40, 48, 6e-4)
@@ -142,7 +141,7 @@ def test_ac1d_cq_bit_exact(ctx, oracle_lib, rng, interp, fast, mult_of):
     want = np.zeros(sh.size, np.uint64)
     o.lib().iaco_ac1d_cq(o.p(I), o.p(km), npix, sh_o, interp, mult, 0, npix, o.p(want))
     out = _zeros(sh.size)
-    ctx.ac1d_cq(_dev(I), _dev(km), npix, sh, interp, mult, out, fast_size=fast)
+    ctx.ac1d_cq(_dev(I), _dev(km), npix, sh, interp, mult, out)
     assert ctx.check() == 0
     np.testing.assert_array_equal(_u64(out), want)
 
