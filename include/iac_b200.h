@@ -339,6 +339,87 @@ iac_status iac_sparsify_frames(iac_ctx *ctx, const float *d_intensity, const int
                                void *stream);
 
 /* ---------------------------------------------------------------------- */
+/* mesh denoiser -- no counterpart in the reference                          */
+/* ---------------------------------------------------------------------- */
+
+/* A 3-level 3D U-Net (channels 16/32/64, 3x3x3 convolutions, average
+ * pooling, nearest upsampling + skip concatenation, residual 1x1 head) that
+ * maps a few-frame pair mesh to an estimate of its many-frame mean.  Volumes
+ * are fp32 [nb][D][H][W] on the device, D, H, W multiples of 4.  Forward and
+ * backward run on hand-written BF16 implicit-GEMM tensor-core kernels with
+ * FP32 accumulation; parameters are fp32 (one flat array, per 3x3x3 layer
+ * W[cout][27][cin] then b[cout]; head w[16], b) updated by AdamW. */
+typedef struct iac_denoiser iac_denoiser;
+
+typedef struct iac_adamw {
+    float lr, beta1, beta2, eps, weight_decay;
+} iac_adamw;
+
+/* number of fp32 parameters */
+uint64_t iac_denoise_param_count(void);
+
+/* Workspace for up to max_batch volumes of D x H x W.  backend 0 runs the
+ * convolutions on tcgen05.mma with TMEM accumulators, 1 on mma.sync. */
+iac_status iac_denoise_create(iac_ctx *ctx, uint32_t max_batch, uint32_t D, uint32_t H, uint32_t W,
+                              int backend, iac_denoiser **out);
+void iac_denoise_destroy(iac_denoiser *dn);
+
+/* He-normal weights, zero biases and head (identity network); resets AdamW. */
+iac_status iac_denoise_init_params(iac_denoiser *dn, uint64_t seed);
+/* host fp32 arrays of iac_denoise_param_count() values; set resets AdamW.
+ * Synchronous. */
+iac_status iac_denoise_set_params(iac_denoiser *dn, const float *h_params);
+iac_status iac_denoise_get_params(iac_denoiser *dn, float *h_params);
+iac_status iac_denoise_get_grads(iac_denoiser *dn, float *h_grads);
+
+/* d_out = network(d_in).  Asynchronous on `stream`. */
+iac_status iac_denoise_forward(iac_denoiser *dn, const float *d_in, uint32_t nb, uint32_t D, uint32_t H,
+                               uint32_t W, float *d_out, void *stream);
+
+/* Forward, loss = mean(weight * (out - target)^2) (weight may be null), and
+ * the parameter gradients (read with iac_denoise_get_grads).  d_out may be
+ * null.  When h_loss is given the call synchronizes `stream` and stores the
+ * loss there. */
+iac_status iac_denoise_backward(iac_denoiser *dn, const float *d_in, const float *d_target,
+                                const float *d_weight, uint32_t nb, uint32_t D, uint32_t H, uint32_t W,
+                                float *d_out, double *h_loss, void *stream);
+
+/* One AdamW step on the gradients of the last backward.  Asynchronous. */
+iac_status iac_denoise_adamw_step(iac_denoiser *dn, const iac_adamw *opt, void *stream);
+
+/* One 3x3x3 convolution layer (stride 1, zero padding 1) on bf16 NDHWC
+ * tensors: y = [relu](conv(concat(up0 ? upsample2(src0) : src0, src1)) + bias).
+ * src0 (c0 channels, may be absent with c0 = 0) is at half resolution when
+ * up0; src1 (c1 channels) and y (cout) are nb x D x H x W.  d_wtile holds the
+ * weights W[co][tap][ci] as bf16 tiles [tap][ci/8][co][8] (tap = 9 (dz+1) +
+ * 3 (dy+1) + dx+1).  The (cin, cout) pairs of the network are supported.
+ * Asynchronous. */
+iac_status iac_denoise_conv3x3(iac_ctx *ctx, int backend, const uint16_t *d_src0, uint32_t c0, int up0,
+                               const uint16_t *d_src1, uint32_t c1, const uint16_t *d_wtile,
+                               const float *d_bias, uint32_t cout, int relu, uint32_t nb, uint32_t D,
+                               uint32_t H, uint32_t W, uint16_t *d_y, void *stream);
+
+/* Weight gradient of that layer: d_dw[co][tap][ci] += sum_v grad[v][co] X[v + off(tap)][ci]
+ * and d_db[co] += sum_v grad[v][co] (fp32, accumulated).  Asynchronous. */
+iac_status iac_denoise_wgrad3x3(iac_ctx *ctx, const uint16_t *d_src0, uint32_t c0, int up0,
+                                const uint16_t *d_src1, uint32_t c1, const uint16_t *d_grad,
+                                uint32_t cout, uint32_t nb, uint32_t D, uint32_t H, uint32_t W,
+                                float *d_dw, float *d_db, void *stream);
+
+/* Network input from a folded S^3 uint64 mesh: its leading E^3 corner times
+ * `scale`, as fp32 (d_f32) and/or bf16 bits (d_bf16).  Asynchronous. */
+iac_status iac_denoise_mesh_input(iac_ctx *ctx, const uint64_t *d_full, uint32_t S, uint32_t E,
+                                  double scale, float *d_f32, uint16_t *d_bf16, void *stream);
+
+/* Training patches: plan (int32 x 5 per patch: mesh index, z0, y0, x0,
+ * transform 0..47 = axis permutation + 6 x reflection bits) cuts P^3 fp32
+ * patches from nmeshes E^3 bf16 meshes.  Plan entries reaching outside the
+ * meshes give zeros and count as out-of-mesh (iac_ctx_check).  Asynchronous. */
+iac_status iac_denoise_crop_patches(iac_ctx *ctx, const uint16_t *d_meshes, uint32_t nmeshes, uint32_t E,
+                                    const int32_t *d_plan, uint32_t nb, uint32_t P, float *d_out,
+                                    void *stream);
+
+/* ---------------------------------------------------------------------- */
 /* micro-benchmarks (roofline denominators)                                 */
 /* ---------------------------------------------------------------------- */
 

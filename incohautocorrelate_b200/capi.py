@@ -75,6 +75,11 @@ class PhotonParams(C.Structure):
                 ("adu_noise", C.c_float), ("value_per_photon", C.c_float)]
 
 
+class AdamW(C.Structure):
+    _fields_ = [("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float),
+                ("eps", C.c_float), ("weight_decay", C.c_float)]
+
+
 # Philox stream tags of csrc/rng.cuh
 RNG_POISSON = 0x01 << 56
 RNG_ROTATION = 0x02 << 56
@@ -132,6 +137,23 @@ def _declare(lib):
     fn("iac_simulate_photons", [_VP, _VP, _U64, _U32, _U64, C.POINTER(PhotonParams), _U64, _VP])
     fn("iac_sparsify_frames", [_VP, _VP, _VP, _VP, _U64, _U32, C.c_float, C.c_float, C.c_int,
                                _VP, _U64, _VP, C.POINTER(_U64), _VP])
+    fn("iac_denoise_param_count", [], _U64)
+    fn("iac_denoise_create", [_VP, _U32, _U32, _U32, _U32, C.c_int, C.POINTER(_VP)])
+    fn("iac_denoise_destroy", [_VP], None)
+    fn("iac_denoise_init_params", [_VP, _U64])
+    fn("iac_denoise_set_params", [_VP, _VP])
+    fn("iac_denoise_get_params", [_VP, _VP])
+    fn("iac_denoise_get_grads", [_VP, _VP])
+    fn("iac_denoise_forward", [_VP, _VP, _U32, _U32, _U32, _U32, _VP, _VP])
+    fn("iac_denoise_backward", [_VP, _VP, _VP, _VP, _U32, _U32, _U32, _U32, _VP,
+                                C.POINTER(C.c_double), _VP])
+    fn("iac_denoise_adamw_step", [_VP, C.POINTER(AdamW), _VP])
+    fn("iac_denoise_conv3x3", [_VP, C.c_int, _VP, _U32, C.c_int, _VP, _U32, _VP, _VP, _U32, C.c_int,
+                               _U32, _U32, _U32, _U32, _VP, _VP])
+    fn("iac_denoise_wgrad3x3", [_VP, _VP, _U32, C.c_int, _VP, _U32, _VP, _U32, _U32, _U32, _U32,
+                                _U32, _VP, _VP, _VP])
+    fn("iac_denoise_mesh_input", [_VP, _VP, _U32, _U32, D, _VP, _VP, _VP])
+    fn("iac_denoise_crop_patches", [_VP, _VP, _U32, _U32, _VP, _U32, _U32, _VP, _VP])
     return lib
 
 
@@ -357,3 +379,115 @@ class Context:
     def bench_scatter_add(self, d_buf, words, word_bits, updates, seed=1, stream=None):
         check(lib().iac_bench_scatter_add(self._h, _ptr(d_buf), int(words), int(word_bits),
                                           int(updates), int(seed), _ptr(stream)))
+
+
+# --------------------------------------------------------------------------
+# mesh denoiser
+# --------------------------------------------------------------------------
+TCGEN05 = 0
+MMA_SYNC = 1
+
+
+def denoise_param_count() -> int:
+    return int(lib().iac_denoise_param_count())
+
+
+class Denoiser:
+    """Owns an iac_denoiser workspace (a 3-level 3D U-Net) on `ctx`'s device."""
+
+    def __init__(self, ctx, max_batch, D, H, W, backend=TCGEN05):
+        self.ctx = ctx
+        h = _VP()
+        check(lib().iac_denoise_create(ctx._h, int(max_batch), int(D), int(H), int(W), int(backend),
+                                       C.byref(h)))
+        self._h = h
+        self.nparams = denoise_param_count()
+
+    def close(self):
+        if self._h:
+            lib().iac_denoise_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init_params(self, seed=0):
+        check(lib().iac_denoise_init_params(self._h, int(seed)))
+
+    def set_params(self, params):
+        import numpy as np
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        assert p.size == self.nparams
+        check(lib().iac_denoise_set_params(self._h, p.ctypes.data))
+
+    def get_params(self):
+        import numpy as np
+        p = np.zeros(self.nparams, np.float32)
+        check(lib().iac_denoise_get_params(self._h, p.ctypes.data))
+        return p
+
+    def get_grads(self):
+        import numpy as np
+        g = np.zeros(self.nparams, np.float32)
+        check(lib().iac_denoise_get_grads(self._h, g.ctypes.data))
+        return g
+
+    def forward(self, d_in, nb, D, H, W, d_out, stream=None):
+        check(lib().iac_denoise_forward(self._h, _ptr(d_in), int(nb), int(D), int(H), int(W),
+                                        _ptr(d_out), _ptr(stream)))
+
+    def backward(self, d_in, d_target, nb, D, H, W, d_weight=None, d_out=None, stream=None,
+                 want_loss=True):
+        loss = C.c_double(0.0)
+        check(lib().iac_denoise_backward(self._h, _ptr(d_in), _ptr(d_target), _ptr(d_weight),
+                                         int(nb), int(D), int(H), int(W), _ptr(d_out),
+                                         C.byref(loss) if want_loss else None, _ptr(stream)))
+        return loss.value if want_loss else None
+
+    def adamw_step(self, lr, beta1=0.9, beta2=0.999, eps=1e-8, weight_decay=1e-4, stream=None):
+        opt = AdamW(lr, beta1, beta2, eps, weight_decay)
+        check(lib().iac_denoise_adamw_step(self._h, C.byref(opt), _ptr(stream)))
+
+
+def denoise_mesh_input(ctx, d_full, S, E, scale, d_f32=None, d_bf16=None, stream=None):
+    check(lib().iac_denoise_mesh_input(ctx._h, _ptr(d_full), int(S), int(E), float(scale),
+                                       _ptr(d_f32), _ptr(d_bf16), _ptr(stream)))
+
+
+def denoise_crop_patches(ctx, d_meshes, nmeshes, E, d_plan, nb, P, d_out, stream=None):
+    check(lib().iac_denoise_crop_patches(ctx._h, _ptr(d_meshes), int(nmeshes), int(E), _ptr(d_plan),
+                                         int(nb), int(P), _ptr(d_out), _ptr(stream)))
+
+
+def denoise_conv3x3(ctx, backend, d_src0, c0, up0, d_src1, c1, d_wtile, d_bias, cout, relu, nb, D, H,
+                    W, d_y, stream=None):
+    check(lib().iac_denoise_conv3x3(ctx._h, int(backend), _ptr(d_src0), int(c0), int(up0),
+                                    _ptr(d_src1), int(c1), _ptr(d_wtile), _ptr(d_bias), int(cout),
+                                    int(relu), int(nb), int(D), int(H), int(W), _ptr(d_y),
+                                    _ptr(stream)))
+
+
+def denoise_wgrad3x3(ctx, d_src0, c0, up0, d_src1, c1, d_grad, cout, nb, D, H, W, d_dw, d_db=None,
+                     stream=None):
+    check(lib().iac_denoise_wgrad3x3(ctx._h, _ptr(d_src0), int(c0), int(up0), _ptr(d_src1), int(c1),
+                                     _ptr(d_grad), int(cout), int(nb), int(D), int(H), int(W),
+                                     _ptr(d_dw), _ptr(d_db), _ptr(stream)))
+
+
+def conv_weight_tiles(w):
+    """W[cout][27][cin] (any float array) -> bf16-ready tile order [27][cin/8][cout][8]."""
+    import numpy as np
+    cout, taps, cin = w.shape
+    return np.ascontiguousarray(w.reshape(cout, taps, cin // 8, 8).transpose(1, 2, 0, 3))
+
+
+def dgrad_weight_tiles(w):
+    """Tiles of the data-gradient layer: Wd(tap)[ci][co] = W[co][26 - tap][ci], as
+    [27][cout/8][cin][8]."""
+    import numpy as np
+    cout, taps, cin = w.shape
+    wt = w[:, ::-1, :].transpose(2, 1, 0)  # [cin][tap'][cout]
+    return conv_weight_tiles(np.ascontiguousarray(wt))

@@ -1,0 +1,1079 @@
+// denoise_kernels.cu -- kernels of the mesh denoiser (no reference
+// counterpart): 3x3x3 convolutions as implicit GEMM on the BF16 tensor cores
+// with FP32 accumulation, their data and weight gradients, pooling, the
+// residual 1x1 head fused with the MSE loss, AdamW, and patch extraction.
+//
+// Implicit GEMM.  A CTA owns TILE_M = 128 consecutive voxels (GEMM rows) and
+// all output channels (GEMM N = cout).  The K loop runs over the 27 taps; one
+// pipeline stage holds one tap: the 128 shifted input rows x cin channels (A)
+// and the tap's cout x cin weights (B).  Rows are gathered with 16-byte
+// cp.async, out-of-volume neighbours zero-filled by the copy itself; the
+// channel concatenation and the nearest 2x upsampling of the decoder inputs
+// are folded into the gather, so neither is materialised.
+//
+// Shared-memory layout of a stage operand: [k-chunk][row][8 channels], one
+// 16-byte row segment per (row, k-chunk).  Eight consecutive rows of one
+// chunk form a contiguous 128-byte "core matrix", which is the canonical
+// K-major, non-swizzled operand layout of tcgen05.mma (stride between 8-row
+// groups = 128 B, stride between the two k-chunks of a K=16 step = rows*16 B)
+// and a bank-conflict-free ldmatrix source for mma.sync.
+//
+// Two backends compute the same GEMM:
+//   backend 0, tcgen05: one thread issues tcgen05.mma (M=128, N=cout, K=16)
+//     into a TMEM accumulator; each stage's MMAs commit to an mbarrier that
+//     releases the stage for the next cp.async; the epilogue reads TMEM with
+//     tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = its 32 voxels);
+//   backend 1, mma.sync.m16n8k16: four warps of 32 voxels x cout each.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+#include "denoise_internal.cuh"
+
+namespace iac {
+namespace dn {
+
+// --------------------------------------------------------------------------
+// PTX helpers
+// --------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32_t bytes)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+__device__ __forceinline__ void fence_proxy_async()
+{
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(addr), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait: false after ~2^20 polls (each try_wait itself suspends for a
+// bounded time), so a lost arrival ends the kernel with an error instead of
+// hanging the GPU
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity)
+{
+    for (uint32_t i = 0; i < (1u << 20); i++)
+        if (mbar_try_wait(addr, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tc_fence_before()
+{
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after()
+{
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols)
+{
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(dst_smem),
+                 "r"(ncols)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish()
+{
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(ncols)
+                 : "memory");
+}
+// D[tmem] (+)= A[smem] * B[smem]^T, kind::f16 (bf16 inputs, fp32 accumulator)
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint32_t mbar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mbar)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+        "[%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+          "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+
+// shared-memory matrix descriptor: K-major, no swizzle; lbo = byte stride
+// between the two 8-element k-chunks of a K=16 step, sbo = byte stride between
+// 8-row groups; bits 46-47 = 1 (descriptor version of sm_100)
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+    return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// instruction descriptor, kind::f16: D fp32 (bits 4-5 = 1), A and B bf16
+// (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3)
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(addr));
+}
+__device__ __forceinline__ void ldsm_x4_t(uint32_t addr, uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3)
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(addr));
+}
+__device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b)
+{
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t *>(&h);
+}
+
+// --------------------------------------------------------------------------
+// voxel decomposition and the shared gather of shifted input rows
+// --------------------------------------------------------------------------
+struct Vox {
+    int n, z, y, x;
+    bool ok;
+};
+__device__ __forceinline__ Vox decode(long long v, int D, int H, int W, long long V)
+{
+    Vox q;
+    q.ok = v < V;
+    if (!q.ok) v = 0;
+    q.x = (int)(v % W);
+    long long r = v / W;
+    q.y = (int)(r % H);
+    r /= H;
+    q.z = (int)(r % D);
+    q.n = (int)(r / D);
+    return q;
+}
+
+// rows of X (concat of upsampled src0 and src1) shifted by tap, into the
+// stage operand at sA ([cin/8][TILE_M][16 B]); zero-filled outside the volume
+template <int CIN>
+__device__ __forceinline__ void gather_rows(uint32_t sA, const bf16 *src0, const bf16 *src1, int c0, int c1,
+                                            int up0, int D, int H, int W, const Vox &q, int row, int tap)
+{
+    const int z = q.z + tap / 9 - 1, y = q.y + (tap / 3) % 3 - 1, x = q.x + tap % 3 - 1;
+    const bool ok = q.ok && (unsigned)z < (unsigned)D && (unsigned)y < (unsigned)H && (unsigned)x < (unsigned)W;
+    const int n0 = c0 >> 3;
+    const bf16 *p0 = src0, *p1 = src1;
+    if (ok) {
+        if (c0) {
+            if (up0)
+                p0 = src0 + ((((long long)q.n * (D >> 1) + (z >> 1)) * (H >> 1) + (y >> 1)) * (W >> 1) + (x >> 1)) * c0;
+            else
+                p0 = src0 + ((((long long)q.n * D + z) * H + y) * W + x) * c0;
+        }
+        if (c1) p1 = src1 + ((((long long)q.n * D + z) * H + y) * W + x) * c1;
+    }
+    const uint32_t bytes = ok ? 16u : 0u;
+#pragma unroll
+    for (int c = 0; c < CIN / 8; c++) {
+        const bf16 *src = c < n0 ? p0 + c * 8 : p1 + (c - n0) * 8;
+        cp_async16(sA + (uint32_t)((c * TILE_M + row) * 16), src, bytes);
+    }
+}
+
+template <int CIN, int COUT>
+__device__ __forceinline__ void load_weights(uint32_t sB, const bf16 *w, int tap, int tid)
+{
+    const bf16 *src = w + (size_t)tap * CIN * COUT;
+    for (int i = tid; i < COUT * CIN / 8; i += CONV_THREADS) cp_async16(sB + i * 16, src + i * 8, 16);
+}
+
+// epilogue for one output row segment of 8 channels: bias, ReLU, bf16 (+fp32)
+__device__ __forceinline__ void store8(const ConvArgs &a, int cout, long long v, int c, const float *val)
+{
+    float o[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        float t = val[j] + (a.bias ? a.bias[c + j] : 0.0f);
+        o[j] = a.relu ? fmaxf(t, 0.0f) : t;
+    }
+    uint4 pk;
+    pk.x = pack_bf16(o[0], o[1]);
+    pk.y = pack_bf16(o[2], o[3]);
+    pk.z = pack_bf16(o[4], o[5]);
+    pk.w = pack_bf16(o[6], o[7]);
+    *reinterpret_cast<uint4 *>(a.y + v * cout + c) = pk;
+    if (a.y32) {
+        float4 *d = reinterpret_cast<float4 *>(a.y32 + v * cout + c);
+        d[0] = make_float4(o[0], o[1], o[2], o[3]);
+        d[1] = make_float4(o[4], o[5], o[6], o[7]);
+    }
+}
+
+// --------------------------------------------------------------------------
+// backend 0: tcgen05.mma with a TMEM accumulator
+// --------------------------------------------------------------------------
+template <int CIN, int COUT>
+struct TcCfg {
+    static constexpr int S = 4;   // stages
+    static constexpr int PF = 2;  // taps in flight ahead of the one being multiplied
+    static constexpr uint32_t A_BYTES = TILE_M * CIN * 2;
+    static constexpr uint32_t B_BYTES = COUT * CIN * 2;
+    static constexpr uint32_t STAGE = A_BYTES + B_BYTES;
+    static constexpr uint32_t SMEM = S * STAGE;
+    static constexpr uint32_t TCOLS = COUT <= 32 ? 32 : (COUT <= 64 ? 64 : 128);
+};
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(CONV_THREADS) conv_tc_kernel(const ConvArgs a)
+{
+    using Cfg = TcCfg<CIN, COUT>;
+    static_assert(COUT % 16 == 0 && COUT <= 256 && CIN % 16 == 0, "tcgen05 M=128 needs N % 16 == 0");
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar[Cfg::S];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_err;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const long long v0 = (long long)blockIdx.x * TILE_M;
+    const Vox q = decode(v0 + tid, a.D, a.H, a.W, a.V);
+    const uint32_t sbase = smem_u32(smem);
+    if (tid == 0) {
+        for (int s = 0; s < Cfg::S; s++) mbar_init(smem_u32(&mbar[s]), 1);
+        fence_mbar_init();
+        s_err = 0;
+    }
+    if (warp == 0) {
+        tmem_alloc(smem_u32(&s_tmem), Cfg::TCOLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    constexpr uint32_t IDESC = idesc_bf16(TILE_M, COUT);
+
+    for (int t = 0; t < Cfg::PF; t++) {
+        const uint32_t sA = sbase + t * Cfg::STAGE;
+        gather_rows<CIN>(sA, a.src0, a.src1, a.c0, a.c1, a.up0, a.D, a.H, a.W, q, tid, t);
+        load_weights<CIN, COUT>(sA + Cfg::A_BYTES, a.w, t, tid);
+        cp_async_commit();
+    }
+    int issued = 0;  // taps whose MMAs were issued
+    for (int t = 0; t < 27; t++) {
+        const int tn = t + Cfg::PF;
+        if (tn < 27) {
+            const int st = tn % Cfg::S;
+            // the stage was last read by the MMAs of tap tn - S
+            if (tn >= Cfg::S && !mbar_wait(smem_u32(&mbar[st]), ((tn - Cfg::S) / Cfg::S) & 1)) s_err = 1;
+            const uint32_t sA = sbase + st * Cfg::STAGE;
+            gather_rows<CIN>(sA, a.src0, a.src1, a.c0, a.c1, a.up0, a.D, a.H, a.W, q, tid, tn);
+            load_weights<CIN, COUT>(sA + Cfg::A_BYTES, a.w, tn, tid);
+        }
+        cp_async_commit();
+        cp_async_wait<Cfg::PF>();
+        fence_proxy_async();
+        __syncthreads();
+        if (s_err) break;
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t sA = sbase + (t % Cfg::S) * Cfg::STAGE, sB = sA + Cfg::A_BYTES;
+#pragma unroll
+            for (int k = 0; k < CIN / 16; k++) {
+                const uint64_t da = smem_desc(sA + k * 2 * (TILE_M * 16), TILE_M * 16, 128);
+                const uint64_t db = smem_desc(sB + k * 2 * (COUT * 16), COUT * 16, 128);
+                umma_bf16(tmem, da, db, IDESC, (t > 0 || k > 0) ? 1u : 0u);
+            }
+            umma_commit(smem_u32(&mbar[t % Cfg::S]));
+        }
+        issued = t + 1;
+    }
+    cp_async_wait_all();
+    // the last commit arrives once every MMA issued before it has completed
+    const bool done =
+        issued > 0 && mbar_wait(smem_u32(&mbar[(issued - 1) % Cfg::S]), ((issued - 1) / Cfg::S) & 1);
+    if ((s_err || !done) && tid == 0 && a.counters) atomicAdd(&a.counters->timeouts, 1ull);
+    tc_fence_after();
+    __syncthreads();
+    if (!s_err && done && issued == 27) {  // CTA-uniform: the TMEM loads are warp-collective
+        const long long v = v0 + tid;
+#pragma unroll
+        for (int c = 0; c < COUT; c += 16) {
+            uint32_t r[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c, r);
+            tmem_wait_ld();
+            if (q.ok) {
+                float f[16];
+#pragma unroll
+                for (int j = 0; j < 16; j++) f[j] = __uint_as_float(r[j]);
+                store8(a, COUT, v, c, f);
+                store8(a, COUT, v, c + 8, f + 8);
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, Cfg::TCOLS);
+}
+
+// --------------------------------------------------------------------------
+// backend 1: mma.sync.m16n8k16 (warp w: rows 32w..32w+31, all cout)
+// --------------------------------------------------------------------------
+template <int CIN, int COUT>
+struct MmaCfg {
+    static constexpr int S = 3;
+    static constexpr int PF = S - 1;
+    static constexpr uint32_t A_BYTES = TILE_M * CIN * 2;
+    static constexpr uint32_t B_BYTES = COUT * CIN * 2;
+    static constexpr uint32_t STAGE = A_BYTES + B_BYTES;
+    static constexpr uint32_t SMEM = S * STAGE;
+};
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(CONV_THREADS) conv_mma_kernel(const ConvArgs a)
+{
+    using Cfg = MmaCfg<CIN, COUT>;
+    constexpr int NT = COUT / 8;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const long long v0 = (long long)blockIdx.x * TILE_M;
+    const Vox q = decode(v0 + tid, a.D, a.H, a.W, a.V);
+    const uint32_t sbase = smem_u32(smem);
+    float acc[2][NT][4];
+#pragma unroll
+    for (int m = 0; m < 2; m++)
+#pragma unroll
+        for (int n = 0; n < NT; n++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) acc[m][n][j] = 0.0f;
+
+    for (int t = 0; t < Cfg::PF; t++) {
+        const uint32_t sA = sbase + t * Cfg::STAGE;
+        gather_rows<CIN>(sA, a.src0, a.src1, a.c0, a.c1, a.up0, a.D, a.H, a.W, q, tid, t);
+        load_weights<CIN, COUT>(sA + Cfg::A_BYTES, a.w, t, tid);
+        cp_async_commit();
+    }
+    for (int t = 0; t < 27; t++) {
+        const int tn = t + Cfg::PF;
+        if (tn < 27) {
+            __syncthreads();  // every warp is done with tap t - 1, whose stage is reused
+            const uint32_t sA = sbase + (tn % Cfg::S) * Cfg::STAGE;
+            gather_rows<CIN>(sA, a.src0, a.src1, a.c0, a.c1, a.up0, a.D, a.H, a.W, q, tid, tn);
+            load_weights<CIN, COUT>(sA + Cfg::A_BYTES, a.w, tn, tid);
+        }
+        cp_async_commit();
+        cp_async_wait<Cfg::PF>();
+        __syncthreads();
+        const uint32_t sA = sbase + (t % Cfg::S) * Cfg::STAGE, sB = sA + Cfg::A_BYTES;
+#pragma unroll
+        for (int k = 0; k < CIN / 16; k++) {
+            uint32_t af[2][4];
+#pragma unroll
+            for (int m = 0; m < 2; m++) {
+                const int row = warp * 32 + m * 16 + (lane & 15);
+                const int ch = 2 * k + (lane >> 4);
+                ldsm_x4(sA + (uint32_t)((ch * TILE_M + row) * 16), af[m][0], af[m][1], af[m][2], af[m][3]);
+            }
+#pragma unroll
+            for (int n2 = 0; n2 < NT / 2; n2++) {
+                uint32_t b0, b1, b2, b3;
+                const int nrow = n2 * 16 + (lane & 7) + ((lane >> 4) << 3);
+                const int ch = 2 * k + ((lane >> 3) & 1);
+                ldsm_x4(sB + (uint32_t)((ch * COUT + nrow) * 16), b0, b1, b2, b3);
+#pragma unroll
+                for (int m = 0; m < 2; m++) {
+                    mma_bf16(acc[m][2 * n2], af[m][0], af[m][1], af[m][2], af[m][3], b0, b1);
+                    mma_bf16(acc[m][2 * n2 + 1], af[m][0], af[m][1], af[m][2], af[m][3], b2, b3);
+                }
+            }
+        }
+    }
+    cp_async_wait_all();
+    // epilogue: thread holds rows g, g+8 of each m16 tile, columns 2t, 2t+1 of each n8 tile
+    const int g = lane >> 2, tq = lane & 3;
+#pragma unroll
+    for (int m = 0; m < 2; m++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const long long v = v0 + warp * 32 + m * 16 + g + 8 * h;
+            if (v >= a.V) continue;
+#pragma unroll
+            for (int n = 0; n < NT; n++) {
+                const int c = n * 8 + 2 * tq;
+                float o0 = acc[m][n][2 * h] + (a.bias ? a.bias[c] : 0.0f);
+                float o1 = acc[m][n][2 * h + 1] + (a.bias ? a.bias[c + 1] : 0.0f);
+                if (a.relu) {
+                    o0 = fmaxf(o0, 0.0f);
+                    o1 = fmaxf(o1, 0.0f);
+                }
+                *reinterpret_cast<uint32_t *>(a.y + v * COUT + c) = pack_bf16(o0, o1);
+                if (a.y32) *reinterpret_cast<float2 *>(a.y32 + v * COUT + c) = make_float2(o0, o1);
+            }
+        }
+}
+
+template <int CIN, int COUT>
+static cudaError_t launch_conv(const ConvArgs &a, int backend, cudaStream_t s)
+{
+    const unsigned grid = (unsigned)((a.V + TILE_M - 1) / TILE_M);
+    if (backend == 0) {
+        const uint32_t smem = TcCfg<CIN, COUT>::SMEM;
+        cudaError_t e = cudaFuncSetAttribute(conv_tc_kernel<CIN, COUT>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        conv_tc_kernel<CIN, COUT><<<grid, CONV_THREADS, smem, s>>>(a);
+    } else {
+        const uint32_t smem = MmaCfg<CIN, COUT>::SMEM;
+        cudaError_t e = cudaFuncSetAttribute(conv_mma_kernel<CIN, COUT>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        conv_mma_kernel<CIN, COUT><<<grid, CONV_THREADS, smem, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t conv3x3(const ConvArgs &a, int cin, int cout, int backend, cudaStream_t s)
+{
+#define IAC_CONV_CASE(CI, CO) \
+    if (cin == CI && cout == CO) return launch_conv<CI, CO>(a, backend, s);
+    IAC_CONV_CASE(16, 16)
+    IAC_CONV_CASE(16, 32)
+    IAC_CONV_CASE(32, 32)
+    IAC_CONV_CASE(32, 64)
+    IAC_CONV_CASE(64, 64)
+    IAC_CONV_CASE(96, 32)
+    IAC_CONV_CASE(48, 16)
+    IAC_CONV_CASE(32, 16)
+    IAC_CONV_CASE(64, 32)
+    IAC_CONV_CASE(32, 96)
+    IAC_CONV_CASE(16, 48)
+#undef IAC_CONV_CASE
+    return cudaErrorInvalidValue;
+}
+
+// --------------------------------------------------------------------------
+// first layer (1 input channel): 27 x 16 MACs per voxel on the FP32 pipe
+// --------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) conv_first_kernel(const float *__restrict__ x, const bf16 *__restrict__ w,
+                                                         const float *__restrict__ bias, bf16 *__restrict__ y,
+                                                         int D, int H, int W, long long V)
+{
+    __shared__ float ws[27][16];
+    __shared__ float bs[16];
+    for (int i = threadIdx.x; i < 27 * 16; i += blockDim.x) ws[i / 16][i % 16] = __bfloat162float(w[i]);
+    if (threadIdx.x < 16) bs[threadIdx.x] = bias[threadIdx.x];
+    __syncthreads();
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    const Vox q = decode(v, D, H, W, V);
+    float acc[16];
+#pragma unroll
+    for (int c = 0; c < 16; c++) acc[c] = bs[c];
+    for (int t = 0; t < 27; t++) {
+        const int z = q.z + t / 9 - 1, yy = q.y + (t / 3) % 3 - 1, xx = q.x + t % 3 - 1;
+        if ((unsigned)z >= (unsigned)D || (unsigned)yy >= (unsigned)H || (unsigned)xx >= (unsigned)W) continue;
+        const float xv = x[(((long long)q.n * D + z) * H + yy) * W + xx];
+#pragma unroll
+        for (int c = 0; c < 16; c++) acc[c] = fmaf(ws[t][c], xv, acc[c]);
+    }
+    uint4 pk[2];
+    uint32_t *u = reinterpret_cast<uint32_t *>(pk);
+#pragma unroll
+    for (int c = 0; c < 16; c += 2) u[c / 2] = pack_bf16(fmaxf(acc[c], 0.0f), fmaxf(acc[c + 1], 0.0f));
+    uint4 *dst = reinterpret_cast<uint4 *>(y + v * 16);
+    dst[0] = pk[0];
+    dst[1] = pk[1];
+}
+
+cudaError_t conv3x3_first(const float *x, const bf16 *w, const float *bias, bf16 *y, int D, int H, int W,
+                          long long V, cudaStream_t s)
+{
+    conv_first_kernel<<<(unsigned)((V + 255) / 256), 256, 0, s>>>(x, w, bias, y, D, H, W, V);
+    return cudaGetLastError();
+}
+
+// --------------------------------------------------------------------------
+// weight gradient: per tap, dW_tap[co][ci] = G^T X_tap over the voxels.
+// CTA = one tap x a strided set of 128-voxel blocks; operands are staged as in
+// the forward ([k-chunk][voxel][8]) and read with ldmatrix.trans, since here
+// the voxels are the GEMM K dimension.  Partial sums are reduced in shared
+// memory and added to dW with one fp32 atomic per element per CTA.
+// --------------------------------------------------------------------------
+template <int CIN, int COUT>
+struct WgCfg {
+    static constexpr int MT = COUT / 16, NT = CIN / 8;
+    static constexpr bool SPLIT_K = MT * NT <= 24;  // warps split voxels, else output tiles
+    static constexpr int TILES = SPLIT_K ? MT * NT : MT * NT / 4;
+    static constexpr uint32_t G_BYTES = TILE_M * COUT * 2;
+    static constexpr uint32_t X_BYTES = TILE_M * CIN * 2;
+    static constexpr uint32_t STAGE = G_BYTES + X_BYTES;
+    static constexpr int S = 2;
+    static constexpr uint32_t SMEM = S * STAGE + COUT * CIN * 4;
+};
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(CONV_THREADS) wgrad_kernel(const WgradArgs a)
+{
+    using Cfg = WgCfg<CIN, COUT>;
+    static_assert(Cfg::SPLIT_K || Cfg::NT % 8 == 0, "tile split: an even number of n tiles per warp");
+    extern __shared__ __align__(128) unsigned char smem[];
+    float *red = reinterpret_cast<float *>(smem + Cfg::S * Cfg::STAGE);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tap = blockIdx.y;
+    const long long nblk = (a.V + TILE_M - 1) / TILE_M;
+    const uint32_t sbase = smem_u32(smem);
+    for (int i = tid; i < COUT * CIN; i += CONV_THREADS) red[i] = 0.0f;
+
+    float acc[Cfg::TILES][4];
+#pragma unroll
+    for (int i = 0; i < Cfg::TILES; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = 0.0f;
+    float bsum = 0.0f;  // bias gradient (centre tap, thread co < COUT)
+
+    auto stage_load = [&](int st, long long b) {
+        const uint32_t sG = sbase + st * Cfg::STAGE, sX = sG + Cfg::G_BYTES;
+        const long long v = b * TILE_M + tid;
+        const Vox q = decode(v, a.D, a.H, a.W, a.V);
+        const bf16 *gp = a.g + (q.ok ? v : 0) * COUT;
+#pragma unroll
+        for (int c = 0; c < COUT / 8; c++)
+            cp_async16(sG + (uint32_t)((c * TILE_M + tid) * 16), gp + c * 8, q.ok ? 16u : 0u);
+        gather_rows<CIN>(sX, a.src0, a.src1, a.c0, a.c1, a.up0, a.D, a.H, a.W, q, tid, tap);
+    };
+
+    long long b = blockIdx.x;
+    if (b < nblk) stage_load(0, b);
+    cp_async_commit();
+    int st = 0;
+    for (; b < nblk; b += gridDim.x) {
+        const long long bn = b + gridDim.x;
+        if (bn < nblk) stage_load(st ^ 1, bn);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        const uint32_t sG = sbase + st * Cfg::STAGE, sX = sG + Cfg::G_BYTES;
+        if (tap == 13 && a.db && tid < COUT) {
+            const bf16 *gs = reinterpret_cast<const bf16 *>(smem + st * Cfg::STAGE);
+            for (int r = 0; r < TILE_M; r++) bsum += __bfloat162float(gs[((tid >> 3) * TILE_M + r) * 8 + (tid & 7)]);
+        }
+        if (Cfg::SPLIT_K) {
+            // warp w: voxels 32w..32w+31 (2 k16 steps), every (m, n) tile
+#pragma unroll
+            for (int ks = 0; ks < 2; ks++) {
+                const int kb = warp * 32 + ks * 16;
+#pragma unroll
+                for (int m = 0; m < Cfg::MT; m++) {
+                    uint32_t a0, a1, a2, a3;
+                    const int vr = kb + (lane & 7) + ((lane >> 4) << 3);
+                    const int ch = 2 * m + ((lane >> 3) & 1);
+                    ldsm_x4_t(sG + (uint32_t)((ch * TILE_M + vr) * 16), a0, a1, a2, a3);
+#pragma unroll
+                    for (int n2 = 0; n2 < Cfg::NT / 2; n2++) {
+                        uint32_t b0, b1, b2, b3;
+                        const int vx = kb + (lane & 7) + (((lane >> 3) & 1) << 3);
+                        const int cx = 2 * n2 + (lane >> 4);
+                        ldsm_x4_t(sX + (uint32_t)((cx * TILE_M + vx) * 16), b0, b1, b2, b3);
+                        mma_bf16(acc[m * Cfg::NT + 2 * n2], a0, a1, a2, a3, b0, b1);
+                        mma_bf16(acc[m * Cfg::NT + 2 * n2 + 1], a0, a1, a2, a3, b2, b3);
+                    }
+                }
+            }
+        } else {
+            // warp w: every voxel, n tiles [w*NT/4, (w+1)*NT/4) of every m tile
+            constexpr int NW = Cfg::NT / 4;
+#pragma unroll
+            for (int ks = 0; ks < TILE_M / 16; ks++) {
+                const int kb = ks * 16;
+#pragma unroll
+                for (int m = 0; m < Cfg::MT; m++) {
+                    uint32_t a0, a1, a2, a3;
+                    const int vr = kb + (lane & 7) + ((lane >> 4) << 3);
+                    const int ch = 2 * m + ((lane >> 3) & 1);
+                    ldsm_x4_t(sG + (uint32_t)((ch * TILE_M + vr) * 16), a0, a1, a2, a3);
+#pragma unroll
+                    for (int n2 = 0; n2 < NW / 2; n2++) {
+                        uint32_t b0, b1, b2, b3;
+                        const int vx = kb + (lane & 7) + (((lane >> 3) & 1) << 3);
+                        const int cx = warp * NW + 2 * n2 + (lane >> 4);
+                        ldsm_x4_t(sX + (uint32_t)((cx * TILE_M + vx) * 16), b0, b1, b2, b3);
+                        mma_bf16(acc[m * NW + 2 * n2], a0, a1, a2, a3, b0, b1);
+                        mma_bf16(acc[m * NW + 2 * n2 + 1], a0, a1, a2, a3, b2, b3);
+                    }
+                }
+            }
+        }
+        __syncthreads();  // the stage is refilled two blocks on
+        st ^= 1;
+    }
+    cp_async_wait_all();
+    // reduce: accumulator element j of tile (m, n): co = m*16 + g + 8*(j>>1), ci = n*8 + 2*tq + (j&1)
+    const int g = lane >> 2, tq = lane & 3;
+    constexpr int NW = Cfg::SPLIT_K ? Cfg::NT : Cfg::NT / 4;
+#pragma unroll
+    for (int i = 0; i < Cfg::TILES; i++) {
+        const int m = i / NW;
+        const int n = Cfg::SPLIT_K ? (i % NW) : warp * NW + (i % NW);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int co = m * 16 + g + 8 * (j >> 1), ci = n * 8 + 2 * tq + (j & 1);
+            atomicAdd(&red[co * CIN + ci], acc[i][j]);
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < COUT * CIN; i += CONV_THREADS) {
+        const int co = i / CIN, ci = i % CIN;
+        const float r = red[i];
+        if (r != 0.0f) atomicAdd(&a.dw[((size_t)co * 27 + tap) * CIN + ci], r);
+    }
+    if (tap == 13 && a.db && tid < COUT && bsum != 0.0f) atomicAdd(&a.db[tid], bsum);
+}
+
+template <int CIN, int COUT>
+static cudaError_t launch_wgrad(const WgradArgs &a, int sms, cudaStream_t s)
+{
+    using Cfg = WgCfg<CIN, COUT>;
+    const long long nblk = (a.V + TILE_M - 1) / TILE_M;
+    const int per_tap = (int)std::max<long long>(1, std::min<long long>(nblk, (4LL * sms + 26) / 27 * 2));
+    cudaError_t e = cudaFuncSetAttribute(wgrad_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)Cfg::SMEM);
+    if (e != cudaSuccess) return e;
+    wgrad_kernel<CIN, COUT><<<dim3(per_tap, 27), CONV_THREADS, Cfg::SMEM, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t wgrad3x3(const WgradArgs &a, int cin, int sms, cudaStream_t s)
+{
+#define IAC_WG_CASE(CI, CO) \
+    if (cin == CI && a.cout == CO) return launch_wgrad<CI, CO>(a, sms, s);
+    IAC_WG_CASE(16, 16)
+    IAC_WG_CASE(16, 32)
+    IAC_WG_CASE(32, 32)
+    IAC_WG_CASE(32, 64)
+    IAC_WG_CASE(64, 64)
+    IAC_WG_CASE(96, 32)
+    IAC_WG_CASE(48, 16)
+#undef IAC_WG_CASE
+    return cudaErrorInvalidValue;
+}
+
+// first layer: dW[co][tap] = sum_v G[v][co] x[v+off(tap)], 432 threads = (tap, co)
+__global__ void __launch_bounds__(448) wgrad_first_kernel(const float *__restrict__ x, const bf16 *__restrict__ g,
+                                                          float *__restrict__ dw, float *__restrict__ db, int D,
+                                                          int H, int W, long long V)
+{
+    __shared__ float gs[TILE_M][17];
+    __shared__ float xs[27][TILE_M];
+    const int tid = threadIdx.x;
+    const int co = tid % 16, tap = tid / 16;
+    float acc = 0.0f;
+    const long long nblk = (V + TILE_M - 1) / TILE_M;
+    for (long long b = blockIdx.x; b < nblk; b += gridDim.x) {
+        __syncthreads();
+        if (tid < TILE_M) {
+            const long long v = b * TILE_M + tid;
+            const Vox q = decode(v, D, H, W, V);
+            for (int t = 0; t < 27; t++) {
+                const int z = q.z + t / 9 - 1, yy = q.y + (t / 3) % 3 - 1, xx = q.x + t % 3 - 1;
+                const bool ok = q.ok && (unsigned)z < (unsigned)D && (unsigned)yy < (unsigned)H &&
+                                (unsigned)xx < (unsigned)W;
+                xs[t][tid] = ok ? x[(((long long)q.n * D + z) * H + yy) * W + xx] : 0.0f;
+            }
+            for (int c = 0; c < 16; c++) gs[tid][c] = q.ok ? __bfloat162float(g[v * 16 + c]) : 0.0f;
+        }
+        __syncthreads();
+        if (tid < 27 * 16) {
+            for (int r = 0; r < TILE_M; r++) acc = fmaf(gs[r][co], xs[tap][r], acc);
+        } else if (tid < 27 * 16 + 16) {
+            for (int r = 0; r < TILE_M; r++) acc += gs[r][tid - 27 * 16];
+        }
+    }
+    if (tid < 27 * 16) {
+        if (acc != 0.0f) atomicAdd(&dw[co * 27 + tap], acc);
+    } else if (tid < 27 * 16 + 16) {
+        if (acc != 0.0f) atomicAdd(&db[tid - 27 * 16], acc);
+    }
+}
+
+cudaError_t wgrad3x3_first(const float *x, const bf16 *g, float *dw, float *db, int D, int H, int W, long long V,
+                           int sms, cudaStream_t s)
+{
+    const long long nblk = (V + TILE_M - 1) / TILE_M;
+    const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(nblk, 2LL * sms));
+    wgrad_first_kernel<<<grid, 448, 0, s>>>(x, g, dw, db, D, H, W, V);
+    return cudaGetLastError();
+}
+
+// --------------------------------------------------------------------------
+// pooling, masks and the decoder's concat/upsample gradient
+// --------------------------------------------------------------------------
+__device__ __forceinline__ void load8(const bf16 *p, float *f)
+{
+    const uint4 u = *reinterpret_cast<const uint4 *>(p);
+    const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&u);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const float2 t = __bfloat1622float2(h[j]);
+        f[2 * j] = t.x;
+        f[2 * j + 1] = t.y;
+    }
+}
+__device__ __forceinline__ void store8b(bf16 *p, const float *f)
+{
+    uint4 u;
+    u.x = pack_bf16(f[0], f[1]);
+    u.y = pack_bf16(f[2], f[3]);
+    u.z = pack_bf16(f[4], f[5]);
+    u.w = pack_bf16(f[6], f[7]);
+    *reinterpret_cast<uint4 *>(p) = u;
+}
+
+// y (D/2 x H/2 x W/2) = mean of the 2x2x2 children; thread = (coarse voxel, 8 channels)
+__global__ void avgpool2_kernel(const bf16 *__restrict__ x, bf16 *__restrict__ y, int C, int D, int H, int W,
+                                long long total)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int nc = C / 8, c = (int)(i % nc) * 8;
+    const long long u = i / nc;
+    const int D2 = D / 2, H2 = H / 2, W2 = W / 2;
+    const Vox q = decode(u, D2, H2, W2, total / nc);
+    float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int k = 0; k < 8; k++) {
+        const long long v = (((long long)q.n * D + 2 * q.z + (k >> 2)) * H + 2 * q.y + ((k >> 1) & 1)) * W + 2 * q.x + (k & 1);
+        float f[8];
+        load8(x + v * C + c, f);
+#pragma unroll
+        for (int j = 0; j < 8; j++) s[j] += f[j];
+    }
+#pragma unroll
+    for (int j = 0; j < 8; j++) s[j] *= 0.125f;
+    store8b(y + u * C + c, s);
+}
+
+cudaError_t avgpool2(const bf16 *x, bf16 *y, int C, int D, int H, int W, int nb, cudaStream_t s)
+{
+    const long long total = (long long)nb * (D / 2) * (H / 2) * (W / 2) * (C / 8);
+    avgpool2_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(x, y, C, D, H, W, total);
+    return cudaGetLastError();
+}
+
+__global__ void relu_mask_kernel(const bf16 *__restrict__ g, const bf16 *__restrict__ y, bf16 *__restrict__ out,
+                                 long long n8)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n8) return;
+    float fg[8], fy[8];
+    load8(g + i * 8, fg);
+    load8(y + i * 8, fy);
+#pragma unroll
+    for (int j = 0; j < 8; j++) fg[j] = fy[j] > 0.0f ? fg[j] : 0.0f;
+    store8b(out + i * 8, fg);
+}
+
+cudaError_t relu_mask(const bf16 *g, const bf16 *y, bf16 *out, long long n, cudaStream_t s)
+{
+    const long long n8 = n / 8;
+    relu_mask_kernel<<<(unsigned)((n8 + 255) / 256), 256, 0, s>>>(g, y, out, n8);
+    return cudaGetLastError();
+}
+
+// gcat [V][c0 + c1] at full resolution: g0 (coarse, c0) = mask(y0) * sum of the
+// 8 children's first c0 channels (backward of nearest upsampling), g1 (full,
+// c1) = the last c1 channels (skip connection)
+__global__ void split_concat_kernel(const bf16 *__restrict__ gcat, int c0, int c1, const bf16 *__restrict__ y0,
+                                    bf16 *__restrict__ g0, bf16 *__restrict__ g1, int D, int H, int W,
+                                    long long n_coarse, long long n_full)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int C = c0 + c1;
+    if (i < n_coarse) {
+        const int nc = c0 / 8, c = (int)(i % nc) * 8;
+        const long long u = i / nc;
+        const Vox q = decode(u, D / 2, H / 2, W / 2, n_coarse / nc);
+        float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int k = 0; k < 8; k++) {
+            const long long v =
+                (((long long)q.n * D + 2 * q.z + (k >> 2)) * H + 2 * q.y + ((k >> 1) & 1)) * W + 2 * q.x + (k & 1);
+            float f[8];
+            load8(gcat + v * C + c, f);
+#pragma unroll
+            for (int j = 0; j < 8; j++) s[j] += f[j];
+        }
+        float fy[8];
+        load8(y0 + u * c0 + c, fy);
+#pragma unroll
+        for (int j = 0; j < 8; j++) s[j] = fy[j] > 0.0f ? s[j] : 0.0f;
+        store8b(g0 + u * c0 + c, s);
+    } else if (i < n_coarse + n_full) {
+        const long long k = i - n_coarse;
+        const int nc = c1 / 8, c = (int)(k % nc) * 8;
+        const long long v = k / nc;
+        *reinterpret_cast<uint4 *>(g1 + v * c1 + c) = *reinterpret_cast<const uint4 *>(gcat + v * C + c0 + c);
+    }
+}
+
+cudaError_t split_concat_grad(const bf16 *gcat, int c0, int c1, const bf16 *y0, bf16 *g0, bf16 *g1, int D, int H,
+                              int W, int nb, cudaStream_t s)
+{
+    const long long V = (long long)nb * D * H * W;
+    const long long nco = V / 8 * (c0 / 8), nfu = V * (c1 / 8);
+    split_concat_kernel<<<(unsigned)((nco + nfu + 255) / 256), 256, 0, s>>>(gcat, c0, c1, y0, g0, g1, D, H, W, nco,
+                                                                             nfu);
+    return cudaGetLastError();
+}
+
+// out = (gskip + gpool(parent) / 8) * (y > 0): gradient of a skip tensor that
+// also fed an average pool
+__global__ void pool_grad_mask_kernel(const bf16 *__restrict__ gskip, const bf16 *__restrict__ gpool,
+                                      const bf16 *__restrict__ y, bf16 *__restrict__ out, int C, int D, int H, int W,
+                                      long long total)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int nc = C / 8, c = (int)(i % nc) * 8;
+    const long long v = i / nc;
+    const Vox q = decode(v, D, H, W, total / nc);
+    const long long u = (((long long)q.n * (D / 2) + q.z / 2) * (H / 2) + q.y / 2) * (W / 2) + q.x / 2;
+    float a[8], b[8], fy[8];
+    load8(gskip + v * C + c, a);
+    load8(gpool + u * C + c, b);
+    load8(y + v * C + c, fy);
+#pragma unroll
+    for (int j = 0; j < 8; j++) a[j] = fy[j] > 0.0f ? a[j] + 0.125f * b[j] : 0.0f;
+    store8b(out + v * C + c, a);
+}
+
+cudaError_t pool_grad_mask(const bf16 *gskip, const bf16 *gpool, const bf16 *y, bf16 *out, int C, int D, int H,
+                           int W, int nb, cudaStream_t s)
+{
+    const long long total = (long long)nb * D * H * W * (C / 8);
+    pool_grad_mask_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(gskip, gpool, y, out, C, D, H, W, total);
+    return cudaGetLastError();
+}
+
+// --------------------------------------------------------------------------
+// residual 1x1 head with the MSE loss and its gradient
+// --------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) head_kernel(const HeadArgs a)
+{
+    __shared__ float red[8][18];
+    const float bias = a.w[16];
+    float w[16];
+#pragma unroll
+    for (int c = 0; c < 16; c++) w[c] = a.w[c];
+    float pw[17];
+#pragma unroll
+    for (int c = 0; c < 17; c++) pw[c] = 0.0f;
+    float ploss = 0.0f;
+    const bool train = a.target != nullptr;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < a.V; v += (long long)gridDim.x * blockDim.x) {
+        float d[16];
+        load8(a.d + v * 16, d);
+        load8(a.d + v * 16 + 8, d + 8);
+        float o = bias;
+#pragma unroll
+        for (int c = 0; c < 16; c++) o = fmaf(w[c], d[c], o);
+        o += a.x[v];
+        if (a.out) a.out[v] = o;
+        if (train) {
+            const float wt = a.weight ? a.weight[v] : 1.0f;
+            const float diff = o - a.target[v];
+            ploss = fmaf(wt * diff, diff, ploss);
+            const float go = (float)(2.0 * a.inv_count) * wt * diff;
+            float gd[16];
+#pragma unroll
+            for (int c = 0; c < 16; c++) {
+                gd[c] = d[c] > 0.0f ? go * w[c] : 0.0f;
+                pw[c] = fmaf(go, d[c], pw[c]);
+            }
+            pw[16] += go;
+            store8b(a.gd + v * 16, gd);
+            store8b(a.gd + v * 16 + 8, gd + 8);
+        }
+    }
+    if (!train) return;
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < 17; c++) {
+        float t = pw[c];
+        for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if (lane == 0) red[wp][c] = t;
+    }
+    for (int o = 16; o; o >>= 1) ploss += __shfl_xor_sync(0xffffffffu, ploss, o);
+    if (lane == 0) red[wp][17] = ploss;
+    __syncthreads();
+    if (threadIdx.x < 18) {
+        float t = 0.0f;
+        for (int k = 0; k < (int)(blockDim.x / 32); k++) t += red[k][threadIdx.x];
+        if (threadIdx.x < 17)
+            atomicAdd(&a.dw[threadIdx.x], t);
+        else
+            atomicAdd(a.loss, (double)t);
+    }
+}
+
+cudaError_t head(const HeadArgs &a, int sms, cudaStream_t s)
+{
+    const long long blocks = (a.V + 255) / 256;
+    head_kernel<<<(unsigned)std::max<long long>(1, std::min<long long>(blocks, 8LL * sms)), 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// --------------------------------------------------------------------------
+// AdamW on the fp32 master weights, then the bf16 B tiles
+// --------------------------------------------------------------------------
+__global__ void adamw_kernel(const AdamArgs a)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    int l = 0;
+    while (l + 1 < a.nlayers && i >= a.layers[l + 1].off) l++;
+    const AdamLayer L = a.layers[l];
+    const long long j = i - L.off;
+    const long long nw = L.taps ? (long long)L.cout * L.taps * L.cin : 16;
+    const bool is_w = j < nw;
+    float p = a.p[i];
+    if (a.update) {
+        const float g = a.g[i];
+        const float m = a.beta1 * a.m[i] + (1.0f - a.beta1) * g;
+        const float v = a.beta2 * a.v[i] + (1.0f - a.beta2) * g * g;
+        a.m[i] = m;
+        a.v[i] = v;
+        const float step = (m / a.bc1) / (sqrtf(v / a.bc2) + a.eps);
+        p -= a.lr * (step + (is_w ? a.weight_decay * p : 0.0f));
+        a.p[i] = p;
+    }
+    if (!L.taps || !is_w) return;
+    const int co = (int)(j / (L.taps * L.cin));
+    const int rem = (int)(j % (L.taps * L.cin));
+    const int tap = rem / L.cin, ci = rem % L.cin;
+    const bf16 h = __float2bfloat16_rn(p);
+    if (L.cin == 1) {
+        a.wf[L.wf_off + tap * L.cout + co] = h;
+        return;
+    }
+    a.wf[L.wf_off + (((long long)tap * (L.cin / 8) + ci / 8) * L.cout + co) * 8 + ci % 8] = h;
+    a.wd[L.wd_off + (((long long)(26 - tap) * (L.cout / 8) + co / 8) * L.cin + ci) * 8 + co % 8] = h;
+}
+
+cudaError_t adamw(const AdamArgs &a, cudaStream_t s)
+{
+    adamw_kernel<<<(unsigned)((a.n + 255) / 256), 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// --------------------------------------------------------------------------
+// training patches: plan[b] = {mesh, z0, y0, x0, transform}; out[b] = P^3 crop
+// of mesh (E^3, bf16) under one of the 48 axis permutations x reflections
+// --------------------------------------------------------------------------
+__global__ void crop_kernel(const bf16 *__restrict__ meshes, int nmesh, int E, const int *__restrict__ plan, int P,
+                            float *__restrict__ out, long long total, DeviceCounters *counters)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const long long per = (long long)P * P * P;
+    const int b = (int)(i / per);
+    const long long r = i % per;
+    int c[3] = {(int)(r / ((long long)P * P)), (int)((r / P) % P), (int)(r % P)};
+    const int *pl = plan + 5 * b;
+    const int perm = pl[4] % 6, flip = pl[4] / 6;
+    const int pa = perm / 2, pb = (perm / 2 + 1 + (perm & 1)) % 3, pc = 3 - pa - pb;
+    const int src_axis[3] = {pa, pb, pc};
+    int s[3];
+    for (int k = 0; k < 3; k++) {
+        int t = c[src_axis[k]];
+        if (flip & (1 << k)) t = P - 1 - t;
+        s[k] = t + pl[1 + k];
+    }
+    if ((unsigned)pl[0] >= (unsigned)nmesh || (unsigned)s[0] >= (unsigned)E || (unsigned)s[1] >= (unsigned)E ||
+        (unsigned)s[2] >= (unsigned)E || (unsigned)pl[4] >= 48u) {
+        out[i] = 0.0f;  // a plan entry outside the meshes: counted, not read
+        if (counters) atomicAdd(&counters->out_of_mesh, 1ull);
+        return;
+    }
+    out[i] = __bfloat162float(meshes[(size_t)pl[0] * E * E * E + ((size_t)s[0] * E + s[1]) * E + s[2]]);
+}
+
+cudaError_t crop_patches(const bf16 *meshes, int nmesh, int E, const int *plan, int nb, int P, float *out,
+                         DeviceCounters *counters, cudaStream_t s)
+{
+    const long long total = (long long)nb * P * P * P;
+    crop_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(meshes, nmesh, E, plan, P, out, total, counters);
+    return cudaGetLastError();
+}
+
+// network input from a pair mesh: the leading E^3 corner of the S^3 uint64
+// mesh times `scale` (1 / (Multiplicator x frames x normaliser)), as fp32
+// and/or bf16
+__global__ void mesh_input_kernel(const unsigned long long *__restrict__ full, int S, int E, double scale,
+                                  float *__restrict__ o32, bf16 *__restrict__ o16, long long total)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int x = (int)(i % E), y = (int)((i / E) % E), z = (int)(i / ((long long)E * E));
+    const float f = (float)((double)full[((size_t)z * S + y) * S + x] * scale);
+    if (o32) o32[i] = f;
+    if (o16) o16[i] = __float2bfloat16_rn(f);
+}
+
+cudaError_t mesh_input(const uint64_t *full, int S, int E, double scale, float *o32, bf16 *o16, cudaStream_t s)
+{
+    const long long total = (long long)E * E * E;
+    mesh_input_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(
+        reinterpret_cast<const unsigned long long *>(full), S, E, scale, o32, o16, total);
+    return cudaGetLastError();
+}
+
+}  // namespace dn
+}  // namespace iac

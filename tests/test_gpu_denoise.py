@@ -1,0 +1,216 @@
+"""The mesh denoiser's device kernels against the float64 CPU oracle
+(oracle/denoise_oracle.py): every 3x3x3 layer shape of the network in both
+tensor-core backends (tcgen05 + TMEM, mma.sync), the weight gradients, the
+whole network's forward pass and parameter gradients, patch extraction, and
+a short training run.
+
+Tolerances follow from the BF16 operands: the kernels multiply bf16 values
+exactly and accumulate in fp32, so a single layer's pre-rounding result is
+within ~1e-6 of the float64 value and its bf16 output within 2^-8 relative;
+whole-network outputs carry one bf16 rounding per layer (relative L2 error
+of the residual below 3e-2) and so do the gradients (per layer: relative L2
+error below 5e-2, cosine similarity above 0.998)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+# (c0, up0, c1, cout): the forward layers and the data-gradient layers of the network
+FWD = [(0, 0, 16, 16), (0, 0, 16, 32), (0, 0, 32, 32), (0, 0, 32, 64), (0, 0, 64, 64), (64, 1, 32, 32),
+       (32, 1, 16, 16)]
+DGRAD = [(0, 0, 32, 16), (0, 0, 64, 32), (0, 0, 32, 96), (0, 0, 16, 48)]
+
+
+def _bf16(a):
+    """fp32 array -> (bf16 bits as int16 torch tensor on the GPU, the float64 values)."""
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(torch.bfloat16)
+    return t.view(torch.int16).cuda(), t.to(torch.float64).numpy()
+
+
+def _from_bf16(t):
+    import torch
+    return t.view(torch.bfloat16).to(torch.float64).cpu().numpy()
+
+
+@pytest.mark.parametrize("backend", [0, 1], ids=["tcgen05", "mma_sync"])
+@pytest.mark.parametrize("c0,up0,c1,cout", FWD + DGRAD)
+@pytest.mark.parametrize("dims", [(2, 8, 8, 16), (2, 4, 6, 10)])
+def test_conv3x3_matches_oracle(ctx, rng, backend, c0, up0, c1, cout, dims):
+    import torch
+    from incohautocorrelate_b200 import capi
+    from oracle import denoise_oracle as O
+    nb, D, H, W = dims
+    cin = c0 + c1
+    s1_q, s1 = _bf16(rng.normal(0, 1, (nb, D, H, W, c1)))
+    s0_q, s0 = (None, None)
+    if c0:
+        s0_q, s0 = _bf16(rng.normal(0, 1, (nb, D // 2, H // 2, W // 2, c0)))
+    w = rng.normal(0, (2.0 / (27 * cin)) ** 0.5, (cout, 27, cin)).astype(np.float32)
+    wt_q, wq = _bf16(capi.conv_weight_tiles(w))
+    w64 = wq.reshape(27, cin // 8, cout, 8).transpose(2, 0, 1, 3).reshape(cout, 27, cin)
+    b = rng.normal(0, 0.1, cout).astype(np.float32)
+    want = O.conv_layer(s0, s1, w64, b.astype(np.float64), True, up0)
+    y = torch.zeros((nb, D, H, W, cout), dtype=torch.int16, device="cuda")
+    capi.denoise_conv3x3(ctx, backend, s0_q, c0, up0, s1_q, c1, wt_q, torch.from_numpy(b).cuda(), cout, 1,
+                         nb, D, H, W, y)
+    torch.cuda.synchronize()
+    assert ctx.check() == 0
+    got = _from_bf16(y)
+    scale = np.abs(want).max()
+    np.testing.assert_allclose(got, want, rtol=8e-3, atol=1e-5 * scale)
+
+
+@pytest.mark.parametrize("c0,up0,c1,cout", [(0, 0, 16, 16), (0, 0, 16, 32), (0, 0, 32, 32), (0, 0, 32, 64),
+                                            (0, 0, 64, 64), (64, 1, 32, 32), (32, 1, 16, 16)])
+def test_wgrad3x3_matches_oracle(ctx, rng, c0, up0, c1, cout):
+    import torch
+    from incohautocorrelate_b200 import capi
+    from oracle import denoise_oracle as O
+    nb, D, H, W = 2, 8, 12, 16
+    cin = c0 + c1
+    s1_q, s1 = _bf16(rng.normal(0, 1, (nb, D, H, W, c1)))
+    s0_q, s0 = (None, None)
+    if c0:
+        s0_q, s0 = _bf16(rng.normal(0, 1, (nb, D // 2, H // 2, W // 2, c0)))
+    g_q, g = _bf16(rng.normal(0, 1, (nb, D, H, W, cout)))
+    want_w, want_b = O.wgrad_layer(s0, s1, g, up0)
+    dw = torch.zeros((cout, 27, cin), dtype=torch.float32, device="cuda")
+    db = torch.zeros(cout, dtype=torch.float32, device="cuda")
+    capi.denoise_wgrad3x3(ctx, s0_q, c0, up0, s1_q, c1, g_q, cout, nb, D, H, W, dw, db)
+    torch.cuda.synchronize()
+    sw = np.abs(want_w).max()
+    np.testing.assert_allclose(dw.cpu().numpy(), want_w, rtol=1e-4, atol=1e-5 * sw)
+    np.testing.assert_allclose(db.cpu().numpy(), want_b, rtol=1e-4, atol=1e-5 * np.abs(want_b).max())
+
+
+def _random_params(rng, head_scale=0.3):
+    from oracle import denoise_oracle as O
+    parts = []
+    for ci, co in O.SPECS:
+        parts.append(rng.normal(0, (2.0 / (27 * ci)) ** 0.5, co * 27 * ci))
+        parts.append(rng.normal(0, 0.05, co))
+    parts.append(rng.normal(0, head_scale, 16))
+    parts.append([0.01])
+    return np.concatenate(parts).astype(np.float32)
+
+
+def _volumes(rng, nb, E):
+    x = rng.gamma(2.0, 0.5, (nb, E, E, E)).astype(np.float32)
+    t = (x * (1 + 0.2 * rng.normal(size=x.shape))).astype(np.float32)
+    return x, t
+
+
+def _bf16_params(p):
+    """The parameters as the device sees them: bf16 weights, fp32 biases and head."""
+    import torch
+    from oracle import denoise_oracle as O
+    q = p.astype(np.float64).copy()
+    o = 0
+    for ci, co in O.SPECS:
+        n = co * 27 * ci
+        q[o:o + n] = torch.from_numpy(p[o:o + n]).to(torch.bfloat16).to(torch.float64).numpy()
+        o += n + co
+    return q
+
+
+@pytest.mark.parametrize("backend", [0, 1], ids=["tcgen05", "mma_sync"])
+def test_network_forward_and_gradients_match_oracle(ctx, rng, backend):
+    import torch
+    from incohautocorrelate_b200 import capi
+    from oracle import denoise_oracle as O
+    nb, E = 2, 16
+    dn = capi.Denoiser(ctx, nb, E, E, E, backend=backend)
+    p = _random_params(rng)
+    dn.set_params(p)
+    x, t = _volumes(rng, nb, E)
+    dx, dt = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+    out = torch.zeros_like(dx)
+    loss = dn.backward(dx, dt, nb, E, E, E, d_out=out)
+    g = dn.get_grads()
+    assert ctx.check() == 0
+    want_loss, want_g, want_out = O.loss_and_grads(_bf16_params(p), x, t)
+    o = out.cpu().numpy()
+    assert np.linalg.norm(o - want_out) / np.linalg.norm(want_out - x) < 3e-2
+    assert abs(loss - want_loss) / want_loss < 3e-2
+    off = 0
+    for l, (ci, co) in enumerate(O.SPECS + [(16, 1)]):
+        n = co * 27 * ci + co if l < 10 else 17
+        a, b = g[off:off + n].astype(np.float64), want_g[off:off + n]
+        rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+        cos = a @ b / (np.linalg.norm(a) * np.linalg.norm(b))
+        assert rel < 5e-2 and cos > 0.998, (l, rel, cos)
+        off += n
+    dn.close()
+
+
+def test_backends_agree_on_a_full_volume(ctx, rng):
+    import torch
+    from incohautocorrelate_b200 import capi
+    nb, E = 1, 32
+    x, _ = _volumes(rng, nb, E)
+    dx = torch.from_numpy(x).cuda()
+    p = _random_params(rng)
+    outs = []
+    for be in (0, 1):
+        dn = capi.Denoiser(ctx, nb, E, E, E, backend=be)
+        dn.set_params(p)
+        o = torch.zeros_like(dx)
+        dn.forward(dx, nb, E, E, E, o)
+        torch.cuda.synchronize()
+        outs.append(o.cpu().numpy() - x)
+        dn.close()
+    assert ctx.check() == 0
+    assert np.linalg.norm(outs[0] - outs[1]) / np.linalg.norm(outs[1]) < 1e-2
+
+
+def test_training_reduces_the_loss(ctx, rng):
+    import torch
+    from incohautocorrelate_b200 import capi
+    nb, E = 2, 16
+    dn = capi.Denoiser(ctx, nb, E, E, E)
+    dn.init_params(seed=3)
+    # target: a smoothed copy of the input
+    x = rng.gamma(2.0, 0.5, (nb, E, E, E)).astype(np.float32)
+    k = np.ones(3) / 3
+    t = x.copy()
+    for ax in (1, 2, 3):
+        t = np.apply_along_axis(lambda v: np.convolve(v, k, mode="same"), ax, t)
+    dx, dt = torch.from_numpy(x).cuda(), torch.from_numpy(t.astype(np.float32)).cuda()
+    first = dn.backward(dx, dt, nb, E, E, E)
+    for _ in range(100):
+        dn.adamw_step(lr=3e-3)
+        last = dn.backward(dx, dt, nb, E, E, E)
+    assert ctx.check() == 0
+    assert last < 0.5 * first, (first, last)
+    dn.close()
+
+
+def test_crop_patches_and_mesh_input(ctx, rng):
+    import torch
+    from incohautocorrelate_b200 import capi
+    E, P, n = 12, 5, 3
+    m = rng.normal(0, 1, (n, E, E, E)).astype(np.float32)
+    mq, m64 = _bf16(m)
+    plan = np.array([[0, 0, 0, 0, 0], [2, 7, 3, 1, 13], [1, 4, 7, 2, 47]], np.int32)
+    out = torch.zeros((3, P, P, P), dtype=torch.float32, device="cuda")
+    capi.denoise_crop_patches(ctx, mq, n, E, torch.from_numpy(plan).cuda(), 3, P, out)
+    assert ctx.check() == 0
+    got = out.cpu().numpy()
+    for b, (i, z0, y0, x0, tr) in enumerate(plan):
+        perm = [(0, 1, 2), (0, 2, 1), (1, 2, 0), (1, 0, 2), (2, 0, 1), (2, 1, 0)][tr % 6]
+        flip = tr // 6
+        for z in range(P):
+            for y in range(P):
+                for x in range(P):
+                    c = (z, y, x)
+                    s = [c[perm[k]] for k in range(3)]
+                    s = [(P - 1 - s[k]) if flip & (1 << k) else s[k] for k in range(3)]
+                    assert got[b, z, y, x] == np.float32(m64[i, s[0] + z0, s[1] + y0, s[2] + x0])
+    S = 7
+    full = rng.integers(0, 1 << 40, S ** 3, dtype=np.uint64)
+    d_full = torch.from_numpy(full.view(np.int64)).cuda()
+    o32 = torch.zeros(4 ** 3, dtype=torch.float32, device="cuda")
+    capi.denoise_mesh_input(ctx, d_full, S, 4, 1e-9, d_f32=o32)
+    want = (full.reshape(S, S, S)[:4, :4, :4].astype(np.float64) * 1e-9).astype(np.float32)
+    np.testing.assert_array_equal(o32.cpu().numpy().reshape(4, 4, 4), want)
