@@ -51,8 +51,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--det", type=int, default=1024,
                     help="edge of the square detector of the dense kernels (1024 = their config)")
+    ap.add_argument("--backend", type=int, default=0,
+                    help="denoiser convolutions: 0 = tcgen05 + TMEM, 1 = mma.sync")
     ap.add_argument("--kernel", default="sparse",
-                    choices=["sparse", "cq_small", "ac1d_cq", "cq_merge", "ac1d_sparse", "simulate"],
+                    choices=["sparse", "cq_small", "ac1d_cq", "cq_merge", "ac1d_sparse", "simulate",
+                             "denoise"],
                     help="sparse is the headline; the others measure the remaining kernels "
                          "of the path on their configurations")
     return ap.parse_args()
@@ -564,9 +567,106 @@ def run_kernel(args):
                     config={"workload": f"{nf} rotated-correlator frames, 256 bins, linear"})
     elif args.kernel == "simulate":
         line.update(simulate_pipeline(args, ctx, stream, clocks, nthreads))
+    elif args.kernel == "denoise":
+        line.update(denoise_bench(args, ctx, stream, clocks, nthreads))
     print(json.dumps(line), flush=True)
     ctx.close()
     return 0
+
+
+# multiply-adds per full-resolution voxel of the denoiser's forward pass:
+# 3x3x3 layers 1->16, 16->16 at full resolution, 16->32, 32->32 at 1/8,
+# 32->64, 64->64 at 1/64, 96->32, 32->32 at 1/8, 48->16, 16->16 at full
+# resolution, and the 16->1 head
+DENOISE_LAYERS = [(1, 16, 1), (16, 16, 1), (16, 32, 8), (32, 32, 8), (32, 64, 64), (64, 64, 64),
+                  (96, 32, 8), (32, 32, 8), (48, 16, 1), (16, 16, 1)]
+DENOISE_FWD_MACS = sum(27 * ci * co / d for ci, co, d in DENOISE_LAYERS) + 16
+# training step: forward + data gradients (all but the first layer) + weight gradients
+DENOISE_TRAIN_MACS = DENOISE_FWD_MACS + (DENOISE_FWD_MACS - 27 * 16 - 16) + DENOISE_FWD_MACS
+
+
+def denoise_bench(args, ctx, stream, clocks, nthreads):
+    """The denoiser's training step (8 patches of 64^3, forward + loss +
+    backward + AdamW) and its inference on a whole 128^3 mesh, plus each
+    3x3x3 layer shape alone in both tensor-core backends."""
+    import torch
+    from incohautocorrelate_b200 import capi
+    sp = stream.cuda_stream
+    rng = np.random.default_rng(11)
+    B, P, E = 8, 64, 128
+    dn = capi.Denoiser(ctx, B, P, P, P, backend=args.backend)
+    parts = []
+    for ci, co, _ in DENOISE_LAYERS:
+        parts += [rng.normal(0, (2.0 / (27 * ci)) ** 0.5, co * 27 * ci), rng.normal(0, 0.05, co)]
+    parts += [rng.normal(0, 0.3, 16), [0.0]]
+    dn.set_params(np.concatenate(parts).astype(np.float32))
+    x = torch.from_numpy(rng.gamma(2.0, 0.5, (B, P, P, P)).astype(np.float32)).cuda()
+    t = x * (1 + 0.2 * torch.randn_like(x))
+    clocks.start()
+
+    def train_step():
+        dn.backward(x, t, B, P, P, P, stream=sp, want_loss=False)
+        dn.adamw_step(lr=1e-5, stream=sp)
+
+    ms_train = _time(train_step, args.steps, max(3, args.warmup), stream)
+    xf = torch.from_numpy(rng.gamma(2.0, 0.5, (1, E, E, E)).astype(np.float32)).cuda()
+    of = torch.zeros_like(xf)
+    ms_fwd = _time(lambda: dn.forward(xf, 1, E, E, E, of, sp), args.steps, max(3, args.warmup), stream)
+    # every 3x3x3 shape alone on the training batch's volume at its level
+    layers = []
+    for ci, co, d in DENOISE_LAYERS[1:]:
+        edge = P // round(d ** (1 / 3))
+        nvox = B * edge ** 3
+        c0 = {96: 64, 48: 32}.get(ci, 0)
+        c1 = ci - c0
+        s1 = torch.randn((B, edge, edge, edge, c1), device="cuda").to(torch.bfloat16).view(torch.int16)
+        s0 = (torch.randn((B, edge // 2, edge // 2, edge // 2, c0), device="cuda")
+              .to(torch.bfloat16).view(torch.int16)) if c0 else None
+        w = torch.from_numpy(capi.conv_weight_tiles(rng.normal(0, 0.1, (co, 27, ci)))).cuda()
+        w = w.to(torch.bfloat16).view(torch.int16)
+        b = torch.zeros(co, device="cuda")
+        y = torch.zeros((nvox, co), dtype=torch.int16, device="cuda")
+        row = {"cin": ci, "cout": co, "volume": f"{B}x{edge}^3", "concat_upsample": bool(c0)}
+        for be, name in ((0, "tcgen05"), (1, "mma_sync")):
+            ms = _time(lambda: capi.denoise_conv3x3(ctx, be, s0, c0, 1, s1, c1, w, b, co, 1, B, edge, edge,
+                                                    edge, y, sp), 10, 3, stream)
+            row[name + "_ms"] = ms
+            row[name + "_tflops"] = 2.0 * 27 * ci * co * nvox / (ms * 1e-3) / 1e12
+        layers.append(row)
+    clk = clocks.stop()
+    peaks = measured_peaks()
+    peak = peaks.get("bf16_tflops_sustained") or 1392.0
+    tf_train = 2.0 * DENOISE_TRAIN_MACS * B * P ** 3 / (ms_train * 1e-3) / 1e12
+    tf_fwd = 2.0 * DENOISE_FWD_MACS * E ** 3 / (ms_fwd * 1e-3) / 1e12
+    out = {"metric": "denoiser training voxels/s (8 x 64^3 patches, forward + backward + AdamW)",
+           "value": B * P ** 3 / (ms_train * 1e-3), "unit": "voxels/s", "ms_per_step": ms_train,
+           "dtype": "bf16 operands, fp32 accumulation",
+           "config": {"workload": "3-level 3D U-Net 16/32/64, 3x3x3 convs, batch 8 x 64^3 (activations "
+                                  "> L2 per step)", "backend": ["tcgen05", "mma.sync"][args.backend],
+                      "params": capi.denoise_param_count(),
+                      "train_flop_per_voxel": 2.0 * DENOISE_TRAIN_MACS,
+                      "forward_flop_per_voxel": 2.0 * DENOISE_FWD_MACS},
+           "inference": {"volume": f"1 x {E}^3", "ms": ms_fwd, "tflops": tf_fwd,
+                         "meshes_per_s": 1e3 / ms_fwd},
+           "layers": layers, "clocks": clk,
+           "roofline": {"bound": "tensor", "achieved": tf_train, "unit": "TFLOP/s", "peak": peak,
+                        "frac": tf_train / peak, "peak_source": "measured bf16_tflops_sustained",
+                        "kernel": "whole training step"}}
+    if not args.no_cpu_baseline:
+        import torch as T
+        from oracle import denoise_oracle as O
+        T.set_num_threads(nthreads)
+        L = [(w.float(), b.float()) for w, b in O.unpack(dn.get_params())]
+        xc = T.from_numpy(rng.gamma(2.0, 0.5, (1, 32, 32, 32)).astype(np.float32))
+        t0 = time.perf_counter()
+        with T.no_grad():
+            O.forward(L, xc)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": 32 ** 3 / dt, "unit": "voxels/s (forward only)", "cores": nthreads,
+                               "kind": "port", "sample": f"torch fp32 CPU forward of the same network on 1 x "
+                                                         f"32^3 ({dt:.2f} s)"}
+    dn.close()
+    return out
 
 
 def simulate_pipeline(args, ctx, stream, clocks, nthreads):

@@ -359,7 +359,9 @@ typedef struct iac_adamw {
 uint64_t iac_denoise_param_count(void);
 
 /* Workspace for up to max_batch volumes of D x H x W.  backend 0 runs the
- * convolutions on tcgen05.mma with TMEM accumulators, 1 on mma.sync. */
+ * convolutions on tcgen05.mma with TMEM accumulators over padded-row slabs
+ * (persistent CTAs), 1 on mma.sync, 2 on tcgen05.mma with one gathered
+ * operand tile per tap. */
 iac_status iac_denoise_create(iac_ctx *ctx, uint32_t max_batch, uint32_t D, uint32_t H, uint32_t W,
                               int backend, iac_denoiser **out);
 void iac_denoise_destroy(iac_denoiser *dn);

@@ -384,8 +384,9 @@ class Context:
 # --------------------------------------------------------------------------
 # mesh denoiser
 # --------------------------------------------------------------------------
-TCGEN05 = 0
+TCGEN05 = 0          # tcgen05 + TMEM over padded-row slabs (default)
 MMA_SYNC = 1
+TCGEN05_PER_TAP = 2
 
 
 def denoise_param_count() -> int:

@@ -122,6 +122,7 @@ ConvArgs conv_args(iac_denoiser *dn, int l, const bf16 *src0, const bf16 *src1, 
     a.W = W;
     a.V = V;
     a.counters = dn->ctx->d_counters;
+    a.sms = dn->ctx->sm_count;
     return a;
 }
 
@@ -139,6 +140,7 @@ iac_status dgrad(iac_denoiser *dn, int l, const bf16 *gp, bf16 *out, int D, int 
     a.W = W;
     a.V = V;
     a.counters = dn->ctx->d_counters;
+    a.sms = dn->ctx->sm_count;
     DN_CHECK(conv3x3(a, SPECS[l].cout, SPECS[l].cin, dn->backend, s), "denoiser data gradient");
     return IAC_OK;
 }
@@ -248,7 +250,8 @@ iac_status iac_denoise_create(iac_ctx *ctx, uint32_t max_batch, uint32_t D, uint
                               iac_denoiser **out)
 {
     IAC_REQUIRE(ctx && out, "null argument");
-    IAC_REQUIRE(backend == 0 || backend == 1, "backend %d (0 = tcgen05, 1 = mma.sync)", backend);
+    IAC_REQUIRE(backend >= 0 && backend <= 2, "backend %d (0 = tcgen05 slabs, 1 = mma.sync, 2 = tcgen05 per tap)",
+                backend);
     IAC_REQUIRE(max_batch >= 1 && D % 4 == 0 && H % 4 == 0 && W % 4 == 0 && D && H && W,
                 "workspace %u x %ux%ux%u: edges must be multiples of 4", max_batch, D, H, W);
     DeviceGuard guard(ctx->device);
@@ -512,7 +515,7 @@ iac_status iac_denoise_conv3x3(iac_ctx *ctx, int backend, const uint16_t *d_src0
                                uint16_t *d_y, void *stream)
 {
     IAC_REQUIRE(ctx && d_src1 && d_wtile && d_y && (c0 == 0 || d_src0), "null argument");
-    IAC_REQUIRE(backend == 0 || backend == 1, "backend %d", backend);
+    IAC_REQUIRE(backend >= 0 && backend <= 2, "backend %d", backend);
     IAC_REQUIRE(c0 % 16 == 0 && c1 % 8 == 0 && c1 > 0, "channels %u + %u", c0, c1);
     IAC_REQUIRE(D && H && W && nb && (!up0 || (D % 2 == 0 && H % 2 == 0 && W % 2 == 0)), "volume %ux%ux%u", D, H,
                 W);
@@ -532,6 +535,7 @@ iac_status iac_denoise_conv3x3(iac_ctx *ctx, int backend, const uint16_t *d_src0
     a.W = (int)W;
     a.V = (long long)nb * D * H * W;
     a.counters = ctx->d_counters;
+    a.sms = ctx->sm_count;
     const cudaError_t e = conv3x3(a, (int)(c0 + c1), (int)cout, backend, (cudaStream_t)stream);
     IAC_REQUIRE(e != cudaErrorInvalidValue, "no 3x3x3 kernel for %u -> %u channels", c0 + c1, cout);
     DN_CHECK(e, "conv3x3");

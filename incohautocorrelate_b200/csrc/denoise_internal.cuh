@@ -40,7 +40,13 @@ struct ConvArgs {
     int D, H, W;         // output (= src1) dims per batch item
     long long V;         // nb * D * H * W
     DeviceCounters *counters;
+    int sms;             // SMs of the device (persistent grids)
 };
+
+// backends of conv3x3
+constexpr int BACKEND_TC_SLAB = 0;  // tcgen05, padded-row slabs, persistent (default)
+constexpr int BACKEND_MMA = 1;      // mma.sync.m16n8k16
+constexpr int BACKEND_TC_TAP = 2;   // tcgen05, one gathered tile per tap
 
 // dW[co][tap][ci] += sum_v G[v][co] X[v+off(tap)][ci], dB[co] += sum_v G[v][co]
 struct WgradArgs {

@@ -24,6 +24,8 @@
 //     releases the stage for the next cp.async; the epilogue reads TMEM with
 //     tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = its 32 voxels);
 //   backend 1, mma.sync.m16n8k16: four warps of 32 voxels x cout each.
+// Backend 0 (the default, conv_slab_kernel) stages each input row once per
+// (tile, dz) instead of once per tap; backend 2 is the per-tap tcgen05 form.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -462,11 +464,212 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_mma_kernel(const ConvArgs a
         }
 }
 
+// --------------------------------------------------------------------------
+// backend 0: tcgen05 on padded-row slabs (default)
+//
+// The output positions of one z-plane are numbered q = y (W+2) + x', x' = x+1,
+// so every row carries its two halo columns; a tile is 128 consecutive q.  For
+// tap (dz, dy, dx) the A row of position q is q + dy (W+2) + dx in plane z+dz,
+// so the nine (dy, dx) taps of one dz read one slab of R = 128 + 2 (W+2) + 2
+// consecutive padded positions at nine row offsets: each tap's operand is the
+// slab's descriptor advanced by 16 B per row of shift (core matrices are any
+// eight consecutive 16-byte rows).  A tile takes three stages (dz = -1, 0, 1),
+// each the slab plus that dz's nine weight tiles; halo-column outputs are
+// computed and dropped (2/(W+2) of the MACs).  CTAs are persistent over tiles
+// and the TMEM accumulator is double-buffered, so the epilogue of tile k runs
+// while the MMAs of tile k+1 execute.
+// --------------------------------------------------------------------------
+struct SlabGeom {
+    int Wp;            // W + 2
+    int R;             // slab rows
+    int T;             // tiles per plane
+    long long ntiles;  // nb * D * T
+    uint32_t slab_bytes, stage_bytes;
+    int S;             // stages in the ring (2..4)
+};
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(CONV_THREADS) conv_slab_kernel(const ConvArgs a, const SlabGeom g)
+{
+    constexpr uint32_t TCOLS = 2 * COUT <= 32 ? 32 : (2 * COUT <= 64 ? 64 : (2 * COUT <= 128 ? 128 : 256));
+    constexpr uint32_t IDESC = idesc_bf16(TILE_M, COUT);
+    constexpr uint32_t WT_BYTES = COUT * CIN * 2;  // one tap's weight tile
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar[4];
+    __shared__ __align__(8) uint64_t accbar[2];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_err;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t sbase = smem_u32(smem);
+    if (tid == 0) {
+        for (int k = 0; k < 4; k++) mbar_init(smem_u32(&mbar[k]), 1);
+        mbar_init(smem_u32(&accbar[0]), 1);
+        mbar_init(smem_u32(&accbar[1]), 1);
+        fence_mbar_init();
+        s_err = 0;
+    }
+    if (warp == 0) {
+        tmem_alloc(smem_u32(&s_tmem), TCOLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const long long my_tiles =
+        blockIdx.x < g.ntiles ? (g.ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+    const long long nst = 3 * my_tiles;
+    const int S = g.S, PF = S >= 3 ? 2 : 1;
+    const int HW = a.H * a.W;
+    const int Hh = a.H >> 1, Wh = a.W >> 1, Dh = a.D >> 1;
+
+    auto load_stage = [&](long long i) {
+        const long long tile = blockIdx.x + (i / 3) * (long long)gridDim.x;
+        const int dz = (int)(i % 3) - 1;
+        const uint32_t sS = sbase + (uint32_t)(i % S) * g.stage_bytes;
+        const uint32_t sW = sS + g.slab_bytes;
+        const long long plane = tile / g.T;  // n * D + z
+        const int q0 = (int)(tile % g.T) * TILE_M;
+        const int n = (int)(plane / a.D), z = (int)(plane % a.D) + dz;
+        const bool zok = (unsigned)z < (unsigned)a.D;
+        for (int r = tid; r < g.R; r += CONV_THREADS) {
+            const int q = q0 - g.Wp - 1 + r;  // >= -Wp - 1
+            const int y = q >= 0 ? q / g.Wp : -1;
+            const int xp = q - y * g.Wp;
+            const bool ok = zok && y >= 0 && y < a.H && xp >= 1 && xp <= a.W;
+            const int x = xp - 1;
+            const bf16 *p0 = a.src0, *p1 = a.src1;
+            if (ok) {
+                if (a.c0) {
+                    if (a.up0)
+                        p0 = a.src0 + ((((long long)n * Dh + (z >> 1)) * Hh + (y >> 1)) * Wh + (x >> 1)) * a.c0;
+                    else
+                        p0 = a.src0 + (((long long)n * a.D + z) * HW + (long long)y * a.W + x) * a.c0;
+                }
+                p1 = a.src1 + (((long long)n * a.D + z) * HW + (long long)y * a.W + x) * a.c1;
+            }
+            const int n0 = a.c0 >> 3;
+#pragma unroll
+            for (int c = 0; c < CIN / 8; c++) {
+                const bf16 *src = c < n0 ? p0 + c * 8 : p1 + (c - n0) * 8;
+                cp_async16(sS + (uint32_t)((c * g.R + r) * 16), src, ok ? 16u : 0u);
+            }
+        }
+        const bf16 *wsrc = a.w + (size_t)(9 * (dz + 1)) * CIN * COUT;
+        for (int k = tid; k < (int)(9 * WT_BYTES / 16); k += CONV_THREADS) cp_async16(sW + k * 16, wsrc + k * 8, 16);
+    };
+
+    auto epilogue = [&](long long k) {
+        const long long tile = blockIdx.x + k * (long long)gridDim.x;
+        const bool ok = mbar_wait(smem_u32(&accbar[k & 1]), (uint32_t)((k >> 1) & 1));
+        if (!ok) s_err = 1;
+        tc_fence_after();
+        const long long plane = tile / g.T;
+        const int q = (int)(tile % g.T) * TILE_M + tid;
+        const int y = q / g.Wp, xp = q - (q / g.Wp) * g.Wp;
+        const bool valid = ok && y < a.H && xp >= 1 && xp <= a.W;
+        const long long v = plane * HW + (long long)y * a.W + (xp - 1);
+#pragma unroll
+        for (int c = 0; c < COUT; c += 16) {
+            uint32_t r[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((k & 1) * COUT + c), r);
+            tmem_wait_ld();
+            if (valid) {
+                float f[16];
+#pragma unroll
+                for (int j = 0; j < 16; j++) f[j] = __uint_as_float(r[j]);
+                store8(a, COUT, v, c, f);
+                store8(a, COUT, v, c + 8, f + 8);
+            }
+        }
+        tc_fence_before();
+    };
+
+    for (long long i = 0; i < PF && i < nst; i++) {
+        load_stage(i);
+        cp_async_commit();
+    }
+    for (long long i = 0; i < nst; i++) {
+        const long long j = i + PF;
+        if (j < nst) {
+            // the slot was last read by the MMAs of stage j - S
+            if (j >= S && !mbar_wait(smem_u32(&mbar[j % S]), (uint32_t)(((j - S) / S) & 1))) s_err = 1;
+            load_stage(j);
+        }
+        cp_async_commit();
+        if (PF == 2)
+            cp_async_wait<2>();
+        else
+            cp_async_wait<1>();
+        fence_proxy_async();
+        __syncthreads();
+        if (s_err) break;
+        const long long k = i / 3;
+        const int dzi = (int)(i % 3);
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t sS = sbase + (uint32_t)(i % S) * g.stage_bytes, sW = sS + g.slab_bytes;
+            const uint32_t dcol = tmem + (uint32_t)((k & 1) * COUT);
+#pragma unroll 1
+            for (int t = 0; t < 9; t++) {
+                const uint32_t r0 = (uint32_t)(g.Wp + 1 + (t / 3 - 1) * g.Wp + (t % 3 - 1));
+#pragma unroll
+                for (int kk = 0; kk < CIN / 16; kk++) {
+                    const uint64_t da = smem_desc(sS + (uint32_t)(kk * 2 * g.R * 16) + r0 * 16, (uint32_t)g.R * 16, 128);
+                    const uint64_t db = smem_desc(sW + t * WT_BYTES + kk * 2 * (COUT * 16), COUT * 16, 128);
+                    umma_bf16(dcol, da, db, IDESC, (dzi > 0 || t > 0 || kk > 0) ? 1u : 0u);
+                }
+            }
+            umma_commit(smem_u32(&mbar[i % S]));
+            if (dzi == 2) umma_commit(smem_u32(&accbar[k & 1]));
+        }
+        if (dzi == 0 && k > 0) epilogue(k - 1);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    if (!s_err && nst > 0) epilogue(my_tiles - 1);
+    if (s_err && tid == 0 && a.counters) atomicAdd(&a.counters->timeouts, 1ull);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, TCOLS);
+}
+
+template <int CIN, int COUT>
+static bool launch_slab(const ConvArgs &a, cudaStream_t s, cudaError_t &err)
+{
+    SlabGeom g{};
+    g.Wp = a.W + 2;
+    g.R = TILE_M + 2 * g.Wp + 2;
+    g.T = (a.H * g.Wp + TILE_M - 1) / TILE_M;
+    const long long nb = a.V / ((long long)a.D * a.H * a.W);
+    g.ntiles = nb * a.D * g.T;
+    g.slab_bytes = (uint32_t)g.R * CIN * 2;
+    g.stage_bytes = g.slab_bytes + 9u * COUT * CIN * 2;
+    const uint32_t budget = 227u * 1024u - 512u;
+    g.S = (int)std::min<uint32_t>(4u, budget / g.stage_bytes);
+    if (g.S < 2 || g.ntiles == 0) return false;
+    const uint32_t smem = (uint32_t)g.S * g.stage_bytes;
+    err = cudaFuncSetAttribute(conv_slab_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return true;
+    int per_sm = 0;
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv_slab_kernel<CIN, COUT>, CONV_THREADS, smem);
+    if (err != cudaSuccess) return true;
+    const long long grid = std::min<long long>(g.ntiles, (long long)std::max(1, per_sm) * std::max(1, a.sms));
+    conv_slab_kernel<CIN, COUT><<<(unsigned)grid, CONV_THREADS, smem, s>>>(a, g);
+    err = cudaGetLastError();
+    return true;
+}
+
 template <int CIN, int COUT>
 static cudaError_t launch_conv(const ConvArgs &a, int backend, cudaStream_t s)
 {
     const unsigned grid = (unsigned)((a.V + TILE_M - 1) / TILE_M);
-    if (backend == 0) {
+    if (backend == BACKEND_TC_SLAB) {
+        cudaError_t e = cudaSuccess;
+        if (launch_slab<CIN, COUT>(a, s, e)) return e;
+        backend = BACKEND_TC_TAP;  // a slab stage does not fit in shared memory
+    }
+    if (backend == BACKEND_TC_TAP) {
         const uint32_t smem = TcCfg<CIN, COUT>::SMEM;
         cudaError_t e = cudaFuncSetAttribute(conv_tc_kernel<CIN, COUT>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

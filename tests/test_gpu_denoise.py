@@ -33,9 +33,12 @@ def _from_bf16(t):
     return t.view(torch.bfloat16).to(torch.float64).cpu().numpy()
 
 
-@pytest.mark.parametrize("backend", [0, 1], ids=["tcgen05", "mma_sync"])
+BACKENDS = dict(argvalues=[0, 1, 2], ids=["tcgen05_slab", "mma_sync", "tcgen05_tap"])
+
+
+@pytest.mark.parametrize("backend", **BACKENDS)
 @pytest.mark.parametrize("c0,up0,c1,cout", FWD + DGRAD)
-@pytest.mark.parametrize("dims", [(2, 8, 8, 16), (2, 4, 6, 10)])
+@pytest.mark.parametrize("dims", [(2, 8, 8, 16), (2, 4, 6, 10), (4, 16, 32, 64)])
 def test_conv3x3_matches_oracle(ctx, rng, backend, c0, up0, c1, cout, dims):
     import torch
     from incohautocorrelate_b200 import capi
@@ -114,7 +117,7 @@ def _bf16_params(p):
     return q
 
 
-@pytest.mark.parametrize("backend", [0, 1], ids=["tcgen05", "mma_sync"])
+@pytest.mark.parametrize("backend", **BACKENDS)
 def test_network_forward_and_gradients_match_oracle(ctx, rng, backend):
     import torch
     from incohautocorrelate_b200 import capi
@@ -147,12 +150,12 @@ def test_network_forward_and_gradients_match_oracle(ctx, rng, backend):
 def test_backends_agree_on_a_full_volume(ctx, rng):
     import torch
     from incohautocorrelate_b200 import capi
-    nb, E = 1, 32
+    nb, E = 1, 64
     x, _ = _volumes(rng, nb, E)
     dx = torch.from_numpy(x).cuda()
     p = _random_params(rng)
     outs = []
-    for be in (0, 1):
+    for be in (0, 1, 2):
         dn = capi.Denoiser(ctx, nb, E, E, E, backend=be)
         dn.set_params(p)
         o = torch.zeros_like(dx)
@@ -161,7 +164,8 @@ def test_backends_agree_on_a_full_volume(ctx, rng):
         outs.append(o.cpu().numpy() - x)
         dn.close()
     assert ctx.check() == 0
-    assert np.linalg.norm(outs[0] - outs[1]) / np.linalg.norm(outs[1]) < 1e-2
+    for o in (outs[0], outs[2]):
+        assert np.linalg.norm(o - outs[1]) / np.linalg.norm(outs[1]) < 1e-2
 
 
 def test_training_reduces_the_loss(ctx, rng):
@@ -214,3 +218,30 @@ def test_crop_patches_and_mesh_input(ctx, rng):
     capi.denoise_mesh_input(ctx, d_full, S, 4, 1e-9, d_f32=o32)
     want = (full.reshape(S, S, S)[:4, :4, :4].astype(np.float64) * 1e-9).astype(np.float32)
     np.testing.assert_array_equal(o32.cpu().numpy().reshape(4, 4, 4), want)
+
+
+def test_trained_denoiser_needs_fewer_frames_than_the_plain_mesh(ctx):
+    """The committed network (trained on 512 random crystals, 500 -> 50 000
+    frames) on held-out crystals it never saw: the denoised 500-frame mesh
+    against an independent 40 000-frame reference matches the plain mesh of
+    several times more frames (measured 9-17x, median 13x, on 32 crystals with
+    a 100 000-frame reference; this test asserts a median above 8x on four)."""
+    import os
+
+    import torch
+    from incohautocorrelate_b200 import capi
+    from incohautocorrelate_b200 import denoise as DN
+    path = os.path.join(os.path.dirname(capi.__file__), "weights", "denoiser_128.npz")
+    params, meta = DN.load_model(path)
+    setup = DN.SimSetup(**meta["setup"])
+    sim = DN.MeshSimulator(ctx, setup)
+    E = setup.crop
+    dn = capi.Denoiser(ctx, 1, E, E, E)
+    dn.set_params(params)
+    summary, rows = DN.evaluate(ctx, sim, dn, meta["norm"], 4, 500, [1000, 2000, 5000], 40000, seed=777,
+                                log=None)
+    assert ctx.check() == 0
+    for r in rows:
+        assert r["err_denoised"] < 0.5 * r["err_plain"][500], r
+    assert summary["median_gain"] > 8.0, summary
+    dn.close()
