@@ -150,8 +150,8 @@ def _declare(lib):
     fn("iac_denoise_adamw_step", [_VP, C.POINTER(AdamW), _VP])
     fn("iac_denoise_conv3x3", [_VP, C.c_int, _VP, _U32, C.c_int, _VP, _U32, _VP, _VP, _U32, C.c_int,
                                _U32, _U32, _U32, _U32, _VP, _VP])
-    fn("iac_denoise_wgrad3x3", [_VP, _VP, _U32, C.c_int, _VP, _U32, _VP, _U32, _U32, _U32, _U32,
-                                _U32, _VP, _VP, _VP])
+    fn("iac_denoise_wgrad3x3", [_VP, C.c_int, _VP, _U32, C.c_int, _VP, _U32, _VP, _U32, _U32, _U32,
+                                _U32, _U32, _VP, _VP, _VP])
     fn("iac_denoise_mesh_input", [_VP, _VP, _U32, _U32, D, _VP, _VP, _VP])
     fn("iac_denoise_crop_patches", [_VP, _VP, _U32, _U32, _VP, _U32, _U32, _VP, _VP])
     return lib
@@ -472,8 +472,9 @@ def denoise_conv3x3(ctx, backend, d_src0, c0, up0, d_src1, c1, d_wtile, d_bias, 
 
 
 def denoise_wgrad3x3(ctx, d_src0, c0, up0, d_src1, c1, d_grad, cout, nb, D, H, W, d_dw, d_db=None,
-                     stream=None):
-    check(lib().iac_denoise_wgrad3x3(ctx._h, _ptr(d_src0), int(c0), int(up0), _ptr(d_src1), int(c1),
+                     stream=None, slabs=True):
+    check(lib().iac_denoise_wgrad3x3(ctx._h, int(bool(slabs)), _ptr(d_src0), int(c0), int(up0), _ptr(d_src1),
+                                     int(c1),
                                      _ptr(d_grad), int(cout), int(nb), int(D), int(H), int(W),
                                      _ptr(d_dw), _ptr(d_db), _ptr(stream)))
 

@@ -167,6 +167,7 @@ iac_status wgrad(iac_denoiser *dn, int l, const bf16 *src0, const bf16 *src1, co
     a.W = W;
     a.V = V;
     a.cout = SPECS[l].cout;
+    a.slabs = dn->backend != BACKEND_TC_TAP;
     DN_CHECK(wgrad3x3(a, cin, dn->ctx->sm_count, s), "denoiser weight gradient");
     return IAC_OK;
 }
@@ -543,9 +544,10 @@ iac_status iac_denoise_conv3x3(iac_ctx *ctx, int backend, const uint16_t *d_src0
     return IAC_OK;
 }
 
-iac_status iac_denoise_wgrad3x3(iac_ctx *ctx, const uint16_t *d_src0, uint32_t c0, int up0, const uint16_t *d_src1,
-                                uint32_t c1, const uint16_t *d_grad, uint32_t cout, uint32_t nb, uint32_t D,
-                                uint32_t H, uint32_t W, float *d_dw, float *d_db, void *stream)
+iac_status iac_denoise_wgrad3x3(iac_ctx *ctx, int slabs, const uint16_t *d_src0, uint32_t c0, int up0,
+                                const uint16_t *d_src1, uint32_t c1, const uint16_t *d_grad, uint32_t cout,
+                                uint32_t nb, uint32_t D, uint32_t H, uint32_t W, float *d_dw, float *d_db,
+                                void *stream)
 {
     IAC_REQUIRE(ctx && d_src1 && d_grad && d_dw && (c0 == 0 || d_src0), "null argument");
     IAC_REQUIRE(D && H && W && nb && (!up0 || (D % 2 == 0 && H % 2 == 0 && W % 2 == 0)), "volume %ux%ux%u", D, H,
@@ -565,6 +567,7 @@ iac_status iac_denoise_wgrad3x3(iac_ctx *ctx, const uint16_t *d_src0, uint32_t c
     a.W = (int)W;
     a.V = (long long)nb * D * H * W;
     a.cout = (int)cout;
+    a.slabs = slabs;
     const cudaError_t e = wgrad3x3(a, (int)(c0 + c1), ctx->sm_count, (cudaStream_t)stream);
     IAC_REQUIRE(e != cudaErrorInvalidValue, "no 3x3x3 weight-gradient kernel for %u -> %u channels", c0 + c1, cout);
     DN_CHECK(e, "wgrad3x3");

@@ -59,6 +59,7 @@ struct WgradArgs {
     int D, H, W;
     long long V;
     int cout;
+    int slabs;           // 1: slab kernel (default), 0: one gathered tile per tap
 };
 
 // kernels (denoise_kernels.cu)

@@ -488,6 +488,40 @@ struct SlabGeom {
     int S;             // stages in the ring (2..4)
 };
 
+// R consecutive padded positions q0 - (W+2) - 1 ... of plane z (batch item n)
+// of X = concat(upsampled src0, src1) into sS ([cin/8][R][16 B]); zero rows
+// for halo columns, rows outside the plane and planes outside the volume
+template <int CIN>
+__device__ __forceinline__ void slab_rows(uint32_t sS, const SlabGeom &g, int q0, int n, int z, const bf16 *src0,
+                                          const bf16 *src1, int c0, int c1, int up0, int D, int H, int W, int tid)
+{
+    const bool zok = (unsigned)z < (unsigned)D;
+    const int HW = H * W;
+    const int n0 = c0 >> 3;
+    for (int r = tid; r < g.R; r += CONV_THREADS) {
+        const int q = q0 - g.Wp - 1 + r;  // >= -Wp - 1
+        const int y = q >= 0 ? q / g.Wp : -1;
+        const int xp = q - y * g.Wp;
+        const bool ok = zok && y >= 0 && y < H && xp >= 1 && xp <= W;
+        const int x = xp - 1;
+        const bf16 *p0 = src0, *p1 = src1;
+        if (ok) {
+            if (c0) {
+                if (up0)
+                    p0 = src0 + ((((long long)n * (D >> 1) + (z >> 1)) * (H >> 1) + (y >> 1)) * (W >> 1) + (x >> 1)) * c0;
+                else
+                    p0 = src0 + (((long long)n * D + z) * HW + (long long)y * W + x) * c0;
+            }
+            p1 = src1 + (((long long)n * D + z) * HW + (long long)y * W + x) * c1;
+        }
+#pragma unroll
+        for (int c = 0; c < CIN / 8; c++) {
+            const bf16 *src = c < n0 ? p0 + c * 8 : p1 + (c - n0) * 8;
+            cp_async16(sS + (uint32_t)((c * g.R + r) * 16), src, ok ? 16u : 0u);
+        }
+    }
+}
+
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(CONV_THREADS) conv_slab_kernel(const ConvArgs a, const SlabGeom g)
 {
@@ -521,7 +555,6 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_slab_kernel(const ConvArgs 
     const long long nst = 3 * my_tiles;
     const int S = g.S, PF = S >= 3 ? 2 : 1;
     const int HW = a.H * a.W;
-    const int Hh = a.H >> 1, Wh = a.W >> 1, Dh = a.D >> 1;
 
     auto load_stage = [&](long long i) {
         const long long tile = blockIdx.x + (i / 3) * (long long)gridDim.x;
@@ -529,32 +562,8 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_slab_kernel(const ConvArgs 
         const uint32_t sS = sbase + (uint32_t)(i % S) * g.stage_bytes;
         const uint32_t sW = sS + g.slab_bytes;
         const long long plane = tile / g.T;  // n * D + z
-        const int q0 = (int)(tile % g.T) * TILE_M;
-        const int n = (int)(plane / a.D), z = (int)(plane % a.D) + dz;
-        const bool zok = (unsigned)z < (unsigned)a.D;
-        for (int r = tid; r < g.R; r += CONV_THREADS) {
-            const int q = q0 - g.Wp - 1 + r;  // >= -Wp - 1
-            const int y = q >= 0 ? q / g.Wp : -1;
-            const int xp = q - y * g.Wp;
-            const bool ok = zok && y >= 0 && y < a.H && xp >= 1 && xp <= a.W;
-            const int x = xp - 1;
-            const bf16 *p0 = a.src0, *p1 = a.src1;
-            if (ok) {
-                if (a.c0) {
-                    if (a.up0)
-                        p0 = a.src0 + ((((long long)n * Dh + (z >> 1)) * Hh + (y >> 1)) * Wh + (x >> 1)) * a.c0;
-                    else
-                        p0 = a.src0 + (((long long)n * a.D + z) * HW + (long long)y * a.W + x) * a.c0;
-                }
-                p1 = a.src1 + (((long long)n * a.D + z) * HW + (long long)y * a.W + x) * a.c1;
-            }
-            const int n0 = a.c0 >> 3;
-#pragma unroll
-            for (int c = 0; c < CIN / 8; c++) {
-                const bf16 *src = c < n0 ? p0 + c * 8 : p1 + (c - n0) * 8;
-                cp_async16(sS + (uint32_t)((c * g.R + r) * 16), src, ok ? 16u : 0u);
-            }
-        }
+        slab_rows<CIN>(sS, g, (int)(tile % g.T) * TILE_M, (int)(plane / a.D), (int)(plane % a.D) + dz, a.src0,
+                       a.src1, a.c0, a.c1, a.up0, a.D, a.H, a.W, tid);
         const bf16 *wsrc = a.w + (size_t)(9 * (dz + 1)) * CIN * COUT;
         for (int k = tid; k < (int)(9 * WT_BYTES / 16); k += CONV_THREADS) cp_async16(sW + k * 16, wsrc + k * 8, 16);
     };
@@ -651,9 +660,27 @@ static bool launch_slab(const ConvArgs &a, cudaStream_t s, cudaError_t &err)
     const uint32_t smem = (uint32_t)g.S * g.stage_bytes;
     err = cudaFuncSetAttribute(conv_slab_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return true;
-    int per_sm = 0;
-    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv_slab_kernel<CIN, COUT>, CONV_THREADS, smem);
+    // prefer the largest shared-memory carveout: several slab CTAs per SM
+    err = cudaFuncSetAttribute(conv_slab_kernel<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               (int)cudaSharedmemCarveoutMaxShared);
     if (err != cudaSuccess) return true;
+    // resident CTAs per SM from the SM's shared memory, registers and TMEM
+    // (512 columns); the occupancy calculator answers 1 for this kernel
+    int dev = 0, smem_sm = 0, reserved = 0, regs_sm = 0;
+    cudaFuncAttributes fa{};
+    if ((err = cudaGetDevice(&dev)) != cudaSuccess) return true;
+    if ((err = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess)
+        return true;
+    if ((err = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev)) != cudaSuccess)
+        return true;
+    if ((err = cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev)) != cudaSuccess)
+        return true;
+    if ((err = cudaFuncGetAttributes(&fa, conv_slab_kernel<CIN, COUT>)) != cudaSuccess) return true;
+    constexpr int TCOLS = 2 * COUT <= 32 ? 32 : (2 * COUT <= 64 ? 64 : (2 * COUT <= 128 ? 128 : 256));
+    int per_sm = smem_sm / (int)(smem + fa.sharedSizeBytes + reserved);
+    per_sm = std::min(per_sm, regs_sm / (std::max(1, fa.numRegs) * CONV_THREADS));
+    per_sm = std::min(per_sm, 512 / TCOLS);
+    per_sm = std::min(per_sm, 16);
     const long long grid = std::min<long long>(g.ntiles, (long long)std::max(1, per_sm) * std::max(1, a.sms));
     conv_slab_kernel<CIN, COUT><<<(unsigned)grid, CONV_THREADS, smem, s>>>(a, g);
     err = cudaGetLastError();
@@ -895,10 +922,172 @@ static cudaError_t launch_wgrad(const WgradArgs &a, int sms, cudaStream_t s)
     return cudaGetLastError();
 }
 
+// Weight gradient on slabs.  The 128-position tiles of the forward slab
+// kernel are the K dimension here: a CTA owns G taps of one dz (G = 9, 3 or 1,
+// as many as its registers hold: G * cout * cin / 32 accumulators per thread)
+// and walks tiles; per tile it stages the gradient rows (zero at halo
+// columns, so only real voxels count) and the dz slab of X once, and every
+// tap of the group reads the slab at its row offset.  Warps split the tile's
+// positions; partial sums are reduced in shared memory, then one fp32 atomic
+// per weight per CTA.
+template <int CIN, int COUT>
+struct WgsCfg {
+    static constexpr int MT = COUT / 16, NT = CIN / 8;
+    static constexpr int G = 9 * MT * NT * 4 <= 96 ? 9 : (3 * MT * NT * 4 <= 96 ? 3 : 1);
+    static constexpr uint32_t G_BYTES = TILE_M * COUT * 2;
+};
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(CONV_THREADS) wgrad_slab_kernel(const WgradArgs a, const SlabGeom g)
+{
+    using Cfg = WgsCfg<CIN, COUT>;
+    constexpr int MT = Cfg::MT, NT = Cfg::NT, G = Cfg::G;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const uint32_t stage_bytes = g.stage_bytes;  // G tile + slab
+    float *red = reinterpret_cast<float *>(smem + 2 * stage_bytes);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tap0 = blockIdx.y * G;
+    const int dz = tap0 / 9 - 1;
+    const uint32_t sbase = smem_u32(smem);
+    for (int i = tid; i < G * COUT * CIN; i += CONV_THREADS) red[i] = 0.0f;
+    const bool bias = a.db && tap0 <= 13 && 13 < tap0 + G;
+    const int HW = a.H * a.W;
+
+    float acc[G][MT][NT][4];
+#pragma unroll
+    for (int t = 0; t < G; t++)
+#pragma unroll
+        for (int m = 0; m < MT; m++)
+#pragma unroll
+            for (int n = 0; n < NT; n++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[t][m][n][j] = 0.0f;
+    float bsum = 0.0f;
+
+    auto load = [&](int st, long long tile) {
+        const uint32_t sG = sbase + (uint32_t)st * stage_bytes, sS = sG + Cfg::G_BYTES;
+        const long long plane = tile / g.T;
+        const int q0 = (int)(tile % g.T) * TILE_M;
+        const int n = (int)(plane / a.D), z = (int)(plane % a.D);
+        // gradient rows of the tile's positions (zero at halo columns / past the plane)
+        {
+            const int q = q0 + tid;
+            const int y = q / g.Wp, xp = q - (q / g.Wp) * g.Wp;
+            const bool ok = y < a.H && xp >= 1 && xp <= a.W;
+            const bf16 *gp = a.g + (ok ? ((long long)plane * HW + (long long)y * a.W + (xp - 1)) * COUT : 0);
+#pragma unroll
+            for (int c = 0; c < COUT / 8; c++)
+                cp_async16(sG + (uint32_t)((c * TILE_M + tid) * 16), gp + c * 8, ok ? 16u : 0u);
+        }
+        slab_rows<CIN>(sS, g, q0, n, z + dz, a.src0, a.src1, a.c0, a.c1, a.up0, a.D, a.H, a.W, tid);
+    };
+
+    long long tile = blockIdx.x;
+    if (tile < g.ntiles) load(0, tile);
+    cp_async_commit();
+    int st = 0;
+    for (; tile < g.ntiles; tile += gridDim.x) {
+        const long long nxt = tile + gridDim.x;
+        if (nxt < g.ntiles) load(st ^ 1, nxt);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        const uint32_t sG = sbase + (uint32_t)st * stage_bytes, sS = sG + Cfg::G_BYTES;
+        if (bias && tid < COUT) {
+            const bf16 *gs = reinterpret_cast<const bf16 *>(smem + (size_t)st * stage_bytes);
+            for (int r = 0; r < TILE_M; r++) bsum += __bfloat162float(gs[((tid >> 3) * TILE_M + r) * 8 + (tid & 7)]);
+        }
+#pragma unroll
+        for (int ks = 0; ks < 2; ks++) {
+            const int kb = warp * 32 + ks * 16;
+            uint32_t af[MT][4];
+#pragma unroll
+            for (int m = 0; m < MT; m++) {
+                const int vr = kb + (lane & 7) + ((lane >> 4) << 3);
+                const int ch = 2 * m + ((lane >> 3) & 1);
+                ldsm_x4_t(sG + (uint32_t)((ch * TILE_M + vr) * 16), af[m][0], af[m][1], af[m][2], af[m][3]);
+            }
+#pragma unroll
+            for (int t = 0; t < G; t++) {
+                const int tap = tap0 + t;
+                const int r0 = g.Wp + 1 + ((tap / 3) % 3 - 1) * g.Wp + (tap % 3 - 1);
+#pragma unroll
+                for (int n2 = 0; n2 < NT / 2; n2++) {
+                    uint32_t b0, b1, b2, b3;
+                    const int vx = r0 + kb + (lane & 7) + (((lane >> 3) & 1) << 3);
+                    const int cx = 2 * n2 + (lane >> 4);
+                    ldsm_x4_t(sS + (uint32_t)((cx * g.R + vx) * 16), b0, b1, b2, b3);
+#pragma unroll
+                    for (int m = 0; m < MT; m++) {
+                        mma_bf16(acc[t][m][2 * n2], af[m][0], af[m][1], af[m][2], af[m][3], b0, b1);
+                        mma_bf16(acc[t][m][2 * n2 + 1], af[m][0], af[m][1], af[m][2], af[m][3], b2, b3);
+                    }
+                }
+            }
+        }
+        __syncthreads();  // the stage is refilled on the next iteration
+        st ^= 1;
+    }
+    cp_async_wait_all();
+    const int gq = lane >> 2, tq = lane & 3;
+#pragma unroll
+    for (int t = 0; t < G; t++)
+#pragma unroll
+        for (int m = 0; m < MT; m++)
+#pragma unroll
+            for (int n = 0; n < NT; n++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int co = m * 16 + gq + 8 * (j >> 1), ci = n * 8 + 2 * tq + (j & 1);
+                    atomicAdd(&red[(t * COUT + co) * CIN + ci], acc[t][m][n][j]);
+                }
+    __syncthreads();
+    for (int i = tid; i < G * COUT * CIN; i += CONV_THREADS) {
+        const int t = i / (COUT * CIN), co = (i / CIN) % COUT, ci = i % CIN;
+        const float r = red[i];
+        if (r != 0.0f) atomicAdd(&a.dw[((size_t)co * 27 + tap0 + t) * CIN + ci], r);
+    }
+    if (bias && tid < COUT && bsum != 0.0f) atomicAdd(&a.db[tid], bsum);
+}
+
+template <int CIN, int COUT>
+static bool launch_wgrad_slab(const WgradArgs &a, int sms, cudaStream_t s, cudaError_t &err)
+{
+    using Cfg = WgsCfg<CIN, COUT>;
+    SlabGeom g{};
+    g.Wp = a.W + 2;
+    g.R = TILE_M + 2 * g.Wp + 2;
+    g.T = (a.H * g.Wp + TILE_M - 1) / TILE_M;
+    const long long nb = a.V / ((long long)a.D * a.H * a.W);
+    g.ntiles = nb * a.D * g.T;
+    g.slab_bytes = (uint32_t)g.R * CIN * 2;
+    g.stage_bytes = Cfg::G_BYTES + g.slab_bytes;
+    g.S = 2;
+    const uint32_t smem = 2 * g.stage_bytes + (uint32_t)Cfg::G * COUT * CIN * 4;
+    // with one tap per CTA a slab (R rows) costs more than the tap's own 128 rows
+    if (Cfg::G == 1 || smem > 227u * 1024u - 512u || g.ntiles == 0) return false;
+    err = cudaFuncSetAttribute(wgrad_slab_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return true;
+    err = cudaFuncSetAttribute(wgrad_slab_kernel<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               (int)cudaSharedmemCarveoutMaxShared);
+    if (err != cudaSuccess) return true;
+    const int groups = 27 / Cfg::G;
+    // about 4 CTAs per SM in total, at least 2 tiles per CTA
+    const long long per_group = std::max<long long>(
+        1, std::min<long long>((g.ntiles + 1) / 2, (4LL * std::max(1, sms) + groups - 1) / groups));
+    wgrad_slab_kernel<CIN, COUT><<<dim3((unsigned)per_group, groups), CONV_THREADS, smem, s>>>(a, g);
+    err = cudaGetLastError();
+    return true;
+}
+
 cudaError_t wgrad3x3(const WgradArgs &a, int cin, int sms, cudaStream_t s)
 {
-#define IAC_WG_CASE(CI, CO) \
-    if (cin == CI && a.cout == CO) return launch_wgrad<CI, CO>(a, sms, s);
+#define IAC_WG_CASE(CI, CO)                                               \
+    if (cin == CI && a.cout == CO) {                                      \
+        cudaError_t e = cudaSuccess;                                      \
+        if (a.slabs && launch_wgrad_slab<CI, CO>(a, sms, s, e)) return e; \
+        return launch_wgrad<CI, CO>(a, sms, s);                           \
+    }
     IAC_WG_CASE(16, 16)
     IAC_WG_CASE(16, 32)
     IAC_WG_CASE(32, 32)

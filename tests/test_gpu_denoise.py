@@ -64,13 +64,15 @@ def test_conv3x3_matches_oracle(ctx, rng, backend, c0, up0, c1, cout, dims):
     np.testing.assert_allclose(got, want, rtol=8e-3, atol=1e-5 * scale)
 
 
+@pytest.mark.parametrize("slabs", [True, False], ids=["slabs", "per_tap"])
 @pytest.mark.parametrize("c0,up0,c1,cout", [(0, 0, 16, 16), (0, 0, 16, 32), (0, 0, 32, 32), (0, 0, 32, 64),
                                             (0, 0, 64, 64), (64, 1, 32, 32), (32, 1, 16, 16)])
-def test_wgrad3x3_matches_oracle(ctx, rng, c0, up0, c1, cout):
+@pytest.mark.parametrize("dims", [(2, 8, 12, 16), (1, 6, 10, 64)])
+def test_wgrad3x3_matches_oracle(ctx, rng, c0, up0, c1, cout, slabs, dims):
     import torch
     from incohautocorrelate_b200 import capi
     from oracle import denoise_oracle as O
-    nb, D, H, W = 2, 8, 12, 16
+    nb, D, H, W = dims
     cin = c0 + c1
     s1_q, s1 = _bf16(rng.normal(0, 1, (nb, D, H, W, c1)))
     s0_q, s0 = (None, None)
@@ -80,7 +82,7 @@ def test_wgrad3x3_matches_oracle(ctx, rng, c0, up0, c1, cout):
     want_w, want_b = O.wgrad_layer(s0, s1, g, up0)
     dw = torch.zeros((cout, 27, cin), dtype=torch.float32, device="cuda")
     db = torch.zeros(cout, dtype=torch.float32, device="cuda")
-    capi.denoise_wgrad3x3(ctx, s0_q, c0, up0, s1_q, c1, g_q, cout, nb, D, H, W, dw, db)
+    capi.denoise_wgrad3x3(ctx, s0_q, c0, up0, s1_q, c1, g_q, cout, nb, D, H, W, dw, db, slabs=slabs)
     torch.cuda.synchronize()
     sw = np.abs(want_w).max()
     np.testing.assert_allclose(dw.cpu().numpy(), want_w, rtol=1e-4, atol=1e-5 * sw)
