@@ -202,7 +202,115 @@ __device__ __forceinline__ void put(const DenseArgs &a, const Window &w, unsigne
         global_put_pair(a, fs, ms, ss, v);
 }
 
-template <int INTERP>
+// round half away from zero as an int: (int)trunc(x + copysign(0.5 - 2^-25, x)).
+// The FP32 sum is correctly rounded and never reaches the next integer unless
+// x is at or past the half, so this equals round(x) for every |x| < 2^23
+// (checked exhaustively against roundf over all such floats).
+__device__ __forceinline__ int round_half_away(float x)
+{
+    return __float2int_rz(fadd(x, copysignf(0.49999997f, x)));
+}
+
+// component of (x, y, z) on axis K (0..2), or the runtime axis k when K < 0
+template <int K>
+__device__ __forceinline__ float axis(float x, float y, float z, int k)
+{
+    if (K == 0) return x;
+    if (K == 1) return y;
+    if (K == 2) return z;
+    return pick(x, y, z, k);
+}
+
+// the pairs (own pixel, staged pixels j0..TILE-1): the exact reference
+// arithmetic, per-thread run-length accumulation of consecutive pairs that
+// land in the same voxel.  KA/KB/KC: axis of q on mesh fs/ms/ss (-1: runtime).
+// CHECK: apply the per-pair MaxQ test (skipped when the two tiles' bounding
+// boxes are entirely within MaxQ, where every pair passes it).
+template <int INTERP, int KA, int KB, int KC, bool CHECK>
+__device__ __forceinline__ void cq_pairs(const DenseArgs &a, const Window &w, unsigned long long *win,
+                                         const float4 *sq, int j0, float k0, float k1, float k2, float Ia)
+{
+    int cur_f = 0, cur_m = 0, cur_s = 0;
+    unsigned long long acc[INTERP ? 8 : 1];
+#pragma unroll
+    for (int c = 0; c < (INTERP ? 8 : 1); c++) acc[c] = 0;
+    bool have = false;
+    for (int j = j0; j < DTILE; j++) {
+        const float4 b = sq[j];
+        const float pv = fmul(Ia, b.w);  // (double)(I_a*I_b) < 1e-37f  <=>  pv < 1e-37f
+        if (pv < 1e-37f) continue;
+        float qx = fsub(k0, b.x), qy = fsub(k1, b.y), qz = fsub(k2, b.z);
+        if (CHECK && fadd(fadd(fmul(qx, qx), fmul(qy, qy)), fmul(qz, qz)) > a.maxq2) continue;
+        qx = fmul(qx, a.vpdq);
+        qy = fmul(qy, a.vpdq);
+        qz = fmul(qz, a.vpdq);
+        const float qa = axis<KA>(qx, qy, qz, a.ka), qb = axis<KB>(qx, qy, qz, a.kb),
+                    qc = axis<KC>(qx, qy, qz, a.kc);
+        int f, m, s;
+        if (INTERP == 0) {
+            // (int)(round(q) + centre) of the reference, in integers
+            f = round_half_away(qa) + a.cab;
+            m = round_half_away(qb) + a.cab;
+            s = round_half_away(qc) + a.cc;
+        } else {
+            f = __float2int_rd(qa) + a.cab;
+            m = __float2int_rd(qb) + a.cab;
+            s = __float2int_rd(qc) + a.cc;
+        }
+        if (!have || f != cur_f || m != cur_m || s != cur_s) {
+            if (have) {
+                if (INTERP == 0) {
+                    put(a, w, win, cur_f, cur_m, cur_s, acc[0]);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 8; c++)
+                        put(a, w, win, cur_f + (c >> 2), cur_m + ((c >> 1) & 1), cur_s + (c & 1), acc[c]);
+                }
+            }
+            have = true;
+            cur_f = f;
+            cur_m = m;
+            cur_s = s;
+#pragma unroll
+            for (int c = 0; c < (INTERP ? 8 : 1); c++) acc[c] = 0;
+        }
+        if (INTERP == 0) {
+            acc[0] += a.mult_int ? scaled_floor(pv, a.mult_int) : d2u64(dmul((double)pv, a.mult));
+        } else {
+            const double vm = dmul((double)pv, a.mult);
+            // IAC/kernel.cl:139-179: Sep = 1 - (q - floor q) in float
+            const double sf = (double)fsub(1.0f, fsub(qa, floorf(qa)));
+            const double sm = (double)fsub(1.0f, fsub(qb, floorf(qb)));
+            const double sz = (double)fsub(1.0f, fsub(qc, floorf(qc)));
+            const double xf[2] = {sf, dsub(1.0, sf)}, yf[2] = {sm, dsub(1.0, sm)}, zf[2] = {sz, dsub(1.0, sz)};
+#pragma unroll
+            for (int c = 0; c < 8; c++)
+                acc[c] += d2u64(dmul(vm, dmul(dmul(xf[c >> 2], yf[(c >> 1) & 1]), zf[c & 1])));
+        }
+    }
+    if (have) {
+        if (INTERP == 0) {
+            put(a, w, win, cur_f, cur_m, cur_s, acc[0]);
+        } else {
+#pragma unroll
+            for (int c = 0; c < 8; c++)
+                put(a, w, win, cur_f + (c >> 2), cur_m + ((c >> 1) & 1), cur_s + (c & 1), acc[c]);
+        }
+    }
+}
+
+// upper bound of |k_a - k_b| over two boxes is below MaxQ with a margin that
+// covers the FP32 rounding of the per-pair test (every pair passes it)
+__device__ __forceinline__ bool boxes_within(const float4 a0, const float4 a1, const float4 b0, const float4 b1,
+                                             float maxq)
+{
+    const float dx = fmaxf(a1.x - b0.x, b1.x - a0.x);
+    const float dy = fmaxf(a1.y - b0.y, b1.y - a0.y);
+    const float dz = fmaxf(a1.z - b0.z, b1.z - a0.z);
+    return dx * dx + dy * dy + dz * dz < maxq * maxq * 0.9999f;
+}
+
+template <int INTERP, int KA, int KB, int KC>
 __global__ void __launch_bounds__(DTILE) cq_small_kernel(const DenseArgs a)
 {
     __shared__ float4 sq[DTILE];
@@ -210,7 +318,6 @@ __global__ void __launch_bounds__(DTILE) cq_small_kernel(const DenseArgs a)
     __shared__ unsigned long long s_pair;
     __shared__ unsigned long long s_self[DTILE / 32];
     const uint32_t T = a.ntiles;
-    const float cabf = (float)a.cab, ccf = (float)a.cc;
     for (;;) {
         if (threadIdx.x == 0) s_pair = atomicAdd(a.queue, 1ull);
         __syncthreads();
@@ -223,6 +330,7 @@ __global__ void __launch_bounds__(DTILE) cq_small_kernel(const DenseArgs a)
             __syncthreads();
             continue;
         }
+        const bool check = !boxes_within(p0, p1, q0, q1, a.maxq);
         // window over the q range of the pair (P - Q), one voxel of margin
         Window w;
         {
@@ -262,73 +370,10 @@ __global__ void __launch_bounds__(DTILE) cq_small_kernel(const DenseArgs a)
                     self = a.mult_int ? scaled_floor(sv, a.mult_int) : d2u64(dmul((double)sv, a.mult));
             }
             const int j0 = (P == Q) ? threadIdx.x + 1 : 0;
-            int cur_f = 0, cur_m = 0, cur_s = 0;
-            unsigned long long acc[INTERP ? 8 : 1];
-#pragma unroll
-            for (int c = 0; c < (INTERP ? 8 : 1); c++) acc[c] = 0;
-            bool have = false;
-            for (int j = j0; j < DTILE; j++) {
-                const float4 b = sq[j];
-                const float pv = fmul(Ia, b.w);  // (double)(I_a*I_b) < 1e-37f  <=>  pv < 1e-37f
-                if (pv < 1e-37f) continue;
-                float qx = fsub(k0, b.x), qy = fsub(k1, b.y), qz = fsub(k2, b.z);
-                if (fadd(fadd(fmul(qx, qx), fmul(qy, qy)), fmul(qz, qz)) > a.maxq2) continue;
-                qx = fmul(qx, a.vpdq);
-                qy = fmul(qy, a.vpdq);
-                qz = fmul(qz, a.vpdq);
-                const float qa = pick(qx, qy, qz, a.ka), qb = pick(qx, qy, qz, a.kb),
-                            qc = pick(qx, qy, qz, a.kc);
-                int f, m, s;
-                if (INTERP == 0) {
-                    f = (int)fadd(round_away_f(qa), cabf);
-                    m = (int)fadd(round_away_f(qb), cabf);
-                    s = (int)fadd(round_away_f(qc), ccf);
-                } else {
-                    f = (int)fadd(floorf(qa), cabf);
-                    m = (int)fadd(floorf(qb), cabf);
-                    s = (int)fadd(floorf(qc), ccf);
-                }
-                if (!have || f != cur_f || m != cur_m || s != cur_s) {
-                    if (have) {
-                        if (INTERP == 0) {
-                            put(a, w, win, cur_f, cur_m, cur_s, acc[0]);
-                        } else {
-#pragma unroll
-                            for (int c = 0; c < 8; c++)
-                                put(a, w, win, cur_f + (c >> 2), cur_m + ((c >> 1) & 1), cur_s + (c & 1), acc[c]);
-                        }
-                    }
-                    have = true;
-                    cur_f = f;
-                    cur_m = m;
-                    cur_s = s;
-#pragma unroll
-                    for (int c = 0; c < (INTERP ? 8 : 1); c++) acc[c] = 0;
-                }
-                if (INTERP == 0) {
-                    acc[0] += a.mult_int ? scaled_floor(pv, a.mult_int) : d2u64(dmul((double)pv, a.mult));
-                } else {
-                    const double vm = dmul((double)pv, a.mult);
-                    // IAC/kernel.cl:139-179: Sep = 1 - (q - floor q) in float
-                    const double sf = (double)fsub(1.0f, fsub(qa, floorf(qa)));
-                    const double sm = (double)fsub(1.0f, fsub(qb, floorf(qb)));
-                    const double sz = (double)fsub(1.0f, fsub(qc, floorf(qc)));
-                    const double xf[2] = {sf, dsub(1.0, sf)}, yf[2] = {sm, dsub(1.0, sm)},
-                                 zf[2] = {sz, dsub(1.0, sz)};
-#pragma unroll
-                    for (int c = 0; c < 8; c++)
-                        acc[c] += d2u64(dmul(vm, dmul(dmul(xf[c >> 2], yf[(c >> 1) & 1]), zf[c & 1])));
-                }
-            }
-            if (have) {
-                if (INTERP == 0) {
-                    put(a, w, win, cur_f, cur_m, cur_s, acc[0]);
-                } else {
-#pragma unroll
-                    for (int c = 0; c < 8; c++)
-                        put(a, w, win, cur_f + (c >> 2), cur_m + ((c >> 1) & 1), cur_s + (c & 1), acc[c]);
-                }
-            }
+            if (check)
+                cq_pairs<INTERP, KA, KB, KC, true>(a, w, win, sq, j0, k0, k1, k2, Ia);
+            else
+                cq_pairs<INTERP, KA, KB, KC, false>(a, w, win, sq, j0, k0, k1, k2, Ia);
         }
         // self pairs of a diagonal tile: once, at the centre
         for (int o = 16; o; o >>= 1) self += __shfl_xor_sync(0xffffffffu, self, o);
@@ -508,10 +553,32 @@ iac_status iac_cq_small(iac_ctx *ctx, const float *d_I, const float *d_kmap, uin
     a.kb = (int)sh->k_b;
     a.kc = (int)sh->k_c;
     const int grid = ctx->sm_count * 8;
-    if (interp == 0)
-        cq_small_kernel<0><<<grid, DTILE, 0, as_stream(stream)>>>(a);
-    else
-        cq_small_kernel<1><<<grid, DTILE, 0, as_stream(stream)>>>(a);
+    // the axis mapping is a permutation for every real detector: one
+    // instantiation per permutation, a runtime-mapped one otherwise
+    const int perm = (a.ka == 0 && a.kb == 1 && a.kc == 2)   ? 0
+                     : (a.ka == 0 && a.kb == 2 && a.kc == 1) ? 1
+                     : (a.ka == 1 && a.kb == 0 && a.kc == 2) ? 2
+                     : (a.ka == 1 && a.kb == 2 && a.kc == 0) ? 3
+                     : (a.ka == 2 && a.kb == 0 && a.kc == 1) ? 4
+                     : (a.ka == 2 && a.kb == 1 && a.kc == 0) ? 5
+                                                             : 6;
+    cudaStream_t s = as_stream(stream);
+#define IAC_CQ_LAUNCH(I)                                                          \
+    switch (perm) {                                                               \
+    case 0: cq_small_kernel<I, 0, 1, 2><<<grid, DTILE, 0, s>>>(a); break;         \
+    case 1: cq_small_kernel<I, 0, 2, 1><<<grid, DTILE, 0, s>>>(a); break;         \
+    case 2: cq_small_kernel<I, 1, 0, 2><<<grid, DTILE, 0, s>>>(a); break;         \
+    case 3: cq_small_kernel<I, 1, 2, 0><<<grid, DTILE, 0, s>>>(a); break;         \
+    case 4: cq_small_kernel<I, 2, 0, 1><<<grid, DTILE, 0, s>>>(a); break;         \
+    case 5: cq_small_kernel<I, 2, 1, 0><<<grid, DTILE, 0, s>>>(a); break;         \
+    default: cq_small_kernel<I, -1, -1, -1><<<grid, DTILE, 0, s>>>(a); break;     \
+    }
+    if (interp == 0) {
+        IAC_CQ_LAUNCH(0)
+    } else {
+        IAC_CQ_LAUNCH(1)
+    }
+#undef IAC_CQ_LAUNCH
     IAC_LAUNCHED(ctx);
     IAC_CUDA(cudaGetLastError());
     return IAC_OK;
