@@ -472,8 +472,8 @@ def denoise_conv3x3(ctx, backend, d_src0, c0, up0, d_src1, c1, d_wtile, d_bias, 
 
 
 def denoise_wgrad3x3(ctx, d_src0, c0, up0, d_src1, c1, d_grad, cout, nb, D, H, W, d_dw, d_db=None,
-                     stream=None, slabs=True):
-    check(lib().iac_denoise_wgrad3x3(ctx._h, int(bool(slabs)), _ptr(d_src0), int(c0), int(up0), _ptr(d_src1),
+                     stream=None, slabs=1):
+    check(lib().iac_denoise_wgrad3x3(ctx._h, int(slabs), _ptr(d_src0), int(c0), int(up0), _ptr(d_src1),
                                      int(c1),
                                      _ptr(d_grad), int(cout), int(nb), int(D), int(H), int(W),
                                      _ptr(d_dw), _ptr(d_db), _ptr(stream)))

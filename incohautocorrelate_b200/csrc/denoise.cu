@@ -53,6 +53,7 @@ struct iac_denoiser {
     // activations
     bf16 *e1a = nullptr, *s1 = nullptr, *p1 = nullptr, *e2a = nullptr, *s2 = nullptr, *p2 = nullptr;
     bf16 *b1 = nullptr, *b2 = nullptr, *d2a = nullptr, *d2b = nullptr, *d1a = nullptr, *d1b = nullptr;
+    bf16 *cat1 = nullptr, *cat2 = nullptr;  // decoder inputs: up(d2b) ++ s1, up(b2) ++ s2
     // gradients
     bf16 *gA = nullptr, *gB = nullptr, *gcat1 = nullptr, *gskip1 = nullptr;  // full resolution
     bf16 *hA = nullptr, *hB = nullptr, *gcat2 = nullptr, *gskip2 = nullptr;  // half
@@ -167,7 +168,15 @@ iac_status wgrad(iac_denoiser *dn, int l, const bf16 *src0, const bf16 *src1, co
     a.W = W;
     a.V = V;
     a.cout = SPECS[l].cout;
-    a.slabs = dn->backend != BACKEND_TC_TAP;
+    // tcgen05 where it measured faster (48 input or 64 output channels),
+    // mma.sync on slabs elsewhere
+    if (dn->backend == BACKEND_TC_TAP)
+        a.slabs = 0;
+    else if (dn->backend == BACKEND_TC_SLAB && (cin == 48 || SPECS[l].cout == 64))
+        a.slabs = 2;
+    else
+        a.slabs = 1;
+    a.counters = dn->ctx->d_counters;
     DN_CHECK(wgrad3x3(a, cin, dn->ctx->sm_count, s), "denoiser weight gradient");
     return IAC_OK;
 }
@@ -221,9 +230,13 @@ iac_status run_forward(iac_denoiser *dn, const float *x, uint32_t nb, uint32_t D
     DN_CHECK(avgpool2(dn->s2, dn->p2, 32, D2, H2, W2, nb, s), "pool 2");
     DN_CHECK(conv3x3(conv_args(dn, 4, nullptr, dn->p2, dn->b1, D4, H4, W4, V4), 32, 64, be, s), "layer 4");
     DN_CHECK(conv3x3(conv_args(dn, 5, nullptr, dn->b1, dn->b2, D4, H4, W4, V4), 64, 64, be, s), "layer 5");
-    DN_CHECK(conv3x3(conv_args(dn, 6, dn->b2, dn->s2, dn->d2a, D2, H2, W2, V2), 96, 32, be, s), "layer 6");
+    // the decoder inputs are materialised (64 + 32 and 32 + 16 channels), so the
+    // 3x3x3 kernels read plain tensors through TMA
+    DN_CHECK(concat_up(dn->b2, 64, dn->s2, 32, dn->cat2, D2, H2, W2, nb, s), "concat 2");
+    DN_CHECK(conv3x3(conv_args(dn, 6, nullptr, dn->cat2, dn->d2a, D2, H2, W2, V2), 96, 32, be, s), "layer 6");
     DN_CHECK(conv3x3(conv_args(dn, 7, nullptr, dn->d2a, dn->d2b, D2, H2, W2, V2), 32, 32, be, s), "layer 7");
-    DN_CHECK(conv3x3(conv_args(dn, 8, dn->d2b, dn->s1, dn->d1a, D, H, W, V), 48, 16, be, s), "layer 8");
+    DN_CHECK(concat_up(dn->d2b, 32, dn->s1, 16, dn->cat1, D, H, W, nb, s), "concat 1");
+    DN_CHECK(conv3x3(conv_args(dn, 8, nullptr, dn->cat1, dn->d1a, D, H, W, V), 48, 16, be, s), "layer 8");
     DN_CHECK(conv3x3(conv_args(dn, 9, nullptr, dn->d1a, dn->d1b, D, H, W, V), 16, 16, be, s), "layer 9");
     return IAC_OK;
 }
@@ -303,6 +316,8 @@ iac_status iac_denoise_create(iac_ctx *ctx, uint32_t max_batch, uint32_t D, uint
     dn->p2 = (bf16 *)A(V4 * 32 * b);
     dn->b1 = (bf16 *)A(V4 * 64 * b);
     dn->b2 = (bf16 *)A(V4 * 64 * b);
+    dn->cat1 = (bf16 *)A(V * 48 * b);
+    dn->cat2 = (bf16 *)A(V2 * 96 * b);
     dn->gA = (bf16 *)A(V * 16 * b);
     dn->gB = (bf16 *)A(V * 16 * b);
     dn->gcat1 = (bf16 *)A(V * 48 * b);
@@ -404,7 +419,7 @@ iac_status iac_denoise_forward(iac_denoiser *dn, const float *d_in, uint32_t nb,
     h.out = d_out;
     h.V = (long long)nb * D * H * W;
     DN_CHECK(head(h, dn->ctx->sm_count, s), "denoiser head");
-    dn->ctx->launches += 14;
+    dn->ctx->launches += 16;
     return IAC_OK;
 }
 
@@ -441,7 +456,7 @@ iac_status iac_denoise_backward(iac_denoiser *dn, const float *d_in, const float
     if ((st = dgrad(dn, 9, dn->gA, dn->gB, D, H, W, V, s)) != IAC_OK) return st;
     DN_CHECK(relu_mask(dn->gB, dn->d1a, dn->gB, V * 16, s), "mask 8");
     // layer 8: X = up(d2b) ++ s1
-    if ((st = wgrad(dn, 8, dn->d2b, dn->s1, dn->gB, D, H, W, V, s)) != IAC_OK) return st;
+    if ((st = wgrad(dn, 8, nullptr, dn->cat1, dn->gB, D, H, W, V, s)) != IAC_OK) return st;
     if ((st = dgrad(dn, 8, dn->gB, dn->gcat1, D, H, W, V, s)) != IAC_OK) return st;
     DN_CHECK(split_concat_grad(dn->gcat1, 32, 16, dn->d2b, dn->hA, dn->gskip1, D, H, W, nb, s), "split 1");
     // layer 7: X = d2a
@@ -449,7 +464,7 @@ iac_status iac_denoise_backward(iac_denoiser *dn, const float *d_in, const float
     if ((st = dgrad(dn, 7, dn->hA, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
     DN_CHECK(relu_mask(dn->hB, dn->d2a, dn->hB, V2 * 32, s), "mask 6");
     // layer 6: X = up(b2) ++ s2
-    if ((st = wgrad(dn, 6, dn->b2, dn->s2, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
+    if ((st = wgrad(dn, 6, nullptr, dn->cat2, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
     if ((st = dgrad(dn, 6, dn->hB, dn->gcat2, D2, H2, W2, V2, s)) != IAC_OK) return st;
     DN_CHECK(split_concat_grad(dn->gcat2, 64, 32, dn->b2, dn->qA, dn->gskip2, D2, H2, W2, nb, s), "split 2");
     // layer 5: X = b1
@@ -476,7 +491,7 @@ iac_status iac_denoise_backward(iac_denoiser *dn, const float *d_in, const float
     DN_CHECK(wgrad3x3_first(d_in, dn->gB, dn->g + dn->p_off[0], dn->g + dn->p_off[0] + 16 * 27, D, H, W, V,
                             dn->ctx->sm_count, s),
              "layer 0 weight gradient");
-    dn->ctx->launches += 48;
+    dn->ctx->launches += 50;
     if (h_loss) {
         double t = 0;
         DN_CHECK(cudaMemcpyAsync(&t, dn->d_loss, 8, cudaMemcpyDeviceToHost, s), "loss");
@@ -568,6 +583,7 @@ iac_status iac_denoise_wgrad3x3(iac_ctx *ctx, int slabs, const uint16_t *d_src0,
     a.V = (long long)nb * D * H * W;
     a.cout = (int)cout;
     a.slabs = slabs;
+    a.counters = ctx->d_counters;
     const cudaError_t e = wgrad3x3(a, (int)(c0 + c1), ctx->sm_count, (cudaStream_t)stream);
     IAC_REQUIRE(e != cudaErrorInvalidValue, "no 3x3x3 weight-gradient kernel for %u -> %u channels", c0 + c1, cout);
     DN_CHECK(e, "wgrad3x3");

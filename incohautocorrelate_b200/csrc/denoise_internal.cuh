@@ -59,7 +59,8 @@ struct WgradArgs {
     int D, H, W;
     long long V;
     int cout;
-    int slabs;           // 1: slab kernel (default), 0: one gathered tile per tap
+    int slabs;           // 2: tcgen05 + TMA, 1: slab kernel (mma.sync), 0: one gathered tile per tap
+    DeviceCounters *counters;
 };
 
 // kernels (denoise_kernels.cu)
@@ -73,6 +74,8 @@ cudaError_t avgpool2(const bf16 *x, bf16 *y, int C, int D, int H, int W, int nb,
 cudaError_t relu_mask(const bf16 *g, const bf16 *y, bf16 *out, long long n, cudaStream_t s);
 cudaError_t split_concat_grad(const bf16 *gcat, int c0, int c1, const bf16 *y0, bf16 *g0,
                               bf16 *g1, int D, int H, int W, int nb, cudaStream_t s);
+cudaError_t concat_up(const bf16 *src0, int c0, const bf16 *src1, int c1, bf16 *out, int D, int H, int W, int nb,
+                      cudaStream_t s);
 cudaError_t pool_grad_mask(const bf16 *gskip, const bf16 *gpool, const bf16 *y, bf16 *out, int C,
                            int D, int H, int W, int nb, cudaStream_t s);
 

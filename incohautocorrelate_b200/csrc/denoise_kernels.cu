@@ -26,9 +26,12 @@
 //   backend 1, mma.sync.m16n8k16: four warps of 32 voxels x cout each.
 // Backend 0 (the default, conv_slab_kernel) stages each input row once per
 // (tile, dz) instead of once per tap; backend 2 is the per-tap tcgen05 form.
+#include <cuda.h>
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "denoise_internal.cuh"
 
@@ -282,7 +285,7 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_tc_kernel(const ConvArgs a)
 {
     using Cfg = TcCfg<CIN, COUT>;
     static_assert(COUT % 16 == 0 && COUT <= 256 && CIN % 16 == 0, "tcgen05 M=128 needs N % 16 == 0");
-    extern __shared__ __align__(128) unsigned char smem[];
+    extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t mbar[Cfg::S];
     __shared__ uint32_t s_tmem;
     __shared__ int s_err;
@@ -386,7 +389,7 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_mma_kernel(const ConvArgs a
 {
     using Cfg = MmaCfg<CIN, COUT>;
     constexpr int NT = COUT / 8;
-    extern __shared__ __align__(128) unsigned char smem[];
+    extern __shared__ __align__(1024) unsigned char smem[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const long long v0 = (long long)blockIdx.x * TILE_M;
     const Vox q = decode(v0 + tid, a.D, a.H, a.W, a.V);
@@ -528,7 +531,7 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_slab_kernel(const ConvArgs 
     constexpr uint32_t TCOLS = 2 * COUT <= 32 ? 32 : (2 * COUT <= 64 ? 64 : (2 * COUT <= 128 ? 128 : 256));
     constexpr uint32_t IDESC = idesc_bf16(TILE_M, COUT);
     constexpr uint32_t WT_BYTES = COUT * CIN * 2;  // one tap's weight tile
-    extern __shared__ __align__(128) unsigned char smem[];
+    extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t mbar[4];
     __shared__ __align__(8) uint64_t accbar[2];
     __shared__ uint32_t s_tmem;
@@ -687,12 +690,316 @@ static bool launch_slab(const ConvArgs &a, cudaStream_t s, cudaError_t &err)
     return true;
 }
 
+// --------------------------------------------------------------------------
+// backend 0 with plain inputs: warp-specialised, TMA-fed tcgen05 convolution.
+//
+// Same padded-position tiles and slab operands as conv_slab_kernel, but a
+// stage is filled by the Tensor Memory Accelerator: one 5-D box (8 channels x
+// W+2 columns x NR rows x 1 plane x 1 item, starting at column -1) per
+// 8-channel chunk, whose out-of-volume elements (halo columns, rows above and
+// below the plane, planes outside the volume) arrive as zeros.  Warp 4 (one
+// lane) produces stages, warp 5 (one lane) issues tcgen05.mma, warps 0-3 drain
+// the double-buffered TMEM accumulator; the roles meet only at mbarriers
+// (full/empty per stage, full/empty per accumulator), every wait bounded.
+// Weights stay resident in shared memory when all 27 taps fit, else each
+// stage carries its dz's nine taps (one bulk copy).
+// --------------------------------------------------------------------------
+struct TmaGeom {
+    int Wp, NR;             // padded row length, padded rows per slab
+    int T;                  // tiles per plane
+    long long ntiles;
+    uint32_t plane_bytes;   // one 8-channel chunk of a slab (multiple of 128)
+    uint32_t box_bytes;     // bytes one box delivers (16 * Wp * NR)
+    uint32_t slab_bytes;    // cin/8 planes
+    uint32_t wstage_bytes;  // weights carried per stage (0: resident)
+    uint32_t stage_bytes;
+    uint32_t wres_bytes;    // shared memory reserved for resident weights (0: per stage)
+    uint32_t wcopy_bytes;   // bytes of the resident weights copied
+    int S;
+};
+
+__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            int c4, uint32_t mbar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5, %6}], [%7];\n" ::"r"(dst),
+        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(mbar)
+        : "memory");
+}
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t mbar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(mbar)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mbar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(mbar) : "memory");
+}
+// bounded wait that also gives up once another role has flagged an error
+__device__ __forceinline__ bool mbar_wait_flag(uint32_t addr, uint32_t parity, volatile int *err)
+{
+    for (uint32_t i = 0; i < (1u << 20); i++) {
+        if (mbar_try_wait(addr, parity)) return true;
+        if (*err) return false;
+    }
+    *err = 1;
+    return false;
+}
+
+__device__ __forceinline__ int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+constexpr int TMA_THREADS = 192;
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(TMA_THREADS) conv_tma_kernel(const __grid_constant__ CUtensorMap xmap,
+                                                               const ConvArgs a, const TmaGeom g)
+{
+    constexpr uint32_t TCOLS = 2 * COUT <= 32 ? 32 : (2 * COUT <= 64 ? 64 : (2 * COUT <= 128 ? 128 : 256));
+    constexpr uint32_t IDESC = idesc_bf16(TILE_M, COUT);
+    constexpr uint32_t WT_BYTES = COUT * CIN * 2;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t full[8], empty[8], accfull[2], accempty[2], wfull;
+    __shared__ uint32_t s_tmem;
+    __shared__ volatile int s_err;
+    __shared__ long long s_issued, s_consumed;  // stages loaded by the producer / multiplied
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t sbase = smem_u32(smem);
+    const uint32_t wbase = sbase;                   // resident weights
+    const uint32_t stbase = sbase + g.wres_bytes;   // stages
+    if (tid == 0) {
+        for (int k = 0; k < g.S; k++) {
+            mbar_init(smem_u32(&full[k]), 1);
+            mbar_init(smem_u32(&empty[k]), 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(smem_u32(&accfull[b]), 1);
+            mbar_init(smem_u32(&accempty[b]), 4);
+        }
+        mbar_init(smem_u32(&wfull), 1);
+        fence_mbar_init();
+        s_err = 0;
+        s_issued = 0;
+        s_consumed = 0;
+    }
+    if (warp == 5) {
+        tmem_alloc(smem_u32(&s_tmem), TCOLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const long long my_tiles =
+        blockIdx.x < g.ntiles ? (g.ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+    const long long nst = 3 * my_tiles;
+    const int HW = a.H * a.W;
+
+    if (warp == 4) {
+        if (lane == 0) {  // producer
+            if (g.wres_bytes) {
+                mbar_expect_tx(smem_u32(&wfull), g.wcopy_bytes);
+                bulk_load(wbase, a.w, g.wcopy_bytes, smem_u32(&wfull));
+            }
+            for (long long i = 0; i < nst; i++) {
+                const int slot = (int)(i % g.S);
+                if (i >= g.S && !mbar_wait_flag(smem_u32(&empty[slot]), (uint32_t)(((i / g.S) - 1) & 1), &s_err))
+                    break;
+                const long long tile = blockIdx.x + (i / 3) * (long long)gridDim.x;
+                const int dz = (int)(i % 3) - 1;
+                const long long plane = tile / g.T;
+                const int q0 = (int)(tile % g.T) * TILE_M;
+                const int n = (int)(plane / a.D), z = (int)(plane % a.D) + dz;
+                const int y_lo = floor_div(q0 - g.Wp - 1, g.Wp);
+                const uint32_t st = stbase + (uint32_t)slot * g.stage_bytes;
+                const uint32_t fb = smem_u32(&full[slot]);
+                mbar_expect_tx(fb, (CIN / 8) * g.box_bytes + g.wstage_bytes);
+#pragma unroll
+                for (int c = 0; c < CIN / 8; c++) tma_load_5d(st + c * g.plane_bytes, &xmap, c * 8, -1, y_lo, z, n, fb);
+                if (g.wstage_bytes)
+                    bulk_load(st + g.slab_bytes, a.w + (size_t)(9 * (dz + 1)) * CIN * COUT, g.wstage_bytes, fb);
+                s_issued = i + 1;
+            }
+        }
+    } else if (warp == 5) {
+        if (lane == 0) {  // MMA issuer
+            bool ok = !g.wres_bytes || mbar_wait_flag(smem_u32(&wfull), 0, &s_err);
+            for (long long i = 0; ok && i < nst; i++) {
+                const int slot = (int)(i % g.S);
+                if (!mbar_wait_flag(smem_u32(&full[slot]), (uint32_t)((i / g.S) & 1), &s_err)) break;
+                const long long k = i / 3;
+                const int dzi = (int)(i % 3);
+                if (dzi == 0 && k >= 2 &&
+                    !mbar_wait_flag(smem_u32(&accempty[k & 1]), (uint32_t)(((k >> 1) - 1) & 1), &s_err))
+                    break;
+                tc_fence_after();
+                const long long tile = blockIdx.x + k * (long long)gridDim.x;
+                const int q0 = (int)(tile % g.T) * TILE_M;
+                const int rel = q0 - floor_div(q0 - g.Wp - 1, g.Wp) * g.Wp;  // q0 within the slab
+                const uint32_t st = stbase + (uint32_t)slot * g.stage_bytes;
+                const uint32_t wt = g.wres_bytes ? wbase + (uint32_t)(9 * dzi) * WT_BYTES : st + g.slab_bytes;
+                const uint32_t dcol = tmem + (uint32_t)((k & 1) * COUT);
+#pragma unroll 1
+                for (int t = 0; t < 9; t++) {
+                    const uint32_t r0 = (uint32_t)(rel + (t / 3 - 1) * g.Wp + (t % 3 - 1));
+#pragma unroll
+                    for (int kk = 0; kk < CIN / 16; kk++) {
+                        const uint64_t da = smem_desc(st + (uint32_t)(2 * kk) * g.plane_bytes + r0 * 16, g.plane_bytes, 128);
+                        const uint64_t db = smem_desc(wt + t * WT_BYTES + kk * 2 * (COUT * 16), COUT * 16, 128);
+                        umma_bf16(dcol, da, db, IDESC, (dzi > 0 || t > 0 || kk > 0) ? 1u : 0u);
+                    }
+                }
+                umma_commit(smem_u32(&empty[slot]));
+                if (dzi == 2) umma_commit(smem_u32(&accfull[k & 1]));
+                s_consumed = i + 1;
+            }
+        }
+    } else {  // epilogue: warps 0-3 own TMEM lanes 32w .. 32w+31
+        for (long long k = 0; k < my_tiles; k++) {
+            if (!mbar_wait_flag(smem_u32(&accfull[k & 1]), (uint32_t)((k >> 1) & 1), &s_err)) break;
+            tc_fence_after();
+            const long long tile = blockIdx.x + k * (long long)gridDim.x;
+            const long long plane = tile / g.T;
+            const int q = (int)(tile % g.T) * TILE_M + tid;
+            const int y = q / g.Wp, xp = q - (q / g.Wp) * g.Wp;
+            const bool valid = y < a.H && xp >= 1 && xp <= a.W;
+            const long long v = plane * HW + (long long)y * a.W + (xp - 1);
+            uint32_t r[COUT];
+#pragma unroll
+            for (int c = 0; c < COUT; c += 16) {
+                uint32_t (&rr)[16] = *reinterpret_cast<uint32_t(*)[16]>(&r[c]);
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((k & 1) * COUT + c), rr);
+            }
+            tmem_wait_ld();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&accempty[k & 1]));
+            if (valid) {
+#pragma unroll
+                for (int c = 0; c < COUT; c += 8) {
+                    float f[8];
+#pragma unroll
+                    for (int j = 0; j < 8; j++) f[j] = __uint_as_float(r[c + j]);
+                    store8(a, COUT, v, c, f);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (s_err) {
+        // after an error: let the copies and MMAs already issued finish (bounded)
+        // before the shared memory and TMEM are released
+        if (tid == 0) {
+            if (a.counters) atomicAdd(&a.counters->timeouts, 1ull);
+            for (long long i = s_consumed; i < s_issued; i++)
+                mbar_wait(smem_u32(&full[i % g.S]), (uint32_t)((i / g.S) & 1));
+            if (s_consumed > 0) {
+                const long long i = s_consumed - 1;
+                mbar_wait(smem_u32(&empty[i % g.S]), (uint32_t)((i / g.S) & 1));
+            }
+        }
+        __syncthreads();
+    }
+    if (warp == 5) {
+        tc_fence_after();
+        tmem_dealloc(tmem, TCOLS);
+    }
+}
+
+// cuTensorMapEncodeTiled from the driver (no link-time dependency on libcuda)
+static PFN_cuTensorMapEncodeTiled tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(p);
+    });
+    return fn;
+}
+
+template <int CIN, int COUT>
+static bool launch_tma(const ConvArgs &a, cudaStream_t s, cudaError_t &err)
+{
+    if (a.c0 != 0 || a.W + 2 > 256 || a.D < 1) return false;  // TMA boxes: plain input, rows of <= 256
+    PFN_cuTensorMapEncodeTiled enc = tensor_map_encoder();
+    if (!enc) return false;
+    if ((reinterpret_cast<uintptr_t>(a.src1) & 15) || (reinterpret_cast<uintptr_t>(a.w) & 15)) return false;
+    TmaGeom g{};
+    g.Wp = a.W + 2;
+    g.NR = 3 + (130 + g.Wp - 1) / g.Wp;  // covers rows y_lo .. y_lo + NR - 1 of every tile
+    if (g.NR > 256) return false;
+    g.T = (a.H * g.Wp + TILE_M - 1) / TILE_M;
+    const long long nb = a.V / ((long long)a.D * a.H * a.W);
+    g.ntiles = nb * a.D * g.T;
+    g.box_bytes = 16u * (uint32_t)g.Wp * (uint32_t)g.NR;
+    g.plane_bytes = (g.box_bytes + 127u) & ~127u;
+    g.slab_bytes = g.plane_bytes * (CIN / 8);
+    const uint32_t w27 = 27u * COUT * CIN * 2;
+    const uint32_t budget = 227u * 1024u - 1024u;
+    g.wcopy_bytes = (w27 <= 64u * 1024u) ? w27 : 0u;
+    g.wres_bytes = (g.wcopy_bytes + 1023u) & ~1023u;
+    g.wstage_bytes = g.wres_bytes ? 0u : 9u * COUT * CIN * 2;
+    g.stage_bytes = (g.slab_bytes + g.wstage_bytes + 1023u) & ~1023u;
+    if (g.wres_bytes && g.wres_bytes + 2 * g.stage_bytes > budget) {  // make room for stages
+        g.wres_bytes = 0;
+        g.wcopy_bytes = 0;
+        g.wstage_bytes = 9u * COUT * CIN * 2;
+        g.stage_bytes = (g.slab_bytes + g.wstage_bytes + 1023u) & ~1023u;
+    }
+    // several CTAs per SM: each tile's MMAs chain on one accumulator, so
+    // independent CTAs keep the tensor pipe busy; 4 stages each when they fit
+    constexpr int TCOLS = 2 * COUT <= 32 ? 32 : (2 * COUT <= 64 ? 64 : (2 * COUT <= 128 ? 128 : 256));
+    int per_sm = 1;
+    g.S = 0;
+    for (int want = std::min(4, 512 / TCOLS); want >= 1; want--) {
+        const uint32_t share = (228u * 1024u) / (uint32_t)want - 2048u;
+        const int S = (int)std::min<uint32_t>(want == 1 ? 8u : 4u, (std::min(share, budget) - g.wres_bytes) / g.stage_bytes);
+        if (g.wres_bytes < share && S >= 2) {
+            per_sm = want;
+            g.S = S;
+            break;
+        }
+    }
+    if (g.S < 2 || g.ntiles == 0) return false;
+    const uint32_t smem = g.wres_bytes + (uint32_t)g.S * g.stage_bytes;
+
+    CUtensorMap map;
+    const cuuint64_t dims[5] = {(cuuint64_t)CIN, (cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.D, (cuuint64_t)nb};
+    const cuuint64_t strides[4] = {(cuuint64_t)CIN * 2, (cuuint64_t)a.W * CIN * 2, (cuuint64_t)a.H * a.W * CIN * 2,
+                                   (cuuint64_t)a.D * a.H * a.W * CIN * 2};
+    const cuuint32_t box[5] = {8u, (cuuint32_t)g.Wp, (cuuint32_t)g.NR, 1u, 1u};
+    const cuuint32_t estr[5] = {1u, 1u, 1u, 1u, 1u};
+    const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16 *>(a.src1), dims, strides, box,
+                           estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return false;
+    err = cudaFuncSetAttribute(conv_tma_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return true;
+    err = cudaFuncSetAttribute(conv_tma_kernel<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               (int)cudaSharedmemCarveoutMaxShared);
+    if (err != cudaSuccess) return true;
+    const long long grid = std::min<long long>(g.ntiles, (long long)per_sm * std::max(1, a.sms));
+    conv_tma_kernel<CIN, COUT><<<(unsigned)grid, TMA_THREADS, smem, s>>>(map, a, g);
+    err = cudaGetLastError();
+    return true;
+}
+
 template <int CIN, int COUT>
 static cudaError_t launch_conv(const ConvArgs &a, int backend, cudaStream_t s)
 {
     const unsigned grid = (unsigned)((a.V + TILE_M - 1) / TILE_M);
     if (backend == BACKEND_TC_SLAB) {
         cudaError_t e = cudaSuccess;
+        if (launch_tma<CIN, COUT>(a, s, e)) return e;
         if (launch_slab<CIN, COUT>(a, s, e)) return e;
         backend = BACKEND_TC_TAP;  // a slab stage does not fit in shared memory
     }
@@ -796,7 +1103,7 @@ __global__ void __launch_bounds__(CONV_THREADS) wgrad_kernel(const WgradArgs a)
 {
     using Cfg = WgCfg<CIN, COUT>;
     static_assert(Cfg::SPLIT_K || Cfg::NT % 8 == 0, "tile split: an even number of n tiles per warp");
-    extern __shared__ __align__(128) unsigned char smem[];
+    extern __shared__ __align__(1024) unsigned char smem[];
     float *red = reinterpret_cast<float *>(smem + Cfg::S * Cfg::STAGE);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tap = blockIdx.y;
@@ -942,7 +1249,7 @@ __global__ void __launch_bounds__(CONV_THREADS) wgrad_slab_kernel(const WgradArg
 {
     using Cfg = WgsCfg<CIN, COUT>;
     constexpr int MT = Cfg::MT, NT = Cfg::NT, G = Cfg::G;
-    extern __shared__ __align__(128) unsigned char smem[];
+    extern __shared__ __align__(1024) unsigned char smem[];
     const uint32_t stage_bytes = g.stage_bytes;  // G tile + slab
     float *red = reinterpret_cast<float *>(smem + 2 * stage_bytes);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -1080,12 +1387,276 @@ static bool launch_wgrad_slab(const WgradArgs &a, int sms, cudaStream_t s, cudaE
     return true;
 }
 
+// Weight gradient on tcgen05, fed by TMA.  Per tap, dW_t^T[ci][co] =
+// sum_q X[q + off(t)][ci] G[q][co] is a GEMM with M = input channels, N =
+// output channels and K = positions.  The staged slab ([chunk][position][8
+// channels]) is exactly the canonical MN-major, non-swizzled operand layout
+// (8 channels x 8 positions per 128-byte core matrix, channel groups one
+// plane apart, position groups 128 B apart), so the tap shift is again a
+// descriptor offset.  M = 64 rows per MMA (input channels beyond cin read
+// padding and are dropped); the accumulators of every tap of the CTA's group
+// live in TMEM for the whole launch and are read once at the end.  Warp 4
+// loads stages with TMA, warp 5 issues the MMAs, warps 0-3 drain TMEM.
+struct WTGeom {
+    int Wp, NR, NRg, T;
+    long long ntiles;
+    uint32_t planeX, planeG;       // one 8-channel chunk plane of X / of the gradient (128-aligned)
+    uint32_t boxX, boxG;           // bytes one box delivers
+    uint32_t stage_bytes;
+    int S;
+};
+
+constexpr int WT_THREADS = 192;
+
+template <int CIN, int COUT>
+struct WtcCfg {
+    static constexpr int MB = (CIN + 63) / 64;  // M blocks of 64 input channels
+    static constexpr int G = 9 * COUT * MB <= 512 ? 9 : (3 * COUT * MB <= 512 ? 3 : 1);
+    static constexpr int COLS = G * COUT * MB;
+    static constexpr uint32_t TCOLS = COLS <= 32 ? 32 : (COLS <= 64 ? 64 : (COLS <= 128 ? 128 : (COLS <= 256 ? 256 : 512)));
+    static constexpr int PAD_PLANES = MB * 8 - CIN / 8;  // planes read past the slab by the padded M rows
+};
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(WT_THREADS) wgrad_tc_kernel(const __grid_constant__ CUtensorMap xmap,
+                                                              const __grid_constant__ CUtensorMap gmap,
+                                                              const WgradArgs a, const WTGeom g)
+{
+    using Cfg = WtcCfg<CIN, COUT>;
+    constexpr int G = Cfg::G, MB = Cfg::MB;
+    constexpr uint32_t IDESC = idesc_bf16(64, COUT) | (1u << 15) | (1u << 16);  // A and B MN-major
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t full[8], empty[8], done;
+    __shared__ uint32_t s_tmem;
+    __shared__ volatile int s_err;
+    __shared__ long long s_issued, s_consumed;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tap0 = blockIdx.y * G;
+    const int dz = tap0 / 9 - 1;
+    const uint32_t sbase = smem_u32(smem);
+    const uint32_t xbytes = (CIN / 8) * g.planeX;
+    if (tid == 0) {
+        for (int k = 0; k < g.S; k++) {
+            mbar_init(smem_u32(&full[k]), 1);
+            mbar_init(smem_u32(&empty[k]), 1);
+        }
+        mbar_init(smem_u32(&done), 1);
+        fence_mbar_init();
+        s_err = 0;
+        s_issued = 0;
+        s_consumed = 0;
+    }
+    if (warp == 5) {
+        tmem_alloc(smem_u32(&s_tmem), Cfg::TCOLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const long long my_tiles =
+        blockIdx.x < g.ntiles ? (g.ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+
+    if (warp == 4) {
+        if (lane == 0) {
+            for (long long k = 0; k < my_tiles; k++) {
+                const int slot = (int)(k % g.S);
+                if (k >= g.S && !mbar_wait_flag(smem_u32(&empty[slot]), (uint32_t)(((k / g.S) - 1) & 1), &s_err))
+                    break;
+                const long long tile = blockIdx.x + k * (long long)gridDim.x;
+                const long long plane = tile / g.T;
+                const int q0 = (int)(tile % g.T) * TILE_M;
+                const int n = (int)(plane / a.D), z = (int)(plane % a.D);
+                const int y_lo = floor_div(q0 - g.Wp - 1, g.Wp), yg_lo = q0 / g.Wp;
+                const uint32_t st = sbase + (uint32_t)slot * g.stage_bytes;
+                const uint32_t fb = smem_u32(&full[slot]);
+                mbar_expect_tx(fb, (CIN / 8) * g.boxX + (COUT / 8) * g.boxG);
+#pragma unroll
+                for (int c = 0; c < CIN / 8; c++) tma_load_5d(st + c * g.planeX, &xmap, c * 8, -1, y_lo, z + dz, n, fb);
+#pragma unroll
+                for (int c = 0; c < COUT / 8; c++)
+                    tma_load_5d(st + xbytes + c * g.planeG, &gmap, c * 8, -1, yg_lo, z, n, fb);
+                s_issued = k + 1;
+            }
+        }
+    } else if (warp == 5) {
+        if (lane == 0) {
+            for (long long k = 0; k < my_tiles; k++) {
+                const int slot = (int)(k % g.S);
+                if (!mbar_wait_flag(smem_u32(&full[slot]), (uint32_t)((k / g.S) & 1), &s_err)) break;
+                tc_fence_after();
+                const long long tile = blockIdx.x + k * (long long)gridDim.x;
+                const int q0 = (int)(tile % g.T) * TILE_M;
+                const int rel = q0 - floor_div(q0 - g.Wp - 1, g.Wp) * g.Wp;
+                const int relg = q0 - (q0 / g.Wp) * g.Wp;
+                const uint32_t sX = sbase + (uint32_t)slot * g.stage_bytes, sG = sX + xbytes;
+#pragma unroll 1
+                for (int t = 0; t < G; t++) {
+                    const int tap = tap0 + t;
+                    const int r0 = rel + ((tap / 3) % 3 - 1) * g.Wp + (tap % 3 - 1);
+#pragma unroll
+                    for (int mb = 0; mb < MB; mb++) {
+                        const uint32_t dcol = tmem + (uint32_t)((t * MB + mb) * COUT);
+#pragma unroll
+                        for (int ks = 0; ks < TILE_M / 16; ks++) {
+                            const uint64_t da = smem_desc(sX + (uint32_t)(mb * 8) * g.planeX + (uint32_t)(r0 + 16 * ks) * 16,
+                                                          128, g.planeX);
+                            const uint64_t db = smem_desc(sG + (uint32_t)(relg + 16 * ks) * 16, 128, g.planeG);
+                            umma_bf16(dcol, da, db, IDESC, (k > 0 || ks > 0) ? 1u : 0u);
+                        }
+                    }
+                }
+                umma_commit(smem_u32(&empty[slot]));
+                s_consumed = k + 1;
+            }
+            if (!s_err && my_tiles > 0) umma_commit(smem_u32(&done));
+        }
+    }
+    __syncthreads();
+    // drain: warps 0-3 read the accumulators (thread = TMEM lane) and add them to dW
+    const bool ok = !s_err && my_tiles > 0;
+    if (warp < 4 && ok) {
+        if (!mbar_wait(smem_u32(&done), 0)) s_err = 1;
+    }
+    __syncthreads();
+    if (warp < 4 && ok && !s_err) {
+        tc_fence_after();
+        // an M = 64 accumulator keeps row i in TMEM lane 32 (i / 16) + i % 16:
+        // lanes 0-15 of each warp's quadrant
+        const int row = lane < 16 ? warp * 16 + lane : -1;
+#pragma unroll 1
+        for (int blk = 0; blk < G * MB; blk++) {
+            uint32_t r[COUT];
+#pragma unroll
+            for (int c = 0; c < COUT; c += 16) {
+                uint32_t (&rr)[16] = *reinterpret_cast<uint32_t(*)[16]>(&r[c]);
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(blk * COUT + c), rr);
+            }
+            tmem_wait_ld();
+            const int t = blk / MB, mb = blk % MB;
+            const int ci = mb * 64 + row;
+            if (row >= 0 && ci < CIN) {
+#pragma unroll
+                for (int co = 0; co < COUT; co++) {
+                    const float v = __uint_as_float(r[co]);
+                    if (v != 0.0f) atomicAdd(&a.dw[((size_t)co * 27 + tap0 + t) * CIN + ci], v);
+                }
+            }
+        }
+        tc_fence_before();
+    }
+    if (s_err && tid == 0) {
+        if (a.counters) atomicAdd(&a.counters->timeouts, 1ull);
+        for (long long k = s_consumed; k < s_issued; k++)
+            mbar_wait(smem_u32(&full[k % g.S]), (uint32_t)((k / g.S) & 1));
+        if (s_consumed > 0) {
+            const long long k = s_consumed - 1;
+            mbar_wait(smem_u32(&empty[k % g.S]), (uint32_t)((k / g.S) & 1));
+        }
+    }
+    __syncthreads();
+    if (warp == 5) {
+        tc_fence_after();
+        tmem_dealloc(tmem, Cfg::TCOLS);
+    }
+}
+
+// bias gradient: db[c] += sum_v g[v][c]
+__global__ void bias_grad_kernel(const bf16 *__restrict__ g, int C, long long V, float *__restrict__ db)
+{
+    extern __shared__ float part[];
+    const int c = threadIdx.x % C, lanes = blockDim.x / C;
+    float s = 0.0f;
+    for (long long v = (long long)blockIdx.x * lanes + threadIdx.x / C; v < V; v += (long long)gridDim.x * lanes)
+        s += __bfloat162float(g[v * C + c]);
+    part[threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.x < C) {
+        float t = 0.0f;
+        for (int k = 0; k < lanes; k++) t += part[k * C + threadIdx.x];
+        atomicAdd(&db[threadIdx.x], t);
+    }
+}
+
+template <int CIN, int COUT>
+static bool launch_wgrad_tc(const WgradArgs &a, int sms, cudaStream_t s, cudaError_t &err)
+{
+    using Cfg = WtcCfg<CIN, COUT>;
+    if (a.c0 != 0 || a.W + 2 > 256) return false;
+    PFN_cuTensorMapEncodeTiled enc = tensor_map_encoder();
+    if (!enc) return false;
+    if ((reinterpret_cast<uintptr_t>(a.src1) & 15) || (reinterpret_cast<uintptr_t>(a.g) & 15)) return false;
+    WTGeom g{};
+    g.Wp = a.W + 2;
+    g.NR = 3 + (130 + g.Wp - 1) / g.Wp;
+    g.NRg = 2 + (TILE_M + g.Wp - 1) / g.Wp;
+    if (g.NR > 256 || g.NRg > 256) return false;
+    g.T = (a.H * g.Wp + TILE_M - 1) / TILE_M;
+    const long long nb = a.V / ((long long)a.D * a.H * a.W);
+    g.ntiles = nb * a.D * g.T;
+    g.boxX = 16u * (uint32_t)g.Wp * (uint32_t)g.NR;
+    g.boxG = 16u * (uint32_t)g.Wp * (uint32_t)g.NRg;
+    g.planeX = (g.boxX + 127u) & ~127u;
+    g.planeG = (g.boxG + 127u) & ~127u;
+    g.stage_bytes = (((CIN / 8) * g.planeX + (COUT / 8) * g.planeG) + 1023u) & ~1023u;
+    // the padded M rows of the last stage read up to PAD_PLANES planes past its slab
+    const uint32_t pad = (uint32_t)Cfg::PAD_PLANES * g.planeX;
+    const uint32_t budget = 227u * 1024u - 2048u;
+    int per_sm = std::min(4, (int)(512 / Cfg::TCOLS));
+    g.S = 0;
+    for (; per_sm >= 1; per_sm--) {
+        const uint32_t share = std::min<uint32_t>(budget, (228u * 1024u) / (uint32_t)per_sm - 2048u);
+        if (share <= pad) continue;
+        const int S = (int)std::min<uint32_t>(4u, (share - pad) / g.stage_bytes);
+        if (S >= 2) {
+            g.S = S;
+            break;
+        }
+    }
+    if (g.S < 2 || g.ntiles == 0) return false;
+    const uint32_t smem = (uint32_t)g.S * g.stage_bytes + pad;
+    CUtensorMap maps[2];
+    const void *bases[2] = {a.src1, a.g};
+    const int chans[2] = {CIN, COUT};
+    const int rows[2] = {g.NR, g.NRg};
+    for (int m = 0; m < 2; m++) {
+        const cuuint64_t C = (cuuint64_t)chans[m];
+        const cuuint64_t dims[5] = {C, (cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.D, (cuuint64_t)nb};
+        const cuuint64_t strides[4] = {C * 2, (cuuint64_t)a.W * C * 2, (cuuint64_t)a.H * a.W * C * 2,
+                                       (cuuint64_t)a.D * a.H * a.W * C * 2};
+        const cuuint32_t box[5] = {8u, (cuuint32_t)g.Wp, (cuuint32_t)rows[m], 1u, 1u};
+        const cuuint32_t estr[5] = {1u, 1u, 1u, 1u, 1u};
+        if (enc(&maps[m], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void *>(bases[m]), dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    }
+    err = cudaFuncSetAttribute(wgrad_tc_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return true;
+    err = cudaFuncSetAttribute(wgrad_tc_kernel<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               (int)cudaSharedmemCarveoutMaxShared);
+    if (err != cudaSuccess) return true;
+    const int groups = 27 / Cfg::G;
+    const long long per_group = std::max<long long>(
+        1, std::min<long long>((g.ntiles + 1) / 2, ((long long)per_sm * std::max(1, sms) + groups - 1) / groups));
+    wgrad_tc_kernel<CIN, COUT><<<dim3((unsigned)per_group, groups), WT_THREADS, smem, s>>>(maps[0], maps[1], a, g);
+    if ((err = cudaGetLastError()) != cudaSuccess) return true;
+    if (a.db) {
+        const int lanes = 256 / COUT;
+        const long long blocks = std::min<long long>((a.V + lanes - 1) / lanes, 4LL * std::max(1, sms));
+        bias_grad_kernel<<<(unsigned)blocks, lanes * COUT, lanes * COUT * sizeof(float), s>>>(a.g, COUT, a.V, a.db);
+        err = cudaGetLastError();
+    }
+    return true;
+}
+
 cudaError_t wgrad3x3(const WgradArgs &a, int cin, int sms, cudaStream_t s)
 {
 #define IAC_WG_CASE(CI, CO)                                               \
     if (cin == CI && a.cout == CO) {                                      \
         cudaError_t e = cudaSuccess;                                      \
-        if (a.slabs && launch_wgrad_slab<CI, CO>(a, sms, s, e)) return e; \
+        if (a.slabs == 2 && launch_wgrad_tc<CI, CO>(a, sms, s, e)) return e; \
+        if (a.slabs >= 1 && launch_wgrad_slab<CI, CO>(a, sms, s, e)) return e; \
         return launch_wgrad<CI, CO>(a, sms, s);                           \
     }
     IAC_WG_CASE(16, 16)
@@ -1099,41 +1670,92 @@ cudaError_t wgrad3x3(const WgradArgs &a, int cin, int sms, cudaStream_t s)
     return cudaErrorInvalidValue;
 }
 
-// first layer: dW[co][tap] = sum_v G[v][co] x[v+off(tap)], 432 threads = (tap, co)
-__global__ void __launch_bounds__(448) wgrad_first_kernel(const float *__restrict__ x, const bf16 *__restrict__ g,
+// first layer: dW[co][tap] = sum_v G[v][co] x[v+off(tap)] and db[co] = sum_v G[v][co]
+// on mma.sync: per block of 128 voxels the 27 shifted inputs (and a column of
+// ones for the bias) are written to shared memory as a bf16 [tap chunk][voxel][8]
+// operand, the gradient rows as [co chunk][voxel][8]; M = 16 output channels,
+// N = 32 columns (27 taps, ones, padding), K = voxels.
+__global__ void __launch_bounds__(128) wgrad_first_kernel(const float *__restrict__ x, const bf16 *__restrict__ g,
                                                           float *__restrict__ dw, float *__restrict__ db, int D,
                                                           int H, int W, long long V)
 {
-    __shared__ float gs[TILE_M][17];
-    __shared__ float xs[27][TILE_M];
-    const int tid = threadIdx.x;
-    const int co = tid % 16, tap = tid / 16;
-    float acc = 0.0f;
+    __shared__ __align__(128) bf16 xs[4][TILE_M][8];
+    __shared__ __align__(128) bf16 gs[2][TILE_M][8];
+    __shared__ float red[16][32];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int i = tid; i < 16 * 32; i += 128) (&red[0][0])[i] = 0.0f;
+    float acc[4][4];
+#pragma unroll
+    for (int n = 0; n < 4; n++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[n][j] = 0.0f;
+    const uint32_t sx = smem_u32(&xs[0][0][0]), sg = smem_u32(&gs[0][0][0]);
     const long long nblk = (V + TILE_M - 1) / TILE_M;
     for (long long b = blockIdx.x; b < nblk; b += gridDim.x) {
         __syncthreads();
-        if (tid < TILE_M) {
+        {
             const long long v = b * TILE_M + tid;
             const Vox q = decode(v, D, H, W, V);
+            float col[32];
+#pragma unroll
             for (int t = 0; t < 27; t++) {
                 const int z = q.z + t / 9 - 1, yy = q.y + (t / 3) % 3 - 1, xx = q.x + t % 3 - 1;
                 const bool ok = q.ok && (unsigned)z < (unsigned)D && (unsigned)yy < (unsigned)H &&
                                 (unsigned)xx < (unsigned)W;
-                xs[t][tid] = ok ? x[(((long long)q.n * D + z) * H + yy) * W + xx] : 0.0f;
+                col[t] = ok ? x[(((long long)q.n * D + z) * H + yy) * W + xx] : 0.0f;
             }
-            for (int c = 0; c < 16; c++) gs[tid][c] = q.ok ? __bfloat162float(g[v * 16 + c]) : 0.0f;
+            col[27] = q.ok ? 1.0f : 0.0f;
+#pragma unroll
+            for (int t = 28; t < 32; t++) col[t] = 0.0f;
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                uint4 u;
+                u.x = pack_bf16(col[8 * c], col[8 * c + 1]);
+                u.y = pack_bf16(col[8 * c + 2], col[8 * c + 3]);
+                u.z = pack_bf16(col[8 * c + 4], col[8 * c + 5]);
+                u.w = pack_bf16(col[8 * c + 6], col[8 * c + 7]);
+                *reinterpret_cast<uint4 *>(&xs[c][tid][0]) = u;
+            }
+            const uint4 z4 = make_uint4(0, 0, 0, 0);
+            const uint4 *gp = reinterpret_cast<const uint4 *>(g + (q.ok ? v : 0) * 16);
+            *reinterpret_cast<uint4 *>(&gs[0][tid][0]) = q.ok ? gp[0] : z4;
+            *reinterpret_cast<uint4 *>(&gs[1][tid][0]) = q.ok ? gp[1] : z4;
         }
         __syncthreads();
-        if (tid < 27 * 16) {
-            for (int r = 0; r < TILE_M; r++) acc = fmaf(gs[r][co], xs[tap][r], acc);
-        } else if (tid < 27 * 16 + 16) {
-            for (int r = 0; r < TILE_M; r++) acc += gs[r][tid - 27 * 16];
+#pragma unroll
+        for (int ks = 0; ks < 2; ks++) {
+            const int kb = warp * 32 + ks * 16;
+            uint32_t a0, a1, a2, a3;
+            {
+                const int vr = kb + (lane & 7) + ((lane >> 4) << 3);
+                const int ch = (lane >> 3) & 1;
+                ldsm_x4_t(sg + (uint32_t)((ch * TILE_M + vr) * 16), a0, a1, a2, a3);
+            }
+#pragma unroll
+            for (int n2 = 0; n2 < 2; n2++) {
+                uint32_t b0, b1, b2, b3;
+                const int vx = kb + (lane & 7) + (((lane >> 3) & 1) << 3);
+                const int cx = 2 * n2 + (lane >> 4);
+                ldsm_x4_t(sx + (uint32_t)((cx * TILE_M + vx) * 16), b0, b1, b2, b3);
+                mma_bf16(acc[2 * n2], a0, a1, a2, a3, b0, b1);
+                mma_bf16(acc[2 * n2 + 1], a0, a1, a2, a3, b2, b3);
+            }
         }
     }
-    if (tid < 27 * 16) {
-        if (acc != 0.0f) atomicAdd(&dw[co * 27 + tap], acc);
-    } else if (tid < 27 * 16 + 16) {
-        if (acc != 0.0f) atomicAdd(&db[tid - 27 * 16], acc);
+    const int gq = lane >> 2, tq = lane & 3;
+#pragma unroll
+    for (int n = 0; n < 4; n++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) atomicAdd(&red[gq + 8 * (j >> 1)][n * 8 + 2 * tq + (j & 1)], acc[n][j]);
+    __syncthreads();
+    for (int i = tid; i < 16 * 28; i += 128) {
+        const int co = i / 28, t = i % 28;
+        const float r = red[co][t];
+        if (r == 0.0f) continue;
+        if (t < 27)
+            atomicAdd(&dw[co * 27 + t], r);
+        else
+            atomicAdd(&db[co], r);
     }
 }
 
@@ -1141,8 +1763,8 @@ cudaError_t wgrad3x3_first(const float *x, const bf16 *g, float *dw, float *db, 
                            int sms, cudaStream_t s)
 {
     const long long nblk = (V + TILE_M - 1) / TILE_M;
-    const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(nblk, 2LL * sms));
-    wgrad_first_kernel<<<grid, 448, 0, s>>>(x, g, dw, db, D, H, W, V);
+    const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(nblk, 8LL * sms));
+    wgrad_first_kernel<<<grid, 128, 0, s>>>(x, g, dw, db, D, H, W, V);
     return cudaGetLastError();
 }
 
@@ -1262,6 +1884,34 @@ cudaError_t split_concat_grad(const bf16 *gcat, int c0, int c1, const bf16 *y0, 
     const long long nco = V / 8 * (c0 / 8), nfu = V * (c1 / 8);
     split_concat_kernel<<<(unsigned)((nco + nfu + 255) / 256), 256, 0, s>>>(gcat, c0, c1, y0, g0, g1, D, H, W, nco,
                                                                              nfu);
+    return cudaGetLastError();
+}
+
+// out[v] = concat(src0 at the coarse parent of v, src1[v]): the decoder input of
+// nearest 2x upsampling followed by skip concatenation
+__global__ void concat_up_kernel(const bf16 *__restrict__ src0, int c0, const bf16 *__restrict__ src1, int c1,
+                                 bf16 *__restrict__ out, int D, int H, int W, long long total)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int C = c0 + c1, nc = C / 8, c = (int)(i % nc) * 8;
+    const long long v = i / nc;
+    uint4 val;
+    if (c < c0) {
+        const Vox q = decode(v, D, H, W, total / nc);
+        const long long u = (((long long)q.n * (D / 2) + q.z / 2) * (H / 2) + q.y / 2) * (W / 2) + q.x / 2;
+        val = *reinterpret_cast<const uint4 *>(src0 + u * c0 + c);
+    } else {
+        val = *reinterpret_cast<const uint4 *>(src1 + v * c1 + (c - c0));
+    }
+    *reinterpret_cast<uint4 *>(out + v * C + c) = val;
+}
+
+cudaError_t concat_up(const bf16 *src0, int c0, const bf16 *src1, int c1, bf16 *out, int D, int H, int W, int nb,
+                      cudaStream_t s)
+{
+    const long long total = (long long)nb * D * H * W * ((c0 + c1) / 8);
+    concat_up_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(src0, c0, src1, c1, out, D, H, W, total);
     return cudaGetLastError();
 }
 
