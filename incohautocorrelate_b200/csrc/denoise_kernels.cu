@@ -31,7 +31,9 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <map>
 #include <mutex>
+#include <utility>
 
 #include "denoise_internal.cuh"
 
@@ -911,6 +913,27 @@ __global__ void __launch_bounds__(TMA_THREADS) conv_tma_kernel(const __grid_cons
     }
 }
 
+// shared-memory attributes of a kernel, set once per process (the largest
+// size asked for so far); the attribute calls are host work on every launch
+// otherwise
+template <typename K>
+static cudaError_t smem_attributes(K kernel, uint32_t smem)
+{
+    static std::mutex mu;
+    static std::map<std::pair<int, const void *>, uint32_t> done;  // (device, kernel) -> size set
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    uint32_t &have = done[{dev, reinterpret_cast<const void *>(kernel)}];
+    if (smem <= have) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess) have = smem;
+    return e;
+}
+
 // cuTensorMapEncodeTiled from the driver (no link-time dependency on libcuda)
 static PFN_cuTensorMapEncodeTiled tensor_map_encoder()
 {
@@ -982,10 +1005,7 @@ static bool launch_tma(const ConvArgs &a, cudaStream_t s, cudaError_t &err)
                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return false;
-    err = cudaFuncSetAttribute(conv_tma_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (err != cudaSuccess) return true;
-    err = cudaFuncSetAttribute(conv_tma_kernel<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                               (int)cudaSharedmemCarveoutMaxShared);
+    err = smem_attributes(conv_tma_kernel<CIN, COUT>, smem);
     if (err != cudaSuccess) return true;
     const long long grid = std::min<long long>(g.ntiles, (long long)per_sm * std::max(1, a.sms));
     conv_tma_kernel<CIN, COUT><<<(unsigned)grid, TMA_THREADS, smem, s>>>(map, a, g);
@@ -1631,10 +1651,7 @@ static bool launch_wgrad_tc(const WgradArgs &a, int sms, cudaStream_t s, cudaErr
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return false;
     }
-    err = cudaFuncSetAttribute(wgrad_tc_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (err != cudaSuccess) return true;
-    err = cudaFuncSetAttribute(wgrad_tc_kernel<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                               (int)cudaSharedmemCarveoutMaxShared);
+    err = smem_attributes(wgrad_tc_kernel<CIN, COUT>, smem);
     if (err != cudaSuccess) return true;
     const int groups = 27 / Cfg::G;
     const long long per_group = std::max<long long>(
