@@ -620,6 +620,25 @@ def denoise_bench(args, ctx, stream, clocks, nthreads):
         dn.adamw_step(lr=1e-5, stream=sp)
 
     ms_train = _time(train_step, args.steps, max(3, args.warmup), stream)
+    # the same step replayed from one captured CUDA graph (patches cut on the device)
+    nm, Em = 4, 128
+    meshes = torch.from_numpy(rng.gamma(2.0, 0.5, (nm, Em, Em, Em)).astype(np.float32)).to(torch.bfloat16)
+    meshes = meshes.view(torch.int16).cuda()
+    gsteps = max(args.steps, 4)
+    plans = np.stack([rng.integers(0, nm, (gsteps, B)), rng.integers(0, Em - P + 1, (gsteps, B)),
+                      rng.integers(0, Em - P + 1, (gsteps, B)), rng.integers(0, Em - P + 1, (gsteps, B)),
+                      rng.integers(0, 48, (gsteps, B))], 2).astype(np.int32)
+    d_plans = torch.from_numpy(plans).cuda()
+    d_lrs = torch.full((gsteps,), 1e-5, dtype=torch.float32, device="cuda")
+    for _ in range(2):  # capture + warm
+        dn.train_steps(meshes, meshes, nm, Em, d_plans, d_lrs, gsteps, B, P, stream=sp)
+    torch.cuda.synchronize()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    dn.train_steps(meshes, meshes, nm, Em, d_plans, d_lrs, gsteps, B, P, stream=sp)
+    g1.record(stream)
+    torch.cuda.synchronize()
+    ms_graph = g0.elapsed_time(g1) / gsteps
     xf = torch.from_numpy(rng.gamma(2.0, 0.5, (1, E, E, E)).astype(np.float32)).cuda()
     of = torch.zeros_like(xf)
     ms_fwd = _time(lambda: dn.forward(xf, 1, E, E, E, of, sp), args.steps, max(3, args.warmup), stream)
@@ -654,6 +673,8 @@ def denoise_bench(args, ctx, stream, clocks, nthreads):
                       "params": capi.denoise_param_count(),
                       "train_flop_per_voxel": 2.0 * DENOISE_TRAIN_MACS,
                       "forward_flop_per_voxel": 2.0 * DENOISE_FWD_MACS},
+           "graph_step": {"ms": ms_graph, "note": "patch crop + forward + backward + AdamW of one step "
+                                                  "captured in a CUDA graph and replayed"},
            "inference": {"volume": f"1 x {E}^3", "ms": ms_fwd, "tflops": tf_fwd,
                          "meshes_per_s": 1e3 / ms_fwd},
            "layers": layers, "clocks": clk,

@@ -411,6 +411,20 @@ iac_status iac_denoise_wgrad3x3(iac_ctx *ctx, int slabs, const uint16_t *d_src0,
                                 uint32_t cout, uint32_t nb, uint32_t D, uint32_t H, uint32_t W,
                                 float *d_dw, float *d_db, void *stream);
 
+/* nsteps training steps replayed from one CUDA graph: per step the patches
+ * of plan d_plans[step] ([nsteps][nb][5] int32, as iac_denoise_crop_patches)
+ * are cut from the nmeshes E^3 bf16 input and target meshes, the loss and
+ * gradients computed and AdamW applied with learning rate d_lrs[step]
+ * (opt->lr is ignored).  d_losses (optional, double[nsteps]) receives each
+ * step's sum of squared errors.  The graph is captured on the first call and
+ * reused while the pointers, sizes and hyper-parameters stay the same.
+ * Asynchronous. */
+iac_status iac_denoise_train_steps(iac_denoiser *dn, const uint16_t *d_in_meshes,
+                                   const uint16_t *d_tgt_meshes, uint32_t nmeshes, uint32_t E,
+                                   const int32_t *d_plans, const float *d_lrs, uint32_t nsteps,
+                                   uint32_t nb, uint32_t P, const iac_adamw *opt, double *d_losses,
+                                   void *stream);
+
 /* Network input from a folded S^3 uint64 mesh: its leading E^3 corner times
  * `scale`, as fp32 (d_f32) and/or bf16 bits (d_bf16).  Asynchronous. */
 iac_status iac_denoise_mesh_input(iac_ctx *ctx, const uint64_t *d_full, uint32_t S, uint32_t E,

@@ -148,6 +148,8 @@ def _declare(lib):
     fn("iac_denoise_backward", [_VP, _VP, _VP, _VP, _U32, _U32, _U32, _U32, _VP,
                                 C.POINTER(C.c_double), _VP])
     fn("iac_denoise_adamw_step", [_VP, C.POINTER(AdamW), _VP])
+    fn("iac_denoise_train_steps", [_VP, _VP, _VP, _U32, _U32, _VP, _VP, _U32, _U32, _U32,
+                                   C.POINTER(AdamW), _VP, _VP])
     fn("iac_denoise_conv3x3", [_VP, C.c_int, _VP, _U32, C.c_int, _VP, _U32, _VP, _VP, _U32, C.c_int,
                                _U32, _U32, _U32, _U32, _VP, _VP])
     fn("iac_denoise_wgrad3x3", [_VP, C.c_int, _VP, _U32, C.c_int, _VP, _U32, _VP, _U32, _U32, _U32,
@@ -451,6 +453,15 @@ class Denoiser:
     def adamw_step(self, lr, beta1=0.9, beta2=0.999, eps=1e-8, weight_decay=1e-4, stream=None):
         opt = AdamW(lr, beta1, beta2, eps, weight_decay)
         check(lib().iac_denoise_adamw_step(self._h, C.byref(opt), _ptr(stream)))
+
+    def train_steps(self, d_in_meshes, d_tgt_meshes, nmeshes, E, d_plans, d_lrs, nsteps, nb, P,
+                    d_losses=None, beta1=0.9, beta2=0.999, eps=1e-8, weight_decay=1e-4, stream=None):
+        """nsteps steps replayed from one CUDA graph (plans [nsteps][nb][5] int32, lrs
+        [nsteps] float32 on the device)."""
+        opt = AdamW(0.0, beta1, beta2, eps, weight_decay)
+        check(lib().iac_denoise_train_steps(self._h, _ptr(d_in_meshes), _ptr(d_tgt_meshes), int(nmeshes),
+                                            int(E), _ptr(d_plans), _ptr(d_lrs), int(nsteps), int(nb),
+                                            int(P), C.byref(opt), _ptr(d_losses), _ptr(stream)))
 
 
 def denoise_mesh_input(ctx, d_full, S, E, scale, d_f32=None, d_bf16=None, stream=None):

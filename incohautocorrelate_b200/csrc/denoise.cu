@@ -59,6 +59,14 @@ struct iac_denoiser {
     bf16 *hA = nullptr, *hB = nullptr, *gcat2 = nullptr, *gskip2 = nullptr;  // half
     bf16 *qA = nullptr, *qB = nullptr;                                       // quarter
     std::vector<void *> allocs;
+    // CUDA graph of one training step (iac_denoise_train_steps)
+    long long *d_step = nullptr;  // [0] replay index, [1] optimizer steps so far
+    float *px = nullptr, *pt = nullptr;
+    double *d_dummy_loss = nullptr;
+    cudaGraphExec_t step_exec = nullptr;
+    std::vector<uintptr_t> step_key;
+    cudaStream_t own_stream = nullptr;  // replay stream for callers on the legacy default stream
+    cudaEvent_t own_ev[2] = {nullptr, nullptr};
 
     void *alloc(size_t bytes)
     {
@@ -69,6 +77,10 @@ struct iac_denoiser {
     }
     ~iac_denoiser()
     {
+        if (step_exec) cudaGraphExecDestroy(step_exec);
+        for (cudaEvent_t e : own_ev)
+            if (e) cudaEventDestroy(e);
+        if (own_stream) cudaStreamDestroy(own_stream);
         for (void *a : allocs) cudaFree(a);
     }
 };
@@ -181,9 +193,12 @@ iac_status wgrad(iac_denoiser *dn, int l, const bf16 *src0, const bf16 *src1, co
     return IAC_OK;
 }
 
-iac_status refresh_tiles(iac_denoiser *dn, const iac_adamw *opt, cudaStream_t s)
+iac_status refresh_tiles(iac_denoiser *dn, const iac_adamw *opt, cudaStream_t s,
+                         const long long *d_step = nullptr, const float *lrs = nullptr)
 {
     AdamArgs a{};
+    a.d_step = d_step;
+    a.lrs = lrs;
     a.p = dn->p;
     a.g = dn->g;
     a.m = dn->m;
@@ -201,7 +216,7 @@ iac_status refresh_tiles(iac_denoiser *dn, const iac_adamw *opt, cudaStream_t s)
         a.layers[l].wd_off = l < NCONV ? dn->wd_off[l] : 0;
     }
     if (opt) {
-        dn->adam_step++;
+        if (!d_step) dn->adam_step++;
         a.update = 1;
         a.lr = opt->lr;
         a.beta1 = opt->beta1;
@@ -247,6 +262,75 @@ uint64_t splitmix(uint64_t &s)
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
     return z ^ (z >> 31);
+}
+
+// forward, loss into loss[d_step ? d_step[0] : 0] (accumulated), gradients into dn->g
+iac_status run_backward(iac_denoiser *dn, const float *d_in, const float *d_target, const float *d_weight, uint32_t nb,
+                        uint32_t D, uint32_t H, uint32_t W, float *d_out, double *loss, const long long *d_step,
+                        cudaStream_t s)
+{
+    iac_status st = IAC_OK;
+    const long long V = (long long)nb * D * H * W, V2 = V / 8, V4 = V / 64;
+    const int D2 = D / 2, H2 = H / 2, W2 = W / 2, D4 = D / 4, H4 = H / 4, W4 = W / 4;
+    DN_CHECK(cudaMemsetAsync(dn->g, 0, dn->nparams * 4, s), "clear gradients");
+    st = run_forward(dn, d_in, nb, D, H, W, s);
+    if (st != IAC_OK) return st;
+    HeadArgs h{};
+    h.x = d_in;
+    h.d = dn->d1b;
+    h.w = dn->p + dn->p_off[10];
+    h.target = d_target;
+    h.weight = d_weight;
+    h.out = d_out;
+    h.gd = dn->gA;  // = d loss / d pre-activation of layer 9
+    h.dw = dn->g + dn->p_off[10];
+    h.loss = loss;
+    h.d_step = d_step;
+    h.V = V;
+    h.inv_count = 1.0 / (double)V;
+    DN_CHECK(head(h, dn->ctx->sm_count, s), "denoiser head");
+    // layer 9: X = d1a
+    if ((st = wgrad(dn, 9, nullptr, dn->d1a, dn->gA, D, H, W, V, s)) != IAC_OK) return st;
+    if ((st = dgrad(dn, 9, dn->gA, dn->gB, D, H, W, V, s)) != IAC_OK) return st;
+    DN_CHECK(relu_mask(dn->gB, dn->d1a, dn->gB, V * 16, s), "mask 8");
+    // layer 8: X = up(d2b) ++ s1
+    if ((st = wgrad(dn, 8, nullptr, dn->cat1, dn->gB, D, H, W, V, s)) != IAC_OK) return st;
+    if ((st = dgrad(dn, 8, dn->gB, dn->gcat1, D, H, W, V, s)) != IAC_OK) return st;
+    DN_CHECK(split_concat_grad(dn->gcat1, 32, 16, dn->d2b, dn->hA, dn->gskip1, D, H, W, nb, s), "split 1");
+    // layer 7: X = d2a
+    if ((st = wgrad(dn, 7, nullptr, dn->d2a, dn->hA, D2, H2, W2, V2, s)) != IAC_OK) return st;
+    if ((st = dgrad(dn, 7, dn->hA, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
+    DN_CHECK(relu_mask(dn->hB, dn->d2a, dn->hB, V2 * 32, s), "mask 6");
+    // layer 6: X = up(b2) ++ s2
+    if ((st = wgrad(dn, 6, nullptr, dn->cat2, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
+    if ((st = dgrad(dn, 6, dn->hB, dn->gcat2, D2, H2, W2, V2, s)) != IAC_OK) return st;
+    DN_CHECK(split_concat_grad(dn->gcat2, 64, 32, dn->b2, dn->qA, dn->gskip2, D2, H2, W2, nb, s), "split 2");
+    // layer 5: X = b1
+    if ((st = wgrad(dn, 5, nullptr, dn->b1, dn->qA, D4, H4, W4, V4, s)) != IAC_OK) return st;
+    if ((st = dgrad(dn, 5, dn->qA, dn->qB, D4, H4, W4, V4, s)) != IAC_OK) return st;
+    DN_CHECK(relu_mask(dn->qB, dn->b1, dn->qB, V4 * 64, s), "mask 4");
+    // layer 4: X = p2
+    if ((st = wgrad(dn, 4, nullptr, dn->p2, dn->qB, D4, H4, W4, V4, s)) != IAC_OK) return st;
+    if ((st = dgrad(dn, 4, dn->qB, dn->qA, D4, H4, W4, V4, s)) != IAC_OK) return st;  // d p2 (32 ch)
+    DN_CHECK(pool_grad_mask(dn->gskip2, dn->qA, dn->s2, dn->hA, 32, D2, H2, W2, nb, s), "pool grad 2");
+    // layer 3: X = e2a
+    if ((st = wgrad(dn, 3, nullptr, dn->e2a, dn->hA, D2, H2, W2, V2, s)) != IAC_OK) return st;
+    if ((st = dgrad(dn, 3, dn->hA, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
+    DN_CHECK(relu_mask(dn->hB, dn->e2a, dn->hB, V2 * 32, s), "mask 2");
+    // layer 2: X = p1
+    if ((st = wgrad(dn, 2, nullptr, dn->p1, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
+    if ((st = dgrad(dn, 2, dn->hB, dn->hA, D2, H2, W2, V2, s)) != IAC_OK) return st;  // d p1 (16 ch)
+    DN_CHECK(pool_grad_mask(dn->gskip1, dn->hA, dn->s1, dn->gA, 16, D, H, W, nb, s), "pool grad 1");
+    // layer 1: X = e1a
+    if ((st = wgrad(dn, 1, nullptr, dn->e1a, dn->gA, D, H, W, V, s)) != IAC_OK) return st;
+    if ((st = dgrad(dn, 1, dn->gA, dn->gB, D, H, W, V, s)) != IAC_OK) return st;
+    DN_CHECK(relu_mask(dn->gB, dn->e1a, dn->gB, V * 16, s), "mask 0");
+    // layer 0: X = input
+    DN_CHECK(wgrad3x3_first(d_in, dn->gB, dn->g + dn->p_off[0], dn->g + dn->p_off[0] + 16 * 27, D, H, W, V,
+                            dn->ctx->sm_count, s),
+             "layer 0 weight gradient");
+    dn->ctx->launches += 50;
+    return IAC_OK;
 }
 
 }  // namespace
@@ -328,6 +412,8 @@ iac_status iac_denoise_create(iac_ctx *ctx, uint32_t max_batch, uint32_t D, uint
     dn->gskip2 = (bf16 *)A(V2 * 32 * b);
     dn->qA = (bf16 *)A(V4 * 64 * b);
     dn->qB = (bf16 *)A(V4 * 64 * b);
+    dn->d_step = (long long *)A(16);
+    dn->d_dummy_loss = (double *)A(8);
     if (!ok) {
         delete dn;
         set_error("device memory for a %u x %ux%ux%u denoiser workspace", max_batch, D, H, W);
@@ -432,71 +518,14 @@ iac_status iac_denoise_backward(iac_denoiser *dn, const float *d_in, const float
     if (st != IAC_OK) return st;
     DeviceGuard guard(dn->ctx->device);
     cudaStream_t s = (cudaStream_t)stream;
-    const long long V = (long long)nb * D * H * W, V2 = V / 8, V4 = V / 64;
-    const int D2 = D / 2, H2 = H / 2, W2 = W / 2, D4 = D / 4, H4 = H / 4, W4 = W / 4;
-    DN_CHECK(cudaMemsetAsync(dn->g, 0, dn->nparams * 4, s), "clear gradients");
     DN_CHECK(cudaMemsetAsync(dn->d_loss, 0, 8, s), "clear loss");
-    st = run_forward(dn, d_in, nb, D, H, W, s);
+    st = run_backward(dn, d_in, d_target, d_weight, nb, D, H, W, d_out, dn->d_loss, nullptr, s);
     if (st != IAC_OK) return st;
-    HeadArgs h{};
-    h.x = d_in;
-    h.d = dn->d1b;
-    h.w = dn->p + dn->p_off[10];
-    h.target = d_target;
-    h.weight = d_weight;
-    h.out = d_out;
-    h.gd = dn->gA;  // = d loss / d pre-activation of layer 9
-    h.dw = dn->g + dn->p_off[10];
-    h.loss = dn->d_loss;
-    h.V = V;
-    h.inv_count = 1.0 / (double)V;
-    DN_CHECK(head(h, dn->ctx->sm_count, s), "denoiser head");
-    // layer 9: X = d1a
-    if ((st = wgrad(dn, 9, nullptr, dn->d1a, dn->gA, D, H, W, V, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 9, dn->gA, dn->gB, D, H, W, V, s)) != IAC_OK) return st;
-    DN_CHECK(relu_mask(dn->gB, dn->d1a, dn->gB, V * 16, s), "mask 8");
-    // layer 8: X = up(d2b) ++ s1
-    if ((st = wgrad(dn, 8, nullptr, dn->cat1, dn->gB, D, H, W, V, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 8, dn->gB, dn->gcat1, D, H, W, V, s)) != IAC_OK) return st;
-    DN_CHECK(split_concat_grad(dn->gcat1, 32, 16, dn->d2b, dn->hA, dn->gskip1, D, H, W, nb, s), "split 1");
-    // layer 7: X = d2a
-    if ((st = wgrad(dn, 7, nullptr, dn->d2a, dn->hA, D2, H2, W2, V2, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 7, dn->hA, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
-    DN_CHECK(relu_mask(dn->hB, dn->d2a, dn->hB, V2 * 32, s), "mask 6");
-    // layer 6: X = up(b2) ++ s2
-    if ((st = wgrad(dn, 6, nullptr, dn->cat2, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 6, dn->hB, dn->gcat2, D2, H2, W2, V2, s)) != IAC_OK) return st;
-    DN_CHECK(split_concat_grad(dn->gcat2, 64, 32, dn->b2, dn->qA, dn->gskip2, D2, H2, W2, nb, s), "split 2");
-    // layer 5: X = b1
-    if ((st = wgrad(dn, 5, nullptr, dn->b1, dn->qA, D4, H4, W4, V4, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 5, dn->qA, dn->qB, D4, H4, W4, V4, s)) != IAC_OK) return st;
-    DN_CHECK(relu_mask(dn->qB, dn->b1, dn->qB, V4 * 64, s), "mask 4");
-    // layer 4: X = p2
-    if ((st = wgrad(dn, 4, nullptr, dn->p2, dn->qB, D4, H4, W4, V4, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 4, dn->qB, dn->qA, D4, H4, W4, V4, s)) != IAC_OK) return st;  // d p2 (32 ch)
-    DN_CHECK(pool_grad_mask(dn->gskip2, dn->qA, dn->s2, dn->hA, 32, D2, H2, W2, nb, s), "pool grad 2");
-    // layer 3: X = e2a
-    if ((st = wgrad(dn, 3, nullptr, dn->e2a, dn->hA, D2, H2, W2, V2, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 3, dn->hA, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
-    DN_CHECK(relu_mask(dn->hB, dn->e2a, dn->hB, V2 * 32, s), "mask 2");
-    // layer 2: X = p1
-    if ((st = wgrad(dn, 2, nullptr, dn->p1, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 2, dn->hB, dn->hA, D2, H2, W2, V2, s)) != IAC_OK) return st;  // d p1 (16 ch)
-    DN_CHECK(pool_grad_mask(dn->gskip1, dn->hA, dn->s1, dn->gA, 16, D, H, W, nb, s), "pool grad 1");
-    // layer 1: X = e1a
-    if ((st = wgrad(dn, 1, nullptr, dn->e1a, dn->gA, D, H, W, V, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 1, dn->gA, dn->gB, D, H, W, V, s)) != IAC_OK) return st;
-    DN_CHECK(relu_mask(dn->gB, dn->e1a, dn->gB, V * 16, s), "mask 0");
-    // layer 0: X = input
-    DN_CHECK(wgrad3x3_first(d_in, dn->gB, dn->g + dn->p_off[0], dn->g + dn->p_off[0] + 16 * 27, D, H, W, V,
-                            dn->ctx->sm_count, s),
-             "layer 0 weight gradient");
-    dn->ctx->launches += 50;
     if (h_loss) {
         double t = 0;
         DN_CHECK(cudaMemcpyAsync(&t, dn->d_loss, 8, cudaMemcpyDeviceToHost, s), "loss");
         DN_CHECK(cudaStreamSynchronize(s), "loss");
-        *h_loss = t / (double)V;
+        *h_loss = t / ((double)nb * D * H * W);
     }
     return IAC_OK;
 }
@@ -510,6 +539,93 @@ iac_status iac_denoise_adamw_step(iac_denoiser *dn, const iac_adamw *opt, void *
     DeviceGuard guard(dn->ctx->device);
     dn->ctx->launches += 1;
     return refresh_tiles(dn, opt, (cudaStream_t)stream);
+}
+
+iac_status iac_denoise_train_steps(iac_denoiser *dn, const uint16_t *d_in_meshes, const uint16_t *d_tgt_meshes,
+                                   uint32_t nmeshes, uint32_t E, const int32_t *d_plans, const float *d_lrs,
+                                   uint32_t nsteps, uint32_t nb, uint32_t P, const iac_adamw *opt, double *d_losses,
+                                   void *stream)
+{
+    IAC_REQUIRE(dn && d_in_meshes && d_tgt_meshes && d_plans && d_lrs && opt, "null argument");
+    IAC_REQUIRE(nsteps >= 1 && nmeshes >= 1 && P >= 4 && P % 4 == 0 && P <= E, "steps %u, meshes %u, patch %u of %u",
+                nsteps, nmeshes, P, E);
+    IAC_REQUIRE(opt->beta1 >= 0 && opt->beta1 < 1 && opt->beta2 >= 0 && opt->beta2 < 1 && opt->eps > 0,
+                "AdamW hyper-parameters out of range");
+    iac_status st = check_dims(dn, nb, P, P, P);
+    if (st != IAC_OK) return st;
+    DeviceGuard guard(dn->ctx->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaStream_t caller = s;
+    if (!s) {
+        // the legacy default stream cannot be captured: replay on a stream of
+        // the denoiser, ordered after and before the caller's work by events
+        if (!dn->own_stream) {
+            DN_CHECK(cudaStreamCreateWithFlags(&dn->own_stream, cudaStreamNonBlocking), "replay stream");
+            DN_CHECK(cudaEventCreateWithFlags(&dn->own_ev[0], cudaEventDisableTiming), "replay event");
+            DN_CHECK(cudaEventCreateWithFlags(&dn->own_ev[1], cudaEventDisableTiming), "replay event");
+        }
+        s = dn->own_stream;
+        DN_CHECK(cudaEventRecord(dn->own_ev[0], caller), "order replay");
+        DN_CHECK(cudaStreamWaitEvent(s, dn->own_ev[0], 0), "order replay");
+    }
+    const size_t vox = (size_t)dn->max_batch * dn->D * dn->H * dn->W;
+    if (!dn->px) {
+        dn->px = (float *)dn->alloc(vox * 4);
+        dn->pt = (float *)dn->alloc(vox * 4);
+        IAC_REQUIRE(dn->px && dn->pt, "device memory for the training patches");
+    }
+    std::vector<uintptr_t> key = {(uintptr_t)d_in_meshes, (uintptr_t)d_tgt_meshes, nmeshes, E,
+                                  (uintptr_t)d_plans, (uintptr_t)d_lrs, nb, P, (uintptr_t)d_losses,
+                                  (uintptr_t)s};
+    const float hp[4] = {opt->beta1, opt->beta2, opt->eps, opt->weight_decay};
+    for (float f : hp) {
+        uint32_t u;
+        std::memcpy(&u, &f, 4);
+        key.push_back(u);
+    }
+    if (!dn->step_exec || key != dn->step_key) {
+        if (dn->step_exec) {
+            cudaGraphExecDestroy(dn->step_exec);
+            dn->step_exec = nullptr;
+        }
+        // one step, captured once: two patch crops, forward + loss + backward,
+        // AdamW (schedule and step count read from device memory), step advance
+        DN_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed), "begin capture");
+        double *loss = d_losses ? d_losses : dn->d_dummy_loss;
+        const long long *step = dn->d_step;
+        cudaError_t ce = crop_patches(reinterpret_cast<const bf16 *>(d_in_meshes), (int)nmeshes, (int)E, d_plans,
+                                      (int)nb, (int)P, dn->px, dn->ctx->d_counters, s, step);
+        if (ce == cudaSuccess)
+            ce = crop_patches(reinterpret_cast<const bf16 *>(d_tgt_meshes), (int)nmeshes, (int)E, d_plans, (int)nb,
+                              (int)P, dn->pt, dn->ctx->d_counters, s, step);
+        if (ce == cudaSuccess) {
+            st = run_backward(dn, dn->px, dn->pt, nullptr, nb, P, P, P, nullptr, d_losses ? loss : dn->d_dummy_loss,
+                              d_losses ? step : nullptr, s);
+            if (st == IAC_OK) st = refresh_tiles(dn, opt, s, step, d_lrs);
+            if (st == IAC_OK) ce = step_counter(dn->d_step, 0, 1, s);
+        }
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(s, &graph);
+        if (ce != cudaSuccess || st != IAC_OK || ee != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            if (st != IAC_OK) return st;
+            DN_CHECK(ce != cudaSuccess ? ce : ee, "capture of the training step");
+        }
+        const cudaError_t ie = cudaGraphInstantiate(&dn->step_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        DN_CHECK(ie, "instantiate the training-step graph");
+        dn->step_key = key;
+    }
+    DN_CHECK(step_counter(dn->d_step, dn->adam_step, 0, s), "reset the step counter");
+    if (d_losses) DN_CHECK(cudaMemsetAsync(d_losses, 0, (size_t)nsteps * 8, s), "clear losses");
+    for (uint32_t i = 0; i < nsteps; i++) DN_CHECK(cudaGraphLaunch(dn->step_exec, s), "training-step graph");
+    if (s != caller) {
+        DN_CHECK(cudaEventRecord(dn->own_ev[1], s), "order replay");
+        DN_CHECK(cudaStreamWaitEvent(caller, dn->own_ev[1], 0), "order replay");
+    }
+    dn->adam_step += nsteps;
+    dn->ctx->launches += (uint64_t)nsteps * 54;
+    return IAC_OK;
 }
 
 iac_status iac_denoise_crop_patches(iac_ctx *ctx, const uint16_t *d_meshes, uint32_t nmeshes, uint32_t E,

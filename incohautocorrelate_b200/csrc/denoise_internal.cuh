@@ -87,7 +87,8 @@ struct HeadArgs {
     float *out;           // [V] or null
     bf16 *gd;             // d(loss)/d(pre-activation of d), [V][16] (training)
     float *dw;            // head weight grads [17]
-    double *loss;         // sum of squared errors (training)
+    double *loss;         // sum of squared errors (training); + d_step[0] when d_step is set
+    const long long *d_step;  // graph replay: d_step[0] = step index
     const float *weight;  // optional per-voxel loss weight [V]
     long long V;
     double inv_count;     // 1 / (number of voxels in the loss)
@@ -109,12 +110,15 @@ struct AdamArgs {
     AdamLayer layers[MAX_LAYERS];
     int nlayers;
     int update;  // 0: only refresh the bf16 tiles from p
+    const long long *d_step;  // graph replay: lr = lrs[d_step[0]], bias corrections of step d_step[1] + 1
+    const float *lrs;
 };
 cudaError_t adamw(const AdamArgs &a, cudaStream_t s);
 
 cudaError_t mesh_input(const uint64_t *full, int S, int E, double scale, float *o32, bf16 *o16, cudaStream_t s);
 cudaError_t crop_patches(const bf16 *meshes, int nmesh, int E, const int *plan, int nb, int P, float *out,
-                         DeviceCounters *counters, cudaStream_t s);
+                         DeviceCounters *counters, cudaStream_t s, const long long *d_step = nullptr);
+cudaError_t step_counter(long long *d_step, long long set_opt, int advance, cudaStream_t s);
 
 }  // namespace dn
 }  // namespace iac

@@ -2018,7 +2018,7 @@ __global__ void __launch_bounds__(256) head_kernel(const HeadArgs a)
         if (threadIdx.x < 17)
             atomicAdd(&a.dw[threadIdx.x], t);
         else
-            atomicAdd(a.loss, (double)t);
+            atomicAdd(a.loss + (a.d_step ? a.d_step[0] : 0), (double)t);
     }
 }
 
@@ -2044,13 +2044,20 @@ __global__ void adamw_kernel(const AdamArgs a)
     const bool is_w = j < nw;
     float p = a.p[i];
     if (a.update) {
+        float lr = a.lr, bc1 = a.bc1, bc2 = a.bc2;
+        if (a.d_step) {  // graph replay: step index and schedule from device memory
+            const float t = (float)(a.d_step[1] + 1);
+            lr = a.lrs[a.d_step[0]];
+            bc1 = 1.0f - powf(a.beta1, t);
+            bc2 = 1.0f - powf(a.beta2, t);
+        }
         const float g = a.g[i];
         const float m = a.beta1 * a.m[i] + (1.0f - a.beta1) * g;
         const float v = a.beta2 * a.v[i] + (1.0f - a.beta2) * g * g;
         a.m[i] = m;
         a.v[i] = v;
-        const float step = (m / a.bc1) / (sqrtf(v / a.bc2) + a.eps);
-        p -= a.lr * (step + (is_w ? a.weight_decay * p : 0.0f));
+        const float step = (m / bc1) / (sqrtf(v / bc2) + a.eps);
+        p -= lr * (step + (is_w ? a.weight_decay * p : 0.0f));
         a.p[i] = p;
     }
     if (!L.taps || !is_w) return;
@@ -2077,7 +2084,8 @@ cudaError_t adamw(const AdamArgs &a, cudaStream_t s)
 // of mesh (E^3, bf16) under one of the 48 axis permutations x reflections
 // --------------------------------------------------------------------------
 __global__ void crop_kernel(const bf16 *__restrict__ meshes, int nmesh, int E, const int *__restrict__ plan, int P,
-                            float *__restrict__ out, long long total, DeviceCounters *counters)
+                            float *__restrict__ out, long long total, DeviceCounters *counters,
+                            const long long *__restrict__ d_step, int nb)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
@@ -2085,7 +2093,12 @@ __global__ void crop_kernel(const bf16 *__restrict__ meshes, int nmesh, int E, c
     const int b = (int)(i / per);
     const long long r = i % per;
     int c[3] = {(int)(r / ((long long)P * P)), (int)((r / P) % P), (int)(r % P)};
-    const int *pl = plan + 5 * b;
+    const int *pl = plan + 5 * ((d_step ? d_step[0] * nb : 0) + b);
+    if ((unsigned)pl[4] >= 48u || (unsigned)pl[0] >= (unsigned)nmesh) {
+        out[i] = 0.0f;  // a plan entry outside the meshes: counted, not read
+        if (counters) atomicAdd(&counters->out_of_mesh, 1ull);
+        return;
+    }
     const int perm = pl[4] % 6, flip = pl[4] / 6;
     const int pa = perm / 2, pb = (perm / 2 + 1 + (perm & 1)) % 3, pc = 3 - pa - pb;
     const int src_axis[3] = {pa, pb, pc};
@@ -2095,8 +2108,7 @@ __global__ void crop_kernel(const bf16 *__restrict__ meshes, int nmesh, int E, c
         if (flip & (1 << k)) t = P - 1 - t;
         s[k] = t + pl[1 + k];
     }
-    if ((unsigned)pl[0] >= (unsigned)nmesh || (unsigned)s[0] >= (unsigned)E || (unsigned)s[1] >= (unsigned)E ||
-        (unsigned)s[2] >= (unsigned)E || (unsigned)pl[4] >= 48u) {
+    if ((unsigned)s[0] >= (unsigned)E || (unsigned)s[1] >= (unsigned)E || (unsigned)s[2] >= (unsigned)E) {
         out[i] = 0.0f;  // a plan entry outside the meshes: counted, not read
         if (counters) atomicAdd(&counters->out_of_mesh, 1ull);
         return;
@@ -2105,10 +2117,29 @@ __global__ void crop_kernel(const bf16 *__restrict__ meshes, int nmesh, int E, c
 }
 
 cudaError_t crop_patches(const bf16 *meshes, int nmesh, int E, const int *plan, int nb, int P, float *out,
-                         DeviceCounters *counters, cudaStream_t s)
+                         DeviceCounters *counters, cudaStream_t s, const long long *d_step)
 {
     const long long total = (long long)nb * P * P * P;
-    crop_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(meshes, nmesh, E, plan, P, out, total, counters);
+    crop_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(meshes, nmesh, E, plan, P, out, total, counters,
+                                                                d_step, nb);
+    return cudaGetLastError();
+}
+
+// graph replay bookkeeping: d_step[0] = replay index, d_step[1] = optimizer steps
+__global__ void step_kernel(long long *d_step, long long set_opt, int mode)
+{
+    if (mode == 0) {
+        d_step[0] = 0;
+        d_step[1] = set_opt;
+    } else {
+        d_step[0] += 1;
+        d_step[1] += 1;
+    }
+}
+
+cudaError_t step_counter(long long *d_step, long long set_opt, int advance, cudaStream_t s)
+{
+    step_kernel<<<1, 1, 0, s>>>(d_step, set_opt, advance);
     return cudaGetLastError();
 }
 

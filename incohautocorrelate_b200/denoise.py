@@ -204,7 +204,10 @@ class TrainConfig:
 
 def train(ctx, xin, tgt, cfg: TrainConfig, log=print, dn=None):
     """Train on random patches (any of the 48 axis permutations/reflections:
-    the crystal ensemble is symmetric under them) of the mesh pairs."""
+    the crystal ensemble is symmetric under them) of the mesh pairs.  Steps
+    run as replays of one captured CUDA graph (iac_denoise_train_steps); the
+    patch plans and the learning-rate schedule (linear warm-up, cosine decay)
+    are uploaded once."""
     import torch
     n, E = xin.shape[0], xin.shape[1]
     P, B = cfg.patch, cfg.batch
@@ -212,38 +215,38 @@ def train(ctx, xin, tgt, cfg: TrainConfig, log=print, dn=None):
         dn = capi.Denoiser(ctx, B, P, P, P, backend=cfg.backend)
         dn.init_params(cfg.seed)
     rng = np.random.default_rng(cfg.seed)
-    x = torch.zeros((B, P, P, P), dtype=torch.float32, device="cuda")
-    t = torch.zeros_like(x)
-    # every step's patch plan (mesh, z0, y0, x0, transform), uploaded once
     plans = np.stack([rng.integers(0, n, (cfg.steps, B)), rng.integers(0, E - P + 1, (cfg.steps, B)),
                       rng.integers(0, E - P + 1, (cfg.steps, B)), rng.integers(0, E - P + 1, (cfg.steps, B)),
                       rng.integers(0, 48, (cfg.steps, B))], 2).astype(np.int32)
-    plan_d = torch.from_numpy(plans).cuda()
+    step = np.arange(cfg.steps)
+    f = np.clip((step - cfg.warmup) / max(1, cfg.steps - cfg.warmup), 0.0, 1.0)
+    lrs = np.where(step < cfg.warmup, cfg.lr * (step + 1) / cfg.warmup,
+                   cfg.lr_min + 0.5 * (cfg.lr - cfg.lr_min) * (1 + np.cos(np.pi * f))).astype(np.float32)
+    chunk = 100
     stream = torch.cuda.current_stream()
+    losses = torch.zeros(chunk, dtype=torch.float64, device="cuda")
     hist = []
     t0 = time.perf_counter()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    timed_from = min(20, cfg.steps - 1)
-    for step in range(cfg.steps):
-        if step == timed_from:
+    timed = 0
+    for s0 in range(0, cfg.steps, chunk):
+        k = min(chunk, cfg.steps - s0)
+        d_plans = torch.from_numpy(np.ascontiguousarray(plans[s0:s0 + k])).cuda()
+        d_lrs = torch.from_numpy(np.ascontiguousarray(lrs[s0:s0 + k])).cuda()
+        if s0 == chunk:
             ev0.record(stream)
-        capi.denoise_crop_patches(ctx, xin, n, E, plan_d[step], B, P, x, stream=stream.cuda_stream)
-        capi.denoise_crop_patches(ctx, tgt, n, E, plan_d[step], B, P, t, stream=stream.cuda_stream)
-        want = step % 100 == 0 or step == cfg.steps - 1
-        loss = dn.backward(x, t, B, P, P, P, stream=stream.cuda_stream, want_loss=want)
-        if step < cfg.warmup:
-            lr = cfg.lr * (step + 1) / cfg.warmup
-        else:
-            f = (step - cfg.warmup) / max(1, cfg.steps - cfg.warmup)
-            lr = cfg.lr_min + 0.5 * (cfg.lr - cfg.lr_min) * (1 + math.cos(math.pi * f))
-        dn.adamw_step(lr=lr, weight_decay=cfg.weight_decay, stream=stream.cuda_stream)
-        if want:
-            hist.append((step, loss))
-            if log:
-                log(f"  step {step:5d}  loss {loss:.5f}  lr {lr:.2e}  {time.perf_counter() - t0:.1f} s")
+        dn.train_steps(xin, tgt, n, E, d_plans, d_lrs, k, B, P, d_losses=losses[:k], stream=stream.cuda_stream,
+                       weight_decay=cfg.weight_decay)
+        if s0 >= chunk:
+            timed += k
+        mean = losses[:k].cpu().numpy() / (B * P ** 3)
+        hist.append((s0, float(mean[0])))
+        if log and (s0 // chunk) % 10 == 0:
+            log(f"  step {s0:5d}  loss {mean[0]:.5f}  lr {lrs[s0]:.2e}  {time.perf_counter() - t0:.1f} s")
     ev1.record(stream)
     torch.cuda.synchronize()
-    ms_step = ev0.elapsed_time(ev1) / max(1, cfg.steps - timed_from)
+    hist.append((cfg.steps - 1, float(losses[(cfg.steps - 1) % chunk].item() / (B * P ** 3))))
+    ms_step = ev0.elapsed_time(ev1) / timed if timed else float("nan")
     return dn, hist, ms_step
 
 

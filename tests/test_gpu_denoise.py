@@ -247,3 +247,47 @@ def test_trained_denoiser_needs_fewer_frames_than_the_plain_mesh(ctx):
         assert r["err_denoised"] < 0.5 * r["err_plain"][500], r
     assert summary["median_gain"] > 8.0, summary
     dn.close()
+
+
+def test_graph_replayed_training_matches_eager_steps(ctx, rng):
+    """iac_denoise_train_steps (one captured step, replayed) follows the same
+    trajectory as the same steps issued one call at a time (fp32 atomics make
+    the sums order-dependent, hence a tolerance)."""
+    import torch
+    from incohautocorrelate_b200 import capi
+    nmesh, E, nb, P, steps = 3, 32, 2, 16, 6
+    m_in = rng.gamma(2.0, 0.5, (nmesh, E, E, E)).astype(np.float32)
+    m_tg = (m_in * (1 + 0.1 * rng.normal(size=m_in.shape))).astype(np.float32)
+    d_in = torch.from_numpy(m_in).to(torch.bfloat16).view(torch.int16).cuda()
+    d_tg = torch.from_numpy(m_tg).to(torch.bfloat16).view(torch.int16).cuda()
+    plans = np.stack([rng.integers(0, nmesh, (steps, nb)), rng.integers(0, E - P + 1, (steps, nb)),
+                      rng.integers(0, E - P + 1, (steps, nb)), rng.integers(0, E - P + 1, (steps, nb)),
+                      rng.integers(0, 48, (steps, nb))], 2).astype(np.int32)
+    lrs = np.linspace(1e-3, 2e-4, steps).astype(np.float32)
+    d_plans, d_lrs = torch.from_numpy(plans).cuda(), torch.from_numpy(lrs).cuda()
+    p0 = _random_params(rng)
+    eager = capi.Denoiser(ctx, nb, P, P, P)
+    eager.set_params(p0)
+    x = torch.zeros((nb, P, P, P), dtype=torch.float32, device="cuda")
+    t = torch.zeros_like(x)
+    want = []
+    for i in range(steps):
+        capi.denoise_crop_patches(ctx, d_in, nmesh, E, d_plans[i], nb, P, x)
+        capi.denoise_crop_patches(ctx, d_tg, nmesh, E, d_plans[i], nb, P, t)
+        want.append(eager.backward(x, t, nb, P, P, P) * nb * P ** 3)
+        eager.adamw_step(lr=float(lrs[i]))
+    graph = capi.Denoiser(ctx, nb, P, P, P)
+    graph.set_params(p0)
+    losses = torch.zeros(steps, dtype=torch.float64, device="cuda")
+    graph.train_steps(d_in, d_tg, nmesh, E, d_plans, d_lrs, steps, nb, P, d_losses=losses)
+    torch.cuda.synchronize()
+    assert ctx.check() == 0
+    np.testing.assert_allclose(losses.cpu().numpy(), want, rtol=2e-3)
+    a, b = graph.get_params(), eager.get_params()
+    assert np.linalg.norm(a - b) / np.linalg.norm(b - p0) < 1e-2
+    # a second call reuses the graph and continues the optimizer's step count
+    graph.train_steps(d_in, d_tg, nmesh, E, d_plans, d_lrs, steps, nb, P, d_losses=losses)
+    torch.cuda.synchronize()
+    assert np.isfinite(losses.cpu().numpy()).all()
+    eager.close()
+    graph.close()
