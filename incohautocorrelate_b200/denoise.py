@@ -225,17 +225,20 @@ def train(ctx, xin, tgt, cfg: TrainConfig, log=print, dn=None):
     chunk = 100
     stream = torch.cuda.current_stream()
     losses = torch.zeros(chunk, dtype=torch.float64, device="cuda")
+    # fixed device buffers, so the captured step graph is reused by every chunk
+    d_plans = torch.zeros((chunk, B, 5), dtype=torch.int32, device="cuda")
+    d_lrs = torch.zeros(chunk, dtype=torch.float32, device="cuda")
     hist = []
     t0 = time.perf_counter()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     timed = 0
     for s0 in range(0, cfg.steps, chunk):
         k = min(chunk, cfg.steps - s0)
-        d_plans = torch.from_numpy(np.ascontiguousarray(plans[s0:s0 + k])).cuda()
-        d_lrs = torch.from_numpy(np.ascontiguousarray(lrs[s0:s0 + k])).cuda()
+        d_plans[:k].copy_(torch.from_numpy(np.ascontiguousarray(plans[s0:s0 + k])))
+        d_lrs[:k].copy_(torch.from_numpy(np.ascontiguousarray(lrs[s0:s0 + k])))
         if s0 == chunk:
             ev0.record(stream)
-        dn.train_steps(xin, tgt, n, E, d_plans, d_lrs, k, B, P, d_losses=losses[:k], stream=stream.cuda_stream,
+        dn.train_steps(xin, tgt, n, E, d_plans, d_lrs, k, B, P, d_losses=losses, stream=stream.cuda_stream,
                        weight_decay=cfg.weight_decay)
         if s0 >= chunk:
             timed += k
