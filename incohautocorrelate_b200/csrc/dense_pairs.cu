@@ -54,6 +54,7 @@ struct DenseArgs {
     unsigned long long npairs;  // tile pairs
     uint32_t nx, ny, ptx;       // 2D patch tiling: row length, rows, patches per row (nx = 0: linear)
     uint32_t mult_int;          // Multiplicator as an integer below 2^29, else 0
+    int key_ok;                 // |round(q * Voxel_per_dq)| < 512 for every pair within MaxQ
     float maxq, maxq2;
     float vpdq;
     double mult;
@@ -299,6 +300,54 @@ __device__ __forceinline__ void cq_pairs(const DenseArgs &a, const Window &w, un
     }
 }
 
+// scaled_floor for a normal p > 0 (every product that passes the 1e-37 test)
+__device__ __forceinline__ unsigned long long scaled_floor_normal(float p, uint32_t M)
+{
+    const uint32_t b = __float_as_uint(p);
+    const unsigned long long prod = (unsigned long long)((b & 0x7fffffu) | 0x800000u) * M;
+    const int sh = (int)(b >> 23) - 150;  // p = mantissa * 2^sh
+    return sh >= 0 ? (prod << sh) : (prod >> min(-sh, 63));
+}
+
+// nearest-voxel pairs with a compile-time axis mapping: the voxel is compared
+// as one packed key f + 1024 m + 2^20 s (components within +-511, which
+// key_ok guarantees for every pair inside MaxQ), the value path is chosen at
+// compile time (MINT: integer Multiplicator)
+template <int KA, int KB, int KC, bool CHECK, bool MINT>
+__device__ __forceinline__ void cq_pairs_nn(const DenseArgs &a, const Window &w, unsigned long long *win,
+                                            const float4 *sq, int j0, float k0, float k1, float k2, float Ia)
+{
+    constexpr int NONE = -2147483647 - 1;
+    int cur = NONE, cf = 0, cm = 0, cs = 0;
+    unsigned long long acc = 0;
+    const float vpdq = a.vpdq;
+#pragma unroll 2
+    for (int j = j0; j < DTILE; j++) {
+        const float4 b = sq[j];
+        const float pv = fmul(Ia, b.w);
+        if (pv < 1e-37f) continue;
+        float qx = fsub(k0, b.x), qy = fsub(k1, b.y), qz = fsub(k2, b.z);
+        if (CHECK && fadd(fadd(fmul(qx, qx), fmul(qy, qy)), fmul(qz, qz)) > a.maxq2) continue;
+        qx = fmul(qx, vpdq);
+        qy = fmul(qy, vpdq);
+        qz = fmul(qz, vpdq);
+        const int f = round_half_away(axis<KA>(qx, qy, qz, 0));
+        const int m = round_half_away(axis<KB>(qx, qy, qz, 0));
+        const int s = round_half_away(axis<KC>(qx, qy, qz, 0));
+        const int key = f + m * 1024 + s * 1048576;
+        if (key != cur) {
+            if (cur != NONE) put(a, w, win, cf + a.cab, cm + a.cab, cs + a.cc, acc);
+            cur = key;
+            cf = f;
+            cm = m;
+            cs = s;
+            acc = 0;
+        }
+        acc += MINT ? scaled_floor_normal(pv, a.mult_int) : d2u64(dmul((double)pv, a.mult));
+    }
+    if (cur != NONE) put(a, w, win, cf + a.cab, cm + a.cab, cs + a.cc, acc);
+}
+
 // upper bound of |k_a - k_b| over two boxes is below MaxQ with a margin that
 // covers the FP32 rounding of the per-pair test (every pair passes it)
 __device__ __forceinline__ bool boxes_within(const float4 a0, const float4 a1, const float4 b0, const float4 b1,
@@ -370,10 +419,23 @@ __global__ void __launch_bounds__(DTILE) cq_small_kernel(const DenseArgs a)
                     self = a.mult_int ? scaled_floor(sv, a.mult_int) : d2u64(dmul((double)sv, a.mult));
             }
             const int j0 = (P == Q) ? threadIdx.x + 1 : 0;
-            if (check)
+            if (INTERP == 0 && KA >= 0 && a.key_ok) {
+                if (a.mult_int) {
+                    if (check)
+                        cq_pairs_nn<KA, KB, KC, true, true>(a, w, win, sq, j0, k0, k1, k2, Ia);
+                    else
+                        cq_pairs_nn<KA, KB, KC, false, true>(a, w, win, sq, j0, k0, k1, k2, Ia);
+                } else {
+                    if (check)
+                        cq_pairs_nn<KA, KB, KC, true, false>(a, w, win, sq, j0, k0, k1, k2, Ia);
+                    else
+                        cq_pairs_nn<KA, KB, KC, false, false>(a, w, win, sq, j0, k0, k1, k2, Ia);
+                }
+            } else if (check) {
                 cq_pairs<INTERP, KA, KB, KC, true>(a, w, win, sq, j0, k0, k1, k2, Ia);
-            else
+            } else {
                 cq_pairs<INTERP, KA, KB, KC, false>(a, w, win, sq, j0, k0, k1, k2, Ia);
+            }
         }
         // self pairs of a diagonal tile: once, at the centre
         for (int o = 16; o; o >>= 1) self += __shfl_xor_sync(0xffffffffu, self, o);
@@ -552,6 +614,9 @@ iac_status iac_cq_small(iac_ctx *ctx, const float *d_I, const float *d_kmap, uin
     a.ka = (int)sh->k_a;
     a.kb = (int)sh->k_b;
     a.kc = (int)sh->k_c;
+    // every pair within MaxQ has |q * Voxel_per_dq| <= MaxQ * Voxel_per_dq (up to
+    // rounding): below 500 the packed voxel key cannot alias
+    a.key_ok = (double)sh->max_q * (double)sh->voxel_per_dq < 500.0;
     const int grid = ctx->sm_count * 8;
     // the axis mapping is a permutation for every real detector: one
     // instantiation per permutation, a runtime-mapped one otherwise
