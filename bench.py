@@ -458,6 +458,12 @@ def _fp32_peak_tflops(clock_mhz):
     return 148 * 128 * 2 * clock_mhz * 1e6 / 1e12
 
 
+# thread instructions per unordered pixel pair (ncu smsp__inst_executed.sum x 32 / pairs, 256^2
+# detector; profiles/cq_small_kernel.md, profiles/ac1d_cq_kernel.md)
+INST_PER_PAIR = {"cq_small": 7698927703 * 32 / (65536 * 65537 / 2),
+                 "ac1d_cq": 8217131069 * 32 / (65536 * 65537 / 2)}
+
+
 def _time(fn, steps, warmup, stream):
     import torch
     for _ in range(warmup):
@@ -528,7 +534,15 @@ def run_kernel(args):
                               "frac": rate * flops / 1e12 / _fp32_peak_tflops(mhz),
                               "peak_source": "derived 148 SM x 128 FP32 lanes x 2 at the sampled "
                                              "clock (no measured FP32 peak)",
-                              "flop_per_pair": flops})
+                              "flop_per_pair": flops,
+                              # the binding resource: instruction issue.  Instructions per pair
+                              # from the committed ncu capture of this kernel (256^2 detector)
+                              "issue": {"inst_per_pair": INST_PER_PAIR[args.kernel],
+                                        "achieved": rate * INST_PER_PAIR[args.kernel],
+                                        "peak": 148 * 4 * 32 * mhz * 1e6,
+                                        "frac": rate * INST_PER_PAIR[args.kernel] / (148 * 4 * 32 * mhz * 1e6),
+                                        "unit": "thread instructions/s",
+                                        "source": f"profiles/{args.kernel}_kernel.md"}})
         if not args.no_cpu_baseline:
             rows = 48
             Ih = np.ascontiguousarray(I)
