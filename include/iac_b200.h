@@ -339,6 +339,26 @@ iac_status iac_sparsify_frames(iac_ctx *ctx, const float *d_intensity, const int
                                void *stream);
 
 /* ---------------------------------------------------------------------- */
+/* averaged intensity and per-event statistics                               */
+/* ---------------------------------------------------------------------- */
+
+/* Detector::LoadAndAverageIntensity (IAC/Detector.cpp:687-790) for a batch of
+ * loaded frames [nframes][npix] (fp32, events in order): masked by d_mask
+ * (int per pixel, optional), then either thresholded and added to d_sum
+ * (step <= 0) or discretised to photons and counted in d_discr (step > 0);
+ * d_sum / d_discr accumulate across batches.  Per frame, d_mean_intensity =
+ * sequential FP32 sum / npix (the event's MeanIntensity) and, with step > 0,
+ * d_photon_sum = the sum itself (PhotonCount = (int)sum).  Bit-exact with the
+ * reference.  Asynchronous. */
+iac_status iac_average_frames(iac_ctx *ctx, const float *d_frames, uint64_t npix, uint32_t nframes,
+                              const int32_t *d_mask, float threshold, float step, float *d_sum,
+                              int64_t *d_discr, float *d_mean_intensity, float *d_photon_sum,
+                              void *stream);
+/* Intensity = (step > 0 ? (float)d_discr : d_sum) * (1 / nframes_total). */
+iac_status iac_average_finish(iac_ctx *ctx, const float *d_sum, const int64_t *d_discr, uint64_t npix,
+                              uint32_t nframes_total, float *d_intensity, void *stream);
+
+/* ---------------------------------------------------------------------- */
 /* mesh denoiser -- no counterpart in the reference                          */
 /* ---------------------------------------------------------------------- */
 

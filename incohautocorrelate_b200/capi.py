@@ -137,6 +137,8 @@ def _declare(lib):
     fn("iac_simulate_photons", [_VP, _VP, _U64, _U32, _U64, C.POINTER(PhotonParams), _U64, _VP])
     fn("iac_sparsify_frames", [_VP, _VP, _VP, _VP, _U64, _U32, C.c_float, C.c_float, C.c_int,
                                _VP, _U64, _VP, C.POINTER(_U64), _VP])
+    fn("iac_average_frames", [_VP, _VP, _U64, _U32, _VP, C.c_float, C.c_float, _VP, _VP, _VP, _VP, _VP])
+    fn("iac_average_finish", [_VP, _VP, _VP, _U64, _U32, _VP, _VP])
     fn("iac_denoise_param_count", [], _U64)
     fn("iac_denoise_create", [_VP, _U32, _U32, _U32, _U32, C.c_int, C.POINTER(_VP)])
     fn("iac_denoise_destroy", [_VP], None)
@@ -377,6 +379,16 @@ class Context:
                                         _ptr(d_offsets), C.byref(tot) if want_total else None,
                                         _ptr(stream)))
         return int(tot.value)
+
+    def average_frames(self, d_frames, npix, nframes, d_mask, threshold, step, d_sum, d_discr,
+                       d_mean, d_photon_sum=None, stream=None):
+        check(lib().iac_average_frames(self._h, _ptr(d_frames), int(npix), int(nframes), _ptr(d_mask),
+                                       float(threshold), float(step), _ptr(d_sum), _ptr(d_discr),
+                                       _ptr(d_mean), _ptr(d_photon_sum), _ptr(stream)))
+
+    def average_finish(self, d_sum, d_discr, npix, nframes_total, d_intensity, stream=None):
+        check(lib().iac_average_finish(self._h, _ptr(d_sum), _ptr(d_discr), int(npix), int(nframes_total),
+                                       _ptr(d_intensity), _ptr(stream)))
 
     def bench_scatter_add(self, d_buf, words, word_bits, updates, seed=1, stream=None):
         check(lib().iac_bench_scatter_add(self._h, _ptr(d_buf), int(words), int(word_bits),

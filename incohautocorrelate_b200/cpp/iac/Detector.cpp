@@ -168,49 +168,60 @@ void Detector::LoadIntensityData(Settings::HitEvent *Event, Settings &Options)
     Checklist.Intensity = true;
 }
 
-// IAC/Detector.cpp:687-790
+// IAC/Detector.cpp:687-790.  Frames are loaded on the host (FrameSource) in
+// batches into pinned memory; masking, thresholding / photon discretisation,
+// the per-pixel accumulation and the per-event sums run on the device
+// (iac_average_frames, bit-exact with the reference).  As in the reference
+// the pixel mask is always applied (a mask of ones when none was loaded).
 void Detector::LoadAndAverageIntensity(std::vector<Settings::HitEvent> &Events, float Threshold,
-                                       float Step, int Lower, int Upper, bool Pixelmask,
+                                       float Step, int Lower, int Upper, bool /*Pixelmask*/,
                                        Settings &Options)
 {
-    if (Events.empty()) return;
+    if (Events.empty() || Upper <= Lower) return;
+    if (!Options.Frames) throw std::runtime_error("Settings::Frames (frame source) is not set");
     if (!Checklist.PixelMask) GenerateFlatOnesPixelMask();
+    iac_ctx *ctx = Options.Context();
+    void *s = Options.Stream();
     const size_t n = Pixels();
-    std::vector<float> tmp(n);
-    std::vector<long> discr(Step > 0 ? n : 0, 0);
-    std::fill(Intensity, Intensity + n, 0.0f);
-    for (int i = Lower; i < Upper; i++) {
-        if (!Options.Frames) throw std::runtime_error("Settings::Frames (frame source) is not set");
-        Options.Frames->Load(Events[i].Filename, Events[i].Dataset, Events[i].Event, tmp.data(), n);
-        if (Pixelmask && Checklist.PixelMask)
-            for (size_t j = 0; j < n; j++) tmp[j] = tmp[j] * (float)PixelMask[j];
-        float sum = 0.0f;
-        if (Step <= 0) {
-            if (Threshold > 0)
-                for (size_t j = 0; j < n; j++)
-                    if (tmp[j] < Threshold) tmp[j] = 0.0f;
-            for (size_t j = 0; j < n; j++)
-                if (tmp[j] >= Threshold) Intensity[j] += tmp[j];
-            for (size_t j = 0; j < n; j++) sum += tmp[j];
-            Events[i].MeanIntensity = sum / ((float)n);
-        } else {
-            for (size_t j = 0; j < n; j++) {
-                if (tmp[j] >= Threshold) {
-                    tmp[j] = std::ceil((tmp[j] - Threshold) / Step) * (float)(tmp[j] >= Threshold);
-                    discr[j] += (long)std::floor(tmp[j] + 0.5);
-                } else {
-                    tmp[j] = 0;
-                }
-            }
-            for (size_t j = 0; j < n; j++) sum += tmp[j];
-            Events[i].PhotonCount = (int)sum;
-            Events[i].MeanIntensity = sum / ((float)n);
+    const uint32_t batch = (uint32_t)std::max<size_t>(1, std::min<size_t>(64, (size_t)(256u << 20) / (4 * n)));
+    void *h_frames = nullptr;
+    Check(iac_host_alloc_pinned(ctx, 4 * n * batch, &h_frames), "pinned frame batch");
+    struct PinnedGuard {
+        iac_ctx *c;
+        void *p;
+        ~PinnedGuard() { iac_host_free_pinned(c, p); }
+    } pin{ctx, h_frames};
+    DevBuf dF(ctx, 4 * n * batch), dMask(ctx, 4 * n), dSum(ctx, 4 * n), dDiscr(ctx, 8 * n), dMean(ctx, 4 * batch),
+        dPh(ctx, 4 * batch), dOut(ctx, 4 * n);
+    Check(iac_memcpy_h2d(ctx, dMask.p, PixelMask, 4 * n, s), "copy mask");
+    Check(iac_memset_device(ctx, dSum.p, 0, 4 * n, s), "clear sum");
+    Check(iac_memset_device(ctx, dDiscr.p, 0, 8 * n, s), "clear counts");
+    std::vector<float> mean(batch), ph(batch);
+    float *hf = static_cast<float *>(h_frames);
+    for (int i0 = Lower; i0 < Upper; i0 += (int)batch) {
+        const uint32_t nb = (uint32_t)std::min<int>((int)batch, Upper - i0);
+        Check(iac_stream_synchronize(ctx, s), "synchronize");  // the pinned batch is free again
+        for (uint32_t k = 0; k < nb; k++)
+            Options.Frames->Load(Events[i0 + k].Filename, Events[i0 + k].Dataset, Events[i0 + k].Event,
+                                 hf + (size_t)k * n, n);
+        Check(iac_memcpy_h2d(ctx, dF.p, hf, 4 * n * nb, s), "copy frames");
+        Check(iac_average_frames(ctx, (const float *)dF.p, n, nb, (const int32_t *)dMask.p, Threshold, Step,
+                                 (float *)dSum.p, (int64_t *)dDiscr.p, (float *)dMean.p, (float *)dPh.p, s),
+              "iac_average_frames");
+        Check(iac_memcpy_d2h(ctx, mean.data(), dMean.p, 4 * nb, s), "copy mean intensities");
+        if (Step > 0) Check(iac_memcpy_d2h(ctx, ph.data(), dPh.p, 4 * nb, s), "copy photon counts");
+        Check(iac_stream_synchronize(ctx, s), "synchronize");
+        for (uint32_t k = 0; k < nb; k++) {
+            Events[i0 + k].MeanIntensity = mean[k];
+            if (Step > 0) Events[i0 + k].PhotonCount = (int)ph[k];
         }
     }
-    if (Step > 0)
-        for (size_t j = 0; j < n; j++) Intensity[j] = (float)discr[j];
-    const float f = 1.0f / ((float)(Upper - Lower));
-    for (size_t j = 0; j < n; j++) Intensity[j] *= f;
+    Check(iac_average_finish(ctx, Step > 0 ? nullptr : (const float *)dSum.p,
+                             Step > 0 ? (const int64_t *)dDiscr.p : nullptr, n, (uint32_t)(Upper - Lower),
+                             (float *)dOut.p, s),
+          "iac_average_finish");
+    Check(iac_memcpy_d2h(ctx, Intensity, dOut.p, 4 * n, s), "copy intensity");
+    Check(iac_stream_synchronize(ctx, s), "synchronize");
     Checklist.Intensity = true;
 }
 

@@ -55,6 +55,8 @@ def _decl(lib):
     fn("iaco_ac1d_shape_init", [P(F), U32, F, P(AC1DShape)])
     fn("iaco_discretize_to_photons", [VP, U64, F, F])
     fn("iaco_sparse_hitlist", [VP, VP, U64, F, F, C.c_int, VP], U64)
+    fn("iaco_average_frames", [VP, U64, U32, VP, F, F, VP, VP, VP, VP])
+    fn("iaco_average_finish", [VP, VP, U64, U32, VP])
     fn("iaco_sparse_ac_halfmesh", [VP, U32, VP, VP, VP], U64)
     fn("iaco_fold_halfmesh", [VP, U32, D, F, F, VP])
     fn("iaco_sparse_ac_cpu_route", [VP, U32, VP, P(MeshShape), C.c_int, C.c_int, C.c_int, F, F,

@@ -151,6 +151,56 @@ void iaco_discretize_to_photons(float *a, uint64_t n, float thr, float step)
     for (uint64_t i = 0; i < n; i++) a[i] = ceilf((a[i] - thr) / step) * (float)(a[i] >= thr);
 }
 
+/* Detector::LoadAndAverageIntensity, IAC/Detector.cpp:687-790, for a batch of
+ * loaded frames (events in order): mask (ParMultiplyElementwise,
+ * IAC/ArrayOperators.h:118-125); without discretisation zero values below a
+ * positive threshold and add values >= threshold to the running intensity
+ * (ParAdd with threshold, IAC/ArrayOperators.h:75-86); with a sampling step
+ * discretise (DiscretizeToPhotones, IAC/Detector.cpp:90-96) and add
+ * (long)floor(v + 0.5) to the per-pixel count; per event the sequential FP32
+ * Sum (IAC/ArrayOperators.h:259-267) gives MeanIntensity = Sum / npix and the
+ * photon sum.  sum / discr accumulate across calls. */
+void iaco_average_frames(const float *frames, uint64_t npix, uint32_t nframes, const int32_t *mask,
+                         float thr, float step, float *sum, int64_t *discr, float *mean_intensity,
+                         float *photon_sum)
+{
+    float *tmp = (float *)malloc(sizeof(float) * npix);
+    for (uint32_t f = 0; f < nframes; f++) {
+        const float *fr = frames + (size_t)f * npix;
+        for (uint64_t j = 0; j < npix; j++) tmp[j] = mask ? fr[j] * (float)mask[j] : fr[j];
+        if (step <= 0) {
+            if (thr > 0)
+                for (uint64_t j = 0; j < npix; j++)
+                    if (tmp[j] < thr) tmp[j] = 0.0f;
+            for (uint64_t j = 0; j < npix; j++)
+                if (tmp[j] >= thr) sum[j] += tmp[j];
+        } else {
+            for (uint64_t j = 0; j < npix; j++) {
+                if (tmp[j] >= thr) {
+                    iaco_discretize_to_photons(&tmp[j], 1, thr, step);
+                    discr[j] += (int64_t)floor(tmp[j] + 0.5);
+                } else {
+                    tmp[j] = 0;
+                }
+            }
+        }
+        float s = 0.0f;
+        for (uint64_t j = 0; j < npix; j++) s += tmp[j];
+        mean_intensity[f] = s / ((float)npix);
+        if (photon_sum && step > 0) photon_sum[f] = s;
+    }
+    free(tmp);
+}
+
+/* the end of LoadAndAverageIntensity: Intensity = (float)count (discretised)
+ * or the running sum, times 1 / nframes (ParMultiplyScalar) */
+void iaco_average_finish(const float *sum, const int64_t *discr, uint64_t npix, uint32_t nframes_total,
+                         float *intensity)
+{
+    const float f = 1.0f / ((float)nframes_total);
+    for (uint64_t j = 0; j < npix; j++) intensity[j] = (discr ? (float)discr[j] : sum[j]) * f;
+}
+
 /* Detector::CreateSparseHitList(Threshold[, Step]), IAC/Detector.cpp:926-958:
  * keep pixels with I >= Threshold and I > 0 in pixel order, then photonise the
  * value.  out4 receives (kx, ky, kz, value) per kept pixel. */

@@ -49,6 +49,11 @@ void iaco_ac1d_shape_init(const float max_q[3], uint32_t array_size, float q_zoo
 
 /* ---- photonisation / sparse list ------------------------------------- */
 void iaco_discretize_to_photons(float *a, uint64_t n, float threshold, float step);
+void iaco_average_frames(const float *frames, uint64_t npix, uint32_t nframes, const int32_t *mask,
+                         float threshold, float step, float *sum, int64_t *discr, float *mean_intensity,
+                         float *photon_sum);
+void iaco_average_finish(const float *sum, const int64_t *discr, uint64_t npix, uint32_t nframes_total,
+                         float *intensity);
 uint64_t iaco_sparse_hitlist(const float *intensity, const float *kmap, uint64_t npix,
                              float threshold, float step, int photonize, float *out4);
 
