@@ -55,7 +55,7 @@ def parse():
                     help="denoiser convolutions: 0 = tcgen05 + TMEM, 1 = mma.sync")
     ap.add_argument("--kernel", default="sparse",
                     choices=["sparse", "cq_small", "ac1d_cq", "cq_merge", "ac1d_sparse", "simulate",
-                             "denoise"],
+                             "denoise", "average"],
                     help="sparse is the headline; the others measure the remaining kernels "
                          "of the path on their configurations")
     return ap.parse_args()
@@ -626,6 +626,54 @@ def run_kernel(args):
         line.update(simulate_pipeline(args, ctx, stream, clocks, nthreads))
     elif args.kernel == "denoise":
         line.update(denoise_bench(args, ctx, stream, clocks, nthreads))
+    elif args.kernel == "average":
+        # LoadAndAverageIntensity on the device: 512 frames of the 1024x512 detector (1.07 GB, > L2),
+        # photon discretisation, mask
+        ny, nx, nf = 1024, 512, 512
+        rng = np.random.default_rng(5)
+        frames = torch.from_numpy(rng.gamma(0.3, 1.0, (nf, ny * nx)).astype(np.float32)).cuda()
+        mask = torch.from_numpy((rng.random(ny * nx) > 0.05).astype(np.int32)).cuda()
+        discr = torch.zeros(ny * nx, dtype=torch.int64, device="cuda")
+        mean = torch.zeros(nf, dtype=torch.float32, device="cuda")
+        phs = torch.zeros(nf, dtype=torch.float32, device="cuda")
+        fn = lambda: ctx.average_frames(frames, ny * nx, nf, mask, 0.2, 1.0, None, discr, mean, phs, sp)
+        clocks.start()
+        ms = _time(fn, args.steps, max(3, args.warmup), stream)
+        clk = clocks.stop()
+        # the same batch without discretisation: the per-frame sums are then arbitrary FP32
+        # values summed sequentially in pixel order, a chain of ny*nx dependent adds per frame
+        fsum = torch.zeros(ny * nx, dtype=torch.float32, device="cuda")
+        fn_f = lambda: ctx.average_frames(frames, ny * nx, nf, mask, 0.2, 0.0, fsum, None, mean, None, sp)
+        ms_f = _time(fn_f, args.steps, max(3, args.warmup), stream)
+        nbytes = frames.numel() * 4 + ny * nx * (4 + 16)  # frames read once, mask, counts read + written
+        peak, kind = measured_peaks()
+        line.update(metric="frames/s averaged (LoadAndAverageIntensity, photon discretisation)",
+                    value=nf / (ms * 1e-3), unit="frames/s", ms_per_step=ms, dtype="fp32+i64", clocks=clk,
+                    config={"workload": f"{nf} frames of {ny}x{nx} (1.07 GB), 5% masked, threshold 0.2, "
+                                        "step 1.0"},
+                    roofline={"bound": "hbm", "achieved": nbytes / (ms * 1e-3) / 1e9, "peak": peak,
+                              "unit": "GB/s", "frac": nbytes / (ms * 1e-3) / 1e9 / peak,
+                              "peak_source": f"{kind} hbm_gbs",
+                              "note": "one pass over the frames: per-pixel photon counts and the exact "
+                                      "integer per-frame photon totals in the same kernel"},
+                    float_mode={"ms_per_step": ms_f, "frames_per_s": nf / (ms_f * 1e-3),
+                                "bound": "sequential FP32 sum per frame: a chain of "
+                                         f"{ny * nx} dependent adds (4 cycles each)"})
+        if not args.no_cpu_baseline:
+            import oracle
+            sub = 16
+            fh = frames[:sub].cpu().numpy()
+            mh = mask.cpu().numpy()
+            so = np.zeros(ny * nx, np.float32)
+            do = np.zeros(ny * nx, np.int64)
+            mo = np.zeros(sub, np.float32)
+            po = np.zeros(sub, np.float32)
+            t0 = time.perf_counter()
+            oracle.lib().iaco_average_frames(oracle.p(fh), ny * nx, sub, oracle.p(mh), 0.2, 1.0, oracle.p(so),
+                                             oracle.p(do), oracle.p(mo), oracle.p(po))
+            dt = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": sub / dt, "unit": "frames/s", "cores": 1, "kind": "port",
+                                    "sample": f"{sub} of the {nf} frames"}
     print(json.dumps(line), flush=True)
     ctx.close()
     return 0
