@@ -154,6 +154,12 @@ class ClockSampler:
 
     def stop(self):
         if self.nvml is not None:
+            n = self.nvml
+            try:  # one more sample at the end of the timed region
+                self.samples.append((n.nvmlDeviceGetClockInfo(self.handle, n.NVML_CLOCK_SM),
+                                     n.nvmlDeviceGetCurrentClocksEventReasons(self.handle)))
+            except Exception:
+                pass
             self._stop.set()
             self._t.join(timeout=2)
             sm = [c for c, _ in self.samples]
@@ -426,7 +432,7 @@ def run_ours(args):
     for _ in range(max(1, args.warmup // 2)):
         ctx.sparse_ac_frames_host(ph_p, off_p, rot_p, nframes, params, mesh_p)
     e2e_times = []
-    for _ in range(max(2, args.steps // 2)):
+    for _ in range(max(5, args.steps)):
         mesh_p.zero_()
         t0 = time.perf_counter()
         ctx.sparse_ac_frames_host(ph_p, off_p, rot_p, nframes, params, mesh_p)

@@ -185,4 +185,28 @@ __device__ __forceinline__ int round_away_i(float x)
     return x < 0.0f ? -r : r;
 }
 
+
+// ---------------------------------------------------------------------------
+// round half away from zero with two FP32 adds and an integer subtract, for
+// the photon-pair kernel.  y = fl(|x| + 0.49999997) reaches the next integer
+// exactly when |x| is at or past the half (exhaustive check over all floats
+// below 2^23: tests/test_rounding.py), and __fadd_rz(y, 2^23) = 2^23 + floor(y)
+// for 0 <= y < 2^23, so its bits minus those of 2^23 are round(|x|).
+// ---------------------------------------------------------------------------
+constexpr int TWO23_BITS = 0x4B000000;  // bits of 2^23
+
+// exact for |x| < 2^23; larger, infinite or NaN x give |result| >= 2^23,
+// outside every mesh
+__device__ __forceinline__ int round_away_rz_i(float x)
+{
+    const int r = __float_as_int(__fadd_rz(fadd(fabsf(x), 0.49999997f), 8388608.0f)) - TWO23_BITS;
+    return x < 0.0f ? -r : r;
+}
+
+// as a float; exact for |x| < 2^23 (callers bound x), NaN stays NaN
+__device__ __forceinline__ float round_away_rz_f(float x)
+{
+    return copysignf(fsub(__fadd_rz(fadd(fabsf(x), 0.49999997f), 8388608.0f), 8388608.0f), x);
+}
+
 }  // namespace iac

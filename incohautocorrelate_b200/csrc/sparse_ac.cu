@@ -207,9 +207,9 @@ __device__ __forceinline__ void add_positive_ss(const SparseArgs &a, int fs, int
 __device__ __forceinline__ void add_nearest(const SparseArgs &a, float q0, float q1, float q2,
                                             unsigned long long v)
 {
-    int fs = a.C + round_away_i(q0);
-    int ms = a.C + round_away_i(q1);
-    int ss = round_away_i(q2);
+    int fs = a.C + round_away_rz_i(q0);
+    int ms = a.C + round_away_rz_i(q1);
+    int ss = round_away_rz_i(q2);
     if (ss < 0) {
         fs = 2 * a.C - fs;
         ms = 2 * a.C - ms;
@@ -272,9 +272,10 @@ __device__ __forceinline__ void bin_pair(const SparseArgs &a, const float4 A, co
             v = d2u64(dmul(dmul((double)A.w, (double)B.w), a.mult));
         float t0 = q0, t1 = q1, t2 = q2;
         if (DMAP) {  // first-level nearest neighbour: back to the voxel centre
-            t0 = round_away_f(q0);
-            t1 = round_away_f(q1);
-            t2 = round_away_f(q2);
+            // |q| <= MaxQ * Voxel_per_dq < 2^22 here (MaxQ test, host check)
+            t0 = round_away_rz_f(q0);
+            t1 = round_away_rz_f(q1);
+            t2 = round_away_rz_f(q2);
         }
         add_nearest(a, rot_row(t0, t1, t2, R[0], R[1], R[2]), rot_row(t0, t1, t2, R[3], R[4], R[5]),
                     rot_row(t0, t1, t2, R[6], R[7], R[8]), v);
@@ -283,7 +284,7 @@ __device__ __forceinline__ void bin_pair(const SparseArgs &a, const float4 A, co
     const double val = dmul((double)A.w, (double)B.w);
     if (DMAP) {
         if (I1 == 0) {
-            const float r0 = round_away_f(q0), r1 = round_away_f(q1), r2 = round_away_f(q2);
+            const float r0 = round_away_rz_f(q0), r1 = round_away_rz_f(q1), r2 = round_away_rz_f(q2);
             add_rotated<I2>(a, val, rot_row(r0, r1, r2, R[0], R[1], R[2]),
                             rot_row(r0, r1, r2, R[3], R[4], R[5]),
                             rot_row(r0, r1, r2, R[6], R[7], R[8]));
@@ -593,6 +594,8 @@ static iac_status check_params(const iac_sparse_params *p)
                 "sparse pair mesh must be cubic with an odd edge (got %u x %u)", s.size_ab, s.size_c);
     IAC_REQUIRE(s.size_ab <= 1621, "mesh edge %u too large (at most 1621)", s.size_ab);
     IAC_REQUIRE(s.voxel_per_dq > 0, "Voxel_per_dq is 0");
+    IAC_REQUIRE((double)s.max_q * s.voxel_per_dq <= 4194304.0,
+                "MaxQ * Voxel_per_dq must be at most 2^22 voxels (got %g)", (double)s.max_q * s.voxel_per_dq);
     IAC_REQUIRE(p->interp_first == 0 || p->interp_first == 1, "interp_first must be 0 or 1");
     IAC_REQUIRE(p->interp_second == 0 || p->interp_second == 1, "interp_second must be 0 or 1");
     IAC_REQUIRE(p->multiplicator > 0, "multiplicator must be positive");
@@ -781,14 +784,17 @@ iac_status iac_sparse_ac_frames_host(iac_ctx *ctx, const float *h_photons,
     const uint32_t S = p->shape.size_ab;
     const size_t half_b = sizeof(uint64_t) * iac_half_mesh_words(S);
     const size_t full_b = sizeof(uint64_t) * iac_full_mesh_words(S);
-    // Pipelining: the frames are cut into chunks of about equal photon count;
-    // chunk k+1 is copied on the copy stream while chunk k is binned.  Every
-    // chunk has its own rebased offsets so it is an independent batch.
+    // Pipelining: the frames are cut into chunks by photon count; chunk k+1 is
+    // copied on the copy stream while chunk k is binned.  Binning is slower
+    // than the copy, so only the first chunk's copy is exposed: it is made a
+    // quarter of the others (1/29 of the photons for 8 chunks).  Every chunk
+    // has its own rebased offsets so it is an independent batch.
     const uint32_t nchunks = std::max<uint32_t>(1, std::min<uint32_t>(IAC_COPY_CHUNKS, nframes / 64));
     std::vector<uint32_t> cut(nchunks + 1, 0);
     cut[nchunks] = nframes;
+    const uint64_t parts = 4 * (uint64_t)nchunks - 3;  // chunk 0: 1 part, the others 4
     for (uint32_t k = 1; k < nchunks; k++) {
-        const uint64_t target = o0 + nph * k / nchunks;
+        const uint64_t target = o0 + nph * (4 * (uint64_t)k - 3) / parts;
         cut[k] = (uint32_t)(std::lower_bound(h_off, h_off + nframes + 1, target) - h_off);
         cut[k] = std::max(cut[k], cut[k - 1]);
     }
