@@ -811,6 +811,14 @@ def denoise_bench(args, ctx, stream, clocks, nthreads):
                                                     edge, y, sp), 10, 3, stream)
             row[name + "_ms"] = ms
             row[name + "_tflops"] = 2.0 * 27 * ci * co * nvox / (ms * 1e-3) / 1e12
+        # the weight gradient of the same shape: tcgen05 (slabs 2) and mma.sync slabs (1)
+        gq = torch.randn((nvox, co), device="cuda").to(torch.bfloat16).view(torch.int16)
+        dw = torch.zeros((co, 27, ci), dtype=torch.float32, device="cuda")
+        for sl, name in ((2, "wgrad_tcgen05"), (1, "wgrad_mma_sync")):
+            ms = _time(lambda: capi.denoise_wgrad3x3(ctx, None, 0, 0, s1, ci, gq, co, B, edge, edge, edge, dw,
+                                                     None, sp, slabs=sl), 10, 3, stream)
+            row[name + "_ms"] = ms
+            row[name + "_tflops"] = 2.0 * 27 * ci * co * nvox / (ms * 1e-3) / 1e12
         layers.append(row)
     clk = clocks.stop()
     peak, peak_src = measured_bf16_tflops()

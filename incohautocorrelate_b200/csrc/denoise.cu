@@ -180,11 +180,11 @@ iac_status wgrad(iac_denoiser *dn, int l, const bf16 *src0, const bf16 *src1, co
     a.W = W;
     a.V = V;
     a.cout = SPECS[l].cout;
-    // tcgen05 where it measured faster (48 input or 64 output channels),
-    // mma.sync on slabs elsewhere
+    // tcgen05 where it measured faster (32 or more input channels: an M = 64
+    // MMA holds at most 16 useful rows for 16), mma.sync on slabs elsewhere
     if (dn->backend == BACKEND_TC_TAP)
         a.slabs = 0;
-    else if (dn->backend == BACKEND_TC_SLAB && (cin == 48 || SPECS[l].cout == 64))
+    else if (dn->backend == BACKEND_TC_SLAB && cin >= 32)
         a.slabs = 2;
     else
         a.slabs = 1;

@@ -1416,7 +1416,10 @@ static bool launch_wgrad_slab(const WgradArgs &a, int sms, cudaStream_t s, cudaE
 // descriptor offset.  M = 64 rows per MMA (input channels beyond cin read
 // padding and are dropped); the accumulators of every tap of the CTA's group
 // live in TMEM for the whole launch and are read once at the end.  Warp 4
-// loads stages with TMA, warp 5 issues the MMAs, warps 0-3 drain TMEM.
+// loads stages with TMA, warps 5.. issue the MMAs (each a share of the taps:
+// a tcgen05.mma takes its issuing thread ~150 cycles whatever its shape while
+// the tensor pipe accepts one every ~40, so several issuers keep it busy),
+// warps 0-3 drain TMEM.
 struct WTGeom {
     int Wp, NR, NRg, T;
     long long ntiles;
@@ -1426,7 +1429,7 @@ struct WTGeom {
     int S;
 };
 
-constexpr int WT_THREADS = 192;
+constexpr int WT_THREADS = 256;  // warps 0-3 drain, 4 loads, 5-7 issue
 
 template <int CIN, int COUT>
 struct WtcCfg {
@@ -1435,6 +1438,7 @@ struct WtcCfg {
     static constexpr int COLS = G * COUT * MB;
     static constexpr uint32_t TCOLS = COLS <= 32 ? 32 : (COLS <= 64 ? 64 : (COLS <= 128 ? 128 : (COLS <= 256 ? 256 : 512)));
     static constexpr int PAD_PLANES = MB * 8 - CIN / 8;  // planes read past the slab by the padded M rows
+    static constexpr int NI = G >= 3 ? 3 : 1;  // MMA-issuing warps, G / NI taps each
 };
 
 template <int CIN, int COUT>
@@ -1443,13 +1447,13 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_tc_kernel(const __grid_const
                                                               const WgradArgs a, const WTGeom g)
 {
     using Cfg = WtcCfg<CIN, COUT>;
-    constexpr int G = Cfg::G, MB = Cfg::MB;
+    constexpr int G = Cfg::G, MB = Cfg::MB, NI = Cfg::NI;
     constexpr uint32_t IDESC = idesc_bf16(64, COUT) | (1u << 15) | (1u << 16);  // A and B MN-major
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t full[8], empty[8], done;
     __shared__ uint32_t s_tmem;
     __shared__ volatile int s_err;
-    __shared__ long long s_issued, s_consumed;
+    __shared__ long long s_issued, s_consumed[NI];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tap0 = blockIdx.y * G;
     const int dz = tap0 / 9 - 1;
@@ -1458,13 +1462,13 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_tc_kernel(const __grid_const
     if (tid == 0) {
         for (int k = 0; k < g.S; k++) {
             mbar_init(smem_u32(&full[k]), 1);
-            mbar_init(smem_u32(&empty[k]), 1);
+            mbar_init(smem_u32(&empty[k]), NI);  // one commit per issuing warp
         }
-        mbar_init(smem_u32(&done), 1);
+        mbar_init(smem_u32(&done), NI);
         fence_mbar_init();
         s_err = 0;
         s_issued = 0;
-        s_consumed = 0;
+        for (int i = 0; i < NI; i++) s_consumed[i] = 0;
     }
     if (warp == 5) {
         tmem_alloc(smem_u32(&s_tmem), Cfg::TCOLS);
@@ -1499,7 +1503,8 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_tc_kernel(const __grid_const
                 s_issued = k + 1;
             }
         }
-    } else if (warp == 5) {
+    } else if (warp >= 5 && warp < 5 + NI) {
+        const int iw = warp - 5;  // this warp's taps: [iw G / NI, (iw + 1) G / NI)
         if (lane == 0) {
             for (long long k = 0; k < my_tiles; k++) {
                 const int slot = (int)(k % g.S);
@@ -1511,7 +1516,7 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_tc_kernel(const __grid_const
                 const int relg = q0 - (q0 / g.Wp) * g.Wp;
                 const uint32_t sX = sbase + (uint32_t)slot * g.stage_bytes, sG = sX + xbytes;
 #pragma unroll 1
-                for (int t = 0; t < G; t++) {
+                for (int t = iw * (G / NI); t < (iw + 1) * (G / NI); t++) {
                     const int tap = tap0 + t;
                     const int r0 = rel + ((tap / 3) % 3 - 1) * g.Wp + (tap % 3 - 1);
 #pragma unroll
@@ -1527,7 +1532,7 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_tc_kernel(const __grid_const
                     }
                 }
                 umma_commit(smem_u32(&empty[slot]));
-                s_consumed = k + 1;
+                s_consumed[iw] = k + 1;
             }
             if (!s_err && my_tiles > 0) umma_commit(smem_u32(&done));
         }
@@ -1567,10 +1572,12 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_tc_kernel(const __grid_const
     }
     if (s_err && tid == 0) {
         if (a.counters) atomicAdd(&a.counters->timeouts, 1ull);
-        for (long long k = s_consumed; k < s_issued; k++)
+        long long consumed = s_consumed[0];
+        for (int i = 1; i < NI; i++) consumed = s_consumed[i] < consumed ? s_consumed[i] : consumed;
+        for (long long k = consumed; k < s_issued; k++)
             mbar_wait(smem_u32(&full[k % g.S]), (uint32_t)((k / g.S) & 1));
-        if (s_consumed > 0) {
-            const long long k = s_consumed - 1;
+        if (consumed > 0) {
+            const long long k = consumed - 1;
             mbar_wait(smem_u32(&empty[k % g.S]), (uint32_t)((k / g.S) & 1));
         }
     }
