@@ -703,6 +703,10 @@ static bool launch_slab(const ConvArgs &a, cudaStream_t s, cudaError_t &err)
 // lane) produces stages, warp 5 (one lane) issues tcgen05.mma, warps 0-3 drain
 // the double-buffered TMEM accumulator; the roles meet only at mbarriers
 // (full/empty per stage, full/empty per accumulator), every wait bounded.
+// NI = 3: warps 5-7 issue, warp 5 + d the stage of dz = d - 1 of every tile
+// into its own accumulator, and the epilogue adds the three (a tcgen05.mma
+// costs its issuing thread ~150 cycles whatever its shape while the tensor
+// pipe accepts one every ~40, so several issuers keep the pipe busy).
 // Weights stay resident in shared memory when all 27 taps fit, else each
 // stage carries its dz's nine taps (one bulk copy).
 // --------------------------------------------------------------------------
@@ -756,20 +760,26 @@ __device__ __forceinline__ bool mbar_wait_flag(uint32_t addr, uint32_t parity, v
 
 __device__ __forceinline__ int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
-constexpr int TMA_THREADS = 192;
+constexpr int TMA_THREADS = 192;  // with NI issuing warps: 32 * (5 + NI)
 
-template <int CIN, int COUT>
-__global__ void __launch_bounds__(TMA_THREADS) conv_tma_kernel(const __grid_constant__ CUtensorMap xmap,
-                                                               const ConvArgs a, const TmaGeom g)
+__host__ __device__ constexpr uint32_t tma_tcols(int cols)
 {
-    constexpr uint32_t TCOLS = 2 * COUT <= 32 ? 32 : (2 * COUT <= 64 ? 64 : (2 * COUT <= 128 ? 128 : 256));
+    return cols <= 32 ? 32 : (cols <= 64 ? 64 : (cols <= 128 ? 128 : (cols <= 256 ? 256 : 512)));
+}
+
+template <int CIN, int COUT, int NI>
+__global__ void __launch_bounds__(256) conv_tma_kernel(const __grid_constant__ CUtensorMap xmap,
+                                                       const ConvArgs a, const TmaGeom g)
+{
+    static_assert(NI == 1 || NI == 3, "one issuer, or one per dz");
+    constexpr uint32_t TCOLS = tma_tcols(2 * NI * COUT);
     constexpr uint32_t IDESC = idesc_bf16(TILE_M, COUT);
     constexpr uint32_t WT_BYTES = COUT * CIN * 2;
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t full[8], empty[8], accfull[2], accempty[2], wfull;
     __shared__ uint32_t s_tmem;
     __shared__ volatile int s_err;
-    __shared__ long long s_issued, s_consumed;  // stages loaded by the producer / multiplied
+    __shared__ long long s_issued, s_last[NI];  // stages loaded by the producer / last multiplied per issuer
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t sbase = smem_u32(smem);
     const uint32_t wbase = sbase;                   // resident weights
@@ -780,14 +790,14 @@ __global__ void __launch_bounds__(TMA_THREADS) conv_tma_kernel(const __grid_cons
             mbar_init(smem_u32(&empty[k]), 1);
         }
         for (int b = 0; b < 2; b++) {
-            mbar_init(smem_u32(&accfull[b]), 1);
+            mbar_init(smem_u32(&accfull[b]), NI);
             mbar_init(smem_u32(&accempty[b]), 4);
         }
         mbar_init(smem_u32(&wfull), 1);
         fence_mbar_init();
         s_err = 0;
         s_issued = 0;
-        s_consumed = 0;
+        for (int i = 0; i < NI; i++) s_last[i] = -1;
     }
     if (warp == 5) {
         tmem_alloc(smem_u32(&s_tmem), TCOLS);
@@ -828,15 +838,16 @@ __global__ void __launch_bounds__(TMA_THREADS) conv_tma_kernel(const __grid_cons
                 s_issued = i + 1;
             }
         }
-    } else if (warp == 5) {
-        if (lane == 0) {  // MMA issuer
+    } else if (warp >= 5 && warp < 5 + NI) {
+        const int iw = warp - 5;
+        if (lane == 0) {  // MMA issuer: every stage (NI = 1) or the stages of dz = iw - 1
             bool ok = !g.wres_bytes || mbar_wait_flag(smem_u32(&wfull), 0, &s_err);
-            for (long long i = 0; ok && i < nst; i++) {
+            for (long long i = iw; ok && i < nst; i += NI) {
                 const int slot = (int)(i % g.S);
                 if (!mbar_wait_flag(smem_u32(&full[slot]), (uint32_t)((i / g.S) & 1), &s_err)) break;
                 const long long k = i / 3;
                 const int dzi = (int)(i % 3);
-                if (dzi == 0 && k >= 2 &&
+                if ((NI == 3 || dzi == 0) && k >= 2 &&
                     !mbar_wait_flag(smem_u32(&accempty[k & 1]), (uint32_t)(((k >> 1) - 1) & 1), &s_err))
                     break;
                 tc_fence_after();
@@ -845,7 +856,7 @@ __global__ void __launch_bounds__(TMA_THREADS) conv_tma_kernel(const __grid_cons
                 const int rel = q0 - floor_div(q0 - g.Wp - 1, g.Wp) * g.Wp;  // q0 within the slab
                 const uint32_t st = stbase + (uint32_t)slot * g.stage_bytes;
                 const uint32_t wt = g.wres_bytes ? wbase + (uint32_t)(9 * dzi) * WT_BYTES : st + g.slab_bytes;
-                const uint32_t dcol = tmem + (uint32_t)((k & 1) * COUT);
+                const uint32_t dcol = tmem + (uint32_t)(((k & 1) * NI + (NI == 3 ? dzi : 0)) * COUT);
 #pragma unroll 1
                 for (int t = 0; t < 9; t++) {
                     const uint32_t r0 = (uint32_t)(rel + (t / 3 - 1) * g.Wp + (t % 3 - 1));
@@ -853,12 +864,12 @@ __global__ void __launch_bounds__(TMA_THREADS) conv_tma_kernel(const __grid_cons
                     for (int kk = 0; kk < CIN / 16; kk++) {
                         const uint64_t da = smem_desc(st + (uint32_t)(2 * kk) * g.plane_bytes + r0 * 16, g.plane_bytes, 128);
                         const uint64_t db = smem_desc(wt + t * WT_BYTES + kk * 2 * (COUT * 16), COUT * 16, 128);
-                        umma_bf16(dcol, da, db, IDESC, (dzi > 0 || t > 0 || kk > 0) ? 1u : 0u);
+                        umma_bf16(dcol, da, db, IDESC, ((NI == 1 && dzi > 0) || t > 0 || kk > 0) ? 1u : 0u);
                     }
                 }
                 umma_commit(smem_u32(&empty[slot]));
-                if (dzi == 2) umma_commit(smem_u32(&accfull[k & 1]));
-                s_consumed = i + 1;
+                if (NI == 3 || dzi == 2) umma_commit(smem_u32(&accfull[k & 1]));
+                s_last[iw] = i;
             }
         }
     } else {  // epilogue: warps 0-3 own TMEM lanes 32w .. 32w+31
@@ -872,10 +883,21 @@ __global__ void __launch_bounds__(TMA_THREADS) conv_tma_kernel(const __grid_cons
             const bool valid = y < a.H && xp >= 1 && xp <= a.W;
             const long long v = plane * HW + (long long)y * a.W + (xp - 1);
             uint32_t r[COUT];
+            const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((k & 1) * NI * COUT);
 #pragma unroll
             for (int c = 0; c < COUT; c += 16) {
                 uint32_t (&rr)[16] = *reinterpret_cast<uint32_t(*)[16]>(&r[c]);
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((k & 1) * COUT + c), rr);
+                tmem_ld16(lane_base + (uint32_t)c, rr);
+                if constexpr (NI == 3) {  // (dz -1) + (dz 0), then + (dz +1)
+                    uint32_t r1[16], r2[16];
+                    tmem_ld16(lane_base + (uint32_t)(COUT + c), r1);
+                    tmem_ld16(lane_base + (uint32_t)(2 * COUT + c), r2);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int j = 0; j < 16; j++)
+                        rr[j] = __float_as_uint(__fadd_rn(__fadd_rn(__uint_as_float(rr[j]), __uint_as_float(r1[j])),
+                                                          __uint_as_float(r2[j])));
+                }
             }
             tmem_wait_ld();
             tc_fence_before();
@@ -898,11 +920,13 @@ __global__ void __launch_bounds__(TMA_THREADS) conv_tma_kernel(const __grid_cons
         // before the shared memory and TMEM are released
         if (tid == 0) {
             if (a.counters) atomicAdd(&a.counters->timeouts, 1ull);
-            for (long long i = s_consumed; i < s_issued; i++)
+            // every copy still in flight: the stages of the last S loads
+            for (long long i = s_issued > g.S ? s_issued - g.S : 0; i < s_issued; i++)
                 mbar_wait(smem_u32(&full[i % g.S]), (uint32_t)((i / g.S) & 1));
-            if (s_consumed > 0) {
-                const long long i = s_consumed - 1;
-                mbar_wait(smem_u32(&empty[i % g.S]), (uint32_t)((i / g.S) & 1));
+            // every issuer's MMAs: its last commit covers all of them
+            for (int w = 0; w < NI; w++) {
+                const long long i = s_last[w];
+                if (i >= 0) mbar_wait(smem_u32(&empty[i % g.S]), (uint32_t)((i / g.S) & 1));
             }
         }
         __syncthreads();
@@ -978,20 +1002,32 @@ static bool launch_tma(const ConvArgs &a, cudaStream_t s, cudaError_t &err)
         g.wstage_bytes = 9u * COUT * CIN * 2;
         g.stage_bytes = (g.slab_bytes + g.wstage_bytes + 1023u) & ~1023u;
     }
-    // several CTAs per SM: each tile's MMAs chain on one accumulator, so
-    // independent CTAs keep the tensor pipe busy; 4 stages each when they fit
-    constexpr int TCOLS = 2 * COUT <= 32 ? 32 : (2 * COUT <= 64 ? 64 : (2 * COUT <= 128 ? 128 : 256));
-    int per_sm = 1;
-    g.S = 0;
-    for (int want = std::min(4, 512 / TCOLS); want >= 1; want--) {
-        const uint32_t share = (228u * 1024u) / (uint32_t)want - 2048u;
-        const int S = (int)std::min<uint32_t>(want == 1 ? 8u : 4u, (std::min(share, budget) - g.wres_bytes) / g.stage_bytes);
-        if (g.wres_bytes < share && S >= 2) {
-            per_sm = want;
-            g.S = S;
-            break;
+    // several CTAs per SM and, where TMEM and shared memory allow, three
+    // issuing warps per CTA: the count of MMA issuers per SM sets the MMA
+    // rate; 4 stages per CTA when they fit
+    auto fit = [&](int ni, int &per_sm, int &S) {
+        per_sm = 0;
+        S = 0;
+        for (int want = std::min(4, (int)(512 / tma_tcols(2 * ni * COUT))); want >= 1; want--) {
+            const uint32_t share = (228u * 1024u) / (uint32_t)want - 2048u;
+            int st = (int)std::min<uint32_t>(want == 1 ? 8u : 4u,
+                                             (std::min(share, budget) - g.wres_bytes) / g.stage_bytes);
+            // three issuers: a multiple of 3 stages, so every slot always
+            // serves the same issuer and its parity waits stay in phase order
+            if (ni == 3) st = st >= 3 ? (st >= 6 ? 6 : 3) : 0;
+            if (g.wres_bytes < share && st >= 2) {
+                per_sm = want;
+                S = st;
+                return;
+            }
         }
-    }
+    };
+    int per_sm = 0, per_sm3 = 0, S1 = 0, S3 = 0;
+    fit(1, per_sm, S1);
+    if (2 * 3 * COUT <= 512) fit(3, per_sm3, S3);
+    const int ni = (S3 >= 2 && per_sm3 >= per_sm) ? 3 : 1;  // more issuers, no fewer CTAs (measured)
+    if (ni == 3) per_sm = per_sm3;
+    g.S = ni == 3 ? S3 : S1;
     if (g.S < 2 || g.ntiles == 0) return false;
     const uint32_t smem = g.wres_bytes + (uint32_t)g.S * g.stage_bytes;
 
@@ -1005,10 +1041,19 @@ static bool launch_tma(const ConvArgs &a, cudaStream_t s, cudaError_t &err)
                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return false;
-    err = smem_attributes(conv_tma_kernel<CIN, COUT>, smem);
-    if (err != cudaSuccess) return true;
     const long long grid = std::min<long long>(g.ntiles, (long long)per_sm * std::max(1, a.sms));
-    conv_tma_kernel<CIN, COUT><<<(unsigned)grid, TMA_THREADS, smem, s>>>(map, a, g);
+    if constexpr (2 * 3 * COUT <= 512) {
+        if (ni == 3) {
+            err = smem_attributes(conv_tma_kernel<CIN, COUT, 3>, smem);
+            if (err != cudaSuccess) return true;
+            conv_tma_kernel<CIN, COUT, 3><<<(unsigned)grid, 32 * (5 + 3), smem, s>>>(map, a, g);
+            err = cudaGetLastError();
+            return true;
+        }
+    }
+    err = smem_attributes(conv_tma_kernel<CIN, COUT, 1>, smem);
+    if (err != cudaSuccess) return true;
+    conv_tma_kernel<CIN, COUT, 1><<<(unsigned)grid, TMA_THREADS, smem, s>>>(map, a, g);
     err = cudaGetLastError();
     return true;
 }
