@@ -722,6 +722,8 @@ struct TmaGeom {
     uint32_t wres_bytes;    // shared memory reserved for resident weights (0: per stage)
     uint32_t wcopy_bytes;   // bytes of the resident weights copied
     int S;
+    int ZC;                 // z-column kernel: output planes per work item
+    long long nitems;       // z-column kernel: nb * T * ceil(D / ZC) work items
 };
 
 __device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
@@ -937,6 +939,216 @@ __global__ void __launch_bounds__(256) conv_tma_kernel(const __grid_constant__ C
     }
 }
 
+// --------------------------------------------------------------------------
+// z-column variant of conv_tma_kernel.  conv_tma_kernel stages the three
+// input-plane slabs (dz = -1, 0, +1) of every output tile, so each input row
+// crosses L2 -> shared memory about 8 times (3 planes x halo rows) and the
+// kernel is bound by that traffic.  Here a work item is one tile position
+// (n, q0) over ZC consecutive output planes z0 .. z0+ZC-1: the producer loads
+// the slab of each input plane z0-1 .. z0+ZC once, and every slab feeds three
+// outputs (planes p+1, p, p-1 as dz = -1, 0, +1).  Warps 5, 6, 7 issue the
+// taps of dz = -1, 0, +1 (warp 5 + i uses the stage of plane z - 1 + i for
+// output z) into their own accumulators; the epilogue adds the three.  Every
+// issuer walks every stage in order (committing the stages it does not use),
+// so a slot's parity waits stay in phase order; an issuer at stage k works on
+// output k - i, so outputs k-2 .. k are in flight together and the
+// accumulators rotate over NB buffers (3 per buffer, 3 * NB * COUT columns).
+// Weights are resident (all 27 taps in shared memory).
+// --------------------------------------------------------------------------
+template <int CIN, int COUT, int NB>
+__global__ void __launch_bounds__(256, 1) conv_zcol_kernel(const __grid_constant__ CUtensorMap xmap,
+                                                        const ConvArgs a, const TmaGeom g)
+{
+    constexpr uint32_t TCOLS = tma_tcols(3 * NB * COUT);
+    static_assert(3 * NB * COUT <= 512, "TMEM holds 512 columns");
+    constexpr uint32_t IDESC = idesc_bf16(TILE_M, COUT);
+    constexpr uint32_t WT_BYTES = COUT * CIN * 2;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t full[8], empty[8], accfull[NB], accempty[NB], wfull;
+    __shared__ uint32_t s_tmem;
+    __shared__ volatile int s_err;
+    __shared__ long long s_issued, s_last[3];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t sbase = smem_u32(smem);
+    const uint32_t wbase = sbase;                   // resident weights
+    const uint32_t stbase = sbase + g.wres_bytes;   // stages: one input-plane slab each
+    if (tid == 0) {
+        for (int k = 0; k < g.S; k++) {
+            mbar_init(smem_u32(&full[k]), 1);
+            mbar_init(smem_u32(&empty[k]), 3);  // every issuer commits every stage
+        }
+        for (int b = 0; b < NB; b++) {
+            mbar_init(smem_u32(&accfull[b]), 3);
+            mbar_init(smem_u32(&accempty[b]), 4);
+        }
+        mbar_init(smem_u32(&wfull), 1);
+        fence_mbar_init();
+        s_err = 0;
+        s_issued = 0;
+        for (int i = 0; i < 3; i++) s_last[i] = -1;
+    }
+    if (warp == 5) {
+        tmem_alloc(smem_u32(&s_tmem), TCOLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const int nzc = (a.D + g.ZC - 1) / g.ZC;  // z-chunks per column
+    const int HW = a.H * a.W;
+    // work item it -> batch item n, tile q0 of the plane, output planes z0 .. z1-1
+    auto item = [&](long long it, int &n, int &q0, int &z0, int &z1) {
+        const long long col = it / nzc;
+        z0 = (int)(it % nzc) * g.ZC;
+        z1 = z0 + g.ZC < a.D ? z0 + g.ZC : a.D;
+        n = (int)(col / g.T);
+        q0 = (int)(col % g.T) * TILE_M;
+    };
+
+    if (warp == 4) {
+        if (lane == 0) {  // producer: one slab per input plane z0-1 .. z1 (planes outside the volume arrive as zeros)
+            mbar_expect_tx(smem_u32(&wfull), g.wcopy_bytes);
+            bulk_load(wbase, a.w, g.wcopy_bytes, smem_u32(&wfull));
+            long long j = 0;
+            bool ok = true;
+            for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
+                int n, q0, z0, z1;
+                item(it, n, q0, z0, z1);
+                const int y_lo = floor_div(q0 - g.Wp - 1, g.Wp);
+                for (int pz = z0 - 1; pz <= z1; pz++, j++) {
+                    const int slot = (int)(j % g.S);
+                    if (j >= g.S && !mbar_wait_flag(smem_u32(&empty[slot]), (uint32_t)(((j / g.S) - 1) & 1), &s_err)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t st = stbase + (uint32_t)slot * g.stage_bytes;
+                    const uint32_t fb = smem_u32(&full[slot]);
+                    mbar_expect_tx(fb, (CIN / 8) * g.box_bytes);
+#pragma unroll
+                    for (int c = 0; c < CIN / 8; c++)
+                        tma_load_5d(st + c * g.plane_bytes, &xmap, c * 8, -1, y_lo, pz, n, fb);
+                    s_issued = j + 1;
+                }
+            }
+        }
+    } else if (warp >= 5) {
+        const int iw = warp - 5;  // taps of dz = iw - 1
+        if (lane == 0) {
+            bool ok = mbar_wait_flag(smem_u32(&wfull), 0, &s_err);
+            long long j = 0, o = 0;  // stages and outputs of this CTA so far
+            for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
+                int n, q0, z0, z1;
+                item(it, n, q0, z0, z1);
+                const int nz = z1 - z0;
+                const int rel = q0 - floor_div(q0 - g.Wp - 1, g.Wp) * g.Wp;  // q0 within the slab
+                for (int k = 0; k < nz + 2; k++, j++) {
+                    const int slot = (int)(j % g.S);
+                    if (!mbar_wait_flag(smem_u32(&full[slot]), (uint32_t)((j / g.S) & 1), &s_err)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const int ol = k - iw;  // the output this plane feeds as dz = iw - 1
+                    if (ol >= 0 && ol < nz) {
+                        const long long og = o + ol;
+                        const int b = (int)(og % NB);
+                        if (og >= NB &&
+                            !mbar_wait_flag(smem_u32(&accempty[b]), (uint32_t)(((og / NB) - 1) & 1), &s_err)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t st = stbase + (uint32_t)slot * g.stage_bytes;
+                        const uint32_t wt = wbase + (uint32_t)(9 * iw) * WT_BYTES;
+                        const uint32_t dcol = tmem + (uint32_t)((b * 3 + iw) * COUT);
+#pragma unroll 1
+                        for (int t = 0; t < 9; t++) {
+                            const uint32_t r0 = (uint32_t)(rel + (t / 3 - 1) * g.Wp + (t % 3 - 1));
+#pragma unroll
+                            for (int kk = 0; kk < CIN / 16; kk++) {
+                                const uint64_t da =
+                                    smem_desc(st + (uint32_t)(2 * kk) * g.plane_bytes + r0 * 16, g.plane_bytes, 128);
+                                const uint64_t db = smem_desc(wt + t * WT_BYTES + kk * 2 * (COUT * 16), COUT * 16, 128);
+                                umma_bf16(dcol, da, db, IDESC, (t > 0 || kk > 0) ? 1u : 0u);
+                            }
+                        }
+                        umma_commit(smem_u32(&accfull[b]));
+                    }
+                    umma_commit(smem_u32(&empty[slot]));
+                    s_last[iw] = j;
+                }
+                o += nz;
+            }
+        }
+    } else {  // epilogue: warps 0-3 own TMEM lanes 32w .. 32w+31
+        long long o = 0;
+        bool ok = true;
+        for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
+            int n, q0, z0, z1;
+            item(it, n, q0, z0, z1);
+            const int q = q0 + tid;
+            const int y = q / g.Wp, xp = q - (q / g.Wp) * g.Wp;
+            const bool valid = y < a.H && xp >= 1 && xp <= a.W;
+            for (int z = z0; z < z1; z++, o++) {
+                const int b = (int)(o % NB);
+                if (!mbar_wait_flag(smem_u32(&accfull[b]), (uint32_t)((o / NB) & 1), &s_err)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                uint32_t r[COUT];
+                const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(b * 3 * COUT);
+#pragma unroll
+                for (int c = 0; c < COUT; c += 16) {
+                    uint32_t (&rr)[16] = *reinterpret_cast<uint32_t(*)[16]>(&r[c]);
+                    uint32_t r1[16], r2[16];
+                    tmem_ld16(lane_base + (uint32_t)c, rr);
+                    tmem_ld16(lane_base + (uint32_t)(COUT + c), r1);
+                    tmem_ld16(lane_base + (uint32_t)(2 * COUT + c), r2);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int jj = 0; jj < 16; jj++)  // (dz -1) + (dz 0), then + (dz +1)
+                        rr[jj] = __float_as_uint(__fadd_rn(__fadd_rn(__uint_as_float(rr[jj]), __uint_as_float(r1[jj])),
+                                                           __uint_as_float(r2[jj])));
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(smem_u32(&accempty[b]));
+                if (valid) {
+                    const long long v = ((long long)n * a.D + z) * HW + (long long)y * a.W + (xp - 1);
+#pragma unroll
+                    for (int c = 0; c < COUT; c += 8) {
+                        float f[8];
+#pragma unroll
+                        for (int jj = 0; jj < 8; jj++) f[jj] = __uint_as_float(r[c + jj]);
+                        store8(a, COUT, v, c, f);
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (s_err) {
+        // after an error: let the copies and MMAs already issued finish (bounded)
+        // before the shared memory and TMEM are released
+        if (tid == 0) {
+            if (a.counters) atomicAdd(&a.counters->timeouts, 1ull);
+            for (long long i = s_issued > g.S ? s_issued - g.S : 0; i < s_issued; i++)
+                mbar_wait(smem_u32(&full[i % g.S]), (uint32_t)((i / g.S) & 1));
+            for (int w = 0; w < 3; w++) {
+                const long long i = s_last[w];
+                if (i >= 0) mbar_wait(smem_u32(&empty[i % g.S]), (uint32_t)((i / g.S) & 1));
+            }
+        }
+        __syncthreads();
+    }
+    if (warp == 5) {
+        tc_fence_after();
+        tmem_dealloc(tmem, TCOLS);
+    }
+}
+
 // shared-memory attributes of a kernel, set once per process (the largest
 // size asked for so far); the attribute calls are host work on every launch
 // otherwise
@@ -971,6 +1183,61 @@ static PFN_cuTensorMapEncodeTiled tensor_map_encoder()
             fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(p);
     });
     return fn;
+}
+
+// accumulator buffers of the z-column kernel: 3 per buffer, NB >= 3 buffers
+// (outputs k-2 .. k are in flight at stage k), within 512 TMEM columns
+template <int COUT>
+struct ZcolNB {
+    static constexpr int value = 12 * COUT <= 512 ? 4 : (9 * COUT <= 512 ? 3 : 0);
+};
+
+// the z-column convolution when its weights stay resident and 4+ stages fit;
+// false leaves the layer to conv_tma_kernel
+template <int CIN, int COUT>
+static bool launch_zcol(const ConvArgs &a, const TmaGeom &g0, const CUtensorMap &map, uint32_t budget,
+                        cudaStream_t s, cudaError_t &err)
+{
+    constexpr int NB = ZcolNB<COUT>::value;
+    if constexpr (NB == 0) {
+        return false;
+    } else {
+        const uint32_t w27 = 27u * COUT * CIN * 2;
+        if (w27 > 64u * 1024u) return false;
+        TmaGeom g = g0;
+        g.wcopy_bytes = w27;
+        g.wres_bytes = (w27 + 1023u) & ~1023u;
+        g.wstage_bytes = 0;
+        g.stage_bytes = (g.slab_bytes + 1023u) & ~1023u;
+        const int tmem_per_sm = (int)(512 / tma_tcols(3 * NB * COUT));
+        int per_sm = 0, S = 0;
+        for (int want = std::min(4, tmem_per_sm); want >= 1; want--) {
+            const uint32_t share = std::min(budget, (228u * 1024u) / (uint32_t)want - 2048u);
+            if (share <= g.wres_bytes) continue;
+            const int st = (int)std::min<uint32_t>(8u, (share - g.wres_bytes) / g.stage_bytes);
+            if (st >= 4) {
+                per_sm = want;
+                S = st;
+                break;
+            }
+        }
+        if (per_sm == 0) return false;
+        g.S = S;
+        const long long nb = a.V / ((long long)a.D * a.H * a.W);
+        const long long grid_max = (long long)per_sm * std::max(1, a.sms);
+        // output planes per work item: the whole depth unless that leaves SMs idle
+        int ZC = a.D;
+        while (ZC > 4 && nb * g.T * ((a.D + ZC - 1) / ZC) < 2 * grid_max) ZC = (ZC + 1) / 2;
+        g.ZC = ZC;
+        g.nitems = nb * g.T * ((a.D + ZC - 1) / ZC);
+        const uint32_t smem = g.wres_bytes + (uint32_t)S * g.stage_bytes;
+        err = smem_attributes(conv_zcol_kernel<CIN, COUT, NB>, smem);
+        if (err != cudaSuccess) return true;
+        const long long grid = std::min<long long>(g.nitems, grid_max);
+        conv_zcol_kernel<CIN, COUT, NB><<<(unsigned)grid, 256, smem, s>>>(map, a, g);
+        err = cudaGetLastError();
+        return true;
+    }
 }
 
 template <int CIN, int COUT>
@@ -1041,6 +1308,7 @@ static bool launch_tma(const ConvArgs &a, cudaStream_t s, cudaError_t &err)
                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return false;
+    if (launch_zcol<CIN, COUT>(a, g, map, budget, s, err)) return true;
     const long long grid = std::min<long long>(g.ntiles, (long long)per_sm * std::max(1, a.sms));
     if constexpr (2 * 3 * COUT <= 512) {
         if (ni == 3) {
