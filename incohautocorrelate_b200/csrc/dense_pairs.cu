@@ -306,7 +306,7 @@ __device__ __forceinline__ unsigned long long scaled_floor_normal(float p, uint3
     const uint32_t b = __float_as_uint(p);
     const unsigned long long prod = (unsigned long long)((b & 0x7fffffu) | 0x800000u) * M;
     const int sh = (int)(b >> 23) - 150;  // p = mantissa * 2^sh
-    return sh >= 0 ? (prod << sh) : (prod >> min(-sh, 63));
+    return sh >= 0 ? (prod << min(sh, 63)) : (prod >> min(-sh, 63));
 }
 
 // nearest-voxel pairs with a compile-time axis mapping: the voxel is compared
@@ -348,6 +348,62 @@ __device__ __forceinline__ void cq_pairs_nn(const DenseArgs &a, const Window &w,
     if (cur != NONE) put(a, w, win, cf + a.cab, cm + a.cab, cs + a.cc, acc);
 }
 
+// shared-memory 64-bit add, issued only where p holds (no branch)
+__device__ __forceinline__ void red_shared_u64_if(bool p, uint32_t addr, unsigned long long v)
+{
+    asm volatile(
+        "{\n\t.reg .pred q;\n\t"
+        "setp.ne.b32 q, %0, 0;\n\t"
+        "@q red.shared.add.u64 [%1], %2;\n\t}\n" ::"r"((int)p),
+        "r"(addr), "l"(v)
+        : "memory");
+}
+
+// cq_pairs_nn when the window is on: every pair inside MaxQ lands in the
+// window (it spans the two tiles' q range with a voxel of margin), so the run
+// key is the voxel's window index itself and a finished run is one predicated
+// shared-memory add.  Pairs that fail the intensity or MaxQ test are masked
+// rather than skipped, so a warp never diverges on them; the only branch is
+// the guard for an index outside the window (non-finite k-vectors), which
+// takes the global path of put().
+template <int KA, int KB, int KC, bool CHECK, bool MINT>
+__device__ __forceinline__ void cq_pairs_win(const DenseArgs &a, const Window &w, unsigned long long *win,
+                                             const float4 *sq, int j0, float k0, float k1, float k2, float Ia)
+{
+    const int D0 = w.dim[0], D01 = w.dim[0] * w.dim[1];
+    const int words = D01 * w.dim[2];
+    const int base = (a.cab - w.lo[0]) + D0 * (a.cab - w.lo[1]) + D01 * (a.cc - w.lo[2]);
+    const uint32_t wb = (uint32_t)__cvta_generic_to_shared(win);
+    const float vpdq = a.vpdq;
+    int cur = 0;
+    bool on = false;  // a run is pending at window index cur
+    unsigned long long acc = 0;
+#pragma unroll 2
+    for (int j = j0; j < DTILE; j++) {
+        const float4 b = sq[j];
+        const float pv = fmul(Ia, b.w);
+        float qx = fsub(k0, b.x), qy = fsub(k1, b.y), qz = fsub(k2, b.z);
+        bool ok = !(pv < 1e-37f);
+        if (CHECK) ok = ok && !(fadd(fadd(fmul(qx, qx), fmul(qy, qy)), fmul(qz, qz)) > a.maxq2);
+        qx = fmul(qx, vpdq);
+        qy = fmul(qy, vpdq);
+        qz = fmul(qz, vpdq);
+        const int f = round_half_away(axis<KA>(qx, qy, qz, 0));
+        const int m = round_half_away(axis<KB>(qx, qy, qz, 0));
+        const int sz = round_half_away(axis<KC>(qx, qy, qz, 0));
+        const int key = base + f + D0 * m + D01 * sz;
+        const unsigned long long v = MINT ? scaled_floor_normal(pv, a.mult_int) : d2u64(dmul((double)pv, a.mult));
+        const bool brk = ok && (!on || key != cur);  // a new run starts at this pair
+        red_shared_u64_if(brk && on, wb + 8u * (uint32_t)cur, acc);
+        const bool inwin = (unsigned)key < (unsigned)words;
+        if (brk && !inwin) global_put_pair(a, f + a.cab, m + a.cab, sz + a.cc, v);
+        acc = brk ? (inwin ? v : 0ull) : (ok ? acc + v : acc);
+        cur = brk ? key : cur;
+        on = brk ? inwin : on;
+    }
+    red_shared_u64_if(on, wb + 8u * (uint32_t)cur, acc);
+}
+
 // upper bound of |k_a - k_b| over two boxes is below MaxQ with a margin that
 // covers the FP32 rounding of the per-pair test (every pair passes it)
 __device__ __forceinline__ bool boxes_within(const float4 a0, const float4 a1, const float4 b0, const float4 b1,
@@ -357,6 +413,14 @@ __device__ __forceinline__ bool boxes_within(const float4 a0, const float4 a1, c
     const float dy = fmaxf(a1.y - b0.y, b1.y - a0.y);
     const float dz = fmaxf(a1.z - b0.z, b1.z - a0.z);
     return dx * dx + dy * dy + dz * dz < maxq * maxq * 0.9999f;
+}
+
+// index within the 16 x 16 patch of thread t's own pixel: lane l of warp w takes
+// x = 4 (l % 4) + w % 4, y = 2 (l / 4) + w / 4 (a bijection of 0..255)
+__device__ __forceinline__ int own_pixel(int t)
+{
+    const int w = t >> 5, l = t & 31;
+    return (2 * (l >> 2) + (w >> 2)) * 16 + 4 * (l & 3) + (w & 3);
 }
 
 template <int INTERP, int KA, int KB, int KC>
@@ -408,7 +472,12 @@ __global__ void __launch_bounds__(DTILE) cq_small_kernel(const DenseArgs a)
                                          : make_float4(0.f, 0.f, 0.f, 0.f);
         }
         __syncthreads();
-        const uint64_t ia = tile_pixel(a, P, threadIdx.x);
+        // own pixel: spread over the patch (x 4 apart, y 2 apart within a warp) so
+        // that a warp's lanes rarely share a voxel and their window adds for one
+        // staged pixel rarely meet at one address; the staged tile keeps its
+        // order (runs of consecutive pixels land in one voxel)
+        const int own = own_pixel(threadIdx.x);
+        const uint64_t ia = tile_pixel(a, P, own);
         unsigned long long self = 0;
         if (ia < a.npix) {
             const float k0 = a.K[3 * ia], k1 = a.K[3 * ia + 1], k2 = a.K[3 * ia + 2];
@@ -418,8 +487,20 @@ __global__ void __launch_bounds__(DTILE) cq_small_kernel(const DenseArgs a)
                 if (!(sv < 1e-37f))
                     self = a.mult_int ? scaled_floor(sv, a.mult_int) : d2u64(dmul((double)sv, a.mult));
             }
-            const int j0 = (P == Q) ? threadIdx.x + 1 : 0;
-            if (INTERP == 0 && KA >= 0 && a.key_ok) {
+            const int j0 = (P == Q) ? own + 1 : 0;
+            if (INTERP == 0 && KA >= 0 && w.on) {
+                if (a.mult_int) {
+                    if (check)
+                        cq_pairs_win<KA, KB, KC, true, true>(a, w, win, sq, j0, k0, k1, k2, Ia);
+                    else
+                        cq_pairs_win<KA, KB, KC, false, true>(a, w, win, sq, j0, k0, k1, k2, Ia);
+                } else {
+                    if (check)
+                        cq_pairs_win<KA, KB, KC, true, false>(a, w, win, sq, j0, k0, k1, k2, Ia);
+                    else
+                        cq_pairs_win<KA, KB, KC, false, false>(a, w, win, sq, j0, k0, k1, k2, Ia);
+                }
+            } else if (INTERP == 0 && KA >= 0 && a.key_ok) {
                 if (a.mult_int) {
                     if (check)
                         cq_pairs_nn<KA, KB, KC, true, true>(a, w, win, sq, j0, k0, k1, k2, Ia);
