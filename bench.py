@@ -515,9 +515,10 @@ def _fp32_peak_tflops(clock_mhz):
     return 148 * 128 * 2 * clock_mhz * 1e6 / 1e12
 
 
-# thread instructions per unordered pixel pair (ncu smsp__inst_executed.sum x 32 / pairs, 256^2
-# detector; profiles/cq_small_kernel.md, profiles/ac1d_cq_kernel.md)
-INST_PER_PAIR = {"cq_small": 7698927703 * 32 / (65536 * 65537 / 2),
+# thread instructions per unordered pixel pair (ncu smsp__inst_executed.sum x 32 / pairs;
+# cq_small on the 1024^2 configuration itself, ac1d_cq on a 256^2 detector;
+# profiles/cq_small_kernel.md, profiles/ac1d_cq_kernel.md)
+INST_PER_PAIR = {"cq_small": 1582131114734 * 32 / (1048576 * 1048577 / 2),
                  "ac1d_cq": 8217131069 * 32 / (65536 * 65537 / 2)}
 
 
