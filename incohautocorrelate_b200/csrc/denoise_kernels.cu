@@ -1746,11 +1746,14 @@ constexpr int WT_THREADS = 256;  // warps 0-3 drain, 4 loads, 5-7 issue
 
 template <int CIN, int COUT>
 struct WtcCfg {
-    static constexpr int MB = (CIN + 63) / 64;  // M blocks of 64 input channels
+    // rows per MMA: 64, or 128 above 64 input channels (an MMA takes one issue
+    // slot of the tensor pipe whatever its M, so fewer, taller MMAs pay)
+    static constexpr int MR = CIN > 64 ? 128 : 64;
+    static constexpr int MB = (CIN + MR - 1) / MR;  // M blocks of MR input channels
     static constexpr int G = 9 * COUT * MB <= 512 ? 9 : (3 * COUT * MB <= 512 ? 3 : 1);
     static constexpr int COLS = G * COUT * MB;
     static constexpr uint32_t TCOLS = COLS <= 32 ? 32 : (COLS <= 64 ? 64 : (COLS <= 128 ? 128 : (COLS <= 256 ? 256 : 512)));
-    static constexpr int PAD_PLANES = MB * 8 - CIN / 8;  // planes read past the slab by the padded M rows
+    static constexpr int PAD_PLANES = MB * MR / 8 - CIN / 8;  // planes read past the slab by the padded M rows
     static constexpr int NI = G >= 3 ? 3 : 1;  // MMA-issuing warps, G / NI taps each
 };
 
@@ -1761,7 +1764,8 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_tc_kernel(const __grid_const
 {
     using Cfg = WtcCfg<CIN, COUT>;
     constexpr int G = Cfg::G, MB = Cfg::MB, NI = Cfg::NI;
-    constexpr uint32_t IDESC = idesc_bf16(64, COUT) | (1u << 15) | (1u << 16);  // A and B MN-major
+    constexpr int MR = Cfg::MR;
+    constexpr uint32_t IDESC = idesc_bf16(MR, COUT) | (1u << 15) | (1u << 16);  // A and B MN-major
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t full[8], empty[8], done;
     __shared__ uint32_t s_tmem;
@@ -1837,7 +1841,7 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_tc_kernel(const __grid_const
                         const uint32_t dcol = tmem + (uint32_t)((t * MB + mb) * COUT);
 #pragma unroll
                         for (int ks = 0; ks < TILE_M / 16; ks++) {
-                            const uint64_t da = smem_desc(sX + (uint32_t)(mb * 8) * g.planeX + (uint32_t)(r0 + 16 * ks) * 16,
+                            const uint64_t da = smem_desc(sX + (uint32_t)(mb * (MR / 8)) * g.planeX + (uint32_t)(r0 + 16 * ks) * 16,
                                                           128, g.planeX);
                             const uint64_t db = smem_desc(sG + (uint32_t)(relg + 16 * ks) * 16, 128, g.planeG);
                             umma_bf16(dcol, da, db, IDESC, (k > 0 || ks > 0) ? 1u : 0u);
@@ -1861,7 +1865,8 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_tc_kernel(const __grid_const
         tc_fence_after();
         // an M = 64 accumulator keeps row i in TMEM lane 32 (i / 16) + i % 16:
         // lanes 0-15 of each warp's quadrant
-        const int row = lane < 16 ? warp * 16 + lane : -1;
+        // (M = 128: row i in lane i)
+        const int row = MR == 128 ? warp * 32 + lane : (lane < 16 ? warp * 16 + lane : -1);
 #pragma unroll 1
         for (int blk = 0; blk < G * MB; blk++) {
             uint32_t r[COUT];
@@ -1872,7 +1877,7 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_tc_kernel(const __grid_const
             }
             tmem_wait_ld();
             const int t = blk / MB, mb = blk % MB;
-            const int ci = mb * 64 + row;
+            const int ci = mb * MR + row;
             if (row >= 0 && ci < CIN) {
 #pragma unroll
                 for (int co = 0; co < COUT; co++) {
