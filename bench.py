@@ -432,7 +432,7 @@ def run_ours(args):
     for _ in range(max(1, args.warmup // 2)):
         ctx.sparse_ac_frames_host(ph_p, off_p, rot_p, nframes, params, mesh_p)
     e2e_times = []
-    for _ in range(max(5, args.steps)):
+    for _ in range(max(15, args.steps)):
         mesh_p.zero_()
         t0 = time.perf_counter()
         ctx.sparse_ac_frames_host(ph_p, off_p, rot_p, nframes, params, mesh_p)
