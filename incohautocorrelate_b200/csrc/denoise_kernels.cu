@@ -203,6 +203,15 @@ __device__ __forceinline__ Vox decode(long long v, int D, int H, int W, long lon
     Vox q;
     q.ok = v < V;
     if (!q.ok) v = 0;
+    if (V < (1ll << 31)) {  // 32-bit divisions where the index fits
+        const uint32_t u = (uint32_t)v;
+        const uint32_t r1 = u / (uint32_t)W, r2 = r1 / (uint32_t)H;
+        q.x = (int)(u - r1 * (uint32_t)W);
+        q.y = (int)(r1 - r2 * (uint32_t)H);
+        q.z = (int)(r2 % (uint32_t)D);
+        q.n = (int)(r2 / (uint32_t)D);
+        return q;
+    }
     q.x = (int)(v % W);
     long long r = v / W;
     q.y = (int)(r % H);
@@ -1414,12 +1423,18 @@ __global__ void __launch_bounds__(256) conv_first_kernel(const float *__restrict
     float acc[16];
 #pragma unroll
     for (int c = 0; c < 16; c++) acc[c] = bs[c];
-    for (int t = 0; t < 27; t++) {
-        const int z = q.z + t / 9 - 1, yy = q.y + (t / 3) % 3 - 1, xx = q.x + t % 3 - 1;
-        if ((unsigned)z >= (unsigned)D || (unsigned)yy >= (unsigned)H || (unsigned)xx >= (unsigned)W) continue;
-        const float xv = x[(((long long)q.n * D + z) * H + yy) * W + xx];
+    // the neighbours are v + dz H W + dy W + dx; taps outside the volume are
+    // skipped (compile-time taps, per-axis edge flags: little integer work per tap)
+    const long long HW = (long long)H * W;
+    const bool in[3][3] = {{q.z > 0, true, q.z + 1 < D}, {q.y > 0, true, q.y + 1 < H}, {q.x > 0, true, q.x + 1 < W}};
 #pragma unroll
-        for (int c = 0; c < 16; c++) acc[c] = fmaf(ws[t][c], xv, acc[c]);
+    for (int t = 0; t < 27; t++) {
+        const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+        if (in[0][dz] && in[1][dy] && in[2][dx]) {
+            const float xv = x[v + (dz - 1) * HW + (long long)(dy - 1) * W + (dx - 1)];
+#pragma unroll
+            for (int c = 0; c < 16; c++) acc[c] = fmaf(ws[t][c], xv, acc[c]);
+        }
     }
     uint4 pk[2];
     uint32_t *u = reinterpret_cast<uint32_t *>(pk);
@@ -2064,12 +2079,15 @@ __global__ void __launch_bounds__(128) wgrad_first_kernel(const float *__restric
             const long long v = b * TILE_M + tid;
             const Vox q = decode(v, D, H, W, V);
             float col[32];
+            // neighbours v + dz H W + dy W + dx, per-axis edge flags (as conv_first_kernel)
+            const long long HW = (long long)H * W;
+            const bool in[3][3] = {{q.z > 0, true, q.z + 1 < D}, {q.y > 0, true, q.y + 1 < H},
+                                   {q.x > 0, true, q.x + 1 < W}};
 #pragma unroll
             for (int t = 0; t < 27; t++) {
-                const int z = q.z + t / 9 - 1, yy = q.y + (t / 3) % 3 - 1, xx = q.x + t % 3 - 1;
-                const bool ok = q.ok && (unsigned)z < (unsigned)D && (unsigned)yy < (unsigned)H &&
-                                (unsigned)xx < (unsigned)W;
-                col[t] = ok ? x[(((long long)q.n * D + z) * H + yy) * W + xx] : 0.0f;
+                const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+                const bool ok = q.ok && in[0][dz] && in[1][dy] && in[2][dx];
+                col[t] = ok ? x[v + (dz - 1) * HW + (long long)(dy - 1) * W + (dx - 1)] : 0.0f;
             }
             col[27] = q.ok ? 1.0f : 0.0f;
 #pragma unroll
