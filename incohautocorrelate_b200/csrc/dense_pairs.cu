@@ -569,7 +569,10 @@ __global__ void __launch_bounds__(DTILE) ac1d_cq_kernel(const DenseArgs a)
                                          : make_float4(0.f, 0.f, 0.f, 0.f);
         }
         __syncthreads();
-        const uint64_t ia = tile_pixel(a, P, threadIdx.x);
+        // own pixel 8 apart from the neighbouring lanes' (a bijection of the tile):
+        // the lanes of a warp then add into different bins for one staged pixel
+        const int own = (int)((threadIdx.x & 31) * 8 + (threadIdx.x >> 5));
+        const uint64_t ia = tile_pixel(a, P, own);
         if (ia < a.npix) {
             const float k0 = a.K[3 * ia], k1 = a.K[3 * ia + 1], k2 = a.K[3 * ia + 2];
             const float Ia = a.I[ia];
@@ -579,7 +582,7 @@ __global__ void __launch_bounds__(DTILE) ac1d_cq_kernel(const DenseArgs a)
                     atomicAdd(&hist[0], a.mult_int ? scaled_floor(sv, a.mult_int)
                                                    : (unsigned long long)(long long)dmul((double)sv, a.mult));
             }
-            const int j0 = (P == Q) ? threadIdx.x + 1 : 0;
+            const int j0 = (P == Q) ? own + 1 : 0;
             for (int j = j0; j < DTILE; j++) {
                 const float4 b = sq[j];
                 const float pv = fmul(Ia, b.w);
