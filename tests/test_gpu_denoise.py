@@ -38,7 +38,7 @@ BACKENDS = dict(argvalues=[0, 1, 2], ids=["tcgen05_slab", "mma_sync", "tcgen05_t
 
 @pytest.mark.parametrize("backend", **BACKENDS)
 @pytest.mark.parametrize("c0,up0,c1,cout", FWD + DGRAD)
-@pytest.mark.parametrize("dims", [(2, 8, 8, 16), (2, 4, 6, 10), (4, 16, 32, 64)])
+@pytest.mark.parametrize("dims", [(2, 8, 8, 16), (2, 4, 6, 10), (4, 16, 32, 64), (3, 2, 6, 14)])
 def test_conv3x3_matches_oracle(ctx, rng, backend, c0, up0, c1, cout, dims):
     import torch
     from incohautocorrelate_b200 import capi
