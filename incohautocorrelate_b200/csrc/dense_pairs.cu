@@ -543,6 +543,13 @@ __global__ void __launch_bounds__(DTILE) cq_small_kernel(const DenseArgs a)
 // --------------------------------------------------------------------------
 // AC1D C(q): |q| histogram in shared memory for the whole launch
 // --------------------------------------------------------------------------
+// b % n without the division when b < n (bins past the histogram are rare)
+__device__ __forceinline__ uint32_t wrap_bin(uint32_t b, uint32_t n)
+{
+    if (b >= n) b %= n;
+    return b;
+}
+
 template <int INTERP>
 __global__ void __launch_bounds__(DTILE) ac1d_cq_kernel(const DenseArgs a)
 {
@@ -595,13 +602,13 @@ __global__ void __launch_bounds__(DTILE) ac1d_cq_kernel(const DenseArgs a)
                 if (INTERP == 0) {
                     // sc = (uint)floor(q + 0.5) with q + 0.5 in double; for q < 2^22
                     // the float sum is exact and gives the same bin
-                    const uint32_t sc = (uint32_t)floorf(fadd(q, 0.5f)) % a.hsize;
+                    const uint32_t sc = wrap_bin((uint32_t)floorf(fadd(q, 0.5f)), a.hsize);
                     const unsigned long long v =
                         a.mult_int ? scaled_floor(pv, a.mult_int) : (unsigned long long)(long long)dmul(val, a.mult);
                     atomicAdd(&hist[sc], 2ull * v);
                 } else {
                     const float fq = floorf(q);
-                    const uint32_t sc1 = (uint32_t)fq % a.hsize, sc2 = ((uint32_t)fq + 1) % a.hsize;
+                    const uint32_t sc1 = wrap_bin((uint32_t)fq, a.hsize), sc2 = wrap_bin((uint32_t)fq + 1, a.hsize);
                     const double sep = (double)fsub(q, fq);
                     const unsigned long long v1 =
                         (unsigned long long)(long long)dmul(dmul(val, dsub(1.0, sep)), a.mult);

@@ -451,6 +451,13 @@ __global__ void sparse_fold_kernel(const unsigned long long *__restrict__ half, 
 // do to bins at or beyond VecSize.  The histogram lives in shared memory for
 // the whole launch.  Work queue and pair enumeration are the pair kernel's.
 // ---------------------------------------------------------------------------
+// b % n without the division when b < n (bins past the histogram are rare)
+__device__ __forceinline__ uint32_t wrap_bin(uint32_t b, uint32_t n)
+{
+    if (b >= n) b %= n;
+    return b;
+}
+
 template <int INTERP>
 __global__ void __launch_bounds__(256) ac1d_sparse_kernel(const SparseArgs a, float maxq, float dqdx,
                                                           uint32_t vecsize,
@@ -507,7 +514,7 @@ __global__ void __launch_bounds__(256) ac1d_sparse_kernel(const SparseArgs a, fl
                     q = __fdiv_rn(q, dqdx);
                     const double val = dmul((double)A.w, (double)B.w);
                     if (INTERP == 0) {
-                        const uint32_t sc = (uint32_t)floor(dadd((double)q, 0.5)) % vecsize;
+                        const uint32_t sc = wrap_bin((uint32_t)floor(dadd((double)q, 0.5)), vecsize);
                         const unsigned long long w = d2u64(dmul(val, a.mult));
                         if (w) atomicAdd(&hist[sc], 2ull * w);
                     } else {
@@ -515,8 +522,8 @@ __global__ void __launch_bounds__(256) ac1d_sparse_kernel(const SparseArgs a, fl
                         const double sep = (double)fsub(q, fq);
                         const unsigned long long w1 = d2u64(dmul(dmul(val, dsub(1.0, sep)), a.mult));
                         const unsigned long long w2 = d2u64(dmul(dmul(val, sep), a.mult));
-                        if (w1) atomicAdd(&hist[(uint32_t)fq % vecsize], 2ull * w1);
-                        if (w2) atomicAdd(&hist[((uint32_t)fq + 1) % vecsize], 2ull * w2);
+                        if (w1) atomicAdd(&hist[wrap_bin((uint32_t)fq, vecsize)], 2ull * w1);
+                        if (w2) atomicAdd(&hist[wrap_bin((uint32_t)fq + 1, vecsize)], 2ull * w2);
                     }
                 }
                 i += dr;
