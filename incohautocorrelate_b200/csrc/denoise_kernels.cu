@@ -1782,7 +1782,7 @@ struct WTGeom {
     int S;
 };
 
-constexpr int WT_THREADS = 256;  // warps 0-3 drain, 4 loads, 5-7 issue
+constexpr int WT_THREADS = 448;  // at most: warps 0-3 drain, 4 loads, 5.. issue (NI <= 9)
 
 template <int CIN, int COUT>
 struct WtcCfg {
@@ -1794,7 +1794,7 @@ struct WtcCfg {
     static constexpr int COLS = G * COUT * MB;
     static constexpr uint32_t TCOLS = COLS <= 32 ? 32 : (COLS <= 64 ? 64 : (COLS <= 128 ? 128 : (COLS <= 256 ? 256 : 512)));
     static constexpr int PAD_PLANES = MB * MR / 8 - CIN / 8;  // planes read past the slab by the padded M rows
-    static constexpr int NI = G >= 3 ? 3 : 1;  // MMA-issuing warps, G / NI taps each
+    static constexpr int NI = G >= 9 ? 9 : (G >= 3 ? 3 : 1);  // MMA-issuing warps, G / NI taps each
 };
 
 template <int CIN, int COUT>
@@ -2021,7 +2021,7 @@ static bool launch_wgrad_tc(const WgradArgs &a, int sms, cudaStream_t s, cudaErr
     const int groups = 27 / Cfg::G;
     const long long per_group = std::max<long long>(
         1, std::min<long long>((g.ntiles + 1) / 2, ((long long)per_sm * std::max(1, sms) + groups - 1) / groups));
-    wgrad_tc_kernel<CIN, COUT><<<dim3((unsigned)per_group, groups), WT_THREADS, smem, s>>>(maps[0], maps[1], a, g);
+    wgrad_tc_kernel<CIN, COUT><<<dim3((unsigned)per_group, groups), 32 * (5 + Cfg::NI), smem, s>>>(maps[0], maps[1], a, g);
     if ((err = cudaGetLastError()) != cudaSuccess) return true;
     if (a.db) {
         const int lanes = 256 / COUT;
