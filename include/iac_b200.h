@@ -75,6 +75,18 @@ iac_status iac_ctx_check(iac_ctx *ctx, void *stream, uint64_t *out_of_mesh);
 const char *iac_status_string(iac_status s);
 const char *iac_last_error(void); /* thread-local message of the last failure */
 int iac_abi_version(void);
+/* Failure paths without a GPU fault (the reference has no error recovery: its
+ * device-pool wait has no timeout, IAC/Detector.cpp:1078-1081).
+ * iac_ctx_set_scratch_limit: the largest device scratch buffer the context may
+ * grow (0: no limit); a call that needs more fails with IAC_ERR_NO_MEMORY before
+ * allocating, which both caps the library's working memory and lets callers
+ * test their out-of-memory handling.
+ * iac_ctx_wait_flag: one device thread waits for *d_flag != 0, at most
+ * max_polls polls of about 1 us (<= 10^7); a wait that runs out is counted and
+ * the next iac_ctx_check returns IAC_ERR_TIMEOUT, the context staying usable:
+ * the error path every bounded wait of the library's kernels takes. */
+iac_status iac_ctx_set_scratch_limit(iac_ctx *ctx, uint64_t max_bytes);
+iac_status iac_ctx_wait_flag(iac_ctx *ctx, const uint32_t *d_flag, uint32_t max_polls, void *stream);
 /* number of launches of this library's kernels since the context was made */
 uint64_t iac_ctx_launch_count(const iac_ctx *ctx);
 

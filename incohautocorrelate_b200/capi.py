@@ -107,6 +107,8 @@ def _declare(lib):
     fn("iac_last_error", [], C.c_char_p)
     fn("iac_abi_version", [], C.c_int)
     fn("iac_ctx_launch_count", [_VP], _U64)
+    fn("iac_ctx_set_scratch_limit", [_VP, _U64])
+    fn("iac_ctx_wait_flag", [_VP, _VP, _U32, _VP])
     fn("iac_calc_kmap", [_VP, _VP, _U64, _VP, C.POINTER(C.c_float), _VP])
     fn("iac_big_mesh_shape", [C.POINTER(C.c_float), C.c_int, C.c_float, C.POINTER(MeshShape)])
     fn("iac_small_cq_mesh_shape", [C.POINTER(C.c_float), C.c_int, C.c_float,
@@ -287,6 +289,16 @@ class Context:
 
     def launches(self) -> int:
         return int(lib().iac_ctx_launch_count(self._h))
+
+    def set_scratch_limit(self, max_bytes: int):
+        """Cap the device scratch the context may grow (0: no limit); larger
+        requests fail with IAC_ERR_NO_MEMORY before allocating."""
+        check(lib().iac_ctx_set_scratch_limit(self._h, int(max_bytes)))
+
+    def wait_flag(self, d_flag, max_polls: int, stream=None):
+        """One device thread waits (bounded) for *d_flag != 0; a wait that runs
+        out makes the next check() raise IAC_ERR_TIMEOUT."""
+        check(lib().iac_ctx_wait_flag(self._h, _ptr(d_flag), int(max_polls), _ptr(stream)))
 
     def check(self, stream=None) -> int:
         """Synchronise and return the number of skipped out-of-mesh writes."""

@@ -79,6 +79,20 @@ void Scratch::release()
 
 }  // namespace iac
 
+namespace {
+// one thread waits for *flag != 0, at most max_polls polls of ~1 us; a wait that
+// runs out is counted in the context's timeout counter (the error path of every
+// bounded wait in the library)
+__global__ void wait_flag_kernel(const volatile uint32_t *flag, uint32_t max_polls, iac::DeviceCounters *ctr)
+{
+    for (uint32_t i = 0; i < max_polls; i++) {
+        if (*flag != 0u) return;
+        __nanosleep(1000);
+    }
+    atomicAdd(&ctr->timeouts, 1ull);
+}
+}  // namespace
+
 using namespace iac;
 
 extern "C" {
@@ -177,6 +191,25 @@ iac_status iac_ctx_check(iac_ctx *ctx, void *stream, uint64_t *out_of_mesh)
                   (unsigned long long)h.out_of_mesh);
         return IAC_ERR_OUT_OF_MESH;
     }
+    return IAC_OK;
+}
+
+iac_status iac_ctx_set_scratch_limit(iac_ctx *ctx, uint64_t max_bytes)
+{
+    IAC_REQUIRE(ctx != nullptr, "iac_ctx_set_scratch_limit: ctx is NULL");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->scratch_limit = max_bytes;
+    return IAC_OK;
+}
+
+iac_status iac_ctx_wait_flag(iac_ctx *ctx, const uint32_t *d_flag, uint32_t max_polls, void *stream)
+{
+    IAC_REQUIRE(ctx && d_flag, "iac_ctx_wait_flag: NULL argument");
+    IAC_REQUIRE(max_polls <= 10000000u, "iac_ctx_wait_flag: at most 10^7 polls (about 10 s)");
+    DeviceGuard g(ctx->device);
+    wait_flag_kernel<<<1, 1, 0, as_stream(stream)>>>(d_flag, max_polls, ctx->d_counters);
+    IAC_LAUNCHED(ctx);
+    IAC_CUDA(cudaGetLastError());
     return IAC_OK;
 }
 

@@ -93,6 +93,7 @@ struct iac_ctx {
         uint32_t edge, tile_pairs, block_threads, ctas_per_sm, cache_hints;
     };
     std::vector<TuningRow> tuning_table;  // autotuner results, tuning/sparse_tuning.tsv
+    uint64_t scratch_limit = 0;  // largest scratch buffer the context may grow (0: no limit)
     cudaStream_t host_stream = nullptr;  // stream of the host-buffer entry points
     cudaStream_t copy_stream = nullptr;  // their host-to-device copies
     cudaEvent_t copy_events[IAC_COPY_CHUNKS + 1] = {};
@@ -108,6 +109,12 @@ inline iac_status stream_scratch(iac_ctx *ctx, void *stream, int slot, size_t by
 {
     std::lock_guard<std::mutex> lk(ctx->mu);
     Scratch &s = ctx->stream_scratch[stream].bufs[slot];
+    if (ctx->scratch_limit && bytes > ctx->scratch_limit && bytes > s.bytes) {
+        set_error("scratch of %zu bytes exceeds the context's limit of %llu bytes", bytes,
+                  (unsigned long long)ctx->scratch_limit);
+        *out = nullptr;
+        return IAC_ERR_NO_MEMORY;
+    }
     iac_status st = s.ensure(bytes);
     *out = s.ptr;
     return st;
