@@ -411,6 +411,7 @@ iac_status iac_average_frames(iac_ctx *ctx, const float *d_frames, uint64_t npix
                               const int32_t *d_mask, float threshold, float step, float *d_sum,
                               int64_t *d_discr, float *d_mean_intensity, float *d_photon_sum, void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(ctx && d_frames && d_mean_intensity, "iac_average_frames: NULL argument");
     IAC_REQUIRE(npix > 0 && nframes > 0, "iac_average_frames: empty batch");
     IAC_REQUIRE(step > 0.0f ? d_discr != nullptr : d_sum != nullptr,
@@ -470,6 +471,7 @@ iac_status iac_average_frames(iac_ctx *ctx, const float *d_frames, uint64_t npix
 iac_status iac_average_finish(iac_ctx *ctx, const float *d_sum, const int64_t *d_discr, uint64_t npix,
                               uint32_t nframes_total, float *d_intensity, void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(ctx && d_intensity && (d_sum || d_discr), "iac_average_finish: NULL argument");
     IAC_REQUIRE(nframes_total > 0, "iac_average_finish: no frames");
     DeviceGuard g(ctx->device);

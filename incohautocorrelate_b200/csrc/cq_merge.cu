@@ -132,6 +132,7 @@ extern "C" iac_status iac_cq_merge(iac_ctx *ctx, const double *d_small_cq, const
                                    uint32_t nframes, const iac_mesh_shape *sh, int interp,
                                    double mult, uint64_t *d_big, void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(ctx && d_small_cq && sh && d_big, "iac_cq_merge: NULL argument");
     IAC_REQUIRE(interp == 0 || interp == 1, "interpolation must be 0 or 1");
     IAC_REQUIRE(sh->size_ab >= 5 && sh->size_ab % 2 == 1 && sh->size_c % 2 == 1 &&

@@ -512,6 +512,7 @@ __global__ void kmap_kernel(const float *__restrict__ pm, uint64_t npix, float *
 extern "C" iac_status iac_calc_kmap(iac_ctx *ctx, const float *d_pm, uint64_t npix, float *d_km,
                                     float max_q[3], void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(ctx && d_pm && d_km && max_q, "iac_calc_kmap: NULL argument");
     IAC_REQUIRE(npix > 0, "iac_calc_kmap: empty pixel map");
     DeviceGuard g(ctx->device);

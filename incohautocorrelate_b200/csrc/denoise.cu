@@ -491,6 +491,7 @@ iac_status iac_denoise_get_grads(iac_denoiser *dn, float *h_grads)
 iac_status iac_denoise_forward(iac_denoiser *dn, const float *d_in, uint32_t nb, uint32_t D, uint32_t H,
                                uint32_t W, float *d_out, void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(dn && d_in && d_out, "null argument");
     iac_status st = check_dims(dn, nb, D, H, W);
     if (st != IAC_OK) return st;
@@ -513,6 +514,7 @@ iac_status iac_denoise_backward(iac_denoiser *dn, const float *d_in, const float
                                 uint32_t nb, uint32_t D, uint32_t H, uint32_t W, float *d_out, double *h_loss,
                                 void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(dn && d_in && d_target, "null argument");
     iac_status st = check_dims(dn, nb, D, H, W);
     if (st != IAC_OK) return st;
@@ -532,6 +534,7 @@ iac_status iac_denoise_backward(iac_denoiser *dn, const float *d_in, const float
 
 iac_status iac_denoise_adamw_step(iac_denoiser *dn, const iac_adamw *opt, void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(dn && opt, "null argument");
     IAC_REQUIRE(opt->lr >= 0 && opt->beta1 >= 0 && opt->beta1 < 1 && opt->beta2 >= 0 && opt->beta2 < 1 &&
                     opt->eps > 0,
@@ -546,6 +549,7 @@ iac_status iac_denoise_train_steps(iac_denoiser *dn, const uint16_t *d_in_meshes
                                    uint32_t nsteps, uint32_t nb, uint32_t P, const iac_adamw *opt, double *d_losses,
                                    void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(dn && d_in_meshes && d_tgt_meshes && d_plans && d_lrs && opt, "null argument");
     IAC_REQUIRE(nsteps >= 1 && nmeshes >= 1 && P >= 4 && P % 4 == 0 && P <= E, "steps %u, meshes %u, patch %u of %u",
                 nsteps, nmeshes, P, E);
@@ -631,6 +635,7 @@ iac_status iac_denoise_train_steps(iac_denoiser *dn, const uint16_t *d_in_meshes
 iac_status iac_denoise_crop_patches(iac_ctx *ctx, const uint16_t *d_meshes, uint32_t nmeshes, uint32_t E,
                                     const int32_t *d_plan, uint32_t nb, uint32_t P, float *d_out, void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(ctx && d_meshes && d_plan && d_out, "null argument");
     IAC_REQUIRE(P >= 1 && P <= E, "patch edge %u outside 1..%u", P, E);
     DeviceGuard guard(ctx->device);
@@ -646,6 +651,7 @@ iac_status iac_denoise_conv3x3(iac_ctx *ctx, int backend, const uint16_t *d_src0
                                uint32_t cout, int relu, uint32_t nb, uint32_t D, uint32_t H, uint32_t W,
                                uint16_t *d_y, void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(ctx && d_src1 && d_wtile && d_y && (c0 == 0 || d_src0), "null argument");
     IAC_REQUIRE(backend >= 0 && backend <= 2, "backend %d", backend);
     IAC_REQUIRE(c0 % 16 == 0 && c1 % 8 == 0 && c1 > 0, "channels %u + %u", c0, c1);
@@ -680,6 +686,7 @@ iac_status iac_denoise_wgrad3x3(iac_ctx *ctx, int slabs, const uint16_t *d_src0,
                                 uint32_t nb, uint32_t D, uint32_t H, uint32_t W, float *d_dw, float *d_db,
                                 void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(ctx && d_src1 && d_grad && d_dw && (c0 == 0 || d_src0), "null argument");
     IAC_REQUIRE(D && H && W && nb && (!up0 || (D % 2 == 0 && H % 2 == 0 && W % 2 == 0)), "volume %ux%ux%u", D, H,
                 W);
@@ -710,6 +717,7 @@ iac_status iac_denoise_wgrad3x3(iac_ctx *ctx, int slabs, const uint16_t *d_src0,
 iac_status iac_denoise_mesh_input(iac_ctx *ctx, const uint64_t *d_full, uint32_t S, uint32_t E, double scale,
                                   float *d_f32, uint16_t *d_bf16, void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(ctx && d_full && (d_f32 || d_bf16), "null argument");
     IAC_REQUIRE(E >= 1 && E <= S, "crop edge %u outside 1..%u", E, S);
     DeviceGuard guard(ctx->device);

@@ -682,6 +682,7 @@ iac_status iac_cq_small(iac_ctx *ctx, const float *d_I, const float *d_kmap, uin
                         uint32_t fast_size, const iac_mesh_shape *sh, int interp, double mult,
                         uint64_t *d_mesh, void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(ctx && d_I && d_kmap && sh && d_mesh, "iac_cq_small: NULL argument");
     IAC_REQUIRE(interp == 0 || interp == 1, "interpolation must be 0 or 1");
     IAC_REQUIRE(npix > 0 && npix < (1ull << 32), "iac_cq_small: pixel count %llu out of range",
@@ -744,6 +745,7 @@ iac_status iac_ac1d_cq(iac_ctx *ctx, const float *d_I, const float *d_kmap, uint
                        const iac_ac1d_shape *sh, int interp, double mult, uint64_t *d_hist,
                        void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(ctx && d_I && d_kmap && sh && d_hist, "iac_ac1d_cq: NULL argument");
     IAC_REQUIRE(interp == 0 || interp == 1, "interpolation must be 0 or 1");
     IAC_REQUIRE(npix > 0 && npix < (1ull << 32), "iac_ac1d_cq: pixel count out of range");

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/iac_b200.h"
+#include <nvtx3/nvToolsExt.h>
 
 #define IAC_COPY_CHUNKS 8
 
@@ -40,6 +41,14 @@ void set_error(const char *fmt, ...);
             return IAC_ERR_INVALID_ARG;      \
         }                                    \
     } while (0)
+
+// NVTX range over a C-ABI call, named after it: visible to Nsight Systems and
+// to ncu --nvtx when a tool is attached, a no-op otherwise (header-only NVTX)
+struct TraceRange {
+    explicit TraceRange(const char *name) { nvtxRangePushA(name); }
+    ~TraceRange() { nvtxRangePop(); }
+};
+#define IAC_TRACE() ::iac::TraceRange iac_trace_range_(__func__)
 
 #define IAC_LAUNCHED(ctx) ((ctx)->launches.fetch_add(1, std::memory_order_relaxed))
 

@@ -458,6 +458,7 @@ iac_status iac_crystal_emitters(iac_ctx *ctx, const double *d_atoms, uint32_t na
                                 uint64_t seed, float *d_emitters, uint32_t *d_em_count,
                                 float *d_rot_event, float *d_rot_crystal, void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(ctx && d_atoms && cp && d_emitters && d_em_count && d_rot_event,
                 "iac_crystal_emitters: NULL argument");
     IAC_REQUIRE(natoms > 0 && nmodes > 0, "iac_crystal_emitters: no atoms or modes");
@@ -490,6 +491,7 @@ iac_status iac_simulate_intensity(iac_ctx *ctx, const float *d_pixel_map, uint64
                                   uint32_t natoms, uint32_t nmodes, uint32_t nframes,
                                   const iac_sim_params *sp, float *d_intensity, void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(ctx && d_pixel_map && d_emitters && d_em_count && sp && d_intensity,
                 "iac_simulate_intensity: NULL argument");
     IAC_REQUIRE(npix > 0 && natoms > 0 && nmodes > 0, "iac_simulate_intensity: empty input");
@@ -531,6 +533,7 @@ iac_status iac_simulate_photons(iac_ctx *ctx, float *d_intensity, uint64_t npix,
                                 uint64_t first_frame, const iac_photon_params *pp, uint64_t seed,
                                 void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(ctx && d_intensity && pp, "iac_simulate_photons: NULL argument");
     IAC_REQUIRE(nframes <= 65535, "at most 65535 frames per call");
     if (nframes == 0 || npix == 0) return IAC_OK;
@@ -565,6 +568,7 @@ iac_status iac_sparsify_frames(iac_ctx *ctx, const float *d_intensity, const int
                                float step, int photonize, float *d_photons, uint64_t capacity,
                                uint64_t *d_frame_offsets, uint64_t *h_total, void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(ctx && d_intensity && d_kmap && d_photons && d_frame_offsets,
                 "iac_sparsify_frames: NULL argument");
     IAC_REQUIRE(!photonize || step > 0, "photon step must be positive");

@@ -640,6 +640,7 @@ iac_status iac_sparse_ac_batch(iac_ctx *ctx, const float *d_photons, const uint6
                                const float *d_rot9, uint32_t nframes, const iac_sparse_params *p,
                                uint64_t *d_half, void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(ctx != nullptr, "iac_sparse_ac_batch: ctx is NULL");
     iac_status st = check_params(p);
     if (st != IAC_OK) return st;
@@ -709,6 +710,7 @@ iac_status iac_ac1d_sparse_batch(iac_ctx *ctx, const float *d_photons, const uin
                                  uint32_t nframes, float max_q, float dqdx, int interp,
                                  double mult, uint64_t *d_hist, void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(ctx != nullptr, "iac_ac1d_sparse_batch: ctx is NULL");
     IAC_REQUIRE(interp == 0 || interp == 1, "interpolation must be 0 or 1");
     IAC_REQUIRE(dqdx > 0 && max_q > 0, "iac_ac1d_sparse_batch: MaxQ and dq must be positive");
@@ -755,6 +757,7 @@ uint32_t iac_ac1d_vecsize(float max_q, float dqdx)
 iac_status iac_sparse_fold(iac_ctx *ctx, const uint64_t *d_half, uint32_t S, uint64_t *d_full,
                            void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(ctx && d_half && d_full, "iac_sparse_fold: NULL argument");
     IAC_REQUIRE(S >= 3 && (S % 2) == 1 && S <= 2047, "iac_sparse_fold: bad mesh edge %u", S);
     DeviceGuard g(ctx->device);
@@ -770,6 +773,7 @@ iac_status iac_sparse_ac_frames_host(iac_ctx *ctx, const float *h_photons,
                                      const uint64_t *h_off, const float *h_rot9, uint32_t nframes,
                                      const iac_sparse_params *p, uint64_t *h_full)
 {
+    IAC_TRACE();
     IAC_REQUIRE(ctx != nullptr, "iac_sparse_ac_frames_host: ctx is NULL");
     iac_status st = check_params(p);
     if (st != IAC_OK) return st;
@@ -921,6 +925,7 @@ extern "C" iac_status iac_sparse_ac_batch_static(iac_ctx *ctx, const float *d_ph
                                                  uint32_t nframes, const iac_sparse_params *p,
                                                  uint64_t *d_half, void *stream)
 {
+    IAC_TRACE();
     IAC_REQUIRE(ctx != nullptr, "iac_sparse_ac_batch_static: ctx is NULL");
     iac_status st = check_params(p);
     if (st != IAC_OK) return st;

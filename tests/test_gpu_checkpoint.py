@@ -1,0 +1,64 @@
+"""Checkpoint and resume of a correlation run (incohautocorrelate_b200.checkpoint):
+a run cut short after a few batches and resumed from its checkpoint, in a new
+context, ends with the oracle's mesh bit for bit; a checkpoint of other binning
+parameters is refused."""
+import numpy as np
+import pytest
+
+from helpers import random_frames, small_detector, to_capi_shape
+
+pytestmark = pytest.mark.gpu
+
+
+def _frames(oracle_lib, rng):
+    from incohautocorrelate_b200 import workloads as W
+    _, km, mq = small_detector()
+    shape = oracle_lib.big_mesh_shape(mq, 31)
+    sizes = rng.integers(0, 90, 300)
+    ph, off = random_frames(km, sizes, rng)
+    rot = W.haar_rotations(len(sizes), seed=41)
+    want, _ = oracle_lib.sparse_batch(ph, off, rot, shape, 0, 0, 1, cpu_gpu=1)
+    return shape, ph, off, rot, want
+
+
+def test_resumed_run_equals_the_oracle(tmp_path, oracle_lib, rng):
+    from incohautocorrelate_b200 import capi
+    from incohautocorrelate_b200.checkpoint import MeshRun
+    shape, ph, off, rot, want = _frames(oracle_lib, rng)
+    p = capi.sparse_params(to_capi_shape(shape), 0, 0, True, 1000.0)
+    S = shape.size_ab
+    path = str(tmp_path / "run.npz")
+    ctx = capi.Context(0)
+    run = MeshRun(ctx, p, S)
+    cursor = run.bin_frames(ph, off, rot, batch=37, checkpoint=path, every=2, stop_after=5)
+    assert cursor == 5 * 37
+    run.bin_frames(ph, off, rot, batch=37, stop_after=1)  # binned after the last save: lost
+    ctx.close()
+    ctx2 = capi.Context(0)
+    try:
+        run2 = MeshRun.resume(ctx2, p, S, path)
+        assert run2.cursor == 4 * 37  # the save after batch 4; batch 5 and the next one re-run
+        assert run2.bin_frames(ph, off, rot, batch=37, checkpoint=path) == len(off) - 1
+        np.testing.assert_array_equal(run2.full_mesh(), want)
+        run3 = MeshRun.resume(ctx2, p, S, path)  # a finished run resumes with nothing to do
+        assert run3.bin_frames(ph, off, rot, batch=37) == len(off) - 1
+        np.testing.assert_array_equal(run3.full_mesh(), want)
+    finally:
+        ctx2.close()
+
+
+def test_checkpoint_of_other_parameters_is_refused(tmp_path, oracle_lib, rng):
+    from incohautocorrelate_b200 import capi
+    from incohautocorrelate_b200.checkpoint import MeshRun
+    shape, ph, off, rot, _ = _frames(oracle_lib, rng)
+    p = capi.sparse_params(to_capi_shape(shape), 0, 0, True, 1000.0)
+    S = shape.size_ab
+    path = str(tmp_path / "run.npz")
+    ctx = capi.Context(0)
+    try:
+        MeshRun(ctx, p, S).bin_frames(ph, off, rot, batch=100, checkpoint=path, stop_after=1)
+        other = capi.sparse_params(to_capi_shape(shape), 0, 0, False, 1000.0)
+        with pytest.raises(ValueError, match="other mesh or binning parameters"):
+            MeshRun.resume(ctx, other, S, path)
+    finally:
+        ctx.close()
