@@ -405,6 +405,12 @@ iac_status iac_denoise_init_params(iac_denoiser *dn, uint64_t seed);
 iac_status iac_denoise_set_params(iac_denoiser *dn, const float *h_params);
 iac_status iac_denoise_get_params(iac_denoiser *dn, float *h_params);
 iac_status iac_denoise_get_grads(iac_denoiser *dn, float *h_grads);
+/* Training state for checkpoint/resume (no counterpart in the reference): the
+ * AdamW moments (nparams floats each) and step count; set_state restores the
+ * parameters, moments and step together (set_params resets the moments). */
+iac_status iac_denoise_get_state(iac_denoiser *dn, float *h_m, float *h_v, uint64_t *h_step);
+iac_status iac_denoise_set_state(iac_denoiser *dn, const float *h_params, const float *h_m, const float *h_v,
+                                 uint64_t step);
 
 /* d_out = network(d_in).  Asynchronous on `stream`. */
 iac_status iac_denoise_forward(iac_denoiser *dn, const float *d_in, uint32_t nb, uint32_t D, uint32_t H,

@@ -148,6 +148,8 @@ def _declare(lib):
     fn("iac_denoise_set_params", [_VP, _VP])
     fn("iac_denoise_get_params", [_VP, _VP])
     fn("iac_denoise_get_grads", [_VP, _VP])
+    fn("iac_denoise_get_state", [_VP, _VP, _VP, C.POINTER(_U64)])
+    fn("iac_denoise_set_state", [_VP, _VP, _VP, _VP, _U64])
     fn("iac_denoise_forward", [_VP, _VP, _U32, _U32, _U32, _U32, _VP, _VP])
     fn("iac_denoise_backward", [_VP, _VP, _VP, _VP, _U32, _U32, _U32, _U32, _VP,
                                 C.POINTER(C.c_double), _VP])
@@ -461,6 +463,25 @@ class Denoiser:
         g = np.zeros(self.nparams, np.float32)
         check(lib().iac_denoise_get_grads(self._h, g.ctypes.data))
         return g
+
+    def get_state(self):
+        """(parameters, AdamW first moments, second moments, optimizer steps)."""
+        import numpy as np
+        m = np.zeros(self.nparams, np.float32)
+        v = np.zeros(self.nparams, np.float32)
+        step = _U64(0)
+        check(lib().iac_denoise_get_state(self._h, m.ctypes.data, v.ctypes.data, C.byref(step)))
+        return self.get_params(), m, v, int(step.value)
+
+    def set_state(self, params, m, v, step: int):
+        """Restore parameters, moments and step count together (a resumed run)."""
+        import numpy as np
+        arrs = [np.ascontiguousarray(a, np.float32) for a in (params, m, v)]
+        for a in arrs:
+            if a.size != self.nparams:
+                raise ValueError(f"state arrays need {self.nparams} values, got {a.size}")
+        check(lib().iac_denoise_set_state(self._h, arrs[0].ctypes.data, arrs[1].ctypes.data,
+                                          arrs[2].ctypes.data, int(step)))
 
     def forward(self, d_in, nb, D, H, W, d_out, stream=None):
         check(lib().iac_denoise_forward(self._h, _ptr(d_in), int(nb), int(D), int(H), int(W),

@@ -479,6 +479,33 @@ iac_status iac_denoise_get_params(iac_denoiser *dn, float *h_params)
     return IAC_OK;
 }
 
+iac_status iac_denoise_get_state(iac_denoiser *dn, float *h_m, float *h_v, uint64_t *h_step)
+{
+    IAC_REQUIRE(dn && h_m && h_v && h_step, "null argument");
+    DeviceGuard guard(dn->ctx->device);
+    DN_CHECK(cudaDeviceSynchronize(), "get optimizer state");
+    DN_CHECK(cudaMemcpy(h_m, dn->m, dn->nparams * 4, cudaMemcpyDeviceToHost), "get first moments");
+    DN_CHECK(cudaMemcpy(h_v, dn->v, dn->nparams * 4, cudaMemcpyDeviceToHost), "get second moments");
+    *h_step = (uint64_t)dn->adam_step;
+    return IAC_OK;
+}
+
+iac_status iac_denoise_set_state(iac_denoiser *dn, const float *h_params, const float *h_m, const float *h_v,
+                                 uint64_t step)
+{
+    IAC_REQUIRE(dn && h_params && h_m && h_v, "null argument");
+    IAC_REQUIRE(step < (1ull << 62), "optimizer step count %llu out of range", (unsigned long long)step);
+    DeviceGuard guard(dn->ctx->device);
+    DN_CHECK(cudaMemcpy(dn->p, h_params, dn->nparams * 4, cudaMemcpyHostToDevice), "set parameters");
+    DN_CHECK(cudaMemcpy(dn->m, h_m, dn->nparams * 4, cudaMemcpyHostToDevice), "set first moments");
+    DN_CHECK(cudaMemcpy(dn->v, h_v, dn->nparams * 4, cudaMemcpyHostToDevice), "set second moments");
+    dn->adam_step = (long long)step;
+    iac_status st = refresh_tiles(dn, nullptr, 0);
+    if (st != IAC_OK) return st;
+    DN_CHECK(cudaDeviceSynchronize(), "set optimizer state");
+    return IAC_OK;
+}
+
 iac_status iac_denoise_get_grads(iac_denoiser *dn, float *h_grads)
 {
     IAC_REQUIRE(dn && h_grads, "null argument");

@@ -316,16 +316,33 @@ def evaluate(ctx, sim: MeshSimulator, dn, norm, n_crystals, frames_in, plain_fra
     return summary, rows
 
 
-def save_model(path, dn, norm, setup: SimSetup, extra=None):
+def save_model(path, dn, norm, setup: SimSetup, extra=None, optimizer_state=False):
+    """Parameters and metadata; with optimizer_state also the AdamW moments and
+    step count, so that training can resume where it stopped (resume_model)."""
     meta = {"norm": norm, "setup": asdict(setup)}
     if extra:
         meta.update(extra)
-    np.savez_compressed(path, params=dn.get_params(), meta=json.dumps(meta))
+    if optimizer_state:
+        params, m, v, step = dn.get_state()
+        np.savez_compressed(path, params=params, meta=json.dumps(meta), adam_m=m, adam_v=v, adam_step=step)
+    else:
+        np.savez_compressed(path, params=dn.get_params(), meta=json.dumps(meta))
 
 
 def load_model(path):
     z = np.load(path)
     return z["params"], json.loads(str(z["meta"]))
+
+
+def resume_model(path, dn):
+    """Restore parameters and, when saved, the optimizer state into `dn`;
+    returns the metadata."""
+    z = np.load(path)
+    if "adam_m" in z.files:
+        dn.set_state(z["params"], z["adam_m"], z["adam_v"], int(z["adam_step"]))
+    else:
+        dn.set_params(z["params"])
+    return json.loads(str(z["meta"]))
 
 
 def main(argv=None):
