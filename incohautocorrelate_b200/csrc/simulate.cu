@@ -247,6 +247,66 @@ __global__ void __launch_bounds__(SIM_THREADS) simulate_kernel(const SimArgs a)
     a.out[(size_t)f * a.npix + p] = total;
 }
 
+// simulate_kernel for crystals whose emitters do not fit the shared-memory
+// stage (more than SIM_MAX_EM, or modes x emitters past 200 KB): per mode and
+// sub-pixel the emitters stream through a stage of SIM_MAX_EM, chunk by chunk
+// in emitter order, so every pixel's phase sum adds the same terms in the same
+// order as the staged kernel
+__global__ void __launch_bounds__(SIM_THREADS) simulate_chunked_kernel(const SimArgs a)
+{
+    __shared__ float4 s_em[SIM_MAX_EM];
+    const uint32_t f = blockIdx.y;
+    const uint64_t p = blockIdx.x * (uint64_t)SIM_THREADS + threadIdx.x;
+    const bool live = p < a.npix;
+    const float pc0 = live ? a.pm[3 * p] : 0.0f, pc1 = live ? a.pm[3 * p + 1] : 0.0f,
+                pc2 = live ? a.pm[3 * p + 2] : 0.0f;
+    const float nsub = (float)((2 * a.susa + 1) * (2 * a.susa + 1));
+    float total = 0.0f;
+    for (uint32_t m = 0; m < a.nmodes; m++) {
+        const uint32_t n = min(a.em_count[(size_t)f * a.nmodes + m], a.natoms);
+        const float4 *src = a.em + ((size_t)f * a.nmodes + m) * a.natoms;
+        float acc = 0.0f;
+        for (int v = -a.susa; v <= a.susa; v++)
+            for (int u = -a.susa; u <= a.susa; u++) {
+                const float c0 = fadd(fadd(pc0, fmul((float)v, a.vs[0])), fmul((float)u, a.us[0]));
+                const float c1 = fadd(fadd(pc1, fmul((float)v, a.vs[1])), fmul((float)u, a.us[1]));
+                const float c2 = fadd(fadd(pc2, fmul((float)v, a.vs[2])), fmul((float)u, a.us[2]));
+                float nk = live ? (float)(1.0 / (double)norm3(c0, c1, c2)) : 0.0f;
+                nk = (float)((double)nk * ((2.0 * 3.1415926535897932) / (double)a.wavelength));
+                const float k0 = fmul(c0, nk), k1 = fmul(c1, nk), k2 = fmul(c2, nk);
+                float re = 0.0f, im = 0.0f;
+                for (uint32_t c = 0; c < n; c += SIM_MAX_EM) {
+                    const uint32_t cn = min(n - c, (uint32_t)SIM_MAX_EM);
+                    __syncthreads();  // the previous chunk is read
+                    for (uint32_t i = threadIdx.x; i < cn; i += SIM_THREADS) s_em[i] = src[c + i];
+                    __syncthreads();
+                    if (!live) continue;
+                    for (uint32_t i = 0; i < cn; i++) {
+                        const float4 e = s_em[i];
+                        float arg = fmul(k0, e.x);
+                        arg = fadd(arg, fmul(k1, e.y));
+                        arg = fadd(arg, fmul(k2, e.z));
+                        arg = fadd(arg, e.w);
+                        float sn, cs;
+                        if (a.accurate) {
+                            sincosf(arg, &sn, &cs);
+                        } else {
+                            const float kk = rintf(arg * INV_TWO_PI);
+                            const float r = fmaf(-kk, TWO_PI_LO, fmaf(-kk, TWO_PI_HI, arg));
+                            __sincosf(r, &sn, &cs);
+                        }
+                        re = fadd(re, cs);
+                        im = fadd(im, sn);
+                    }
+                }
+                const float a2 = fadd(fmul(re, re), fmul(im, im));
+                acc = fadd(acc, a.amplitude_sq ? a2 : __fsqrt_rn(a2));
+            }
+        total = fadd(total, __fdiv_rn(acc, nsub));
+    }
+    if (live) a.out[(size_t)f * a.npix + p] = total;
+}
+
 // per-frame double sum, one CTA per frame
 __global__ void frame_sum_kernel(const float *__restrict__ I, uint64_t npix, double *__restrict__ sums)
 {
@@ -495,9 +555,6 @@ iac_status iac_simulate_intensity(iac_ctx *ctx, const float *d_pixel_map, uint64
     IAC_REQUIRE(ctx && d_pixel_map && d_emitters && d_em_count && sp && d_intensity,
                 "iac_simulate_intensity: NULL argument");
     IAC_REQUIRE(npix > 0 && natoms > 0 && nmodes > 0, "iac_simulate_intensity: empty input");
-    IAC_REQUIRE(natoms <= SIM_MAX_EM, "at most %d emitters per crystal (got %u)", SIM_MAX_EM, natoms);
-    IAC_REQUIRE(nmodes * std::min(natoms, (uint32_t)SIM_MAX_EM) * 16 <= 200 * 1024,
-                "modes x emitters exceed the shared-memory stage");
     IAC_REQUIRE(sp->subsampling >= 0 && sp->subsampling <= 16, "SubSampling out of range");
     IAC_REQUIRE(sp->wavelength > 0, "wavelength must be positive");
     IAC_REQUIRE(nframes <= 65535, "at most 65535 frames per call");
@@ -520,10 +577,15 @@ iac_status iac_simulate_intensity(iac_ctx *ctx, const float *d_pixel_map, uint64
     a.amplitude_sq = sp->intensity_squared;
     a.accurate = sp->accurate_sincos;
     a.out = d_intensity;
-    const size_t smem = sizeof(float4) * nmodes * std::min(natoms, (uint32_t)SIM_MAX_EM);
-    IAC_CUDA(cudaFuncSetAttribute(simulate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid((unsigned)((npix + SIM_THREADS - 1) / SIM_THREADS), nframes);
-    simulate_kernel<<<grid, SIM_THREADS, smem, as_stream(stream)>>>(a);
+    if (natoms <= (uint32_t)SIM_MAX_EM && (uint64_t)nmodes * natoms * 16 <= 200 * 1024) {
+        // every mode's emitters staged at once
+        const size_t smem = sizeof(float4) * nmodes * natoms;
+        IAC_CUDA(cudaFuncSetAttribute(simulate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        simulate_kernel<<<grid, SIM_THREADS, smem, as_stream(stream)>>>(a);
+    } else {
+        simulate_chunked_kernel<<<grid, SIM_THREADS, 0, as_stream(stream)>>>(a);
+    }
     IAC_LAUNCHED(ctx);
     IAC_CUDA(cudaGetLastError());
     return IAC_OK;

@@ -145,6 +145,35 @@ def test_simulated_intensity_against_reference_arithmetic(ctx, oracle_lib, susa,
         np.testing.assert_allclose(want, f64, atol=1e-3 * scale, rtol=0)
 
 
+@pytest.mark.parametrize("cells,nmodes", [((10, 10, 15), 2), ((10, 10, 10), 14)])
+def test_large_crystals_stream_through_shared_memory(ctx, oracle_lib, cells, nmodes):
+    """Crystals past the shared-memory stage (1 500 emitters; 14 modes x 1 000
+    emitters) take the chunked kernel: same tolerance against the oracle."""
+    import torch
+    from incohautocorrelate_b200 import capi
+    o = oracle_lib
+    pm = _sim_setup(o, npx=24)
+    npix = pm.size // 3
+    atoms = lattice(o, cells=cells)
+    nframes = 2
+    em, cnt, rot, rc = gpu_emitters(ctx, atoms, nframes, nmodes, seed=9)
+    us = 2e7
+    sp = capi.SimParams(0, (C.c_double * 3)(us, 0, 0), (C.c_double * 3)(0, us, 0), 1.55, 1, 0)
+    out = torch.zeros((nframes, npix), dtype=torch.float32, device="cuda")
+    ctx.simulate_intensity(_dev(pm), npix, em, cnt, len(atoms), nmodes, nframes, sp, out)
+    got, emn = out.cpu().numpy(), em.cpu().numpy()
+    P = np.array([len(atoms), 1, 0, us, 0, 0, 0, us, 0, 1.55], np.float64)
+    for f in range(nframes):
+        want = np.zeros(npix, np.float32)
+        for m in range(nmodes):
+            e = np.ascontiguousarray(emn[f, m])
+            t = np.zeros(npix, np.float32)
+            o.lib().iaco_simulate_crystal(o.p(pm), npix, o.p(e), len(e), o.p(P), 1, o.p(t))
+            want += t
+        np.testing.assert_allclose(got[f], want, atol=2e-5 * float(want.max()), rtol=0)
+    assert ctx.check() == 0
+
+
 def test_poisson_draws_match_oracle(ctx, oracle_lib):
     """Rescaled intensity -> counter-based Poisson draws: the GPU counts equal
     the oracle's draws from the same streams (both evaluate exp/log/cos in
