@@ -53,13 +53,14 @@ class SimSetup:
     mesh_edge: int = 127  # MeshSize argument: the mesh is (edge + 2)^3
     crop: int = 128
     chunk: int = 2000
-    max_emitters: int = 1024
+    max_emitters: int = 2048  # the largest crystal below: 8 x 8 x 8 cells x 4
 
 
-def random_crystal(rng, max_emitters=1024):
+def random_crystal(rng, max_emitters=2048):
     """Emitter positions (A, centred) of a random crystal: cubic lattice
     constant a in [3, 6], 2..8 cells per axis, 1..4 emitters per cell at
-    random fractional positions (at most max_emitters in total)."""
+    random fractional positions (8 to 2048 emitters; a smaller max_emitters
+    redraws the larger crystals)."""
     while True:
         a = float(rng.uniform(3.0, 6.0))
         cells = rng.integers(2, 9, size=3)

@@ -226,7 +226,7 @@ def test_trained_denoiser_needs_fewer_frames_than_the_plain_mesh(ctx):
     """The committed network (trained on 512 random crystals, 500 -> 50 000
     frames) on held-out crystals it never saw: the denoised 500-frame mesh
     against an independent 40 000-frame reference matches the plain mesh of
-    several times more frames (measured 10-20x, median 15x, on 32 crystals with
+    several times more frames (measured 13-26x, median 19x, on 32 crystals with
     a 100 000-frame reference; this test asserts a median above 8x on four)."""
     import os
 
