@@ -609,6 +609,63 @@ static iac_status check_params(const iac_sparse_params *p)
     return IAC_OK;
 }
 
+// Work-queue memory of one batch: tile table (nframes + 1), queue counter,
+// per-frame small-count flags (nframes bytes).
+struct QueueMem {
+    unsigned long long *tile_off;
+    unsigned long long *queue;
+    unsigned char *flags;
+};
+
+// Planner, count check and pair kernel of one batch into the half mesh d_half.
+static iac_status launch_pair_batch(iac_ctx *ctx, const float *d_photons, const uint64_t *d_off,
+                                    const float *d_rot9, uint32_t nframes, const iac_sparse_params *p,
+                                    const QueueMem &q, uint64_t *d_half, cudaStream_t s)
+{
+    const iac_sparse_tuning tun = effective_tuning(ctx, p->shape.size_ab);
+    sparse_plan_kernel<<<1, PLAN_THREADS, 0, s>>>(d_off, nframes, tun.tile_pairs, q.tile_off, q.queue);
+    IAC_LAUNCHED(ctx);
+    IAC_CUDA(cudaGetLastError());
+    const bool mult_small_int = p->multiplicator >= 1.0 && p->multiplicator <= 1024.0 &&
+                                p->multiplicator == std::floor(p->multiplicator);
+    unsigned char *flags = nullptr;
+    if (mult_small_int && p->interp_second == 0 && !(p->double_map && p->interp_first == 1)) {
+        const uint32_t blocks = (uint32_t)(((uint64_t)nframes * 32 + 255) / 256);
+        sparse_count_check_kernel<<<blocks, 256, 0, s>>>(reinterpret_cast<const float4 *>(d_photons),
+                                                         d_off, nframes, q.flags);
+        IAC_LAUNCHED(ctx);
+        IAC_CUDA(cudaGetLastError());
+        flags = q.flags;
+    }
+    SparseArgs a;
+    a.photons = reinterpret_cast<const float4 *>(d_photons);
+    a.offsets = d_off;
+    a.rot = d_rot9;
+    a.tile_off = q.tile_off;
+    a.half = reinterpret_cast<unsigned long long *>(d_half);
+    a.queue = q.queue;
+    a.counters = ctx->d_counters;
+    a.nframes = nframes;
+    a.tile_pairs = tun.tile_pairs;
+    a.S = (int)p->shape.size_ab;
+    a.C = (a.S - 1) / 2;
+    a.half_ss = (a.S + 1) / 2;
+    a.plane = (uint32_t)a.S * (uint32_t)a.S;
+    a.maxq = p->shape.max_q;
+    a.maxq2 = sqrt_threshold(p->shape.max_q);
+    a.vpdq = (float)p->shape.voxel_per_dq;
+    a.mult = p->multiplicator;
+    a.mult_f = (float)p->multiplicator;
+    a.small_counts = flags;
+    a.cache_hints = tun.cache_hints == 1 ? 1 : 0;
+    a.mesh_policy = 0;
+    const PairKernel k = pick_kernel(p->double_map, p->interp_first, p->interp_second);
+    k<<<ctx->sm_count * (int)tun.ctas_per_sm, tun.block_threads, 0, s>>>(a);
+    IAC_LAUNCHED(ctx);
+    IAC_CUDA(cudaGetLastError());
+    return IAC_OK;
+}
+
 }  // namespace iac
 
 using namespace iac;
@@ -649,61 +706,13 @@ iac_status iac_sparse_ac_batch(iac_ctx *ctx, const float *d_photons, const uint6
     IAC_REQUIRE((reinterpret_cast<uintptr_t>(d_photons) & 15) == 0,
                 "photon array must be 16-byte aligned (float4 per photon)");
     DeviceGuard g(ctx->device);
-    const iac_sparse_tuning tun = effective_tuning(ctx, p->shape.size_ab);
-
     void *scratch = nullptr;
     const size_t table_bytes = ((sizeof(unsigned long long) * ((size_t)nframes + 1) + 127) / 128) * 128;
     st = stream_scratch(ctx, stream, SLOT_TILES, table_bytes + 128 + nframes, &scratch);
     if (st != IAC_OK) return st;
-    unsigned long long *tile_off = (unsigned long long *)scratch;
-    unsigned long long *queue = (unsigned long long *)((char *)scratch + table_bytes);
-    unsigned char *flags = (unsigned char *)scratch + table_bytes + 128;
-
-    cudaStream_t s = as_stream(stream);
-    sparse_plan_kernel<<<1, PLAN_THREADS, 0, s>>>(d_off, nframes, tun.tile_pairs, tile_off, queue);
-    IAC_LAUNCHED(ctx);
-    IAC_CUDA(cudaGetLastError());
-    const bool mult_small_int = p->multiplicator >= 1.0 && p->multiplicator <= 1024.0 &&
-                                p->multiplicator == std::floor(p->multiplicator);
-    if (mult_small_int && p->interp_second == 0 && !(p->double_map && p->interp_first == 1)) {
-        const uint32_t blocks = (uint32_t)(((uint64_t)nframes * 32 + 255) / 256);
-        sparse_count_check_kernel<<<blocks, 256, 0, s>>>(
-            reinterpret_cast<const float4 *>(d_photons), d_off, nframes, flags);
-        IAC_LAUNCHED(ctx);
-        IAC_CUDA(cudaGetLastError());
-    } else {
-        flags = nullptr;
-    }
-
-    SparseArgs a;
-    a.photons = reinterpret_cast<const float4 *>(d_photons);
-    a.offsets = d_off;
-    a.rot = d_rot9;
-    a.tile_off = tile_off;
-    a.half = reinterpret_cast<unsigned long long *>(d_half);
-    a.queue = queue;
-    a.counters = ctx->d_counters;
-    a.nframes = nframes;
-    a.tile_pairs = tun.tile_pairs;
-    a.S = (int)p->shape.size_ab;
-    a.C = (a.S - 1) / 2;
-    a.half_ss = (a.S + 1) / 2;
-    a.plane = (uint32_t)a.S * (uint32_t)a.S;
-    a.maxq = p->shape.max_q;
-    a.maxq2 = sqrt_threshold(p->shape.max_q);
-    a.vpdq = (float)p->shape.voxel_per_dq;
-    a.mult = p->multiplicator;
-    a.mult_f = (float)p->multiplicator;
-    a.small_counts = flags;
-    a.cache_hints = tun.cache_hints == 1 ? 1 : 0;
-    a.mesh_policy = 0;
-
-    const PairKernel k = pick_kernel(p->double_map, p->interp_first, p->interp_second);
-    const int grid = ctx->sm_count * (int)tun.ctas_per_sm;
-    k<<<grid, tun.block_threads, 0, s>>>(a);
-    IAC_LAUNCHED(ctx);
-    IAC_CUDA(cudaGetLastError());
-    return IAC_OK;
+    const QueueMem q{(unsigned long long *)scratch, (unsigned long long *)((char *)scratch + table_bytes),
+                     (unsigned char *)scratch + table_bytes + 128};
+    return launch_pair_batch(ctx, d_photons, d_off, d_rot9, nframes, p, q, d_half, as_stream(stream));
 }
 
 iac_status iac_ac1d_sparse_batch(iac_ctx *ctx, const float *d_photons, const uint64_t *d_off,
@@ -940,51 +949,7 @@ extern "C" iac_status iac_sparse_ac_batch_static(iac_ctx *ctx, const float *d_ph
     DeviceGuard g(ctx->device);
     void *base = nullptr;
     if ((st = static_scratch_address(ctx->device, &base)) != IAC_OK) return st;
-    const iac_sparse_tuning tun = effective_tuning(ctx, p->shape.size_ab);
-    unsigned long long *tile_off = (unsigned long long *)base;
-    unsigned long long *queue = (unsigned long long *)((char *)base + STATIC_TABLE_BYTES);
-    unsigned char *flags = (unsigned char *)base + STATIC_TABLE_BYTES + STATIC_QUEUE_BYTES;
-
-    cudaStream_t s = as_stream(stream);
-    sparse_plan_kernel<<<1, PLAN_THREADS, 0, s>>>(d_off, nframes, tun.tile_pairs, tile_off, queue);
-    IAC_LAUNCHED(ctx);
-    IAC_CUDA(cudaGetLastError());
-    const bool mult_small_int = p->multiplicator >= 1.0 && p->multiplicator <= 1024.0 &&
-                                p->multiplicator == std::floor(p->multiplicator);
-    if (mult_small_int && p->interp_second == 0 && !(p->double_map && p->interp_first == 1)) {
-        const uint32_t blocks = (uint32_t)(((uint64_t)nframes * 32 + 255) / 256);
-        sparse_count_check_kernel<<<blocks, 256, 0, s>>>(reinterpret_cast<const float4 *>(d_photons),
-                                                         d_off, nframes, flags);
-        IAC_LAUNCHED(ctx);
-        IAC_CUDA(cudaGetLastError());
-    } else {
-        flags = nullptr;
-    }
-    SparseArgs a;
-    a.photons = reinterpret_cast<const float4 *>(d_photons);
-    a.offsets = d_off;
-    a.rot = d_rot9;
-    a.tile_off = tile_off;
-    a.half = reinterpret_cast<unsigned long long *>(d_half);
-    a.queue = queue;
-    a.counters = ctx->d_counters;
-    a.nframes = nframes;
-    a.tile_pairs = tun.tile_pairs;
-    a.S = (int)p->shape.size_ab;
-    a.C = (a.S - 1) / 2;
-    a.half_ss = (a.S + 1) / 2;
-    a.plane = (uint32_t)a.S * (uint32_t)a.S;
-    a.maxq = p->shape.max_q;
-    a.maxq2 = sqrt_threshold(p->shape.max_q);
-    a.vpdq = (float)p->shape.voxel_per_dq;
-    a.mult = p->multiplicator;
-    a.mult_f = (float)p->multiplicator;
-    a.small_counts = flags;
-    a.cache_hints = tun.cache_hints == 1 ? 1 : 0;
-    a.mesh_policy = 0;
-    const PairKernel k = pick_kernel(p->double_map, p->interp_first, p->interp_second);
-    k<<<ctx->sm_count * (int)tun.ctas_per_sm, tun.block_threads, 0, s>>>(a);
-    IAC_LAUNCHED(ctx);
-    IAC_CUDA(cudaGetLastError());
-    return IAC_OK;
+    const QueueMem q{(unsigned long long *)base, (unsigned long long *)((char *)base + STATIC_TABLE_BYTES),
+                     (unsigned char *)base + STATIC_TABLE_BYTES + STATIC_QUEUE_BYTES};
+    return launch_pair_batch(ctx, d_photons, d_off, d_rot9, nframes, p, q, d_half, as_stream(stream));
 }
