@@ -26,7 +26,7 @@ TABLE = os.path.join(HERE, "tuning", "sparse_tuning.tsv")
 
 GRID = dict(tile_pairs=[1024, 2048, 4096, 8192, 16384],
             block_threads=[128, 256],
-            ctas_per_sm=[4, 8, 16],
+            ctas_per_sm=[4, 6, 8, 12, 16],
             cache_hints=[2, 1])
 
 
