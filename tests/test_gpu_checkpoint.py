@@ -98,8 +98,12 @@ def test_denoiser_training_resumes_with_its_optimizer_state(rng):
         dn3 = capi.Denoiser(ctx, 2, 16, 16, 16)
         dn3.set_params(p)  # parameters only: moments and step start again
         c = steps(dn3, 4)
-        resumed, restarted = np.abs(b - a).max(), np.abs(c - a).max()
-        assert resumed < 1e-4 * np.abs(a).max(), resumed
+        # L2 norms over all parameters: AdamW divides by sqrt(v), so the float
+        # atomics' ordering noise can move a parameter whose gradient is near
+        # zero by a visible amount; the run as a whole must still follow.
+        moved = np.linalg.norm(a - p)
+        resumed, restarted = np.linalg.norm(b - a), np.linalg.norm(c - a)
+        assert resumed < 1e-2 * moved, (resumed, moved)
         assert restarted > 10 * resumed, (restarted, resumed)
         for d in (dn, dn2, dn3):
             d.close()
