@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--cpu-frames", type=int, default=1500,
                     help="frames per step of the --impl reference arm")
     ap.add_argument("--cpu-baseline-frames", type=int, default=100_000,
-                    help="frames of the cpu_baseline sample (all 100 000: about 12 s on 16 host threads)")
+                    help="frames of the cpu_baseline sample (all 100 000: about 8 s on 16 host threads)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--det", type=int, default=1024,
                     help="edge of the square detector of the dense kernels (1024 = their config)")

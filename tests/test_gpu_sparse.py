@@ -131,6 +131,27 @@ def test_tuning_does_not_change_the_mesh(ctx, oracle_lib, rng, tuning):
     np.testing.assert_array_equal(got, want)
 
 
+@pytest.mark.parametrize("edge", [5, 7, 15])
+@pytest.mark.parametrize("dmap,i1,i2", [(0, 0, 0), (1, 0, 0), (1, 1, 1)])
+def test_tiny_meshes_inside_the_shared_box(ctx, oracle_lib, rng, edge, dmap, i1, i2):
+    """Meshes of 7^3, 9^3 and 17^3 (the smallest MeshSize with a nonzero
+    Voxel_per_dq for this detector is 5): the per-CTA shared-memory box around
+    q = 0 shrinks to the mesh's centre C and covers whole planes; at 1 and 16
+    CTAs per SM (largest and smallest box).  Frames of at most 25 photons keep
+    every frame's sum in one voxel below the reference device route's fold
+    quirk (about 1.05e7; all 300 pairs x 9 x 1000, twice on ss = 0, is 5.4e6)."""
+    from incohautocorrelate_b200 import workloads as W
+    _, km, mq = small_detector()
+    shape = oracle_lib.big_mesh_shape(mq, edge)
+    ph, off = random_frames(km, [0, 2, 12, 25, 7, 25, 19], rng, integer=(i1 == 0 and i2 == 0))
+    rot = W.haar_rotations(7, seed=13)
+    want, o1 = oracle_lib.sparse_batch(ph, off, rot, shape, i1, i2, dmap, cpu_gpu=1)
+    for tuning in (dict(ctas_per_sm=1), dict(ctas_per_sm=16, block_threads=128)):
+        got, o2 = gpu_full_mesh(ctx, ph, off, rot, shape, dmap, i1, i2, tuning=tuning)
+        assert o2 == o1
+        np.testing.assert_array_equal(got, want)
+
+
 def test_empty_inputs(ctx, oracle_lib):
     _, km, mq = small_detector()
     shape = oracle_lib.big_mesh_shape(mq, 31)
