@@ -178,7 +178,6 @@ __device__ __forceinline__ unsigned long long d2u64(double x) { return __double2
 // (which only non-orthonormal rotations produce) take roundf.
 // ---------------------------------------------------------------------------
 constexpr float ROUND_MAGIC = 12582912.0f;  // 1.5 * 2^23
-constexpr int ROUND_MAGIC_BITS = 0x4B400000;
 
 __device__ __forceinline__ float round_away_f(float x)
 {
@@ -188,19 +187,6 @@ __device__ __forceinline__ float round_away_f(float x)
     if (fsub(a, r) == 0.5f) r = fadd(r, 1.0f);
     return copysignf(r, x);
 }
-
-// round_away_f(x) as int, for |x| < 2^22; larger magnitudes return a value far
-// outside every mesh (the caller's bounds check rejects it).
-__device__ __forceinline__ int round_away_i(float x)
-{
-    const float a = fabsf(x);
-    if (!(a < 4194304.0f)) return 1 << 30;
-    const float y = fadd(a, ROUND_MAGIC);
-    int r = __float_as_int(y) - ROUND_MAGIC_BITS;
-    if (fsub(a, fsub(y, ROUND_MAGIC)) == 0.5f) r += 1;
-    return x < 0.0f ? -r : r;
-}
-
 
 // ---------------------------------------------------------------------------
 // round half away from zero with two FP32 adds and an integer subtract, for
