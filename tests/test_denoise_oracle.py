@@ -64,3 +64,25 @@ def test_oracle_gradients_against_finite_differences():
         pm[i] -= h
         fd = (O.loss_and_grads(pp, x, t)[0] - O.loss_and_grads(pm, x, t)[0]) / (2 * h)
         assert abs(fd - g[i]) <= 1e-6 * max(1e-3, abs(g[i])) + 1e-9, (i, fd, g[i])
+
+
+def test_training_crystals_span_the_whole_distribution():
+    """denoise.random_crystal: lattice constant in [3, 6] A, 2-8 cells per axis,
+    1-4 emitters per cell, so 8 to 2048 emitters, centred; a smaller
+    max_emitters redraws the larger crystals."""
+    from incohautocorrelate_b200 import denoise as DN
+    rng = np.random.default_rng(5)
+    counts = []
+    for _ in range(3000):
+        pos, desc = DN.random_crystal(rng)
+        assert 3.0 <= desc["a"] <= 6.0
+        assert all(2 <= c <= 8 for c in desc["cells"]) and 1 <= desc["per_cell"] <= 4
+        n = int(np.prod(desc["cells"])) * desc["per_cell"]
+        assert pos.shape == (n, 3)
+        np.testing.assert_allclose(pos.mean(0), 0.0, atol=1e-9)
+        counts.append(n)
+    assert min(counts) >= 8 and max(counts) <= 2048
+    assert max(counts) > 1024  # the tail past the simulator's shared-memory stage is drawn
+    for _ in range(300):
+        pos, _ = DN.random_crystal(rng, max_emitters=256)
+        assert len(pos) <= 256
