@@ -274,6 +274,34 @@ iac_status iac_ac1d_sparse_batch(iac_ctx *ctx, const float *d_photons,
                                  float dqdx, int interp, double multiplicator, uint64_t *d_hist,
                                  void *stream);
 
+/* Route of a frame in iac_ac1d_uw_batch. */
+#define IAC_AC1D_ROUTE_REFERENCE (-1) /* per frame, as IAC/AC1D.cpp:251-253 decides */
+#define IAC_AC1D_ROUTE_HOST 0         /* the reference's CPU loop (IAC/AC1D.cpp:254-293) */
+#define IAC_AC1D_ROUTE_DEVICE 1       /* AutoCorr_sparseHL_AAV (IAC/AC1D.cpp:295-379) */
+
+/* Words (uint64) of the accumulator of iac_ac1d_uw_batch: VecSize + 2 * Size. */
+uint64_t iac_ac1d_uw_words(const iac_ac1d_shape *shape);
+
+/* Both routes of Calculate_AC_UW_Mapped (IAC/AC1D.cpp:201-391) for a batch of
+ * photon lists (layout as iac_sparse_ac_batch).  With route
+ * IAC_AC1D_ROUTE_REFERENCE each frame takes the route the reference picks:
+ * the CPU loop when (float)n / (float)detector_pixels < 0.0075f, which counts
+ * every unordered pair k >= j with a factor 2 in float (self pair included:
+ * 2 v^2 at bin 0) into Size bins, else the device kernel (every ordered pair,
+ * Multiplicator 100, bins modulo VecSize).  d_acc (uint64[iac_ac1d_uw_words],
+ * zeroed before the first batch, then accumulated) holds both routes' sums;
+ * iac_ac1d_uw_finish turns it into AC_UW.  For photon counts with nearest
+ * binning AC_UW equals the reference's bit for bit; linear binning sums
+ * fractional floats in double, equal to the reference's up to the order of
+ * the double additions.  VecSize + 2 Size <= 24576.  Asynchronous. */
+iac_status iac_ac1d_uw_batch(iac_ctx *ctx, const float *d_photons, const uint64_t *d_frame_offsets,
+                             uint32_t nframes, uint64_t detector_pixels, const iac_ac1d_shape *shape,
+                             int interp, int route, uint64_t *d_acc, void *stream);
+/* AC_UW (double[Size]) from the accumulator: device-route sums / 100 plus
+ * the host-route sums (IAC/AC1D.cpp:366-375 and :263-292).  Asynchronous. */
+iac_status iac_ac1d_uw_finish(iac_ctx *ctx, const uint64_t *d_acc, const iac_ac1d_shape *shape,
+                              double *d_ac_uw, void *stream);
+
 /* ---------------------------------------------------------------------- */
 /* (d) simulator                                                            */
 /* ---------------------------------------------------------------------- */

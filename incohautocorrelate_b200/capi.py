@@ -23,6 +23,11 @@ IAC_ERR_UNSUPPORTED = 6
 NEAREST = 0
 LINEAR = 1
 
+# AC1D sparse route (iac_ac1d_uw_batch)
+AC1D_ROUTE_REFERENCE = -1
+AC1D_ROUTE_HOST = 0
+AC1D_ROUTE_DEVICE = 1
+
 
 class IacError(RuntimeError):
     def __init__(self, status: int, message: str):
@@ -132,6 +137,9 @@ def _declare(lib):
     fn("iac_ac1d_cq", [_VP, _VP, _VP, _U64, C.POINTER(AC1DShape), C.c_int, D, _VP, _VP])
     fn("iac_ac1d_vecsize", [C.c_float, C.c_float], _U32)
     fn("iac_ac1d_sparse_batch", [_VP, _VP, _VP, _U32, C.c_float, C.c_float, C.c_int, D, _VP, _VP])
+    fn("iac_ac1d_uw_words", [C.POINTER(AC1DShape)], _U64)
+    fn("iac_ac1d_uw_batch", [_VP, _VP, _VP, _U32, _U64, C.POINTER(AC1DShape), C.c_int, C.c_int, _VP, _VP])
+    fn("iac_ac1d_uw_finish", [_VP, _VP, C.POINTER(AC1DShape), _VP, _VP])
     fn("iac_crystal_emitters", [_VP, _VP, _U32, _U32, _U32, C.POINTER(CrystalParams), _U64, _VP,
                                 _VP, _VP, _VP, _VP])
     fn("iac_simulate_intensity", [_VP, _VP, _U64, _VP, _VP, _U32, _U32, _U32,
@@ -232,6 +240,11 @@ def cq_merge_weights(h_rot9, h_mean_intensity, h_small_cq):
 
 def ac1d_vecsize(max_q: float, dqdx: float) -> int:
     return int(lib().iac_ac1d_vecsize(float(max_q), float(dqdx)))
+
+
+def ac1d_uw_words(shape: AC1DShape) -> int:
+    """uint64 words of the accumulator of Context.ac1d_uw_batch."""
+    return int(lib().iac_ac1d_uw_words(C.byref(shape)))
 
 
 def half_mesh_words(S: int) -> int:
@@ -365,6 +378,15 @@ class Context:
         check(lib().iac_ac1d_sparse_batch(self._h, _ptr(d_photons), _ptr(d_offsets), int(nframes),
                                           float(max_q), float(dqdx), int(interp), float(mult),
                                           _ptr(d_hist), _ptr(stream)))
+
+    def ac1d_uw_batch(self, d_photons, d_offsets, nframes, detector_pixels, shape, interp, d_acc,
+                      route=AC1D_ROUTE_REFERENCE, stream=None):
+        check(lib().iac_ac1d_uw_batch(self._h, _ptr(d_photons), _ptr(d_offsets), int(nframes),
+                                      int(detector_pixels), C.byref(shape), int(interp), int(route),
+                                      _ptr(d_acc), _ptr(stream)))
+
+    def ac1d_uw_finish(self, d_acc, shape, d_ac_uw, stream=None):
+        check(lib().iac_ac1d_uw_finish(self._h, _ptr(d_acc), C.byref(shape), _ptr(d_ac_uw), _ptr(stream)))
 
     def crystal_emitters(self, d_atoms, natoms, nframes, nmodes, cparams, seed, d_em, d_count,
                          d_rot_event, d_rot_crystal=None, stream=None):

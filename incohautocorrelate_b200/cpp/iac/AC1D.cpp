@@ -87,9 +87,10 @@ void AC1D::Calculate_AC_UW_MR(Settings &Options, Detector &RefDet, Settings::Int
     iac_ctx *ctx = Options.Context();
     void *s = Options.Stream();
     const size_t n = RefDet.Pixels();
-    const uint32_t vs = iac_ac1d_vecsize(Shape.Max_Q, Shape.dq_per_Step);
-    DevBuf dH(ctx, 8 * (size_t)vs);
-    Check(iac_memset_device(ctx, dH.p, 0, 8 * (size_t)vs, s), "clear histogram");
+    const iac_ac1d_shape sh{Shape.Size, Shape.Max_Q, Shape.dq_per_Step};
+    const uint64_t words = iac_ac1d_uw_words(&sh);
+    DevBuf dA(ctx, 8 * (size_t)words), dU(ctx, 8 * (size_t)Shape.Size);
+    Check(iac_memset_device(ctx, dA.p, 0, 8 * (size_t)words, s), "clear accumulator");
     Detector Det(RefDet, true);
     std::vector<float> photons;
     std::vector<uint64_t> off{0};
@@ -99,9 +100,10 @@ void AC1D::Calculate_AC_UW_MR(Settings &Options, Detector &RefDet, Settings::Int
         DevBuf dP(ctx, std::max<size_t>(photons.size(), 4) * 4), dO(ctx, 8 * off.size());
         Check(iac_memcpy_h2d(ctx, dP.p, photons.data(), photons.size() * 4, s), "copy photons");
         Check(iac_memcpy_h2d(ctx, dO.p, off.data(), 8 * off.size(), s), "copy offsets");
-        Check(iac_ac1d_sparse_batch(ctx, (const float *)dP.p, (const uint64_t *)dO.p, (uint32_t)nf, Shape.Max_Q,
-                                    Shape.dq_per_Step, Mode, 100.0, (uint64_t *)dH.p, s),
-              "iac_ac1d_sparse_batch");
+        // each frame takes the route the reference picks for it (IAC/AC1D.cpp:251-253)
+        Check(iac_ac1d_uw_batch(ctx, (const float *)dP.p, (const uint64_t *)dO.p, (uint32_t)nf, (uint64_t)n, &sh,
+                                Mode, IAC_AC1D_ROUTE_REFERENCE, (uint64_t *)dA.p, s),
+              "iac_ac1d_uw_batch");
         Check(iac_stream_synchronize(ctx, s), "synchronize");
         photons.clear();
         off.assign(1, 0);
@@ -115,12 +117,11 @@ void AC1D::Calculate_AC_UW_MR(Settings &Options, Detector &RefDet, Settings::Int
         if (off.size() - 1 >= Options.SparseBatchFrames) flush();
     }
     flush();
-    std::vector<uint64_t> h(vs);
-    Check(iac_memcpy_d2h(ctx, h.data(), dH.p, 8 * (size_t)vs, s), "copy histogram");
-    Check(iac_stream_synchronize(ctx, s), "synchronize");
+    Check(iac_ac1d_uw_finish(ctx, (const uint64_t *)dA.p, &sh, (double *)dU.p, s), "iac_ac1d_uw_finish");
     delete[] AC_UW;
     AC_UW = new double[Shape.Size]();
-    for (uint32_t j = 0; j < vs && j < Shape.Size; j++) AC_UW[j] = (double)h[j] / 100.0;
+    Check(iac_memcpy_d2h(ctx, AC_UW, dU.p, 8 * (size_t)Shape.Size, s), "copy AC_UW");
+    Check(iac_stream_synchronize(ctx, s), "synchronize");
 }
 
 void AC1D::CalcAC()

@@ -35,7 +35,8 @@ public:
     // C(|q|) of the detector's (mean) intensity, IAC/AC1D.cpp:61-195
     void Calculate_CQ(Detector &Det, Settings &Options, Settings::Interpolation IterpolMode);
     // unweighted AC(|q|) of events [Lower, Upper) read through Options.Frames,
-    // IAC/AC1D.cpp:393-469 (device route for every frame; Threads is ignored)
+    // IAC/AC1D.cpp:393-469; every frame takes the route the reference picks for
+    // it (IAC/AC1D.cpp:251-253), both routes run on the device; Threads is ignored
     void Calculate_AC_UW_MR(Settings &Options, Detector &RefDet, Settings::Interpolation IterpolMode,
                             std::array<float, 2> Photonisation, unsigned int LowerBoundary,
                             unsigned int UpperBoundary, unsigned int Threads = 200);

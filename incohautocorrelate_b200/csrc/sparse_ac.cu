@@ -477,15 +477,31 @@ __global__ void sparse_fold_kernel(const unsigned long long *__restrict__ half, 
 }
 
 // ---------------------------------------------------------------------------
-// AC1D of sparse photon lists: AutoCorr_sparseHL_AAV (IAC/kernel.cl:863-950)
-// summed over frames.  Every ordered pair of a frame, self pairs included,
-// adds (uint64)(v_a * v_b * Mult) at bin floor(|q|/dq + 0.5) (nearest) or
-// splits it over floor(|q|/dq) and the next bin (linear).  The two orders of
-// a distinct pair give the same |q| and value, so each distinct pair adds
-// twice its value.  Bins are taken modulo VecSize, which is what the
-// reference's sub-histogram layout and index-modulo fold (IAC/AC1D.cpp:366-375)
-// do to bins at or beyond VecSize.  The histogram lives in shared memory for
-// the whole launch.  Work queue and pair enumeration are the pair kernel's.
+// AC_UW of sparse photon lists: both routes of Calculate_AC_UW_Mapped
+// (IAC/AC1D.cpp:248-379).  The reference picks a route per frame: with fewer
+// than 0.75 % of the detector's pixels hit ((float)n / (float)pixels < 0.0075f,
+// :251-253) it loops on the host over k >= j (:254-293); otherwise it launches
+// AutoCorr_sparseHL_AAV (IAC/kernel.cl:863-950, host side :295-379).
+//
+// Device route: every ordered pair of a frame, self pairs included, adds
+// (uint64)(v_a * v_b * Mult) at bin floor(|q|/dq + 0.5) (nearest) or splits
+// it over floor(|q|/dq) and the next bin (linear).  The two orders of a
+// distinct pair give the same |q| and value, so each distinct pair adds twice
+// its value.  Bins are taken modulo VecSize, which is what the reference's
+// sub-histogram layout and index-modulo fold (IAC/AC1D.cpp:366-375) do to bins
+// at or beyond VecSize.
+//
+// Host route: every unordered pair k >= j adds the float 2*(v_j*v_k)
+// (nearest), or 2*((v_j*v_k)*(1-Sep)) and 2*((v_j*v_k)*Sep) (linear), to a
+// double histogram of Size bins; the factor 2 also doubles the self pair.
+// These floats are whole numbers for photon counts (nearest): those are summed
+// in uint64, exactly, so the double totals equal the reference's sequential
+// double sums bit for bit.  Any other value is summed with double atomics,
+// whose order differs from the reference's loop by rounding only.
+//
+// The histograms live in shared memory for the whole launch; the work queue
+// and the pair enumeration are the pair kernel's.  A tile belongs to one
+// frame, so the route branch is uniform across the CTA.
 // ---------------------------------------------------------------------------
 // b % n without the division when b < n (bins past the histogram are rare)
 __device__ __forceinline__ uint32_t wrap_bin(uint32_t b, uint32_t n)
@@ -494,17 +510,45 @@ __device__ __forceinline__ uint32_t wrap_bin(uint32_t b, uint32_t n)
     return b;
 }
 
+struct AC1DArgs {
+    float maxq, dqdx;
+    uint32_t vecsize;   // device-route bins (VecSize)
+    uint32_t size;      // host-route bins (Shape.Size; 0 when no frame takes the host route)
+    float det_pixels;   // (float) detector pixel count, for the route choice
+    int route;          // -1: the reference's choice per frame, 0: host route, 1: device route
+    unsigned long long *dev_out;  // vecsize words
+    unsigned long long *int_out;  // size words: host-route whole-number values
+    double *frac_out;             // size doubles: host-route other values
+};
+
+// host-route value v (>= 0) into bin b
+__device__ __forceinline__ void host_route_add(const SparseArgs &a, const AC1DArgs &b, unsigned long long *hint,
+                                               double *hfrac, uint32_t bin, float v)
+{
+    if (bin >= b.size) {  // only for inconsistent MaxQ / dq; the reference writes out of bounds
+        atomicAdd(&a.counters->out_of_mesh, 1ull);
+        return;
+    }
+    if (v == 0.0f) return;
+    if (v == truncf(v) && v < 1.8e19f)
+        atomicAdd(&hint[bin], (unsigned long long)__float2ull_rz(v));
+    else
+        atomicAdd(&hfrac[bin], (double)v);
+}
+
 template <int INTERP>
-__global__ void __launch_bounds__(256) ac1d_sparse_kernel(const SparseArgs a, float maxq, float dqdx,
-                                                          uint32_t vecsize,
-                                                          unsigned long long *__restrict__ out)
+__global__ void __launch_bounds__(256) ac1d_sparse_kernel(const SparseArgs a, const AC1DArgs b)
 {
     extern __shared__ unsigned long long hist[];
+    unsigned long long *hdev = hist, *hint = hist + b.vecsize;
+    double *hfrac = reinterpret_cast<double *>(hist + b.vecsize + b.size);
     __shared__ unsigned long long s_tile;
     __shared__ uint32_t s_frame;
-    for (uint32_t i = threadIdx.x; i < vecsize; i += blockDim.x) hist[i] = 0;
+    const uint32_t words = b.vecsize + 2 * b.size;
+    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) hist[i] = 0;  // 0 bits = +0.0
     const unsigned long long ntiles = a.tile_off[a.nframes];
     const uint32_t nthr = blockDim.x;
+    const float maxq = b.maxq, dqdx = b.dqdx;
     for (;;) {
         if (threadIdx.x == 0) {
             const unsigned long long t = atomicAdd(a.queue, 1ull);
@@ -526,11 +570,19 @@ __global__ void __launch_bounds__(256) ac1d_sparse_kernel(const SparseArgs a, fl
         const uint32_t n = (uint32_t)(a.offsets[f + 1] - base);
         const unsigned long long chunk = t - a.tile_off[f];
         const float4 *__restrict__ P = a.photons + base;
+        // SHLsizeQuot < 0.0075f (IAC/AC1D.cpp:251-253), in the reference's float arithmetic
+        const bool host =
+            b.route == 0 || (b.route < 0 && __fdiv_rn(__uint2float_rn(n), b.det_pixels) < 0.0075f);
         if (chunk == 0)  // self pairs: q = 0, bin 0 (linear: bin 0 gets all of it, bin 1 nothing)
             for (uint32_t i = threadIdx.x; i < n; i += nthr) {
-                const double v = (double)P[i].w;
-                const unsigned long long w = d2u64(dmul(dmul(v, v), a.mult));
-                if (w) atomicAdd(&hist[0], w);
+                const float w = P[i].w;
+                if (host) {
+                    host_route_add(a, b, hint, hfrac, 0, fmul(2.0f, fmul(w, w)));
+                } else {
+                    const double v = (double)w;
+                    const unsigned long long u = d2u64(dmul(dmul(v, v), a.mult));
+                    if (u) atomicAdd(&hdev[0], u);
+                }
             }
         const unsigned long long npairs = (unsigned long long)n * (n - 1) / 2;
         const unsigned long long p0 = chunk * a.tile_pairs;
@@ -548,18 +600,31 @@ __global__ void __launch_bounds__(256) ac1d_sparse_kernel(const SparseArgs a, fl
                 float q = __fsqrt_rn(fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz)));
                 if (!(q > maxq)) {
                     q = __fdiv_rn(q, dqdx);
-                    const double val = dmul((double)A.w, (double)B.w);
-                    if (INTERP == 0) {
-                        const uint32_t sc = wrap_bin((uint32_t)floor(dadd((double)q, 0.5)), vecsize);
-                        const unsigned long long w = d2u64(dmul(val, a.mult));
-                        if (w) atomicAdd(&hist[sc], 2ull * w);
+                    if (host) {
+                        const float pv = fmul(A.w, B.w);
+                        if (INTERP == 0) {
+                            host_route_add(a, b, hint, hfrac, (uint32_t)floor(dadd((double)q, 0.5)),
+                                           fmul(2.0f, pv));
+                        } else {
+                            const float fq = floorf(q);
+                            const float sep = fsub(q, fq);
+                            host_route_add(a, b, hint, hfrac, (uint32_t)fq, fmul(2.0f, fmul(pv, fsub(1.0f, sep))));
+                            host_route_add(a, b, hint, hfrac, (uint32_t)fq + 1, fmul(2.0f, fmul(pv, sep)));
+                        }
                     } else {
-                        const float fq = floorf(q);
-                        const double sep = (double)fsub(q, fq);
-                        const unsigned long long w1 = d2u64(dmul(dmul(val, dsub(1.0, sep)), a.mult));
-                        const unsigned long long w2 = d2u64(dmul(dmul(val, sep), a.mult));
-                        if (w1) atomicAdd(&hist[wrap_bin((uint32_t)fq, vecsize)], 2ull * w1);
-                        if (w2) atomicAdd(&hist[wrap_bin((uint32_t)fq + 1, vecsize)], 2ull * w2);
+                        const double val = dmul((double)A.w, (double)B.w);
+                        if (INTERP == 0) {
+                            const uint32_t sc = wrap_bin((uint32_t)floor(dadd((double)q, 0.5)), b.vecsize);
+                            const unsigned long long w = d2u64(dmul(val, a.mult));
+                            if (w) atomicAdd(&hdev[sc], 2ull * w);
+                        } else {
+                            const float fq = floorf(q);
+                            const double sep = (double)fsub(q, fq);
+                            const unsigned long long w1 = d2u64(dmul(dmul(val, dsub(1.0, sep)), a.mult));
+                            const unsigned long long w2 = d2u64(dmul(dmul(val, sep), a.mult));
+                            if (w1) atomicAdd(&hdev[wrap_bin((uint32_t)fq, b.vecsize)], 2ull * w1);
+                            if (w2) atomicAdd(&hdev[wrap_bin((uint32_t)fq + 1, b.vecsize)], 2ull * w2);
+                        }
                     }
                 }
                 i += dr;
@@ -573,8 +638,24 @@ __global__ void __launch_bounds__(256) ac1d_sparse_kernel(const SparseArgs a, fl
         __syncthreads();
     }
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < vecsize; i += blockDim.x)
-        if (hist[i]) atomicAdd(&out[i], hist[i]);
+    for (uint32_t i = threadIdx.x; i < b.vecsize; i += blockDim.x)
+        if (hdev[i]) atomicAdd(&b.dev_out[i], hdev[i]);
+    for (uint32_t i = threadIdx.x; i < b.size; i += blockDim.x) {
+        if (hint[i]) atomicAdd(&b.int_out[i], hint[i]);
+        if (hfrac[i] != 0.0) atomicAdd(&b.frac_out[i], hfrac[i]);
+    }
+}
+
+// AC_UW[j] = dev[j] / Mult (j < VecSize) + int[j] + frac[j]
+__global__ void ac1d_uw_finish_kernel(const unsigned long long *__restrict__ dev,
+                                      const unsigned long long *__restrict__ in, const double *__restrict__ fr,
+                                      uint32_t vecsize, uint32_t size, double mult, double *__restrict__ ac)
+{
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= size) return;
+    double v = j < vecsize ? __ddiv_rn((double)dev[j], mult) : 0.0;
+    v = dadd(v, (double)in[j]);
+    ac[j] = dadd(v, fr[j]);
 }
 
 typedef void (*PairKernel)(SparseArgs);
@@ -728,6 +809,42 @@ static iac_status launch_pair_batch(iac_ctx *ctx, const float *d_photons, const 
     return IAC_OK;
 }
 
+// Planner and AC1D kernel of one batch (shared memory: both routes' histograms).
+static iac_status launch_ac1d_batch(iac_ctx *ctx, const float *d_photons, const uint64_t *d_off,
+                                    uint32_t nframes, int interp, double mult, const AC1DArgs &b, void *stream)
+{
+    DeviceGuard g(ctx->device);
+    const iac_sparse_tuning tun = effective_tuning(ctx, 0);
+    void *scratch = nullptr;
+    const size_t table_bytes = ((sizeof(unsigned long long) * ((size_t)nframes + 1) + 127) / 128) * 128;
+    iac_status st = stream_scratch(ctx, stream, SLOT_TILES, table_bytes + 128 + nframes, &scratch);
+    if (st != IAC_OK) return st;
+    unsigned long long *tile_off = (unsigned long long *)scratch;
+    unsigned long long *queue = (unsigned long long *)((char *)scratch + table_bytes);
+    cudaStream_t s = as_stream(stream);
+    sparse_plan_kernel<<<1, PLAN_THREADS, 0, s>>>(d_off, nframes, tun.tile_pairs, tile_off, queue);
+    IAC_LAUNCHED(ctx);
+    IAC_CUDA(cudaGetLastError());
+    SparseArgs a{};
+    a.photons = reinterpret_cast<const float4 *>(d_photons);
+    a.offsets = d_off;
+    a.tile_off = tile_off;
+    a.queue = queue;
+    a.counters = ctx->d_counters;
+    a.nframes = nframes;
+    a.tile_pairs = tun.tile_pairs;
+    a.mult = mult;
+    const size_t smem = sizeof(unsigned long long) * ((size_t)b.vecsize + 2 * (size_t)b.size);
+    auto k = interp == 0 ? ac1d_sparse_kernel<0> : ac1d_sparse_kernel<1>;
+    IAC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // as many persistent CTAs as fit: four per SM, fewer when the histograms are large
+    const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(4, (200u << 10) / std::max<size_t>(smem, 1)));
+    k<<<ctx->sm_count * per_sm, 256, smem, s>>>(a, b);
+    IAC_LAUNCHED(ctx);
+    IAC_CUDA(cudaGetLastError());
+    return IAC_OK;
+}
+
 }  // namespace iac
 
 using namespace iac;
@@ -790,31 +907,71 @@ iac_status iac_ac1d_sparse_batch(iac_ctx *ctx, const float *d_photons, const uin
     IAC_REQUIRE(vecsize >= 1 && vecsize <= 24576, "VecSize %u out of range [1, 24576]", vecsize);
     if (nframes == 0) return IAC_OK;
     IAC_REQUIRE(d_photons && d_off && d_hist, "iac_ac1d_sparse_batch: NULL pointer");
+    IAC_REQUIRE((reinterpret_cast<uintptr_t>(d_photons) & 15) == 0,
+                "photon array must be 16-byte aligned (float4 per photon)");
+    AC1DArgs b{};
+    b.maxq = max_q;
+    b.dqdx = dqdx;
+    b.vecsize = vecsize;
+    b.size = 0;
+    b.det_pixels = 1.0f;
+    b.route = 1;
+    b.dev_out = (unsigned long long *)d_hist;
+    return launch_ac1d_batch(ctx, d_photons, d_off, nframes, interp, mult, b, stream);
+}
+
+uint64_t iac_ac1d_uw_words(const iac_ac1d_shape *sh)
+{
+    if (!sh || !(sh->dq_per_step > 0) || !(sh->max_q > 0)) return 0;
+    return (uint64_t)iac_ac1d_vecsize(sh->max_q, sh->dq_per_step) + 2ull * sh->size;
+}
+
+iac_status iac_ac1d_uw_batch(iac_ctx *ctx, const float *d_photons, const uint64_t *d_off, uint32_t nframes,
+                             uint64_t detector_pixels, const iac_ac1d_shape *sh, int interp, int route,
+                             uint64_t *d_acc, void *stream)
+{
+    IAC_TRACE();
+    IAC_REQUIRE(ctx != nullptr && sh != nullptr, "iac_ac1d_uw_batch: NULL argument");
+    IAC_REQUIRE(interp == 0 || interp == 1, "interpolation must be 0 or 1");
+    IAC_REQUIRE(route >= -1 && route <= 1, "route must be -1 (per frame), 0 (host) or 1 (device)");
+    IAC_REQUIRE(sh->dq_per_step > 0 && sh->max_q > 0, "iac_ac1d_uw_batch: MaxQ and dq must be positive");
+    IAC_REQUIRE(detector_pixels > 0 && detector_pixels < (1ull << 32),
+                "iac_ac1d_uw_batch: detector pixel count %llu out of range", (unsigned long long)detector_pixels);
+    const uint32_t vecsize = iac_ac1d_vecsize(sh->max_q, sh->dq_per_step);
+    IAC_REQUIRE(sh->size >= 3 && vecsize >= 1, "AC1D size %u too small", sh->size);
+    IAC_REQUIRE((uint64_t)vecsize + 2ull * sh->size <= 24576,
+                "AC1D size %u too large: VecSize + 2 Size must be at most 24576 (shared-memory histograms)",
+                sh->size);
+    if (nframes == 0) return IAC_OK;
+    IAC_REQUIRE(d_photons && d_off && d_acc, "iac_ac1d_uw_batch: NULL pointer");
+    IAC_REQUIRE((reinterpret_cast<uintptr_t>(d_photons) & 15) == 0,
+                "photon array must be 16-byte aligned (float4 per photon)");
+    IAC_REQUIRE((reinterpret_cast<uintptr_t>(d_acc) & 7) == 0, "accumulator must be 8-byte aligned");
+    AC1DArgs b{};
+    b.maxq = sh->max_q;
+    b.dqdx = sh->dq_per_step;
+    b.vecsize = vecsize;
+    b.size = sh->size;
+    b.det_pixels = (float)detector_pixels;
+    b.route = route;
+    b.dev_out = (unsigned long long *)d_acc;
+    b.int_out = b.dev_out + vecsize;
+    b.frac_out = reinterpret_cast<double *>(b.int_out + sh->size);
+    return launch_ac1d_batch(ctx, d_photons, d_off, nframes, interp, 100.0, b, stream);
+}
+
+iac_status iac_ac1d_uw_finish(iac_ctx *ctx, const uint64_t *d_acc, const iac_ac1d_shape *sh, double *d_ac_uw,
+                              void *stream)
+{
+    IAC_TRACE();
+    IAC_REQUIRE(ctx && sh && d_acc && d_ac_uw, "iac_ac1d_uw_finish: NULL argument");
+    IAC_REQUIRE(sh->dq_per_step > 0 && sh->max_q > 0 && sh->size >= 3, "iac_ac1d_uw_finish: bad shape");
+    const uint32_t vecsize = iac_ac1d_vecsize(sh->max_q, sh->dq_per_step);
     DeviceGuard g(ctx->device);
-    const iac_sparse_tuning tun = effective_tuning(ctx, 0);
-    void *scratch = nullptr;
-    const size_t table_bytes = ((sizeof(unsigned long long) * ((size_t)nframes + 1) + 127) / 128) * 128;
-    iac_status st = stream_scratch(ctx, stream, SLOT_TILES, table_bytes + 128 + nframes, &scratch);
-    if (st != IAC_OK) return st;
-    unsigned long long *tile_off = (unsigned long long *)scratch;
-    unsigned long long *queue = (unsigned long long *)((char *)scratch + table_bytes);
-    cudaStream_t s = as_stream(stream);
-    sparse_plan_kernel<<<1, PLAN_THREADS, 0, s>>>(d_off, nframes, tun.tile_pairs, tile_off, queue);
-    IAC_LAUNCHED(ctx);
-    IAC_CUDA(cudaGetLastError());
-    SparseArgs a{};
-    a.photons = reinterpret_cast<const float4 *>(d_photons);
-    a.offsets = d_off;
-    a.tile_off = tile_off;
-    a.queue = queue;
-    a.counters = ctx->d_counters;
-    a.nframes = nframes;
-    a.tile_pairs = tun.tile_pairs;
-    a.mult = mult;
-    const size_t smem = sizeof(unsigned long long) * vecsize;
-    auto k = interp == 0 ? ac1d_sparse_kernel<0> : ac1d_sparse_kernel<1>;
-    IAC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<ctx->sm_count * 4, 256, smem, s>>>(a, max_q, dqdx, vecsize, (unsigned long long *)d_hist);
+    const unsigned long long *dev = (const unsigned long long *)d_acc;
+    ac1d_uw_finish_kernel<<<(sh->size + 255) / 256, 256, 0, as_stream(stream)>>>(
+        dev, dev + vecsize, reinterpret_cast<const double *>(dev + vecsize + sh->size), vecsize, sh->size, 100.0,
+        d_ac_uw);
     IAC_LAUNCHED(ctx);
     IAC_CUDA(cudaGetLastError());
     return IAC_OK;

@@ -74,6 +74,7 @@ def _decl(lib):
     fn("iaco_ac1d_vecsize", [F, F], U32)
     fn("iaco_ac1d_sparse_frame", [VP, U32, F, F, C.c_int, D, VP])
     fn("iaco_ac1d_sparse_frame_cpu_route", [VP, U32, F, F, C.c_int, VP])
+    fn("iaco_ac1d_uw_frames", [VP, VP, U32, U64, F, F, U32, C.c_int, C.c_int, VP])
     fn("iaco_simulate_crystal", [VP, U64, VP, U32, VP, C.c_int, VP])
     fn("iaco_simulate_crystal_f64", [VP, U64, VP, U32, VP, C.c_int, VP])
     fn("iaco_philox4x32_10", [P(U32), P(U32), P(U32)])

@@ -896,6 +896,35 @@ void iaco_ac1d_sparse_frame_cpu_route(const float *HL, uint32_t n, float max_q, 
         }
 }
 
+/* Calculate_AC_UW_Mapped over a list of frames, IAC/AC1D.cpp:201-391: per
+ * frame the route the reference picks (route < 0: the CPU loop when
+ * (float)n / (float)det_pixels < 0.0075f, :251-253; route 0: always the CPU
+ * loop; route 1: always the device kernel), each adding into the double AC_M
+ * of `size` bins in frame order.  The device route adds its integer totals /
+ * 100 (:364-375; the reference adds each of its 10000 sub-histograms' words /
+ * 100 in turn, the same doubles whenever the words are multiples of 100, as
+ * they are for photon counts with nearest binning). */
+void iaco_ac1d_uw_frames(const float *HL, const uint64_t *off, uint32_t nframes, uint64_t det_pixels,
+                         float max_q, float dqdx, uint32_t size, int interp, int route, double *ac)
+{
+    const uint32_t vs = iaco_ac1d_vecsize(max_q, dqdx);
+    uint64_t *tmp = (uint64_t *)malloc(sizeof(uint64_t) * vs);
+    for (uint32_t f = 0; f < nframes; f++) {
+        const uint32_t n = (uint32_t)(off[f + 1] - off[f]);
+        const float *hl = HL + 4 * off[f];
+        const float quot = (float)n / (float)det_pixels;
+        const int cpu = route < 0 ? (quot < 0.0075f) : (route == 0);
+        if (cpu) {
+            iaco_ac1d_sparse_frame_cpu_route(hl, n, max_q, dqdx, interp, ac);
+        } else {
+            memset(tmp, 0, sizeof(uint64_t) * vs);
+            iaco_ac1d_sparse_frame(hl, n, max_q, dqdx, interp, 100.0, tmp);
+            for (uint32_t j = 0; j < vs && j < size; j++) ac[j] += (double)tmp[j] / 100.0;
+        }
+    }
+    free(tmp);
+}
+
 /* ===================================================================== */
 /* (d) simulator                                                         */
 /* ===================================================================== */

@@ -108,6 +108,12 @@ void iaco_ac1d_sparse_frame(const float *hl4, uint32_t n, float max_q, float dqd
 void iaco_ac1d_sparse_frame_cpu_route(const float *hl4, uint32_t n, float max_q, float dqdx,
                                       int interp, double *ac);
 
+/* Both routes of Calculate_AC_UW_Mapped over frames (route -1: the
+ * reference's per-frame choice, 0: CPU loop, 1: device kernel). */
+void iaco_ac1d_uw_frames(const float *hl4, const uint64_t *frame_offsets, uint32_t nframes,
+                         uint64_t det_pixels, float max_q, float dqdx, uint32_t size, int interp,
+                         int route, double *ac);
+
 /* ---- (d) simulator --------------------------------------------------- */
 void iaco_simulate_crystal(const float *pixel_map, uint64_t npix, const float *em4, uint32_t nem,
                            const double params[10], int intensity_mode, float *out);

@@ -54,16 +54,17 @@ def _eval_xml(path, d, mesh, angular, step=1.0):
 <Misc><EchoLevel>0</EchoLevel></Misc></EvalSettings></root>""")
 
 
-def _dataset(d, nframes=150, seed=4):
-    """40x56 coarse flat detector, 5 % masked, frames of Poisson(0.08) photon
-    counts scaled to ADU, random orientations; written as the raw files the
-    driver reads."""
+def _dataset(d, nframes=150, seed=4, rates=(0.08,)):
+    """40x56 coarse flat detector, 5 % masked, frames of Poisson photon counts
+    (mean rates[f % len(rates)] per pixel) scaled to ADU, random
+    orientations; written as the raw files the driver reads."""
     from incohautocorrelate_b200 import workloads as W
     rng = np.random.default_rng(seed)
     ny, nx = 40, 56
     pm = W.flat_pixel_map(ny, nx, pitch=5e-4, dist=0.1)
     mask = W.random_mask(ny * nx, 0.05, seed)
-    frames = (rng.poisson(0.08, (nframes, ny * nx)) * 1.0).astype(np.float32)
+    lam = np.array([rates[f % len(rates)] for f in range(nframes)])[:, None]
+    frames = (rng.poisson(lam, (nframes, ny * nx)) * 1.0).astype(np.float32)
     rots = W.haar_rotations(nframes, seed + 1)
     rots = np.array([[float("%f" % v) for v in R] for R in rots], np.float32)  # as written to XML
     pm.tofile(f"{d}/pm.raw")
@@ -146,9 +147,13 @@ def test_iac_run_3d_evaluation_matches_oracle(tmp_path, oracle_lib):
 
 @pytest.mark.gpu
 def test_iac_run_angular_averaged_evaluation_matches_oracle(tmp_path, oracle_lib):
+    """Frames alternate between ~8 % and ~0.4 % hit pixels, so AC1D's sparse
+    AC_UW takes both of the reference's routes (host loop below 0.75 %,
+    IAC/AC1D.cpp:251-253); linear binning sums fractional floats, equal up to
+    the order of the double additions."""
     o = oracle_lib
     d = str(tmp_path)
-    pm, mask, frames, rots = _dataset(d, nframes=80, seed=9)
+    pm, mask, frames, rots = _dataset(d, nframes=80, seed=9, rates=(0.08, 0.004))
     _eval_xml(f"{d}/eval.xml", d, 101, True)
     r = subprocess.run([RUN, "-e", f"{d}/eval.xml"], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
@@ -161,16 +166,19 @@ def test_iac_run_angular_averaged_evaluation_matches_oracle(tmp_path, oracle_lib
     o.lib().iaco_ac1d_cq(o.p(I), o.p(km), npix, sh, 1, mult, 0, npix, o.p(h))
     np.testing.assert_allclose(np.fromfile(f"{d}/cq.bin", np.float64), h.astype(np.float64) / mult,
                                rtol=1e-12, atol=0)
-    vs = o.lib().iaco_ac1d_vecsize(sh.max_q, sh.dq_per_step)
-    acuw = np.zeros(sh.size)
+    hl, off = [], [0]
     for f in range(len(frames)):
         t = (frames[f] * mask.astype(np.float32)).astype(np.float32)
         out = np.zeros((npix, 4), np.float32)
         n = o.lib().iaco_sparse_hitlist(o.p(t), o.p(km), npix, 0.0, 1.0, 1, o.p(out))
-        hh = np.zeros(vs, np.uint64)
-        o.lib().iaco_ac1d_sparse_frame(o.p(np.ascontiguousarray(out[:n])), n, sh.max_q, sh.dq_per_step, 1,
-                                       100.0, o.p(hh))
-        acuw[:vs] += hh.astype(np.float64) / 100.0
+        hl.append(out[:n])
+        off.append(off[-1] + n)
+    off = np.array(off, np.uint64)
+    host = (np.diff(off).astype(np.float32) / np.float32(npix)) < np.float32(0.0075)
+    assert host.any() and not host.all()
+    acuw = np.zeros(sh.size)
+    o.lib().iaco_ac1d_uw_frames(o.p(np.ascontiguousarray(np.concatenate(hl))), o.p(off), len(frames), npix,
+                                sh.max_q, sh.dq_per_step, sh.size, 1, -1, o.p(acuw))
     np.testing.assert_allclose(np.fromfile(f"{d}/acuw.bin", np.float64), acuw, rtol=1e-12, atol=0)
 
 
