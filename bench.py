@@ -1,21 +1,30 @@
 #!/usr/bin/env python
-"""Benchmark of the batched rotated photon-pair correlator.
+"""Benchmark of the batched rotated photon-pair correlator and the rest of
+the pair-correlation path.
 
-Workload (the configuration the headline metric is quoted on): 1024x512
-two-panel detector, 5 % masked, 100 000 frames whose photon counts are
-Poisson(lambda_f) with lambda_f log-normal (median 80, sigma 0.8), uniform SO(3)
-orientation per frame, 201^3 uint64 mesh (MeshSize 199), nearest/nearest with
-double mapping, Multiplicator 1000.  Seeded synthetic data of that shape.
+Workload of the headline metric: 1024x512 two-panel detector, 5 % masked,
+100 000 frames whose photon counts are Poisson(lambda_f) with lambda_f
+log-normal (median 80, sigma 0.8), uniform SO(3) orientation per frame, 201^3
+uint64 mesh (MeshSize 199), nearest/nearest with double mapping,
+Multiplicator 1000.  Seeded synthetic data of that shape.
 
 One step = the whole batch through the hot path: clear the half mesh, plan the
 work queue, bin every photon pair (persistent kernel), fold into the full mesh.
 `value` times steps with inputs resident in HBM; `e2e` times the C-ABI host
-entry point (pinned host photon lists in, full mesh out) per step.
+entry point with pinned host photon lists, the batches of a run accumulating
+into a device-resident mesh that is folded and read back once at the end of
+the run.  On one GPU the line also carries `parts`: one timed step of each
+other part of the path on its configuration (dense C(q) and AC1D C(q) on
+1024^2, the C(q) merge, AC1D of sparse frames with the reference's route
+choice, the simulator feeding the correlator, the denoiser's training step and
+a frames-to-error check of the committed denoiser weights).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--scaling weak|strong] [--no-parts] [--kernel PART]
 
-Under torchrun (N > 1) every rank bins its own 100 000 frames (weak scaling)
-and the per-rank meshes are summed on rank 0 with one NCCL reduce per step.
+Under torchrun (N > 1) every rank bins its own 100 000 frames (--scaling weak)
+or a pair-balanced share of one 100 000-frame batch (--scaling strong), and
+the per-rank meshes are summed on rank 0 with one NCCL reduce per step.
 """
 from __future__ import annotations
 
@@ -46,20 +55,27 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--frames", type=int, default=100_000)
+    ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
+                    help="multi-GPU runs: weak = 100 000 frames per rank, strong = one 100 000-frame "
+                         "batch shared by the ranks")
     ap.add_argument("--cpu-frames", type=int, default=1500,
                     help="frames per step of the --impl reference arm")
     ap.add_argument("--cpu-baseline-frames", type=int, default=100_000,
                     help="frames of the cpu_baseline sample (all 100 000: about 8 s on 16 host threads)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parts", action="store_true",
+                    help="headline only: skip the timed step of every other part of the path")
+    ap.add_argument("--f2e-crystals", type=int, default=4,
+                    help="held-out crystals of the frames-to-error part")
     ap.add_argument("--det", type=int, default=1024,
                     help="edge of the square detector of the dense kernels (1024 = their config)")
     ap.add_argument("--backend", type=int, default=0,
                     help="denoiser convolutions: 0 = tcgen05 + TMEM, 1 = mma.sync")
     ap.add_argument("--kernel", default="sparse",
-                    choices=["sparse", "cq_small", "ac1d_cq", "cq_merge", "ac1d_sparse", "simulate",
-                             "denoise", "average"],
-                    help="sparse is the headline; the others measure the remaining kernels "
-                         "of the path on their configurations")
+                    choices=["sparse", "cq_small", "ac1d_cq", "cq_merge", "ac1d_sparse", "ac1d_uw", "simulate",
+                             "denoise", "frames_to_error", "average"],
+                    help="sparse is the headline; the others print one line for that part of the path "
+                         "on its configuration")
     return ap.parse_args()
 
 
@@ -298,14 +314,28 @@ def measured_bf16_tflops():
     return 1400.0, "fallback (1.4 PFLOP/s sustained)"
 
 
-def committed_traffic():
-    """dram bytes per launch of the pair kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "sparse_pairs_rotated.json")
-    if os.path.exists(p):
-        with open(p) as fh:
-            d = json.load(fh)
-        return d.get("dram_bytes_per_full_launch")
-    return None
+def pair_box_radius(C, ctas_per_sm):
+    """Half-width of the pair kernel's shared-memory box around q = 0 for a
+    tuning row (the library's rule: 10, shrunk until ctas_per_sm boxes of
+    (R + 1)(2R + 1)^2 words fit in 200 KB, at most the mesh centre)."""
+    budget = (200 << 10) // max(1, ctas_per_sm)
+    r = min(10, C)
+    while r > 0 and 8 * (r + 1) * (2 * r + 1) ** 2 > budget:
+        r -= 1
+    return r
+
+
+def box_value_share(half, S, R, self_sum):
+    """Share of the distinct pairs' mesh value that lands in the box of
+    half-width R around q = 0 (ss <= R, |fs - C| <= R, |ms - C| <= R); the
+    self pairs (all at the centre) are left out.  With photon counts mostly 1
+    this is close to the share of the pair kernel's updates the box takes."""
+    import torch
+    C = (S - 1) // 2
+    h = half.view(-1)[: S * S * ((S + 1) // 2)].view((S + 1) // 2, S, S)
+    tot = float(h.double().sum().item()) - self_sum
+    box = float(h[: R + 1, C - R: C + R + 1, C - R: C + R + 1].double().sum().item()) - self_sum
+    return box / tot if tot > 0 else 0.0
 
 
 def run_ours(args):
@@ -317,16 +347,19 @@ def run_ours(args):
     import torch.distributed as dist
 
     from incohautocorrelate_b200 import capi, shard
-    from incohautocorrelate_b200 import workloads as W
 
-    cfg = W.rotated_config(nframes=args.frames, seed=2 + 7919 * rank)
-    ph_h, off_h, rot_h = cfg["photons"], cfg["offsets"], cfg["rot"]
+    ph_h, off_h, rot_h, cfg = shard.rank_workload(rank, world, args.scaling, args.frames, seed=2)
     nframes = len(off_h) - 1
     pairs = _pairs(off_h)
     ctx = capi.Context(dev)
     shape = capi.big_mesh_shape(cfg["max_q"], cfg["mesh_size"])
     S = shape.size_ab
     params = capi.sparse_params(shape, capi.NEAREST, capi.NEAREST, True, 1000.0)
+    total_pairs = pairs
+    if distributed:
+        t = torch.tensor([pairs], dtype=torch.int64, device="cuda")
+        dist.all_reduce(t)
+        total_pairs = int(t.item())
 
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
@@ -337,18 +370,8 @@ def run_ours(args):
     full = torch.zeros(capi.full_mesh_words(S), dtype=torch.int64, device="cuda")
 
     # -- the L2 atomic rate the pair kernel is bound by (same footprint) ------
-    def scatter_rate(bits):
-        scratch = torch.zeros(capi.half_mesh_words(S), dtype=torch.int64, device="cuda")
-        upd = 1 << 30
-        ctx.bench_scatter_add(scratch, scratch.numel(), bits, upd // 8, 1, sptr)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        ctx.bench_scatter_add(scratch, scratch.numel(), bits, upd, 2, sptr)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        return upd / (e0.elapsed_time(e1) * 1e-3)
-    atomic_peak = scatter_rate(64)
-    atomic_peak_u32 = scatter_rate(32)
+    atomic_peak = scatter_rate(ctx, stream, capi.half_mesh_words(S), 64)
+    atomic_peak_u32 = scatter_rate(ctx, stream, capi.half_mesh_words(S), 32)
 
     ev = []
 
@@ -394,7 +417,6 @@ def run_ours(args):
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    total_pairs = pairs * world
     value = total_pairs * args.steps / (ms * 1e-3)
 
     # -- the same step captured once in a CUDA graph and replayed (1 GPU) --
@@ -426,75 +448,114 @@ def run_ours(args):
         graph_ms = g0.elapsed_time(g1) / args.steps
         del graph
 
-    # -- end to end through the C-ABI host entry point (pinned host buffers) --
+    # -- roofline of the pair kernel: L2 64-bit atomic updates ---------------
+    # one update per distinct pair (two on the ss = 0 plane, one per frame for
+    # its summed self pairs); the denominator is the scattered-atomic rate
+    # measured above on a buffer of the half mesh's size.  The voxels within R
+    # of q = 0 go to each CTA's shared-memory box instead of L2.
+    step()
+    torch.cuda.synchronize()
+    updates = pairs - int(len(ph_h))
+    upd_rate = updates / (ms_kernel * 1e-3)
+    tun = ctx.sparse_tuning(S)
+    R = pair_box_radius((S - 1) // 2, tun["ctas_per_sm"])
+    self_sum = 1000.0 * float((ph_h[:, 3].astype(np.float64) ** 2).sum())
+    share = box_value_share(half, S, R, self_sum) if R > 0 else 0.0
+
+    # -- end to end: pinned host photon lists -> device-resident mesh --------
     ph_p = torch.from_numpy(ph_h).pin_memory()
     off_p = torch.from_numpy(off_h.view(np.int64)).pin_memory()
     rot_p = torch.from_numpy(rot_h).pin_memory()
     mesh_p = torch.zeros(capi.full_mesh_words(S), dtype=torch.int64).pin_memory()
-    for _ in range(max(1, args.warmup // 2)):
-        ctx.sparse_ac_frames_host(ph_p, off_p, rot_p, nframes, params, mesh_p)
-    e2e_times = []
-    # The host mesh accumulates over the steps, as ACMesh does over a run's
-    # batches (Detector::AutoCorrelateSparseList adds to it).  It is not cleared
-    # between steps: a 65 MB CPU memset just before the call leaves the pinned
-    # buffer dirty in the CPU caches and slows the copies into and out of it by
-    # 1-2 ms, a cost of the benchmark loop rather than of the path.
-    for _ in range(max(15, args.steps)):
-        t0 = time.perf_counter()
-        ctx.sparse_ac_frames_host(ph_p, off_p, rot_p, nframes, params, mesh_p)
-        e2e_times.append(time.perf_counter() - t0)
-    e2e_s = statistics.median(e2e_times)
+    e_half = torch.zeros_like(half)
+    e_full = torch.zeros_like(full)
+
+    def e2e_run(nsteps):
+        e_half.zero_()
+        e_full.zero_()
+        for _ in range(nsteps):
+            ctx.sparse_ac_frames_host_to_device(ph_p, off_p, rot_p, nframes, params, e_half, sptr)
+        ctx.sparse_fold(e_half, S, e_full, sptr)
+        if distributed:
+            shard.reduce_mesh(e_full, dst=0)
+        if rank == 0:
+            mesh_p.copy_(e_full, non_blocking=True)
+        torch.cuda.synchronize()
+
+    e2e_run(1)
+    if distributed:
+        dist.barrier()
+    t0 = time.perf_counter()
+    e2e_run(args.steps)
+    e2e_s = time.perf_counter() - t0
     if distributed:
         t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    h2d = ph_h.nbytes + off_h.nbytes + rot_h.nbytes + 8 * capi.full_mesh_words(S)
-    d2h = 8 * capi.full_mesh_words(S)
+    h2d = ph_h.nbytes + off_h.nbytes + rot_h.nbytes
+    d2h = 8 * capi.full_mesh_words(S) / args.steps if rank == 0 else 0
 
-    # -- roofline of the pair kernel --------------------------------------
-    # algorithmic bytes per launch: one 8-byte read-modify-write (16 B) per
-    # mesh update (pairs off the ss = 0 plane update once, on it twice; self
-    # pairs of a frame are summed into one update) plus 16 B per photon read.
-    hbm_peak, peak_kind = measured_peaks()
-    updates = pairs - int(len(ph_h))  # distinct pairs: ~one update each
-    alg_bytes = 16.0 * updates + 16.0 * len(ph_h)
-    achieved = alg_bytes / (ms_kernel * 1e-3) / 1e9
-    traffic = committed_traffic()
-    upd_rate = updates / (ms_kernel * 1e-3)
+    # the reference's per-call contract: every call uploads the caller's host
+    # mesh and reads it back (iac_sparse_ac_frames_host), median of 15 calls
+    sync_call = None
+    if not distributed:
+        ctx.sparse_ac_frames_host(ph_p, off_p, rot_p, nframes, params, mesh_p)
+        tt = []
+        for _ in range(max(15, args.steps)):
+            t0 = time.perf_counter()
+            ctx.sparse_ac_frames_host(ph_p, off_p, rot_p, nframes, params, mesh_p)
+            tt.append(time.perf_counter() - t0)
+        sync_s = statistics.median(tt)
+        sync_call = {"value": pairs / sync_s, "unit": UNIT, "seconds_per_call": sync_s,
+                     "h2d_bytes_per_call": int(h2d + 8 * capi.full_mesh_words(S)),
+                     "d2h_bytes_per_call": int(8 * capi.full_mesh_words(S)),
+                     "note": "iac_sparse_ac_frames_host: the caller's 65 MB host mesh is uploaded and read "
+                             "back on every call (+= semantics of ACMesh::Mesh per batch)"}
 
     line = None
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": args.scaling, "vs_baseline": None,
             "dtype": "fp32+u64", "data": "synthetic (seeded; shapes of the rotated-correlator "
                                               "configuration)",
             "config": {"workload": WORKLOAD, "frames_per_gpu": nframes, "pairs_per_gpu": pairs,
+                       "batch_frames": cfg["batch_frames"], "pairs_total": total_pairs,
                        "photons_per_gpu": int(len(ph_h)), "mesh": S,
                        "interpolation": "nearest/nearest, double mapping",
                        "l2": "inputs larger than L2 (photon lists 176 MB > 126 MB)",
-                       "parallelism": f"frame-sharded dp{world}" if world > 1 else "1 GPU",
-                       "tuning": ctx.sparse_tuning(S)},
+                       "parallelism": (f"frame-sharded dp{world} ({args.scaling} scaling)" if world > 1
+                                       else "1 GPU"),
+                       "tuning": tun},
             "clocks": clk, "gpu_launches": launches,
             "graph": None if graph_ms is None else {
                 "ms_per_step": graph_ms, "value": total_pairs / (graph_ms * 1e-3),
                 "note": "the step (clear, plan, bin, fold) captured in one CUDA graph and replayed"},
             "out_of_mesh_writes": oob,
-            "e2e": {"value": total_pairs / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "seconds_per_step": e2e_s},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                         "frac": achieved / hbm_peak, "traffic": traffic,
-                         "peak_source": f"{peak_kind} hbm_gbs",
-                         "kernel": "sparse_pairs_kernel (+ planner)",
-                         "kernel_ms": ms_kernel,
-                         "limiter": "L2 64-bit atomic adds",
-                         "atomic_updates_per_s": upd_rate,
-                         "atomic_peak_per_s": atomic_peak,
-                         "atomic_frac": upd_rate / atomic_peak,
+            "e2e": {"value": total_pairs * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "seconds_per_step": e2e_s / args.steps,
+                    "frac_of_value": (total_pairs * args.steps / e2e_s) / value,
+                    "note": f"{args.steps} batches of pinned host photon lists "
+                            "(iac_sparse_ac_frames_host_to_device: chunked copies overlapping the binning) "
+                            "accumulate into a device-resident mesh that is folded and read back once at "
+                            "the end of the run; d2h per step = the 65 MB mesh / steps"},
+            "e2e_sync_call": sync_call,
+            "roofline": {"bound": "l2_atomic", "achieved": upd_rate, "peak": atomic_peak,
+                         "unit": "updates/s", "frac": upd_rate / atomic_peak, "traffic": None,
+                         "peak_source": "measured in this run: 2^30 scattered u64 atomic adds into a buffer "
+                                        "of the half mesh's size (iac_bench_scatter_add)",
+                         "kernel": "sparse_pairs_kernel (+ planner)", "kernel_ms": ms_kernel,
+                         "updates_per_launch": updates,
+                         "box": {"radius": R, "value_share": share,
+                                 "l2_updates_per_s": upd_rate * (1 - share),
+                                 "l2_frac": upd_rate * (1 - share) / atomic_peak,
+                                 "note": "updates within R of q = 0 go to a per-CTA shared-memory box; "
+                                         "l2_frac counts only the updates that reach L2 (box share "
+                                         "estimated from the mesh value it holds)"},
                          "atomic_peak_u32_per_s": atomic_peak_u32,
-                         "atomic_peak_source": "measured in this run: 2^30 scattered u64 atomic "
-                                               "adds into a buffer of the half-mesh size"},
+                         "traffic_note": "DRAM bytes are not measured in the run; the half mesh stays in "
+                                         "L2 and each photon is read once"},
         }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nthreads = cores()
@@ -504,6 +565,8 @@ def run_ours(args):
             "value": v, "unit": UNIT, "cores": nthreads, "kind": "port",
             "sample": f"first {nb} frames ({cp} pairs, {secs:.1f} s) "
                       "through the reference's CPU route, OpenMP on all host threads"}
+    if rank == 0 and world == 1 and not args.no_parts:
+        line["parts"] = run_parts(args, ctx, stream, atomic_peak)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -513,20 +576,28 @@ def run_ours(args):
     return 0
 
 
+def scatter_rate(ctx, stream, words, bits):
+    """Scattered atomic adds per second into a buffer of `words` words."""
+    import torch
+    scratch = torch.zeros(words, dtype=torch.int64, device="cuda")
+    upd = 1 << 30
+    sptr = stream.cuda_stream
+    ctx.bench_scatter_add(scratch, scratch.numel(), bits, upd // 8, 1, sptr)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.bench_scatter_add(scratch, scratch.numel(), bits, upd, 2, sptr)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return upd / (e0.elapsed_time(e1) * 1e-3)
+
+
 # ---------------------------------------------------------------------------
-# the other kernels of the path, each on its configuration (one JSON line)
+# the other parts of the path, each on its configuration
 # ---------------------------------------------------------------------------
 def _fp32_peak_tflops(clock_mhz):
     """FP32 FMA peak of 148 SMs x 128 lanes x 2 flop at the sampled clock (no
     measured FP32 figure exists for this pool; derived, not measured)."""
     return 148 * 128 * 2 * clock_mhz * 1e6 / 1e12
-
-
-# thread instructions per unordered pixel pair (ncu smsp__inst_executed.sum x 32 / pairs;
-# cq_small on the 1024^2 configuration itself, ac1d_cq on a 256^2 detector;
-# profiles/cq_small_kernel.md, profiles/ac1d_cq_kernel.md)
-INST_PER_PAIR = {"cq_small": 1582131114734 * 32 / (1048576 * 1048577 / 2),
-                 "ac1d_cq": 8217131069 * 32 / (65536 * 65537 / 2)}
 
 
 def _time(fn, steps, warmup, stream):
@@ -551,194 +622,317 @@ def _dense_inputs(ny, nx, gap=None):
     return I, km, mq
 
 
+def _fp32_roofline(rate, flops, clk, what):
+    mhz = clk.get("sm_mhz") or 1965.0
+    peak = _fp32_peak_tflops(mhz)
+    return {"bound": "fp32", "achieved": rate * flops / 1e12, "peak": peak, "unit": "TFLOP/s",
+            "frac": rate * flops / 1e12 / peak, "flop_per_unit": flops, "unit_of_work": what,
+            "peak_source": "derived: 148 SM x 128 FP32 lanes x 2 at the sampled clock (no measured FP32 peak)"}
+
+
+def part_dense(kind, args, ctx, stream, steps, warmup, nthreads):
+    """All 5.5e11 unordered pixel pairs of the 1024^2 radial mean-intensity
+    map: nearest-voxel C(q) on the 255-edge small mesh, or the 2 048-bin
+    linear AC1D histogram."""
+    import torch
+    import oracle
+    from incohautocorrelate_b200 import capi
+    sp = stream.cuda_stream
+    I, km, mq = _dense_inputs(args.det, args.det)
+    npix = I.size
+    dI, dk = torch.from_numpy(I).cuda(), torch.from_numpy(km).cuda()
+    pairs = npix * (npix + 1) // 2
+    if kind == "cq_small":
+        sh = capi.small_cq_mesh_shape(mq, 253)
+        mult = capi.cq_small_multiplicator(I)
+        out = torch.zeros(sh.size_ab * sh.size_ab * sh.size_c, dtype=torch.int64, device="cuda")
+        fn = lambda: (out.zero_(), ctx.cq_small(dI, dk, npix, sh, 0, mult, out, sp, fast_size=args.det))
+        desc = f"small C(q) mesh {sh.size_ab}x{sh.size_ab}x{sh.size_c}, nearest"
+        # diff 3, norm 5, product 1, scale 3
+        flops = 12.0
+    else:
+        sh = capi.ac1d_shape(mq, 2048)
+        mult = capi.ac1d_cq_multiplicator(I)
+        out = torch.zeros(sh.size, dtype=torch.int64, device="cuda")
+        fn = lambda: (out.zero_(), ctx.ac1d_cq(dI, dk, npix, sh, 1, mult, out, sp))
+        desc = "AC1D 2048 bins, linear"
+        # diff 3, norm 5, product 1, sqrt 1, divide 1
+        flops = 11.0
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms = _time(fn, steps, warmup, stream)
+    clk = clocks.stop()
+    rate = pairs / (ms * 1e-3)
+    res = {"metric": f"pixel pairs/s into {desc}", "value": rate, "unit": "pairs/s", "ms_per_step": ms,
+           "steps": steps, "dtype": "fp32+u64",
+           "config": {"workload": f"{args.det}x{args.det} radial mean intensity, 5% masked, "
+                                  f"all {pairs:.3g} unordered pixel pairs", "pixels": npix},
+           "clocks": clk, "roofline": _fp32_roofline(rate, flops, clk, "unordered pixel pair")}
+    if not args.no_cpu_baseline:
+        rows = 48
+        t0 = time.perf_counter()
+        if kind == "cq_small":
+            so = oracle.small_cq_mesh_shape(mq, 253)
+            m = np.zeros(so.size_ab * so.size_ab * so.size_c, np.uint64)
+            oracle.lib().iaco_cq_small(oracle.p(I), oracle.p(km), npix, so, 0, mult, npix // 2, npix // 2 + rows,
+                                       oracle.p(m))
+        else:
+            so = oracle.ac1d_shape(mq, 2048)
+            m = np.zeros(so.size, np.uint64)
+            oracle.lib().iaco_ac1d_cq(oracle.p(I), oracle.p(km), npix, so, 1, mult, npix // 2, npix // 2 + rows,
+                                      oracle.p(m))
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": rows * npix / 2 / dt, "unit": "pairs/s", "cores": nthreads, "kind": "port",
+                               "sample": f"{rows} work items (rows) x {npix} pixels of the reference's ordered-pair "
+                                         f"loop ({dt:.1f} s, OpenMP over rows), counted as unordered pairs "
+                                         "(2 ordered = 1)"}
+    return res
+
+
+def part_cq_merge(args, ctx, stream, steps, warmup, nthreads, atomic_peak):
+    """Merge_CQ: every non-zero voxel of the 1024x512 detector's small C(q)
+    mesh rotated by each of 100 000 SO(3) frames into the 201^3 mesh."""
+    import torch
+    import oracle
+    from incohautocorrelate_b200 import capi
+    from incohautocorrelate_b200 import workloads as W
+    sp = stream.cuda_stream
+    I, km, mq = _dense_inputs(512, 1024, gap=512)
+    npix = I.size
+    sh = capi.small_cq_mesh_shape(mq, 199)
+    mult = capi.cq_small_multiplicator(I)
+    small_u = torch.zeros(sh.size_ab * sh.size_ab * sh.size_c, dtype=torch.int64, device="cuda")
+    ctx.cq_small(torch.from_numpy(I).cuda(), torch.from_numpy(km).cuda(), npix, sh, 0, mult, small_u, sp,
+                 fast_size=1024)
+    small = small_u.cpu().numpy().view(np.uint64).astype(np.float64) / mult
+    nf = args.frames
+    R = W.haar_rotations(nf, seed=3)
+    MI = np.random.default_rng(4).uniform(0.5e-4, 4e-4, nf).astype(np.float32)
+    rw, m = capi.cq_merge_weights(R, MI, small)
+    d_small, d_rw = torch.from_numpy(small).cuda(), torch.from_numpy(rw).cuda()
+    big = torch.zeros(sh.size_ab ** 3, dtype=torch.int64, device="cuda")
+    nvox = int((small >= np.float32(1e-37)).sum())
+    fn = lambda: (big.zero_(), ctx.cq_merge(d_small, d_rw, nf, sh, 0, m, big, sp))
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms = _time(fn, steps, warmup, stream)
+    clk = clocks.stop()
+    rate = nvox * nf / (ms * 1e-3)
+    res = {"metric": "voxel-frame scatters/s (C(q) merge)", "value": rate, "unit": "scatters/s",
+           "ms_per_step": ms, "steps": steps, "dtype": "fp32+u64",
+           "config": {"workload": f"small C(q) {sh.size_ab}x{sh.size_ab}x{sh.size_c} ({nvox} non-zero voxels) "
+                                  f"x {nf} SO(3) frames into {sh.size_ab}^3"},
+           "clocks": clk,
+           "roofline": {"bound": "l2_atomic", "achieved": rate, "peak": atomic_peak, "unit": "updates/s",
+                        "frac": rate / atomic_peak,
+                        "peak_source": "scattered u64 atomic adds measured in this run",
+                        "note": "one 64-bit L2 atomic per (voxel, frame)"}}
+    if not args.no_cpu_baseline:
+        sub = min(nvox, 20000)
+        so = oracle.small_cq_mesh_shape(mq, 199)
+        out = np.zeros(sh.size_ab ** 3, np.uint64)
+        nz = np.nonzero(small >= np.float32(1e-37))[0]
+        v0 = int(nz[len(nz) // 2])
+        t0 = time.perf_counter()
+        oracle.lib().iaco_cq_merge(oracle.p(small), oracle.p(rw.reshape(-1)), min(nf, 2000), so, 0, m, v0, v0 + sub,
+                                   oracle.p(out))
+        dt = time.perf_counter() - t0
+        done = int(((small[v0:v0 + sub]) >= np.float32(1e-37)).sum()) * min(nf, 2000)
+        res["cpu_baseline"] = {"value": done / dt, "unit": "scatters/s", "cores": nthreads, "kind": "port",
+                               "sample": f"{sub} voxels x {min(nf, 2000)} frames of the reference's Merge_CQ loop"}
+    return res
+
+
+def part_ac1d(kind, args, ctx, stream, steps, warmup, nthreads):
+    """AC1D of the rotated-correlator frames (100 000 frames, 2 048 bins).
+    "ac1d_uw": the reference's per-frame route choice; every frame of this
+    workload has fewer than 0.75 % hits and takes the host loop (k >= j, factor
+    2), run on the device, nearest binning.  "ac1d_sparse": the
+    AutoCorr_sparseHL_AAV kernel's route forced on every frame, linear."""
+    import torch
+    import oracle
+    from incohautocorrelate_b200 import capi
+    from incohautocorrelate_b200 import workloads as W
+    sp = stream.cuda_stream
+    cfg = W.rotated_config(nframes=args.frames, seed=2)
+    sh = capi.ac1d_shape(cfg["max_q"], 2048)
+    ph = torch.from_numpy(cfg["photons"]).cuda()
+    off = torch.from_numpy(cfg["offsets"].view(np.int64)).cuda()
+    nf = len(cfg["offsets"]) - 1
+    if kind == "ac1d_uw":
+        acc = torch.zeros(capi.ac1d_uw_words(sh), dtype=torch.int64, device="cuda")
+        uw = torch.zeros(sh.size, dtype=torch.float64, device="cuda")
+        fn = lambda: (acc.zero_(), ctx.ac1d_uw_batch(ph, off, nf, cfg["npix"], sh, 0, acc, stream=sp),
+                      ctx.ac1d_uw_finish(acc, sh, uw, sp))
+        desc = "reference route choice (all frames: host loop, k >= j), nearest"
+    else:
+        vs = capi.ac1d_vecsize(sh.max_q, sh.dq_per_step)
+        hist = torch.zeros(vs, dtype=torch.int64, device="cuda")
+        fn = lambda: (hist.zero_(), ctx.ac1d_sparse_batch(ph, off, nf, sh.max_q, sh.dq_per_step, 1, 100.0, hist, sp))
+        desc = "device route (ordered pairs), linear"
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms = _time(fn, steps, warmup, stream)
+    clk = clocks.stop()
+    pairs = _pairs(cfg["offsets"])
+    rate = pairs / (ms * 1e-3)
+    res = {"metric": "photon pairs/s into the AC1D histogram", "value": rate, "unit": "pairs/s", "ms_per_step": ms,
+           "steps": steps, "dtype": "fp32+u64/f64", "clocks": clk,
+           "config": {"workload": f"{nf} rotated-correlator frames (1024x512), 2048 bins, {desc}"},
+           "roofline": _fp32_roofline(rate, 11.0, clk, "unordered photon pair (diff 3, norm 5, product 1, "
+                                                       "sqrt 1, divide 1)")}
+    if not args.no_cpu_baseline and kind == "ac1d_uw":
+        f = 3000
+        off_h = cfg["offsets"][: f + 1]
+        ac = np.zeros(sh.size)
+        t0 = time.perf_counter()
+        oracle.lib().iaco_ac1d_uw_frames(oracle.p(cfg["photons"]), oracle.p(off_h), f, cfg["npix"], sh.max_q,
+                                         sh.dq_per_step, sh.size, 0, -1, oracle.p(ac))
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": _pairs(off_h) / dt, "unit": "pairs/s", "cores": 1, "kind": "port",
+                               "sample": f"first {f} frames through the reference's host loop "
+                                         f"(Calculate_AC_UW_Mapped, one thread per frame range; {dt:.2f} s)"}
+    return res
+
+
+def part_average(args, ctx, stream, steps, warmup, nthreads):
+    """LoadAndAverageIntensity on the device: 512 frames of the 1024x512
+    detector (1.07 GB, > L2), photon discretisation, mask."""
+    import torch
+    sp = stream.cuda_stream
+    ny, nx, nf = 1024, 512, 512
+    rng = np.random.default_rng(5)
+    frames = torch.from_numpy(rng.gamma(0.3, 1.0, (nf, ny * nx)).astype(np.float32)).cuda()
+    mask = torch.from_numpy((rng.random(ny * nx) > 0.05).astype(np.int32)).cuda()
+    discr = torch.zeros(ny * nx, dtype=torch.int64, device="cuda")
+    mean = torch.zeros(nf, dtype=torch.float32, device="cuda")
+    phs = torch.zeros(nf, dtype=torch.float32, device="cuda")
+    fn = lambda: ctx.average_frames(frames, ny * nx, nf, mask, 0.2, 1.0, None, discr, mean, phs, sp)
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms = _time(fn, steps, max(3, warmup), stream)
+    clk = clocks.stop()
+    # the same batch without discretisation: the per-frame sums are then arbitrary FP32
+    # values summed sequentially in pixel order, a chain of ny*nx dependent adds per frame
+    fsum = torch.zeros(ny * nx, dtype=torch.float32, device="cuda")
+    fn_f = lambda: ctx.average_frames(frames, ny * nx, nf, mask, 0.2, 0.0, fsum, None, mean, None, sp)
+    ms_f = _time(fn_f, steps, max(3, warmup), stream)
+    nbytes = frames.numel() * 4 + ny * nx * (4 + 16)  # frames read once, mask, counts read + written
+    peak, kind = measured_peaks()
+    res = {"metric": "frames/s averaged (LoadAndAverageIntensity, photon discretisation)",
+           "value": nf / (ms * 1e-3), "unit": "frames/s", "ms_per_step": ms, "dtype": "fp32+i64", "clocks": clk,
+           "config": {"workload": f"{nf} frames of {ny}x{nx} (1.07 GB), 5% masked, threshold 0.2, step 1.0"},
+           "roofline": {"bound": "hbm", "achieved": nbytes / (ms * 1e-3) / 1e9, "peak": peak,
+                        "unit": "GB/s", "frac": nbytes / (ms * 1e-3) / 1e9 / peak,
+                        "peak_source": f"{kind} hbm_gbs",
+                        "note": "one pass over the frames: per-pixel photon counts and the exact "
+                                "integer per-frame photon totals in the same kernel"},
+           "float_mode": {"ms_per_step": ms_f, "frames_per_s": nf / (ms_f * 1e-3),
+                          "bound": "sequential FP32 sum per frame: a chain of "
+                                   f"{ny * nx} dependent adds (4 cycles each)"}}
+    if not args.no_cpu_baseline:
+        import oracle
+        sub = 16
+        fh = frames[:sub].cpu().numpy()
+        mh = mask.cpu().numpy()
+        so = np.zeros(ny * nx, np.float32)
+        do = np.zeros(ny * nx, np.int64)
+        mo = np.zeros(sub, np.float32)
+        po = np.zeros(sub, np.float32)
+        t0 = time.perf_counter()
+        oracle.lib().iaco_average_frames(oracle.p(fh), ny * nx, sub, oracle.p(mh), 0.2, 1.0, oracle.p(so),
+                                         oracle.p(do), oracle.p(mo), oracle.p(po))
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": sub / dt, "unit": "frames/s", "cores": 1, "kind": "port",
+                               "sample": f"{sub} of the {nf} frames"}
+    return res
+
+
+def part_frames_to_error(args, ctx, stream):
+    """The second half of the headline metric: frames the plain mesh needs to
+    reach the voxel-wise RMS error (against an independent 100 000-frame
+    reference) that the committed denoiser reaches from 500 frames, on
+    held-out random crystals simulated and correlated on the device."""
+    import torch
+    from incohautocorrelate_b200 import capi
+    from incohautocorrelate_b200 import denoise as D
+    params, meta = D.load_model(os.path.join(ROOT, "incohautocorrelate_b200", "weights", "denoiser_128.npz"))
+    setup = D.SimSetup(**meta["setup"])
+    sim = D.MeshSimulator(ctx, setup, stream=stream)
+    E = setup.crop
+    dn = capi.Denoiser(ctx, 1, E, E, E, backend=args.backend)
+    dn.set_params(params)
+    frames_in = int(meta["frames_in"])
+    plain = [frames_in, 1000, 2000, 5000, 10000, 20000, 50000]
+    clocks = ClockSampler(0)
+    clocks.start()
+    t0 = time.perf_counter()
+    summary, rows = D.evaluate(ctx, sim, dn, meta["norm"], args.f2e_crystals, frames_in, plain, 100000,
+                               seed=9001, log=None)
+    secs = time.perf_counter() - t0
+    clk = clocks.stop()
+    dn.close()
+    assert ctx.check() == 0
+    return {"metric": "frames to set mesh error, denoised vs plain (median over held-out crystals)",
+            "value": summary["median_gain"], "unit": "x fewer frames", "higher_is_better": True,
+            "dtype": "bf16 network, fp32 accumulation; uint64 meshes",
+            "config": {"workload": f"{args.f2e_crystals} held-out random crystals (a 3-6 A, 2-8 cells per axis, "
+                                   "1-4 emitters per cell), 128x128 detector of 0.3 mm pixels at 0.1 m, 0.02 "
+                                   "photons/pixel, 4 modes, 129^3 mesh; denoised 500-frame mesh vs plain meshes "
+                                   "of 500-50 000 frames against an independent 100 000-frame reference",
+                       "weights": "incohautocorrelate_b200/weights/denoiser_128.npz"},
+            "min_gain": summary["min_gain"], "geomean_gain": summary["geomean_gain"],
+            "gains": [r["gain"] for r in rows], "emitters": [r["emitters"] for r in rows],
+            "seconds": secs, "frames_simulated": sim.frames,
+            "frames_per_s": sim.frames / secs, "clocks": clk, "roofline": None,
+            "cpu_baseline": None,
+            "note": "no counterpart in the reference (its output of record is the plain mesh)"}
+
+
+def run_parts(args, ctx, stream, atomic_peak):
+    """One timed step (after one untimed) of every other part of the path."""
+    nthreads = cores()
+    parts = {}
+    for name, fn in (("cq_small", lambda: part_dense("cq_small", args, ctx, stream, 1, 1, nthreads)),
+                     ("ac1d_cq", lambda: part_dense("ac1d_cq", args, ctx, stream, 1, 1, nthreads)),
+                     ("cq_merge", lambda: part_cq_merge(args, ctx, stream, 1, 1, nthreads, atomic_peak)),
+                     ("ac1d_uw", lambda: part_ac1d("ac1d_uw", args, ctx, stream, 2, 1, nthreads)),
+                     ("simulate", lambda: simulate_pipeline(args, ctx, stream, nthreads, steps=2, warmup=1)),
+                     ("denoise", lambda: denoise_bench(args, ctx, stream, nthreads, layers=False)),
+                     ("frames_to_error", lambda: part_frames_to_error(args, ctx, stream))):
+        try:
+            parts[name] = fn()
+        except Exception as e:  # one part failing must not hide the headline
+            parts[name] = {"error": f"{type(e).__name__}: {e}"}
+    return parts
+
+
 def run_kernel(args):
     import torch
     from incohautocorrelate_b200 import capi
-    from incohautocorrelate_b200 import workloads as W
     torch.cuda.set_device(0)
     ctx = capi.Context(0)
     stream = torch.cuda.current_stream()
-    sp = stream.cuda_stream
     nthreads = cores()
-    clocks = ClockSampler(0)
-    line = {"metric": None, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic",
-            "kernel": args.kernel}
-    import oracle
-    if args.kernel in ("cq_small", "ac1d_cq"):
-        I, km, mq = _dense_inputs(args.det, args.det)
-        npix = I.size
-        dI, dk = torch.from_numpy(I).cuda(), torch.from_numpy(km).cuda()
-        pairs = npix * (npix + 1) // 2
-        if args.kernel == "cq_small":
-            sh = capi.small_cq_mesh_shape(mq, 253)
-            mult = capi.cq_small_multiplicator(I)
-            out = torch.zeros(sh.size_ab * sh.size_ab * sh.size_c, dtype=torch.int64, device="cuda")
-            fn = lambda: (out.zero_(), ctx.cq_small(dI, dk, npix, sh, 0, mult, out, sp, fast_size=args.det))
-            shape_desc = f"small C(q) mesh {sh.size_ab}x{sh.size_ab}x{sh.size_c}"
-        else:
-            sh = capi.ac1d_shape(mq, 2048)
-            mult = capi.ac1d_cq_multiplicator(I)
-            out = torch.zeros(sh.size, dtype=torch.int64, device="cuda")
-            fn = lambda: (out.zero_(), ctx.ac1d_cq(dI, dk, npix, sh, 1, mult, out, sp))
-            shape_desc = "AC1D 2048 bins, linear"
-        clocks.start()
-        ms = _time(fn, args.steps, min(args.warmup, 1), stream)
-        clk = clocks.stop()
-        rate = pairs / (ms * 1e-3)
-        # FP32 work per unordered pair: diff 3, norm 5, product 1, scale 3 (3D) / div 1
-        flops = 12.0
-        mhz = clk["sm_mhz"] or 1965.0
-        line.update(metric=f"pixel pairs/s into {shape_desc}", value=rate, unit="pairs/s",
-                    ms_per_step=ms, dtype="fp32+u64",
-                    config={"workload": f"{args.det}x{args.det} radial mean intensity, 5% masked, "
-                                        f"all {pairs:.3g} unordered pixel pairs", "pixels": npix},
-                    clocks=clk,
-                    roofline={"bound": "fp32", "achieved": rate * flops / 1e12,
-                              "peak": _fp32_peak_tflops(mhz), "unit": "TFLOP/s",
-                              "frac": rate * flops / 1e12 / _fp32_peak_tflops(mhz),
-                              "peak_source": "derived 148 SM x 128 FP32 lanes x 2 at the sampled "
-                                             "clock (no measured FP32 peak)",
-                              "flop_per_pair": flops,
-                              # the binding resource: instruction issue.  Instructions per pair
-                              # from the committed ncu capture of this kernel (256^2 detector)
-                              "issue": {"inst_per_pair": INST_PER_PAIR[args.kernel],
-                                        "achieved": rate * INST_PER_PAIR[args.kernel],
-                                        "peak": 148 * 4 * 32 * mhz * 1e6,
-                                        "frac": rate * INST_PER_PAIR[args.kernel] / (148 * 4 * 32 * mhz * 1e6),
-                                        "unit": "thread instructions/s",
-                                        "source": f"profiles/{args.kernel}_kernel.md"}})
-        if not args.no_cpu_baseline:
-            rows = 48
-            Ih = np.ascontiguousarray(I)
-            t0 = time.perf_counter()
-            if args.kernel == "cq_small":
-                so = oracle.small_cq_mesh_shape(mq, 253)
-                m = np.zeros(so.size_ab * so.size_ab * so.size_c, np.uint64)
-                oracle.lib().iaco_cq_small(oracle.p(Ih), oracle.p(km), npix, so, 0, mult,
-                                           npix // 2, npix // 2 + rows, oracle.p(m))
-            else:
-                so = oracle.ac1d_shape(mq, 2048)
-                m = np.zeros(so.size, np.uint64)
-                oracle.lib().iaco_ac1d_cq(oracle.p(Ih), oracle.p(km), npix, so, 1, mult,
-                                          npix // 2, npix // 2 + rows, oracle.p(m))
-            dt = time.perf_counter() - t0
-            line["cpu_baseline"] = {"value": rows * npix / 2 / dt, "unit": "pairs/s",
-                                    "cores": nthreads, "kind": "port",
-                                    "sample": f"{rows} rows x {npix} pixels of the reference's "
-                                              f"ordered-pair loop ({dt:.1f} s), counted as "
-                                              "unordered pairs (2 ordered = 1)"}
-    elif args.kernel == "cq_merge":
-        I, km, mq = _dense_inputs(512, 1024, gap=512)
-        npix = I.size
-        sh = capi.small_cq_mesh_shape(mq, 199)
-        mult = capi.cq_small_multiplicator(I)
-        small_u = torch.zeros(sh.size_ab * sh.size_ab * sh.size_c, dtype=torch.int64, device="cuda")
-        ctx.cq_small(torch.from_numpy(I).cuda(), torch.from_numpy(km).cuda(), npix, sh, 0, mult,
-                     small_u, sp, fast_size=1024)
-        small = (small_u.cpu().numpy().view(np.uint64).astype(np.float64) / mult)
-        nf = args.frames
-        R = W.haar_rotations(nf, seed=3)
-        MI = np.random.default_rng(4).uniform(0.5e-4, 4e-4, nf).astype(np.float32)
-        rw, m = capi.cq_merge_weights(R, MI, small)
-        d_small, d_rw = torch.from_numpy(small).cuda(), torch.from_numpy(rw).cuda()
-        big = torch.zeros(sh.size_ab ** 3, dtype=torch.int64, device="cuda")
-        nvox = int((small >= np.float32(1e-37)).sum())
-        fn = lambda: (big.zero_(), ctx.cq_merge(d_small, d_rw, nf, sh, 0, m, big, sp))
-        clocks.start()
-        ms = _time(fn, args.steps, min(args.warmup, 1), stream)
-        clk = clocks.stop()
-        rate = nvox * nf / (ms * 1e-3)
-        line.update(metric="voxel-frame scatters/s (C(q) merge)", value=rate, unit="scatters/s",
-                    ms_per_step=ms, dtype="fp32+u64",
-                    config={"workload": f"small C(q) {sh.size_ab}x{sh.size_ab}x{sh.size_c} "
-                                        f"({nvox} non-zero voxels) x {nf} SO(3) frames into "
-                                        f"{sh.size_ab}^3"},
-                    clocks=clk,
-                    roofline={"bound": "l2-atomic", "achieved": rate, "unit": "updates/s",
-                              "note": "one 64-bit L2 atomic per (voxel, frame)"})
-        if not args.no_cpu_baseline:
-            sub = min(nvox, 20000)
-            so = oracle.small_cq_mesh_shape(mq, 199)
-            out = np.zeros(sh.size_ab ** 3, np.uint64)
-            nz = np.nonzero(small >= np.float32(1e-37))[0]
-            v0 = int(nz[len(nz) // 2])
-            t0 = time.perf_counter()
-            oracle.lib().iaco_cq_merge(oracle.p(small), oracle.p(rw.reshape(-1)), min(nf, 2000), so,
-                                       0, m, v0, v0 + sub, oracle.p(out))
-            dt = time.perf_counter() - t0
-            done = int(((small[v0:v0 + sub]) >= np.float32(1e-37)).sum()) * min(nf, 2000)
-            line["cpu_baseline"] = {"value": done / dt, "unit": "scatters/s", "cores": nthreads,
-                                    "kind": "port", "sample": f"{sub} voxels x {min(nf, 2000)} frames"}
-    elif args.kernel == "ac1d_sparse":
-        cfg = W.rotated_config(nframes=args.frames, seed=2)
-        sh = capi.ac1d_shape(cfg["max_q"], 256)
-        vs = capi.ac1d_vecsize(sh.max_q, sh.dq_per_step)
-        ph = torch.from_numpy(cfg["photons"]).cuda()
-        off = torch.from_numpy(cfg["offsets"].view(np.int64)).cuda()
-        hist = torch.zeros(vs, dtype=torch.int64, device="cuda")
-        nf = len(cfg["offsets"]) - 1
-        fn = lambda: (hist.zero_(), ctx.ac1d_sparse_batch(ph, off, nf, sh.max_q, sh.dq_per_step, 1,
-                                                          100.0, hist, sp))
-        clocks.start()
-        ms = _time(fn, args.steps, args.warmup, stream)
-        clk = clocks.stop()
-        pairs = _pairs(cfg["offsets"])
-        line.update(metric="photon pairs/s into the AC1D histogram", value=pairs / (ms * 1e-3),
-                    unit="pairs/s", ms_per_step=ms, dtype="fp32+u64", clocks=clk,
-                    config={"workload": f"{nf} rotated-correlator frames, 256 bins, linear"})
-    elif args.kernel == "simulate":
-        line.update(simulate_pipeline(args, ctx, stream, clocks, nthreads))
-    elif args.kernel == "denoise":
-        line.update(denoise_bench(args, ctx, stream, clocks, nthreads))
-    elif args.kernel == "average":
-        # LoadAndAverageIntensity on the device: 512 frames of the 1024x512 detector (1.07 GB, > L2),
-        # photon discretisation, mask
-        ny, nx, nf = 1024, 512, 512
-        rng = np.random.default_rng(5)
-        frames = torch.from_numpy(rng.gamma(0.3, 1.0, (nf, ny * nx)).astype(np.float32)).cuda()
-        mask = torch.from_numpy((rng.random(ny * nx) > 0.05).astype(np.int32)).cuda()
-        discr = torch.zeros(ny * nx, dtype=torch.int64, device="cuda")
-        mean = torch.zeros(nf, dtype=torch.float32, device="cuda")
-        phs = torch.zeros(nf, dtype=torch.float32, device="cuda")
-        fn = lambda: ctx.average_frames(frames, ny * nx, nf, mask, 0.2, 1.0, None, discr, mean, phs, sp)
-        clocks.start()
-        ms = _time(fn, args.steps, max(3, args.warmup), stream)
-        clk = clocks.stop()
-        # the same batch without discretisation: the per-frame sums are then arbitrary FP32
-        # values summed sequentially in pixel order, a chain of ny*nx dependent adds per frame
-        fsum = torch.zeros(ny * nx, dtype=torch.float32, device="cuda")
-        fn_f = lambda: ctx.average_frames(frames, ny * nx, nf, mask, 0.2, 0.0, fsum, None, mean, None, sp)
-        ms_f = _time(fn_f, args.steps, max(3, args.warmup), stream)
-        nbytes = frames.numel() * 4 + ny * nx * (4 + 16)  # frames read once, mask, counts read + written
-        peak, kind = measured_peaks()
-        line.update(metric="frames/s averaged (LoadAndAverageIntensity, photon discretisation)",
-                    value=nf / (ms * 1e-3), unit="frames/s", ms_per_step=ms, dtype="fp32+i64", clocks=clk,
-                    config={"workload": f"{nf} frames of {ny}x{nx} (1.07 GB), 5% masked, threshold 0.2, "
-                                        "step 1.0"},
-                    roofline={"bound": "hbm", "achieved": nbytes / (ms * 1e-3) / 1e9, "peak": peak,
-                              "unit": "GB/s", "frac": nbytes / (ms * 1e-3) / 1e9 / peak,
-                              "peak_source": f"{kind} hbm_gbs",
-                              "note": "one pass over the frames: per-pixel photon counts and the exact "
-                                      "integer per-frame photon totals in the same kernel"},
-                    float_mode={"ms_per_step": ms_f, "frames_per_s": nf / (ms_f * 1e-3),
-                                "bound": "sequential FP32 sum per frame: a chain of "
-                                         f"{ny * nx} dependent adds (4 cycles each)"})
-        if not args.no_cpu_baseline:
-            import oracle
-            sub = 16
-            fh = frames[:sub].cpu().numpy()
-            mh = mask.cpu().numpy()
-            so = np.zeros(ny * nx, np.float32)
-            do = np.zeros(ny * nx, np.int64)
-            mo = np.zeros(sub, np.float32)
-            po = np.zeros(sub, np.float32)
-            t0 = time.perf_counter()
-            oracle.lib().iaco_average_frames(oracle.p(fh), ny * nx, sub, oracle.p(mh), 0.2, 1.0, oracle.p(so),
-                                             oracle.p(do), oracle.p(mo), oracle.p(po))
-            dt = time.perf_counter() - t0
-            line["cpu_baseline"] = {"value": sub / dt, "unit": "frames/s", "cores": 1, "kind": "port",
-                                    "sample": f"{sub} of the {nf} frames"}
+    k = args.kernel
+    if k in ("cq_small", "ac1d_cq"):
+        res = part_dense(k, args, ctx, stream, args.steps, min(args.warmup, 1), nthreads)
+    elif k == "cq_merge":
+        peak = scatter_rate(ctx, stream, capi.half_mesh_words(201), 64)
+        res = part_cq_merge(args, ctx, stream, args.steps, min(args.warmup, 1), nthreads, peak)
+    elif k in ("ac1d_sparse", "ac1d_uw"):
+        res = part_ac1d(k, args, ctx, stream, args.steps, args.warmup, nthreads)
+    elif k == "simulate":
+        res = simulate_pipeline(args, ctx, stream, nthreads, steps=args.steps, warmup=args.warmup)
+    elif k == "denoise":
+        res = denoise_bench(args, ctx, stream, nthreads, layers=True)
+    elif k == "frames_to_error":
+        res = part_frames_to_error(args, ctx, stream)
+    else:
+        res = part_average(args, ctx, stream, args.steps, args.warmup, nthreads)
+    line = {"n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "data": "synthetic", "kernel": k}
+    line.update(res)
     print(json.dumps(line), flush=True)
     ctx.close()
     return 0
@@ -755,10 +949,10 @@ DENOISE_FWD_MACS = sum(27 * ci * co / d for ci, co, d in DENOISE_LAYERS) + 16
 DENOISE_TRAIN_MACS = DENOISE_FWD_MACS + (DENOISE_FWD_MACS - 27 * 16 - 16) + DENOISE_FWD_MACS
 
 
-def denoise_bench(args, ctx, stream, clocks, nthreads):
+def denoise_bench(args, ctx, stream, nthreads, layers=True):
     """The denoiser's training step (8 patches of 64^3, forward + loss +
-    backward + AdamW) and its inference on a whole 128^3 mesh, plus each
-    3x3x3 layer shape alone in both tensor-core backends."""
+    backward + AdamW) and its inference on a whole 128^3 mesh, plus (layers)
+    each 3x3x3 layer shape alone in both tensor-core backends."""
     import torch
     from incohautocorrelate_b200 import capi
     sp = stream.cuda_stream
@@ -772,6 +966,7 @@ def denoise_bench(args, ctx, stream, clocks, nthreads):
     dn.set_params(np.concatenate(parts).astype(np.float32))
     x = torch.from_numpy(rng.gamma(2.0, 0.5, (B, P, P, P)).astype(np.float32)).cuda()
     t = x * (1 + 0.2 * torch.randn_like(x))
+    clocks = ClockSampler(0)
     clocks.start()
 
     def train_step():
@@ -804,8 +999,8 @@ def denoise_bench(args, ctx, stream, clocks, nthreads):
     # every 3x3x3 shape alone on the training batch's volume at its level (the
     # decoder's concatenated inputs are materialised by the network, so every
     # layer reads one plain tensor)
-    layers = []
-    for ci, co, d in DENOISE_LAYERS[1:]:
+    layer_rows = []
+    for ci, co, d in (DENOISE_LAYERS[1:] if layers else []):
         edge = P // round(d ** (1 / 3))
         nvox = B * edge ** 3
         s1 = torch.randn((B, edge, edge, edge, ci), device="cuda").to(torch.bfloat16).view(torch.int16)
@@ -827,7 +1022,7 @@ def denoise_bench(args, ctx, stream, clocks, nthreads):
                                                      None, sp, slabs=sl), 10, 3, stream)
             row[name + "_ms"] = ms
             row[name + "_tflops"] = 2.0 * 27 * ci * co * nvox / (ms * 1e-3) / 1e12
-        layers.append(row)
+        layer_rows.append(row)
     clk = clocks.stop()
     peak, peak_src = measured_bf16_tflops()
     tf_train = 2.0 * DENOISE_TRAIN_MACS * B * P ** 3 / (ms_train * 1e-3) / 1e12
@@ -844,7 +1039,7 @@ def denoise_bench(args, ctx, stream, clocks, nthreads):
                                                   "captured in a CUDA graph and replayed"},
            "inference": {"volume": f"1 x {E}^3", "ms": ms_fwd, "tflops": tf_fwd,
                          "meshes_per_s": 1e3 / ms_fwd},
-           "layers": layers, "clocks": clk,
+           "layers": layer_rows, "clocks": clk,
            "roofline": {"bound": "tensor", "achieved": tf_train, "unit": "TFLOP/s", "peak": peak,
                         "frac": tf_train / peak, "peak_source": peak_src,
                         "kernel": "whole training step"}}
@@ -865,7 +1060,7 @@ def denoise_bench(args, ctx, stream, clocks, nthreads):
     return out
 
 
-def simulate_pipeline(args, ctx, stream, clocks, nthreads):
+def simulate_pipeline(args, ctx, stream, nthreads, steps=3, warmup=1):
     """512x512 detector (75 um at 0.10 m), 5x5x8 simple-cubic crystal (a = 4 A,
     200 emitters), 4 modes, SuSa 0, lambda 1.55 A, I = sum_modes |Psi|^2, mean
     0.02 photons per pixel, random orientations: emitters -> intensity ->
@@ -919,24 +1114,25 @@ def simulate_pipeline(args, ctx, stream, clocks, nthreads):
                             want_total=False)
         ctx.sparse_ac_batch(phot, offs, rot, chunk, params, half, sp)
 
-    for k in range(args.warmup):
+    for k in range(warmup):
         step(k)
     torch.cuda.synchronize()
     ev["intensity"].clear()
+    clocks = ClockSampler(0)
     clocks.start()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(stream)
-    for k in range(args.steps):
-        step(args.warmup + k)
+    for k in range(steps):
+        step(warmup + k)
     b.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms = a.elapsed_time(b) / args.steps
+    ms = a.elapsed_time(b) / steps
     ms_int = sum(x.elapsed_time(y) for x, y in ev["intensity"]) / len(ev["intensity"])
     terms = npix * na * nmodes * chunk
     mufu_peak = 148 * 16 * (clk["sm_mhz"] or 1965.0) * 1e6 / 2  # two SFU ops per term
     out = {"metric": "simulated frames/s into the 201^3 pair mesh", "value": chunk / (ms * 1e-3),
-           "unit": "frames/s", "ms_per_step": ms, "dtype": "fp32",
+           "unit": "frames/s", "ms_per_step": ms, "steps": steps, "dtype": "fp32",
            "config": {"workload": "512x512, 5x5x8 crystal (200 emitters), 4 modes, SuSa 0, "
                                   "|Psi|^2, 0.02 photons/pixel, random orientation",
                       "frames_per_step": chunk},

@@ -70,7 +70,10 @@ iac_status iac_ctx_destroy(iac_ctx *ctx);
  * error counters: writes skipped because their voxel lay outside the mesh
  * (the reference writes them out of bounds; IAC_ERR_OUT_OF_MESH), photons
  * dropped because a photon list was full (IAC_ERR_NO_MEMORY) and bounded
- * waits that ran out (IAC_ERR_TIMEOUT). */
+ * waits that ran out (IAC_ERR_TIMEOUT).  The counters are shared by all of
+ * the context's streams but only `stream` is waited for: work still running on
+ * another stream may count after the read, and its counts are then cleared
+ * with the others -- synchronise those streams first. */
 iac_status iac_ctx_check(iac_ctx *ctx, void *stream, uint64_t *out_of_mesh);
 const char *iac_status_string(iac_status s);
 const char *iac_last_error(void); /* thread-local message of the last failure */
@@ -175,6 +178,20 @@ iac_status iac_sparse_ac_frames_host(iac_ctx *ctx, const float *h_photons,
                                      uint32_t nframes, const iac_sparse_params *params,
                                      uint64_t *h_full_mesh);
 
+/* Host photon lists binned into a device half mesh that the caller keeps
+ * resident across calls (no counterpart call in the reference, whose ACMesh
+ * lives on the host and is read back after every frame,
+ * IAC/Detector.cpp:1100-1170): a run of many batches pays the mesh transfer
+ * once, at its end (iac_sparse_fold + one copy), instead of per batch as
+ * iac_sparse_ac_frames_host does.  d_half (uint64[iac_half_mesh_words(S)])
+ * accumulates; the frames are copied in chunks that overlap the binning on
+ * `stream`.  Returns once the host buffers have been read; the binning
+ * continues on `stream`.  Calls on one context are serialised. */
+iac_status iac_sparse_ac_frames_host_to_device(iac_ctx *ctx, const float *h_photons,
+                                               const uint64_t *h_frame_offsets, const float *h_rot9,
+                                               uint32_t nframes, const iac_sparse_params *params,
+                                               uint64_t *d_half_mesh, void *stream);
+
 /* Allocation-free form of iac_sparse_ac_batch (no counterpart in the
  * reference, which creates OpenCL buffers on every call).  For callers that
  * may not allocate device memory while they run -- an acquisition loop that
@@ -184,8 +201,9 @@ iac_status iac_sparse_ac_frames_host(iac_ctx *ctx, const float *h_photons,
  * on every GPU that loads it, until the process exits) and calls no
  * allocator.  Same arguments and result as iac_sparse_ac_batch, at most
  * 200 000 frames per call (more is rejected with IAC_ERR_INVALID_ARG).
- * The first call on a device looks up the array's device address; make that
- * first call before any stream capture.  Calls share the array: two calls
+ * iac_ctx_create looks up the array's device address on the context's device
+ * (a step that may load the library's device code there); the call itself
+ * only uses the address the context keeps.  Calls share the array: two calls
  * that run on the GPU at the same time (on different streams) race, so keep
  * them on one stream or otherwise ordered. */
 iac_status iac_sparse_ac_batch_static(iac_ctx *ctx, const float *d_photons,
@@ -230,6 +248,18 @@ iac_status iac_cq_small(iac_ctx *ctx, const float *d_intensity, const float *d_k
                         uint64_t npix, uint32_t fast_size, const iac_mesh_shape *small_shape,
                         int interp, double multiplicator, uint64_t *d_mesh, void *stream);
 
+/* The work items `ind` = d_rows[0 .. nrows) of AutoCorr_CQ_small
+ * (IAC/kernel.cl:27-184): for each listed pixel ind and every pixel i, the
+ * ordered pair (ind, i) binned exactly as that work item does, accumulated into
+ * d_mesh (no reflection; the mesh is the sum of these items over every ind,
+ * which iac_cq_small computes pair-symmetrically).  For checking a full-size
+ * detector against the oracle on a subset of rows.  Row indices >= npix are
+ * counted (iac_ctx_check, IAC_ERR_OUT_OF_MESH) and skipped.  nrows <= 16 776 960.
+ * Asynchronous. */
+iac_status iac_cq_small_rows(iac_ctx *ctx, const float *d_intensity, const float *d_kmap, uint64_t npix,
+                             const uint32_t *d_rows, uint32_t nrows, const iac_mesh_shape *small_shape,
+                             int interp, double multiplicator, uint64_t *d_mesh, void *stream);
+
 /* Rotation/weight table and Multiplicator of Detector::Merge_smallCofQ
  * (IAC/Detector.cpp:1339-1427): h_rw10 gets 9 rotation floats + the rounded
  * weight MeanIntensity^2 per frame.  Host arithmetic. */
@@ -259,6 +289,15 @@ iac_status iac_ac1d_cq_multiplicator(const float *h_intensity, uint64_t npix, do
 iac_status iac_ac1d_cq(iac_ctx *ctx, const float *d_intensity, const float *d_kmap,
                        uint64_t npix, const iac_ac1d_shape *shape, int interp,
                        double multiplicator, uint64_t *d_hist, void *stream);
+
+/* The work items `ind` = d_rows[0 .. nrows) of AutoCorr_CQ_AV
+ * (IAC/kernel.cl:656-764) into d_hist (uint64[shape.size], accumulated), each
+ * ordered pair (ind, i) binned exactly as that work item does (bins modulo
+ * Size, the sub-histogram fold).  Summed over every ind it equals iac_ac1d_cq.
+ * Asynchronous. */
+iac_status iac_ac1d_cq_rows(iac_ctx *ctx, const float *d_intensity, const float *d_kmap, uint64_t npix,
+                            const uint32_t *d_rows, uint32_t nrows, const iac_ac1d_shape *shape, int interp,
+                            double multiplicator, uint64_t *d_hist, void *stream);
 
 /* VecSize = ceil(MaxQ / dq) - 1 of Calculate_AC_UW_Mapped (IAC/AC1D.cpp:301). */
 uint32_t iac_ac1d_vecsize(float max_q, float dqdx);

@@ -125,6 +125,7 @@ def _declare(lib):
     fn("iac_sparse_fold", [_VP, _VP, _U32, _VP, _VP])
     fn("iac_sparse_ac_batch_static", [_VP, _VP, _VP, _VP, _U32, C.POINTER(SparseParams), _VP, _VP])
     fn("iac_sparse_ac_frames_host", [_VP, _VP, _VP, _VP, _U32, C.POINTER(SparseParams), _VP])
+    fn("iac_sparse_ac_frames_host_to_device", [_VP, _VP, _VP, _VP, _U32, C.POINTER(SparseParams), _VP, _VP])
     fn("iac_sparse_set_tuning", [_VP, C.POINTER(SparseTuning)])
     fn("iac_sparse_get_tuning", [_VP, _U32, C.POINTER(SparseTuning)])
     fn("iac_bench_scatter_add", [_VP, _VP, _U64, C.c_int, _U64, _U32, _VP])
@@ -136,6 +137,8 @@ def _declare(lib):
     fn("iac_ac1d_cq_multiplicator", [_VP, _U64, C.POINTER(D)])
     fn("iac_ac1d_cq", [_VP, _VP, _VP, _U64, C.POINTER(AC1DShape), C.c_int, D, _VP, _VP])
     fn("iac_ac1d_vecsize", [C.c_float, C.c_float], _U32)
+    fn("iac_cq_small_rows", [_VP, _VP, _VP, _U64, _VP, _U32, C.POINTER(MeshShape), C.c_int, D, _VP, _VP])
+    fn("iac_ac1d_cq_rows", [_VP, _VP, _VP, _U64, _VP, _U32, C.POINTER(AC1DShape), C.c_int, D, _VP, _VP])
     fn("iac_ac1d_sparse_batch", [_VP, _VP, _VP, _U32, C.c_float, C.c_float, C.c_int, D, _VP, _VP])
     fn("iac_ac1d_uw_words", [C.POINTER(AC1DShape)], _U64)
     fn("iac_ac1d_uw_batch", [_VP, _VP, _VP, _U32, _U64, C.POINTER(AC1DShape), C.c_int, C.c_int, _VP, _VP])
@@ -350,6 +353,12 @@ class Context:
                                               _ptr(h_rot), int(nframes), C.byref(params),
                                               _ptr(h_full)))
 
+    def sparse_ac_frames_host_to_device(self, h_photons, h_offsets, h_rot, nframes, params, d_half,
+                                        stream=None):
+        check(lib().iac_sparse_ac_frames_host_to_device(self._h, _ptr(h_photons), _ptr(h_offsets), _ptr(h_rot),
+                                                        int(nframes), C.byref(params), _ptr(d_half),
+                                                        _ptr(stream)))
+
     def set_sparse_tuning(self, tile_pairs=0, block_threads=0, ctas_per_sm=0, cache_hints=0):
         t = SparseTuning(int(tile_pairs), int(block_threads), int(ctas_per_sm), int(cache_hints))
         check(lib().iac_sparse_set_tuning(self._h, C.byref(t)))
@@ -364,6 +373,14 @@ class Context:
         check(lib().iac_cq_small(self._h, _ptr(d_I), _ptr(d_kmap), int(npix), int(fast_size),
                                  C.byref(shape), int(interp), float(mult), _ptr(d_mesh),
                                  _ptr(stream)))
+
+    def cq_small_rows(self, d_I, d_kmap, npix, d_rows, nrows, shape, interp, mult, d_mesh, stream=None):
+        check(lib().iac_cq_small_rows(self._h, _ptr(d_I), _ptr(d_kmap), int(npix), _ptr(d_rows), int(nrows),
+                                      C.byref(shape), int(interp), float(mult), _ptr(d_mesh), _ptr(stream)))
+
+    def ac1d_cq_rows(self, d_I, d_kmap, npix, d_rows, nrows, shape, interp, mult, d_hist, stream=None):
+        check(lib().iac_ac1d_cq_rows(self._h, _ptr(d_I), _ptr(d_kmap), int(npix), _ptr(d_rows), int(nrows),
+                                     C.byref(shape), int(interp), float(mult), _ptr(d_hist), _ptr(stream)))
 
     def cq_merge(self, d_small, d_rw, nframes, shape, interp, mult, d_big, stream=None):
         check(lib().iac_cq_merge(self._h, _ptr(d_small), _ptr(d_rw), int(nframes), C.byref(shape),

@@ -12,21 +12,36 @@ very mesh an uninterrupted run gives, bit for bit.
     full = run.full_mesh()                       # folded, uint64[S^3]
 
 A checkpoint is one .npz file, written to a temporary name and renamed, so a
-crash while saving leaves the previous checkpoint intact.
+crash while saving leaves the previous checkpoint intact.  It records which
+event list was being binned (frame count and a digest of the frame offsets and
+rotations), and a resumed run refuses to continue on another list, which would
+silently mix two runs into one mesh at the saved cursor.
 """
 from __future__ import annotations
 
+import hashlib
 import os
 
 import numpy as np
 
-_FORMAT = 1
+_FORMAT = 2
+
+
+def event_list_digest(offsets, rot) -> str:
+    """Identity of an event list: its frame count and a SHA-256 of its frame
+    offsets and rotation matrices."""
+    off = np.ascontiguousarray(offsets, np.uint64)
+    h = hashlib.sha256()
+    h.update(np.int64(len(off) - 1).tobytes())
+    h.update(off.tobytes())
+    h.update(np.ascontiguousarray(rot, np.float32).tobytes())
+    return h.hexdigest()
 
 
 class MeshRun:
     """Frames binned into one device half mesh, in batches, from a cursor."""
 
-    def __init__(self, ctx, params, S: int, half=None, cursor: int = 0):
+    def __init__(self, ctx, params, S: int, half=None, cursor: int = 0, events: str | None = None):
         import torch
 
         from . import capi
@@ -40,6 +55,7 @@ class MeshRun:
                 raise ValueError(f"checkpoint half mesh has {h.size} words, mesh {self.S} needs {words}")
             self.half = torch.from_numpy(h).cuda()
         self.cursor = int(cursor)
+        self.events = events  # digest of the event list being binned (set by the first bin_frames)
 
     # -- state ---------------------------------------------------------------
     def _key(self) -> np.ndarray:
@@ -54,7 +70,7 @@ class MeshRun:
         tmp = path + ".tmp.npz"
         np.savez(tmp, format=_FORMAT, half=self.half.cpu().numpy().view(np.uint64), cursor=self.cursor,
                  key=self._key(), max_q=np.float32(self.params.shape.max_q),
-                 multiplicator=np.float64(self.params.multiplicator))
+                 multiplicator=np.float64(self.params.multiplicator), events=self.events or "")
         os.replace(tmp, path)
 
     @classmethod
@@ -63,7 +79,7 @@ class MeshRun:
         with np.load(path) as z:
             if int(z["format"]) != _FORMAT:
                 raise ValueError(f"{path}: checkpoint format {int(z['format'])}, expected {_FORMAT}")
-            run = cls(ctx, params, S, half=z["half"], cursor=int(z["cursor"]))
+            run = cls(ctx, params, S, half=z["half"], cursor=int(z["cursor"]), events=str(z["events"]) or None)
             if not (np.array_equal(z["key"], run._key()) and float(z["max_q"]) == float(np.float32(params.shape.max_q))
                     and float(z["multiplicator"]) == float(params.multiplicator)):
                 raise ValueError(f"{path}: saved with other mesh or binning parameters")
@@ -79,6 +95,12 @@ class MeshRun:
         import torch
         off = np.asarray(offsets, np.uint64)
         nframes = len(off) - 1
+        digest = event_list_digest(off, rot)
+        if self.events is None:
+            self.events = digest
+        elif self.events != digest:
+            raise ValueError("the run was binning another event list (frame count, offsets or rotations differ); "
+                             "resuming it on this one would mix two runs into one mesh")
         done = 0
         while self.cursor < nframes:
             f0, f1 = self.cursor, min(nframes, self.cursor + int(batch))

@@ -143,6 +143,13 @@ iac_status iac_ctx_create(int device, iac_ctx **out)
     }
     cudaMemset(c->d_counters, 0, sizeof(DeviceCounters));
     cudaDeviceSynchronize();
+    // device address of the allocation-free entry point's fixed scratch array
+    const iac_status st = static_scratch_setup(c);
+    if (st != IAC_OK) {
+        cudaFree(c->d_counters);
+        delete c;
+        return st;
+    }
     load_tuning_table(c);
     *out = c;
     return IAC_OK;
@@ -161,6 +168,7 @@ iac_status iac_ctx_destroy(iac_ctx *ctx)
         if (ctx->d_counters) cudaFree(ctx->d_counters);
         for (auto &e : ctx->copy_events)
             if (e) cudaEventDestroy(e);
+        if (ctx->staging_free) cudaEventDestroy(ctx->staging_free);
         if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
         if (ctx->host_stream) cudaStreamDestroy(ctx->host_stream);
     }

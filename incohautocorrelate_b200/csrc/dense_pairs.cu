@@ -625,6 +625,163 @@ __global__ void __launch_bounds__(DTILE) ac1d_cq_kernel(const DenseArgs a)
         if (hist[i]) atomicAdd(&a.out[i], hist[i]);
 }
 
+// --------------------------------------------------------------------------
+// Row lists: the reference's own work decomposition.  Work item `ind` of
+// AutoCorr_CQ_small / AutoCorr_CQ_AV visits every pixel i and bins the
+// ordered pair (ind, i) (IAC/kernel.cl:78-182, :696-762); the mesh is the sum
+// of these independent items.  The kernels below evaluate the items of a list
+// of rows, each pair in the reference's arithmetic and order, so that a
+// full-size detector can be checked against the oracle on a subset of rows and
+// the unordered-pair kernels above against the sum over every row.  A CTA
+// stages 256 consecutive pixels and each thread walks them for its row.
+// --------------------------------------------------------------------------
+__device__ __forceinline__ void global_put(const DenseArgs &a, int fs, int ms, int ss, unsigned long long v)
+{
+    if (v == 0) return;
+    if ((unsigned)fs >= (unsigned)a.ab || (unsigned)ms >= (unsigned)a.ab || (unsigned)ss >= (unsigned)a.sc)
+        atomicAdd(&a.counters->out_of_mesh, 1ull);
+    else
+        atomicAdd(&a.out[(uint64_t)fs + (uint64_t)ms * a.ab + (uint64_t)ss * a.ab * a.ab], v);
+}
+
+// the staged column tile of a row-list kernel: 256 consecutive pixels as (k, I)
+__device__ __forceinline__ void stage_columns(const DenseArgs &a, uint64_t col_tile, float4 *sq)
+{
+    const uint64_t j = col_tile * DTILE + threadIdx.x;
+    sq[threadIdx.x] = j < a.npix ? make_float4(a.K[3 * j], a.K[3 * j + 1], a.K[3 * j + 2], a.I[j])
+                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// C(q) small mesh, rows x all pixels: grid (column tiles, row tiles)
+template <int INTERP>
+__global__ void __launch_bounds__(DTILE) cq_rows_kernel(const DenseArgs a, const uint32_t *__restrict__ rows,
+                                                        uint32_t nrows)
+{
+    __shared__ float4 sq[DTILE];
+    stage_columns(a, blockIdx.x, sq);
+    __syncthreads();
+    const uint32_t r = blockIdx.y * DTILE + threadIdx.x;
+    if (r >= nrows) return;
+    const uint32_t ind = rows[r];
+    if (ind >= a.npix) {
+        if (blockIdx.x == 0) atomicAdd(&a.counters->out_of_mesh, 1ull);
+        return;
+    }
+    const float k0 = a.K[3 * (uint64_t)ind], k1 = a.K[3 * (uint64_t)ind + 1], k2 = a.K[3 * (uint64_t)ind + 2];
+    const float Ia = a.I[ind];
+    int cf = 0, cm = 0, cs = 0;
+    bool have = false;
+    unsigned long long acc[INTERP ? 8 : 1];
+#pragma unroll
+    for (int c = 0; c < (INTERP ? 8 : 1); c++) acc[c] = 0;
+    for (int j = 0; j < DTILE; j++) {
+        const float4 b = sq[j];
+        const float pv = fmul(Ia, b.w);  // Val = (double)(I_ind * I_i)
+        if (pv < 1e-37f) continue;
+        float qx = fsub(k0, b.x), qy = fsub(k1, b.y), qz = fsub(k2, b.z);
+        if (fadd(fadd(fmul(qx, qx), fmul(qy, qy)), fmul(qz, qz)) > a.maxq2) continue;
+        qx = fmul(qx, a.vpdq);
+        qy = fmul(qy, a.vpdq);
+        qz = fmul(qz, a.vpdq);
+        const float qa = pick(qx, qy, qz, a.ka), qb = pick(qx, qy, qz, a.kb), qc = pick(qx, qy, qz, a.kc);
+        int f, m, sv;
+        if (INTERP == 0) {
+            f = round_half_away(qa) + a.cab;
+            m = round_half_away(qb) + a.cab;
+            sv = round_half_away(qc) + a.cc;
+        } else {
+            f = __float2int_rd(qa) + a.cab;
+            m = __float2int_rd(qb) + a.cab;
+            sv = __float2int_rd(qc) + a.cc;
+        }
+        if (!have || f != cf || m != cm || sv != cs) {
+            if (have) {
+#pragma unroll
+                for (int c = 0; c < (INTERP ? 8 : 1); c++)
+                    global_put(a, cf + (c >> 2), cm + ((c >> 1) & 1), cs + (c & 1), acc[c]);
+            }
+            have = true;
+            cf = f;
+            cm = m;
+            cs = sv;
+#pragma unroll
+            for (int c = 0; c < (INTERP ? 8 : 1); c++) acc[c] = 0;
+        }
+        if (INTERP == 0) {
+            acc[0] += a.mult_int ? scaled_floor(pv, a.mult_int) : d2u64(dmul((double)pv, a.mult));
+        } else {
+            const double vm = dmul((double)pv, a.mult);
+            const double sf = (double)fsub(1.0f, fsub(qa, floorf(qa)));
+            const double sm = (double)fsub(1.0f, fsub(qb, floorf(qb)));
+            const double sz = (double)fsub(1.0f, fsub(qc, floorf(qc)));
+            const double xf[2] = {sf, dsub(1.0, sf)}, yf[2] = {sm, dsub(1.0, sm)}, zf[2] = {sz, dsub(1.0, sz)};
+#pragma unroll
+            for (int c = 0; c < 8; c++) acc[c] += d2u64(dmul(vm, dmul(dmul(xf[c >> 2], yf[(c >> 1) & 1]), zf[c & 1])));
+        }
+    }
+    if (have) {
+#pragma unroll
+        for (int c = 0; c < (INTERP ? 8 : 1); c++)
+            global_put(a, cf + (c >> 2), cm + ((c >> 1) & 1), cs + (c & 1), acc[c]);
+    }
+}
+
+// AC1D |q| histogram, rows x all pixels: persistent CTAs over (row tile,
+// column tile) items, the histogram in shared memory for the whole launch
+template <int INTERP>
+__global__ void __launch_bounds__(DTILE) ac1d_rows_kernel(const DenseArgs a, const uint32_t *__restrict__ rows,
+                                                          uint32_t nrows)
+{
+    extern __shared__ unsigned long long hist[];
+    __shared__ float4 sq[DTILE];
+    __shared__ unsigned long long s_item;
+    for (uint32_t i = threadIdx.x; i < a.hsize; i += DTILE) hist[i] = 0;
+    const uint64_t ncol = (a.npix + DTILE - 1) / DTILE;
+    const unsigned long long nitems = (unsigned long long)ncol * ((nrows + DTILE - 1) / DTILE);
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(a.queue, 1ull);
+        __syncthreads();
+        const unsigned long long it = s_item;
+        if (it >= nitems) break;
+        const uint64_t rt = it / ncol, ct = it - rt * ncol;
+        stage_columns(a, ct, sq);
+        __syncthreads();
+        const uint64_t r = rt * DTILE + threadIdx.x;
+        const uint32_t ind = r < nrows ? rows[r] : 0xffffffffu;
+        if (r < nrows && ind >= a.npix && ct == 0) atomicAdd(&a.counters->out_of_mesh, 1ull);
+        if (ind < a.npix) {
+            const float k0 = a.K[3 * (uint64_t)ind], k1 = a.K[3 * (uint64_t)ind + 1], k2 = a.K[3 * (uint64_t)ind + 2];
+            const float Ia = a.I[ind];
+            for (int j = 0; j < DTILE; j++) {
+                const float4 b = sq[j];
+                const float pv = fmul(Ia, b.w);
+                if (pv < 1e-37f) continue;
+                const double val = (double)pv;
+                const float dx = fsub(k0, b.x), dy = fsub(k1, b.y), dz = fsub(k2, b.z);
+                float q = __fsqrt_rn(fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz)));
+                if (q > a.maxq) continue;
+                q = __fdiv_rn(q, a.dq);
+                if (INTERP == 0) {
+                    const uint32_t sc = wrap_bin((uint32_t)floor(dadd((double)q, 0.5)), a.hsize);
+                    atomicAdd(&hist[sc], a.mult_int ? scaled_floor(pv, a.mult_int)
+                                                    : (unsigned long long)(long long)dmul(val, a.mult));
+                } else {
+                    const float fq = floorf(q);
+                    const double sep = (double)fsub(q, fq);
+                    atomicAdd(&hist[wrap_bin((uint32_t)fq, a.hsize)],
+                              (unsigned long long)(long long)dmul(dmul(val, dsub(1.0, sep)), a.mult));
+                    atomicAdd(&hist[wrap_bin((uint32_t)fq + 1, a.hsize)],
+                              (unsigned long long)(long long)dmul(dmul(val, sep), a.mult));
+                }
+            }
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < a.hsize; i += DTILE)
+        if (hist[i]) atomicAdd(&a.out[i], hist[i]);
+}
+
 static float sqrt_threshold(float m)
 {
     if (!(m >= 0.0f) || std::isinf(m)) return m;
@@ -766,6 +923,92 @@ iac_status iac_ac1d_cq(iac_ctx *ctx, const float *d_I, const float *d_kmap, uint
     auto k = interp == 0 ? ac1d_cq_kernel<0> : ac1d_cq_kernel<1>;
     IAC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<ctx->sm_count * 8, DTILE, smem, as_stream(stream)>>>(a);
+    IAC_LAUNCHED(ctx);
+    IAC_CUDA(cudaGetLastError());
+    return IAC_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+iac_status iac_cq_small_rows(iac_ctx *ctx, const float *d_I, const float *d_kmap, uint64_t npix,
+                             const uint32_t *d_rows, uint32_t nrows, const iac_mesh_shape *sh, int interp,
+                             double mult, uint64_t *d_mesh, void *stream)
+{
+    IAC_TRACE();
+    IAC_REQUIRE(ctx && d_I && d_kmap && sh && d_mesh && d_rows, "iac_cq_small_rows: NULL argument");
+    IAC_REQUIRE(interp == 0 || interp == 1, "interpolation must be 0 or 1");
+    IAC_REQUIRE(npix > 0 && npix < (1ull << 32), "iac_cq_small_rows: pixel count %llu out of range",
+                (unsigned long long)npix);
+    IAC_REQUIRE(nrows >= 1 && nrows <= 65535u * DTILE, "iac_cq_small_rows: %u rows out of range [1, %u]", nrows,
+                65535u * DTILE);
+    IAC_REQUIRE(sh->size_ab >= 5 && sh->size_ab % 2 == 1 && sh->size_c >= 1 && sh->size_c % 2 == 1,
+                "small mesh sizes must be odd");
+    IAC_REQUIRE(sh->k_a < 3 && sh->k_b < 3 && sh->k_c < 3, "bad axis alignment");
+    IAC_REQUIRE(mult > 0, "multiplicator must be positive");
+    DeviceGuard g(ctx->device);
+    DenseArgs a{};
+    a.I = d_I;
+    a.K = d_kmap;
+    a.npix = npix;
+    a.mult = mult;
+    a.mult_int = (mult >= 1.0 && mult < 536870912.0 && mult == std::floor(mult)) ? (uint32_t)mult : 0u;
+    a.counters = ctx->d_counters;
+    a.out = (unsigned long long *)d_mesh;
+    a.maxq = sh->max_q;
+    a.maxq2 = sqrt_threshold(sh->max_q);
+    a.vpdq = (float)sh->voxel_per_dq;
+    a.ab = (int)sh->size_ab;
+    a.sc = (int)sh->size_c;
+    a.cab = (a.ab - 1) / 2;
+    a.cc = (a.sc - 1) / 2;
+    a.ka = (int)sh->k_a;
+    a.kb = (int)sh->k_b;
+    a.kc = (int)sh->k_c;
+    const dim3 grid((unsigned)((npix + DTILE - 1) / DTILE), (nrows + DTILE - 1) / DTILE);
+    if (interp == 0)
+        cq_rows_kernel<0><<<grid, DTILE, 0, as_stream(stream)>>>(a, d_rows, nrows);
+    else
+        cq_rows_kernel<1><<<grid, DTILE, 0, as_stream(stream)>>>(a, d_rows, nrows);
+    IAC_LAUNCHED(ctx);
+    IAC_CUDA(cudaGetLastError());
+    return IAC_OK;
+}
+
+iac_status iac_ac1d_cq_rows(iac_ctx *ctx, const float *d_I, const float *d_kmap, uint64_t npix,
+                            const uint32_t *d_rows, uint32_t nrows, const iac_ac1d_shape *sh, int interp,
+                            double mult, uint64_t *d_hist, void *stream)
+{
+    IAC_TRACE();
+    IAC_REQUIRE(ctx && d_I && d_kmap && sh && d_hist && d_rows, "iac_ac1d_cq_rows: NULL argument");
+    IAC_REQUIRE(interp == 0 || interp == 1, "interpolation must be 0 or 1");
+    IAC_REQUIRE(npix > 0 && npix < (1ull << 32), "iac_ac1d_cq_rows: pixel count out of range");
+    IAC_REQUIRE(nrows >= 1, "iac_ac1d_cq_rows: no rows");
+    IAC_REQUIRE(sh->size >= 3 && sh->size <= 24576, "AC1D size %u out of range [3, 24576]", sh->size);
+    IAC_REQUIRE(mult > 0, "multiplicator must be positive");
+    DeviceGuard g(ctx->device);
+    DenseArgs a{};
+    a.I = d_I;
+    a.K = d_kmap;
+    a.npix = npix;
+    a.mult = mult;
+    a.mult_int = (mult >= 1.0 && mult < 536870912.0 && mult == std::floor(mult)) ? (uint32_t)mult : 0u;
+    a.counters = ctx->d_counters;
+    a.out = (unsigned long long *)d_hist;
+    a.maxq = sh->max_q;
+    a.hsize = sh->size;
+    a.dq = sh->dq_per_step;
+    void *scr = nullptr;
+    iac_status st = stream_scratch(ctx, stream, SLOT_AUX0, 256, &scr);
+    if (st != IAC_OK) return st;
+    a.queue = (unsigned long long *)scr;
+    cudaStream_t s = as_stream(stream);
+    IAC_CUDA(cudaMemsetAsync(a.queue, 0, sizeof(unsigned long long), s));
+    const size_t smem = sizeof(unsigned long long) * sh->size;
+    auto k = interp == 0 ? ac1d_rows_kernel<0> : ac1d_rows_kernel<1>;
+    IAC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<ctx->sm_count * 4, DTILE, smem, s>>>(a, d_rows, nrows);
     IAC_LAUNCHED(ctx);
     IAC_CUDA(cudaGetLastError());
     return IAC_OK;

@@ -106,12 +106,20 @@ struct iac_ctx {
     cudaStream_t host_stream = nullptr;  // stream of the host-buffer entry points
     cudaStream_t copy_stream = nullptr;  // their host-to-device copies
     cudaEvent_t copy_events[IAC_COPY_CHUNKS + 1] = {};
+    cudaEvent_t staging_free = nullptr;  // recorded after the binning that read the host-entry staging
+    std::mutex host_mu;                  // one host-buffer entry point at a time (shared copy stream)
+    void *static_scratch = nullptr;      // device address of iac_sparse_ac_batch_static's fixed array
     std::atomic<uint64_t> launches{0};
 };
 
 namespace iac {
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Looks up, with the context's device current, the device address of the
+// fixed scratch array of iac_sparse_ac_batch_static (sparse_ac.cu) and keeps
+// it in the context.
+iac_status static_scratch_setup(iac_ctx *ctx);
 
 // Scratch slot `slot` of `stream`, grown to at least `bytes`.
 inline iac_status stream_scratch(iac_ctx *ctx, void *stream, int slot, size_t bytes, void **out)

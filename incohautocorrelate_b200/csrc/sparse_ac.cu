@@ -997,37 +997,37 @@ iac_status iac_sparse_fold(iac_ctx *ctx, const uint64_t *d_half, uint32_t S, uin
     return IAC_OK;
 }
 
-iac_status iac_sparse_ac_frames_host(iac_ctx *ctx, const float *h_photons,
-                                     const uint64_t *h_off, const float *h_rot9, uint32_t nframes,
-                                     const iac_sparse_params *p, uint64_t *h_full)
+}  // extern "C"
+
+namespace iac {
+
+// Streams and events of the host-buffer entry points, created on first use.
+static iac_status host_streams(iac_ctx *ctx)
 {
-    IAC_TRACE();
-    IAC_REQUIRE(ctx != nullptr, "iac_sparse_ac_frames_host: ctx is NULL");
-    iac_status st = check_params(p);
-    if (st != IAC_OK) return st;
-    IAC_REQUIRE(h_off && h_full, "iac_sparse_ac_frames_host: NULL pointer");
-    if (nframes == 0) return IAC_OK;
-    IAC_REQUIRE(h_photons && h_rot9, "iac_sparse_ac_frames_host: NULL pointer");
-    DeviceGuard g(ctx->device);
-    {
-        std::lock_guard<std::mutex> lk(ctx->mu);
-        if (!ctx->host_stream) IAC_CUDA(cudaStreamCreateWithFlags(&ctx->host_stream, cudaStreamNonBlocking));
-        if (!ctx->copy_stream) IAC_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
-        if (!ctx->copy_events[0])
-            for (auto &e : ctx->copy_events) IAC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    }
-    cudaStream_t s = ctx->host_stream, cs = ctx->copy_stream;
-    void *key = (void *)s;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!ctx->host_stream) IAC_CUDA(cudaStreamCreateWithFlags(&ctx->host_stream, cudaStreamNonBlocking));
+    if (!ctx->copy_stream) IAC_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    if (!ctx->copy_events[0])
+        for (auto &e : ctx->copy_events) IAC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    if (!ctx->staging_free) IAC_CUDA(cudaEventCreateWithFlags(&ctx->staging_free, cudaEventDisableTiming));
+    return IAC_OK;
+}
+
+// Host photon lists -> device staging (scratch of `key`) -> pair kernel into
+// d_half on stream s.  The frames are cut into chunks by photon count; chunk
+// k+1 is copied on the copy stream while chunk k is binned.  Binning is
+// slower than the copy, so only the first chunk's copy is exposed: it is made
+// a quarter of the others (1/29 of the photons for 8 chunks).  Every chunk has
+// its own rebased offsets so it is an independent batch.  The copies wait for
+// the previous call's binning (staging_free), whose staging they overwrite.
+static iac_status stage_and_bin(iac_ctx *ctx, const float *h_photons, const uint64_t *h_off, const float *h_rot9,
+                                uint32_t nframes, const iac_sparse_params *p, uint64_t *d_half, cudaStream_t s,
+                                void *key)
+{
+    iac_status st;
+    cudaStream_t cs = ctx->copy_stream;
     const uint64_t o0 = h_off[0];
     const uint64_t nph = h_off[nframes] - o0;
-    const uint32_t S = p->shape.size_ab;
-    const size_t half_b = sizeof(uint64_t) * iac_half_mesh_words(S);
-    const size_t full_b = sizeof(uint64_t) * iac_full_mesh_words(S);
-    // Pipelining: the frames are cut into chunks by photon count; chunk k+1 is
-    // copied on the copy stream while chunk k is binned.  Binning is slower
-    // than the copy, so only the first chunk's copy is exposed: it is made a
-    // quarter of the others (1/29 of the photons for 8 chunks).  Every chunk
-    // has its own rebased offsets so it is an independent batch.
     const uint32_t nchunks = std::max<uint32_t>(1, std::min<uint32_t>(IAC_COPY_CHUNKS, nframes / 64));
     std::vector<uint32_t> cut(nchunks + 1, 0);
     cut[nchunks] = nframes;
@@ -1037,12 +1037,11 @@ iac_status iac_sparse_ac_frames_host(iac_ctx *ctx, const float *h_photons,
         cut[k] = (uint32_t)(std::lower_bound(h_off, h_off + nframes + 1, target) - h_off);
         cut[k] = std::max(cut[k], cut[k - 1]);
     }
-    void *d_ph, *d_off, *d_rot, *d_half, *d_full;
+    void *d_ph, *d_off, *d_rot;
     if ((st = stream_scratch(ctx, key, SLOT_PHOTONS, 16 * nph + 16, &d_ph)) != IAC_OK) return st;
-    if ((st = stream_scratch(ctx, key, SLOT_OFFSETS, 8 * ((size_t)nframes + nchunks + 1), &d_off)) != IAC_OK) return st;
+    if ((st = stream_scratch(ctx, key, SLOT_OFFSETS, 8 * ((size_t)nframes + nchunks + 1), &d_off)) != IAC_OK)
+        return st;
     if ((st = stream_scratch(ctx, key, SLOT_ROT, 36 * (size_t)nframes, &d_rot)) != IAC_OK) return st;
-    if ((st = stream_scratch(ctx, key, SLOT_HALF, half_b, &d_half)) != IAC_OK) return st;
-    if ((st = stream_scratch(ctx, key, SLOT_FULL, full_b, &d_full)) != IAC_OK) return st;
     std::vector<uint64_t> off((size_t)nframes + nchunks);
     size_t w = 0;
     std::vector<size_t> off_pos(nchunks);
@@ -1056,9 +1055,10 @@ iac_status iac_sparse_ac_frames_host(iac_ctx *ctx, const float *h_photons,
         const size_t tb = ((sizeof(unsigned long long) * ((size_t)nframes + 1) + 127) / 128) * 128;
         if ((st = stream_scratch(ctx, key, SLOT_TILES, tb + 128 + nframes, &t)) != IAC_OK) return st;
     }
-    // the previous call's chunk copies must be done before the staging is reused
+    // the previous call's copies are done (its host buffers may be reused by
+    // the caller) and its binning has read the staging these copies overwrite
     IAC_CUDA(cudaStreamSynchronize(cs));
-    IAC_CUDA(cudaMemsetAsync(d_half, 0, half_b, s));
+    IAC_CUDA(cudaStreamWaitEvent(cs, ctx->staging_free, 0));
     IAC_CUDA(cudaMemcpyAsync(d_off, off.data(), 8 * w, cudaMemcpyHostToDevice, cs));
     for (uint32_t k = 0; k < nchunks; k++) {
         const uint32_t f0 = cut[k], f1 = cut[k + 1];
@@ -1074,18 +1074,73 @@ iac_status iac_sparse_ac_frames_host(iac_ctx *ctx, const float *h_photons,
         if (f1 > f0) {
             st = iac_sparse_ac_batch(ctx, (const float *)((char *)d_ph + 16 * p0),
                                      (const uint64_t *)d_off + off_pos[k], (const float *)d_rot + 9 * (size_t)f0,
-                                     f1 - f0, p, (uint64_t *)d_half, key);
+                                     f1 - f0, p, d_half, (void *)s);
             if (st != IAC_OK) return st;
         }
     }
+    IAC_CUDA(cudaEventRecord(ctx->staging_free, s));
+    return IAC_OK;
+}
+
+}  // namespace iac
+
+extern "C" {
+
+iac_status iac_sparse_ac_frames_host(iac_ctx *ctx, const float *h_photons,
+                                     const uint64_t *h_off, const float *h_rot9, uint32_t nframes,
+                                     const iac_sparse_params *p, uint64_t *h_full)
+{
+    IAC_TRACE();
+    IAC_REQUIRE(ctx != nullptr, "iac_sparse_ac_frames_host: ctx is NULL");
+    iac_status st = check_params(p);
+    if (st != IAC_OK) return st;
+    IAC_REQUIRE(h_off && h_full, "iac_sparse_ac_frames_host: NULL pointer");
+    if (nframes == 0) return IAC_OK;
+    IAC_REQUIRE(h_photons && h_rot9, "iac_sparse_ac_frames_host: NULL pointer");
+    DeviceGuard g(ctx->device);
+    std::lock_guard<std::mutex> hl(ctx->host_mu);
+    if ((st = host_streams(ctx)) != IAC_OK) return st;
+    cudaStream_t s = ctx->host_stream, cs = ctx->copy_stream;
+    void *key = (void *)s;
+    const uint32_t S = p->shape.size_ab;
+    const size_t half_b = sizeof(uint64_t) * iac_half_mesh_words(S);
+    const size_t full_b = sizeof(uint64_t) * iac_full_mesh_words(S);
+    void *d_half, *d_full;
+    if ((st = stream_scratch(ctx, key, SLOT_HALF, half_b, &d_half)) != IAC_OK) return st;
+    if ((st = stream_scratch(ctx, key, SLOT_FULL, full_b, &d_full)) != IAC_OK) return st;
+    IAC_CUDA(cudaMemsetAsync(d_half, 0, half_b, s));
+    if ((st = stage_and_bin(ctx, h_photons, h_off, h_rot9, nframes, p, (uint64_t *)d_half, s, key)) != IAC_OK)
+        return st;
     // the mesh the caller holds, uploaded behind the photon stream
+    const uint32_t ev = IAC_COPY_CHUNKS;
     IAC_CUDA(cudaMemcpyAsync(d_full, h_full, full_b, cudaMemcpyHostToDevice, cs));
-    IAC_CUDA(cudaEventRecord(ctx->copy_events[nchunks], cs));
-    IAC_CUDA(cudaStreamWaitEvent(s, ctx->copy_events[nchunks], 0));
+    IAC_CUDA(cudaEventRecord(ctx->copy_events[ev], cs));
+    IAC_CUDA(cudaStreamWaitEvent(s, ctx->copy_events[ev], 0));
     st = iac_sparse_fold(ctx, (const uint64_t *)d_half, S, (uint64_t *)d_full, key);
     if (st != IAC_OK) return st;
     IAC_CUDA(cudaMemcpyAsync(h_full, d_full, full_b, cudaMemcpyDeviceToHost, s));
     IAC_CUDA(cudaStreamSynchronize(s));
+    return IAC_OK;
+}
+
+iac_status iac_sparse_ac_frames_host_to_device(iac_ctx *ctx, const float *h_photons, const uint64_t *h_off,
+                                               const float *h_rot9, uint32_t nframes, const iac_sparse_params *p,
+                                               uint64_t *d_half, void *stream)
+{
+    IAC_TRACE();
+    IAC_REQUIRE(ctx != nullptr, "iac_sparse_ac_frames_host_to_device: ctx is NULL");
+    iac_status st = check_params(p);
+    if (st != IAC_OK) return st;
+    IAC_REQUIRE(h_off && d_half, "iac_sparse_ac_frames_host_to_device: NULL pointer");
+    if (nframes == 0) return IAC_OK;
+    IAC_REQUIRE(h_photons && h_rot9, "iac_sparse_ac_frames_host_to_device: NULL pointer");
+    DeviceGuard g(ctx->device);
+    std::lock_guard<std::mutex> hl(ctx->host_mu);
+    if ((st = host_streams(ctx)) != IAC_OK) return st;
+    cudaStream_t s = as_stream(stream);
+    if ((st = stage_and_bin(ctx, h_photons, h_off, h_rot9, nframes, p, d_half, s, stream)) != IAC_OK) return st;
+    // the host buffers have been read once the copies are done; binning goes on
+    IAC_CUDA(cudaStreamSynchronize(ctx->copy_stream));
     return IAC_OK;
 }
 
@@ -1104,13 +1159,18 @@ iac_status iac_sparse_ac_frames_host(iac_ctx *ctx, const float *h_photons,
 // device memory that is part of the loaded library, so it never allocates.
 //
 // The array's name in host code only stands in for the symbol; the kernels
-// need its device address, which cudaGetSymbolAddress gives once per device
-// (looked up on the first call made on that device, with the device current).
-// The array is shared by every call on the device and keeps the previous
-// call's contents: the planner kernel rewrites the whole tile table and
-// resets the queue counter before the pair kernel reads them, so nothing has
-// to be cleared from the host, but two calls running on the GPU at the same
-// time (e.g. on two streams) would overwrite each other's queue.
+// need its device address, which cudaGetSymbolAddress gives.  The context
+// looks it up once, when it is created (iac_ctx_create, with its device
+// current: the step that may load the library's device code and place the
+// array on that device), and keeps it; the entry point itself only reads it.
+// A context does not outlive a reset of its device (cudaDeviceReset ends every
+// context's device state), so the kept address is never stale while the
+// context is usable.  The array is shared by every call on the device and
+// keeps the previous call's contents: the planner kernel rewrites the whole
+// tile table and resets the queue counter before the pair kernel reads them,
+// so nothing has to be cleared from the host, but two calls running on the
+// GPU at the same time (e.g. on two streams) would overwrite each other's
+// queue.
 // ---------------------------------------------------------------------------
 namespace iac {
 
@@ -1122,27 +1182,17 @@ constexpr size_t STATIC_SCRATCH_BYTES = STATIC_TABLE_BYTES + STATIC_QUEUE_BYTES 
 
 static __device__ __align__(256) unsigned char g_sparse_static_scratch[STATIC_SCRATCH_BYTES];
 
-constexpr int STATIC_MAX_DEVICES = 64;
-static std::mutex g_static_mu;
-static void *g_static_addr[STATIC_MAX_DEVICES];
-
-// Device address of g_sparse_static_scratch on `dev` (which must be current).
-static iac_status static_scratch_address(int dev, void **out)
+iac_status static_scratch_setup(iac_ctx *ctx)
 {
-    IAC_REQUIRE(dev >= 0 && dev < STATIC_MAX_DEVICES, "device %d beyond the %d supported", dev,
-                STATIC_MAX_DEVICES);
-    std::lock_guard<std::mutex> lk(g_static_mu);
-    if (!g_static_addr[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_sparse_static_scratch);
-        if (e != cudaSuccess || !p) {
-            set_error("cudaGetSymbolAddress of the fixed scratch failed on device %d: %s", dev,
-                      cudaGetErrorString(e));
-            return IAC_ERR_CUDA;
-        }
-        g_static_addr[dev] = p;
+    DeviceGuard g(ctx->device);
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_sparse_static_scratch);
+    if (e != cudaSuccess || !p) {
+        set_error("cudaGetSymbolAddress of the fixed scratch failed on device %d: %s", ctx->device,
+                  cudaGetErrorString(e));
+        return IAC_ERR_CUDA;
     }
-    *out = g_static_addr[dev];
+    ctx->static_scratch = p;
     return IAC_OK;
 }
 
@@ -1157,18 +1207,18 @@ extern "C" iac_status iac_sparse_ac_batch_static(iac_ctx *ctx, const float *d_ph
     IAC_REQUIRE(ctx != nullptr, "iac_sparse_ac_batch_static: ctx is NULL");
     iac_status st = check_params(p);
     if (st != IAC_OK) return st;
-    IAC_REQUIRE(nframes <= STATIC_MAX_FRAMES,
-                "iac_sparse_ac_batch_static: %u frames requested; its fixed scratch holds the work "
-                "queue of at most %u frames per call (split the batch or use iac_sparse_ac_batch)",
-                nframes, STATIC_MAX_FRAMES);
     if (nframes == 0) return IAC_OK;
     IAC_REQUIRE(d_photons && d_off && d_rot9 && d_half, "iac_sparse_ac_batch_static: NULL pointer");
     IAC_REQUIRE((reinterpret_cast<uintptr_t>(d_photons) & 15) == 0,
                 "photon array must be 16-byte aligned (float4 per photon)");
+    IAC_REQUIRE(nframes <= STATIC_MAX_FRAMES,
+                "iac_sparse_ac_batch_static: %u frames requested; its fixed scratch holds the work "
+                "queue of at most %u frames per call (split the batch or use iac_sparse_ac_batch)",
+                nframes, STATIC_MAX_FRAMES);
+    IAC_REQUIRE(ctx->static_scratch != nullptr, "iac_sparse_ac_batch_static: the context has no fixed scratch");
     DeviceGuard g(ctx->device);
-    void *base = nullptr;
-    if ((st = static_scratch_address(ctx->device, &base)) != IAC_OK) return st;
-    const QueueMem q{(unsigned long long *)base, (unsigned long long *)((char *)base + STATIC_TABLE_BYTES),
+    char *base = (char *)ctx->static_scratch;
+    const QueueMem q{(unsigned long long *)base, (unsigned long long *)(base + STATIC_TABLE_BYTES),
                      (unsigned char *)base + STATIC_TABLE_BYTES + STATIC_QUEUE_BYTES};
     return launch_pair_batch(ctx, d_photons, d_off, d_rot9, nframes, p, q, d_half, as_stream(stream));
 }

@@ -39,6 +39,26 @@ def shard(photons, offsets, rot, rank: int, world: int):
     return photons[p0:p1], off[f0:f1 + 1] - off[f0], rot[f0:f1], (f0, f1)
 
 
+def rank_workload(rank: int, world: int, scaling: str, nframes: int, seed: int):
+    """The rotated-correlator frames one rank bins in a multi-process run.
+
+    scaling "weak": every rank bins its own `nframes` frames (seed offset by
+    rank), so the work per rank stays fixed as ranks are added; "strong": the
+    ranks share one batch of `nframes` frames, each binning a contiguous range
+    of about equal pair count.  Returns (photons, offsets, rotations, info)."""
+    from . import workloads as W
+    if scaling == "weak":
+        cfg = W.rotated_config(nframes=nframes, seed=seed + 7919 * rank)
+        info = {"frames": (0, nframes), "batch_frames": nframes * world}
+        return cfg["photons"], cfg["offsets"], cfg["rot"], dict(cfg, **info)
+    if scaling != "strong":
+        raise ValueError(f"scaling must be 'weak' or 'strong', not {scaling!r}")
+    cfg = W.rotated_config(nframes=nframes, seed=seed)
+    ph, off, rot, rng = shard(cfg["photons"], cfg["offsets"], cfg["rot"], rank, world)
+    info = {"frames": rng, "batch_frames": nframes}
+    return ph, off, rot, dict(cfg, **info)
+
+
 def reduce_mesh(mesh, dst: int = 0):
     """Sum the ranks' uint64 meshes (held as int64 tensors) onto `dst`.  Two's
     complement addition makes the int64 sum the uint64 sum modulo 2^64."""

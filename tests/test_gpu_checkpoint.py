@@ -60,6 +60,16 @@ def test_checkpoint_of_other_parameters_is_refused(tmp_path, oracle_lib, rng):
         other = capi.sparse_params(to_capi_shape(shape), 0, 0, False, 1000.0)
         with pytest.raises(ValueError, match="other mesh or binning parameters"):
             MeshRun.resume(ctx, other, S, path)
+        # the same parameters but another event list: reordered frames, or fewer
+        run = MeshRun.resume(ctx, p, S, path)
+        order = np.arange(len(off) - 1)[::-1]
+        n = np.diff(off.astype(np.int64))[order]
+        off2 = np.concatenate([[0], np.cumsum(n)]).astype(np.uint64)
+        ph2 = np.concatenate([ph[int(off[f]):int(off[f + 1])] for f in order])
+        for args in ((ph2, off2, rot[order]), (ph, off[:-5], rot[:-5])):
+            with pytest.raises(ValueError, match="another event list"):
+                run.bin_frames(*args, batch=100)
+        assert run.bin_frames(ph, off, rot, batch=100) == len(off) - 1  # the saved list continues
     finally:
         ctx.close()
 

@@ -213,6 +213,42 @@ def test_host_entry_point_pipelined_chunks(ctx, oracle_lib):
     np.testing.assert_array_equal(mesh.numpy().view(np.uint64), part)
 
 
+def test_host_entry_point_into_a_resident_device_mesh(ctx, oracle_lib):
+    """iac_sparse_ac_frames_host_to_device: host photon lists of three batches
+    (one of them a sub-range with non-zero first offset) accumulate into one
+    device half mesh on a caller stream; folded once at the end, the mesh is
+    the oracle's.  The host buffers are refilled between calls (the call
+    returns once they have been read)."""
+    import torch
+    from incohautocorrelate_b200 import capi, workloads as W
+    cfg = W.rotated_config(nframes=2400, seed=33)
+    shape = oracle_lib.big_mesh_shape(cfg["max_q"], cfg["mesh_size"])
+    want, _ = oracle_lib.sparse_batch(cfg["photons"], cfg["offsets"], cfg["rot"], shape, cpu_gpu=-1,
+                                      det_pixels=cfg["npix"])
+    p = capi.sparse_params(to_capi_shape(shape))
+    S = shape.size_ab
+    stream = torch.cuda.Stream()
+    half = torch.zeros(capi.half_mesh_words(S), dtype=torch.int64, device="cuda")
+    full = torch.zeros(capi.full_mesh_words(S), dtype=torch.int64, device="cuda")
+    off_all = cfg["offsets"]
+    ph_buf = torch.zeros((len(cfg["photons"]), 4), dtype=torch.float32).pin_memory()
+    off_buf = torch.zeros(2401, dtype=torch.int64).pin_memory()
+    rot_buf = torch.zeros((2400, 9), dtype=torch.float32).pin_memory()
+    for f0, f1, rebase in ((0, 1000, True), (1000, 1900, False), (1900, 2400, True)):
+        p0, p1 = int(off_all[f0]), int(off_all[f1])
+        # rebased offsets index the buffer from 0; the others from the batch's
+        # place in the whole photon array
+        at = 0 if rebase else p0
+        ph_buf[at: at + p1 - p0].copy_(torch.from_numpy(cfg["photons"][p0:p1]))
+        off_buf[: f1 - f0 + 1].copy_(torch.from_numpy(off_all[f0:f1 + 1].astype(np.int64) - p0 + at))
+        rot_buf[: f1 - f0].copy_(torch.from_numpy(cfg["rot"][f0:f1]))
+        ctx.sparse_ac_frames_host_to_device(ph_buf, off_buf, rot_buf, f1 - f0, p, half, stream.cuda_stream)
+    ctx.sparse_fold(half, S, full, stream.cuda_stream)
+    stream.synchronize()
+    assert ctx.check() == 0
+    np.testing.assert_array_equal(full.cpu().numpy().view(np.uint64), want)
+
+
 def test_cache_hint_setting_does_not_change_the_mesh(ctx, oracle_lib, rng):
     from incohautocorrelate_b200 import workloads as W
     _, km, mq = small_detector()

@@ -1,7 +1,9 @@
-"""Two ranks over gloo on the CPU: frames are sharded by pair count, every rank
-bins its shard (the oracle stands in for the device kernel here), one
-reduction sums the meshes, and the result is bit-identical to a single
-process binning every frame."""
+"""Two ranks over gloo on the CPU: each rank takes its frames exactly as the
+multi-GPU benchmark does (shard.rank_workload: a pair-balanced share of one
+batch for strong scaling, its own frames for weak scaling), bins them (the
+oracle stands in for the device kernel here), and the int64 view of its uint64
+mesh goes through the same shard.reduce_mesh call; the result is
+bit-identical to a single process binning every rank's frames."""
 import os
 import socket
 
@@ -17,43 +19,54 @@ def _free_port():
     return p
 
 
-def _rank_main(rank, world, port, out_dir):
+NFRAMES, SEED = 120, 5
+
+
+def _rank_main(rank, world, port, out_dir, scaling):
     import torch
     import torch.distributed as dist
 
     import oracle
-    from incohautocorrelate_b200 import shard, workloads as W
+    from incohautocorrelate_b200 import shard
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        cfg = W.rotated_config(nframes=120, seed=5)
+        ph, off, rot, cfg = shard.rank_workload(rank, world, scaling, NFRAMES, SEED)
         shape = oracle.big_mesh_shape(cfg["max_q"], 63)
-        ph, off, rot, (f0, f1) = shard.shard(cfg["photons"], cfg["offsets"], cfg["rot"], rank, world)
         mesh, _ = oracle.sparse_batch(ph, off, rot, shape, cpu_gpu=-1, det_pixels=cfg["npix"])
-        t = torch.from_numpy(mesh.view(np.int64).copy())
-        shard.reduce_mesh(t, dst=0)
+        full = torch.from_numpy(mesh.view(np.int64).copy())  # the benchmark's int64 mesh tensor
+        shard.reduce_mesh(full, dst=0)
         if rank == 0:
-            np.save(os.path.join(out_dir, "reduced.npy"), t.numpy().view(np.uint64))
-        np.save(os.path.join(out_dir, f"range{rank}.npy"), np.array([f0, f1]))
+            np.save(os.path.join(out_dir, "reduced.npy"), full.numpy().view(np.uint64))
+        np.save(os.path.join(out_dir, f"range{rank}.npy"), np.array(cfg["frames"]))
     finally:
         dist.destroy_process_group()
 
 
-def test_two_rank_gloo_reduction_is_bit_exact(tmp_path, oracle_lib):
+@pytest.mark.parametrize("scaling", ["strong", "weak"])
+def test_two_rank_gloo_reduction_is_bit_exact(tmp_path, oracle_lib, scaling):
     import torch.multiprocessing as mp
 
-    from incohautocorrelate_b200 import workloads as W
+    from incohautocorrelate_b200 import shard, workloads as W
     port = _free_port()
-    mp.start_processes(_rank_main, args=(2, port, str(tmp_path)), nprocs=2, join=True,
+    mp.start_processes(_rank_main, args=(2, port, str(tmp_path), scaling), nprocs=2, join=True,
                        start_method="spawn")
     r0 = np.load(tmp_path / "range0.npy")
     r1 = np.load(tmp_path / "range1.npy")
-    assert r0[0] == 0 and r0[1] == r1[0] and r1[1] == 120
-    cfg = W.rotated_config(nframes=120, seed=5)
+    cfg = W.rotated_config(nframes=NFRAMES, seed=SEED)
     shape = oracle_lib.big_mesh_shape(cfg["max_q"], 63)
-    want, _ = oracle_lib.sparse_batch(cfg["photons"], cfg["offsets"], cfg["rot"], shape, cpu_gpu=-1,
-                                      det_pixels=cfg["npix"])
+    if scaling == "strong":  # one batch, split at a frame boundary
+        assert r0[0] == 0 and r0[1] == r1[0] and r1[1] == NFRAMES
+        want, _ = oracle_lib.sparse_batch(cfg["photons"], cfg["offsets"], cfg["rot"], shape, cpu_gpu=-1,
+                                          det_pixels=cfg["npix"])
+    else:  # every rank its own batch: the sum of the two single-process meshes
+        want = np.zeros(shape.size_ab ** 3, np.uint64)
+        for r in range(2):
+            ph, off, rot, c = shard.rank_workload(r, 2, "weak", NFRAMES, SEED)
+            m, _ = oracle_lib.sparse_batch(ph, off, rot, shape, cpu_gpu=-1, det_pixels=c["npix"])
+            want += m
+    assert want.sum() > 0
     np.testing.assert_array_equal(np.load(tmp_path / "reduced.npy"), want)
 
 

@@ -52,7 +52,38 @@ def test_static_scratch_entry_rejects_batches_beyond_its_array(ctx):
     from incohautocorrelate_b200 import capi
     shape = capi.big_mesh_shape([0.7, 0.4, 0.1], 31)
     params = capi.sparse_params(shape)
+    # aligned placeholder pointers: the frame limit is checked before any launch
     with pytest.raises(capi.IacError) as e:
-        ctx.sparse_ac_batch_static(1, 1, 1, 200001, params, 1)
+        ctx.sparse_ac_batch_static(256, 256, 256, 200001, params, 256)
     assert e.value.status == capi.IAC_ERR_INVALID_ARG
     assert "200000" in str(e.value)
+
+
+def test_static_scratch_entry_needs_no_scratch_allocation(ctx):
+    """With the context's scratch capped at 64 bytes, on a new stream (which
+    has no scratch yet), the allocating entry point fails with
+    IAC_ERR_NO_MEMORY before allocating, while the allocation-free one bins
+    the batch, bit for bit as the allocating one did without the cap."""
+    import torch
+    from incohautocorrelate_b200 import capi, workloads as W
+    cfg = W.rotated_config(nframes=1500, seed=23)
+    shape = capi.big_mesh_shape(cfg["max_q"], cfg["mesh_size"])
+    params = capi.sparse_params(shape)
+    S = shape.size_ab
+    want = _run(ctx, ctx.sparse_ac_batch, cfg["photons"], cfg["offsets"], cfg["rot"], params, S)
+    c = capi.Context(0)
+    try:
+        c.set_scratch_limit(64)
+        s = torch.cuda.Stream()
+        ph, off, rot = _dev(cfg["photons"]), _dev(cfg["offsets"].view(np.int64)), _dev(cfg["rot"])
+        half = torch.zeros(capi.half_mesh_words(S), dtype=torch.int64, device="cuda")
+        with pytest.raises(capi.IacError) as e:
+            c.sparse_ac_batch(ph, off, rot, 1500, params, half, s.cuda_stream)
+        assert e.value.status == capi.IAC_ERR_NO_MEMORY
+        c.sparse_ac_batch_static(ph, off, rot, 1500, params, half, s.cuda_stream)
+        full = torch.zeros(capi.full_mesh_words(S), dtype=torch.int64, device="cuda")
+        c.sparse_fold(half, S, full, s.cuda_stream)
+        assert c.check(s.cuda_stream) == 0
+        np.testing.assert_array_equal(full.cpu().numpy().view(np.uint64), want)
+    finally:
+        c.close()
