@@ -1158,6 +1158,230 @@ __global__ void __launch_bounds__(256, 1) conv_zcol_kernel(const __grid_constant
     }
 }
 
+// --------------------------------------------------------------------------
+// z-column convolution with the three dz taps of an in-plane offset in one
+// MMA.  conv_zcol_kernel feeds each staged input-plane slab to three output
+// planes through three issuers, each multiplying the same shifted A tile
+// (128 positions x 16 channels, 4 KB of shared memory per K step) by an
+// N = cout weight tile: with N = 16 the tensor pipe spends its time reading A.
+// Here B is the concatenation [W(dz=-1) | W(dz=0) | W(dz=+1)] of the in-plane
+// tap (dy, dx), N = 3 cout, so each A tile is read once for all three output
+// planes: stage k (input plane p = z0 - 1 + k) writes the partial sums
+// P_k = A_p x Bcat into TMEM region k % NB, whose block b (dz = b - 1) belongs
+// to output plane p + 1 - b.  Output z0 + ol is P_ol[block 0] + P_ol+1[block 1]
+// + P_ol+2[block 2], complete once stage ol + 2 is; the epilogue adds the three
+// blocks in the order (dz -1) + (dz 0), then + (dz +1), and frees region ol.
+// NISS issuing warps take the stages in turn (a tcgen05.mma occupies its
+// issuing thread for longer than the tensor pipe needs for it); the regions
+// rotate over NB >= 3 buffers, NB - 3 stages of slack between issue and drain.
+// The concatenated weights (27 cin cout bf16) are built in shared memory by all
+// threads at the start, from the [tap][cin/8][cout][8] tiles.
+// --------------------------------------------------------------------------
+template <int CIN, int COUT, int NB, int NISS>
+__global__ void __launch_bounds__(32 * (5 + NISS), 1) conv_zcat_kernel(const __grid_constant__ CUtensorMap xmap,
+                                                                      const ConvArgs a, const TmaGeom g)
+{
+    constexpr int N3 = 3 * COUT;
+    constexpr uint32_t TCOLS = tma_tcols(NB * N3);
+    static_assert(NB >= 3 && NB * N3 <= 512, "three regions in flight within 512 TMEM columns");
+    static_assert(N3 % 16 == 0 && N3 <= 256, "M = 128 MMAs take N = 16 .. 256 in steps of 16");
+    constexpr uint32_t IDESC = idesc_bf16(TILE_M, N3);
+    constexpr uint32_t WT9_BYTES = N3 * CIN * 2;  // one in-plane tap, all three dz
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t full[8], empty[8], accfull[NB], accempty[NB];
+    __shared__ uint32_t s_tmem;
+    __shared__ volatile int s_err;
+    __shared__ long long s_issued, s_last[NISS];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t sbase = smem_u32(smem);
+    const uint32_t wbase = sbase;                   // concatenated weights [t9][cin/8][3 cout][8]
+    const uint32_t stbase = sbase + g.wres_bytes;   // stages: one input-plane slab each
+    // Bcat(t9)[kc][dzi * COUT + co][8] = W(tap = 9 dzi + t9)[kc][co][8]
+    for (int i = tid; i < 27 * CIN * COUT / 8; i += blockDim.x) {
+        const int co = i % COUT;
+        int r = i / COUT;
+        const int dzi = r % 3;
+        r /= 3;
+        const int kc = r % (CIN / 8), t9 = r / (CIN / 8);
+        const uint4 v = *reinterpret_cast<const uint4 *>(a.w + (((size_t)(9 * dzi + t9) * (CIN / 8) + kc) * COUT + co) * 8);
+        *reinterpret_cast<uint4 *>(smem + (size_t)i * 16) = v;
+    }
+    fence_proxy_async();  // the weights written by threads, read by the tensor core
+    if (tid == 0) {
+        for (int k = 0; k < g.S; k++) {
+            mbar_init(smem_u32(&full[k]), 1);
+            mbar_init(smem_u32(&empty[k]), 1);
+        }
+        for (int b = 0; b < NB; b++) {
+            mbar_init(smem_u32(&accfull[b]), 1);
+            mbar_init(smem_u32(&accempty[b]), 4);
+        }
+        fence_mbar_init();
+        s_err = 0;
+        s_issued = 0;
+        for (int i = 0; i < NISS; i++) s_last[i] = -1;
+    }
+    if (warp == 5) {
+        tmem_alloc(smem_u32(&s_tmem), TCOLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const int nzc = (a.D + g.ZC - 1) / g.ZC;  // z-chunks per column
+    const int HW = a.H * a.W;
+    auto item = [&](long long it, int &n, int &q0, int &z0, int &z1) {
+        const long long col = it / nzc;
+        z0 = (int)(it % nzc) * g.ZC;
+        z1 = z0 + g.ZC < a.D ? z0 + g.ZC : a.D;
+        n = (int)(col / g.T);
+        q0 = (int)(col % g.T) * TILE_M;
+    };
+
+    if (warp == 4) {
+        if (lane == 0) {  // producer: one slab per input plane z0-1 .. z1 (planes outside the volume arrive as zeros)
+            long long j = 0;
+            bool ok = true;
+            for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
+                int n, q0, z0, z1;
+                item(it, n, q0, z0, z1);
+                const int y_lo = floor_div(q0 - g.Wp - 1, g.Wp);
+                for (int pz = z0 - 1; pz <= z1; pz++, j++) {
+                    const int slot = (int)(j % g.S);
+                    if (j >= g.S && !mbar_wait_flag(smem_u32(&empty[slot]), (uint32_t)(((j / g.S) - 1) & 1), &s_err)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t st = stbase + (uint32_t)slot * g.stage_bytes;
+                    const uint32_t fb = smem_u32(&full[slot]);
+                    mbar_expect_tx(fb, (CIN / 8) * g.box_bytes);
+#pragma unroll
+                    for (int c = 0; c < CIN / 8; c++)
+                        tma_load_5d(st + c * g.plane_bytes, &xmap, c * 8, -1, y_lo, pz, n, fb);
+                    s_issued = j + 1;
+                }
+            }
+        }
+    } else if (warp >= 5) {
+        const int iw = warp - 5;  // stages j with j % NISS == iw
+        if (lane == 0) {
+            long long j = 0;
+            bool ok = true;
+            for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
+                int n, q0, z0, z1;
+                item(it, n, q0, z0, z1);
+                const int rel = q0 - floor_div(q0 - g.Wp - 1, g.Wp) * g.Wp;  // q0 within the slab
+                for (int k = 0; k < z1 - z0 + 2; k++, j++) {
+                    if ((int)(j % NISS) != iw) continue;
+                    const int slot = (int)(j % g.S);
+                    const int r = (int)(j % NB);
+                    if (!mbar_wait_flag(smem_u32(&full[slot]), (uint32_t)((j / g.S) & 1), &s_err) ||
+                        (j >= NB && !mbar_wait_flag(smem_u32(&accempty[r]), (uint32_t)(((j / NB) - 1) & 1), &s_err))) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t st = stbase + (uint32_t)slot * g.stage_bytes;
+                    const uint32_t dcol = tmem + (uint32_t)(r * N3);
+#pragma unroll 1
+                    for (int t = 0; t < 9; t++) {
+                        const uint32_t r0 = (uint32_t)(rel + (t / 3 - 1) * g.Wp + (t % 3 - 1));
+#pragma unroll
+                        for (int kk = 0; kk < CIN / 16; kk++) {
+                            const uint64_t da =
+                                smem_desc(st + (uint32_t)(2 * kk) * g.plane_bytes + r0 * 16, g.plane_bytes, 128);
+                            const uint64_t db = smem_desc(wbase + t * WT9_BYTES + kk * 2 * (N3 * 16), N3 * 16, 128);
+                            umma_bf16(dcol, da, db, IDESC, (t > 0 || kk > 0) ? 1u : 0u);
+                        }
+                    }
+                    umma_commit(smem_u32(&empty[slot]));
+                    umma_commit(smem_u32(&accfull[r]));
+                    s_last[iw] = j;
+                }
+            }
+        }
+    } else {  // epilogue: warps 0-3 own TMEM lanes 32w .. 32w+31
+        long long j = 0, waited = 0;  // this CTA's stages so far / stages whose MMAs are known complete
+        bool ok = true;
+        for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
+            int n, q0, z0, z1;
+            item(it, n, q0, z0, z1);
+            const int nz = z1 - z0;
+            const int q = q0 + tid;
+            const int y = q / g.Wp, xp = q - (q / g.Wp) * g.Wp;
+            const bool valid = y < a.H && xp >= 1 && xp <= a.W;
+            for (int ol = 0; ok && ol < nz; ol++) {
+                for (; waited <= j + ol + 2; waited++)
+                    if (!mbar_wait_flag(smem_u32(&accfull[waited % NB]), (uint32_t)((waited / NB) & 1), &s_err)) {
+                        ok = false;
+                        break;
+                    }
+                if (!ok) break;
+                tc_fence_after();
+                uint32_t rr[COUT];
+                const uint32_t lb = tmem + ((uint32_t)(warp * 32) << 16);
+                const uint32_t c0 = (uint32_t)(((j + ol) % NB) * N3);
+                const uint32_t c1 = (uint32_t)(((j + ol + 1) % NB) * N3 + COUT);
+                const uint32_t c2 = (uint32_t)(((j + ol + 2) % NB) * N3 + 2 * COUT);
+#pragma unroll
+                for (int c = 0; c < COUT; c += 16) {
+                    uint32_t (&r0)[16] = *reinterpret_cast<uint32_t(*)[16]>(&rr[c]);
+                    uint32_t r1[16], r2[16];
+                    tmem_ld16(lb + c0 + (uint32_t)c, r0);
+                    tmem_ld16(lb + c1 + (uint32_t)c, r1);
+                    tmem_ld16(lb + c2 + (uint32_t)c, r2);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int jj = 0; jj < 16; jj++)  // (dz -1) + (dz 0), then + (dz +1)
+                        r0[jj] = __float_as_uint(__fadd_rn(__fadd_rn(__uint_as_float(r0[jj]), __uint_as_float(r1[jj])),
+                                                           __uint_as_float(r2[jj])));
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(smem_u32(&accempty[(j + ol) % NB]));  // stage ol's last reader
+                if (valid) {
+                    const long long v = ((long long)n * a.D + z0 + ol) * HW + (long long)y * a.W + (xp - 1);
+#pragma unroll
+                    for (int c = 0; c < COUT; c += 8) {
+                        float f[8];
+#pragma unroll
+                        for (int jj = 0; jj < 8; jj++) f[jj] = __uint_as_float(rr[c + jj]);
+                        store8(a, COUT, v, c, f);
+                    }
+                }
+            }
+            if (!ok) break;
+            // the item's last two stages feed outputs past z1 only: their regions are free now
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(smem_u32(&accempty[(j + nz) % NB]));
+                mbar_arrive(smem_u32(&accempty[(j + nz + 1) % NB]));
+            }
+            j += nz + 2;
+        }
+    }
+    __syncthreads();
+    if (s_err) {
+        // after an error: let the copies and MMAs already issued finish (bounded)
+        // before the shared memory and TMEM are released
+        if (tid == 0) {
+            if (a.counters) atomicAdd(&a.counters->timeouts, 1ull);
+            for (long long i = s_issued > g.S ? s_issued - g.S : 0; i < s_issued; i++)
+                mbar_wait(smem_u32(&full[i % g.S]), (uint32_t)((i / g.S) & 1));
+            for (int w = 0; w < NISS; w++) {
+                const long long i = s_last[w];
+                if (i >= 0) mbar_wait(smem_u32(&empty[i % g.S]), (uint32_t)((i / g.S) & 1));
+            }
+        }
+        __syncthreads();
+    }
+    if (warp == 5) {
+        tc_fence_after();
+        tmem_dealloc(tmem, TCOLS);
+    }
+}
+
 // shared-memory attributes of a kernel, set once per process (the largest
 // size asked for so far); the attribute calls are host work on every launch
 // otherwise
@@ -1239,6 +1463,70 @@ static void launch_zcol_nb(const ConvArgs &a, TmaGeom g, const CUtensorMap &map,
     const long long grid = std::min<long long>(g.nitems, grid_max);
     conv_zcol_kernel<CIN, COUT, NB><<<(unsigned)grid, 256, smem, s>>>(map, a, g);
     err = cudaGetLastError();
+}
+
+// regions (NB) and issuing warps (NISS) of the concatenated-dz z-column
+// kernel per output channel count: N = 3 cout columns per region, NB >= 3
+// regions within the TMEM allocation the CTAs of an SM share
+template <int COUT>
+struct ZcatCfg {
+    static constexpr int N3 = 3 * COUT;
+    static constexpr int NB = 5 * N3 <= 256 ? 5 : (5 * N3 <= 512 ? 5 : (3 * N3 <= 512 ? 3 : 0));
+    static constexpr int PER_SM = (int)(512 / tma_tcols(NB > 0 ? NB * N3 : 512));  // CTAs per SM by TMEM
+    static constexpr int NISS = PER_SM >= 2 ? 2 : 3;
+};
+
+// the concatenated-dz z-column convolution (conv_zcat_kernel) when its
+// weights stay resident and 4+ stages fit; false leaves the layer to the
+// others.  IAC_DENOISE_ZCAT=0 in the environment turns it off (for comparing
+// the kernels).
+template <int CIN, int COUT>
+static bool launch_zcat(const ConvArgs &a, const TmaGeom &g0, const CUtensorMap &map, uint32_t budget,
+                        cudaStream_t s, cudaError_t &err)
+{
+    using Z = ZcatCfg<COUT>;
+    if constexpr (Z::NB == 0 || 3 * COUT > 256) {
+        return false;
+    } else {
+        static const bool off = [] {
+            const char *e = getenv("IAC_DENOISE_ZCAT");
+            return e && e[0] == '0';
+        }();
+        if (off) return false;
+        const uint32_t w27 = 27u * COUT * CIN * 2;
+        if (w27 > 96u * 1024u) return false;
+        TmaGeom g = g0;
+        g.wcopy_bytes = w27;
+        g.wres_bytes = (w27 + 1023u) & ~1023u;
+        g.wstage_bytes = 0;
+        g.stage_bytes = (g.slab_bytes + 1023u) & ~1023u;
+        int per_sm = 0, S = 0;
+        for (int want = Z::PER_SM; want >= 1 && per_sm == 0; want--) {
+            const uint32_t share = std::min(budget, (228u * 1024u) / (uint32_t)want - 2048u);
+            if (share <= g.wres_bytes) continue;
+            const int st = (int)std::min<uint32_t>(8u, (share - g.wres_bytes) / g.stage_bytes);
+            if (st >= 4) {
+                per_sm = want;
+                S = st;
+            }
+        }
+        if (per_sm == 0) return false;
+        g.S = S;
+        const long long nb = a.V / ((long long)a.D * a.H * a.W);
+        const long long grid_max = (long long)per_sm * std::max(1, a.sms);
+        int ZC = a.D;  // output planes per work item: the whole depth unless that leaves SMs idle
+        while (ZC > 4 && nb * g.T * ((a.D + ZC - 1) / ZC) < 2 * grid_max) ZC = (ZC + 1) / 2;
+        g.ZC = ZC;
+        g.nitems = nb * g.T * ((a.D + ZC - 1) / ZC);
+        const uint32_t smem = g.wres_bytes + (uint32_t)S * g.stage_bytes;
+        auto k = conv_zcat_kernel<CIN, COUT, Z::NB, Z::NISS>;
+        err = smem_attributes(k, smem);
+        if (err != cudaSuccess) return true;
+        const long long grid = std::min<long long>(g.nitems, grid_max);
+        k<<<(unsigned)grid, 32 * (5 + Z::NISS), smem, s>>>(map, a, g);
+        err = cudaGetLastError();
+        return true;
+    }
 }
 
 // the z-column convolution when its weights stay resident and 4+ stages fit;
@@ -1342,6 +1630,7 @@ static bool launch_tma(const ConvArgs &a, cudaStream_t s, cudaError_t &err)
                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return false;
+    if (launch_zcat<CIN, COUT>(a, g, map, budget, s, err)) return true;
     if (launch_zcol<CIN, COUT>(a, g, map, budget, s, err)) return true;
     const long long grid = std::min<long long>(g.ntiles, (long long)per_sm * std::max(1, a.sms));
     if constexpr (2 * 3 * COUT <= 512) {

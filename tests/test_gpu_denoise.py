@@ -17,7 +17,7 @@ pytestmark = pytest.mark.gpu
 
 # (c0, up0, c1, cout): the forward layers and the data-gradient layers of the network
 FWD = [(0, 0, 16, 16), (0, 0, 16, 32), (0, 0, 32, 32), (0, 0, 32, 64), (0, 0, 64, 64), (64, 1, 32, 32),
-       (32, 1, 16, 16)]
+       (32, 1, 16, 16), (0, 0, 96, 32), (0, 0, 48, 16)]
 DGRAD = [(0, 0, 32, 16), (0, 0, 64, 32), (0, 0, 32, 96), (0, 0, 16, 48)]
 
 
