@@ -508,9 +508,12 @@ iac_status iac_denoise_conv3x3(iac_ctx *ctx, int backend, const uint16_t *d_src0
 
 /* Weight gradient of that layer: d_dw[co][tap][ci] += sum_v grad[v][co] X[v + off(tap)][ci]
  * and d_db[co] += sum_v grad[v][co] (fp32, accumulated; d_db may be null).
- * slabs = 2 runs it on tcgen05 (TMEM accumulators, TMA-fed stages; plain
- * inputs only, else as 1), 1 on mma.sync staging each input row once per
- * tile and dz, 0 on mma.sync with one gathered tile per tap.  Asynchronous. */
+ * slabs = 3 runs it on tcgen05 with the three dz planes of a tile stacked
+ * into one MMA operand (16/32 input channels: the input slabs along M; 48 in,
+ * 16 out: the gradient slabs along N; other shapes as 2), 2 on tcgen05 with
+ * one dz per CTA (TMEM accumulators, TMA-fed stages; plain inputs only, else
+ * as 1), 1 on mma.sync staging each input row once per tile and dz, 0 on
+ * mma.sync with one gathered tile per tap.  Asynchronous. */
 iac_status iac_denoise_wgrad3x3(iac_ctx *ctx, int slabs, const uint16_t *d_src0, uint32_t c0, int up0,
                                 const uint16_t *d_src1, uint32_t c1, const uint16_t *d_grad,
                                 uint32_t cout, uint32_t nb, uint32_t D, uint32_t H, uint32_t W,

@@ -158,6 +158,17 @@ iac_status dgrad(iac_denoiser *dn, int l, const bf16 *gp, bf16 *out, int D, int 
     return IAC_OK;
 }
 
+// IAC_DENOISE_WGRAD_ZS=0 in the environment keeps the weight gradients on one
+// dz per CTA (for comparing the kernels)
+static bool wgrad_zs_enabled()
+{
+    static const bool on = [] {
+        const char *e = getenv("IAC_DENOISE_WGRAD_ZS");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 iac_status wgrad(iac_denoiser *dn, int l, const bf16 *src0, const bf16 *src1, const bf16 *gp, int D, int H,
                  int W, long long V, cudaStream_t s)
 {
@@ -180,12 +191,13 @@ iac_status wgrad(iac_denoiser *dn, int l, const bf16 *src0, const bf16 *src1, co
     a.W = W;
     a.V = V;
     a.cout = SPECS[l].cout;
-    // tcgen05 where it measured faster (32 or more input channels: an M = 64
-    // MMA holds at most 16 useful rows for 16), mma.sync on slabs elsewhere
+    // tcgen05 with the dz planes stacked into one MMA operand where the layer's
+    // shape has a configuration (wgrad3x3 falls back to one dz per CTA, then
+    // to mma.sync on slabs), mma.sync on slabs for the mma.sync backend
     if (dn->backend == BACKEND_TC_TAP)
         a.slabs = 0;
-    else if (dn->backend == BACKEND_TC_SLAB && cin >= 32)
-        a.slabs = 2;
+    else if (dn->backend == BACKEND_TC_SLAB)
+        a.slabs = wgrad_zs_enabled() ? 3 : (cin >= 32 ? 2 : 1);
     else
         a.slabs = 1;
     a.counters = dn->ctx->d_counters;

@@ -2235,6 +2235,198 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_tc_kernel(const __grid_const
     }
 }
 
+// --------------------------------------------------------------------------
+// weight gradient with the three dz planes stacked into one MMA operand.
+// wgrad_tc_kernel runs one dz per CTA (blockIdx.y), so an MMA has M = cin
+// rows (64 for 16 or 48 channels, 25-75 % of them padding) and N = cout = 16
+// columns, and each stage's X and gradient slabs are staged three times.
+// Here one stage holds all that one tile needs for its 27 taps, laid out so
+// that the dz axis becomes part of an MMA dimension (the chunk planes of
+// consecutive slabs are equally spaced, so they stack in one descriptor):
+//   PX = 3: X slabs of planes z-1, z, z+1 stacked along M (M = 3 cin rows:
+//           row (dz + 1) cin + ci), the gradient slab of plane z as B (N = cout);
+//   PX = 1: the X slab of plane z as A (M = cin), the gradient slabs of
+//           planes z+1, z, z-1 stacked along N (column (dz + 1) cout + co):
+//           X(z) pairs with G(z - dz), which is dz's term for output plane z - dz.
+// Either way a stage yields every tap of the tile: issuer warp 5 + t takes
+// the in-plane tap t = 3 (dy + 1) + dx + 1 and accumulates its (M x N) block
+// in TMEM for the whole launch.  Stages of every (item, plane, tile) are
+// independent (planes outside the volume arrive as zeros), so the CTAs are
+// persistent over all tiles.
+// --------------------------------------------------------------------------
+template <int CIN, int COUT, int PX>
+struct WzsCfg {
+    static constexpr int PG = PX == 3 ? 1 : 3;
+    static constexpr int MROWS = PX * CIN;              // real M rows
+    static constexpr int MR = MROWS > 64 ? 128 : 64;    // rows per MMA
+    static constexpr int MB = (MROWS + MR - 1) / MR;    // M blocks
+    static constexpr int N = PG * COUT;                 // MMA columns
+    static constexpr int COLS = 9 * N * MB;
+    static constexpr uint32_t TCOLS = COLS <= 32 ? 32 : (COLS <= 64 ? 64 : (COLS <= 128 ? 128 : (COLS <= 256 ? 256 : 512)));
+    static constexpr int XREAL = PX * CIN / 8;          // X chunk planes loaded
+    static constexpr int XPLANES = MB * MR / 8;         // X chunk planes the MMAs read (padding rows: garbage)
+    static constexpr int GPLANES = PG * COUT / 8;
+    static constexpr bool OK = COLS <= 512 && N <= 256 && N % (MR == 128 ? 16 : 8) == 0;
+};
+
+template <int CIN, int COUT, int PX>
+__global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_constant__ CUtensorMap xmap,
+                                                              const __grid_constant__ CUtensorMap gmap,
+                                                              const WgradArgs a, const WTGeom g)
+{
+    using Z = WzsCfg<CIN, COUT, PX>;
+    constexpr int MB = Z::MB, MR = Z::MR, N = Z::N;
+    constexpr uint32_t IDESC = idesc_bf16(MR, N) | (1u << 15) | (1u << 16);  // A and B MN-major
+    constexpr int NI = 9;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t full[8], empty[8], done;
+    __shared__ uint32_t s_tmem;
+    __shared__ volatile int s_err;
+    __shared__ long long s_issued, s_consumed[NI];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t sbase = smem_u32(smem);
+    const uint32_t xbytes = (uint32_t)Z::XPLANES * g.planeX;
+    if (tid == 0) {
+        for (int k = 0; k < g.S; k++) {
+            mbar_init(smem_u32(&full[k]), 1);
+            mbar_init(smem_u32(&empty[k]), NI);  // one commit per issuing warp
+        }
+        mbar_init(smem_u32(&done), NI);
+        fence_mbar_init();
+        s_err = 0;
+        s_issued = 0;
+        for (int i = 0; i < NI; i++) s_consumed[i] = 0;
+    }
+    if (warp == 5) {
+        tmem_alloc(smem_u32(&s_tmem), Z::TCOLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const long long my_tiles =
+        blockIdx.x < g.ntiles ? (g.ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+
+    if (warp == 4) {
+        if (lane == 0) {
+            for (long long k = 0; k < my_tiles; k++) {
+                const int slot = (int)(k % g.S);
+                if (k >= g.S && !mbar_wait_flag(smem_u32(&empty[slot]), (uint32_t)(((k / g.S) - 1) & 1), &s_err))
+                    break;
+                const long long tile = blockIdx.x + k * (long long)gridDim.x;
+                const long long plane = tile / g.T;
+                const int q0 = (int)(tile % g.T) * TILE_M;
+                const int n = (int)(plane / a.D), z = (int)(plane % a.D);
+                const int y_lo = floor_div(q0 - g.Wp - 1, g.Wp), yg_lo = q0 / g.Wp;
+                const uint32_t st = sbase + (uint32_t)slot * g.stage_bytes;
+                const uint32_t fb = smem_u32(&full[slot]);
+                mbar_expect_tx(fb, (uint32_t)Z::XREAL * g.boxX + (uint32_t)Z::GPLANES * g.boxG);
+#pragma unroll
+                for (int px = 0; px < PX; px++)
+#pragma unroll
+                    for (int c = 0; c < CIN / 8; c++)
+                        tma_load_5d(st + (uint32_t)(px * (CIN / 8) + c) * g.planeX, &xmap, c * 8, -1, y_lo,
+                                    PX == 3 ? z - 1 + px : z, n, fb);
+#pragma unroll
+                for (int pg = 0; pg < Z::PG; pg++)
+#pragma unroll
+                    for (int c = 0; c < COUT / 8; c++)
+                        tma_load_5d(st + xbytes + (uint32_t)(pg * (COUT / 8) + c) * g.planeG, &gmap, c * 8, -1, yg_lo,
+                                    Z::PG == 3 ? z + 1 - pg : z, n, fb);
+                s_issued = k + 1;
+            }
+        }
+    } else if (warp >= 5 && warp < 5 + NI) {
+        const int t = warp - 5;  // in-plane tap 3 (dy + 1) + dx + 1
+        if (lane == 0) {
+            for (long long k = 0; k < my_tiles; k++) {
+                const int slot = (int)(k % g.S);
+                if (!mbar_wait_flag(smem_u32(&full[slot]), (uint32_t)((k / g.S) & 1), &s_err)) break;
+                tc_fence_after();
+                const long long tile = blockIdx.x + k * (long long)gridDim.x;
+                const int q0 = (int)(tile % g.T) * TILE_M;
+                const int rel = q0 - floor_div(q0 - g.Wp - 1, g.Wp) * g.Wp;
+                const int relg = q0 - (q0 / g.Wp) * g.Wp;
+                const int r0 = rel + (t / 3 - 1) * g.Wp + (t % 3 - 1);
+                const uint32_t sX = sbase + (uint32_t)slot * g.stage_bytes, sG = sX + xbytes;
+#pragma unroll
+                for (int mb = 0; mb < MB; mb++) {
+                    const uint32_t dcol = tmem + (uint32_t)((t * MB + mb) * N);
+#pragma unroll
+                    for (int ks = 0; ks < TILE_M / 16; ks++) {
+                        const uint64_t da =
+                            smem_desc(sX + (uint32_t)(mb * (MR / 8)) * g.planeX + (uint32_t)(r0 + 16 * ks) * 16, 128, g.planeX);
+                        const uint64_t db = smem_desc(sG + (uint32_t)(relg + 16 * ks) * 16, 128, g.planeG);
+                        umma_bf16(dcol, da, db, IDESC, (k > 0 || ks > 0) ? 1u : 0u);
+                    }
+                }
+                umma_commit(smem_u32(&empty[slot]));
+                s_consumed[t] = k + 1;
+            }
+            if (!s_err && my_tiles > 0) umma_commit(smem_u32(&done));
+        }
+    }
+    __syncthreads();
+    // drain: warps 0-3 read the accumulators (thread = TMEM lane) and add them to dW
+    const bool ok = !s_err && my_tiles > 0;
+    if (warp < 4 && ok) {
+        if (!mbar_wait(smem_u32(&done), 0)) s_err = 1;
+    }
+    __syncthreads();
+    if (warp < 4 && ok && !s_err) {
+        tc_fence_after();
+        // an M = 64 accumulator keeps row i in TMEM lane 32 (i / 16) + i % 16; M = 128: row i in lane i
+        const int row = MR == 128 ? warp * 32 + lane : (lane < 16 ? warp * 16 + lane : -1);
+#pragma unroll 1
+        for (int blk = 0; blk < 9 * MB; blk++) {
+            uint32_t r[N];
+#pragma unroll
+            for (int c = 0; c < N; c += 16) {
+                uint32_t (&rr)[16] = *reinterpret_cast<uint32_t(*)[16]>(&r[c]);
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(blk * N + c), rr);
+            }
+            tmem_wait_ld();
+            const int t = blk / MB, mb = blk % MB;
+            const int m = mb * MR + row;
+            if (row >= 0 && m < Z::MROWS) {
+                if (PX == 3) {  // row (dz + 1) cin + ci, column co
+                    const int tap = 9 * (m / CIN) + t, ci = m % CIN;
+#pragma unroll
+                    for (int co = 0; co < COUT; co++) {
+                        const float v = __uint_as_float(r[co]);
+                        if (v != 0.0f) atomicAdd(&a.dw[((size_t)co * 27 + tap) * CIN + ci], v);
+                    }
+                } else {  // row ci, column (dz + 1) cout + co
+#pragma unroll
+                    for (int nn = 0; nn < N; nn++) {
+                        const float v = __uint_as_float(r[nn]);
+                        if (v != 0.0f)
+                            atomicAdd(&a.dw[((size_t)(nn % COUT) * 27 + 9 * (nn / COUT) + t) * CIN + m], v);
+                    }
+                }
+            }
+        }
+        tc_fence_before();
+    }
+    if (s_err && tid == 0) {
+        if (a.counters) atomicAdd(&a.counters->timeouts, 1ull);
+        long long consumed = s_consumed[0];
+        for (int i = 1; i < NI; i++) consumed = s_consumed[i] < consumed ? s_consumed[i] : consumed;
+        for (long long k = consumed; k < s_issued; k++)
+            mbar_wait(smem_u32(&full[k % g.S]), (uint32_t)((k / g.S) & 1));
+        if (consumed > 0) {
+            const long long k = consumed - 1;
+            mbar_wait(smem_u32(&empty[k % g.S]), (uint32_t)((k / g.S) & 1));
+        }
+    }
+    __syncthreads();
+    if (warp == 5) {
+        tc_fence_after();
+        tmem_dealloc(tmem, Z::TCOLS);
+    }
+}
+
 // bias gradient: db[c] += sum_v g[v][c]
 __global__ void bias_grad_kernel(const bf16 *__restrict__ g, int C, long long V, float *__restrict__ db)
 {
@@ -2321,12 +2513,91 @@ static bool launch_wgrad_tc(const WgradArgs &a, int sms, cudaStream_t s, cudaErr
     return true;
 }
 
+// the dz-stacked tcgen05 weight gradient (wgrad_zs_kernel); false when the
+// layer's shape has no configuration or a stage does not fit
+template <int CIN, int COUT, int PX>
+static bool launch_wgrad_zs(const WgradArgs &a, int sms, cudaStream_t s, cudaError_t &err)
+{
+    using Z = WzsCfg<CIN, COUT, PX>;
+    if constexpr (!Z::OK) {
+        return false;
+    } else {
+        if (a.c0 != 0 || a.W + 2 > 256) return false;
+        PFN_cuTensorMapEncodeTiled enc = tensor_map_encoder();
+        if (!enc) return false;
+        if ((reinterpret_cast<uintptr_t>(a.src1) & 15) || (reinterpret_cast<uintptr_t>(a.g) & 15)) return false;
+        WTGeom g{};
+        g.Wp = a.W + 2;
+        g.NR = 3 + (130 + g.Wp - 1) / g.Wp;
+        g.NRg = 2 + (TILE_M + g.Wp - 1) / g.Wp;
+        if (g.NR > 256 || g.NRg > 256) return false;
+        g.T = (a.H * g.Wp + TILE_M - 1) / TILE_M;
+        const long long nb = a.V / ((long long)a.D * a.H * a.W);
+        g.ntiles = nb * a.D * g.T;
+        g.boxX = 16u * (uint32_t)g.Wp * (uint32_t)g.NR;
+        g.boxG = 16u * (uint32_t)g.Wp * (uint32_t)g.NRg;
+        g.planeX = (g.boxX + 127u) & ~127u;
+        g.planeG = (g.boxG + 127u) & ~127u;
+        g.stage_bytes = (((uint32_t)Z::XPLANES * g.planeX + (uint32_t)Z::GPLANES * g.planeG) + 1023u) & ~1023u;
+        const uint32_t budget = 227u * 1024u - 2048u;
+        int per_sm = std::min(2, (int)(512 / Z::TCOLS));
+        g.S = 0;
+        for (; per_sm >= 1; per_sm--) {
+            const uint32_t share = std::min<uint32_t>(budget, (228u * 1024u) / (uint32_t)per_sm - 2048u);
+            const int S = (int)std::min<uint32_t>(6u, share / g.stage_bytes);
+            if (S >= 2) {
+                g.S = S;
+                break;
+            }
+        }
+        if (g.S < 2 || g.ntiles == 0) return false;
+        const uint32_t smem = (uint32_t)g.S * g.stage_bytes;
+        CUtensorMap maps[2];
+        const void *bases[2] = {a.src1, a.g};
+        const int chans[2] = {CIN, COUT};
+        const int rows[2] = {g.NR, g.NRg};
+        for (int m = 0; m < 2; m++) {
+            const cuuint64_t C = (cuuint64_t)chans[m];
+            const cuuint64_t dims[5] = {C, (cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.D, (cuuint64_t)nb};
+            const cuuint64_t strides[4] = {C * 2, (cuuint64_t)a.W * C * 2, (cuuint64_t)a.H * a.W * C * 2,
+                                           (cuuint64_t)a.D * a.H * a.W * C * 2};
+            const cuuint32_t box[5] = {8u, (cuuint32_t)g.Wp, (cuuint32_t)rows[m], 1u, 1u};
+            const cuuint32_t estr[5] = {1u, 1u, 1u, 1u, 1u};
+            if (enc(&maps[m], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void *>(bases[m]), dims, strides, box,
+                    estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                return false;
+        }
+        err = smem_attributes(wgrad_zs_kernel<CIN, COUT, PX>, smem);
+        if (err != cudaSuccess) return true;
+        const long long grid = std::min<long long>(g.ntiles, (long long)per_sm * std::max(1, sms));
+        wgrad_zs_kernel<CIN, COUT, PX><<<(unsigned)grid, 32 * (5 + 9), smem, s>>>(maps[0], maps[1], a, g);
+        if ((err = cudaGetLastError()) != cudaSuccess) return true;
+        if (a.db) {
+            const int lanes = 256 / COUT;
+            const long long blocks = std::min<long long>((a.V + lanes - 1) / lanes, 4LL * std::max(1, sms));
+            bias_grad_kernel<<<(unsigned)blocks, lanes * COUT, lanes * COUT * sizeof(float), s>>>(a.g, COUT, a.V, a.db);
+            err = cudaGetLastError();
+        }
+        return true;
+    }
+}
+
+// which operand carries the dz axis in wgrad_zs_kernel: the one whose three
+// planes give the fewer MMA rows x columns (X along M for 16 or 32 input
+// channels, the gradient along N for 48 input and 16 output channels)
+template <int CIN, int COUT>
+struct WzsPick {
+    static constexpr int PX = (CIN == 48 && COUT == 16) ? 1 : 3;
+};
+
 cudaError_t wgrad3x3(const WgradArgs &a, int cin, int sms, cudaStream_t s)
 {
 #define IAC_WG_CASE(CI, CO)                                               \
     if (cin == CI && a.cout == CO) {                                      \
         cudaError_t e = cudaSuccess;                                      \
-        if (a.slabs == 2 && launch_wgrad_tc<CI, CO>(a, sms, s, e)) return e; \
+        if (a.slabs == 3 && launch_wgrad_zs<CI, CO, WzsPick<CI, CO>::PX>(a, sms, s, e)) return e; \
+        if (a.slabs >= 2 && launch_wgrad_tc<CI, CO>(a, sms, s, e)) return e; \
         if (a.slabs >= 1 && launch_wgrad_slab<CI, CO>(a, sms, s, e)) return e; \
         return launch_wgrad<CI, CO>(a, sms, s);                           \
     }

@@ -64,9 +64,10 @@ def test_conv3x3_matches_oracle(ctx, rng, backend, c0, up0, c1, cout, dims):
     np.testing.assert_allclose(got, want, rtol=8e-3, atol=1e-5 * scale)
 
 
-@pytest.mark.parametrize("slabs", [2, 1, 0], ids=["tcgen05", "slabs", "per_tap"])
+@pytest.mark.parametrize("slabs", [3, 2, 1, 0], ids=["tcgen05_dz_stacked", "tcgen05", "slabs", "per_tap"])
 @pytest.mark.parametrize("c0,up0,c1,cout", [(0, 0, 16, 16), (0, 0, 16, 32), (0, 0, 32, 32), (0, 0, 32, 64),
-                                            (0, 0, 64, 64), (64, 1, 32, 32), (32, 1, 16, 16)])
+                                            (0, 0, 64, 64), (64, 1, 32, 32), (32, 1, 16, 16), (0, 0, 48, 16),
+                                            (0, 0, 96, 32)])
 @pytest.mark.parametrize("dims", [(2, 8, 12, 16), (1, 6, 10, 64)])
 def test_wgrad3x3_matches_oracle(ctx, rng, c0, up0, c1, cout, slabs, dims):
     import torch
