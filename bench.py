@@ -71,6 +71,10 @@ def parse():
                     help="edge of the square detector of the dense kernels (1024 = their config)")
     ap.add_argument("--backend", type=int, default=0,
                     help="denoiser convolutions: 0 = tcgen05 + TMEM, 1 = mma.sync")
+    ap.add_argument("--dn-batch", type=int, default=8,
+                    help="denoiser training patches per step (8 = the training configuration)")
+    ap.add_argument("--no-layers", action="store_true",
+                    help="--kernel denoise: skip timing every layer shape alone")
     ap.add_argument("--kernel", default="sparse",
                     choices=["sparse", "cq_small", "ac1d_cq", "cq_merge", "ac1d_sparse", "ac1d_uw", "simulate",
                              "denoise", "frames_to_error", "average"],
@@ -925,7 +929,7 @@ def run_kernel(args):
     elif k == "simulate":
         res = simulate_pipeline(args, ctx, stream, nthreads, steps=args.steps, warmup=args.warmup)
     elif k == "denoise":
-        res = denoise_bench(args, ctx, stream, nthreads, layers=True)
+        res = denoise_bench(args, ctx, stream, nthreads, layers=not args.no_layers)
     elif k == "frames_to_error":
         res = part_frames_to_error(args, ctx, stream)
     else:
@@ -957,7 +961,7 @@ def denoise_bench(args, ctx, stream, nthreads, layers=True):
     from incohautocorrelate_b200 import capi
     sp = stream.cuda_stream
     rng = np.random.default_rng(11)
-    B, P, E = 8, 64, 128
+    B, P, E = args.dn_batch, 64, 128
     dn = capi.Denoiser(ctx, B, P, P, P, backend=args.backend)
     parts = []
     for ci, co, _ in DENOISE_LAYERS:
@@ -1027,10 +1031,10 @@ def denoise_bench(args, ctx, stream, nthreads, layers=True):
     peak, peak_src = measured_bf16_tflops()
     tf_train = 2.0 * DENOISE_TRAIN_MACS * B * P ** 3 / (ms_train * 1e-3) / 1e12
     tf_fwd = 2.0 * DENOISE_FWD_MACS * E ** 3 / (ms_fwd * 1e-3) / 1e12
-    out = {"metric": "denoiser training voxels/s (8 x 64^3 patches, forward + backward + AdamW)",
+    out = {"metric": f"denoiser training voxels/s ({B} x 64^3 patches, forward + backward + AdamW)",
            "value": B * P ** 3 / (ms_train * 1e-3), "unit": "voxels/s", "ms_per_step": ms_train,
            "dtype": "bf16 operands, fp32 accumulation",
-           "config": {"workload": "3-level 3D U-Net 16/32/64, 3x3x3 convs, batch 8 x 64^3 (activations "
+           "config": {"workload": f"3-level 3D U-Net 16/32/64, 3x3x3 convs, batch {B} x 64^3 (activations "
                                   "> L2 per step)", "backend": ["tcgen05 slabs", "mma.sync", "tcgen05 per tap"][args.backend],
                       "params": capi.denoise_param_count(),
                       "train_flop_per_voxel": 2.0 * DENOISE_TRAIN_MACS,

@@ -168,7 +168,8 @@ iac_status iac_ctx_destroy(iac_ctx *ctx)
         if (ctx->d_counters) cudaFree(ctx->d_counters);
         for (auto &e : ctx->copy_events)
             if (e) cudaEventDestroy(e);
-        if (ctx->staging_free) cudaEventDestroy(ctx->staging_free);
+        for (auto &e : ctx->staging_free)
+            if (e) cudaEventDestroy(e);
         if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
         if (ctx->host_stream) cudaStreamDestroy(ctx->host_stream);
     }

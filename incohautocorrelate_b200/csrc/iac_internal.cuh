@@ -81,6 +81,9 @@ enum ScratchSlot {
     SLOT_FULL,
     SLOT_AUX0,
     SLOT_AUX1,
+    SLOT_PHOTONS2,    // second staging set of the host-buffer entry points
+    SLOT_OFFSETS2,
+    SLOT_ROT2,
     SLOT_COUNT
 };
 struct StreamScratch {
@@ -106,7 +109,8 @@ struct iac_ctx {
     cudaStream_t host_stream = nullptr;  // stream of the host-buffer entry points
     cudaStream_t copy_stream = nullptr;  // their host-to-device copies
     cudaEvent_t copy_events[IAC_COPY_CHUNKS + 1] = {};
-    cudaEvent_t staging_free = nullptr;  // recorded after the binning that read the host-entry staging
+    cudaEvent_t staging_free[2] = {};    // recorded after the binning that read host-entry staging set 0 / 1
+    int staging_set = 0;                 // the set the next host-entry call fills
     std::mutex host_mu;                  // one host-buffer entry point at a time (shared copy stream)
     void *static_scratch = nullptr;      // device address of iac_sparse_ac_batch_static's fixed array
     std::atomic<uint64_t> launches{0};

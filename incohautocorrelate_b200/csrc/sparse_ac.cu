@@ -1009,26 +1009,35 @@ static iac_status host_streams(iac_ctx *ctx)
     if (!ctx->copy_stream) IAC_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
     if (!ctx->copy_events[0])
         for (auto &e : ctx->copy_events) IAC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    if (!ctx->staging_free) IAC_CUDA(cudaEventCreateWithFlags(&ctx->staging_free, cudaEventDisableTiming));
+    if (!ctx->staging_free[0])
+        for (auto &e : ctx->staging_free) IAC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     return IAC_OK;
 }
 
 // Host photon lists -> device staging (scratch of `key`) -> pair kernel into
-// d_half on stream s.  The frames are cut into chunks by photon count; chunk
-// k+1 is copied on the copy stream while chunk k is binned.  Binning is
-// slower than the copy, so only the first chunk's copy is exposed: it is made
-// a quarter of the others (1/29 of the photons for 8 chunks).  Every chunk has
-// its own rebased offsets so it is an independent batch.  The copies wait for
-// the previous call's binning (staging_free), whose staging they overwrite.
+// d_half on stream s.  Two staging sets alternate between calls, so a call's
+// copies overlap the previous call's binning; each set is reused only after
+// the binning that read it (staging_free).  When the previous call's binning
+// is still running (a run of consecutive calls) the whole batch is copied
+// behind it and binned in one launch.  Otherwise the frames are cut into
+// chunks by photon count, chunk k+1 copied on the copy stream while chunk k
+// is binned; binning is slower than the copy, so only the first chunk's copy
+// is exposed: it is made a quarter of the others (1/29 of the photons for 8
+// chunks).  Every chunk has its own rebased offsets so it is an independent
+// batch.
 static iac_status stage_and_bin(iac_ctx *ctx, const float *h_photons, const uint64_t *h_off, const float *h_rot9,
                                 uint32_t nframes, const iac_sparse_params *p, uint64_t *d_half, cudaStream_t s,
                                 void *key)
 {
     iac_status st;
     cudaStream_t cs = ctx->copy_stream;
+    const int set = ctx->staging_set;
+    ctx->staging_set ^= 1;
+    const bool behind = cudaEventQuery(ctx->staging_free[set ^ 1]) == cudaErrorNotReady;
     const uint64_t o0 = h_off[0];
     const uint64_t nph = h_off[nframes] - o0;
-    const uint32_t nchunks = std::max<uint32_t>(1, std::min<uint32_t>(IAC_COPY_CHUNKS, nframes / 64));
+    const uint32_t nchunks =
+        behind ? 1u : std::max<uint32_t>(1, std::min<uint32_t>(IAC_COPY_CHUNKS, nframes / 64));
     std::vector<uint32_t> cut(nchunks + 1, 0);
     cut[nchunks] = nframes;
     const uint64_t parts = 4 * (uint64_t)nchunks - 3;  // chunk 0: 1 part, the others 4
@@ -1038,10 +1047,12 @@ static iac_status stage_and_bin(iac_ctx *ctx, const float *h_photons, const uint
         cut[k] = std::max(cut[k], cut[k - 1]);
     }
     void *d_ph, *d_off, *d_rot;
-    if ((st = stream_scratch(ctx, key, SLOT_PHOTONS, 16 * nph + 16, &d_ph)) != IAC_OK) return st;
-    if ((st = stream_scratch(ctx, key, SLOT_OFFSETS, 8 * ((size_t)nframes + nchunks + 1), &d_off)) != IAC_OK)
+    const int sp = set ? SLOT_PHOTONS2 : SLOT_PHOTONS, so = set ? SLOT_OFFSETS2 : SLOT_OFFSETS,
+              sr = set ? SLOT_ROT2 : SLOT_ROT;
+    if ((st = stream_scratch(ctx, key, sp, 16 * nph + 16, &d_ph)) != IAC_OK) return st;
+    if ((st = stream_scratch(ctx, key, so, 8 * ((size_t)nframes + IAC_COPY_CHUNKS + 1), &d_off)) != IAC_OK)
         return st;
-    if ((st = stream_scratch(ctx, key, SLOT_ROT, 36 * (size_t)nframes, &d_rot)) != IAC_OK) return st;
+    if ((st = stream_scratch(ctx, key, sr, 36 * (size_t)nframes, &d_rot)) != IAC_OK) return st;
     std::vector<uint64_t> off((size_t)nframes + nchunks);
     size_t w = 0;
     std::vector<size_t> off_pos(nchunks);
@@ -1055,10 +1066,8 @@ static iac_status stage_and_bin(iac_ctx *ctx, const float *h_photons, const uint
         const size_t tb = ((sizeof(unsigned long long) * ((size_t)nframes + 1) + 127) / 128) * 128;
         if ((st = stream_scratch(ctx, key, SLOT_TILES, tb + 128 + nframes, &t)) != IAC_OK) return st;
     }
-    // the previous call's copies are done (its host buffers may be reused by
-    // the caller) and its binning has read the staging these copies overwrite
-    IAC_CUDA(cudaStreamSynchronize(cs));
-    IAC_CUDA(cudaStreamWaitEvent(cs, ctx->staging_free, 0));
+    // the binning that last read this staging set is done before it is overwritten
+    IAC_CUDA(cudaStreamWaitEvent(cs, ctx->staging_free[set], 0));
     IAC_CUDA(cudaMemcpyAsync(d_off, off.data(), 8 * w, cudaMemcpyHostToDevice, cs));
     for (uint32_t k = 0; k < nchunks; k++) {
         const uint32_t f0 = cut[k], f1 = cut[k + 1];
@@ -1078,7 +1087,7 @@ static iac_status stage_and_bin(iac_ctx *ctx, const float *h_photons, const uint
             if (st != IAC_OK) return st;
         }
     }
-    IAC_CUDA(cudaEventRecord(ctx->staging_free, s));
+    IAC_CUDA(cudaEventRecord(ctx->staging_free[set], s));
     return IAC_OK;
 }
 
