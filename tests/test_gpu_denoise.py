@@ -223,31 +223,60 @@ def test_crop_patches_and_mesh_input(ctx, rng):
     np.testing.assert_array_equal(o32.cpu().numpy().reshape(4, 4, 4), want)
 
 
-def test_trained_denoiser_needs_fewer_frames_than_the_plain_mesh(ctx):
-    """The committed network (trained on 512 random crystals, 500 -> 50 000
-    frames) on held-out crystals it never saw: the denoised 500-frame mesh
-    against an independent 40 000-frame reference matches the plain mesh of
-    several times more frames (measured 13-26x, median 19x, on 32 crystals with
-    a 100 000-frame reference; this test asserts a median above 8x on four)."""
+def _frames_to_error(ctx, setup, n_crystals, plain, n_ref, seed):
     import os
 
-    import torch
     from incohautocorrelate_b200 import capi
     from incohautocorrelate_b200 import denoise as DN
     path = os.path.join(os.path.dirname(capi.__file__), "weights", "denoiser_128.npz")
     params, meta = DN.load_model(path)
-    setup = DN.SimSetup(**meta["setup"])
     sim = DN.MeshSimulator(ctx, setup)
     E = setup.crop
     dn = capi.Denoiser(ctx, 1, E, E, E)
     dn.set_params(params)
-    summary, rows = DN.evaluate(ctx, sim, dn, meta["norm"], 4, 500, [1000, 2000, 5000], 40000, seed=777,
-                                log=None)
+    summary, rows = DN.evaluate(ctx, sim, dn, meta["norm"], n_crystals, 500, plain, n_ref, seed=seed, log=None)
     assert ctx.check() == 0
+    dn.close()
+    return summary, rows
+
+
+def test_trained_denoiser_needs_fewer_frames_than_the_plain_mesh(ctx):
+    """The committed network (trained on 512 random crystals, 500 -> 50 000
+    frames) on held-out crystals it never saw: the denoised 500-frame mesh
+    against an independent 40 000-frame reference matches the plain mesh of
+    at least 10 times more frames (median over four crystals; measured
+    13-26x, median 19x, on 32 crystals with a 100 000-frame reference)."""
+    import os
+
+    from incohautocorrelate_b200 import capi
+    from incohautocorrelate_b200 import denoise as DN
+    _, meta = DN.load_model(os.path.join(os.path.dirname(capi.__file__), "weights", "denoiser_128.npz"))
+    summary, rows = _frames_to_error(ctx, DN.SimSetup(**meta["setup"]), 4, [1000, 2000, 5000], 40000, seed=777)
     for r in rows:
         assert r["err_denoised"] < 0.5 * r["err_plain"][500], r
-    assert summary["median_gain"] > 8.0, summary
-    dn.close()
+    assert summary["median_gain"] >= 10.0, summary
+
+
+def test_trained_denoiser_gain_holds_on_the_512_pixel_detector(ctx):
+    """The simulator configuration's detector -- 512 x 512 pixels of 75 um at
+    0.1 m, the same angular range and 129^3 mesh as the 128 x 128 x 0.3 mm
+    detector the network was trained on -- at the training's photon budget per
+    frame (328 photons: 0.02 per 0.3 mm pixel): the finer pixel grid changes the
+    k-vectors of every photon, and the denoised 500-frame mesh still needs at
+    least 10 times fewer frames than the plain mesh (median of three held-out
+    crystals against an independent 20 000-frame reference)."""
+    import os
+
+    from incohautocorrelate_b200 import capi
+    from incohautocorrelate_b200 import denoise as DN
+    _, meta = DN.load_model(os.path.join(os.path.dirname(capi.__file__), "weights", "denoiser_128.npz"))
+    base = DN.SimSetup(**meta["setup"])
+    setup = DN.SimSetup(**dict(meta["setup"], det=512, pitch=base.pitch * base.det / 512,
+                               photons_per_pixel=base.photons_per_pixel * (base.det / 512) ** 2, chunk=500))
+    summary, rows = _frames_to_error(ctx, setup, 3, [1000, 2000, 5000], 20000, seed=4242)
+    for r in rows:
+        assert r["err_denoised"] < 0.5 * r["err_plain"][500], r
+    assert summary["median_gain"] >= 10.0, summary
 
 
 def test_graph_replayed_training_matches_eager_steps(ctx, rng):
