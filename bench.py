@@ -999,7 +999,12 @@ def denoise_bench(args, ctx, stream, nthreads, layers=True):
     ms_graph = g0.elapsed_time(g1) / gsteps
     xf = torch.from_numpy(rng.gamma(2.0, 0.5, (1, E, E, E)).astype(np.float32)).cuda()
     of = torch.zeros_like(xf)
-    ms_fwd = _time(lambda: dn.forward(xf, 1, E, E, E, of, sp), args.steps, max(3, args.warmup), stream)
+    dn_inf = dn if B * P ** 3 >= E ** 3 else capi.Denoiser(ctx, 1, E, E, E, backend=args.backend)
+    if dn_inf is not dn:
+        dn_inf.set_params(dn.get_params())
+    ms_fwd = _time(lambda: dn_inf.forward(xf, 1, E, E, E, of, sp), args.steps, max(3, args.warmup), stream)
+    if dn_inf is not dn:
+        dn_inf.close()
     # every 3x3x3 shape alone on the training batch's volume at its level (the
     # decoder's concatenated inputs are materialised by the network, so every
     # layer reads one plain tensor)
@@ -1021,7 +1026,7 @@ def denoise_bench(args, ctx, stream, nthreads, layers=True):
         # the weight gradient of the same shape: tcgen05 (slabs 2) and mma.sync slabs (1)
         gq = torch.randn((nvox, co), device="cuda").to(torch.bfloat16).view(torch.int16)
         dw = torch.zeros((co, 27, ci), dtype=torch.float32, device="cuda")
-        for sl, name in ((2, "wgrad_tcgen05"), (1, "wgrad_mma_sync")):
+        for sl, name in ((3, "wgrad_tcgen05_dz"), (2, "wgrad_tcgen05"), (1, "wgrad_mma_sync")):
             ms = _time(lambda: capi.denoise_wgrad3x3(ctx, None, 0, 0, s1, ci, gq, co, B, edge, edge, edge, dw,
                                                      None, sp, slabs=sl), 10, 3, stream)
             row[name + "_ms"] = ms

@@ -2252,7 +2252,10 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_tc_kernel(const __grid_const
 // the in-plane tap t = 3 (dy + 1) + dx + 1 and accumulates its (M x N) block
 // in TMEM for the whole launch.  Stages of every (item, plane, tile) are
 // independent (planes outside the volume arrive as zeros), so the CTAs are
-// persistent over all tiles.
+// persistent over all tiles.  The bias gradient comes with it: the first of
+// the padding rows of A is an 8-channel plane of ones, written once into every
+// stage slot, so its accumulator row holds sum_v G[v][co] (the gradient is
+// zero at the padded positions).
 // --------------------------------------------------------------------------
 template <int CIN, int COUT, int PX>
 struct WzsCfg {
@@ -2286,6 +2289,13 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_const
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t sbase = smem_u32(smem);
     const uint32_t xbytes = (uint32_t)Z::XPLANES * g.planeX;
+    static_assert(Z::XPLANES > Z::XREAL, "a padding plane of A carries the ones of the bias gradient");
+    // the ones plane of every stage slot (never written by the loads)
+    for (int k = 0; k < g.S; k++) {
+        uint4 *ones = reinterpret_cast<uint4 *>(smem + (size_t)k * g.stage_bytes + (size_t)Z::XREAL * g.planeX);
+        for (uint32_t i = tid; i < g.planeX / 16; i += blockDim.x) ones[i] = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);
+    }
+    fence_proxy_async();  // written by threads, read by the tensor core
     if (tid == 0) {
         for (int k = 0; k < g.S; k++) {
             mbar_init(smem_u32(&full[k]), 1);
@@ -2389,6 +2399,13 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_const
             tmem_wait_ld();
             const int t = blk / MB, mb = blk % MB;
             const int m = mb * MR + row;
+            if (a.db && t == 4 && row >= 0 && m == Z::XREAL * 8) {  // the ones row: sum_v G[v][co]
+#pragma unroll
+                for (int co = 0; co < COUT; co++) {
+                    const float v = __uint_as_float(r[PX == 3 ? co : COUT + co]);  // PX = 1: the plane-z block
+                    if (v != 0.0f) atomicAdd(&a.db[co], v);
+                }
+            }
             if (row >= 0 && m < Z::MROWS) {
                 if (PX == 3) {  // row (dz + 1) cin + ci, column co
                     const int tap = 9 * (m / CIN) + t, ci = m % CIN;
@@ -2572,13 +2589,7 @@ static bool launch_wgrad_zs(const WgradArgs &a, int sms, cudaStream_t s, cudaErr
         if (err != cudaSuccess) return true;
         const long long grid = std::min<long long>(g.ntiles, (long long)per_sm * std::max(1, sms));
         wgrad_zs_kernel<CIN, COUT, PX><<<(unsigned)grid, 32 * (5 + 9), smem, s>>>(maps[0], maps[1], a, g);
-        if ((err = cudaGetLastError()) != cudaSuccess) return true;
-        if (a.db) {
-            const int lanes = 256 / COUT;
-            const long long blocks = std::min<long long>((a.V + lanes - 1) / lanes, 4LL * std::max(1, sms));
-            bias_grad_kernel<<<(unsigned)blocks, lanes * COUT, lanes * COUT * sizeof(float), s>>>(a.g, COUT, a.V, a.db);
-            err = cudaGetLastError();
-        }
+        err = cudaGetLastError();  // the kernel also adds the bias gradient (its ones row)
         return true;
     }
 }
