@@ -255,6 +255,30 @@ __device__ __forceinline__ void load_weights(uint32_t sB, const bf16 *w, int tap
     for (int i = tid; i < COUT * CIN / 8; i += CONV_THREADS) cp_async16(sB + i * 16, src + i * 8, 16);
 }
 
+// epilogue for one output row segment of 8 channels with the bias already in
+// registers (b: channels c .. c+7): ReLU, bf16 (+fp32)
+__device__ __forceinline__ void store8_b(const ConvArgs &a, int cout, long long v, int c, const float *val,
+                                         const float *b)
+{
+    float o[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const float t = val[j] + b[j];
+        o[j] = a.relu ? fmaxf(t, 0.0f) : t;
+    }
+    uint4 pk;
+    pk.x = pack_bf16(o[0], o[1]);
+    pk.y = pack_bf16(o[2], o[3]);
+    pk.z = pack_bf16(o[4], o[5]);
+    pk.w = pack_bf16(o[6], o[7]);
+    *reinterpret_cast<uint4 *>(a.y + v * cout + c) = pk;
+    if (a.y32) {
+        float4 *d = reinterpret_cast<float4 *>(a.y32 + v * cout + c);
+        d[0] = make_float4(o[0], o[1], o[2], o[3]);
+        d[1] = make_float4(o[4], o[5], o[6], o[7]);
+    }
+}
+
 // epilogue for one output row segment of 8 channels: bias, ReLU, bf16 (+fp32)
 __device__ __forceinline__ void store8(const ConvArgs &a, int cout, long long v, int c, const float *val)
 {
@@ -1169,17 +1193,26 @@ __global__ void __launch_bounds__(256, 1) conv_zcol_kernel(const __grid_constant
 // planes: stage k (input plane p = z0 - 1 + k) writes the partial sums
 // P_k = A_p x Bcat into TMEM region k % NB, whose block b (dz = b - 1) belongs
 // to output plane p + 1 - b.  Output z0 + ol is P_ol[block 0] + P_ol+1[block 1]
-// + P_ol+2[block 2], complete once stage ol + 2 is; the epilogue adds the three
-// blocks in the order (dz -1) + (dz 0), then + (dz +1), and frees region ol.
-// NISS issuing warps take the stages in turn (a tcgen05.mma occupies its
-// issuing thread for longer than the tensor pipe needs for it); the regions
-// rotate over NB >= 3 buffers, NB - 3 stages of slack between issue and drain.
-// The concatenated weights (27 cin cout bf16) are built in shared memory by all
-// threads at the start, from the [tap][cin/8][cout][8] tiles.
+// + P_ol+2[block 2], complete once stages ol .. ol + 2 are; the epilogue adds
+// the three blocks in the order (dz -1) + (dz 0), then + (dz +1).
+// Roles: warps 0-7 drain in two groups of four (group g takes the outputs
+// ol = g mod 2, each warp the 32 TMEM lanes of its quadrant, the bias in
+// registers), warp 8 loads slabs by TMA, warps 9 .. 8 + NISS issue the MMAs of
+// the stages in turn (a tcgen05.mma occupies its issuing thread for longer
+// than the tensor pipe needs for it).  A region is reused once both groups
+// are done with it: after output ol a group frees the regions of stages ol and
+// ol + 1 (its next output starts at stage ol + 2), and at the end of a work
+// item the stages it never read.  The regions rotate over NB >= 3 buffers.
+// The concatenated weights (27 cin cout bf16) are built in shared memory by
+// all threads at the start, from the [tap][cin/8][cout][8] tiles.
 // --------------------------------------------------------------------------
-template <int CIN, int COUT, int NB, int NISS>
-__global__ void __launch_bounds__(32 * (5 + NISS), 1) conv_zcat_kernel(const __grid_constant__ CUtensorMap xmap,
-                                                                      const ConvArgs a, const TmaGeom g)
+constexpr int ZCAT_EPI_WARPS = 8;
+constexpr int ZCAT_PRODUCER = 8;  // warp index of the TMA producer
+constexpr int ZCAT_ISSUER0 = 9;   // first MMA-issuing warp
+
+template <int CIN, int COUT, int NB, int NISS, int MINB>
+__global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
+    conv_zcat_kernel(const __grid_constant__ CUtensorMap xmap, const ConvArgs a, const TmaGeom g)
 {
     constexpr int N3 = 3 * COUT;
     constexpr uint32_t TCOLS = tma_tcols(NB * N3);
@@ -1214,14 +1247,14 @@ __global__ void __launch_bounds__(32 * (5 + NISS), 1) conv_zcat_kernel(const __g
         }
         for (int b = 0; b < NB; b++) {
             mbar_init(smem_u32(&accfull[b]), 1);
-            mbar_init(smem_u32(&accempty[b]), 4);
+            mbar_init(smem_u32(&accempty[b]), ZCAT_EPI_WARPS);  // both drain groups
         }
         fence_mbar_init();
         s_err = 0;
         s_issued = 0;
         for (int i = 0; i < NISS; i++) s_last[i] = -1;
     }
-    if (warp == 5) {
+    if (warp == ZCAT_PRODUCER) {
         tmem_alloc(smem_u32(&s_tmem), TCOLS);
         tmem_relinquish();
     }
@@ -1239,8 +1272,8 @@ __global__ void __launch_bounds__(32 * (5 + NISS), 1) conv_zcat_kernel(const __g
         q0 = (int)(col % g.T) * TILE_M;
     };
 
-    if (warp == 4) {
-        if (lane == 0) {  // producer: one slab per input plane z0-1 .. z1 (planes outside the volume arrive as zeros)
+    if (warp == ZCAT_PRODUCER) {
+        if (lane == 0) {  // one slab per input plane z0-1 .. z1 (planes outside the volume arrive as zeros)
             long long j = 0;
             bool ok = true;
             for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
@@ -1263,8 +1296,8 @@ __global__ void __launch_bounds__(32 * (5 + NISS), 1) conv_zcat_kernel(const __g
                 }
             }
         }
-    } else if (warp >= 5) {
-        const int iw = warp - 5;  // stages j with j % NISS == iw
+    } else if (warp >= ZCAT_ISSUER0) {
+        const int iw = warp - ZCAT_ISSUER0;  // stages j with j % NISS == iw
         if (lane == 0) {
             long long j = 0;
             bool ok = true;
@@ -1301,26 +1334,39 @@ __global__ void __launch_bounds__(32 * (5 + NISS), 1) conv_zcat_kernel(const __g
                 }
             }
         }
-    } else {  // epilogue: warps 0-3 own TMEM lanes 32w .. 32w+31
-        long long j = 0, waited = 0;  // this CTA's stages so far / stages whose MMAs are known complete
+    } else {  // drain: group grp = warp / 4 takes outputs ol = grp mod 2; warp % 4 = its TMEM quadrant
+        const int grp = warp >> 2, quad = warp & 3;
+        const int row = quad * 32 + lane;  // this thread's position in the tile
+        float bias[COUT];
+#pragma unroll
+        for (int c = 0; c < COUT; c++) bias[c] = a.bias ? a.bias[c] : 0.0f;
+        const uint32_t lb = tmem + ((uint32_t)(quad * 32) << 16);
+        auto release = [&](long long stage) {  // this warp is done with the region of `stage`
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&accempty[stage % NB]));
+        };
+        long long j = 0;  // this CTA's stages before the current item
         bool ok = true;
         for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
             int n, q0, z0, z1;
             item(it, n, q0, z0, z1);
             const int nz = z1 - z0;
-            const int q = q0 + tid;
+            const int q = q0 + row;
             const int y = q / g.Wp, xp = q - (q / g.Wp) * g.Wp;
             const bool valid = y < a.H && xp >= 1 && xp <= a.W;
-            for (int ol = 0; ok && ol < nz; ol++) {
-                for (; waited <= j + ol + 2; waited++)
-                    if (!mbar_wait_flag(smem_u32(&accfull[waited % NB]), (uint32_t)((waited / NB) & 1), &s_err)) {
+            // stages this group never reads: those before its first output
+            for (int k = 0; k < grp && k < nz + 2; k++) release(j + k);
+            int last = -1;  // this group's last output of the item
+            for (int ol = grp; ok && ol < nz; ol += 2) {
+                for (int k = 0; k < 3; k++)
+                    if (!mbar_wait_flag(smem_u32(&accfull[(j + ol + k) % NB]), (uint32_t)(((j + ol + k) / NB) & 1),
+                                        &s_err)) {
                         ok = false;
                         break;
                     }
                 if (!ok) break;
                 tc_fence_after();
                 uint32_t rr[COUT];
-                const uint32_t lb = tmem + ((uint32_t)(warp * 32) << 16);
                 const uint32_t c0 = (uint32_t)(((j + ol) % NB) * N3);
                 const uint32_t c1 = (uint32_t)(((j + ol + 1) % NB) * N3 + COUT);
                 const uint32_t c2 = (uint32_t)(((j + ol + 2) % NB) * N3 + 2 * COUT);
@@ -1338,8 +1384,9 @@ __global__ void __launch_bounds__(32 * (5 + NISS), 1) conv_zcat_kernel(const __g
                                                            __uint_as_float(r2[jj])));
                 }
                 tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(smem_u32(&accempty[(j + ol) % NB]));  // stage ol's last reader
+                release(j + ol);  // the next output of this group starts at stage ol + 2
+                release(j + ol + 1);
+                last = ol;
                 if (valid) {
                     const long long v = ((long long)n * a.D + z0 + ol) * HW + (long long)y * a.W + (xp - 1);
 #pragma unroll
@@ -1347,17 +1394,13 @@ __global__ void __launch_bounds__(32 * (5 + NISS), 1) conv_zcat_kernel(const __g
                         float f[8];
 #pragma unroll
                         for (int jj = 0; jj < 8; jj++) f[jj] = __uint_as_float(rr[c + jj]);
-                        store8(a, COUT, v, c, f);
+                        store8_b(a, COUT, v, c, f, bias + c);
                     }
                 }
             }
             if (!ok) break;
-            // the item's last two stages feed outputs past z1 only: their regions are free now
-            __syncwarp();
-            if (lane == 0) {
-                mbar_arrive(smem_u32(&accempty[(j + nz) % NB]));
-                mbar_arrive(smem_u32(&accempty[(j + nz + 1) % NB]));
-            }
+            // the stages after this group's last output (or all but the first grp if it had none)
+            for (int k = last >= 0 ? last + 2 : grp; k < nz + 2; k++) release(j + k);
             j += nz + 2;
         }
     }
@@ -1376,7 +1419,7 @@ __global__ void __launch_bounds__(32 * (5 + NISS), 1) conv_zcat_kernel(const __g
         }
         __syncthreads();
     }
-    if (warp == 5) {
+    if (warp == ZCAT_PRODUCER) {
         tc_fence_after();
         tmem_dealloc(tmem, TCOLS);
     }
@@ -1514,16 +1557,28 @@ static bool launch_zcat(const ConvArgs &a, const TmaGeom &g0, const CUtensorMap 
         g.S = S;
         const long long nb = a.V / ((long long)a.D * a.H * a.W);
         const long long grid_max = (long long)per_sm * std::max(1, a.sms);
-        int ZC = a.D;  // output planes per work item: the whole depth unless that leaves SMs idle
-        while (ZC > 4 && nb * g.T * ((a.D + ZC - 1) / ZC) < 2 * grid_max) ZC = (ZC + 1) / 2;
+        // output planes per work item: a work item of ZC outputs takes ZC + 2 stages (every
+        // stage costs the same MMAs), and the CTAs run ceil(items / grid) rounds of them:
+        // the depth split with the fewest stages on the busiest CTA
+        int ZC = a.D;
+        long long best = -1;
+        for (int zc = a.D; zc >= 1; zc = zc > 1 ? (zc + 1) / 2 : 0) {
+            const long long items = nb * g.T * ((a.D + zc - 1) / zc);
+            const long long cost = ((items + grid_max - 1) / grid_max) * (zc + 2);
+            if (best < 0 || cost < best) {
+                best = cost;
+                ZC = zc;
+            }
+            if (zc == 1) break;
+        }
         g.ZC = ZC;
         g.nitems = nb * g.T * ((a.D + ZC - 1) / ZC);
         const uint32_t smem = g.wres_bytes + (uint32_t)S * g.stage_bytes;
-        auto k = conv_zcat_kernel<CIN, COUT, Z::NB, Z::NISS>;
+        auto k = conv_zcat_kernel<CIN, COUT, Z::NB, Z::NISS, Z::PER_SM>;
         err = smem_attributes(k, smem);
         if (err != cudaSuccess) return true;
         const long long grid = std::min<long long>(g.nitems, grid_max);
-        k<<<(unsigned)grid, 32 * (5 + Z::NISS), smem, s>>>(map, a, g);
+        k<<<(unsigned)grid, 32 * (ZCAT_ISSUER0 + Z::NISS), smem, s>>>(map, a, g);
         err = cudaGetLastError();
         return true;
     }
@@ -2064,6 +2119,7 @@ static bool launch_wgrad_slab(const WgradArgs &a, int sms, cudaStream_t s, cudaE
 // warps 0-3 drain TMEM.
 struct WTGeom {
     int Wp, NR, NRg, T;
+    int KT;                        // positions per tile (wgrad_zs_kernel; TILE_M elsewhere)
     long long ntiles;
     uint32_t planeX, planeG;       // one 8-channel chunk plane of X / of the gradient (128-aligned)
     uint32_t boxX, boxG;           // bytes one box delivers
@@ -2252,7 +2308,9 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_tc_kernel(const __grid_const
 // the in-plane tap t = 3 (dy + 1) + dx + 1 and accumulates its (M x N) block
 // in TMEM for the whole launch.  Stages of every (item, plane, tile) are
 // independent (planes outside the volume arrive as zeros), so the CTAs are
-// persistent over all tiles.  The bias gradient comes with it: the first of
+// persistent over all tiles; a tile is KT consecutive padded positions of a
+// plane (K = KT per stage: longer tiles stage fewer halo rows per position).
+// The bias gradient comes with it: the first of
 // the padding rows of A is an 8-channel plane of ones, written once into every
 // stage slot, so its accumulator row holds sum_v G[v][co] (the gradient is
 // zero at the padded positions).
@@ -2326,7 +2384,7 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_const
                     break;
                 const long long tile = blockIdx.x + k * (long long)gridDim.x;
                 const long long plane = tile / g.T;
-                const int q0 = (int)(tile % g.T) * TILE_M;
+                const int q0 = (int)(tile % g.T) * g.KT;
                 const int n = (int)(plane / a.D), z = (int)(plane % a.D);
                 const int y_lo = floor_div(q0 - g.Wp - 1, g.Wp), yg_lo = q0 / g.Wp;
                 const uint32_t st = sbase + (uint32_t)slot * g.stage_bytes;
@@ -2355,7 +2413,7 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_const
                 if (!mbar_wait_flag(smem_u32(&full[slot]), (uint32_t)((k / g.S) & 1), &s_err)) break;
                 tc_fence_after();
                 const long long tile = blockIdx.x + k * (long long)gridDim.x;
-                const int q0 = (int)(tile % g.T) * TILE_M;
+                const int q0 = (int)(tile % g.T) * g.KT;
                 const int rel = q0 - floor_div(q0 - g.Wp - 1, g.Wp) * g.Wp;
                 const int relg = q0 - (q0 / g.Wp) * g.Wp;
                 const int r0 = rel + (t / 3 - 1) * g.Wp + (t % 3 - 1);
@@ -2363,8 +2421,8 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_const
 #pragma unroll
                 for (int mb = 0; mb < MB; mb++) {
                     const uint32_t dcol = tmem + (uint32_t)((t * MB + mb) * N);
-#pragma unroll
-                    for (int ks = 0; ks < TILE_M / 16; ks++) {
+#pragma unroll 4
+                    for (int ks = 0; ks < g.KT / 16; ks++) {
                         const uint64_t da =
                             smem_desc(sX + (uint32_t)(mb * (MR / 8)) * g.planeX + (uint32_t)(r0 + 16 * ks) * 16, 128, g.planeX);
                         const uint64_t db = smem_desc(sG + (uint32_t)(relg + 16 * ks) * 16, 128, g.planeG);
@@ -2545,27 +2603,40 @@ static bool launch_wgrad_zs(const WgradArgs &a, int sms, cudaStream_t s, cudaErr
         if ((reinterpret_cast<uintptr_t>(a.src1) & 15) || (reinterpret_cast<uintptr_t>(a.g) & 15)) return false;
         WTGeom g{};
         g.Wp = a.W + 2;
-        g.NR = 3 + (130 + g.Wp - 1) / g.Wp;
-        g.NRg = 2 + (TILE_M + g.Wp - 1) / g.Wp;
-        if (g.NR > 256 || g.NRg > 256) return false;
-        g.T = (a.H * g.Wp + TILE_M - 1) / TILE_M;
         const long long nb = a.V / ((long long)a.D * a.H * a.W);
-        g.ntiles = nb * a.D * g.T;
-        g.boxX = 16u * (uint32_t)g.Wp * (uint32_t)g.NR;
-        g.boxG = 16u * (uint32_t)g.Wp * (uint32_t)g.NRg;
-        g.planeX = (g.boxX + 127u) & ~127u;
-        g.planeG = (g.boxG + 127u) & ~127u;
-        g.stage_bytes = (((uint32_t)Z::XPLANES * g.planeX + (uint32_t)Z::GPLANES * g.planeG) + 1023u) & ~1023u;
         const uint32_t budget = 227u * 1024u - 2048u;
-        int per_sm = std::min(2, (int)(512 / Z::TCOLS));
-        g.S = 0;
-        for (; per_sm >= 1; per_sm--) {
-            const uint32_t share = std::min<uint32_t>(budget, (228u * 1024u) / (uint32_t)per_sm - 2048u);
-            const int S = (int)std::min<uint32_t>(6u, share / g.stage_bytes);
-            if (S >= 2) {
-                g.S = S;
-                break;
+        // positions per tile: 256 (fewer halo rows staged per position) where two stages fit
+        // and the tiles still outnumber the CTAs twice, else 128; IAC_DENOISE_WGRAD_KT forces one
+        static const int kt_env = [] {
+            const char *e = getenv("IAC_DENOISE_WGRAD_KT");
+            return e ? atoi(e) : 0;
+        }();
+        int per_sm = 0;
+        for (int KT : {256, 128}) {
+            if (kt_env && KT != kt_env) continue;
+            g.KT = KT;
+            g.NR = 3 + (KT + 2 + g.Wp - 1) / g.Wp;
+            g.NRg = 2 + (KT + g.Wp - 1) / g.Wp;
+            if (g.NR > 256 || g.NRg > 256) continue;
+            g.T = (a.H * g.Wp + KT - 1) / KT;
+            g.ntiles = nb * a.D * g.T;
+            g.boxX = 16u * (uint32_t)g.Wp * (uint32_t)g.NR;
+            g.boxG = 16u * (uint32_t)g.Wp * (uint32_t)g.NRg;
+            g.planeX = (g.boxX + 127u) & ~127u;
+            g.planeG = (g.boxG + 127u) & ~127u;
+            g.stage_bytes = (((uint32_t)Z::XPLANES * g.planeX + (uint32_t)Z::GPLANES * g.planeG) + 1023u) & ~1023u;
+            g.S = 0;
+            const int min_stages = 2;
+            for (per_sm = std::min(2, (int)(512 / Z::TCOLS)); per_sm >= 1; per_sm--) {
+                const uint32_t share = std::min<uint32_t>(budget, (228u * 1024u) / (uint32_t)per_sm - 2048u);
+                const int S = (int)std::min<uint32_t>(6u, share / g.stage_bytes);
+                if (S >= min_stages) {
+                    g.S = S;
+                    break;
+                }
             }
+            if (g.S >= min_stages && g.ntiles >= 2LL * per_sm * std::max(1, sms)) break;
+            g.S = 0;
         }
         if (g.S < 2 || g.ntiles == 0) return false;
         const uint32_t smem = (uint32_t)g.S * g.stage_bytes;
