@@ -139,11 +139,14 @@ ConvArgs conv_args(iac_denoiser *dn, int l, const bf16 *src0, const bf16 *src1, 
     return a;
 }
 
-// data gradient of layer l: G (cout channels) -> dX (cin channels)
+// data gradient of layer l: G (cout channels) -> dX (cin channels); with
+// relu_y (the forward activation dX belongs to) the ReLU derivative is applied
+// in the same kernel: dX = 0 where relu_y <= 0
 iac_status dgrad(iac_denoiser *dn, int l, const bf16 *gp, bf16 *out, int D, int H, int W, long long V,
-                 cudaStream_t s)
+                 cudaStream_t s, const bf16 *relu_y = nullptr)
 {
     ConvArgs a{};
+    a.mask_y = relu_y;
     a.src1 = gp;
     a.c1 = SPECS[l].cout;
     a.w = dn->wd + dn->wd_off[l];
@@ -303,45 +306,40 @@ iac_status run_backward(iac_denoiser *dn, const float *d_in, const float *d_targ
     DN_CHECK(head(h, dn->ctx->sm_count, s), "denoiser head");
     // layer 9: X = d1a
     if ((st = wgrad(dn, 9, nullptr, dn->d1a, dn->gA, D, H, W, V, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 9, dn->gA, dn->gB, D, H, W, V, s)) != IAC_OK) return st;
-    DN_CHECK(relu_mask(dn->gB, dn->d1a, dn->gB, V * 16, s), "mask 8");
+    if ((st = dgrad(dn, 9, dn->gA, dn->gB, D, H, W, V, s, dn->d1a)) != IAC_OK) return st;
     // layer 8: X = up(d2b) ++ s1
     if ((st = wgrad(dn, 8, nullptr, dn->cat1, dn->gB, D, H, W, V, s)) != IAC_OK) return st;
     if ((st = dgrad(dn, 8, dn->gB, dn->gcat1, D, H, W, V, s)) != IAC_OK) return st;
     DN_CHECK(split_concat_grad(dn->gcat1, 32, 16, dn->d2b, dn->hA, dn->gskip1, D, H, W, nb, s), "split 1");
     // layer 7: X = d2a
     if ((st = wgrad(dn, 7, nullptr, dn->d2a, dn->hA, D2, H2, W2, V2, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 7, dn->hA, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
-    DN_CHECK(relu_mask(dn->hB, dn->d2a, dn->hB, V2 * 32, s), "mask 6");
+    if ((st = dgrad(dn, 7, dn->hA, dn->hB, D2, H2, W2, V2, s, dn->d2a)) != IAC_OK) return st;
     // layer 6: X = up(b2) ++ s2
     if ((st = wgrad(dn, 6, nullptr, dn->cat2, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
     if ((st = dgrad(dn, 6, dn->hB, dn->gcat2, D2, H2, W2, V2, s)) != IAC_OK) return st;
     DN_CHECK(split_concat_grad(dn->gcat2, 64, 32, dn->b2, dn->qA, dn->gskip2, D2, H2, W2, nb, s), "split 2");
     // layer 5: X = b1
     if ((st = wgrad(dn, 5, nullptr, dn->b1, dn->qA, D4, H4, W4, V4, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 5, dn->qA, dn->qB, D4, H4, W4, V4, s)) != IAC_OK) return st;
-    DN_CHECK(relu_mask(dn->qB, dn->b1, dn->qB, V4 * 64, s), "mask 4");
+    if ((st = dgrad(dn, 5, dn->qA, dn->qB, D4, H4, W4, V4, s, dn->b1)) != IAC_OK) return st;
     // layer 4: X = p2
     if ((st = wgrad(dn, 4, nullptr, dn->p2, dn->qB, D4, H4, W4, V4, s)) != IAC_OK) return st;
     if ((st = dgrad(dn, 4, dn->qB, dn->qA, D4, H4, W4, V4, s)) != IAC_OK) return st;  // d p2 (32 ch)
     DN_CHECK(pool_grad_mask(dn->gskip2, dn->qA, dn->s2, dn->hA, 32, D2, H2, W2, nb, s), "pool grad 2");
     // layer 3: X = e2a
     if ((st = wgrad(dn, 3, nullptr, dn->e2a, dn->hA, D2, H2, W2, V2, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 3, dn->hA, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
-    DN_CHECK(relu_mask(dn->hB, dn->e2a, dn->hB, V2 * 32, s), "mask 2");
+    if ((st = dgrad(dn, 3, dn->hA, dn->hB, D2, H2, W2, V2, s, dn->e2a)) != IAC_OK) return st;
     // layer 2: X = p1
     if ((st = wgrad(dn, 2, nullptr, dn->p1, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
     if ((st = dgrad(dn, 2, dn->hB, dn->hA, D2, H2, W2, V2, s)) != IAC_OK) return st;  // d p1 (16 ch)
     DN_CHECK(pool_grad_mask(dn->gskip1, dn->hA, dn->s1, dn->gA, 16, D, H, W, nb, s), "pool grad 1");
     // layer 1: X = e1a
     if ((st = wgrad(dn, 1, nullptr, dn->e1a, dn->gA, D, H, W, V, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 1, dn->gA, dn->gB, D, H, W, V, s)) != IAC_OK) return st;
-    DN_CHECK(relu_mask(dn->gB, dn->e1a, dn->gB, V * 16, s), "mask 0");
+    if ((st = dgrad(dn, 1, dn->gA, dn->gB, D, H, W, V, s, dn->e1a)) != IAC_OK) return st;
     // layer 0: X = input
     DN_CHECK(wgrad3x3_first(d_in, dn->gB, dn->g + dn->p_off[0], dn->g + dn->p_off[0] + 16 * 27, D, H, W, V,
                             dn->ctx->sm_count, s),
              "layer 0 weight gradient");
-    dn->ctx->launches += 50;
+    dn->ctx->launches += 45;
     return IAC_OK;
 }
 
@@ -667,7 +665,7 @@ iac_status iac_denoise_train_steps(iac_denoiser *dn, const uint16_t *d_in_meshes
         DN_CHECK(cudaStreamWaitEvent(caller, dn->own_ev[1], 0), "order replay");
     }
     dn->adam_step += nsteps;
-    dn->ctx->launches += (uint64_t)nsteps * 54;
+    dn->ctx->launches += (uint64_t)nsteps * 49;
     return IAC_OK;
 }
 

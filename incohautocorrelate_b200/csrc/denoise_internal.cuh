@@ -37,6 +37,7 @@ struct ConvArgs {
     bf16 *y;             // [V][cout]
     float *y32;          // optional fp32 copy of the output
     int relu;
+    const bf16 *mask_y;  // optional [V][cout]: outputs where mask_y <= 0 are set to 0 (ReLU derivative)
     int D, H, W;         // output (= src1) dims per batch item
     long long V;         // nb * D * H * W
     DeviceCounters *counters;

@@ -255,6 +255,20 @@ __device__ __forceinline__ void load_weights(uint32_t sB, const bf16 *w, int tap
     for (int i = tid; i < COUT * CIN / 8; i += CONV_THREADS) cp_async16(sB + i * 16, src + i * 8, 16);
 }
 
+// o[j] = 0 where the forward activation y (8 bf16 at y8) is not positive: the
+// ReLU derivative applied to a data gradient in the epilogue that produces it
+__device__ __forceinline__ void mask8(const bf16 *y8, float *o)
+{
+    const uint4 raw = *reinterpret_cast<const uint4 *>(y8);
+    const uint32_t w[4] = {raw.x, raw.y, raw.z, raw.w};
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        // a bf16 is positive when its sign bit is clear and it is not +0
+        if ((w[j] & 0x8000u) || !(w[j] & 0x7FFFu)) o[2 * j] = 0.0f;
+        if ((w[j] & 0x80000000u) || !(w[j] & 0x7FFF0000u)) o[2 * j + 1] = 0.0f;
+    }
+}
+
 // epilogue for one output row segment of 8 channels with the bias already in
 // registers (b: channels c .. c+7): ReLU, bf16 (+fp32)
 __device__ __forceinline__ void store8_b(const ConvArgs &a, int cout, long long v, int c, const float *val,
@@ -266,6 +280,7 @@ __device__ __forceinline__ void store8_b(const ConvArgs &a, int cout, long long 
         const float t = val[j] + b[j];
         o[j] = a.relu ? fmaxf(t, 0.0f) : t;
     }
+    if (a.mask_y) mask8(a.mask_y + v * cout + c, o);
     uint4 pk;
     pk.x = pack_bf16(o[0], o[1]);
     pk.y = pack_bf16(o[2], o[3]);
@@ -288,6 +303,7 @@ __device__ __forceinline__ void store8(const ConvArgs &a, int cout, long long v,
         float t = val[j] + (a.bias ? a.bias[c + j] : 0.0f);
         o[j] = a.relu ? fmaxf(t, 0.0f) : t;
     }
+    if (a.mask_y) mask8(a.mask_y + v * cout + c, o);
     uint4 pk;
     pk.x = pack_bf16(o[0], o[1]);
     pk.y = pack_bf16(o[2], o[3]);
@@ -495,6 +511,11 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_mma_kernel(const ConvArgs a
                 if (a.relu) {
                     o0 = fmaxf(o0, 0.0f);
                     o1 = fmaxf(o1, 0.0f);
+                }
+                if (a.mask_y) {  // ReLU derivative: 0 where the forward activation is not positive
+                    const uint32_t w = *reinterpret_cast<const uint32_t *>(a.mask_y + v * COUT + c);
+                    if ((w & 0x8000u) || !(w & 0x7FFFu)) o0 = 0.0f;
+                    if ((w & 0x80000000u) || !(w & 0x7FFF0000u)) o1 = 0.0f;
                 }
                 *reinterpret_cast<uint32_t *>(a.y + v * COUT + c) = pack_bf16(o0, o1);
                 if (a.y32) *reinterpret_cast<float2 *>(a.y32 + v * COUT + c) = make_float2(o0, o1);
@@ -1574,11 +1595,24 @@ static bool launch_zcat(const ConvArgs &a, const TmaGeom &g0, const CUtensorMap 
         g.ZC = ZC;
         g.nitems = nb * g.T * ((a.D + ZC - 1) / ZC);
         const uint32_t smem = g.wres_bytes + (uint32_t)S * g.stage_bytes;
-        auto k = conv_zcat_kernel<CIN, COUT, Z::NB, Z::NISS, Z::PER_SM>;
-        err = smem_attributes(k, smem);
-        if (err != cudaSuccess) return true;
+        // IAC_DENOISE_ZCAT_ISS=3 runs three issuing warps where two are the default (for
+        // comparing the issue rates)
+        static const bool iss3 = [] {
+            const char *e = getenv("IAC_DENOISE_ZCAT_ISS");
+            return e && e[0] == '3';
+        }();
         const long long grid = std::min<long long>(g.nitems, grid_max);
-        k<<<(unsigned)grid, 32 * (ZCAT_ISSUER0 + Z::NISS), smem, s>>>(map, a, g);
+        if (Z::NISS == 2 && iss3) {
+            auto k = conv_zcat_kernel<CIN, COUT, Z::NB, 3, Z::PER_SM>;
+            err = smem_attributes(k, smem);
+            if (err != cudaSuccess) return true;
+            k<<<(unsigned)grid, 32 * (ZCAT_ISSUER0 + 3), smem, s>>>(map, a, g);
+        } else {
+            auto k = conv_zcat_kernel<CIN, COUT, Z::NB, Z::NISS, Z::PER_SM>;
+            err = smem_attributes(k, smem);
+            if (err != cudaSuccess) return true;
+            k<<<(unsigned)grid, 32 * (ZCAT_ISSUER0 + Z::NISS), smem, s>>>(map, a, g);
+        }
         err = cudaGetLastError();
         return true;
     }
