@@ -1338,14 +1338,18 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
                     tc_fence_after();
                     const uint32_t st = stbase + (uint32_t)slot * g.stage_bytes;
                     const uint32_t dcol = tmem + (uint32_t)(r * N3);
-#pragma unroll 1
+                    // descriptors: the start-address field (16-byte units, low 14 bits) moves
+                    // by whole units from one MMA to the next and never leaves [0, 2^14), so
+                    // each is the stage's base descriptor plus a small (signed) offset
+                    const uint64_t da0 = smem_desc(st + (uint32_t)rel * 16, g.plane_bytes, 128);
+                    const uint64_t db0 = smem_desc(wbase, N3 * 16, 128);
+#pragma unroll
                     for (int t = 0; t < 9; t++) {
-                        const uint32_t r0 = (uint32_t)(rel + (t / 3 - 1) * g.Wp + (t % 3 - 1));
+                        const int64_t toff = (int64_t)((t / 3 - 1) * g.Wp + (t % 3 - 1));  // rows of 16 B
 #pragma unroll
                         for (int kk = 0; kk < CIN / 16; kk++) {
-                            const uint64_t da =
-                                smem_desc(st + (uint32_t)(2 * kk) * g.plane_bytes + r0 * 16, g.plane_bytes, 128);
-                            const uint64_t db = smem_desc(wbase + t * WT9_BYTES + kk * 2 * (N3 * 16), N3 * 16, 128);
+                            const uint64_t da = da0 + (uint64_t)(toff + (int64_t)((2 * kk * g.plane_bytes) >> 4));
+                            const uint64_t db = db0 + (uint64_t)((t * WT9_BYTES + kk * 2 * (N3 * 16)) >> 4);
                             umma_bf16(dcol, da, db, IDESC, (t > 0 || kk > 0) ? 1u : 0u);
                         }
                     }
@@ -2356,12 +2360,16 @@ struct WzsCfg {
     static constexpr int MR = MROWS > 64 ? 128 : 64;    // rows per MMA
     static constexpr int MB = (MROWS + MR - 1) / MR;    // M blocks
     static constexpr int N = PG * COUT;                 // MMA columns
-    static constexpr int COLS = 9 * N * MB;
+    // in-plane taps per CTA: all nine, or the fewest groups whose accumulators fit TMEM
+    static constexpr int NTG = 9 * N * MB <= 512 ? 1 : (5 * N * MB <= 512 ? 2 : (3 * N * MB <= 512 ? 3 : 9));
+    static constexpr int TPG = (9 + NTG - 1) / NTG;     // taps of a group (the last may have fewer)
+    static constexpr int COLS = TPG * N * MB;
     static constexpr uint32_t TCOLS = COLS <= 32 ? 32 : (COLS <= 64 ? 64 : (COLS <= 128 ? 128 : (COLS <= 256 ? 256 : 512)));
     static constexpr int XREAL = PX * CIN / 8;          // X chunk planes loaded
     static constexpr int XPLANES = MB * MR / 8;         // X chunk planes the MMAs read (padding rows: garbage)
     static constexpr int GPLANES = PG * COUT / 8;
-    static constexpr bool OK = COLS <= 512 && N <= 256 && N % (MR == 128 ? 16 : 8) == 0;
+    static constexpr bool OK = COLS <= 512 && N <= 256 && N % (MR == 128 ? 16 : 8) == 0 && XPLANES > XREAL &&
+                               NTG <= 3;
 };
 
 template <int CIN, int COUT, int PX>
@@ -2372,7 +2380,9 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_const
     using Z = WzsCfg<CIN, COUT, PX>;
     constexpr int MB = Z::MB, MR = Z::MR, N = Z::N;
     constexpr uint32_t IDESC = idesc_bf16(MR, N) | (1u << 15) | (1u << 16);  // A and B MN-major
-    constexpr int NI = 9;
+    constexpr int NI = Z::TPG;  // issuing warps: one per in-plane tap of this CTA's group
+    const int tg0 = (int)blockIdx.y * Z::TPG;                     // first in-plane tap of the group
+    const int ntap = 9 - tg0 < Z::TPG ? 9 - tg0 : Z::TPG;         // taps of the group
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t full[8], empty[8], done;
     __shared__ uint32_t s_tmem;
@@ -2391,9 +2401,9 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_const
     if (tid == 0) {
         for (int k = 0; k < g.S; k++) {
             mbar_init(smem_u32(&full[k]), 1);
-            mbar_init(smem_u32(&empty[k]), NI);  // one commit per issuing warp
+            mbar_init(smem_u32(&empty[k]), ntap);  // one commit per issuing warp
         }
-        mbar_init(smem_u32(&done), NI);
+        mbar_init(smem_u32(&done), ntap);
         fence_mbar_init();
         s_err = 0;
         s_issued = 0;
@@ -2439,8 +2449,8 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_const
                 s_issued = k + 1;
             }
         }
-    } else if (warp >= 5 && warp < 5 + NI) {
-        const int t = warp - 5;  // in-plane tap 3 (dy + 1) + dx + 1
+    } else if (warp >= 5 && warp < 5 + ntap) {
+        const int tl = warp - 5, t = tg0 + tl;  // in-plane tap 3 (dy + 1) + dx + 1
         if (lane == 0) {
             for (long long k = 0; k < my_tiles; k++) {
                 const int slot = (int)(k % g.S);
@@ -2452,19 +2462,20 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_const
                 const int relg = q0 - (q0 / g.Wp) * g.Wp;
                 const int r0 = rel + (t / 3 - 1) * g.Wp + (t % 3 - 1);
                 const uint32_t sX = sbase + (uint32_t)slot * g.stage_bytes, sG = sX + xbytes;
+                // descriptors advance by 16 positions (16 units of 16 B) per K step
+                const uint64_t db0 = smem_desc(sG + (uint32_t)relg * 16, 128, g.planeG);
 #pragma unroll
                 for (int mb = 0; mb < MB; mb++) {
-                    const uint32_t dcol = tmem + (uint32_t)((t * MB + mb) * N);
-#pragma unroll 4
-                    for (int ks = 0; ks < g.KT / 16; ks++) {
-                        const uint64_t da =
-                            smem_desc(sX + (uint32_t)(mb * (MR / 8)) * g.planeX + (uint32_t)(r0 + 16 * ks) * 16, 128, g.planeX);
-                        const uint64_t db = smem_desc(sG + (uint32_t)(relg + 16 * ks) * 16, 128, g.planeG);
-                        umma_bf16(dcol, da, db, IDESC, (k > 0 || ks > 0) ? 1u : 0u);
-                    }
+                    const uint32_t dcol = tmem + (uint32_t)((tl * MB + mb) * N);
+                    const uint64_t da0 = smem_desc(sX + (uint32_t)(mb * (MR / 8)) * g.planeX + (uint32_t)r0 * 16, 128, g.planeX);
+                    const int nks = g.KT / 16;
+#pragma unroll 8
+                    for (int ks = 0; ks < nks; ks++)
+                        umma_bf16(dcol, da0 + (uint64_t)(16 * ks), db0 + (uint64_t)(16 * ks), IDESC,
+                                  (k > 0 || ks > 0) ? 1u : 0u);
                 }
                 umma_commit(smem_u32(&empty[slot]));
-                s_consumed[t] = k + 1;
+                s_consumed[tl] = k + 1;
             }
             if (!s_err && my_tiles > 0) umma_commit(smem_u32(&done));
         }
@@ -2481,7 +2492,7 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_const
         // an M = 64 accumulator keeps row i in TMEM lane 32 (i / 16) + i % 16; M = 128: row i in lane i
         const int row = MR == 128 ? warp * 32 + lane : (lane < 16 ? warp * 16 + lane : -1);
 #pragma unroll 1
-        for (int blk = 0; blk < 9 * MB; blk++) {
+        for (int blk = 0; blk < ntap * MB; blk++) {
             uint32_t r[N];
 #pragma unroll
             for (int c = 0; c < N; c += 16) {
@@ -2489,7 +2500,7 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_const
                 tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(blk * N + c), rr);
             }
             tmem_wait_ld();
-            const int t = blk / MB, mb = blk % MB;
+            const int t = tg0 + blk / MB, mb = blk % MB;
             const int m = mb * MR + row;
             if (a.db && t == 4 && row >= 0 && m == Z::XREAL * 8) {  // the ones row: sum_v G[v][co]
 #pragma unroll
@@ -2521,7 +2532,7 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_const
     if (s_err && tid == 0) {
         if (a.counters) atomicAdd(&a.counters->timeouts, 1ull);
         long long consumed = s_consumed[0];
-        for (int i = 1; i < NI; i++) consumed = s_consumed[i] < consumed ? s_consumed[i] : consumed;
+        for (int i = 1; i < ntap; i++) consumed = s_consumed[i] < consumed ? s_consumed[i] : consumed;
         for (long long k = consumed; k < s_issued; k++)
             mbar_wait(smem_u32(&full[k % g.S]), (uint32_t)((k / g.S) & 1));
         if (consumed > 0) {
@@ -2692,8 +2703,11 @@ static bool launch_wgrad_zs(const WgradArgs &a, int sms, cudaStream_t s, cudaErr
         }
         err = smem_attributes(wgrad_zs_kernel<CIN, COUT, PX>, smem);
         if (err != cudaSuccess) return true;
-        const long long grid = std::min<long long>(g.ntiles, (long long)per_sm * std::max(1, sms));
-        wgrad_zs_kernel<CIN, COUT, PX><<<(unsigned)grid, 32 * (5 + 9), smem, s>>>(maps[0], maps[1], a, g);
+        // with tap groups every group stages the tiles again: fewer CTAs per group
+        const long long grid =
+            std::min<long long>(g.ntiles, ((long long)per_sm * std::max(1, sms) + Z::NTG - 1) / Z::NTG);
+        wgrad_zs_kernel<CIN, COUT, PX><<<dim3((unsigned)grid, Z::NTG), 32 * (5 + Z::TPG), smem, s>>>(maps[0], maps[1],
+                                                                                                 a, g);
         err = cudaGetLastError();  // the kernel also adds the bias gradient (its ones row)
         return true;
     }
@@ -2701,10 +2715,10 @@ static bool launch_wgrad_zs(const WgradArgs &a, int sms, cudaStream_t s, cudaErr
 
 // which operand carries the dz axis in wgrad_zs_kernel: the one whose three
 // planes give the fewer MMA rows x columns (X along M for 16 or 32 input
-// channels, the gradient along N for 48 input and 16 output channels)
+// channels, the gradient along N for 48 -> 16 and 96 -> 32)
 template <int CIN, int COUT>
 struct WzsPick {
-    static constexpr int PX = (CIN == 48 && COUT == 16) ? 1 : 3;
+    static constexpr int PX = ((CIN == 48 && COUT == 16) || (CIN == 96 && COUT == 32)) ? 1 : 3;
 };
 
 cudaError_t wgrad3x3(const WgradArgs &a, int cin, int sms, cudaStream_t s)
