@@ -1231,11 +1231,12 @@ constexpr int ZCAT_EPI_WARPS = 8;
 constexpr int ZCAT_PRODUCER = 8;  // warp index of the TMA producer
 constexpr int ZCAT_ISSUER0 = 9;   // first MMA-issuing warp
 
-template <int CIN, int COUT, int NB, int NISS, int MINB>
+template <int CIN, int COUT, int COUTH, int NB, int NISS, int MINB>
 __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
     conv_zcat_kernel(const __grid_constant__ CUtensorMap xmap, const ConvArgs a, const TmaGeom g)
 {
-    constexpr int N3 = 3 * COUT;
+    constexpr int N3 = 3 * COUTH;  // COUTH of the COUT output channels per CTA: blockIdx.y selects them
+    const int c_lo = (int)blockIdx.y * COUTH;
     constexpr uint32_t TCOLS = tma_tcols(NB * N3);
     static_assert(NB >= 3 && NB * N3 <= 512, "three regions in flight within 512 TMEM columns");
     static_assert(N3 % 16 == 0 && N3 <= 256, "M = 128 MMAs take N = 16 .. 256 in steps of 16");
@@ -1250,14 +1251,15 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
     const uint32_t sbase = smem_u32(smem);
     const uint32_t wbase = sbase;                   // concatenated weights [t9][cin/8][3 cout][8]
     const uint32_t stbase = sbase + g.wres_bytes;   // stages: one input-plane slab each
-    // Bcat(t9)[kc][dzi * COUT + co][8] = W(tap = 9 dzi + t9)[kc][co][8]
-    for (int i = tid; i < 27 * CIN * COUT / 8; i += blockDim.x) {
-        const int co = i % COUT;
-        int r = i / COUT;
+    // Bcat(t9)[kc][dzi * COUTH + co][8] = W(tap = 9 dzi + t9)[kc][c_lo + co][8]
+    for (int i = tid; i < 27 * CIN * COUTH / 8; i += blockDim.x) {
+        const int co = i % COUTH;
+        int r = i / COUTH;
         const int dzi = r % 3;
         r /= 3;
         const int kc = r % (CIN / 8), t9 = r / (CIN / 8);
-        const uint4 v = *reinterpret_cast<const uint4 *>(a.w + (((size_t)(9 * dzi + t9) * (CIN / 8) + kc) * COUT + co) * 8);
+        const uint4 v =
+            *reinterpret_cast<const uint4 *>(a.w + (((size_t)(9 * dzi + t9) * (CIN / 8) + kc) * COUT + c_lo + co) * 8);
         *reinterpret_cast<uint4 *>(smem + (size_t)i * 16) = v;
     }
     fence_proxy_async();  // the weights written by threads, read by the tensor core
@@ -1362,9 +1364,9 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
     } else {  // drain: group grp = warp / 4 takes outputs ol = grp mod 2; warp % 4 = its TMEM quadrant
         const int grp = warp >> 2, quad = warp & 3;
         const int row = quad * 32 + lane;  // this thread's position in the tile
-        float bias[COUT];
+        float bias[COUTH];
 #pragma unroll
-        for (int c = 0; c < COUT; c++) bias[c] = a.bias ? a.bias[c] : 0.0f;
+        for (int c = 0; c < COUTH; c++) bias[c] = a.bias ? a.bias[c_lo + c] : 0.0f;
         const uint32_t lb = tmem + ((uint32_t)(quad * 32) << 16);
         auto release = [&](long long stage) {  // this warp is done with the region of `stage`
             __syncwarp();
@@ -1391,12 +1393,12 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
                     }
                 if (!ok) break;
                 tc_fence_after();
-                uint32_t rr[COUT];
+                uint32_t rr[COUTH];
                 const uint32_t c0 = (uint32_t)(((j + ol) % NB) * N3);
-                const uint32_t c1 = (uint32_t)(((j + ol + 1) % NB) * N3 + COUT);
-                const uint32_t c2 = (uint32_t)(((j + ol + 2) % NB) * N3 + 2 * COUT);
+                const uint32_t c1 = (uint32_t)(((j + ol + 1) % NB) * N3 + COUTH);
+                const uint32_t c2 = (uint32_t)(((j + ol + 2) % NB) * N3 + 2 * COUTH);
 #pragma unroll
-                for (int c = 0; c < COUT; c += 16) {
+                for (int c = 0; c < COUTH; c += 16) {
                     uint32_t (&r0)[16] = *reinterpret_cast<uint32_t(*)[16]>(&rr[c]);
                     uint32_t r1[16], r2[16];
                     tmem_ld16(lb + c0 + (uint32_t)c, r0);
@@ -1415,11 +1417,11 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
                 if (valid) {
                     const long long v = ((long long)n * a.D + z0 + ol) * HW + (long long)y * a.W + (xp - 1);
 #pragma unroll
-                    for (int c = 0; c < COUT; c += 8) {
+                    for (int c = 0; c < COUTH; c += 8) {
                         float f[8];
 #pragma unroll
                         for (int jj = 0; jj < 8; jj++) f[jj] = __uint_as_float(rr[c + jj]);
-                        store8_b(a, COUT, v, c, f, bias + c);
+                        store8_b(a, COUT, v, c_lo + c, f, bias + c);
                     }
                 }
             }
@@ -1536,9 +1538,16 @@ static void launch_zcol_nb(const ConvArgs &a, TmaGeom g, const CUtensorMap &map,
 // regions (NB) and issuing warps (NISS) of the concatenated-dz z-column
 // kernel per output channel count: N = 3 cout columns per region, NB >= 3
 // regions within the TMEM allocation the CTAs of an SM share
-template <int COUT>
+template <int CIN, int COUT>
 struct ZcatCfg {
-    static constexpr int N3 = 3 * COUT;
+    // output channels per CTA: all of them, or a split where the concatenated
+    // weights of all would not stay resident in 96 KB (27 cin cout bf16) or N = 3 cout
+    // would pass 256 (96 -> 32: 16 per CTA; 32 -> 96: 48; 64 -> 64: 16)
+    static constexpr bool FITS_ALL = 3 * COUT <= 256 && CIN * COUT <= 1820;
+    static constexpr int COUTH = FITS_ALL ? COUT
+                                 : (COUT % 48 == 0 && CIN * 48 <= 1820) ? 48
+                                 : (COUT % 16 == 0 && CIN * 16 <= 1820) ? 16 : COUT;
+    static constexpr int N3 = 3 * COUTH;
     static constexpr int NB = 5 * N3 <= 256 ? 5 : (5 * N3 <= 512 ? 5 : (3 * N3 <= 512 ? 3 : 0));
     static constexpr int PER_SM = (int)(512 / tma_tcols(NB > 0 ? NB * N3 : 512));  // CTAs per SM by TMEM
     static constexpr int NISS = PER_SM >= 2 ? 2 : 3;
@@ -1552,8 +1561,8 @@ template <int CIN, int COUT>
 static bool launch_zcat(const ConvArgs &a, const TmaGeom &g0, const CUtensorMap &map, uint32_t budget,
                         cudaStream_t s, cudaError_t &err)
 {
-    using Z = ZcatCfg<COUT>;
-    if constexpr (Z::NB == 0 || 3 * COUT > 256) {
+    using Z = ZcatCfg<CIN, COUT>;
+    if constexpr (Z::NB == 0 || Z::N3 > 256 || COUT % Z::COUTH != 0) {
         return false;
     } else {
         static const bool off = [] {
@@ -1561,7 +1570,8 @@ static bool launch_zcat(const ConvArgs &a, const TmaGeom &g0, const CUtensorMap 
             return e && e[0] == '0';
         }();
         if (off) return false;
-        const uint32_t w27 = 27u * COUT * CIN * 2;
+        constexpr int NG = COUT / Z::COUTH;  // output-channel groups (blockIdx.y)
+        const uint32_t w27 = 27u * Z::COUTH * CIN * 2;
         if (w27 > 96u * 1024u) return false;
         TmaGeom g = g0;
         g.wcopy_bytes = w27;
@@ -1573,7 +1583,7 @@ static bool launch_zcat(const ConvArgs &a, const TmaGeom &g0, const CUtensorMap 
             const uint32_t share = std::min(budget, (228u * 1024u) / (uint32_t)want - 2048u);
             if (share <= g.wres_bytes) continue;
             const int st = (int)std::min<uint32_t>(8u, (share - g.wres_bytes) / g.stage_bytes);
-            if (st >= 4) {
+            if (st >= (NG > 1 ? 3 : 4)) {
                 per_sm = want;
                 S = st;
             }
@@ -1581,7 +1591,7 @@ static bool launch_zcat(const ConvArgs &a, const TmaGeom &g0, const CUtensorMap 
         if (per_sm == 0) return false;
         g.S = S;
         const long long nb = a.V / ((long long)a.D * a.H * a.W);
-        const long long grid_max = (long long)per_sm * std::max(1, a.sms);
+        const long long grid_max = ((long long)per_sm * std::max(1, a.sms) + NG - 1) / NG;  // per channel group
         // output planes per work item: a work item of ZC outputs takes ZC + 2 stages (every
         // stage costs the same MMAs), and the CTAs run ceil(items / grid) rounds of them:
         // the depth split with the fewest stages on the busiest CTA
@@ -1599,24 +1609,11 @@ static bool launch_zcat(const ConvArgs &a, const TmaGeom &g0, const CUtensorMap 
         g.ZC = ZC;
         g.nitems = nb * g.T * ((a.D + ZC - 1) / ZC);
         const uint32_t smem = g.wres_bytes + (uint32_t)S * g.stage_bytes;
-        // IAC_DENOISE_ZCAT_ISS=3 runs three issuing warps where two are the default (for
-        // comparing the issue rates)
-        static const bool iss3 = [] {
-            const char *e = getenv("IAC_DENOISE_ZCAT_ISS");
-            return e && e[0] == '3';
-        }();
         const long long grid = std::min<long long>(g.nitems, grid_max);
-        if (Z::NISS == 2 && iss3) {
-            auto k = conv_zcat_kernel<CIN, COUT, Z::NB, 3, Z::PER_SM>;
-            err = smem_attributes(k, smem);
-            if (err != cudaSuccess) return true;
-            k<<<(unsigned)grid, 32 * (ZCAT_ISSUER0 + 3), smem, s>>>(map, a, g);
-        } else {
-            auto k = conv_zcat_kernel<CIN, COUT, Z::NB, Z::NISS, Z::PER_SM>;
-            err = smem_attributes(k, smem);
-            if (err != cudaSuccess) return true;
-            k<<<(unsigned)grid, 32 * (ZCAT_ISSUER0 + Z::NISS), smem, s>>>(map, a, g);
-        }
+        auto k = conv_zcat_kernel<CIN, COUT, Z::COUTH, Z::NB, Z::NISS, Z::PER_SM>;
+        err = smem_attributes(k, smem);
+        if (err != cudaSuccess) return true;
+        k<<<dim3((unsigned)grid, NG), 32 * (ZCAT_ISSUER0 + Z::NISS), smem, s>>>(map, a, g);
         err = cudaGetLastError();
         return true;
     }
@@ -2344,7 +2341,10 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_tc_kernel(const __grid_const
 //           X(z) pairs with G(z - dz), which is dz's term for output plane z - dz.
 // Either way a stage yields every tap of the tile: issuer warp 5 + t takes
 // the in-plane tap t = 3 (dy + 1) + dx + 1 and accumulates its (M x N) block
-// in TMEM for the whole launch.  Stages of every (item, plane, tile) are
+// in TMEM for the whole launch.  Where nine such blocks exceed TMEM's 512
+// columns (96 -> 32: N = 96; 32 -> 64: N = 64), blockIdx.y splits the nine
+// in-plane taps into groups of five and four, each group staging the tiles
+// on its own.  Stages of every (item, plane, tile) are
 // independent (planes outside the volume arrive as zeros), so the CTAs are
 // persistent over all tiles; a tile is KT consecutive padded positions of a
 // plane (K = KT per stage: longer tiles stage fewer halo rows per position).
