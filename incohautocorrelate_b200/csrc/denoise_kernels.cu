@@ -1224,6 +1224,10 @@ __global__ void __launch_bounds__(256, 1) conv_zcol_kernel(const __grid_constant
 // are done with it: after output ol a group frees the regions of stages ol and
 // ol + 1 (its next output starts at stage ol + 2), and at the end of a work
 // item the stages it never read.  The regions rotate over NB >= 3 buffers.
+// Slabs arrive as one TMA box per 8 channels (rows of 16 bytes).  Loading them
+// with warp-wide cp.async instead (16 bytes per thread, coalesced, zero-fill
+// by byte count) measured 1.6x slower at 16 -> 16: the loads in flight per SM
+// are too few to cover the latency.
 // The concatenated weights (27 cin cout bf16) are built in shared memory by
 // all threads at the start, from the [tap][cin/8][cout][8] tiles.
 // --------------------------------------------------------------------------
@@ -1246,7 +1250,7 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
     __shared__ __align__(8) uint64_t full[8], empty[8], accfull[NB], accempty[NB];
     __shared__ uint32_t s_tmem;
     __shared__ volatile int s_err;
-    __shared__ long long s_issued, s_last[NISS];
+    __shared__ int s_issued, s_last[NISS];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t sbase = smem_u32(smem);
     const uint32_t wbase = sbase;                   // concatenated weights [t9][cin/8][3 cout][8]
@@ -1297,15 +1301,14 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
 
     if (warp == ZCAT_PRODUCER) {
         if (lane == 0) {  // one slab per input plane z0-1 .. z1 (planes outside the volume arrive as zeros)
-            long long j = 0;
+            int j = 0, slot = 0, round = 0;  // slot = j % S, round = j / S
             bool ok = true;
             for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
                 int n, q0, z0, z1;
                 item(it, n, q0, z0, z1);
                 const int y_lo = floor_div(q0 - g.Wp - 1, g.Wp);
                 for (int pz = z0 - 1; pz <= z1; pz++, j++) {
-                    const int slot = (int)(j % g.S);
-                    if (j >= g.S && !mbar_wait_flag(smem_u32(&empty[slot]), (uint32_t)(((j / g.S) - 1) & 1), &s_err)) {
+                    if (j >= g.S && !mbar_wait_flag(smem_u32(&empty[slot]), (uint32_t)((round - 1) & 1), &s_err)) {
                         ok = false;
                         break;
                     }
@@ -1316,30 +1319,41 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
                     for (int c = 0; c < CIN / 8; c++)
                         tma_load_5d(st + c * g.plane_bytes, &xmap, c * 8, -1, y_lo, pz, n, fb);
                     s_issued = j + 1;
+                    if (++slot == g.S) {
+                        slot = 0;
+                        round++;
+                    }
                 }
             }
         }
     } else if (warp >= ZCAT_ISSUER0) {
         const int iw = warp - ZCAT_ISSUER0;  // stages j with j % NISS == iw
         if (lane == 0) {
-            long long j = 0;
+            int j = 0, slot = 0, round = 0, r = 0, rround = 0;  // slot = j % S, round = j / S, r = j % NB, rround = j / NB
             bool ok = true;
             for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
                 int n, q0, z0, z1;
                 item(it, n, q0, z0, z1);
                 const int rel = q0 - floor_div(q0 - g.Wp - 1, g.Wp) * g.Wp;  // q0 within the slab
                 for (int k = 0; k < z1 - z0 + 2; k++, j++) {
-                    if ((int)(j % NISS) != iw) continue;
-                    const int slot = (int)(j % g.S);
-                    const int r = (int)(j % NB);
-                    if (!mbar_wait_flag(smem_u32(&full[slot]), (uint32_t)((j / g.S) & 1), &s_err) ||
-                        (j >= NB && !mbar_wait_flag(smem_u32(&accempty[r]), (uint32_t)(((j / NB) - 1) & 1), &s_err))) {
+                    const int cur_slot = slot, cur_round = round, cur_r = r, cur_rround = rround;
+                    if (++slot == g.S) {
+                        slot = 0;
+                        round++;
+                    }
+                    if (++r == NB) {
+                        r = 0;
+                        rround++;
+                    }
+                    if (j % NISS != iw) continue;
+                    if (!mbar_wait_flag(smem_u32(&full[cur_slot]), (uint32_t)(cur_round & 1), &s_err) ||
+                        (j >= NB && !mbar_wait_flag(smem_u32(&accempty[cur_r]), (uint32_t)((cur_rround - 1) & 1), &s_err))) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t st = stbase + (uint32_t)slot * g.stage_bytes;
-                    const uint32_t dcol = tmem + (uint32_t)(r * N3);
+                    const uint32_t st = stbase + (uint32_t)cur_slot * g.stage_bytes;
+                    const uint32_t dcol = tmem + (uint32_t)(cur_r * N3);
                     // descriptors: the start-address field (16-byte units, low 14 bits) moves
                     // by whole units from one MMA to the next and never leaves [0, 2^14), so
                     // each is the stage's base descriptor plus a small (signed) offset
@@ -1355,8 +1369,8 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
                             umma_bf16(dcol, da, db, IDESC, (t > 0 || kk > 0) ? 1u : 0u);
                         }
                     }
-                    umma_commit(smem_u32(&empty[slot]));
-                    umma_commit(smem_u32(&accfull[r]));
+                    umma_commit(smem_u32(&empty[cur_slot]));
+                    umma_commit(smem_u32(&accfull[cur_r]));
                     s_last[iw] = j;
                 }
             }
@@ -1372,7 +1386,7 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&accempty[stage % NB]));
         };
-        long long j = 0;  // this CTA's stages before the current item
+        int j = 0;  // this CTA's stages before the current item
         bool ok = true;
         for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
             int n, q0, z0, z1;
@@ -1437,10 +1451,10 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
         // before the shared memory and TMEM are released
         if (tid == 0) {
             if (a.counters) atomicAdd(&a.counters->timeouts, 1ull);
-            for (long long i = s_issued > g.S ? s_issued - g.S : 0; i < s_issued; i++)
+            for (int i = s_issued > g.S ? s_issued - g.S : 0; i < s_issued; i++)
                 mbar_wait(smem_u32(&full[i % g.S]), (uint32_t)((i / g.S) & 1));
             for (int w = 0; w < NISS; w++) {
-                const long long i = s_last[w];
+                const int i = s_last[w];
                 if (i >= 0) mbar_wait(smem_u32(&empty[i % g.S]), (uint32_t)((i / g.S) & 1));
             }
         }
@@ -1785,49 +1799,82 @@ cudaError_t conv3x3(const ConvArgs &a, int cin, int cout, int backend, cudaStrea
 }
 
 // --------------------------------------------------------------------------
-// first layer (1 input channel): 27 x 16 MACs per voxel on the FP32 pipe
+// first layer (1 input channel): 27 x 16 MACs per voxel on the FP32 pipe.
+// A thread takes four consecutive voxels of a row: per (dz, dy) it loads the
+// six input values the four need and applies the three dx taps to all four
+// (the weights of a tap are read from shared memory once for four voxels, as
+// four float4), so the kernel is bound by its FMAs, not by shared-memory
+// loads.  Taps outside the volume read 0 (zero padding); a voxel's sums run
+// over the taps in order.  W is a multiple of 4.
 // --------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) conv_first_kernel(const float *__restrict__ x, const bf16 *__restrict__ w,
                                                          const float *__restrict__ bias, bf16 *__restrict__ y,
                                                          int D, int H, int W, long long V)
 {
-    __shared__ float ws[27][16];
+    __shared__ float4 ws[27][4];
     __shared__ float bs[16];
-    for (int i = threadIdx.x; i < 27 * 16; i += blockDim.x) ws[i / 16][i % 16] = __bfloat162float(w[i]);
+    for (int i = threadIdx.x; i < 27 * 16; i += blockDim.x)
+        reinterpret_cast<float *>(ws)[i] = __bfloat162float(w[i]);
     if (threadIdx.x < 16) bs[threadIdx.x] = bias[threadIdx.x];
     __syncthreads();
-    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= V) return;
-    const Vox q = decode(v, D, H, W, V);
-    float acc[16];
+    const long long v0 = 4 * ((long long)blockIdx.x * blockDim.x + threadIdx.x);  // first of four voxels
+    if (v0 >= V) return;
+    const Vox q = decode(v0, D, H, W, V);
+    float acc[4][16];
 #pragma unroll
-    for (int c = 0; c < 16; c++) acc[c] = bs[c];
-    // the neighbours are v + dz H W + dy W + dx; taps outside the volume are
-    // skipped (compile-time taps, per-axis edge flags: little integer work per tap)
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int c = 0; c < 16; c++) acc[i][c] = bs[c];
     const long long HW = (long long)H * W;
-    const bool in[3][3] = {{q.z > 0, true, q.z + 1 < D}, {q.y > 0, true, q.y + 1 < H}, {q.x > 0, true, q.x + 1 < W}};
+    const bool left = q.x > 0, right = q.x + 4 < W;
 #pragma unroll
-    for (int t = 0; t < 27; t++) {
-        const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
-        if (in[0][dz] && in[1][dy] && in[2][dx]) {
-            const float xv = x[v + (dz - 1) * HW + (long long)(dy - 1) * W + (dx - 1)];
+    for (int dz = 0; dz < 3; dz++) {
+        const bool zin = (unsigned)(q.z + dz - 1) < (unsigned)D;
 #pragma unroll
-            for (int c = 0; c < 16; c++) acc[c] = fmaf(ws[t][c], xv, acc[c]);
+        for (int dy = 0; dy < 3; dy++) {
+            const bool in = zin && (unsigned)(q.y + dy - 1) < (unsigned)H;
+            const float *row = x + v0 + (dz - 1) * HW + (long long)(dy - 1) * W;  // voxel x0 of the row
+            float r[6];
+            r[0] = in && left ? row[-1] : 0.0f;
+#pragma unroll
+            for (int k = 0; k < 4; k++) r[k + 1] = in ? row[k] : 0.0f;
+            r[5] = in && right ? row[4] : 0.0f;
+#pragma unroll
+            for (int dx = 0; dx < 3; dx++) {
+                const int t = 9 * dz + 3 * dy + dx;
+#pragma unroll
+                for (int c4 = 0; c4 < 4; c4++) {
+                    const float4 wv = ws[t][c4];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const float xv = r[i + dx];
+                        acc[i][4 * c4] = fmaf(wv.x, xv, acc[i][4 * c4]);
+                        acc[i][4 * c4 + 1] = fmaf(wv.y, xv, acc[i][4 * c4 + 1]);
+                        acc[i][4 * c4 + 2] = fmaf(wv.z, xv, acc[i][4 * c4 + 2]);
+                        acc[i][4 * c4 + 3] = fmaf(wv.w, xv, acc[i][4 * c4 + 3]);
+                    }
+                }
+            }
         }
     }
-    uint4 pk[2];
-    uint32_t *u = reinterpret_cast<uint32_t *>(pk);
 #pragma unroll
-    for (int c = 0; c < 16; c += 2) u[c / 2] = pack_bf16(fmaxf(acc[c], 0.0f), fmaxf(acc[c + 1], 0.0f));
-    uint4 *dst = reinterpret_cast<uint4 *>(y + v * 16);
-    dst[0] = pk[0];
-    dst[1] = pk[1];
+    for (int i = 0; i < 4; i++) {
+        uint4 pk[2];
+        uint32_t *u = reinterpret_cast<uint32_t *>(pk);
+#pragma unroll
+        for (int c = 0; c < 16; c += 2) u[c / 2] = pack_bf16(fmaxf(acc[i][c], 0.0f), fmaxf(acc[i][c + 1], 0.0f));
+        uint4 *dst = reinterpret_cast<uint4 *>(y + (v0 + i) * 16);
+        dst[0] = pk[0];
+        dst[1] = pk[1];
+    }
 }
 
 cudaError_t conv3x3_first(const float *x, const bf16 *w, const float *bias, bf16 *y, int D, int H, int W,
                           long long V, cudaStream_t s)
 {
-    conv_first_kernel<<<(unsigned)((V + 255) / 256), 256, 0, s>>>(x, w, bias, y, D, H, W, V);
+    if (W % 4) return cudaErrorInvalidValue;
+    const long long threads = V / 4;
+    conv_first_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(x, w, bias, y, D, H, W, V);
     return cudaGetLastError();
 }
 
@@ -2743,45 +2790,77 @@ cudaError_t wgrad3x3(const WgradArgs &a, int cin, int sms, cudaStream_t s)
 }
 
 // first layer: dW[co][tap] = sum_v G[v][co] x[v+off(tap)] and db[co] = sum_v G[v][co]
-// on mma.sync: per block of 128 voxels the 27 shifted inputs (and a column of
-// ones for the bias) are written to shared memory as a bf16 [tap chunk][voxel][8]
-// operand, the gradient rows as [co chunk][voxel][8]; M = 16 output channels,
-// N = 32 columns (27 taps, ones, padding), K = voxels.
-__global__ void __launch_bounds__(128) wgrad_first_kernel(const float *__restrict__ x, const bf16 *__restrict__ g,
-                                                          float *__restrict__ dw, float *__restrict__ db, int D,
-                                                          int H, int W, long long V)
+// on mma.sync, warp by warp: a warp takes 128 voxels at a time, a lane four
+// consecutive voxels of a row (it loads the six input values per (dz, dy) that
+// the four need, as conv_first_kernel).  The lane writes the 27 shifted inputs
+// of its voxels, a one for the bias and four zeros as bf16 rows of 32 columns
+// into the warp's own shared-memory operand [column chunk][voxel][8], the
+// gradient rows as [co chunk][voxel][8] (voxel 4 lane + i in row 32 i + lane:
+// the sum over voxels does not depend on their order, and consecutive lanes
+// write consecutive rows, free of bank conflicts); M = 16 output channels,
+// N = 32 columns, K = 128 voxels.  Only warp barriers inside the loop.
+constexpr int WGF_WARPS = 8;
+constexpr int WGF_ROWS = 128;  // voxels per warp and iteration
+constexpr int WGF_WARP_BYTES = (4 + 2) * WGF_ROWS * 16;
+__global__ void __launch_bounds__(32 * WGF_WARPS, 2) wgrad_first_kernel(const float *__restrict__ x,
+                                                                        const bf16 *__restrict__ g,
+                                                                        float *__restrict__ dw,
+                                                                        float *__restrict__ db, int D, int H,
+                                                                        int W, long long V)
 {
-    __shared__ __align__(128) bf16 xs[4][TILE_M][8];
-    __shared__ __align__(128) bf16 gs[2][TILE_M][8];
+    extern __shared__ __align__(128) unsigned char wgf_smem[];
     __shared__ float red[16][32];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    for (int i = tid; i < 16 * 32; i += 128) (&red[0][0])[i] = 0.0f;
+    for (int i = tid; i < 16 * 32; i += blockDim.x) (&red[0][0])[i] = 0.0f;
     float acc[4][4];
 #pragma unroll
     for (int n = 0; n < 4; n++)
 #pragma unroll
         for (int j = 0; j < 4; j++) acc[n][j] = 0.0f;
-    const uint32_t sx = smem_u32(&xs[0][0][0]), sg = smem_u32(&gs[0][0][0]);
-    const long long nblk = (V + TILE_M - 1) / TILE_M;
-    for (long long b = blockIdx.x; b < nblk; b += gridDim.x) {
-        __syncthreads();
-        {
-            const long long v = b * TILE_M + tid;
-            const Vox q = decode(v, D, H, W, V);
-            float col[32];
-            // neighbours v + dz H W + dy W + dx, per-axis edge flags (as conv_first_kernel)
-            const long long HW = (long long)H * W;
-            const bool in[3][3] = {{q.z > 0, true, q.z + 1 < D}, {q.y > 0, true, q.y + 1 < H},
-                                   {q.x > 0, true, q.x + 1 < W}};
+    unsigned char *mine = wgf_smem + warp * WGF_WARP_BYTES;
+    uint4 *xs = reinterpret_cast<uint4 *>(mine);                       // [4][128] rows of 8 bf16
+    uint4 *gs = reinterpret_cast<uint4 *>(mine + 4 * WGF_ROWS * 16);   // [2][128]
+    const uint32_t sx = smem_u32(xs), sg = smem_u32(gs);
+    const long long HW = (long long)H * W;
+    const long long ngroups = (V + WGF_ROWS - 1) / WGF_ROWS;
+    const long long stride = (long long)gridDim.x * WGF_WARPS;
+    for (long long grp = (long long)blockIdx.x * WGF_WARPS + warp; grp < ngroups; grp += stride) {
+        const long long v0 = grp * WGF_ROWS + 4 * lane;
+        const Vox q = decode(v0, D, H, W, V);
+        float r[9][6];
+        const bool left = q.x > 0, right = q.x + 4 < W;
 #pragma unroll
-            for (int t = 0; t < 27; t++) {
-                const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
-                const bool ok = q.ok && in[0][dz] && in[1][dy] && in[2][dx];
-                col[t] = ok ? x[v + (dz - 1) * HW + (long long)(dy - 1) * W + (dx - 1)] : 0.0f;
+        for (int dz = 0; dz < 3; dz++) {
+            const bool zin = q.ok && (unsigned)(q.z + dz - 1) < (unsigned)D;
+#pragma unroll
+            for (int dy = 0; dy < 3; dy++) {
+                const bool in = zin && (unsigned)(q.y + dy - 1) < (unsigned)H;
+                const float *row = x + (q.ok ? v0 : 0) + (dz - 1) * HW + (long long)(dy - 1) * W;
+                float *rr = r[3 * dz + dy];
+                rr[0] = in && left ? row[-1] : 0.0f;
+#pragma unroll
+                for (int k = 0; k < 4; k++) rr[k + 1] = in ? row[k] : 0.0f;
+                rr[5] = in && right ? row[4] : 0.0f;
             }
+        }
+        uint4 gv[4][2];
+        const uint4 z4 = make_uint4(0, 0, 0, 0);
+        const uint4 *gp = reinterpret_cast<const uint4 *>(g + (q.ok ? v0 : 0) * 16);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            gv[i][0] = q.ok ? gp[2 * i] : z4;
+            gv[i][1] = q.ok ? gp[2 * i + 1] : z4;
+        }
+        __syncwarp();  // the previous iteration's fragments are read
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            float col[32];
+#pragma unroll
+            for (int t = 0; t < 27; t++) col[t] = r[t / 3][i + t % 3];
             col[27] = q.ok ? 1.0f : 0.0f;
 #pragma unroll
             for (int t = 28; t < 32; t++) col[t] = 0.0f;
+            const int row = 32 * i + lane;
 #pragma unroll
             for (int c = 0; c < 4; c++) {
                 uint4 u;
@@ -2789,57 +2868,61 @@ __global__ void __launch_bounds__(128) wgrad_first_kernel(const float *__restric
                 u.y = pack_bf16(col[8 * c + 2], col[8 * c + 3]);
                 u.z = pack_bf16(col[8 * c + 4], col[8 * c + 5]);
                 u.w = pack_bf16(col[8 * c + 6], col[8 * c + 7]);
-                *reinterpret_cast<uint4 *>(&xs[c][tid][0]) = u;
+                xs[c * WGF_ROWS + row] = u;
             }
-            const uint4 z4 = make_uint4(0, 0, 0, 0);
-            const uint4 *gp = reinterpret_cast<const uint4 *>(g + (q.ok ? v : 0) * 16);
-            *reinterpret_cast<uint4 *>(&gs[0][tid][0]) = q.ok ? gp[0] : z4;
-            *reinterpret_cast<uint4 *>(&gs[1][tid][0]) = q.ok ? gp[1] : z4;
+            gs[row] = gv[i][0];
+            gs[WGF_ROWS + row] = gv[i][1];
         }
-        __syncthreads();
+        __syncwarp();
 #pragma unroll
-        for (int ks = 0; ks < 2; ks++) {
-            const int kb = warp * 32 + ks * 16;
+        for (int ks = 0; ks < WGF_ROWS / 16; ks++) {
+            const int kb = ks * 16;
             uint32_t a0, a1, a2, a3;
             {
                 const int vr = kb + (lane & 7) + ((lane >> 4) << 3);
                 const int ch = (lane >> 3) & 1;
-                ldsm_x4_t(sg + (uint32_t)((ch * TILE_M + vr) * 16), a0, a1, a2, a3);
+                ldsm_x4_t(sg + (uint32_t)((ch * WGF_ROWS + vr) * 16), a0, a1, a2, a3);
             }
 #pragma unroll
             for (int n2 = 0; n2 < 2; n2++) {
                 uint32_t b0, b1, b2, b3;
                 const int vx = kb + (lane & 7) + (((lane >> 3) & 1) << 3);
                 const int cx = 2 * n2 + (lane >> 4);
-                ldsm_x4_t(sx + (uint32_t)((cx * TILE_M + vx) * 16), b0, b1, b2, b3);
+                ldsm_x4_t(sx + (uint32_t)((cx * WGF_ROWS + vx) * 16), b0, b1, b2, b3);
                 mma_bf16(acc[2 * n2], a0, a1, a2, a3, b0, b1);
                 mma_bf16(acc[2 * n2 + 1], a0, a1, a2, a3, b2, b3);
             }
         }
     }
+    __syncthreads();  // red is zeroed
     const int gq = lane >> 2, tq = lane & 3;
 #pragma unroll
     for (int n = 0; n < 4; n++)
 #pragma unroll
         for (int j = 0; j < 4; j++) atomicAdd(&red[gq + 8 * (j >> 1)][n * 8 + 2 * tq + (j & 1)], acc[n][j]);
     __syncthreads();
-    for (int i = tid; i < 16 * 28; i += 128) {
+    for (int i = tid; i < 16 * 28; i += blockDim.x) {
         const int co = i / 28, t = i % 28;
-        const float r = red[co][t];
-        if (r == 0.0f) continue;
+        const float rv = red[co][t];
+        if (rv == 0.0f) continue;
         if (t < 27)
-            atomicAdd(&dw[co * 27 + t], r);
+            atomicAdd(&dw[co * 27 + t], rv);
         else
-            atomicAdd(&db[co], r);
+            atomicAdd(&db[co], rv);
     }
 }
 
 cudaError_t wgrad3x3_first(const float *x, const bf16 *g, float *dw, float *db, int D, int H, int W, long long V,
                            int sms, cudaStream_t s)
 {
-    const long long nblk = (V + TILE_M - 1) / TILE_M;
-    const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(nblk, 8LL * sms));
-    wgrad_first_kernel<<<grid, 128, 0, s>>>(x, g, dw, db, D, H, W, V);
+    if (W % 4) return cudaErrorInvalidValue;
+    const int smem = WGF_WARPS * WGF_WARP_BYTES;
+    const cudaError_t e = cudaFuncSetAttribute(wgrad_first_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const long long ngroups = (V + WGF_ROWS - 1) / WGF_ROWS;
+    const long long blocks = (ngroups + WGF_WARPS - 1) / WGF_WARPS;
+    const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(blocks, 2LL * sms));
+    wgrad_first_kernel<<<grid, 32 * WGF_WARPS, smem, s>>>(x, g, dw, db, D, H, W, V);
     return cudaGetLastError();
 }
 
