@@ -156,6 +156,16 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
     return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
            ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
+// K-major operand with the 32-byte swizzle: rows of 16 bf16 (32 bytes, the two
+// 16-byte halves exchanged in rows 4-7 of every 8), 8-row groups 256 bytes
+// apart (SBO), layout type 6 at bit 61, base offset 0.  The swizzle acts on
+// absolute shared-memory address bits, as the TMA's SWIZZLE_32B writes them,
+// so the start may sit at any row (checked for row offsets 0 .. 67).
+__device__ __forceinline__ uint64_t smem_desc_sw32(uint32_t addr)
+{
+    return (uint64_t)((addr & 0x3FFFFu) >> 4) | (1ull << 16) | ((uint64_t)(256u >> 4) << 32) | (1ull << 46) |
+           (6ull << 61);
+}
 // instruction descriptor, kind::f16: D fp32 (bits 4-5 = 1), A and B bf16
 // (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
 __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N)
@@ -1224,10 +1234,13 @@ __global__ void __launch_bounds__(256, 1) conv_zcol_kernel(const __grid_constant
 // are done with it: after output ol a group frees the regions of stages ol and
 // ol + 1 (its next output starts at stage ol + 2), and at the end of a work
 // item the stages it never read.  The regions rotate over NB >= 3 buffers.
-// Slabs arrive as one TMA box per 8 channels (rows of 16 bytes).  Loading them
-// with warp-wide cp.async instead (16 bytes per thread, coalesced, zero-fill
-// by byte count) measured 1.6x slower at 16 -> 16: the loads in flight per SM
-// are too few to cover the latency.
+// Slabs arrive as one TMA box per 16 channels with the 32-byte swizzle: rows
+// of 32 bytes, stage layout [cin/16][position][16 channels], read by the MMAs
+// as swizzled K-major tiles from any row.  The TMA unit moves about one box row
+// per clock, so 16-byte rows (one box per 8 channels, the unswizzled K-major
+// layout) left the issuers waiting on slabs 40 % of the time at 16 -> 16.
+// Loading with warp-wide cp.async (16 bytes per thread, coalesced) measured
+// 1.6x slower still: too few loads in flight per SM to cover the latency.
 // The concatenated weights (27 cin cout bf16) are built in shared memory by
 // all threads at the start, from the [tap][cin/8][cout][8] tiles.
 // --------------------------------------------------------------------------
@@ -1239,6 +1252,7 @@ template <int CIN, int COUT, int COUTH, int NB, int NISS, int MINB>
 __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
     conv_zcat_kernel(const __grid_constant__ CUtensorMap xmap, const ConvArgs a, const TmaGeom g)
 {
+    static_assert(CIN % 16 == 0, "slabs of 16-channel planes");
     constexpr int N3 = 3 * COUTH;  // COUTH of the COUT output channels per CTA: blockIdx.y selects them
     const int c_lo = (int)blockIdx.y * COUTH;
     constexpr uint32_t TCOLS = tma_tcols(NB * N3);
@@ -1314,10 +1328,10 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
                     }
                     const uint32_t st = stbase + (uint32_t)slot * g.stage_bytes;
                     const uint32_t fb = smem_u32(&full[slot]);
-                    mbar_expect_tx(fb, (CIN / 8) * g.box_bytes);
+                    mbar_expect_tx(fb, (CIN / 16) * g.box_bytes);
 #pragma unroll
-                    for (int c = 0; c < CIN / 8; c++)
-                        tma_load_5d(st + c * g.plane_bytes, &xmap, c * 8, -1, y_lo, pz, n, fb);
+                    for (int c = 0; c < CIN / 16; c++)
+                        tma_load_5d(st + c * g.plane_bytes, &xmap, c * 16, -1, y_lo, pz, n, fb);
                     s_issued = j + 1;
                     if (++slot == g.S) {
                         slot = 0;
@@ -1357,14 +1371,14 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
                     // descriptors: the start-address field (16-byte units, low 14 bits) moves
                     // by whole units from one MMA to the next and never leaves [0, 2^14), so
                     // each is the stage's base descriptor plus a small (signed) offset
-                    const uint64_t da0 = smem_desc(st + (uint32_t)rel * 16, g.plane_bytes, 128);
+                    const uint64_t da0 = smem_desc_sw32(st + (uint32_t)rel * 32);
                     const uint64_t db0 = smem_desc(wbase, N3 * 16, 128);
 #pragma unroll
                     for (int t = 0; t < 9; t++) {
-                        const int64_t toff = (int64_t)((t / 3 - 1) * g.Wp + (t % 3 - 1));  // rows of 16 B
+                        const int64_t toff = (int64_t)(2 * ((t / 3 - 1) * g.Wp + (t % 3 - 1)));  // rows of 32 B, in 16 B
 #pragma unroll
                         for (int kk = 0; kk < CIN / 16; kk++) {
-                            const uint64_t da = da0 + (uint64_t)(toff + (int64_t)((2 * kk * g.plane_bytes) >> 4));
+                            const uint64_t da = da0 + (uint64_t)(toff + (int64_t)((kk * g.plane_bytes) >> 4));
                             const uint64_t db = db0 + (uint64_t)((t * WT9_BYTES + kk * 2 * (N3 * 16)) >> 4);
                             umma_bf16(dcol, da, db, IDESC, (t > 0 || kk > 0) ? 1u : 0u);
                         }
@@ -1572,8 +1586,7 @@ struct ZcatCfg {
 // others.  IAC_DENOISE_ZCAT=0 in the environment turns it off (for comparing
 // the kernels).
 template <int CIN, int COUT>
-static bool launch_zcat(const ConvArgs &a, const TmaGeom &g0, const CUtensorMap &map, uint32_t budget,
-                        cudaStream_t s, cudaError_t &err)
+static bool launch_zcat(const ConvArgs &a, const TmaGeom &g0, uint32_t budget, cudaStream_t s, cudaError_t &err)
 {
     using Z = ZcatCfg<CIN, COUT>;
     if constexpr (Z::NB == 0 || Z::N3 > 256 || COUT % Z::COUTH != 0) {
@@ -1591,7 +1604,24 @@ static bool launch_zcat(const ConvArgs &a, const TmaGeom &g0, const CUtensorMap 
         g.wcopy_bytes = w27;
         g.wres_bytes = (w27 + 1023u) & ~1023u;
         g.wstage_bytes = 0;
+        // slabs as 32-byte swizzled rows: one box of 16 channels x Wp x NR per plane
+        g.box_bytes = 32u * (uint32_t)g.Wp * (uint32_t)g.NR;
+        g.plane_bytes = (g.box_bytes + 255u) & ~255u;
+        g.slab_bytes = g.plane_bytes * (CIN / 16);
         g.stage_bytes = (g.slab_bytes + 1023u) & ~1023u;
+        const long long nb = a.V / ((long long)a.D * a.H * a.W);
+        PFN_cuTensorMapEncodeTiled enc = tensor_map_encoder();
+        if (!enc) return false;
+        CUtensorMap map;
+        const cuuint64_t dims[5] = {(cuuint64_t)CIN, (cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.D, (cuuint64_t)nb};
+        const cuuint64_t strides[4] = {(cuuint64_t)CIN * 2, (cuuint64_t)a.W * CIN * 2,
+                                       (cuuint64_t)a.H * a.W * CIN * 2, (cuuint64_t)a.D * a.H * a.W * CIN * 2};
+        const cuuint32_t box[5] = {16u, (cuuint32_t)g.Wp, (cuuint32_t)g.NR, 1u, 1u};
+        const cuuint32_t estr[5] = {1u, 1u, 1u, 1u, 1u};
+        if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16 *>(a.src1), dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
         int per_sm = 0, S = 0;
         for (int want = Z::PER_SM; want >= 1 && per_sm == 0; want--) {
             const uint32_t share = std::min(budget, (228u * 1024u) / (uint32_t)want - 2048u);
@@ -1604,7 +1634,6 @@ static bool launch_zcat(const ConvArgs &a, const TmaGeom &g0, const CUtensorMap 
         }
         if (per_sm == 0) return false;
         g.S = S;
-        const long long nb = a.V / ((long long)a.D * a.H * a.W);
         const long long grid_max = ((long long)per_sm * std::max(1, a.sms) + NG - 1) / NG;  // per channel group
         // output planes per work item: a work item of ZC outputs takes ZC + 2 stages (every
         // stage costs the same MMAs), and the CTAs run ceil(items / grid) rounds of them:
@@ -1734,7 +1763,7 @@ static bool launch_tma(const ConvArgs &a, cudaStream_t s, cudaError_t &err)
                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return false;
-    if (launch_zcat<CIN, COUT>(a, g, map, budget, s, err)) return true;
+    if (launch_zcat<CIN, COUT>(a, g, budget, s, err)) return true;
     if (launch_zcol<CIN, COUT>(a, g, map, budget, s, err)) return true;
     const long long grid = std::min<long long>(g.ntiles, (long long)per_sm * std::max(1, a.sms));
     if constexpr (2 * 3 * COUT <= 512) {
