@@ -166,6 +166,15 @@ __device__ __forceinline__ uint64_t smem_desc_sw32(uint32_t addr)
     return (uint64_t)((addr & 0x3FFFFu) >> 4) | (1ull << 16) | ((uint64_t)(256u >> 4) << 32) | (1ull << 46) |
            (6ull << 61);
 }
+// MN-major operand with the 32-byte swizzle: 16 M (or N) elements per 32-byte
+// row, one row per K index, 8-row groups 256 bytes apart (SBO), 16-element
+// M blocks `mblock` bytes apart (LBO); the same rows as smem_desc_sw32, read
+// transposed, from any row
+__device__ __forceinline__ uint64_t smem_desc_sw32_mn(uint32_t addr, uint32_t mblock)
+{
+    return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)((mblock >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)(256u >> 4) << 32) | (1ull << 46) | (6ull << 61);
+}
 // instruction descriptor, kind::f16: D fp32 (bits 4-5 = 1), A and B bf16
 // (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
 __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N)
@@ -2232,7 +2241,7 @@ struct WTGeom {
     int Wp, NR, NRg, T;
     int KT;                        // positions per tile (wgrad_zs_kernel; TILE_M elsewhere)
     long long ntiles;
-    uint32_t planeX, planeG;       // one 8-channel chunk plane of X / of the gradient (128-aligned)
+    uint32_t planeX, planeG;       // one channel-chunk plane of X / of the gradient in a stage
     uint32_t boxX, boxG;           // bytes one box delivers
     uint32_t stage_bytes;
     int S;
@@ -2409,12 +2418,17 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_tc_kernel(const __grid_const
 // columns, and each stage's X and gradient slabs are staged three times.
 // Here one stage holds all that one tile needs for its 27 taps, laid out so
 // that the dz axis becomes part of an MMA dimension (the chunk planes of
-// consecutive slabs are equally spaced, so they stack in one descriptor):
-//   PX = 3: X slabs of planes z-1, z, z+1 stacked along M (M = 3 cin rows:
-//           row (dz + 1) cin + ci), the gradient slab of plane z as B (N = cout);
-//   PX = 1: the X slab of plane z as A (M = cin), the gradient slabs of
-//           planes z+1, z, z-1 stacked along N (column (dz + 1) cout + co):
-//           X(z) pairs with G(z - dz), which is dz's term for output plane z - dz.
+// consecutive slabs are equally spaced, so they stack in one descriptor).
+// A stage covers ZSTEP gradient planes z0 .. z0 + ZSTEP - 1 and stacks NX X
+// slabs (planes z0 + XLO ..) along M and NG gradient slabs (planes z0 + GLO ..)
+// along N; the block of X plane p and gradient plane p' holds the dz = p - p'
+// term of output plane p', kept where |dz| <= 1:
+//   MODE 0: X planes z-1, z, z+1 along M (M = 3 cin), the gradient of plane z
+//           as B (N = cout);
+//   MODE 1: the X plane z as A (M = cin), gradient planes z-1, z, z+1 along N;
+//   MODE 2: X planes z0-1 .. z0+3 along M, gradient planes z0 .. z0+2 along N:
+//           three output planes per stage, 9 of the 15 blocks kept, a third
+//           of the MMAs (and of the X slab loads) of MODE 0 per output plane.
 // Either way a stage yields every tap of the tile: issuer warp 5 + t takes
 // the in-plane tap t = 3 (dy + 1) + dx + 1 and accumulates its (M x N) block
 // in TMEM for the whole launch.  Where nine such blocks exceed TMEM's 512
@@ -2424,36 +2438,44 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_tc_kernel(const __grid_const
 // independent (planes outside the volume arrive as zeros), so the CTAs are
 // persistent over all tiles; a tile is KT consecutive padded positions of a
 // plane (K = KT per stage: longer tiles stage fewer halo rows per position).
-// The bias gradient comes with it: the first of
-// the padding rows of A is an 8-channel plane of ones, written once into every
-// stage slot, so its accumulator row holds sum_v G[v][co] (the gradient is
-// zero at the padded positions).
+// Slabs arrive as one 32-byte-swizzled TMA box per 16 channels (stage planes
+// [position][16 channels]) and are read as MN-major operands: the TMA unit
+// moves about one box row per clock, so rows of 32 bytes stage a slab in half
+// the time of the unswizzled layout's 16-byte rows.
+// The bias gradient comes with it: the first of the padding rows of A is a
+// 16-channel plane of ones, written once into every stage slot, so its
+// accumulator row holds sum_v G[v][co] (the gradient is zero at the padded
+// positions).
 // --------------------------------------------------------------------------
-template <int CIN, int COUT, int PX>
+template <int CIN, int COUT, int MODE>
 struct WzsCfg {
-    static constexpr int PG = PX == 3 ? 1 : 3;
-    static constexpr int MROWS = PX * CIN;              // real M rows
+    static constexpr int NX = MODE == 0 ? 3 : (MODE == 1 ? 1 : 5);  // X planes per stage (along M)
+    static constexpr int NG = MODE == 0 ? 1 : 3;                     // gradient planes per stage (along N)
+    static constexpr int ZSTEP = MODE == 2 ? 3 : 1;                  // gradient planes a stage owns
+    static constexpr int XLO = MODE == 1 ? 0 : -1;                   // first X plane - z0
+    static constexpr int GLO = MODE == 1 ? -1 : 0;                   // first gradient plane - z0
+    static constexpr int MROWS = NX * CIN;              // real M rows
     static constexpr int MR = MROWS > 64 ? 128 : 64;    // rows per MMA
     static constexpr int MB = (MROWS + MR - 1) / MR;    // M blocks
-    static constexpr int N = PG * COUT;                 // MMA columns
+    static constexpr int N = NG * COUT;                 // MMA columns
     // in-plane taps per CTA: all nine, or the fewest groups whose accumulators fit TMEM
     static constexpr int NTG = 9 * N * MB <= 512 ? 1 : (5 * N * MB <= 512 ? 2 : (3 * N * MB <= 512 ? 3 : 9));
     static constexpr int TPG = (9 + NTG - 1) / NTG;     // taps of a group (the last may have fewer)
     static constexpr int COLS = TPG * N * MB;
     static constexpr uint32_t TCOLS = COLS <= 32 ? 32 : (COLS <= 64 ? 64 : (COLS <= 128 ? 128 : (COLS <= 256 ? 256 : 512)));
-    static constexpr int XREAL = PX * CIN / 8;          // X chunk planes loaded
-    static constexpr int XPLANES = MB * MR / 8;         // X chunk planes the MMAs read (padding rows: garbage)
-    static constexpr int GPLANES = PG * COUT / 8;
+    static constexpr int XREAL = NX * CIN / 16;         // X planes of 16 channels loaded
+    static constexpr int XPLANES = MB * MR / 16;        // X planes the MMAs read (padding rows: garbage)
+    static constexpr int GPLANES = NG * COUT / 16;
     static constexpr bool OK = COLS <= 512 && N <= 256 && N % (MR == 128 ? 16 : 8) == 0 && XPLANES > XREAL &&
-                               NTG <= 3;
+                               NTG <= 3 && CIN % 16 == 0 && COUT % 16 == 0;
 };
 
-template <int CIN, int COUT, int PX>
+template <int CIN, int COUT, int MODE>
 __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_constant__ CUtensorMap xmap,
                                                               const __grid_constant__ CUtensorMap gmap,
                                                               const WgradArgs a, const WTGeom g)
 {
-    using Z = WzsCfg<CIN, COUT, PX>;
+    using Z = WzsCfg<CIN, COUT, MODE>;
     constexpr int MB = Z::MB, MR = Z::MR, N = Z::N;
     constexpr uint32_t IDESC = idesc_bf16(MR, N) | (1u << 15) | (1u << 16);  // A and B MN-major
     constexpr int NI = Z::TPG;  // issuing warps: one per in-plane tap of this CTA's group
@@ -2503,25 +2525,26 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_const
                 if (k >= g.S && !mbar_wait_flag(smem_u32(&empty[slot]), (uint32_t)(((k / g.S) - 1) & 1), &s_err))
                     break;
                 const long long tile = blockIdx.x + k * (long long)gridDim.x;
-                const long long plane = tile / g.T;
+                const long long plane = tile / g.T;  // (batch item, group of ZSTEP gradient planes)
                 const int q0 = (int)(tile % g.T) * g.KT;
-                const int n = (int)(plane / a.D), z = (int)(plane % a.D);
+                const int nzg = (a.D + Z::ZSTEP - 1) / Z::ZSTEP;
+                const int n = (int)(plane / nzg), z0 = (int)(plane % nzg) * Z::ZSTEP;
                 const int y_lo = floor_div(q0 - g.Wp - 1, g.Wp), yg_lo = q0 / g.Wp;
                 const uint32_t st = sbase + (uint32_t)slot * g.stage_bytes;
                 const uint32_t fb = smem_u32(&full[slot]);
                 mbar_expect_tx(fb, (uint32_t)Z::XREAL * g.boxX + (uint32_t)Z::GPLANES * g.boxG);
 #pragma unroll
-                for (int px = 0; px < PX; px++)
+                for (int b = 0; b < Z::NX; b++)
 #pragma unroll
-                    for (int c = 0; c < CIN / 8; c++)
-                        tma_load_5d(st + (uint32_t)(px * (CIN / 8) + c) * g.planeX, &xmap, c * 8, -1, y_lo,
-                                    PX == 3 ? z - 1 + px : z, n, fb);
+                    for (int c = 0; c < CIN / 16; c++)
+                        tma_load_5d(st + (uint32_t)(b * (CIN / 16) + c) * g.planeX, &xmap, c * 16, -1, y_lo,
+                                    z0 + Z::XLO + b, n, fb);
 #pragma unroll
-                for (int pg = 0; pg < Z::PG; pg++)
+                for (int pg = 0; pg < Z::NG; pg++)
 #pragma unroll
-                    for (int c = 0; c < COUT / 8; c++)
-                        tma_load_5d(st + xbytes + (uint32_t)(pg * (COUT / 8) + c) * g.planeG, &gmap, c * 8, -1, yg_lo,
-                                    Z::PG == 3 ? z + 1 - pg : z, n, fb);
+                    for (int c = 0; c < COUT / 16; c++)
+                        tma_load_5d(st + xbytes + (uint32_t)(pg * (COUT / 16) + c) * g.planeG, &gmap, c * 16, -1,
+                                    yg_lo, z0 + Z::GLO + pg, n, fb);
                 s_issued = k + 1;
             }
         }
@@ -2538,16 +2561,17 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_const
                 const int relg = q0 - (q0 / g.Wp) * g.Wp;
                 const int r0 = rel + (t / 3 - 1) * g.Wp + (t % 3 - 1);
                 const uint32_t sX = sbase + (uint32_t)slot * g.stage_bytes, sG = sX + xbytes;
-                // descriptors advance by 16 positions (16 units of 16 B) per K step
-                const uint64_t db0 = smem_desc(sG + (uint32_t)relg * 16, 128, g.planeG);
+                // descriptors advance by 16 positions (16 rows of 32 B, 32 units of 16 B) per K step
+                const uint64_t db0 = smem_desc_sw32_mn(sG + (uint32_t)relg * 32, g.planeG);
 #pragma unroll
                 for (int mb = 0; mb < MB; mb++) {
                     const uint32_t dcol = tmem + (uint32_t)((tl * MB + mb) * N);
-                    const uint64_t da0 = smem_desc(sX + (uint32_t)(mb * (MR / 8)) * g.planeX + (uint32_t)r0 * 16, 128, g.planeX);
+                    const uint64_t da0 =
+                        smem_desc_sw32_mn(sX + (uint32_t)(mb * (MR / 16)) * g.planeX + (uint32_t)r0 * 32, g.planeX);
                     const int nks = g.KT / 16;
 #pragma unroll 8
                     for (int ks = 0; ks < nks; ks++)
-                        umma_bf16(dcol, da0 + (uint64_t)(16 * ks), db0 + (uint64_t)(16 * ks), IDESC,
+                        umma_bf16(dcol, da0 + (uint64_t)(32 * ks), db0 + (uint64_t)(32 * ks), IDESC,
                                   (k > 0 || ks > 0) ? 1u : 0u);
                 }
                 umma_commit(smem_u32(&empty[slot]));
@@ -2578,28 +2602,23 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_const
             tmem_wait_ld();
             const int t = tg0 + blk / MB, mb = blk % MB;
             const int m = mb * MR + row;
-            if (a.db && t == 4 && row >= 0 && m == Z::XREAL * 8) {  // the ones row: sum_v G[v][co]
+            if (a.db && t == 4 && row >= 0 && m == Z::XREAL * 16) {  // the ones row: sum_v G[v][co]
 #pragma unroll
-                for (int co = 0; co < COUT; co++) {
-                    const float v = __uint_as_float(r[PX == 3 ? co : COUT + co]);  // PX = 1: the plane-z block
-                    if (v != 0.0f) atomicAdd(&a.db[co], v);
+                for (int nn = 0; nn < N; nn++) {
+                    const int c = nn / COUT;  // gradient plane z0 + GLO + c: counted by the stage that owns it
+                    if (Z::GLO + c < 0 || Z::GLO + c >= Z::ZSTEP) continue;
+                    const float v = __uint_as_float(r[nn]);
+                    if (v != 0.0f) atomicAdd(&a.db[nn % COUT], v);
                 }
             }
-            if (row >= 0 && m < Z::MROWS) {
-                if (PX == 3) {  // row (dz + 1) cin + ci, column co
-                    const int tap = 9 * (m / CIN) + t, ci = m % CIN;
+            if (row >= 0 && m < Z::MROWS) {  // row b cin + ci (X plane b), column c cout + co (gradient plane c)
+                const int b = m / CIN, ci = m % CIN;
 #pragma unroll
-                    for (int co = 0; co < COUT; co++) {
-                        const float v = __uint_as_float(r[co]);
-                        if (v != 0.0f) atomicAdd(&a.dw[((size_t)co * 27 + tap) * CIN + ci], v);
-                    }
-                } else {  // row ci, column (dz + 1) cout + co
-#pragma unroll
-                    for (int nn = 0; nn < N; nn++) {
-                        const float v = __uint_as_float(r[nn]);
-                        if (v != 0.0f)
-                            atomicAdd(&a.dw[((size_t)(nn % COUT) * 27 + 9 * (nn / COUT) + t) * CIN + m], v);
-                    }
+                for (int nn = 0; nn < N; nn++) {
+                    const int dz = (Z::XLO + b) - (Z::GLO + nn / COUT);
+                    if (dz < -1 || dz > 1) continue;
+                    const float v = __uint_as_float(r[nn]);
+                    if (v != 0.0f) atomicAdd(&a.dw[((size_t)(nn % COUT) * 27 + 9 * (dz + 1) + t) * CIN + ci], v);
                 }
             }
         }
@@ -2711,10 +2730,10 @@ static bool launch_wgrad_tc(const WgradArgs &a, int sms, cudaStream_t s, cudaErr
 
 // the dz-stacked tcgen05 weight gradient (wgrad_zs_kernel); false when the
 // layer's shape has no configuration or a stage does not fit
-template <int CIN, int COUT, int PX>
+template <int CIN, int COUT, int MODE>
 static bool launch_wgrad_zs(const WgradArgs &a, int sms, cudaStream_t s, cudaError_t &err)
 {
-    using Z = WzsCfg<CIN, COUT, PX>;
+    using Z = WzsCfg<CIN, COUT, MODE>;
     if constexpr (!Z::OK) {
         return false;
     } else {
@@ -2740,11 +2759,11 @@ static bool launch_wgrad_zs(const WgradArgs &a, int sms, cudaStream_t s, cudaErr
             g.NRg = 2 + (KT + g.Wp - 1) / g.Wp;
             if (g.NR > 256 || g.NRg > 256) continue;
             g.T = (a.H * g.Wp + KT - 1) / KT;
-            g.ntiles = nb * a.D * g.T;
-            g.boxX = 16u * (uint32_t)g.Wp * (uint32_t)g.NR;
-            g.boxG = 16u * (uint32_t)g.Wp * (uint32_t)g.NRg;
-            g.planeX = (g.boxX + 127u) & ~127u;
-            g.planeG = (g.boxG + 127u) & ~127u;
+            g.ntiles = nb * ((a.D + Z::ZSTEP - 1) / Z::ZSTEP) * g.T;
+            g.boxX = 32u * (uint32_t)g.Wp * (uint32_t)g.NR;  // planes of 16 channels, 32-byte rows
+            g.boxG = 32u * (uint32_t)g.Wp * (uint32_t)g.NRg;
+            g.planeX = (g.boxX + 255u) & ~255u;
+            g.planeG = (g.boxG + 255u) & ~255u;
             g.stage_bytes = (((uint32_t)Z::XPLANES * g.planeX + (uint32_t)Z::GPLANES * g.planeG) + 1023u) & ~1023u;
             g.S = 0;
             const int min_stages = 2;
@@ -2770,31 +2789,35 @@ static bool launch_wgrad_zs(const WgradArgs &a, int sms, cudaStream_t s, cudaErr
             const cuuint64_t dims[5] = {C, (cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.D, (cuuint64_t)nb};
             const cuuint64_t strides[4] = {C * 2, (cuuint64_t)a.W * C * 2, (cuuint64_t)a.H * a.W * C * 2,
                                            (cuuint64_t)a.D * a.H * a.W * C * 2};
-            const cuuint32_t box[5] = {8u, (cuuint32_t)g.Wp, (cuuint32_t)rows[m], 1u, 1u};
+            const cuuint32_t box[5] = {16u, (cuuint32_t)g.Wp, (cuuint32_t)rows[m], 1u, 1u};
             const cuuint32_t estr[5] = {1u, 1u, 1u, 1u, 1u};
             if (enc(&maps[m], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void *>(bases[m]), dims, strides, box,
-                    estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
                 return false;
         }
-        err = smem_attributes(wgrad_zs_kernel<CIN, COUT, PX>, smem);
+        err = smem_attributes(wgrad_zs_kernel<CIN, COUT, MODE>, smem);
         if (err != cudaSuccess) return true;
         // with tap groups every group stages the tiles again: fewer CTAs per group
         const long long grid =
             std::min<long long>(g.ntiles, ((long long)per_sm * std::max(1, sms) + Z::NTG - 1) / Z::NTG);
-        wgrad_zs_kernel<CIN, COUT, PX><<<dim3((unsigned)grid, Z::NTG), 32 * (5 + Z::TPG), smem, s>>>(maps[0], maps[1],
-                                                                                                 a, g);
+        wgrad_zs_kernel<CIN, COUT, MODE><<<dim3((unsigned)grid, Z::NTG), 32 * (5 + Z::TPG), smem, s>>>(maps[0], maps[1],
+                                                                                                   a, g);
         err = cudaGetLastError();  // the kernel also adds the bias gradient (its ones row)
         return true;
     }
 }
 
-// which operand carries the dz axis in wgrad_zs_kernel: the one whose three
-// planes give the fewer MMA rows x columns (X along M for 16 or 32 input
-// channels, the gradient along N for 48 -> 16 and 96 -> 32)
+// the stage layout of wgrad_zs_kernel per layer: three output planes per stage
+// (MODE 2) for 16 -> 16, where one plane's MMAs are 64 x 16 and the issue rate
+// bounds the kernel; else the dz axis on the operand whose three planes give
+// the fewer MMA rows x columns (X along M for 16 or 32 input channels, the
+// gradient along N for 48 -> 16 and 96 -> 32)
 template <int CIN, int COUT>
 struct WzsPick {
-    static constexpr int PX = ((CIN == 48 && COUT == 16) || (CIN == 96 && COUT == 32)) ? 1 : 3;
+    static constexpr int MODE = (CIN == 16 && COUT == 16)
+                                    ? 2
+                                    : (((CIN == 48 && COUT == 16) || (CIN == 96 && COUT == 32)) ? 1 : 0);
 };
 
 cudaError_t wgrad3x3(const WgradArgs &a, int cin, int sms, cudaStream_t s)
@@ -2802,7 +2825,7 @@ cudaError_t wgrad3x3(const WgradArgs &a, int cin, int sms, cudaStream_t s)
 #define IAC_WG_CASE(CI, CO)                                               \
     if (cin == CI && a.cout == CO) {                                      \
         cudaError_t e = cudaSuccess;                                      \
-        if (a.slabs == 3 && launch_wgrad_zs<CI, CO, WzsPick<CI, CO>::PX>(a, sms, s, e)) return e; \
+        if (a.slabs == 3 && launch_wgrad_zs<CI, CO, WzsPick<CI, CO>::MODE>(a, sms, s, e)) return e; \
         if (a.slabs >= 2 && launch_wgrad_tc<CI, CO>(a, sms, s, e)) return e; \
         if (a.slabs >= 1 && launch_wgrad_slab<CI, CO>(a, sms, s, e)) return e; \
         return launch_wgrad<CI, CO>(a, sms, s);                           \
