@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(32 * (SUM_WARP + 1)) frame_sums_kernel(
     }
     if (!ok) s_err = 1;
     __syncthreads();
-    if (threadIdx.x == 0 && s_err && ctr) atomicAdd(&ctr->timeouts, 1ull);
+    if (threadIdx.x == 0 && s_err) note_timeout(ctr, SITE_AVERAGE);
 }
 
 __global__ void photon_means_kernel(const unsigned long long *__restrict__ total, uint32_t nframes, uint64_t npix,

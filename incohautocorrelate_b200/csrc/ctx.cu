@@ -89,7 +89,7 @@ __global__ void wait_flag_kernel(const volatile uint32_t *flag, uint32_t max_pol
         if (*flag != 0u) return;
         __nanosleep(1000);
     }
-    atomicAdd(&ctr->timeouts, 1ull);
+    iac::note_timeout(ctr, iac::SITE_WAIT_TEST);
 }
 }  // namespace
 
@@ -107,6 +107,7 @@ const char *iac_status_string(iac_status s)
     case IAC_ERR_TIMEOUT: return "device wait timed out";
     case IAC_ERR_OUT_OF_MESH: return "writes outside the mesh were skipped";
     case IAC_ERR_UNSUPPORTED: return "unsupported";
+    case IAC_ERR_BOUNDS: return "bounds check failed";
     }
     return "unknown status";
 }
@@ -187,8 +188,18 @@ iac_status iac_ctx_check(iac_ctx *ctx, void *stream, uint64_t *out_of_mesh)
     IAC_CUDA(cudaMemset(ctx->d_counters, 0, sizeof h));
     if (out_of_mesh) *out_of_mesh = h.out_of_mesh;
     if (h.timeouts) {
-        set_error("%llu bounded device waits ran out", (unsigned long long)h.timeouts);
+        char sites[256] = "";
+        for (int k = 0; k < SITE_COUNT; k++)
+            if (h.timeout_sites & (1ull << k)) {
+                if (sites[0]) strncat(sites, ", ", sizeof sites - strlen(sites) - 1);
+                strncat(sites, WAIT_SITE_NAMES[k], sizeof sites - strlen(sites) - 1);
+            }
+        set_error("%llu bounded device waits ran out (%s)", (unsigned long long)h.timeouts, sites);
         return IAC_ERR_TIMEOUT;
+    }
+    if (h.bad_stores) {
+        set_error("%llu stores failed a bounds check and were skipped", (unsigned long long)h.bad_stores);
+        return IAC_ERR_BOUNDS;
     }
     if (h.photon_overflow) {
         set_error("%llu photons did not fit the photon-list capacity and were dropped",

@@ -288,6 +288,19 @@ __device__ __forceinline__ void mask8(const bf16 *y8, float *o)
     }
 }
 
+// the copy of packed channels c .. of voxel v into the decoder input the
+// output is the skip part of (voxels beyond cat_voxels are counted as bad
+// stores and skipped)
+template <typename T>
+__device__ __forceinline__ void store_cat(const ConvArgs &a, long long v, int c, T pk)
+{
+    if (v >= a.cat_voxels) {
+        if (a.counters) atomicAdd(&a.counters->bad_stores, 1ull);
+        return;
+    }
+    *reinterpret_cast<T *>(a.ycat + v * a.cat_c + a.cat_off + c) = pk;
+}
+
 // epilogue for one output row segment of 8 channels with the bias already in
 // registers (b: channels c .. c+7): ReLU, bf16 (+fp32)
 __device__ __forceinline__ void store8_b(const ConvArgs &a, int cout, long long v, int c, const float *val,
@@ -306,6 +319,7 @@ __device__ __forceinline__ void store8_b(const ConvArgs &a, int cout, long long 
     pk.z = pack_bf16(o[4], o[5]);
     pk.w = pack_bf16(o[6], o[7]);
     *reinterpret_cast<uint4 *>(a.y + v * cout + c) = pk;
+    if (a.ycat) store_cat(a, v, c, pk);
     if (a.y32) {
         float4 *d = reinterpret_cast<float4 *>(a.y32 + v * cout + c);
         d[0] = make_float4(o[0], o[1], o[2], o[3]);
@@ -329,6 +343,7 @@ __device__ __forceinline__ void store8(const ConvArgs &a, int cout, long long v,
     pk.z = pack_bf16(o[4], o[5]);
     pk.w = pack_bf16(o[6], o[7]);
     *reinterpret_cast<uint4 *>(a.y + v * cout + c) = pk;
+    if (a.ycat) store_cat(a, v, c, pk);
     if (a.y32) {
         float4 *d = reinterpret_cast<float4 *>(a.y32 + v * cout + c);
         d[0] = make_float4(o[0], o[1], o[2], o[3]);
@@ -417,7 +432,7 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_tc_kernel(const ConvArgs a)
     // the last commit arrives once every MMA issued before it has completed
     const bool done =
         issued > 0 && mbar_wait(smem_u32(&mbar[(issued - 1) % Cfg::S]), ((issued - 1) / Cfg::S) & 1);
-    if ((s_err || !done) && tid == 0 && a.counters) atomicAdd(&a.counters->timeouts, 1ull);
+    if ((s_err || !done) && tid == 0) note_timeout(a.counters, SITE_CONV_TAP);
     tc_fence_after();
     __syncthreads();
     if (!s_err && done && issued == 27) {  // CTA-uniform: the TMEM loads are warp-collective
@@ -536,7 +551,9 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_mma_kernel(const ConvArgs a
                     if ((w & 0x8000u) || !(w & 0x7FFFu)) o0 = 0.0f;
                     if ((w & 0x80000000u) || !(w & 0x7FFF0000u)) o1 = 0.0f;
                 }
-                *reinterpret_cast<uint32_t *>(a.y + v * COUT + c) = pack_bf16(o0, o1);
+                const uint32_t pk = pack_bf16(o0, o1);
+                *reinterpret_cast<uint32_t *>(a.y + v * COUT + c) = pk;
+                if (a.ycat) store_cat(a, v, c, pk);
                 if (a.y32) *reinterpret_cast<float2 *>(a.y32 + v * COUT + c) = make_float2(o0, o1);
             }
         }
@@ -650,6 +667,7 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_slab_kernel(const ConvArgs 
         const long long tile = blockIdx.x + k * (long long)gridDim.x;
         const bool ok = mbar_wait(smem_u32(&accbar[k & 1]), (uint32_t)((k >> 1) & 1));
         if (!ok) s_err = 1;
+        __syncwarp();  // converged for the warp-collective TMEM loads
         tc_fence_after();
         const long long plane = tile / g.T;
         const int q = (int)(tile % g.T) * TILE_M + tid;
@@ -715,7 +733,7 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_slab_kernel(const ConvArgs 
     cp_async_wait_all();
     __syncthreads();
     if (!s_err && nst > 0) epilogue(my_tiles - 1);
-    if (s_err && tid == 0 && a.counters) atomicAdd(&a.counters->timeouts, 1ull);
+    if (s_err && tid == 0) note_timeout(a.counters, SITE_CONV_SLAB);
     tc_fence_before();
     __syncthreads();
     if (warp == 0) tmem_dealloc(tmem, TCOLS);
@@ -950,6 +968,7 @@ __global__ void __launch_bounds__(256) conv_tma_kernel(const __grid_constant__ C
     } else {  // epilogue: warps 0-3 own TMEM lanes 32w .. 32w+31
         for (long long k = 0; k < my_tiles; k++) {
             if (!mbar_wait_flag(smem_u32(&accfull[k & 1]), (uint32_t)((k >> 1) & 1), &s_err)) break;
+            __syncwarp();  // converged for the warp-collective TMEM loads
             tc_fence_after();
             const long long tile = blockIdx.x + k * (long long)gridDim.x;
             const long long plane = tile / g.T;
@@ -994,7 +1013,7 @@ __global__ void __launch_bounds__(256) conv_tma_kernel(const __grid_constant__ C
         // after an error: let the copies and MMAs already issued finish (bounded)
         // before the shared memory and TMEM are released
         if (tid == 0) {
-            if (a.counters) atomicAdd(&a.counters->timeouts, 1ull);
+            note_timeout(a.counters, SITE_CONV_TMA);
             // every copy still in flight: the stages of the last S loads
             for (long long i = s_issued > g.S ? s_issued - g.S : 0; i < s_issued; i++)
                 mbar_wait(smem_u32(&full[i % g.S]), (uint32_t)((i / g.S) & 1));
@@ -1169,6 +1188,7 @@ __global__ void __launch_bounds__(256, 1) conv_zcol_kernel(const __grid_constant
                     ok = false;
                     break;
                 }
+                __syncwarp();  // converged for the warp-collective TMEM loads
                 tc_fence_after();
                 uint32_t r[COUT];
                 const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(b * 3 * COUT);
@@ -1206,7 +1226,7 @@ __global__ void __launch_bounds__(256, 1) conv_zcol_kernel(const __grid_constant
         // after an error: let the copies and MMAs already issued finish (bounded)
         // before the shared memory and TMEM are released
         if (tid == 0) {
-            if (a.counters) atomicAdd(&a.counters->timeouts, 1ull);
+            note_timeout(a.counters, SITE_CONV_ZCOL);
             for (long long i = s_issued > g.S ? s_issued - g.S : 0; i < s_issued; i++)
                 mbar_wait(smem_u32(&full[i % g.S]), (uint32_t)((i / g.S) & 1));
             for (int w = 0; w < 3; w++) {
@@ -1409,6 +1429,16 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&accempty[stage % NB]));
         };
+        // a stage this group never reads is released only once its MMAs have
+        // completed: an arrival before that could land in the region's previous
+        // phase (the release of stage - NB) while a slower warp still reads it,
+        // when the warps of a group run at different speeds (tiles whose lower
+        // rows are padding store nothing)
+        auto release_unread = [&](long long stage) -> bool {
+            if (!mbar_wait_flag(smem_u32(&accfull[stage % NB]), (uint32_t)((stage / NB) & 1), &s_err)) return false;
+            release(stage);
+            return true;
+        };
         int j = 0;  // this CTA's stages before the current item
         bool ok = true;
         for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
@@ -1419,7 +1449,7 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
             const int y = q / g.Wp, xp = q - (q / g.Wp) * g.Wp;
             const bool valid = y < a.H && xp >= 1 && xp <= a.W;
             // stages this group never reads: those before its first output
-            for (int k = 0; k < grp && k < nz + 2; k++) release(j + k);
+            for (int k = 0; ok && k < grp && k < nz + 2; k++) ok = release_unread(j + k);
             int last = -1;  // this group's last output of the item
             for (int ol = grp; ok && ol < nz; ol += 2) {
                 for (int k = 0; k < 3; k++)
@@ -1429,6 +1459,9 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
                         break;
                     }
                 if (!ok) break;
+                // the warp converges before the warp-collective TMEM loads: the
+                // previous output's stores diverge on `valid` and may be slow
+                __syncwarp();
                 tc_fence_after();
                 uint32_t rr[COUTH];
                 const uint32_t c0 = (uint32_t)(((j + ol) % NB) * N3);
@@ -1463,8 +1496,11 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
                 }
             }
             if (!ok) break;
-            // the stages after this group's last output (or all but the first grp if it had none)
-            for (int k = last >= 0 ? last + 2 : grp; k < nz + 2; k++) release(j + k);
+            // the stages after this group's last output (or all but the first grp if it had none);
+            // stage last + 2 was read by the last output
+            for (int k = last >= 0 ? last + 2 : grp; ok && k < nz + 2; k++)
+                ok = (last >= 0 && k == last + 2) ? (release(j + k), true) : release_unread(j + k);
+            if (!ok) break;
             j += nz + 2;
         }
     }
@@ -1473,7 +1509,7 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
         // after an error: let the copies and MMAs already issued finish (bounded)
         // before the shared memory and TMEM are released
         if (tid == 0) {
-            if (a.counters) atomicAdd(&a.counters->timeouts, 1ull);
+            note_timeout(a.counters, SITE_CONV_ZCAT);
             for (int i = s_issued > g.S ? s_issued - g.S : 0; i < s_issued; i++)
                 mbar_wait(smem_u32(&full[i % g.S]), (uint32_t)((i / g.S) & 1));
             for (int w = 0; w < NISS; w++) {
@@ -2394,7 +2430,7 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_tc_kernel(const __grid_const
         tc_fence_before();
     }
     if (s_err && tid == 0) {
-        if (a.counters) atomicAdd(&a.counters->timeouts, 1ull);
+        note_timeout(a.counters, SITE_WGRAD_TC);
         long long consumed = s_consumed[0];
         for (int i = 1; i < NI; i++) consumed = s_consumed[i] < consumed ? s_consumed[i] : consumed;
         for (long long k = consumed; k < s_issued; k++)
@@ -2625,7 +2661,7 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_const
         tc_fence_before();
     }
     if (s_err && tid == 0) {
-        if (a.counters) atomicAdd(&a.counters->timeouts, 1ull);
+        note_timeout(a.counters, SITE_WGRAD_ZS);
         long long consumed = s_consumed[0];
         for (int i = 1; i < ntap; i++) consumed = s_consumed[i] < consumed ? s_consumed[i] : consumed;
         for (long long k = consumed; k < s_issued; k++)
@@ -3053,83 +3089,76 @@ cudaError_t relu_mask(const bf16 *g, const bf16 *y, bf16 *out, long long n, cuda
 }
 
 // gcat [V][c0 + c1] at full resolution: g0 (coarse, c0) = mask(y0) * sum of the
-// 8 children's first c0 channels (backward of nearest upsampling), g1 (full,
-// c1) = the last c1 channels (skip connection)
+// 8 children's first c0 channels (backward of nearest upsampling); the last c1
+// channels, the skip connection's gradient, are read in place by pool_grad_mask
 __global__ void split_concat_kernel(const bf16 *__restrict__ gcat, int c0, int c1, const bf16 *__restrict__ y0,
-                                    bf16 *__restrict__ g0, bf16 *__restrict__ g1, int D, int H, int W,
-                                    long long n_coarse, long long n_full)
+                                    bf16 *__restrict__ g0, int D, int H, int W, long long n_coarse)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int C = c0 + c1;
-    if (i < n_coarse) {
-        const int nc = c0 / 8, c = (int)(i % nc) * 8;
-        const long long u = i / nc;
-        const Vox q = decode(u, D / 2, H / 2, W / 2, n_coarse / nc);
-        float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        for (int k = 0; k < 8; k++) {
-            const long long v =
-                (((long long)q.n * D + 2 * q.z + (k >> 2)) * H + 2 * q.y + ((k >> 1) & 1)) * W + 2 * q.x + (k & 1);
-            float f[8];
-            load8(gcat + v * C + c, f);
+    if (i >= n_coarse) return;
+    const int nc = c0 / 8, c = (int)(i % nc) * 8;
+    const long long u = i / nc;
+    const Vox q = decode(u, D / 2, H / 2, W / 2, n_coarse / nc);
+    float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int k = 0; k < 8; k++) {
+        const long long v =
+            (((long long)q.n * D + 2 * q.z + (k >> 2)) * H + 2 * q.y + ((k >> 1) & 1)) * W + 2 * q.x + (k & 1);
+        float f[8];
+        load8(gcat + v * C + c, f);
 #pragma unroll
-            for (int j = 0; j < 8; j++) s[j] += f[j];
-        }
-        float fy[8];
-        load8(y0 + u * c0 + c, fy);
-#pragma unroll
-        for (int j = 0; j < 8; j++) s[j] = fy[j] > 0.0f ? s[j] : 0.0f;
-        store8b(g0 + u * c0 + c, s);
-    } else if (i < n_coarse + n_full) {
-        const long long k = i - n_coarse;
-        const int nc = c1 / 8, c = (int)(k % nc) * 8;
-        const long long v = k / nc;
-        *reinterpret_cast<uint4 *>(g1 + v * c1 + c) = *reinterpret_cast<const uint4 *>(gcat + v * C + c0 + c);
+        for (int j = 0; j < 8; j++) s[j] += f[j];
     }
+    float fy[8];
+    load8(y0 + u * c0 + c, fy);
+#pragma unroll
+    for (int j = 0; j < 8; j++) s[j] = fy[j] > 0.0f ? s[j] : 0.0f;
+    store8b(g0 + u * c0 + c, s);
 }
 
-cudaError_t split_concat_grad(const bf16 *gcat, int c0, int c1, const bf16 *y0, bf16 *g0, bf16 *g1, int D, int H,
-                              int W, int nb, cudaStream_t s)
+cudaError_t split_concat_grad(const bf16 *gcat, int c0, int c1, const bf16 *y0, bf16 *g0, int D, int H, int W,
+                              int nb, cudaStream_t s)
 {
     const long long V = (long long)nb * D * H * W;
-    const long long nco = V / 8 * (c0 / 8), nfu = V * (c1 / 8);
-    split_concat_kernel<<<(unsigned)((nco + nfu + 255) / 256), 256, 0, s>>>(gcat, c0, c1, y0, g0, g1, D, H, W, nco,
-                                                                             nfu);
+    const long long nco = V / 8 * (c0 / 8);
+    split_concat_kernel<<<(unsigned)((nco + 255) / 256), 256, 0, s>>>(gcat, c0, c1, y0, g0, D, H, W, nco);
     return cudaGetLastError();
 }
 
-// out[v] = concat(src0 at the coarse parent of v, src1[v]): the decoder input of
-// nearest 2x upsampling followed by skip concatenation
-__global__ void concat_up_kernel(const bf16 *__restrict__ src0, int c0, const bf16 *__restrict__ src1, int c1,
-                                 bf16 *__restrict__ out, int D, int H, int W, long long total)
+// cat[v][0 .. c0) = src0[parent(v)]: the coarse part of a decoder input
+// (nearest 2x upsampling; the skip part is written by the layer that makes
+// it).  Thread = (coarse voxel, 8 channels): one load, the 8 children stored.
+// D, H, W: the full resolution.
+__global__ void upsample_into_kernel(const bf16 *__restrict__ src0, int c0, bf16 *__restrict__ cat, int C, int D,
+                                     int H, int W, long long total)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
-    const int C = c0 + c1, nc = C / 8, c = (int)(i % nc) * 8;
-    const long long v = i / nc;
-    uint4 val;
-    if (c < c0) {
-        const Vox q = decode(v, D, H, W, total / nc);
-        const long long u = (((long long)q.n * (D / 2) + q.z / 2) * (H / 2) + q.y / 2) * (W / 2) + q.x / 2;
-        val = *reinterpret_cast<const uint4 *>(src0 + u * c0 + c);
-    } else {
-        val = *reinterpret_cast<const uint4 *>(src1 + v * c1 + (c - c0));
+    const int nc = c0 / 8, c = (int)(i % nc) * 8;
+    const long long u = i / nc;
+    const Vox q = decode(u, D / 2, H / 2, W / 2, total / nc);
+    const uint4 val = *reinterpret_cast<const uint4 *>(src0 + u * c0 + c);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const long long v =
+            (((long long)q.n * D + 2 * q.z + (k >> 2)) * H + 2 * q.y + ((k >> 1) & 1)) * W + 2 * q.x + (k & 1);
+        *reinterpret_cast<uint4 *>(cat + v * C + c) = val;
     }
-    *reinterpret_cast<uint4 *>(out + v * C + c) = val;
 }
 
-cudaError_t concat_up(const bf16 *src0, int c0, const bf16 *src1, int c1, bf16 *out, int D, int H, int W, int nb,
-                      cudaStream_t s)
+cudaError_t upsample_into(const bf16 *src0, int c0, bf16 *cat, int C, int D, int H, int W, int nb, cudaStream_t s)
 {
-    const long long total = (long long)nb * D * H * W * ((c0 + c1) / 8);
-    concat_up_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(src0, c0, src1, c1, out, D, H, W, total);
+    const long long total = (long long)nb * (D / 2) * (H / 2) * (W / 2) * (c0 / 8);
+    upsample_into_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(src0, c0, cat, C, D, H, W, total);
     return cudaGetLastError();
 }
 
 // out = (gskip + gpool(parent) / 8) * (y > 0): gradient of a skip tensor that
-// also fed an average pool
-__global__ void pool_grad_mask_kernel(const bf16 *__restrict__ gskip, const bf16 *__restrict__ gpool,
-                                      const bf16 *__restrict__ y, bf16 *__restrict__ out, int C, int D, int H, int W,
-                                      long long total)
+// also fed an average pool; gskip has gskip_stride channels per voxel (the
+// skip channels of the decoder input's gradient, read in place)
+__global__ void pool_grad_mask_kernel(const bf16 *__restrict__ gskip, int gskip_stride,
+                                      const bf16 *__restrict__ gpool, const bf16 *__restrict__ y,
+                                      bf16 *__restrict__ out, int C, int D, int H, int W, long long total)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
@@ -3138,7 +3167,7 @@ __global__ void pool_grad_mask_kernel(const bf16 *__restrict__ gskip, const bf16
     const Vox q = decode(v, D, H, W, total / nc);
     const long long u = (((long long)q.n * (D / 2) + q.z / 2) * (H / 2) + q.y / 2) * (W / 2) + q.x / 2;
     float a[8], b[8], fy[8];
-    load8(gskip + v * C + c, a);
+    load8(gskip + v * gskip_stride + c, a);
     load8(gpool + u * C + c, b);
     load8(y + v * C + c, fy);
 #pragma unroll
@@ -3146,11 +3175,12 @@ __global__ void pool_grad_mask_kernel(const bf16 *__restrict__ gskip, const bf16
     store8b(out + v * C + c, a);
 }
 
-cudaError_t pool_grad_mask(const bf16 *gskip, const bf16 *gpool, const bf16 *y, bf16 *out, int C, int D, int H,
-                           int W, int nb, cudaStream_t s)
+cudaError_t pool_grad_mask(const bf16 *gskip, int gskip_stride, const bf16 *gpool, const bf16 *y, bf16 *out, int C,
+                           int D, int H, int W, int nb, cudaStream_t s)
 {
     const long long total = (long long)nb * D * H * W * (C / 8);
-    pool_grad_mask_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(gskip, gpool, y, out, C, D, H, W, total);
+    pool_grad_mask_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(gskip, gskip_stride, gpool, y, out, C, D,
+                                                                          H, W, total);
     return cudaGetLastError();
 }
 

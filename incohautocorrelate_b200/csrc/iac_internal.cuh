@@ -59,8 +59,34 @@ struct DeviceCounters {
     unsigned long long out_of_mesh;
     unsigned long long timeouts;
     unsigned long long photon_overflow;  // photons beyond a photon-list capacity (dropped)
-    unsigned long long pad[5];
+    unsigned long long timeout_sites;    // bit k: a kernel of WAIT_SITE_NAMES[k] gave up a bounded wait
+    unsigned long long bad_stores;       // stores whose index failed a kernel's bounds check (skipped)
+    unsigned long long pad[3];
 };
+
+// kernels with bounded waits, as bits of DeviceCounters::timeout_sites
+enum WaitSite {
+    SITE_AVERAGE = 0,
+    SITE_WAIT_TEST,
+    SITE_CONV_TAP,
+    SITE_CONV_SLAB,
+    SITE_CONV_TMA,
+    SITE_CONV_ZCOL,
+    SITE_CONV_ZCAT,
+    SITE_WGRAD_TC,
+    SITE_WGRAD_ZS,
+    SITE_COUNT
+};
+constexpr const char *WAIT_SITE_NAMES[SITE_COUNT] = {"average",        "flag wait",      "conv (per tap)",
+                                                     "conv (slabs)",   "conv (TMA)",     "conv (z-column)",
+                                                     "conv (dz-concat)", "weight gradient", "weight gradient (dz-stacked)"};
+
+__device__ __forceinline__ void note_timeout(DeviceCounters *c, int site)
+{
+    if (!c) return;
+    atomicAdd(&c->timeouts, 1ull);
+    atomicOr(&c->timeout_sites, 1ull << site);
+}
 
 // A growable device scratch buffer owned by the context.
 struct Scratch {
