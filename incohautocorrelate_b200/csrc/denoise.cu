@@ -55,6 +55,7 @@ struct iac_denoiser {
     bf16 *b1 = nullptr, *b2 = nullptr, *d2a = nullptr, *d2b = nullptr, *d1a = nullptr, *d1b = nullptr;
     bf16 *cat1 = nullptr, *cat2 = nullptr;  // decoder inputs: up(d2b) ++ s1, up(b2) ++ s2
     long long cat1_voxels = 0;              // voxels of cat1 (cat2: an eighth)
+    uint64_t step_launches = 0;             // kernels in the training-step graph
     // gradients
     bf16 *gA = nullptr, *gB = nullptr, *gcat1 = nullptr;  // full resolution
     bf16 *hA = nullptr, *hB = nullptr, *gcat2 = nullptr;  // half
@@ -351,7 +352,6 @@ iac_status run_backward(iac_denoiser *dn, const float *d_in, const float *d_targ
     DN_CHECK(wgrad3x3_first(d_in, dn->gB, dn->g + dn->p_off[0], dn->g + dn->p_off[0] + 16 * 27, D, H, W, V,
                             dn->ctx->sm_count, s),
              "layer 0 weight gradient");
-    dn->ctx->launches += 45;
     return IAC_OK;
 }
 
@@ -554,7 +554,7 @@ iac_status iac_denoise_forward(iac_denoiser *dn, const float *d_in, uint32_t nb,
     h.out = d_out;
     h.V = (long long)nb * D * H * W;
     DN_CHECK(head(h, dn->ctx->sm_count, s), "denoiser head");
-    dn->ctx->launches += 16;
+    dn->ctx->launches += take_launches();
     return IAC_OK;
 }
 
@@ -570,6 +570,7 @@ iac_status iac_denoise_backward(iac_denoiser *dn, const float *d_in, const float
     cudaStream_t s = (cudaStream_t)stream;
     DN_CHECK(cudaMemsetAsync(dn->d_loss, 0, 8, s), "clear loss");
     st = run_backward(dn, d_in, d_target, d_weight, nb, D, H, W, d_out, dn->d_loss, nullptr, s);
+    dn->ctx->launches += take_launches();
     if (st != IAC_OK) return st;
     if (h_loss) {
         double t = 0;
@@ -588,8 +589,9 @@ iac_status iac_denoise_adamw_step(iac_denoiser *dn, const iac_adamw *opt, void *
                     opt->eps > 0,
                 "AdamW hyper-parameters out of range");
     DeviceGuard guard(dn->ctx->device);
-    dn->ctx->launches += 1;
-    return refresh_tiles(dn, opt, (cudaStream_t)stream);
+    const iac_status st = refresh_tiles(dn, opt, (cudaStream_t)stream);
+    dn->ctx->launches += take_launches();
+    return st;
 }
 
 iac_status iac_denoise_train_steps(iac_denoiser *dn, const uint16_t *d_in_meshes, const uint16_t *d_tgt_meshes,
@@ -658,6 +660,7 @@ iac_status iac_denoise_train_steps(iac_denoiser *dn, const uint16_t *d_in_meshes
         }
         cudaGraph_t graph = nullptr;
         const cudaError_t ee = cudaStreamEndCapture(s, &graph);
+        dn->step_launches = take_launches();  // recorded now, launched by every replay
         if (ce != cudaSuccess || st != IAC_OK || ee != cudaSuccess) {
             if (graph) cudaGraphDestroy(graph);
             if (st != IAC_OK) return st;
@@ -676,7 +679,7 @@ iac_status iac_denoise_train_steps(iac_denoiser *dn, const uint16_t *d_in_meshes
         DN_CHECK(cudaStreamWaitEvent(caller, dn->own_ev[1], 0), "order replay");
     }
     dn->adam_step += nsteps;
-    dn->ctx->launches += (uint64_t)nsteps * 49;
+    dn->ctx->launches += (uint64_t)nsteps * dn->step_launches + take_launches();
     return IAC_OK;
 }
 
@@ -690,7 +693,7 @@ iac_status iac_denoise_crop_patches(iac_ctx *ctx, const uint16_t *d_meshes, uint
     DN_CHECK(crop_patches(reinterpret_cast<const bf16 *>(d_meshes), (int)nmeshes, (int)E, d_plan, (int)nb, (int)P,
                           d_out, ctx->d_counters, (cudaStream_t)stream),
              "crop patches");
-    ctx->launches += 1;
+    ctx->launches += take_launches();
     return IAC_OK;
 }
 
@@ -725,7 +728,7 @@ iac_status iac_denoise_conv3x3(iac_ctx *ctx, int backend, const uint16_t *d_src0
     const cudaError_t e = conv3x3(a, (int)(c0 + c1), (int)cout, backend, (cudaStream_t)stream);
     IAC_REQUIRE(e != cudaErrorInvalidValue, "no 3x3x3 kernel for %u -> %u channels", c0 + c1, cout);
     DN_CHECK(e, "conv3x3");
-    ctx->launches += 1;
+    ctx->launches += take_launches();
     return IAC_OK;
 }
 
@@ -758,7 +761,7 @@ iac_status iac_denoise_wgrad3x3(iac_ctx *ctx, int slabs, const uint16_t *d_src0,
     const cudaError_t e = wgrad3x3(a, (int)(c0 + c1), ctx->sm_count, (cudaStream_t)stream);
     IAC_REQUIRE(e != cudaErrorInvalidValue, "no 3x3x3 weight-gradient kernel for %u -> %u channels", c0 + c1, cout);
     DN_CHECK(e, "wgrad3x3");
-    ctx->launches += 1;
+    ctx->launches += take_launches();
     return IAC_OK;
 }
 
@@ -772,7 +775,7 @@ iac_status iac_denoise_mesh_input(iac_ctx *ctx, const uint64_t *d_full, uint32_t
     DN_CHECK(mesh_input(d_full, (int)S, (int)E, scale, d_f32, reinterpret_cast<bf16 *>(d_bf16),
                         (cudaStream_t)stream),
              "mesh input");
-    ctx->launches += 1;
+    ctx->launches += take_launches();
     return IAC_OK;
 }
 

@@ -69,6 +69,10 @@ struct WgradArgs {
     DeviceCounters *counters;
 };
 
+// kernels launched by the calling host thread since the previous call (every
+// launch helper below counts its launches)
+uint64_t take_launches();
+
 // kernels (denoise_kernels.cu)
 cudaError_t conv3x3(const ConvArgs &a, int cin, int cout, int backend, cudaStream_t s);
 cudaError_t conv3x3_first(const float *x, const bf16 *w, const float *bias, bf16 *y, int D, int H,

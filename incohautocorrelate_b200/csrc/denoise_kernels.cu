@@ -40,6 +40,15 @@
 namespace iac {
 namespace dn {
 
+// kernels launched by this host thread since the last take_launches()
+static thread_local uint64_t launch_count = 0;
+uint64_t take_launches()
+{
+    const uint64_t n = launch_count;
+    launch_count = 0;
+    return n;
+}
+
 // --------------------------------------------------------------------------
 // PTX helpers
 // --------------------------------------------------------------------------
@@ -778,6 +787,7 @@ static bool launch_slab(const ConvArgs &a, cudaStream_t s, cudaError_t &err)
     per_sm = std::min(per_sm, 512 / TCOLS);
     per_sm = std::min(per_sm, 16);
     const long long grid = std::min<long long>(g.ntiles, (long long)std::max(1, per_sm) * std::max(1, a.sms));
+    ++launch_count;
     conv_slab_kernel<CIN, COUT><<<(unsigned)grid, CONV_THREADS, smem, s>>>(a, g);
     err = cudaGetLastError();
     return true;
@@ -1604,6 +1614,7 @@ static void launch_zcol_nb(const ConvArgs &a, TmaGeom g, const CUtensorMap &map,
     err = smem_attributes(conv_zcol_kernel<CIN, COUT, NB>, smem);
     if (err != cudaSuccess) return;
     const long long grid = std::min<long long>(g.nitems, grid_max);
+    ++launch_count;
     conv_zcol_kernel<CIN, COUT, NB><<<(unsigned)grid, 256, smem, s>>>(map, a, g);
     err = cudaGetLastError();
 }
@@ -1701,6 +1712,7 @@ static bool launch_zcat(const ConvArgs &a, const TmaGeom &g0, uint32_t budget, c
         auto k = conv_zcat_kernel<CIN, COUT, Z::COUTH, Z::NB, Z::NISS, Z::PER_SM>;
         err = smem_attributes(k, smem);
         if (err != cudaSuccess) return true;
+        ++launch_count;
         k<<<dim3((unsigned)grid, NG), 32 * (ZCAT_ISSUER0 + Z::NISS), smem, s>>>(map, a, g);
         err = cudaGetLastError();
         return true;
@@ -1815,6 +1827,7 @@ static bool launch_tma(const ConvArgs &a, cudaStream_t s, cudaError_t &err)
         if (ni == 3) {
             err = smem_attributes(conv_tma_kernel<CIN, COUT, 3>, smem);
             if (err != cudaSuccess) return true;
+            ++launch_count;
             conv_tma_kernel<CIN, COUT, 3><<<(unsigned)grid, 32 * (5 + 3), smem, s>>>(map, a, g);
             err = cudaGetLastError();
             return true;
@@ -1822,6 +1835,7 @@ static bool launch_tma(const ConvArgs &a, cudaStream_t s, cudaError_t &err)
     }
     err = smem_attributes(conv_tma_kernel<CIN, COUT, 1>, smem);
     if (err != cudaSuccess) return true;
+    ++launch_count;
     conv_tma_kernel<CIN, COUT, 1><<<(unsigned)grid, TMA_THREADS, smem, s>>>(map, a, g);
     err = cudaGetLastError();
     return true;
@@ -1842,12 +1856,14 @@ static cudaError_t launch_conv(const ConvArgs &a, int backend, cudaStream_t s)
         cudaError_t e = cudaFuncSetAttribute(conv_tc_kernel<CIN, COUT>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
+        ++launch_count;
         conv_tc_kernel<CIN, COUT><<<grid, CONV_THREADS, smem, s>>>(a);
     } else {
         const uint32_t smem = MmaCfg<CIN, COUT>::SMEM;
         cudaError_t e = cudaFuncSetAttribute(conv_mma_kernel<CIN, COUT>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
+        ++launch_count;
         conv_mma_kernel<CIN, COUT><<<grid, CONV_THREADS, smem, s>>>(a);
     }
     return cudaGetLastError();
@@ -1948,6 +1964,7 @@ cudaError_t conv3x3_first(const float *x, const bf16 *w, const float *bias, bf16
 {
     if (W % 4) return cudaErrorInvalidValue;
     const long long threads = V / 4;
+    ++launch_count;
     conv_first_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(x, w, bias, y, D, H, W, V);
     return cudaGetLastError();
 }
@@ -2098,6 +2115,7 @@ static cudaError_t launch_wgrad(const WgradArgs &a, int sms, cudaStream_t s)
     cudaError_t e = cudaFuncSetAttribute(wgrad_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)Cfg::SMEM);
     if (e != cudaSuccess) return e;
+    ++launch_count;
     wgrad_kernel<CIN, COUT><<<dim3(per_tap, 27), CONV_THREADS, Cfg::SMEM, s>>>(a);
     return cudaGetLastError();
 }
@@ -2255,6 +2273,7 @@ static bool launch_wgrad_slab(const WgradArgs &a, int sms, cudaStream_t s, cudaE
     // about 4 CTAs per SM in total, at least 2 tiles per CTA
     const long long per_group = std::max<long long>(
         1, std::min<long long>((g.ntiles + 1) / 2, (4LL * std::max(1, sms) + groups - 1) / groups));
+    ++launch_count;
     wgrad_slab_kernel<CIN, COUT><<<dim3((unsigned)per_group, groups), CONV_THREADS, smem, s>>>(a, g);
     err = cudaGetLastError();
     return true;
@@ -2753,11 +2772,13 @@ static bool launch_wgrad_tc(const WgradArgs &a, int sms, cudaStream_t s, cudaErr
     const int groups = 27 / Cfg::G;
     const long long per_group = std::max<long long>(
         1, std::min<long long>((g.ntiles + 1) / 2, ((long long)per_sm * std::max(1, sms) + groups - 1) / groups));
+    ++launch_count;
     wgrad_tc_kernel<CIN, COUT><<<dim3((unsigned)per_group, groups), 32 * (5 + Cfg::NI), smem, s>>>(maps[0], maps[1], a, g);
     if ((err = cudaGetLastError()) != cudaSuccess) return true;
     if (a.db) {
         const int lanes = 256 / COUT;
         const long long blocks = std::min<long long>((a.V + lanes - 1) / lanes, 4LL * std::max(1, sms));
+        ++launch_count;
         bias_grad_kernel<<<(unsigned)blocks, lanes * COUT, lanes * COUT * sizeof(float), s>>>(a.g, COUT, a.V, a.db);
         err = cudaGetLastError();
     }
@@ -2837,6 +2858,7 @@ static bool launch_wgrad_zs(const WgradArgs &a, int sms, cudaStream_t s, cudaErr
         // with tap groups every group stages the tiles again: fewer CTAs per group
         const long long grid =
             std::min<long long>(g.ntiles, ((long long)per_sm * std::max(1, sms) + Z::NTG - 1) / Z::NTG);
+        ++launch_count;
         wgrad_zs_kernel<CIN, COUT, MODE><<<dim3((unsigned)grid, Z::NTG), 32 * (5 + Z::TPG), smem, s>>>(maps[0], maps[1],
                                                                                                    a, g);
         err = cudaGetLastError();  // the kernel also adds the bias gradient (its ones row)
@@ -3010,6 +3032,7 @@ cudaError_t wgrad3x3_first(const float *x, const bf16 *g, float *dw, float *db, 
     const long long ngroups = (V + WGF_ROWS - 1) / WGF_ROWS;
     const long long blocks = (ngroups + WGF_WARPS - 1) / WGF_WARPS;
     const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(blocks, 2LL * sms));
+    ++launch_count;
     wgrad_first_kernel<<<grid, 32 * WGF_WARPS, smem, s>>>(x, g, dw, db, D, H, W, V);
     return cudaGetLastError();
 }
@@ -3064,6 +3087,7 @@ __global__ void avgpool2_kernel(const bf16 *__restrict__ x, bf16 *__restrict__ y
 cudaError_t avgpool2(const bf16 *x, bf16 *y, int C, int D, int H, int W, int nb, cudaStream_t s)
 {
     const long long total = (long long)nb * (D / 2) * (H / 2) * (W / 2) * (C / 8);
+    ++launch_count;
     avgpool2_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(x, y, C, D, H, W, total);
     return cudaGetLastError();
 }
@@ -3084,6 +3108,7 @@ __global__ void relu_mask_kernel(const bf16 *__restrict__ g, const bf16 *__restr
 cudaError_t relu_mask(const bf16 *g, const bf16 *y, bf16 *out, long long n, cudaStream_t s)
 {
     const long long n8 = n / 8;
+    ++launch_count;
     relu_mask_kernel<<<(unsigned)((n8 + 255) / 256), 256, 0, s>>>(g, y, out, n8);
     return cudaGetLastError();
 }
@@ -3121,6 +3146,7 @@ cudaError_t split_concat_grad(const bf16 *gcat, int c0, int c1, const bf16 *y0, 
 {
     const long long V = (long long)nb * D * H * W;
     const long long nco = V / 8 * (c0 / 8);
+    ++launch_count;
     split_concat_kernel<<<(unsigned)((nco + 255) / 256), 256, 0, s>>>(gcat, c0, c1, y0, g0, D, H, W, nco);
     return cudaGetLastError();
 }
@@ -3149,6 +3175,7 @@ __global__ void upsample_into_kernel(const bf16 *__restrict__ src0, int c0, bf16
 cudaError_t upsample_into(const bf16 *src0, int c0, bf16 *cat, int C, int D, int H, int W, int nb, cudaStream_t s)
 {
     const long long total = (long long)nb * (D / 2) * (H / 2) * (W / 2) * (c0 / 8);
+    ++launch_count;
     upsample_into_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(src0, c0, cat, C, D, H, W, total);
     return cudaGetLastError();
 }
@@ -3179,6 +3206,7 @@ cudaError_t pool_grad_mask(const bf16 *gskip, int gskip_stride, const bf16 *gpoo
                            int D, int H, int W, int nb, cudaStream_t s)
 {
     const long long total = (long long)nb * D * H * W * (C / 8);
+    ++launch_count;
     pool_grad_mask_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(gskip, gskip_stride, gpool, y, out, C, D,
                                                                           H, W, total);
     return cudaGetLastError();
@@ -3248,6 +3276,7 @@ __global__ void __launch_bounds__(256) head_kernel(const HeadArgs a)
 cudaError_t head(const HeadArgs &a, int sms, cudaStream_t s)
 {
     const long long blocks = (a.V + 255) / 256;
+    ++launch_count;
     head_kernel<<<(unsigned)std::max<long long>(1, std::min<long long>(blocks, 8LL * sms)), 256, 0, s>>>(a);
     return cudaGetLastError();
 }
@@ -3298,6 +3327,7 @@ __global__ void adamw_kernel(const AdamArgs a)
 
 cudaError_t adamw(const AdamArgs &a, cudaStream_t s)
 {
+    ++launch_count;
     adamw_kernel<<<(unsigned)((a.n + 255) / 256), 256, 0, s>>>(a);
     return cudaGetLastError();
 }
@@ -3343,6 +3373,7 @@ cudaError_t crop_patches(const bf16 *meshes, int nmesh, int E, const int *plan, 
                          DeviceCounters *counters, cudaStream_t s, const long long *d_step)
 {
     const long long total = (long long)nb * P * P * P;
+    ++launch_count;
     crop_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(meshes, nmesh, E, plan, P, out, total, counters,
                                                                 d_step, nb);
     return cudaGetLastError();
@@ -3362,6 +3393,7 @@ __global__ void step_kernel(long long *d_step, long long set_opt, int mode)
 
 cudaError_t step_counter(long long *d_step, long long set_opt, int advance, cudaStream_t s)
 {
+    ++launch_count;
     step_kernel<<<1, 1, 0, s>>>(d_step, set_opt, advance);
     return cudaGetLastError();
 }
@@ -3383,6 +3415,7 @@ __global__ void mesh_input_kernel(const unsigned long long *__restrict__ full, i
 cudaError_t mesh_input(const uint64_t *full, int S, int E, double scale, float *o32, bf16 *o16, cudaStream_t s)
 {
     const long long total = (long long)E * E * E;
+    ++launch_count;
     mesh_input_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(
         reinterpret_cast<const unsigned long long *>(full), S, E, scale, o32, o16, total);
     return cudaGetLastError();
