@@ -1897,6 +1897,7 @@ cudaError_t conv3x3(const ConvArgs &a, int cin, int cout, int backend, cudaStrea
 // loads.  Taps outside the volume read 0 (zero padding); a voxel's sums run
 // over the taps in order.  W is a multiple of 4.
 // --------------------------------------------------------------------------
+template <bool VEC>  // VEC: x is 16-byte aligned (the middle four of a row's six loads as one float4)
 __global__ void __launch_bounds__(256) conv_first_kernel(const float *__restrict__ x, const bf16 *__restrict__ w,
                                                          const float *__restrict__ bias, bf16 *__restrict__ y,
                                                          int D, int H, int W, long long V)
@@ -1925,9 +1926,15 @@ __global__ void __launch_bounds__(256) conv_first_kernel(const float *__restrict
             const bool in = zin && (unsigned)(q.y + dy - 1) < (unsigned)H;
             const float *row = x + v0 + (dz - 1) * HW + (long long)(dy - 1) * W;  // voxel x0 of the row
             float r[6];
+            // the four voxels' own column as one 16-byte load (x0, W and H W are multiples of 4)
+            const float4 mid = !in ? make_float4(0.0f, 0.0f, 0.0f, 0.0f)
+                                   : (VEC ? *reinterpret_cast<const float4 *>(row)
+                                          : make_float4(row[0], row[1], row[2], row[3]));
             r[0] = in && left ? row[-1] : 0.0f;
-#pragma unroll
-            for (int k = 0; k < 4; k++) r[k + 1] = in ? row[k] : 0.0f;
+            r[1] = mid.x;
+            r[2] = mid.y;
+            r[3] = mid.z;
+            r[4] = mid.w;
             r[5] = in && right ? row[4] : 0.0f;
 #pragma unroll
             for (int dx = 0; dx < 3; dx++) {
@@ -1965,7 +1972,10 @@ cudaError_t conv3x3_first(const float *x, const bf16 *w, const float *bias, bf16
     if (W % 4) return cudaErrorInvalidValue;
     const long long threads = V / 4;
     ++launch_count;
-    conv_first_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(x, w, bias, y, D, H, W, V);
+    if ((reinterpret_cast<uintptr_t>(x) & 15) == 0)
+        conv_first_kernel<true><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(x, w, bias, y, D, H, W, V);
+    else
+        conv_first_kernel<false><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(x, w, bias, y, D, H, W, V);
     return cudaGetLastError();
 }
 
@@ -2912,6 +2922,7 @@ cudaError_t wgrad3x3(const WgradArgs &a, int cin, int sms, cudaStream_t s)
 constexpr int WGF_WARPS = 8;
 constexpr int WGF_ROWS = 128;  // voxels per warp and iteration
 constexpr int WGF_WARP_BYTES = (4 + 2) * WGF_ROWS * 16;
+template <bool VEC>  // VEC: x is 16-byte aligned
 __global__ void __launch_bounds__(32 * WGF_WARPS, 2) wgrad_first_kernel(const float *__restrict__ x,
                                                                         const bf16 *__restrict__ g,
                                                                         float *__restrict__ dw,
@@ -2947,9 +2958,14 @@ __global__ void __launch_bounds__(32 * WGF_WARPS, 2) wgrad_first_kernel(const fl
                 const bool in = zin && (unsigned)(q.y + dy - 1) < (unsigned)H;
                 const float *row = x + (q.ok ? v0 : 0) + (dz - 1) * HW + (long long)(dy - 1) * W;
                 float *rr = r[3 * dz + dy];
+                const float4 mid = !in ? make_float4(0.0f, 0.0f, 0.0f, 0.0f)
+                                       : (VEC ? *reinterpret_cast<const float4 *>(row)
+                                              : make_float4(row[0], row[1], row[2], row[3]));
                 rr[0] = in && left ? row[-1] : 0.0f;
-#pragma unroll
-                for (int k = 0; k < 4; k++) rr[k + 1] = in ? row[k] : 0.0f;
+                rr[1] = mid.x;
+                rr[2] = mid.y;
+                rr[3] = mid.z;
+                rr[4] = mid.w;
                 rr[5] = in && right ? row[4] : 0.0f;
             }
         }
@@ -3027,13 +3043,15 @@ cudaError_t wgrad3x3_first(const float *x, const bf16 *g, float *dw, float *db, 
 {
     if (W % 4) return cudaErrorInvalidValue;
     const int smem = WGF_WARPS * WGF_WARP_BYTES;
-    const cudaError_t e = cudaFuncSetAttribute(wgrad_first_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const bool vec = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
+    auto k = vec ? wgrad_first_kernel<true> : wgrad_first_kernel<false>;
+    const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     const long long ngroups = (V + WGF_ROWS - 1) / WGF_ROWS;
     const long long blocks = (ngroups + WGF_WARPS - 1) / WGF_WARPS;
     const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(blocks, 2LL * sms));
     ++launch_count;
-    wgrad_first_kernel<<<grid, 32 * WGF_WARPS, smem, s>>>(x, g, dw, db, D, H, W, V);
+    k<<<grid, 32 * WGF_WARPS, smem, s>>>(x, g, dw, db, D, H, W, V);
     return cudaGetLastError();
 }
 
