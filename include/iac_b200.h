@@ -32,8 +32,7 @@ typedef enum {
     IAC_ERR_NO_MEMORY = 3,    /* device or pinned allocation failed */
     IAC_ERR_TIMEOUT = 4,      /* a bounded device-side wait ran out */
     IAC_ERR_OUT_OF_MESH = 5,  /* writes fell outside the mesh and were skipped */
-    IAC_ERR_UNSUPPORTED = 6,  /* no sm_100 device, or a mode not built */
-    IAC_ERR_BOUNDS = 7        /* a kernel's bounds check skipped stores (an internal error) */
+    IAC_ERR_UNSUPPORTED = 6   /* no sm_100 device, or a mode not built */
 } iac_status;
 
 /* Settings::Interpolation, IAC/Settings.h:158 */

@@ -19,7 +19,6 @@ IAC_ERR_NO_MEMORY = 3
 IAC_ERR_TIMEOUT = 4
 IAC_ERR_OUT_OF_MESH = 5
 IAC_ERR_UNSUPPORTED = 6
-IAC_ERR_BOUNDS = 7
 
 NEAREST = 0
 LINEAR = 1

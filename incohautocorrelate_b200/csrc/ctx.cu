@@ -107,7 +107,6 @@ const char *iac_status_string(iac_status s)
     case IAC_ERR_TIMEOUT: return "device wait timed out";
     case IAC_ERR_OUT_OF_MESH: return "writes outside the mesh were skipped";
     case IAC_ERR_UNSUPPORTED: return "unsupported";
-    case IAC_ERR_BOUNDS: return "bounds check failed";
     }
     return "unknown status";
 }
@@ -196,10 +195,6 @@ iac_status iac_ctx_check(iac_ctx *ctx, void *stream, uint64_t *out_of_mesh)
             }
         set_error("%llu bounded device waits ran out (%s)", (unsigned long long)h.timeouts, sites);
         return IAC_ERR_TIMEOUT;
-    }
-    if (h.bad_stores) {
-        set_error("%llu stores failed a bounds check and were skipped", (unsigned long long)h.bad_stores);
-        return IAC_ERR_BOUNDS;
     }
     if (h.photon_overflow) {
         set_error("%llu photons did not fit the photon-list capacity and were dropped",

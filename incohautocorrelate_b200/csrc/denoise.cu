@@ -54,7 +54,6 @@ struct iac_denoiser {
     bf16 *e1a = nullptr, *s1 = nullptr, *p1 = nullptr, *e2a = nullptr, *s2 = nullptr, *p2 = nullptr;
     bf16 *b1 = nullptr, *b2 = nullptr, *d2a = nullptr, *d2b = nullptr, *d1a = nullptr, *d1b = nullptr;
     bf16 *cat1 = nullptr, *cat2 = nullptr;  // decoder inputs: up(d2b) ++ s1, up(b2) ++ s2
-    long long cat1_voxels = 0;              // voxels of cat1 (cat2: an eighth)
     uint64_t step_launches = 0;             // kernels in the training-step graph
     // gradients
     bf16 *gA = nullptr, *gB = nullptr, *gcat1 = nullptr;  // full resolution
@@ -255,30 +254,20 @@ iac_status run_forward(iac_denoiser *dn, const float *x, uint32_t nb, uint32_t D
     const int be = dn->backend;
     DN_CHECK(conv3x3_first(x, dn->wf + dn->wf_off[0], dn->p + dn->p_off[0] + 16 * 27, dn->e1a, D, H, W, V, s),
              "denoiser layer 0");
-    // the decoder inputs (64 + 32 and 32 + 16 channels) are materialised, so the
-    // 3x3x3 kernels read plain tensors through TMA: the layers making the skip
-    // parts also write them there, the coarse parts are upsampled into them
-    ConvArgs a1 = conv_args(dn, 1, nullptr, dn->e1a, dn->s1, D, H, W, V);
-    a1.ycat = dn->cat1;
-    a1.cat_voxels = dn->cat1_voxels;
-    a1.cat_c = 48;
-    a1.cat_off = 32;
-    DN_CHECK(conv3x3(a1, 16, 16, be, s), "layer 1");
-    DN_CHECK(avgpool2(dn->s1, dn->p1, 16, D, H, W, nb, s), "pool 1");
+    DN_CHECK(conv3x3(conv_args(dn, 1, nullptr, dn->e1a, dn->s1, D, H, W, V), 16, 16, be, s), "layer 1");
+    DN_CHECK(avgpool2(dn->s1, 16, dn->p1, 16, D, H, W, nb, s), "pool 1");
     DN_CHECK(conv3x3(conv_args(dn, 2, nullptr, dn->p1, dn->e2a, D2, H2, W2, V2), 16, 32, be, s), "layer 2");
-    ConvArgs a3 = conv_args(dn, 3, nullptr, dn->e2a, dn->s2, D2, H2, W2, V2);
-    a3.ycat = dn->cat2;
-    a3.cat_voxels = dn->cat1_voxels / 8;
-    a3.cat_c = 96;
-    a3.cat_off = 64;
-    DN_CHECK(conv3x3(a3, 32, 32, be, s), "layer 3");
-    DN_CHECK(avgpool2(dn->s2, dn->p2, 32, D2, H2, W2, nb, s), "pool 2");
+    DN_CHECK(conv3x3(conv_args(dn, 3, nullptr, dn->e2a, dn->s2, D2, H2, W2, V2), 32, 32, be, s), "layer 3");
+    DN_CHECK(avgpool2(dn->s2, 32, dn->p2, 32, D2, H2, W2, nb, s), "pool 2");
     DN_CHECK(conv3x3(conv_args(dn, 4, nullptr, dn->p2, dn->b1, D4, H4, W4, V4), 32, 64, be, s), "layer 4");
     DN_CHECK(conv3x3(conv_args(dn, 5, nullptr, dn->b1, dn->b2, D4, H4, W4, V4), 64, 64, be, s), "layer 5");
-    DN_CHECK(upsample_into(dn->b2, 64, dn->cat2, 96, D2, H2, W2, nb, s), "upsample 2");
+    // the decoder inputs (64 + 32 and 32 + 16 channels) are materialised, so the
+    // 3x3x3 kernels read plain tensors through TMA: the coarse part upsampled,
+    // the skip tensor copied
+    DN_CHECK(concat_up(dn->b2, 64, dn->s2, 32, dn->cat2, D2, H2, W2, nb, s), "concat 2");
     DN_CHECK(conv3x3(conv_args(dn, 6, nullptr, dn->cat2, dn->d2a, D2, H2, W2, V2), 96, 32, be, s), "layer 6");
     DN_CHECK(conv3x3(conv_args(dn, 7, nullptr, dn->d2a, dn->d2b, D2, H2, W2, V2), 32, 32, be, s), "layer 7");
-    DN_CHECK(upsample_into(dn->d2b, 32, dn->cat1, 48, D, H, W, nb, s), "upsample 1");
+    DN_CHECK(concat_up(dn->d2b, 32, dn->s1, 16, dn->cat1, D, H, W, nb, s), "concat 1");
     DN_CHECK(conv3x3(conv_args(dn, 8, nullptr, dn->cat1, dn->d1a, D, H, W, V), 48, 16, be, s), "layer 8");
     DN_CHECK(conv3x3(conv_args(dn, 9, nullptr, dn->d1a, dn->d1b, D, H, W, V), 16, 16, be, s), "layer 9");
     return IAC_OK;
@@ -337,14 +326,14 @@ iac_status run_backward(iac_denoiser *dn, const float *d_in, const float *d_targ
     // layer 4: X = p2
     if ((st = wgrad(dn, 4, nullptr, dn->p2, dn->qB, D4, H4, W4, V4, s)) != IAC_OK) return st;
     if ((st = dgrad(dn, 4, dn->qB, dn->qA, D4, H4, W4, V4, s)) != IAC_OK) return st;  // d p2 (32 ch)
-    DN_CHECK(pool_grad_mask(dn->gcat2 + 64, 96, dn->qA, dn->s2, dn->hA, 32, D2, H2, W2, nb, s), "pool grad 2");
+    DN_CHECK(pool_grad_mask(dn->gcat2 + 64, 96, dn->qA, dn->s2, 32, dn->hA, 32, D2, H2, W2, nb, s), "pool grad 2");
     // layer 3: X = e2a
     if ((st = wgrad(dn, 3, nullptr, dn->e2a, dn->hA, D2, H2, W2, V2, s)) != IAC_OK) return st;
     if ((st = dgrad(dn, 3, dn->hA, dn->hB, D2, H2, W2, V2, s, dn->e2a)) != IAC_OK) return st;
     // layer 2: X = p1
     if ((st = wgrad(dn, 2, nullptr, dn->p1, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
     if ((st = dgrad(dn, 2, dn->hB, dn->hA, D2, H2, W2, V2, s)) != IAC_OK) return st;  // d p1 (16 ch)
-    DN_CHECK(pool_grad_mask(dn->gcat1 + 32, 48, dn->hA, dn->s1, dn->gA, 16, D, H, W, nb, s), "pool grad 1");
+    DN_CHECK(pool_grad_mask(dn->gcat1 + 32, 48, dn->hA, dn->s1, 16, dn->gA, 16, D, H, W, nb, s), "pool grad 1");
     // layer 1: X = e1a
     if ((st = wgrad(dn, 1, nullptr, dn->e1a, dn->gA, D, H, W, V, s)) != IAC_OK) return st;
     if ((st = dgrad(dn, 1, dn->gA, dn->gB, D, H, W, V, s, dn->e1a)) != IAC_OK) return st;
@@ -411,9 +400,9 @@ iac_status iac_denoise_create(iac_ctx *ctx, uint32_t max_batch, uint32_t D, uint
     dn->d_loss = (double *)A(8);
     const size_t b = 2;
     dn->e1a = (bf16 *)A(V * 16 * b);
-    dn->s1 = (bf16 *)A(V * 16 * b);
     dn->d1a = (bf16 *)A(V * 16 * b);
     dn->d1b = (bf16 *)A(V * 16 * b);
+    dn->s1 = (bf16 *)A(V * 16 * b);
     dn->p1 = (bf16 *)A(V2 * 16 * b);
     dn->e2a = (bf16 *)A(V2 * 32 * b);
     dn->s2 = (bf16 *)A(V2 * 32 * b);
@@ -423,7 +412,6 @@ iac_status iac_denoise_create(iac_ctx *ctx, uint32_t max_batch, uint32_t D, uint
     dn->b1 = (bf16 *)A(V4 * 64 * b);
     dn->b2 = (bf16 *)A(V4 * 64 * b);
     dn->cat1 = (bf16 *)A(V * 48 * b);
-    dn->cat1_voxels = (long long)V;
     dn->cat2 = (bf16 *)A(V2 * 96 * b);
     dn->gA = (bf16 *)A(V * 16 * b);
     dn->gB = (bf16 *)A(V * 16 * b);

@@ -38,11 +38,6 @@ struct ConvArgs {
     float *y32;          // optional fp32 copy of the output
     int relu;
     const bf16 *mask_y;  // optional [V][cout]: outputs where mask_y <= 0 are set to 0 (ReLU derivative)
-    // optional second destination: the decoder input this output is the skip
-    // part of, ycat[v][cat_off + co] with cat_c channels per voxel
-    bf16 *ycat;
-    int cat_c, cat_off;
-    long long cat_voxels;  // voxels ycat holds
     int D, H, W;         // output (= src1) dims per batch item
     long long V;         // nb * D * H * W
     DeviceCounters *counters;
@@ -80,13 +75,14 @@ cudaError_t conv3x3_first(const float *x, const bf16 *w, const float *bias, bf16
 cudaError_t wgrad3x3(const WgradArgs &a, int cin, int sms, cudaStream_t s);
 cudaError_t wgrad3x3_first(const float *x, const bf16 *g, float *dw, float *db, int D, int H, int W,
                            long long V, int sms, cudaStream_t s);
-cudaError_t avgpool2(const bf16 *x, bf16 *y, int C, int D, int H, int W, int nb, cudaStream_t s);
+cudaError_t avgpool2(const bf16 *x, int x_stride, bf16 *y, int C, int D, int H, int W, int nb, cudaStream_t s);
 cudaError_t relu_mask(const bf16 *g, const bf16 *y, bf16 *out, long long n, cudaStream_t s);
 cudaError_t split_concat_grad(const bf16 *gcat, int c0, int c1, const bf16 *y0, bf16 *g0, int D, int H, int W,
                               int nb, cudaStream_t s);
-cudaError_t upsample_into(const bf16 *src0, int c0, bf16 *cat, int C, int D, int H, int W, int nb, cudaStream_t s);
-cudaError_t pool_grad_mask(const bf16 *gskip, int gskip_stride, const bf16 *gpool, const bf16 *y, bf16 *out, int C,
-                           int D, int H, int W, int nb, cudaStream_t s);
+cudaError_t concat_up(const bf16 *src0, int c0, const bf16 *src1, int c1, bf16 *cat, int D, int H, int W, int nb,
+                      cudaStream_t s);
+cudaError_t pool_grad_mask(const bf16 *gskip, int gskip_stride, const bf16 *gpool, const bf16 *y, int y_stride,
+                           bf16 *out, int C, int D, int H, int W, int nb, cudaStream_t s);
 
 struct HeadArgs {
     const float *x;       // network input (residual), [V]

@@ -297,19 +297,6 @@ __device__ __forceinline__ void mask8(const bf16 *y8, float *o)
     }
 }
 
-// the copy of packed channels c .. of voxel v into the decoder input the
-// output is the skip part of (voxels beyond cat_voxels are counted as bad
-// stores and skipped)
-template <typename T>
-__device__ __forceinline__ void store_cat(const ConvArgs &a, long long v, int c, T pk)
-{
-    if (v >= a.cat_voxels) {
-        if (a.counters) atomicAdd(&a.counters->bad_stores, 1ull);
-        return;
-    }
-    *reinterpret_cast<T *>(a.ycat + v * a.cat_c + a.cat_off + c) = pk;
-}
-
 // epilogue for one output row segment of 8 channels with the bias already in
 // registers (b: channels c .. c+7): ReLU, bf16 (+fp32)
 __device__ __forceinline__ void store8_b(const ConvArgs &a, int cout, long long v, int c, const float *val,
@@ -328,7 +315,37 @@ __device__ __forceinline__ void store8_b(const ConvArgs &a, int cout, long long 
     pk.z = pack_bf16(o[4], o[5]);
     pk.w = pack_bf16(o[6], o[7]);
     *reinterpret_cast<uint4 *>(a.y + v * cout + c) = pk;
-    if (a.ycat) store_cat(a, v, c, pk);
+    if (a.y32) {
+        float4 *d = reinterpret_cast<float4 *>(a.y32 + v * cout + c);
+        d[0] = make_float4(o[0], o[1], o[2], o[3]);
+        d[1] = make_float4(o[4], o[5], o[6], o[7]);
+    }
+}
+
+// store8_b with the ReLU mask of the 8 channels already loaded (mk, when a.mask_y is set)
+__device__ __forceinline__ void store8_bm(const ConvArgs &a, int cout, long long v, int c, const float *val,
+                                          const float *b, uint4 mk)
+{
+    float o[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const float t = val[j] + b[j];
+        o[j] = a.relu ? fmaxf(t, 0.0f) : t;
+    }
+    if (a.mask_y) {
+        const uint32_t w[4] = {mk.x, mk.y, mk.z, mk.w};
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if ((w[j] & 0x8000u) || !(w[j] & 0x7FFFu)) o[2 * j] = 0.0f;
+            if ((w[j] & 0x80000000u) || !(w[j] & 0x7FFF0000u)) o[2 * j + 1] = 0.0f;
+        }
+    }
+    uint4 pk;
+    pk.x = pack_bf16(o[0], o[1]);
+    pk.y = pack_bf16(o[2], o[3]);
+    pk.z = pack_bf16(o[4], o[5]);
+    pk.w = pack_bf16(o[6], o[7]);
+    *reinterpret_cast<uint4 *>(a.y + v * cout + c) = pk;
     if (a.y32) {
         float4 *d = reinterpret_cast<float4 *>(a.y32 + v * cout + c);
         d[0] = make_float4(o[0], o[1], o[2], o[3]);
@@ -352,7 +369,6 @@ __device__ __forceinline__ void store8(const ConvArgs &a, int cout, long long v,
     pk.z = pack_bf16(o[4], o[5]);
     pk.w = pack_bf16(o[6], o[7]);
     *reinterpret_cast<uint4 *>(a.y + v * cout + c) = pk;
-    if (a.ycat) store_cat(a, v, c, pk);
     if (a.y32) {
         float4 *d = reinterpret_cast<float4 *>(a.y32 + v * cout + c);
         d[0] = make_float4(o[0], o[1], o[2], o[3]);
@@ -562,7 +578,6 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_mma_kernel(const ConvArgs a
                 }
                 const uint32_t pk = pack_bf16(o0, o1);
                 *reinterpret_cast<uint32_t *>(a.y + v * COUT + c) = pk;
-                if (a.ycat) store_cat(a, v, c, pk);
                 if (a.y32) *reinterpret_cast<float2 *>(a.y32 + v * COUT + c) = make_float2(o0, o1);
             }
         }
@@ -1535,6 +1550,306 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
     }
 }
 
+// K-major operand with the 64-byte swizzle: rows of 32 bf16 (64 bytes), 8-row
+// groups 512 bytes apart (SBO), layout type 4.  The start may sit at any row,
+// and at +32 bytes within a row for its second K step (checked for row offsets
+// 0 .. 67, base-offset field 0).
+__device__ __forceinline__ uint64_t smem_desc_sw64(uint32_t addr)
+{
+    return (uint64_t)((addr & 0x3FFFFu) >> 4) | (1ull << 16) | ((uint64_t)(512u >> 4) << 32) | (1ull << 46) |
+           (4ull << 61);
+}
+
+// --------------------------------------------------------------------------
+// x-pair z-column convolution for 16 input channels.  conv_zcat_kernel stages
+// one 32-byte TMA row per padded position; at 16 channels the TMA unit's row
+// rate (about one per clock per SM) bounds it.  Here the 16-channel NDHWC
+// tensor is viewed as rows of x-pairs (two voxels, 64 bytes) and staged with
+// the 64-byte swizzle: a slab row is a padded pair position q = y Wq + px
+// (Wq = W/2 + 2, pair px holding voxels 2px - 2 and 2px - 1, pairs 0 and
+// Wq - 1 the zero halo), a tile 128 pair positions = 256 voxel slots, and a
+// slab of rows y_lo .. y_lo + NR - 1 reaches every pair a tile's taps need.
+// An MMA row is a pair (K = 32: both voxels' 16 channels) and its N = 96
+// columns are (dz, output voxel j of the pair, 16 output channels).  Output
+// voxel 2p + j takes input voxel 2(p + pdx) + k (k: K step = voxel of the
+// input pair) at dx = 2 pdx + k - j, so a pair tap (dy, pdx) multiplies the
+// pair row shifted by dy Wq + pdx by B(dy, pdx, k)[n][ci] = W(dz, dy, dx)[co][ci]
+// where |dx| <= 1, else 0: the pair taps pdx = -1 and +1 need only their K step
+// k = 1 and k = 0 (the other is all zeros), so a stage issues 12 MMAs of
+// 128 x 96 x 16 for 256 voxels where conv_zcat_kernel issues 18 of 128 x 48 x 16,
+// reads fewer operand bytes, and stages its slab in 2.8x fewer TMA rows.  The
+// z-column structure, the TMEM regions (NB of 96 columns), the roles and the
+// release protocol are conv_zcat_kernel's; with one CTA per SM (480 TMEM
+// columns) the drain runs in three groups of four warps (outputs ol = g mod 3),
+// and a drain thread stores its pair's two voxels; a data gradient's ReLU mask
+// for them is loaded before the thread waits for the output's MMAs.
+// --------------------------------------------------------------------------
+constexpr int ZPAIR_NB = 5;
+constexpr int ZPAIR_NISS = 3;
+constexpr int ZPAIR_GROUPS = 3;                        // drain groups of four warps
+constexpr int ZPAIR_DRAIN = 4 * ZPAIR_GROUPS;          // drain warps
+constexpr int ZPAIR_PRODUCER = ZPAIR_DRAIN;            // warp index of the TMA producer
+constexpr int ZPAIR_ISSUER0 = ZPAIR_DRAIN + 1;         // first MMA-issuing warp
+constexpr int ZPAIR_N = 96;                            // 3 dz x 2 voxels x 16 channels
+constexpr uint32_t ZPAIR_WBYTES = 9u * 2u * 2u * ZPAIR_N * 16u;  // [pair tap][k][kc][n][8] bf16
+
+template <int COUT>
+__global__ void __launch_bounds__(32 * (ZPAIR_ISSUER0 + ZPAIR_NISS), 1)
+    conv_zpair_kernel(const __grid_constant__ CUtensorMap xmap, const ConvArgs a, const TmaGeom g)
+{
+    constexpr int CIN = 16, NB = ZPAIR_NB, NISS = ZPAIR_NISS, N3 = ZPAIR_N;
+    const int c_lo = (int)blockIdx.y * 16;
+    constexpr uint32_t TCOLS = tma_tcols(NB * N3);
+    static_assert(NB * N3 <= 512, "NB regions within 512 TMEM columns");
+    constexpr uint32_t IDESC = idesc_bf16(TILE_M, N3);
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t full[8], empty[8], accfull[NB], accempty[NB];
+    __shared__ uint32_t s_tmem;
+    __shared__ volatile int s_err;
+    __shared__ int s_issued, s_last[NISS];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t sbase = smem_u32(smem);
+    const uint32_t wbase = sbase;                  // pair-tap weights [9][2][2][96][8]
+    const uint32_t stbase = sbase + g.wres_bytes;  // stages: one input-plane pair slab each
+    // B(pt, k)[kc][n][e], pt = 3 (dy + 1) + pdx + 1, n = 32 dzi + 16 j + co, ci = 8 kc + e
+    for (int i = tid; i < 9 * 2 * 2 * N3; i += blockDim.x) {
+        const int n = i % N3;
+        int r = i / N3;
+        const int kc = r % 2;
+        r /= 2;
+        const int k = r % 2, pt = r / 2;
+        const int dzi = n / 32, j = (n / 16) % 2, co = c_lo + n % 16;
+        const int dy = pt / 3 - 1, pdx = pt % 3 - 1;
+        const int dx = 2 * pdx + k - j;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (dx >= -1 && dx <= 1) {
+            const int tap = 9 * dzi + 3 * (dy + 1) + dx + 1;
+            v = *reinterpret_cast<const uint4 *>(a.w + (((size_t)tap * (CIN / 8) + kc) * COUT + co) * 8);
+        }
+        *reinterpret_cast<uint4 *>(smem + (size_t)i * 16) = v;
+    }
+    fence_proxy_async();  // the weights written by threads, read by the tensor core
+    if (tid == 0) {
+        for (int k = 0; k < g.S; k++) {
+            mbar_init(smem_u32(&full[k]), 1);
+            mbar_init(smem_u32(&empty[k]), 1);
+        }
+        for (int b = 0; b < NB; b++) {
+            mbar_init(smem_u32(&accfull[b]), 1);
+            mbar_init(smem_u32(&accempty[b]), ZPAIR_DRAIN);  // every drain warp
+        }
+        fence_mbar_init();
+        s_err = 0;
+        s_issued = 0;
+        for (int i = 0; i < NISS; i++) s_last[i] = -1;
+    }
+    if (warp == ZPAIR_PRODUCER) {
+        tmem_alloc(smem_u32(&s_tmem), TCOLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const int nzc = (a.D + g.ZC - 1) / g.ZC;  // z-chunks per column
+    const int HW = a.H * a.W;
+    const int WP = g.Wp;                      // padded pairs per row
+    auto item = [&](long long it, int &n, int &q0, int &z0, int &z1) {
+        const long long col = it / nzc;
+        z0 = (int)(it % nzc) * g.ZC;
+        z1 = z0 + g.ZC < a.D ? z0 + g.ZC : a.D;
+        n = (int)(col / g.T);
+        q0 = (int)(col % g.T) * TILE_M;
+    };
+
+    if (warp == ZPAIR_PRODUCER) {
+        if (lane == 0) {  // one pair slab per input plane z0-1 .. z1 (planes outside the volume arrive as zeros)
+            int j = 0, slot = 0, round = 0;
+            bool ok = true;
+            for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
+                int n, q0, z0, z1;
+                item(it, n, q0, z0, z1);
+                const int y_lo = floor_div(q0 - WP - 1, WP);
+                for (int pz = z0 - 1; pz <= z1; pz++, j++) {
+                    if (j >= g.S && !mbar_wait_flag(smem_u32(&empty[slot]), (uint32_t)((round - 1) & 1), &s_err)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t st = stbase + (uint32_t)slot * g.stage_bytes;
+                    const uint32_t fb = smem_u32(&full[slot]);
+                    mbar_expect_tx(fb, g.box_bytes);
+                    tma_load_5d(st, &xmap, 0, -1, y_lo, pz, n, fb);  // pairs -1 .. Wq - 2 of rows y_lo ..
+                    s_issued = j + 1;
+                    if (++slot == g.S) {
+                        slot = 0;
+                        round++;
+                    }
+                }
+            }
+        }
+    } else if (warp >= ZPAIR_ISSUER0) {
+        const int iw = warp - ZPAIR_ISSUER0;  // stages j with j % NISS == iw
+        if (lane == 0) {
+            int j = 0, slot = 0, round = 0, r = 0, rround = 0;
+            bool ok = true;
+            for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
+                int n, q0, z0, z1;
+                item(it, n, q0, z0, z1);
+                const int rel = q0 - floor_div(q0 - WP - 1, WP) * WP;  // q0 within the slab
+                for (int k = 0; k < z1 - z0 + 2; k++, j++) {
+                    const int cur_slot = slot, cur_round = round, cur_r = r, cur_rround = rround;
+                    if (++slot == g.S) {
+                        slot = 0;
+                        round++;
+                    }
+                    if (++r == NB) {
+                        r = 0;
+                        rround++;
+                    }
+                    if (j % NISS != iw) continue;
+                    if (!mbar_wait_flag(smem_u32(&full[cur_slot]), (uint32_t)(cur_round & 1), &s_err) ||
+                        (j >= NB && !mbar_wait_flag(smem_u32(&accempty[cur_r]), (uint32_t)((cur_rround - 1) & 1), &s_err))) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t st = stbase + (uint32_t)cur_slot * g.stage_bytes;
+                    const uint32_t dcol = tmem + (uint32_t)(cur_r * N3);
+                    // descriptors as a base plus offsets in 16-byte units: a pair row is 4 units,
+                    // the second K step of a row 2 units in; a (pair tap, k) weight block
+                    // 2 N3 units
+                    const uint64_t da0 = smem_desc_sw64(st + (uint32_t)rel * 64);
+                    const uint64_t db0 = smem_desc(wbase, N3 * 16, 128);
+                    bool first = true;
+#pragma unroll
+                    for (int pt = 0; pt < 9; pt++) {
+                        const int dy = pt / 3 - 1, pdx = pt % 3 - 1;
+#pragma unroll
+                        for (int kk = 0; kk < 2; kk++) {
+                            if ((pdx == -1 && kk == 0) || (pdx == 1 && kk == 1)) continue;  // all-zero weights
+                            const uint64_t da = da0 + (uint64_t)(int64_t)(4 * (dy * WP + pdx) + 2 * kk);
+                            const uint64_t db = db0 + (uint64_t)((uint32_t)((pt * 2 + kk) * 2 * N3));
+                            umma_bf16(dcol, da, db, IDESC, first ? 0u : 1u);
+                            first = false;
+                        }
+                    }
+                    umma_commit(smem_u32(&empty[cur_slot]));
+                    umma_commit(smem_u32(&accfull[cur_r]));
+                    s_last[iw] = j;
+                }
+            }
+        }
+    } else {  // drain: group grp = warp / 4 takes outputs ol = grp mod ZPAIR_GROUPS; warp % 4 = its TMEM quadrant
+        constexpr int NG = ZPAIR_GROUPS;
+        const int grp = warp >> 2, quad = warp & 3;
+        const int row = quad * 32 + lane;  // this thread's pair position in the tile
+        float bias[16];
+#pragma unroll
+        for (int c = 0; c < 16; c++) bias[c] = a.bias ? a.bias[c_lo + c] : 0.0f;
+        const uint32_t lb = tmem + ((uint32_t)(quad * 32) << 16);
+        auto release = [&](long long stage) {
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&accempty[stage % NB]));
+        };
+        // a stage this warp has not read is released only once its MMAs have completed (an
+        // earlier arrival could complete the region's previous phase while a slower warp reads it)
+        auto release_unread = [&](long long stage) -> bool {
+            if (!mbar_wait_flag(smem_u32(&accfull[stage % NB]), (uint32_t)((stage / NB) & 1), &s_err)) return false;
+            release(stage);
+            return true;
+        };
+        // every warp releases every stage of an item once: those before its group's first
+        // output, after output ol the stages ol .. ol + NG - 1 (the first three read by it), and
+        // at the end those after its last output's range
+        int j = 0;
+        bool ok = true;
+        for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
+            int n, q0, z0, z1;
+            item(it, n, q0, z0, z1);
+            const int nz = z1 - z0;
+            const int q = q0 + row;
+            const int y = q / WP, px = q - (q / WP) * WP;
+            const bool valid = y < a.H && px >= 1 && 2 * px <= a.W;
+            for (int k = 0; ok && k < grp && k < nz + 2; k++) ok = release_unread(j + k);
+            int last = -1;
+            for (int ol = grp; ok && ol < nz; ol += NG) {
+                const long long v = ((long long)n * a.D + z0 + ol) * HW + (long long)y * a.W + (2 * px - 2);
+                uint4 mk[4] = {};  // the ReLU mask of the pair's two voxels, loaded ahead of the MMA waits
+                if (a.mask_y && valid) {
+#pragma unroll
+                    for (int m = 0; m < 4; m++)
+                        mk[m] = *reinterpret_cast<const uint4 *>(a.mask_y + (v + (m >> 1)) * COUT + c_lo + 8 * (m & 1));
+                }
+                for (int k = 0; k < 3; k++)
+                    if (!mbar_wait_flag(smem_u32(&accfull[(j + ol + k) % NB]), (uint32_t)(((j + ol + k) / NB) & 1),
+                                        &s_err)) {
+                        ok = false;
+                        break;
+                    }
+                if (!ok) break;
+                __syncwarp();  // converged for the warp-collective TMEM loads
+                tc_fence_after();
+                uint32_t rr[32];
+                const uint32_t c0 = (uint32_t)(((j + ol) % NB) * N3);            // dz -1 block of stage ol
+                const uint32_t c1 = (uint32_t)(((j + ol + 1) % NB) * N3 + 32);   // dz 0 of stage ol + 1
+                const uint32_t c2 = (uint32_t)(((j + ol + 2) % NB) * N3 + 64);   // dz +1 of stage ol + 2
+#pragma unroll
+                for (int c = 0; c < 32; c += 16) {
+                    uint32_t (&r0)[16] = *reinterpret_cast<uint32_t(*)[16]>(&rr[c]);
+                    uint32_t t[16];
+                    tmem_ld16(lb + c0 + (uint32_t)c, r0);
+                    tmem_ld16(lb + c1 + (uint32_t)c, t);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int jj = 0; jj < 16; jj++)  // (dz -1) + (dz 0)
+                        r0[jj] = __float_as_uint(__fadd_rn(__uint_as_float(r0[jj]), __uint_as_float(t[jj])));
+                    tmem_ld16(lb + c2 + (uint32_t)c, t);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int jj = 0; jj < 16; jj++)  // then + (dz +1)
+                        r0[jj] = __float_as_uint(__fadd_rn(__uint_as_float(r0[jj]), __uint_as_float(t[jj])));
+                }
+                tc_fence_before();
+                for (int k = 0; k < 3 && ol + k < nz + 2 && k < NG; k++) release(j + ol + k);  // read
+                last = ol;
+                if (valid) {
+#pragma unroll
+                    for (int jv = 0; jv < 2; jv++)  // the pair's two voxels
+#pragma unroll
+                        for (int c = 0; c < 16; c += 8) {
+                            float f[8];
+#pragma unroll
+                            for (int jj = 0; jj < 8; jj++) f[jj] = __uint_as_float(rr[16 * jv + c + jj]);
+                            store8_bm(a, COUT, v + jv, c_lo + c, f, bias + c, mk[2 * jv + c / 8]);
+                        }
+                }
+                for (int k = 3; ok && k < NG && ol + k < nz + 2; k++) ok = release_unread(j + ol + k);  // not read
+            }
+            if (!ok) break;
+            for (int k = last >= 0 ? last + NG : grp; ok && k < nz + 2; k++) ok = release_unread(j + k);
+            if (!ok) break;
+            j += nz + 2;
+        }
+    }
+    __syncthreads();
+    if (s_err) {
+        if (tid == 0) {
+            note_timeout(a.counters, SITE_CONV_ZCAT);
+            for (int i = s_issued > g.S ? s_issued - g.S : 0; i < s_issued; i++)
+                mbar_wait(smem_u32(&full[i % g.S]), (uint32_t)((i / g.S) & 1));
+            for (int w = 0; w < NISS; w++) {
+                const int i = s_last[w];
+                if (i >= 0) mbar_wait(smem_u32(&empty[i % g.S]), (uint32_t)((i / g.S) & 1));
+            }
+        }
+        __syncthreads();
+    }
+    if (warp == ZPAIR_PRODUCER) {
+        tc_fence_after();
+        tmem_dealloc(tmem, TCOLS);
+    }
+}
+
 // shared-memory attributes of a kernel, set once per process (the largest
 // size asked for so far); the attribute calls are host work on every launch
 // otherwise
@@ -1719,6 +2034,78 @@ static bool launch_zcat(const ConvArgs &a, const TmaGeom &g0, uint32_t budget, c
     }
 }
 
+// the x-pair z-column convolution (conv_zpair_kernel) for 16 input channels;
+// false leaves the layer to the others.  IAC_DENOISE_ZPAIR=0 in the
+// environment turns it off (for comparing the kernels).
+template <int CIN, int COUT>
+static bool launch_zpair(const ConvArgs &a, cudaStream_t s, cudaError_t &err)
+{
+    if constexpr (CIN != 16 || COUT != 16) {  // 32 or 48 outputs: re-staging the slab per group loses
+        return false;
+    } else {
+        static const bool off = [] {
+            const char *e = getenv("IAC_DENOISE_ZPAIR");
+            return e && e[0] == '0';
+        }();
+        if (off) return false;
+        if (a.c0 != 0 || (a.W & 1) || a.W / 2 + 2 > 256 || a.D < 1) return false;
+        if (reinterpret_cast<uintptr_t>(a.src1) & 15) return false;
+        PFN_cuTensorMapEncodeTiled enc = tensor_map_encoder();
+        if (!enc) return false;
+        TmaGeom g{};
+        g.Wp = a.W / 2 + 2;                      // padded pairs per row
+        g.NR = 3 + (130 + g.Wp - 1) / g.Wp;      // covers rows y_lo .. y_lo + NR - 1 of every tile
+        if (g.NR > 256) return false;
+        g.T = (a.H * g.Wp + TILE_M - 1) / TILE_M;
+        const long long nb = a.V / ((long long)a.D * a.H * a.W);
+        g.ntiles = nb * a.D * g.T;
+        g.box_bytes = 64u * (uint32_t)g.Wp * (uint32_t)g.NR;
+        g.plane_bytes = (g.box_bytes + 1023u) & ~1023u;
+        g.slab_bytes = g.plane_bytes;
+        g.stage_bytes = g.plane_bytes;
+        g.wcopy_bytes = ZPAIR_WBYTES;
+        g.wres_bytes = (ZPAIR_WBYTES + 1023u) & ~1023u;
+        g.wstage_bytes = 0;
+        const uint32_t budget = 227u * 1024u - 2048u;
+        if (g.wres_bytes + 4u * g.stage_bytes > budget) return false;
+        g.S = (int)std::min<uint32_t>(8u, (budget - g.wres_bytes) / g.stage_bytes);
+        constexpr int NG = COUT / 16;  // output-channel groups (blockIdx.y)
+        const long long grid_max = ((long long)std::max(1, a.sms) + NG - 1) / NG;  // one CTA per SM
+        int ZC = a.D;
+        long long best = -1;
+        for (int zc = a.D; zc >= 1; zc = zc > 1 ? (zc + 1) / 2 : 0) {
+            const long long items = nb * g.T * ((a.D + zc - 1) / zc);
+            const long long cost = ((items + grid_max - 1) / grid_max) * (zc + 2);
+            if (best < 0 || cost < best) {
+                best = cost;
+                ZC = zc;
+            }
+            if (zc == 1) break;
+        }
+        g.ZC = ZC;
+        g.nitems = nb * g.T * ((a.D + ZC - 1) / ZC);
+        CUtensorMap map;
+        const cuuint64_t dims[5] = {32u, (cuuint64_t)(a.W / 2), (cuuint64_t)a.H, (cuuint64_t)a.D, (cuuint64_t)nb};
+        const cuuint64_t strides[4] = {64u, (cuuint64_t)a.W * 32u, (cuuint64_t)a.H * a.W * 32u,
+                                       (cuuint64_t)a.D * a.H * a.W * 32u};
+        const cuuint32_t box[5] = {32u, (cuuint32_t)g.Wp, (cuuint32_t)g.NR, 1u, 1u};
+        const cuuint32_t estr[5] = {1u, 1u, 1u, 1u, 1u};
+        if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16 *>(a.src1), dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+        const uint32_t smem = g.wres_bytes + (uint32_t)g.S * g.stage_bytes;
+        const long long grid = std::min<long long>(g.nitems, grid_max);
+        auto k = conv_zpair_kernel<COUT>;
+        err = smem_attributes(k, smem);
+        if (err != cudaSuccess) return true;
+        ++launch_count;
+        k<<<dim3((unsigned)grid, NG), 32 * (ZPAIR_ISSUER0 + ZPAIR_NISS), smem, s>>>(map, a, g);
+        err = cudaGetLastError();
+        return true;
+    }
+}
+
 // the z-column convolution when its weights stay resident and 4+ stages fit;
 // false leaves the layer to conv_tma_kernel
 template <int CIN, int COUT>
@@ -1820,6 +2207,7 @@ static bool launch_tma(const ConvArgs &a, cudaStream_t s, cudaError_t &err)
                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return false;
+    if (launch_zpair<CIN, COUT>(a, s, err)) return true;
     if (launch_zcat<CIN, COUT>(a, g, budget, s, err)) return true;
     if (launch_zcol<CIN, COUT>(a, g, map, budget, s, err)) return true;
     const long long grid = std::min<long long>(g.ntiles, (long long)per_sm * std::max(1, a.sms));
@@ -3080,8 +3468,8 @@ __device__ __forceinline__ void store8b(bf16 *p, const float *f)
 }
 
 // y (D/2 x H/2 x W/2) = mean of the 2x2x2 children; thread = (coarse voxel, 8 channels)
-__global__ void avgpool2_kernel(const bf16 *__restrict__ x, bf16 *__restrict__ y, int C, int D, int H, int W,
-                                long long total)
+__global__ void avgpool2_kernel(const bf16 *__restrict__ x, int x_stride, bf16 *__restrict__ y, int C, int D,
+                                int H, int W, long long total)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
@@ -3093,7 +3481,7 @@ __global__ void avgpool2_kernel(const bf16 *__restrict__ x, bf16 *__restrict__ y
     for (int k = 0; k < 8; k++) {
         const long long v = (((long long)q.n * D + 2 * q.z + (k >> 2)) * H + 2 * q.y + ((k >> 1) & 1)) * W + 2 * q.x + (k & 1);
         float f[8];
-        load8(x + v * C + c, f);
+        load8(x + v * x_stride + c, f);
 #pragma unroll
         for (int j = 0; j < 8; j++) s[j] += f[j];
     }
@@ -3102,11 +3490,11 @@ __global__ void avgpool2_kernel(const bf16 *__restrict__ x, bf16 *__restrict__ y
     store8b(y + u * C + c, s);
 }
 
-cudaError_t avgpool2(const bf16 *x, bf16 *y, int C, int D, int H, int W, int nb, cudaStream_t s)
+cudaError_t avgpool2(const bf16 *x, int x_stride, bf16 *y, int C, int D, int H, int W, int nb, cudaStream_t s)
 {
     const long long total = (long long)nb * (D / 2) * (H / 2) * (W / 2) * (C / 8);
     ++launch_count;
-    avgpool2_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(x, y, C, D, H, W, total);
+    avgpool2_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(x, x_stride, y, C, D, H, W, total);
     return cudaGetLastError();
 }
 
@@ -3169,40 +3557,50 @@ cudaError_t split_concat_grad(const bf16 *gcat, int c0, int c1, const bf16 *y0, 
     return cudaGetLastError();
 }
 
-// cat[v][0 .. c0) = src0[parent(v)]: the coarse part of a decoder input
-// (nearest 2x upsampling; the skip part is written by the layer that makes
-// it).  Thread = (coarse voxel, 8 channels): one load, the 8 children stored.
-// D, H, W: the full resolution.
-__global__ void upsample_into_kernel(const bf16 *__restrict__ src0, int c0, bf16 *__restrict__ cat, int C, int D,
-                                     int H, int W, long long total)
+// cat[v] = src0[parent(v)] ++ src1[v]: a decoder input, the coarse part
+// nearest-upsampled (2x), the skip tensor after it.  The first n_coarse
+// threads take (coarse voxel, 8 channels): one load, the 8 children stored;
+// the rest copy the skip tensor 16 bytes each.  D, H, W: the full resolution.
+__global__ void concat_up_kernel(const bf16 *__restrict__ src0, int c0, const bf16 *__restrict__ src1, int c1,
+                                 bf16 *__restrict__ cat, int D, int H, int W, long long n_coarse, long long n_skip)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= total) return;
-    const int nc = c0 / 8, c = (int)(i % nc) * 8;
-    const long long u = i / nc;
-    const Vox q = decode(u, D / 2, H / 2, W / 2, total / nc);
-    const uint4 val = *reinterpret_cast<const uint4 *>(src0 + u * c0 + c);
+    const int C = c0 + c1;
+    if (i < n_coarse) {
+        const int nc = c0 / 8, c = (int)(i % nc) * 8;
+        const long long u = i / nc;
+        const Vox q = decode(u, D / 2, H / 2, W / 2, n_coarse / nc);
+        const uint4 val = *reinterpret_cast<const uint4 *>(src0 + u * c0 + c);
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-        const long long v =
-            (((long long)q.n * D + 2 * q.z + (k >> 2)) * H + 2 * q.y + ((k >> 1) & 1)) * W + 2 * q.x + (k & 1);
-        *reinterpret_cast<uint4 *>(cat + v * C + c) = val;
+        for (int k = 0; k < 8; k++) {
+            const long long v =
+                (((long long)q.n * D + 2 * q.z + (k >> 2)) * H + 2 * q.y + ((k >> 1) & 1)) * W + 2 * q.x + (k & 1);
+            *reinterpret_cast<uint4 *>(cat + v * C + c) = val;
+        }
+    } else if (i < n_coarse + n_skip) {
+        const long long k = i - n_coarse;
+        const int nc = c1 / 8, c = (int)(k % nc) * 8;
+        const long long v = k / nc;
+        *reinterpret_cast<uint4 *>(cat + v * C + c0 + c) = *reinterpret_cast<const uint4 *>(src1 + v * c1 + c);
     }
 }
 
-cudaError_t upsample_into(const bf16 *src0, int c0, bf16 *cat, int C, int D, int H, int W, int nb, cudaStream_t s)
+cudaError_t concat_up(const bf16 *src0, int c0, const bf16 *src1, int c1, bf16 *cat, int D, int H, int W, int nb,
+                      cudaStream_t s)
 {
-    const long long total = (long long)nb * (D / 2) * (H / 2) * (W / 2) * (c0 / 8);
+    const long long V = (long long)nb * D * H * W;
+    const long long nco = V / 8 * (c0 / 8), nsk = V * (c1 / 8);
     ++launch_count;
-    upsample_into_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(src0, c0, cat, C, D, H, W, total);
+    concat_up_kernel<<<(unsigned)((nco + nsk + 255) / 256), 256, 0, s>>>(src0, c0, src1, c1, cat, D, H, W, nco, nsk);
     return cudaGetLastError();
 }
 
 // out = (gskip + gpool(parent) / 8) * (y > 0): gradient of a skip tensor that
-// also fed an average pool; gskip has gskip_stride channels per voxel (the
-// skip channels of the decoder input's gradient, read in place)
+// also fed an average pool; gskip and y have gskip_stride and y_stride
+// channels per voxel (the skip channels of the decoder input's gradient and
+// of the decoder input, read in place)
 __global__ void pool_grad_mask_kernel(const bf16 *__restrict__ gskip, int gskip_stride,
-                                      const bf16 *__restrict__ gpool, const bf16 *__restrict__ y,
+                                      const bf16 *__restrict__ gpool, const bf16 *__restrict__ y, int y_stride,
                                       bf16 *__restrict__ out, int C, int D, int H, int W, long long total)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -3214,19 +3612,19 @@ __global__ void pool_grad_mask_kernel(const bf16 *__restrict__ gskip, int gskip_
     float a[8], b[8], fy[8];
     load8(gskip + v * gskip_stride + c, a);
     load8(gpool + u * C + c, b);
-    load8(y + v * C + c, fy);
+    load8(y + v * y_stride + c, fy);
 #pragma unroll
     for (int j = 0; j < 8; j++) a[j] = fy[j] > 0.0f ? a[j] + 0.125f * b[j] : 0.0f;
     store8b(out + v * C + c, a);
 }
 
-cudaError_t pool_grad_mask(const bf16 *gskip, int gskip_stride, const bf16 *gpool, const bf16 *y, bf16 *out, int C,
-                           int D, int H, int W, int nb, cudaStream_t s)
+cudaError_t pool_grad_mask(const bf16 *gskip, int gskip_stride, const bf16 *gpool, const bf16 *y, int y_stride,
+                           bf16 *out, int C, int D, int H, int W, int nb, cudaStream_t s)
 {
     const long long total = (long long)nb * D * H * W * (C / 8);
     ++launch_count;
-    pool_grad_mask_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(gskip, gskip_stride, gpool, y, out, C, D,
-                                                                          H, W, total);
+    pool_grad_mask_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(gskip, gskip_stride, gpool, y, y_stride,
+                                                                          out, C, D, H, W, total);
     return cudaGetLastError();
 }
 

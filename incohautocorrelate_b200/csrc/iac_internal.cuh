@@ -60,8 +60,7 @@ struct DeviceCounters {
     unsigned long long timeouts;
     unsigned long long photon_overflow;  // photons beyond a photon-list capacity (dropped)
     unsigned long long timeout_sites;    // bit k: a kernel of WAIT_SITE_NAMES[k] gave up a bounded wait
-    unsigned long long bad_stores;       // stores whose index failed a kernel's bounds check (skipped)
-    unsigned long long pad[3];
+    unsigned long long pad[4];
 };
 
 // kernels with bounded waits, as bits of DeviceCounters::timeout_sites
