@@ -175,14 +175,14 @@ __device__ __forceinline__ uint64_t smem_desc_sw32(uint32_t addr)
     return (uint64_t)((addr & 0x3FFFFu) >> 4) | (1ull << 16) | ((uint64_t)(256u >> 4) << 32) | (1ull << 46) |
            (6ull << 61);
 }
-// MN-major operand with the 32-byte swizzle: 16 M (or N) elements per 32-byte
-// row, one row per K index, 8-row groups 256 bytes apart (SBO), 16-element
-// M blocks `mblock` bytes apart (LBO); the same rows as smem_desc_sw32, read
-// transposed, from any row
-__device__ __forceinline__ uint64_t smem_desc_sw32_mn(uint32_t addr, uint32_t mblock)
+// MN-major operand with rows of 32 or 64 bytes (16 or 32 M elements of one K
+// index, the 32- or 64-byte swizzle), M blocks `mblock` bytes apart (LBO),
+// 8-row groups 8 rows apart (SBO), layout type 6 or 4; as with the K-major
+// operands the start may sit at any row (checked for both swizzles)
+__device__ __forceinline__ uint64_t smem_desc_swz_mn(uint32_t addr, uint32_t rowbytes, uint32_t mblock)
 {
     return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)((mblock >> 4) & 0x3FFFu) << 16) |
-           ((uint64_t)(256u >> 4) << 32) | (1ull << 46) | (6ull << 61);
+           ((uint64_t)((8u * rowbytes) >> 4) << 32) | (1ull << 46) | ((rowbytes == 32 ? 6ull : 4ull) << 61);
 }
 // instruction descriptor, kind::f16: D fp32 (bits 4-5 = 1), A and B bf16
 // (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
@@ -2891,14 +2891,14 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_tc_kernel(const __grid_const
 // independent (planes outside the volume arrive as zeros), so the CTAs are
 // persistent over all tiles; a tile is KT consecutive padded positions of a
 // plane (K = KT per stage: longer tiles stage fewer halo rows per position).
-// Slabs arrive as one 32-byte-swizzled TMA box per 16 channels (stage planes
-// [position][16 channels]) and are read as MN-major operands: the TMA unit
-// moves about one box row per clock, so rows of 32 bytes stage a slab in half
-// the time of the unswizzled layout's 16-byte rows.
+// Slabs arrive as one swizzled TMA box per 32 channels (64-byte rows) where the
+// channel count is a multiple of 32, else per 16 (32-byte rows), stage planes
+// [position][channels], read as MN-major operands: the TMA unit moves about one
+// box row per clock, so wider rows stage a slab in fewer rows than the
+// unswizzled layout's 16-byte rows.
 // The bias gradient comes with it: the first of the padding rows of A is a
-// 16-channel plane of ones, written once into every stage slot, so its
-// accumulator row holds sum_v G[v][co] (the gradient is zero at the padded
-// positions).
+// plane of ones, written once into every stage slot, so its accumulator row
+// holds sum_v G[v][co] (the gradient is zero at the padded positions).
 // --------------------------------------------------------------------------
 template <int CIN, int COUT, int MODE>
 struct WzsCfg {
@@ -2916,9 +2916,12 @@ struct WzsCfg {
     static constexpr int TPG = (9 + NTG - 1) / NTG;     // taps of a group (the last may have fewer)
     static constexpr int COLS = TPG * N * MB;
     static constexpr uint32_t TCOLS = COLS <= 32 ? 32 : (COLS <= 64 ? 64 : (COLS <= 128 ? 128 : (COLS <= 256 ? 256 : 512)));
-    static constexpr int XREAL = NX * CIN / 16;         // X planes of 16 channels loaded
-    static constexpr int XPLANES = MB * MR / 16;        // X planes the MMAs read (padding rows: garbage)
-    static constexpr int GPLANES = NG * COUT / 16;
+    // channels per staged plane (a swizzled row of 64 or 32 bytes): 32 where they divide
+    static constexpr int XW = CIN % 32 == 0 ? 32 : 16;
+    static constexpr int GW = COUT % 32 == 0 ? 32 : 16;
+    static constexpr int XREAL = NX * CIN / XW;         // X planes loaded
+    static constexpr int XPLANES = MB * MR / XW;        // X planes the MMAs read (padding rows: garbage)
+    static constexpr int GPLANES = NG * COUT / GW;
     static constexpr bool OK = COLS <= 512 && N <= 256 && N % (MR == 128 ? 16 : 8) == 0 && XPLANES > XREAL &&
                                NTG <= 3 && CIN % 16 == 0 && COUT % 16 == 0;
 };
@@ -2989,14 +2992,14 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_const
 #pragma unroll
                 for (int b = 0; b < Z::NX; b++)
 #pragma unroll
-                    for (int c = 0; c < CIN / 16; c++)
-                        tma_load_5d(st + (uint32_t)(b * (CIN / 16) + c) * g.planeX, &xmap, c * 16, -1, y_lo,
+                    for (int c = 0; c < CIN / Z::XW; c++)
+                        tma_load_5d(st + (uint32_t)(b * (CIN / Z::XW) + c) * g.planeX, &xmap, c * Z::XW, -1, y_lo,
                                     z0 + Z::XLO + b, n, fb);
 #pragma unroll
                 for (int pg = 0; pg < Z::NG; pg++)
 #pragma unroll
-                    for (int c = 0; c < COUT / 16; c++)
-                        tma_load_5d(st + xbytes + (uint32_t)(pg * (COUT / 16) + c) * g.planeG, &gmap, c * 16, -1,
+                    for (int c = 0; c < COUT / Z::GW; c++)
+                        tma_load_5d(st + xbytes + (uint32_t)(pg * (COUT / Z::GW) + c) * g.planeG, &gmap, c * Z::GW, -1,
                                     yg_lo, z0 + Z::GLO + pg, n, fb);
                 s_issued = k + 1;
             }
@@ -3014,17 +3017,18 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_const
                 const int relg = q0 - (q0 / g.Wp) * g.Wp;
                 const int r0 = rel + (t / 3 - 1) * g.Wp + (t % 3 - 1);
                 const uint32_t sX = sbase + (uint32_t)slot * g.stage_bytes, sG = sX + xbytes;
-                // descriptors advance by 16 positions (16 rows of 32 B, 32 units of 16 B) per K step
-                const uint64_t db0 = smem_desc_sw32_mn(sG + (uint32_t)relg * 32, g.planeG);
+                // descriptors advance by 16 positions (16 rows, RB units of 16 B) per K step
+                constexpr uint32_t RBX = 2 * Z::XW, RBG = 2 * Z::GW;  // bytes per staged row
+                const uint64_t db0 = smem_desc_swz_mn(sG + (uint32_t)relg * RBG, RBG, g.planeG);
 #pragma unroll
                 for (int mb = 0; mb < MB; mb++) {
                     const uint32_t dcol = tmem + (uint32_t)((tl * MB + mb) * N);
-                    const uint64_t da0 =
-                        smem_desc_sw32_mn(sX + (uint32_t)(mb * (MR / 16)) * g.planeX + (uint32_t)r0 * 32, g.planeX);
+                    const uint64_t da0 = smem_desc_swz_mn(
+                        sX + (uint32_t)(mb * (MR / Z::XW)) * g.planeX + (uint32_t)r0 * RBX, RBX, g.planeX);
                     const int nks = g.KT / 16;
 #pragma unroll 8
                     for (int ks = 0; ks < nks; ks++)
-                        umma_bf16(dcol, da0 + (uint64_t)(32 * ks), db0 + (uint64_t)(32 * ks), IDESC,
+                        umma_bf16(dcol, da0 + (uint64_t)(RBX * ks), db0 + (uint64_t)(RBG * ks), IDESC,
                                   (k > 0 || ks > 0) ? 1u : 0u);
                 }
                 umma_commit(smem_u32(&empty[slot]));
@@ -3055,7 +3059,7 @@ __global__ void __launch_bounds__(WT_THREADS) wgrad_zs_kernel(const __grid_const
             tmem_wait_ld();
             const int t = tg0 + blk / MB, mb = blk % MB;
             const int m = mb * MR + row;
-            if (a.db && t == 4 && row >= 0 && m == Z::XREAL * 16) {  // the ones row: sum_v G[v][co]
+            if (a.db && t == 4 && row >= 0 && m == Z::XREAL * Z::XW) {  // the ones row: sum_v G[v][co]
 #pragma unroll
                 for (int nn = 0; nn < N; nn++) {
                     const int c = nn / COUT;  // gradient plane z0 + GLO + c: counted by the stage that owns it
@@ -3215,10 +3219,11 @@ static bool launch_wgrad_zs(const WgradArgs &a, int sms, cudaStream_t s, cudaErr
             if (g.NR > 256 || g.NRg > 256) continue;
             g.T = (a.H * g.Wp + KT - 1) / KT;
             g.ntiles = nb * ((a.D + Z::ZSTEP - 1) / Z::ZSTEP) * g.T;
-            g.boxX = 32u * (uint32_t)g.Wp * (uint32_t)g.NR;  // planes of 16 channels, 32-byte rows
-            g.boxG = 32u * (uint32_t)g.Wp * (uint32_t)g.NRg;
-            g.planeX = (g.boxX + 255u) & ~255u;
-            g.planeG = (g.boxG + 255u) & ~255u;
+            g.boxX = 2u * Z::XW * (uint32_t)g.Wp * (uint32_t)g.NR;  // planes of XW channels, 2 XW-byte rows
+            g.boxG = 2u * Z::GW * (uint32_t)g.Wp * (uint32_t)g.NRg;
+            // planes aligned to their swizzle pattern (8 rows)
+            g.planeX = (g.boxX + 16u * Z::XW - 1u) & ~(16u * Z::XW - 1u);
+            g.planeG = (g.boxG + 16u * Z::GW - 1u) & ~(16u * Z::GW - 1u);
             g.stage_bytes = (((uint32_t)Z::XPLANES * g.planeX + (uint32_t)Z::GPLANES * g.planeG) + 1023u) & ~1023u;
             g.S = 0;
             const int min_stages = 2;
@@ -3244,11 +3249,12 @@ static bool launch_wgrad_zs(const WgradArgs &a, int sms, cudaStream_t s, cudaErr
             const cuuint64_t dims[5] = {C, (cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.D, (cuuint64_t)nb};
             const cuuint64_t strides[4] = {C * 2, (cuuint64_t)a.W * C * 2, (cuuint64_t)a.H * a.W * C * 2,
                                            (cuuint64_t)a.D * a.H * a.W * C * 2};
-            const cuuint32_t box[5] = {16u, (cuuint32_t)g.Wp, (cuuint32_t)rows[m], 1u, 1u};
+            const cuuint32_t w = m == 0 ? Z::XW : Z::GW;
+            const cuuint32_t box[5] = {w, (cuuint32_t)g.Wp, (cuuint32_t)rows[m], 1u, 1u};
             const cuuint32_t estr[5] = {1u, 1u, 1u, 1u, 1u};
             if (enc(&maps[m], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void *>(bases[m]), dims, strides, box,
-                    estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                    estr, CU_TENSOR_MAP_INTERLEAVE_NONE, w == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
                 return false;
         }
         err = smem_attributes(wgrad_zs_kernel<CIN, COUT, MODE>, smem);
