@@ -59,6 +59,7 @@ def test_bounded_wait_times_out_and_the_context_stays_usable(oracle_lib, rng):
             ctx.check()
         assert err.value.status == capi.IAC_ERR_TIMEOUT
         assert "bounded device waits ran out" in str(err.value)
+        assert "(flag wait)" in str(err.value)  # the report names the kernel whose wait gave up
         assert ctx.check() == 0  # the counter was cleared by the report
         flag.fill_(1)  # a set flag ends the wait at once, however long the limit
         ctx.wait_flag(flag, 10_000_000)
