@@ -56,8 +56,8 @@ struct iac_denoiser {
     bf16 *cat1 = nullptr, *cat2 = nullptr;  // decoder inputs: up(d2b) ++ s1, up(b2) ++ s2
     uint64_t step_launches = 0;             // kernels in the training-step graph
     // gradients
-    bf16 *gA = nullptr, *gB = nullptr, *gcat1 = nullptr;  // full resolution
-    bf16 *hA = nullptr, *hB = nullptr, *gcat2 = nullptr;  // half
+    bf16 *gA = nullptr, *gB = nullptr, *gup1 = nullptr, *gskip1 = nullptr;  // full resolution
+    bf16 *hA = nullptr, *hB = nullptr, *gup2 = nullptr, *gskip2 = nullptr;  // half
     bf16 *qA = nullptr, *qB = nullptr;                                       // quarter
     std::vector<void *> allocs;
     // CUDA graph of one training step (iac_denoise_train_steps)
@@ -144,7 +144,7 @@ ConvArgs conv_args(iac_denoiser *dn, int l, const bf16 *src0, const bf16 *src1, 
 // relu_y (the forward activation dX belongs to) the ReLU derivative is applied
 // in the same kernel: dX = 0 where relu_y <= 0
 iac_status dgrad(iac_denoiser *dn, int l, const bf16 *gp, bf16 *out, int D, int H, int W, long long V,
-                 cudaStream_t s, const bf16 *relu_y = nullptr)
+                 cudaStream_t s, const bf16 *relu_y = nullptr, bf16 *out2 = nullptr, int split = 0)
 {
     ConvArgs a{};
     a.mask_y = relu_y;
@@ -152,6 +152,8 @@ iac_status dgrad(iac_denoiser *dn, int l, const bf16 *gp, bf16 *out, int D, int 
     a.c1 = SPECS[l].cout;
     a.w = dn->wd + dn->wd_off[l];
     a.y = out;
+    a.y2 = out2;  // with out2: channels split.. of dX there, the first split in out
+    a.split = split;
     a.D = D;
     a.H = H;
     a.W = W;
@@ -311,29 +313,30 @@ iac_status run_backward(iac_denoiser *dn, const float *d_in, const float *d_targ
     if ((st = dgrad(dn, 9, dn->gA, dn->gB, D, H, W, V, s, dn->d1a)) != IAC_OK) return st;
     // layer 8: X = up(d2b) ++ s1
     if ((st = wgrad(dn, 8, nullptr, dn->cat1, dn->gB, D, H, W, V, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 8, dn->gB, dn->gcat1, D, H, W, V, s)) != IAC_OK) return st;
-    DN_CHECK(split_concat_grad(dn->gcat1, 32, 16, dn->d2b, dn->hA, D, H, W, nb, s), "split 1");
+    // the decoder input's gradient in two parts: the upsampled 32 channels, the skip 16
+    if ((st = dgrad(dn, 8, dn->gB, dn->gup1, D, H, W, V, s, nullptr, dn->gskip1, 32)) != IAC_OK) return st;
+    DN_CHECK(split_concat_grad(dn->gup1, 32, dn->d2b, dn->hA, D, H, W, nb, s), "split 1");
     // layer 7: X = d2a
     if ((st = wgrad(dn, 7, nullptr, dn->d2a, dn->hA, D2, H2, W2, V2, s)) != IAC_OK) return st;
     if ((st = dgrad(dn, 7, dn->hA, dn->hB, D2, H2, W2, V2, s, dn->d2a)) != IAC_OK) return st;
     // layer 6: X = up(b2) ++ s2
     if ((st = wgrad(dn, 6, nullptr, dn->cat2, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 6, dn->hB, dn->gcat2, D2, H2, W2, V2, s)) != IAC_OK) return st;
-    DN_CHECK(split_concat_grad(dn->gcat2, 64, 32, dn->b2, dn->qA, D2, H2, W2, nb, s), "split 2");
+    if ((st = dgrad(dn, 6, dn->hB, dn->gup2, D2, H2, W2, V2, s, nullptr, dn->gskip2, 64)) != IAC_OK) return st;
+    DN_CHECK(split_concat_grad(dn->gup2, 64, dn->b2, dn->qA, D2, H2, W2, nb, s), "split 2");
     // layer 5: X = b1
     if ((st = wgrad(dn, 5, nullptr, dn->b1, dn->qA, D4, H4, W4, V4, s)) != IAC_OK) return st;
     if ((st = dgrad(dn, 5, dn->qA, dn->qB, D4, H4, W4, V4, s, dn->b1)) != IAC_OK) return st;
     // layer 4: X = p2
     if ((st = wgrad(dn, 4, nullptr, dn->p2, dn->qB, D4, H4, W4, V4, s)) != IAC_OK) return st;
     if ((st = dgrad(dn, 4, dn->qB, dn->qA, D4, H4, W4, V4, s)) != IAC_OK) return st;  // d p2 (32 ch)
-    DN_CHECK(pool_grad_mask(dn->gcat2 + 64, 96, dn->qA, dn->s2, 32, dn->hA, 32, D2, H2, W2, nb, s), "pool grad 2");
+    DN_CHECK(pool_grad_mask(dn->gskip2, 32, dn->qA, dn->s2, 32, dn->hA, 32, D2, H2, W2, nb, s), "pool grad 2");
     // layer 3: X = e2a
     if ((st = wgrad(dn, 3, nullptr, dn->e2a, dn->hA, D2, H2, W2, V2, s)) != IAC_OK) return st;
     if ((st = dgrad(dn, 3, dn->hA, dn->hB, D2, H2, W2, V2, s, dn->e2a)) != IAC_OK) return st;
     // layer 2: X = p1
     if ((st = wgrad(dn, 2, nullptr, dn->p1, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
     if ((st = dgrad(dn, 2, dn->hB, dn->hA, D2, H2, W2, V2, s)) != IAC_OK) return st;  // d p1 (16 ch)
-    DN_CHECK(pool_grad_mask(dn->gcat1 + 32, 48, dn->hA, dn->s1, 16, dn->gA, 16, D, H, W, nb, s), "pool grad 1");
+    DN_CHECK(pool_grad_mask(dn->gskip1, 16, dn->hA, dn->s1, 16, dn->gA, 16, D, H, W, nb, s), "pool grad 1");
     // layer 1: X = e1a
     if ((st = wgrad(dn, 1, nullptr, dn->e1a, dn->gA, D, H, W, V, s)) != IAC_OK) return st;
     if ((st = dgrad(dn, 1, dn->gA, dn->gB, D, H, W, V, s, dn->e1a)) != IAC_OK) return st;
@@ -415,10 +418,12 @@ iac_status iac_denoise_create(iac_ctx *ctx, uint32_t max_batch, uint32_t D, uint
     dn->cat2 = (bf16 *)A(V2 * 96 * b);
     dn->gA = (bf16 *)A(V * 16 * b);
     dn->gB = (bf16 *)A(V * 16 * b);
-    dn->gcat1 = (bf16 *)A(V * 48 * b);
+    dn->gup1 = (bf16 *)A(V * 32 * b);
+    dn->gskip1 = (bf16 *)A(V * 16 * b);
     dn->hA = (bf16 *)A(V2 * 32 * b);
     dn->hB = (bf16 *)A(V2 * 32 * b);
-    dn->gcat2 = (bf16 *)A(V2 * 96 * b);
+    dn->gup2 = (bf16 *)A(V2 * 64 * b);
+    dn->gskip2 = (bf16 *)A(V2 * 32 * b);
     dn->qA = (bf16 *)A(V4 * 64 * b);
     dn->qB = (bf16 *)A(V4 * 64 * b);
     dn->d_step = (long long *)A(16);

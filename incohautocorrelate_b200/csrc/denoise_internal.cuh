@@ -38,6 +38,10 @@ struct ConvArgs {
     float *y32;          // optional fp32 copy of the output
     int relu;
     const bf16 *mask_y;  // optional [V][cout]: outputs where mask_y <= 0 are set to 0 (ReLU derivative)
+    // optional split output: channels split .. cout - 1 go to y2 ([V][cout - split]), the
+    // first split channels to y ([V][split]) - the decoder input's gradient, coarse and skip parts
+    bf16 *y2;
+    int split;
     int D, H, W;         // output (= src1) dims per batch item
     long long V;         // nb * D * H * W
     DeviceCounters *counters;
@@ -77,8 +81,8 @@ cudaError_t wgrad3x3_first(const float *x, const bf16 *g, float *dw, float *db, 
                            long long V, int sms, cudaStream_t s);
 cudaError_t avgpool2(const bf16 *x, int x_stride, bf16 *y, int C, int D, int H, int W, int nb, cudaStream_t s);
 cudaError_t relu_mask(const bf16 *g, const bf16 *y, bf16 *out, long long n, cudaStream_t s);
-cudaError_t split_concat_grad(const bf16 *gcat, int c0, int c1, const bf16 *y0, bf16 *g0, int D, int H, int W,
-                              int nb, cudaStream_t s);
+cudaError_t split_concat_grad(const bf16 *gup, int c0, const bf16 *y0, bf16 *g0, int D, int H, int W, int nb,
+                              cudaStream_t s);
 cudaError_t concat_up(const bf16 *src0, int c0, const bf16 *src1, int c1, bf16 *cat, int D, int H, int W, int nb,
                       cudaStream_t s);
 cudaError_t pool_grad_mask(const bf16 *gskip, int gskip_stride, const bf16 *gpool, const bf16 *y, int y_stride,

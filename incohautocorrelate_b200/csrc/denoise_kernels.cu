@@ -297,6 +297,14 @@ __device__ __forceinline__ void mask8(const bf16 *y8, float *o)
     }
 }
 
+// where output channels c .. of voxel v go: y ([V][cout]), or with a split
+// output y ([V][split]) below `split` and y2 ([V][cout - split]) from it
+__device__ __forceinline__ bf16 *out_ptr(const ConvArgs &a, int cout, long long v, int c)
+{
+    if (!a.y2) return a.y + v * cout + c;
+    return c < a.split ? a.y + v * a.split + c : a.y2 + v * (cout - a.split) + (c - a.split);
+}
+
 // epilogue for one output row segment of 8 channels with the bias already in
 // registers (b: channels c .. c+7): ReLU, bf16 (+fp32)
 __device__ __forceinline__ void store8_b(const ConvArgs &a, int cout, long long v, int c, const float *val,
@@ -314,7 +322,7 @@ __device__ __forceinline__ void store8_b(const ConvArgs &a, int cout, long long 
     pk.y = pack_bf16(o[2], o[3]);
     pk.z = pack_bf16(o[4], o[5]);
     pk.w = pack_bf16(o[6], o[7]);
-    *reinterpret_cast<uint4 *>(a.y + v * cout + c) = pk;
+    *reinterpret_cast<uint4 *>(out_ptr(a, cout, v, c)) = pk;
     if (a.y32) {
         float4 *d = reinterpret_cast<float4 *>(a.y32 + v * cout + c);
         d[0] = make_float4(o[0], o[1], o[2], o[3]);
@@ -345,7 +353,7 @@ __device__ __forceinline__ void store8_bm(const ConvArgs &a, int cout, long long
     pk.y = pack_bf16(o[2], o[3]);
     pk.z = pack_bf16(o[4], o[5]);
     pk.w = pack_bf16(o[6], o[7]);
-    *reinterpret_cast<uint4 *>(a.y + v * cout + c) = pk;
+    *reinterpret_cast<uint4 *>(out_ptr(a, cout, v, c)) = pk;
     if (a.y32) {
         float4 *d = reinterpret_cast<float4 *>(a.y32 + v * cout + c);
         d[0] = make_float4(o[0], o[1], o[2], o[3]);
@@ -368,7 +376,7 @@ __device__ __forceinline__ void store8(const ConvArgs &a, int cout, long long v,
     pk.y = pack_bf16(o[2], o[3]);
     pk.z = pack_bf16(o[4], o[5]);
     pk.w = pack_bf16(o[6], o[7]);
-    *reinterpret_cast<uint4 *>(a.y + v * cout + c) = pk;
+    *reinterpret_cast<uint4 *>(out_ptr(a, cout, v, c)) = pk;
     if (a.y32) {
         float4 *d = reinterpret_cast<float4 *>(a.y32 + v * cout + c);
         d[0] = make_float4(o[0], o[1], o[2], o[3]);
@@ -577,7 +585,7 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_mma_kernel(const ConvArgs a
                     if ((w & 0x80000000u) || !(w & 0x7FFF0000u)) o1 = 0.0f;
                 }
                 const uint32_t pk = pack_bf16(o0, o1);
-                *reinterpret_cast<uint32_t *>(a.y + v * COUT + c) = pk;
+                *reinterpret_cast<uint32_t *>(out_ptr(a, COUT, v, c)) = pk;
                 if (a.y32) *reinterpret_cast<float2 *>(a.y32 + v * COUT + c) = make_float2(o0, o1);
             }
         }
@@ -3525,14 +3533,13 @@ cudaError_t relu_mask(const bf16 *g, const bf16 *y, bf16 *out, long long n, cuda
     return cudaGetLastError();
 }
 
-// gcat [V][c0 + c1] at full resolution: g0 (coarse, c0) = mask(y0) * sum of the
-// 8 children's first c0 channels (backward of nearest upsampling); the last c1
-// channels, the skip connection's gradient, are read in place by pool_grad_mask
-__global__ void split_concat_kernel(const bf16 *__restrict__ gcat, int c0, int c1, const bf16 *__restrict__ y0,
+// gup [V][c0] at full resolution, the gradient of a decoder input's upsampled
+// part: g0 (coarse, c0) = mask(y0) * sum of the 8 children (backward of
+// nearest upsampling); the skip part's gradient went to its own buffer
+__global__ void split_concat_kernel(const bf16 *__restrict__ gup, int c0, const bf16 *__restrict__ y0,
                                     bf16 *__restrict__ g0, int D, int H, int W, long long n_coarse)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int C = c0 + c1;
     if (i >= n_coarse) return;
     const int nc = c0 / 8, c = (int)(i % nc) * 8;
     const long long u = i / nc;
@@ -3542,7 +3549,7 @@ __global__ void split_concat_kernel(const bf16 *__restrict__ gcat, int c0, int c
         const long long v =
             (((long long)q.n * D + 2 * q.z + (k >> 2)) * H + 2 * q.y + ((k >> 1) & 1)) * W + 2 * q.x + (k & 1);
         float f[8];
-        load8(gcat + v * C + c, f);
+        load8(gup + v * c0 + c, f);
 #pragma unroll
         for (int j = 0; j < 8; j++) s[j] += f[j];
     }
@@ -3553,13 +3560,13 @@ __global__ void split_concat_kernel(const bf16 *__restrict__ gcat, int c0, int c
     store8b(g0 + u * c0 + c, s);
 }
 
-cudaError_t split_concat_grad(const bf16 *gcat, int c0, int c1, const bf16 *y0, bf16 *g0, int D, int H, int W,
-                              int nb, cudaStream_t s)
+cudaError_t split_concat_grad(const bf16 *gup, int c0, const bf16 *y0, bf16 *g0, int D, int H, int W, int nb,
+                              cudaStream_t s)
 {
     const long long V = (long long)nb * D * H * W;
     const long long nco = V / 8 * (c0 / 8);
     ++launch_count;
-    split_concat_kernel<<<(unsigned)((nco + 255) / 256), 256, 0, s>>>(gcat, c0, c1, y0, g0, D, H, W, nco);
+    split_concat_kernel<<<(unsigned)((nco + 255) / 256), 256, 0, s>>>(gup, c0, y0, g0, D, H, W, nco);
     return cudaGetLastError();
 }
 
