@@ -1365,12 +1365,30 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = s_tmem;
-    const int nzc = (a.D + g.ZC - 1) / g.ZC;  // z-chunks per column
     const int HW = a.H * a.W;
-    auto item = [&](long long it, int &n, int &q0, int &z0, int &z1) {
-        const long long col = it / nzc;
-        z0 = (int)(it % nzc) * g.ZC;
-        z1 = z0 + g.ZC < a.D ? z0 + g.ZC : a.D;
+    // work: with g.ZC > 0, items of ZC output planes of a column dealt round
+    // robin (g.nitems items); with g.ZC == 0, an equal contiguous share of the
+    // g.nitems (column, plane) pairs per CTA, walked as runs within a column.
+    // A run of Z planes takes Z + 2 stages; the launcher picks the scheme with
+    // the fewer stages on the busiest CTA.
+    const bool rr = g.ZC > 0;
+    const int nzc = rr ? (a.D + g.ZC - 1) / g.ZC : 1;  // z-chunks per column
+    const long long c_begin = rr ? (long long)blockIdx.x : g.nitems * blockIdx.x / gridDim.x;
+    const long long c_end = rr ? g.nitems : g.nitems * (blockIdx.x + 1) / gridDim.x;
+    auto item = [&](long long &cur, int &n, int &q0, int &z0, int &z1) {
+        long long col;
+        if (rr) {
+            col = cur / nzc;
+            z0 = (int)(cur % nzc) * g.ZC;
+            z1 = z0 + g.ZC < a.D ? z0 + g.ZC : a.D;
+            cur += gridDim.x;
+        } else {
+            col = cur / a.D;
+            z0 = (int)(cur - col * a.D);
+            const long long left = c_end - cur;
+            z1 = (long long)(a.D - z0) <= left ? a.D : z0 + (int)left;
+            cur += z1 - z0;
+        }
         n = (int)(col / g.T);
         q0 = (int)(col % g.T) * TILE_M;
     };
@@ -1379,9 +1397,9 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
         if (lane == 0) {  // one slab per input plane z0-1 .. z1 (planes outside the volume arrive as zeros)
             int j = 0, slot = 0, round = 0;  // slot = j % S, round = j / S
             bool ok = true;
-            for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
+            for (long long cur = c_begin; ok && cur < c_end;) {
                 int n, q0, z0, z1;
-                item(it, n, q0, z0, z1);
+                item(cur, n, q0, z0, z1);
                 const int y_lo = floor_div(q0 - g.Wp - 1, g.Wp);
                 for (int pz = z0 - 1; pz <= z1; pz++, j++) {
                     if (j >= g.S && !mbar_wait_flag(smem_u32(&empty[slot]), (uint32_t)((round - 1) & 1), &s_err)) {
@@ -1407,9 +1425,9 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
         if (lane == 0) {
             int j = 0, slot = 0, round = 0, r = 0, rround = 0;  // slot = j % S, round = j / S, r = j % NB, rround = j / NB
             bool ok = true;
-            for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
+            for (long long cur = c_begin; ok && cur < c_end;) {
                 int n, q0, z0, z1;
-                item(it, n, q0, z0, z1);
+                item(cur, n, q0, z0, z1);
                 const int rel = q0 - floor_div(q0 - g.Wp - 1, g.Wp) * g.Wp;  // q0 within the slab
                 for (int k = 0; k < z1 - z0 + 2; k++, j++) {
                     const int cur_slot = slot, cur_round = round, cur_r = r, cur_rround = rround;
@@ -1474,9 +1492,9 @@ __global__ void __launch_bounds__(32 * (ZCAT_ISSUER0 + NISS), MINB)
         };
         int j = 0;  // this CTA's stages before the current item
         bool ok = true;
-        for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
+        for (long long cur = c_begin; ok && cur < c_end;) {
             int n, q0, z0, z1;
-            item(it, n, q0, z0, z1);
+            item(cur, n, q0, z0, z1);
             const int nz = z1 - z0;
             const int q = q0 + row;
             const int y = q / g.Wp, xp = q - (q / g.Wp) * g.Wp;
@@ -1659,13 +1677,31 @@ __global__ void __launch_bounds__(32 * (ZPAIR_ISSUER0 + ZPAIR_NISS), 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = s_tmem;
-    const int nzc = (a.D + g.ZC - 1) / g.ZC;  // z-chunks per column
     const int HW = a.H * a.W;
     const int WP = g.Wp;                      // padded pairs per row
-    auto item = [&](long long it, int &n, int &q0, int &z0, int &z1) {
-        const long long col = it / nzc;
-        z0 = (int)(it % nzc) * g.ZC;
-        z1 = z0 + g.ZC < a.D ? z0 + g.ZC : a.D;
+    // work: with g.ZC > 0, items of ZC output planes of a column dealt round
+    // robin (g.nitems items); with g.ZC == 0, an equal contiguous share of the
+    // g.nitems (column, plane) pairs per CTA, walked as runs within a column.
+    // A run of Z planes takes Z + 2 stages; the launcher picks the scheme with
+    // the fewer stages on the busiest CTA.
+    const bool rr = g.ZC > 0;
+    const int nzc = rr ? (a.D + g.ZC - 1) / g.ZC : 1;  // z-chunks per column
+    const long long c_begin = rr ? (long long)blockIdx.x : g.nitems * blockIdx.x / gridDim.x;
+    const long long c_end = rr ? g.nitems : g.nitems * (blockIdx.x + 1) / gridDim.x;
+    auto item = [&](long long &cur, int &n, int &q0, int &z0, int &z1) {
+        long long col;
+        if (rr) {
+            col = cur / nzc;
+            z0 = (int)(cur % nzc) * g.ZC;
+            z1 = z0 + g.ZC < a.D ? z0 + g.ZC : a.D;
+            cur += gridDim.x;
+        } else {
+            col = cur / a.D;
+            z0 = (int)(cur - col * a.D);
+            const long long left = c_end - cur;
+            z1 = (long long)(a.D - z0) <= left ? a.D : z0 + (int)left;
+            cur += z1 - z0;
+        }
         n = (int)(col / g.T);
         q0 = (int)(col % g.T) * TILE_M;
     };
@@ -1674,9 +1710,9 @@ __global__ void __launch_bounds__(32 * (ZPAIR_ISSUER0 + ZPAIR_NISS), 1)
         if (lane == 0) {  // one pair slab per input plane z0-1 .. z1 (planes outside the volume arrive as zeros)
             int j = 0, slot = 0, round = 0;
             bool ok = true;
-            for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
+            for (long long cur = c_begin; ok && cur < c_end;) {
                 int n, q0, z0, z1;
-                item(it, n, q0, z0, z1);
+                item(cur, n, q0, z0, z1);
                 const int y_lo = floor_div(q0 - WP - 1, WP);
                 for (int pz = z0 - 1; pz <= z1; pz++, j++) {
                     if (j >= g.S && !mbar_wait_flag(smem_u32(&empty[slot]), (uint32_t)((round - 1) & 1), &s_err)) {
@@ -1700,9 +1736,9 @@ __global__ void __launch_bounds__(32 * (ZPAIR_ISSUER0 + ZPAIR_NISS), 1)
         if (lane == 0) {
             int j = 0, slot = 0, round = 0, r = 0, rround = 0;
             bool ok = true;
-            for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
+            for (long long cur = c_begin; ok && cur < c_end;) {
                 int n, q0, z0, z1;
-                item(it, n, q0, z0, z1);
+                item(cur, n, q0, z0, z1);
                 const int rel = q0 - floor_div(q0 - WP - 1, WP) * WP;  // q0 within the slab
                 for (int k = 0; k < z1 - z0 + 2; k++, j++) {
                     const int cur_slot = slot, cur_round = round, cur_r = r, cur_rround = rround;
@@ -1771,9 +1807,9 @@ __global__ void __launch_bounds__(32 * (ZPAIR_ISSUER0 + ZPAIR_NISS), 1)
         // at the end those after its last output's range
         int j = 0;
         bool ok = true;
-        for (long long it = blockIdx.x; ok && it < g.nitems; it += gridDim.x) {
+        for (long long cur = c_begin; ok && cur < c_end;) {
             int n, q0, z0, z1;
-            item(it, n, q0, z0, z1);
+            item(cur, n, q0, z0, z1);
             const int nz = z1 - z0;
             const int q = q0 + row;
             const int y = q / WP, px = q - (q / WP) * WP;
@@ -1960,6 +1996,41 @@ struct ZcatCfg {
     static constexpr int NISS = PER_SM >= 2 ? 2 : 3;
 };
 
+// the work split of the z-column kernels (TmaGeom::ZC, nitems): items of ZC
+// planes dealt round robin, or equal contiguous shares of the (column, plane)
+// pairs; whichever leaves the busiest CTA the fewer stages (a run of Z planes
+// of one column takes Z + 2)
+static void zcol_work_split(TmaGeom &g, long long ncols, int D, long long grid)
+{
+    long long best = -1;
+    for (int zc = D; zc >= 1; zc = zc > 1 ? (zc + 1) / 2 : 0) {
+        const long long items = ncols * ((D + zc - 1) / zc);
+        const long long cost = ((items + grid - 1) / grid) * (zc + 2);
+        if (best < 0 || cost < best) {
+            best = cost;
+            g.ZC = zc;
+            g.nitems = items;
+        }
+        if (zc == 1) break;
+    }
+    const long long total = ncols * D;
+    long long worst = 0;
+    for (long long b = 0; b < grid; b++) {
+        long long cur = total * b / grid, stages = 0;
+        const long long end = total * (b + 1) / grid;
+        while (cur < end) {
+            const long long z0 = cur % D, run = std::min<long long>(D - z0, end - cur);
+            stages += run + 2;
+            cur += run;
+        }
+        worst = std::max(worst, stages);
+    }
+    if (worst < best) {
+        g.ZC = 0;
+        g.nitems = total;
+    }
+}
+
 // the concatenated-dz z-column convolution (conv_zcat_kernel) when its
 // weights stay resident and 4+ stages fit; false leaves the layer to the
 // others.  IAC_DENOISE_ZCAT=0 in the environment turns it off (for comparing
@@ -2014,24 +2085,10 @@ static bool launch_zcat(const ConvArgs &a, const TmaGeom &g0, uint32_t budget, c
         if (per_sm == 0) return false;
         g.S = S;
         const long long grid_max = ((long long)per_sm * std::max(1, a.sms) + NG - 1) / NG;  // per channel group
-        // output planes per work item: a work item of ZC outputs takes ZC + 2 stages (every
-        // stage costs the same MMAs), and the CTAs run ceil(items / grid) rounds of them:
-        // the depth split with the fewest stages on the busiest CTA
-        int ZC = a.D;
-        long long best = -1;
-        for (int zc = a.D; zc >= 1; zc = zc > 1 ? (zc + 1) / 2 : 0) {
-            const long long items = nb * g.T * ((a.D + zc - 1) / zc);
-            const long long cost = ((items + grid_max - 1) / grid_max) * (zc + 2);
-            if (best < 0 || cost < best) {
-                best = cost;
-                ZC = zc;
-            }
-            if (zc == 1) break;
-        }
-        g.ZC = ZC;
-        g.nitems = nb * g.T * ((a.D + ZC - 1) / ZC);
+        const long long grid0 = std::min<long long>(nb * g.T * a.D, grid_max);
+        zcol_work_split(g, nb * g.T, a.D, grid0);
+        const long long grid = g.ZC ? std::min<long long>(grid0, g.nitems) : grid0;
         const uint32_t smem = g.wres_bytes + (uint32_t)S * g.stage_bytes;
-        const long long grid = std::min<long long>(g.nitems, grid_max);
         auto k = conv_zcat_kernel<CIN, COUT, Z::COUTH, Z::NB, Z::NISS, Z::PER_SM>;
         err = smem_attributes(k, smem);
         if (err != cudaSuccess) return true;
@@ -2079,19 +2136,8 @@ static bool launch_zpair(const ConvArgs &a, cudaStream_t s, cudaError_t &err)
         g.S = (int)std::min<uint32_t>(8u, (budget - g.wres_bytes) / g.stage_bytes);
         constexpr int NG = COUT / 16;  // output-channel groups (blockIdx.y)
         const long long grid_max = ((long long)std::max(1, a.sms) + NG - 1) / NG;  // one CTA per SM
-        int ZC = a.D;
-        long long best = -1;
-        for (int zc = a.D; zc >= 1; zc = zc > 1 ? (zc + 1) / 2 : 0) {
-            const long long items = nb * g.T * ((a.D + zc - 1) / zc);
-            const long long cost = ((items + grid_max - 1) / grid_max) * (zc + 2);
-            if (best < 0 || cost < best) {
-                best = cost;
-                ZC = zc;
-            }
-            if (zc == 1) break;
-        }
-        g.ZC = ZC;
-        g.nitems = nb * g.T * ((a.D + ZC - 1) / ZC);
+        const long long grid0 = std::min<long long>(nb * g.T * a.D, grid_max);
+        zcol_work_split(g, nb * g.T, a.D, grid0);
         CUtensorMap map;
         const cuuint64_t dims[5] = {32u, (cuuint64_t)(a.W / 2), (cuuint64_t)a.H, (cuuint64_t)a.D, (cuuint64_t)nb};
         const cuuint64_t strides[4] = {64u, (cuuint64_t)a.W * 32u, (cuuint64_t)a.H * a.W * 32u,
