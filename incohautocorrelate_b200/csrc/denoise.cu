@@ -66,8 +66,10 @@ struct iac_denoiser {
     double *d_dummy_loss = nullptr;
     cudaGraphExec_t step_exec = nullptr;
     std::vector<uintptr_t> step_key;
-    cudaStream_t own_stream = nullptr;  // replay stream for callers on the legacy default stream
+    cudaStream_t own_stream = nullptr;  // capture and replay stream of the step graph (highest priority)
     cudaEvent_t own_ev[2] = {nullptr, nullptr};
+    cudaStream_t side = nullptr;          // the weight gradients' stream in the backward
+    cudaEvent_t ev_g[10] = {}, ev_w[10] = {};  // per layer: its G ready, its weight gradient done
 
     void *alloc(size_t bytes)
     {
@@ -81,6 +83,11 @@ struct iac_denoiser {
         if (step_exec) cudaGraphExecDestroy(step_exec);
         for (cudaEvent_t e : own_ev)
             if (e) cudaEventDestroy(e);
+        for (int l = 0; l < 10; l++) {
+            if (ev_g[l]) cudaEventDestroy(ev_g[l]);
+            if (ev_w[l]) cudaEventDestroy(ev_w[l]);
+        }
+        if (side) cudaStreamDestroy(side);
         if (own_stream) cudaStreamDestroy(own_stream);
         for (void *a : allocs) cudaFree(a);
     }
@@ -308,42 +315,76 @@ iac_status run_backward(iac_denoiser *dn, const float *d_in, const float *d_targ
     h.V = V;
     h.inv_count = 1.0 / (double)V;
     DN_CHECK(head(h, dn->ctx->sm_count, s), "denoiser head");
+    // The weight gradients run on a side stream beside the chain of data
+    // gradients: wgrad(l) needs only the gradient G(l) and its layer's input,
+    // and its result is read by AdamW alone. Each wgrad waits for its G (an
+    // event on the main stream), and the main stream waits for wgrad(k) before
+    // it overwrites a buffer wgrad(k) reads (the gradient buffers are reused
+    // down the network); at the end the main stream waits for the side stream.
+    cudaStream_t sw = dn->side;
+    auto fork_wgrad = [&](int l, const bf16 *x, const bf16 *g, int d, int hh, int ww, long long v) -> iac_status {
+        DN_CHECK(cudaEventRecord(dn->ev_g[l], s), "weight-gradient fork");
+        DN_CHECK(cudaStreamWaitEvent(sw, dn->ev_g[l], 0), "weight-gradient fork");
+        iac_status r = wgrad(dn, l, nullptr, x, g, d, hh, ww, v, sw);
+        if (r != IAC_OK) return r;
+        DN_CHECK(cudaEventRecord(dn->ev_w[l], sw), "weight-gradient done");
+        return IAC_OK;
+    };
+    auto after_wgrad = [&](int l) -> iac_status {
+        DN_CHECK(cudaStreamWaitEvent(s, dn->ev_w[l], 0), "weight-gradient join");
+        return IAC_OK;
+    };
+#define DN_TRY(expr)                    \
+    do {                                \
+        if ((st = (expr)) != IAC_OK) return st; \
+    } while (0)
     // layer 9: X = d1a
-    if ((st = wgrad(dn, 9, nullptr, dn->d1a, dn->gA, D, H, W, V, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 9, dn->gA, dn->gB, D, H, W, V, s, dn->d1a)) != IAC_OK) return st;
-    // layer 8: X = up(d2b) ++ s1
-    if ((st = wgrad(dn, 8, nullptr, dn->cat1, dn->gB, D, H, W, V, s)) != IAC_OK) return st;
-    // the decoder input's gradient in two parts: the upsampled 32 channels, the skip 16
-    if ((st = dgrad(dn, 8, dn->gB, dn->gup1, D, H, W, V, s, nullptr, dn->gskip1, 32)) != IAC_OK) return st;
+    DN_TRY(fork_wgrad(9, dn->d1a, dn->gA, D, H, W, V));
+    DN_TRY(dgrad(dn, 9, dn->gA, dn->gB, D, H, W, V, s, dn->d1a));
+    // layer 8: X = up(d2b) ++ s1; the decoder input's gradient in two parts: the upsampled 32
+    // channels, the skip 16
+    DN_TRY(fork_wgrad(8, dn->cat1, dn->gB, D, H, W, V));
+    DN_TRY(dgrad(dn, 8, dn->gB, dn->gup1, D, H, W, V, s, nullptr, dn->gskip1, 32));
     DN_CHECK(split_concat_grad(dn->gup1, 32, dn->d2b, dn->hA, D, H, W, nb, s), "split 1");
     // layer 7: X = d2a
-    if ((st = wgrad(dn, 7, nullptr, dn->d2a, dn->hA, D2, H2, W2, V2, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 7, dn->hA, dn->hB, D2, H2, W2, V2, s, dn->d2a)) != IAC_OK) return st;
+    DN_TRY(fork_wgrad(7, dn->d2a, dn->hA, D2, H2, W2, V2));
+    DN_TRY(dgrad(dn, 7, dn->hA, dn->hB, D2, H2, W2, V2, s, dn->d2a));
     // layer 6: X = up(b2) ++ s2
-    if ((st = wgrad(dn, 6, nullptr, dn->cat2, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 6, dn->hB, dn->gup2, D2, H2, W2, V2, s, nullptr, dn->gskip2, 64)) != IAC_OK) return st;
+    DN_TRY(fork_wgrad(6, dn->cat2, dn->hB, D2, H2, W2, V2));
+    DN_TRY(dgrad(dn, 6, dn->hB, dn->gup2, D2, H2, W2, V2, s, nullptr, dn->gskip2, 64));
     DN_CHECK(split_concat_grad(dn->gup2, 64, dn->b2, dn->qA, D2, H2, W2, nb, s), "split 2");
     // layer 5: X = b1
-    if ((st = wgrad(dn, 5, nullptr, dn->b1, dn->qA, D4, H4, W4, V4, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 5, dn->qA, dn->qB, D4, H4, W4, V4, s, dn->b1)) != IAC_OK) return st;
-    // layer 4: X = p2
-    if ((st = wgrad(dn, 4, nullptr, dn->p2, dn->qB, D4, H4, W4, V4, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 4, dn->qB, dn->qA, D4, H4, W4, V4, s)) != IAC_OK) return st;  // d p2 (32 ch)
+    DN_TRY(fork_wgrad(5, dn->b1, dn->qA, D4, H4, W4, V4));
+    DN_TRY(dgrad(dn, 5, dn->qA, dn->qB, D4, H4, W4, V4, s, dn->b1));
+    // layer 4: X = p2; its data gradient overwrites qA (wgrad 5's G)
+    DN_TRY(fork_wgrad(4, dn->p2, dn->qB, D4, H4, W4, V4));
+    DN_TRY(after_wgrad(5));
+    DN_TRY(dgrad(dn, 4, dn->qB, dn->qA, D4, H4, W4, V4, s));  // d p2 (32 ch)
+    DN_TRY(after_wgrad(7));  // hA (wgrad 7's G) is overwritten next
     DN_CHECK(pool_grad_mask(dn->gskip2, 32, dn->qA, dn->s2, 32, dn->hA, 32, D2, H2, W2, nb, s), "pool grad 2");
     // layer 3: X = e2a
-    if ((st = wgrad(dn, 3, nullptr, dn->e2a, dn->hA, D2, H2, W2, V2, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 3, dn->hA, dn->hB, D2, H2, W2, V2, s, dn->e2a)) != IAC_OK) return st;
+    DN_TRY(fork_wgrad(3, dn->e2a, dn->hA, D2, H2, W2, V2));
+    DN_TRY(after_wgrad(6));  // hB
+    DN_TRY(dgrad(dn, 3, dn->hA, dn->hB, D2, H2, W2, V2, s, dn->e2a));
     // layer 2: X = p1
-    if ((st = wgrad(dn, 2, nullptr, dn->p1, dn->hB, D2, H2, W2, V2, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 2, dn->hB, dn->hA, D2, H2, W2, V2, s)) != IAC_OK) return st;  // d p1 (16 ch)
+    DN_TRY(fork_wgrad(2, dn->p1, dn->hB, D2, H2, W2, V2));
+    DN_TRY(after_wgrad(3));  // hA
+    DN_TRY(dgrad(dn, 2, dn->hB, dn->hA, D2, H2, W2, V2, s));  // d p1 (16 ch)
+    DN_TRY(after_wgrad(9));  // gA
     DN_CHECK(pool_grad_mask(dn->gskip1, 16, dn->hA, dn->s1, 16, dn->gA, 16, D, H, W, nb, s), "pool grad 1");
     // layer 1: X = e1a
-    if ((st = wgrad(dn, 1, nullptr, dn->e1a, dn->gA, D, H, W, V, s)) != IAC_OK) return st;
-    if ((st = dgrad(dn, 1, dn->gA, dn->gB, D, H, W, V, s, dn->e1a)) != IAC_OK) return st;
-    // layer 0: X = input
+    DN_TRY(fork_wgrad(1, dn->e1a, dn->gA, D, H, W, V));
+    DN_TRY(after_wgrad(8));  // gB
+    DN_TRY(dgrad(dn, 1, dn->gA, dn->gB, D, H, W, V, s, dn->e1a));
+#undef DN_TRY
+    // layer 0: X = input, on the side stream too; then the main stream waits for all
+    DN_CHECK(cudaEventRecord(dn->ev_g[0], s), "weight-gradient fork");
+    DN_CHECK(cudaStreamWaitEvent(sw, dn->ev_g[0], 0), "weight-gradient fork");
     DN_CHECK(wgrad3x3_first(d_in, dn->gB, dn->g + dn->p_off[0], dn->g + dn->p_off[0] + 16 * 27, D, H, W, V,
-                            dn->ctx->sm_count, s),
+                            dn->ctx->sm_count, sw),
              "layer 0 weight gradient");
+    DN_CHECK(cudaEventRecord(dn->ev_w[0], sw), "weight-gradient done");
+    DN_CHECK(cudaStreamWaitEvent(s, dn->ev_w[0], 0), "weight-gradient join");
     return IAC_OK;
 }
 
@@ -432,6 +473,15 @@ iac_status iac_denoise_create(iac_ctx *ctx, uint32_t max_batch, uint32_t D, uint
         delete dn;
         set_error("device memory for a %u x %ux%ux%u denoiser workspace", max_batch, D, H, W);
         return IAC_ERR_NO_MEMORY;
+    }
+    bool evs = cudaStreamCreateWithFlags(&dn->side, cudaStreamNonBlocking) == cudaSuccess;
+    for (int l = 0; l < 10 && evs; l++)
+        evs = cudaEventCreateWithFlags(&dn->ev_g[l], cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&dn->ev_w[l], cudaEventDisableTiming) == cudaSuccess;
+    if (!evs) {
+        delete dn;
+        set_error("the denoiser's weight-gradient stream and events");
+        return IAC_ERR_CUDA;
     }
     cudaMemset(dn->p, 0, off * 4);
     cudaMemset(dn->g, 0, off * 4);
@@ -601,20 +651,21 @@ iac_status iac_denoise_train_steps(iac_denoiser *dn, const uint16_t *d_in_meshes
     iac_status st = check_dims(dn, nb, P, P, P);
     if (st != IAC_OK) return st;
     DeviceGuard guard(dn->ctx->device);
-    cudaStream_t s = (cudaStream_t)stream;
-    cudaStream_t caller = s;
-    if (!s) {
-        // the legacy default stream cannot be captured: replay on a stream of
-        // the denoiser, ordered after and before the caller's work by events
-        if (!dn->own_stream) {
-            DN_CHECK(cudaStreamCreateWithFlags(&dn->own_stream, cudaStreamNonBlocking), "replay stream");
-            DN_CHECK(cudaEventCreateWithFlags(&dn->own_ev[0], cudaEventDisableTiming), "replay event");
-            DN_CHECK(cudaEventCreateWithFlags(&dn->own_ev[1], cudaEventDisableTiming), "replay event");
-        }
-        s = dn->own_stream;
-        DN_CHECK(cudaEventRecord(dn->own_ev[0], caller), "order replay");
-        DN_CHECK(cudaStreamWaitEvent(s, dn->own_ev[0], 0), "order replay");
+    cudaStream_t caller = (cudaStream_t)stream;
+    // the step is captured and replayed on a stream of the denoiser at the highest
+    // priority, ordered after and before the caller's work by events: its kernel
+    // nodes keep that priority (the chain of data gradients) over the weight
+    // gradients' branch, which is captured from the lower-priority side stream
+    if (!dn->own_stream) {
+        int least = 0, greatest = 0;
+        DN_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priorities");
+        DN_CHECK(cudaStreamCreateWithPriority(&dn->own_stream, cudaStreamNonBlocking, greatest), "replay stream");
+        DN_CHECK(cudaEventCreateWithFlags(&dn->own_ev[0], cudaEventDisableTiming), "replay event");
+        DN_CHECK(cudaEventCreateWithFlags(&dn->own_ev[1], cudaEventDisableTiming), "replay event");
     }
+    cudaStream_t s = dn->own_stream;
+    DN_CHECK(cudaEventRecord(dn->own_ev[0], caller), "order replay");
+    DN_CHECK(cudaStreamWaitEvent(s, dn->own_ev[0], 0), "order replay");
     const size_t vox = (size_t)dn->max_batch * dn->D * dn->H * dn->W;
     if (!dn->px) {
         dn->px = (float *)dn->alloc(vox * 4);
@@ -659,7 +710,7 @@ iac_status iac_denoise_train_steps(iac_denoiser *dn, const uint16_t *d_in_meshes
             if (st != IAC_OK) return st;
             DN_CHECK(ce != cudaSuccess ? ce : ee, "capture of the training step");
         }
-        const cudaError_t ie = cudaGraphInstantiate(&dn->step_exec, graph, 0);
+        const cudaError_t ie = cudaGraphInstantiate(&dn->step_exec, graph, cudaGraphInstantiateFlagUseNodePriority);
         cudaGraphDestroy(graph);
         DN_CHECK(ie, "instantiate the training-step graph");
         dn->step_key = key;
@@ -667,10 +718,8 @@ iac_status iac_denoise_train_steps(iac_denoiser *dn, const uint16_t *d_in_meshes
     DN_CHECK(step_counter(dn->d_step, dn->adam_step, 0, s), "reset the step counter");
     if (d_losses) DN_CHECK(cudaMemsetAsync(d_losses, 0, (size_t)nsteps * 8, s), "clear losses");
     for (uint32_t i = 0; i < nsteps; i++) DN_CHECK(cudaGraphLaunch(dn->step_exec, s), "training-step graph");
-    if (s != caller) {
-        DN_CHECK(cudaEventRecord(dn->own_ev[1], s), "order replay");
-        DN_CHECK(cudaStreamWaitEvent(caller, dn->own_ev[1], 0), "order replay");
-    }
+    DN_CHECK(cudaEventRecord(dn->own_ev[1], s), "order replay");
+    DN_CHECK(cudaStreamWaitEvent(caller, dn->own_ev[1], 0), "order replay");
     dn->adam_step += nsteps;
     dn->ctx->launches += (uint64_t)nsteps * dn->step_launches + take_launches();
     return IAC_OK;
