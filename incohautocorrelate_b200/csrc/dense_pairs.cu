@@ -118,9 +118,12 @@ __global__ void tile_box_kernel(const DenseArgs a, float4 *__restrict__ box)
     const float *__restrict__ K = a.K;
     const float *__restrict__ I = a.I;
     float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    float imax = 0.0f;  // largest |I| of the tile (NaN propagates: the tile then takes no fast path)
     if (i < a.npix && I[i] != 0.0f) {  // zero-intensity pixels never contribute
 #pragma unroll
         for (int d = 0; d < 3; d++) mn[d] = mx[d] = K[3 * i + d];
+        imax = fabsf(I[i]);
+        if (imax != imax) imax = INFINITY;
     }
 #pragma unroll
     for (int d = 0; d < 3; d++)
@@ -128,21 +131,24 @@ __global__ void tile_box_kernel(const DenseArgs a, float4 *__restrict__ box)
             mn[d] = fminf(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
             mx[d] = fmaxf(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
         }
-    __shared__ float s[6][DTILE / 32];
+    for (int o = 16; o; o >>= 1) imax = fmaxf(imax, __shfl_xor_sync(0xffffffffu, imax, o));
+    __shared__ float s[7][DTILE / 32];
     const int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0)
+    if ((threadIdx.x & 31) == 0) {
         for (int d = 0; d < 3; d++) {
             s[d][w] = mn[d];
             s[3 + d][w] = mx[d];
         }
+        s[6][w] = imax;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
-        float r[6];
-        for (int d = 0; d < 6; d++) {
+        float r[7];
+        for (int d = 0; d < 7; d++) {
             r[d] = s[d][0];
             for (int j = 1; j < DTILE / 32; j++) r[d] = d < 3 ? fminf(r[d], s[d][j]) : fmaxf(r[d], s[d][j]);
         }
-        box[2 * t] = make_float4(r[0], r[1], r[2], 0.f);
+        box[2 * t] = make_float4(r[0], r[1], r[2], r[6]);
         box[2 * t + 1] = make_float4(r[3], r[4], r[5], 0.f);
     }
 }
@@ -404,6 +410,116 @@ __device__ __forceinline__ void cq_pairs_win(const DenseArgs &a, const Window &w
     red_shared_u64_if(on, wb + 8u * (uint32_t)cur, acc);
 }
 
+// ---- two consecutive staged pixels per step, FP32 work as f32x2 pairs ----
+// add/sub/mul.rn.f32x2 (sm_100) round each lane exactly as the scalar
+// instruction does, so the pair of results is bit-identical to two scalar ops.
+// Unlike scalar mul.rn/add.rn, a packed multiply whose product feeds a packed
+// add can come out of ptxas as one fused FFMA2 (one rounding instead of two),
+// so products are only packed where no add consumes them.
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b)
+{
+    float2 r;
+    asm("{\n\t.reg .b64 x, y, z;\n\tmov.b64 x, {%2, %3};\n\tmov.b64 y, {%4, %5};\n\t"
+        "sub.rn.f32x2 z, x, y;\n\tmov.b64 {%0, %1}, z;\n\t}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 f2add(float2 a, float2 b)
+{
+    float2 r;
+    asm("{\n\t.reg .b64 x, y, z;\n\tmov.b64 x, {%2, %3};\n\tmov.b64 y, {%4, %5};\n\t"
+        "add.rn.f32x2 z, x, y;\n\tmov.b64 {%0, %1}, z;\n\t}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b)
+{
+    float2 r;
+    asm("{\n\t.reg .b64 x, y, z;\n\tmov.b64 x, {%2, %3};\n\tmov.b64 y, {%4, %5};\n\t"
+        "mul.rn.f32x2 z, x, y;\n\tmov.b64 {%0, %1}, z;\n\t}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+
+// round half away from zero of both lanes, as ints (see round_half_away)
+__device__ __forceinline__ int2 f2round_half_away(float2 x)
+{
+    const float2 t = f2add(x, make_float2(copysignf(0.49999997f, x.x), copysignf(0.49999997f, x.y)));
+    return make_int2(__float2int_rz(t.x), __float2int_rz(t.y));
+}
+
+// floor(p * M) for 0 <= p < 2^23 and an integer M < 2^29: p = m * 2^(e - 150)
+// with e >= 1 gives (m * M) >> (150 - e), a shift of at least one bit; the
+// product is below 2^53, so shifts past 63 (p below 2^-87, or p = 0 with its
+// implicit bit forced on) give 0
+__device__ __forceinline__ unsigned long long scaled_floor_small(float p, uint32_t M)
+{
+    const uint32_t b = __float_as_uint(p);
+    const unsigned long long prod = (unsigned long long)((b & 0x7fffffu) | 0x800000u) * M;
+    return prod >> min(150 - (int)(b >> 23), 63);
+}
+
+// one pair of the packed window path: a pair that fails the intensity or
+// MaxQ test adds 0 at the pending voxel (it neither starts nor ends a run)
+__device__ __forceinline__ void win_step(const DenseArgs &a, uint32_t wb, int words, bool ok, int key, float pv,
+                                         int f, int m, int sz, int &cur, unsigned long long &acc)
+{
+    if (ok && (unsigned)key >= (unsigned)words) {  // non-finite k-vectors only
+        global_put_pair(a, f + a.cab, m + a.cab, sz + a.cc, scaled_floor_small(pv, a.mult_int));
+        ok = false;
+    }
+    const int k = ok ? key : cur;
+    const unsigned long long v = scaled_floor_small(ok ? pv : 0.0f, a.mult_int);
+    const bool brk = k != cur;
+    red_shared_u64_if(brk, wb + 8u * (uint32_t)cur, acc);
+    acc = (brk ? 0ull : acc) + v;
+    cur = k;
+}
+
+// cq_pairs_win for an integer Multiplicator and tile pairs whose products stay
+// below 2^23: the staged tile holds consecutive pixels j, j+1 as
+// (x_j, x_j+1, y_j, y_j+1), (z_j, z_j+1, I_j, I_j+1), and each step evaluates
+// both pairs with f32x2 arithmetic (the same roundings as the scalar path),
+// then bins them in order.  j0 may be odd (diagonal tiles): the first step
+// then masks its lower lane.
+template <int KA, int KB, int KC, bool CHECK>
+__device__ __forceinline__ void cq_pairs_win2(const DenseArgs &a, const Window &w, unsigned long long *win,
+                                              const float4 *sp, int j0, float k0, float k1, float k2, float Ia)
+{
+    const int D0 = w.dim[0], D01 = w.dim[0] * w.dim[1];
+    const int words = D01 * w.dim[2];
+    const int base = (a.cab - w.lo[0]) + D0 * (a.cab - w.lo[1]) + D01 * (a.cc - w.lo[2]);
+    const uint32_t wb = (uint32_t)__cvta_generic_to_shared(win);
+    const float2 vp2 = make_float2(a.vpdq, a.vpdq), K0 = make_float2(k0, k0), K1 = make_float2(k1, k1),
+                 K2 = make_float2(k2, k2), IA = make_float2(Ia, Ia);
+    int cur = 0;  // pending run: window index cur, value acc (0 before the first pair)
+    unsigned long long acc = 0;
+    auto step = [&](int jp, bool lo_on) {
+        const float4 A = sp[2 * jp], B = sp[2 * jp + 1];
+        const float2 pv = f2mul(IA, make_float2(B.z, B.w));
+        float2 qx = f2sub(K0, make_float2(A.x, A.y)), qy = f2sub(K1, make_float2(A.z, A.w)),
+               qz = f2sub(K2, make_float2(B.x, B.y));
+        bool ok0 = lo_on && !(pv.x < 1e-37f), ok1 = !(pv.y < 1e-37f);
+        if (CHECK) {  // scalar: ptxas may fuse a packed multiply and add into one FFMA2
+            ok0 = ok0 && !(fadd(fadd(fmul(qx.x, qx.x), fmul(qy.x, qy.x)), fmul(qz.x, qz.x)) > a.maxq2);
+            ok1 = ok1 && !(fadd(fadd(fmul(qx.y, qx.y), fmul(qy.y, qy.y)), fmul(qz.y, qz.y)) > a.maxq2);
+        }
+        qx = f2mul(qx, vp2);
+        qy = f2mul(qy, vp2);
+        qz = f2mul(qz, vp2);
+        const int2 f = f2round_half_away(KA == 0 ? qx : KA == 1 ? qy : qz);
+        const int2 m = f2round_half_away(KB == 0 ? qx : KB == 1 ? qy : qz);
+        const int2 sz = f2round_half_away(KC == 0 ? qx : KC == 1 ? qy : qz);
+        win_step(a, wb, words, ok0, base + f.x + D0 * m.x + D01 * sz.x, pv.x, f.x, m.x, sz.x, cur, acc);
+        win_step(a, wb, words, ok1, base + f.y + D0 * m.y + D01 * sz.y, pv.y, f.y, m.y, sz.y, cur, acc);
+    };
+    int jp = j0 >> 1;
+    if (j0 & 1) step(jp++, false);
+#pragma unroll 2
+    for (; jp < DTILE / 2; jp++) step(jp, true);
+    red_shared_u64_if(acc != 0ull, wb + 8u * (uint32_t)cur, acc);
+}
+
 // upper bound of |k_a - k_b| over two boxes is below MaxQ with a margin that
 // covers the FP32 rounding of the per-pair test (every pair passes it)
 __device__ __forceinline__ bool boxes_within(const float4 a0, const float4 a1, const float4 b0, const float4 b1,
@@ -424,7 +540,7 @@ __device__ __forceinline__ int own_pixel(int t)
 }
 
 template <int INTERP, int KA, int KB, int KC>
-__global__ void __launch_bounds__(DTILE) cq_small_kernel(const DenseArgs a)
+__global__ void __launch_bounds__(DTILE, 6) cq_small_kernel(const DenseArgs a)
 {
     __shared__ float4 sq[DTILE];
     __shared__ unsigned long long win[WINDOW_WORDS];
@@ -465,11 +581,23 @@ __global__ void __launch_bounds__(DTILE) cq_small_kernel(const DenseArgs a)
             if (w.on)
                 for (int i = threadIdx.x; i < words; i += DTILE) win[i] = 0ull;
         }
-        // stage tile Q
+        // integer Multiplicator and every product of the two tiles below 2^23
+        // (the tiles' largest |I|): the packed window path
+        const bool packed = INTERP == 0 && KA >= 0 && w.on && a.mult_int != 0u && fmul(p0.w, q0.w) < 8388608.0f;
+        // stage tile Q: (k, I) per pixel, or interleaved per pixel pair for the packed path
         {
             const uint64_t j = tile_pixel(a, Q, threadIdx.x);
-            sq[threadIdx.x] = j < a.npix ? make_float4(a.K[3 * j], a.K[3 * j + 1], a.K[3 * j + 2], a.I[j])
-                                         : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 v = j < a.npix ? make_float4(a.K[3 * j], a.K[3 * j + 1], a.K[3 * j + 2], a.I[j])
+                                        : make_float4(0.f, 0.f, 0.f, 0.f);
+            if (packed) {
+                float *spf = reinterpret_cast<float *>(sq) + (threadIdx.x >> 1) * 8 + (threadIdx.x & 1);
+                spf[0] = v.x;
+                spf[2] = v.y;
+                spf[4] = v.z;
+                spf[6] = v.w;
+            } else {
+                sq[threadIdx.x] = v;
+            }
         }
         __syncthreads();
         // own pixel: spread over the patch (x 4 apart, y 2 apart within a warp) so
@@ -488,7 +616,12 @@ __global__ void __launch_bounds__(DTILE) cq_small_kernel(const DenseArgs a)
                     self = a.mult_int ? scaled_floor(sv, a.mult_int) : d2u64(dmul((double)sv, a.mult));
             }
             const int j0 = (P == Q) ? own + 1 : 0;
-            if (INTERP == 0 && KA >= 0 && w.on) {
+            if (packed) {
+                if (check)
+                    cq_pairs_win2<KA, KB, KC, true>(a, w, win, sq, j0, k0, k1, k2, Ia);
+                else
+                    cq_pairs_win2<KA, KB, KC, false>(a, w, win, sq, j0, k0, k1, k2, Ia);
+            } else if (INTERP == 0 && KA >= 0 && w.on) {
                 if (a.mult_int) {
                     if (check)
                         cq_pairs_win<KA, KB, KC, true, true>(a, w, win, sq, j0, k0, k1, k2, Ia);
@@ -553,10 +686,12 @@ __device__ __forceinline__ uint32_t wrap_bin(uint32_t b, uint32_t n)
 template <int INTERP>
 __global__ void __launch_bounds__(DTILE) ac1d_cq_kernel(const DenseArgs a)
 {
-    extern __shared__ unsigned long long hist[];
+    // the launch's histogram as split 64-bit counters: low words, then high words
+    extern __shared__ uint32_t hist32[];
+    uint32_t *const hlo = hist32, *const hhi = hist32 + a.hsize;
     __shared__ float4 sq[DTILE];
     __shared__ unsigned long long s_pair;
-    for (uint32_t i = threadIdx.x; i < a.hsize; i += DTILE) hist[i] = 0;
+    for (uint32_t i = threadIdx.x; i < 2 * a.hsize; i += DTILE) hist32[i] = 0;
     const uint32_t T = a.ntiles;
     for (;;) {
         if (threadIdx.x == 0) s_pair = atomicAdd(a.queue, 1ull);
@@ -586,8 +721,9 @@ __global__ void __launch_bounds__(DTILE) ac1d_cq_kernel(const DenseArgs a)
             if (P == Q) {  // self pair: q = 0 -> bin 0, once
                 const float sv = fmul(Ia, Ia);
                 if (!(sv < 1e-37f))
-                    atomicAdd(&hist[0], a.mult_int ? scaled_floor(sv, a.mult_int)
-                                                   : (unsigned long long)(long long)dmul((double)sv, a.mult));
+                    shared_add_u64_split(hlo, hhi, 0,
+                                         a.mult_int ? scaled_floor(sv, a.mult_int)
+                                                    : (unsigned long long)(long long)dmul((double)sv, a.mult));
             }
             const int j0 = (P == Q) ? own + 1 : 0;
             for (int j = j0; j < DTILE; j++) {
@@ -605,7 +741,7 @@ __global__ void __launch_bounds__(DTILE) ac1d_cq_kernel(const DenseArgs a)
                     const uint32_t sc = wrap_bin((uint32_t)floorf(fadd(q, 0.5f)), a.hsize);
                     const unsigned long long v =
                         a.mult_int ? scaled_floor(pv, a.mult_int) : (unsigned long long)(long long)dmul(val, a.mult);
-                    atomicAdd(&hist[sc], 2ull * v);
+                    shared_add_u64_split(hlo, hhi, sc, 2ull * v);
                 } else {
                     const float fq = floorf(q);
                     const uint32_t sc1 = wrap_bin((uint32_t)fq, a.hsize), sc2 = wrap_bin((uint32_t)fq + 1, a.hsize);
@@ -613,16 +749,18 @@ __global__ void __launch_bounds__(DTILE) ac1d_cq_kernel(const DenseArgs a)
                     const unsigned long long v1 =
                         (unsigned long long)(long long)dmul(dmul(val, dsub(1.0, sep)), a.mult);
                     const unsigned long long v2 = (unsigned long long)(long long)dmul(dmul(val, sep), a.mult);
-                    atomicAdd(&hist[sc1], 2ull * v1);
-                    atomicAdd(&hist[sc2], 2ull * v2);
+                    shared_add_u64_split(hlo, hhi, sc1, 2ull * v1);
+                    shared_add_u64_split(hlo, hhi, sc2, 2ull * v2);
                 }
             }
         }
         __syncthreads();
     }
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < a.hsize; i += DTILE)
-        if (hist[i]) atomicAdd(&a.out[i], hist[i]);
+    for (uint32_t i = threadIdx.x; i < a.hsize; i += DTILE) {
+        const unsigned long long v = split_word(hlo, hhi, i);
+        if (v) atomicAdd(&a.out[i], v);
+    }
 }
 
 // --------------------------------------------------------------------------

@@ -521,9 +521,17 @@ struct AC1DArgs {
     double *frac_out;             // size doubles: host-route other values
 };
 
+// shared-memory histograms of one CTA: 64-bit counters as split 32-bit words
+// (shared_add_u64_split), host-route fractions as doubles
+struct AC1DHist {
+    uint32_t *dev_lo, *dev_hi;  // vecsize words each
+    uint32_t *int_lo, *int_hi;  // size words each
+    double *frac;               // size doubles
+};
+
 // host-route value v (>= 0) into bin b
-__device__ __forceinline__ void host_route_add(const SparseArgs &a, const AC1DArgs &b, unsigned long long *hint,
-                                               double *hfrac, uint32_t bin, float v)
+__device__ __forceinline__ void host_route_add(const SparseArgs &a, const AC1DArgs &b, const AC1DHist &h,
+                                               uint32_t bin, float v)
 {
     if (bin >= b.size) {  // only for inconsistent MaxQ / dq; the reference writes out of bounds
         atomicAdd(&a.counters->out_of_mesh, 1ull);
@@ -531,17 +539,21 @@ __device__ __forceinline__ void host_route_add(const SparseArgs &a, const AC1DAr
     }
     if (v == 0.0f) return;
     if (v == truncf(v) && v < 1.8e19f)
-        atomicAdd(&hint[bin], (unsigned long long)__float2ull_rz(v));
+        shared_add_u64_split(h.int_lo, h.int_hi, bin, (unsigned long long)__float2ull_rz(v));
     else
-        atomicAdd(&hfrac[bin], (double)v);
+        atomicAdd(&h.frac[bin], (double)v);
 }
 
 template <int INTERP>
 __global__ void __launch_bounds__(256) ac1d_sparse_kernel(const SparseArgs a, const AC1DArgs b)
 {
     extern __shared__ unsigned long long hist[];
-    unsigned long long *hdev = hist, *hint = hist + b.vecsize;
-    double *hfrac = reinterpret_cast<double *>(hist + b.vecsize + b.size);
+    AC1DHist h;
+    h.dev_lo = reinterpret_cast<uint32_t *>(hist);
+    h.dev_hi = h.dev_lo + b.vecsize;
+    h.int_lo = h.dev_hi + b.vecsize;
+    h.int_hi = h.int_lo + b.size;
+    h.frac = reinterpret_cast<double *>(hist + b.vecsize + b.size);
     __shared__ unsigned long long s_tile;
     __shared__ uint32_t s_frame;
     const uint32_t words = b.vecsize + 2 * b.size;
@@ -577,11 +589,11 @@ __global__ void __launch_bounds__(256) ac1d_sparse_kernel(const SparseArgs a, co
             for (uint32_t i = threadIdx.x; i < n; i += nthr) {
                 const float w = P[i].w;
                 if (host) {
-                    host_route_add(a, b, hint, hfrac, 0, fmul(2.0f, fmul(w, w)));
+                    host_route_add(a, b, h, 0, fmul(2.0f, fmul(w, w)));
                 } else {
                     const double v = (double)w;
                     const unsigned long long u = d2u64(dmul(dmul(v, v), a.mult));
-                    if (u) atomicAdd(&hdev[0], u);
+                    if (u) shared_add_u64_split(h.dev_lo, h.dev_hi, 0, u);
                 }
             }
         const unsigned long long npairs = (unsigned long long)n * (n - 1) / 2;
@@ -603,27 +615,27 @@ __global__ void __launch_bounds__(256) ac1d_sparse_kernel(const SparseArgs a, co
                     if (host) {
                         const float pv = fmul(A.w, B.w);
                         if (INTERP == 0) {
-                            host_route_add(a, b, hint, hfrac, (uint32_t)floor(dadd((double)q, 0.5)),
-                                           fmul(2.0f, pv));
+                            host_route_add(a, b, h, (uint32_t)floor(dadd((double)q, 0.5)), fmul(2.0f, pv));
                         } else {
                             const float fq = floorf(q);
                             const float sep = fsub(q, fq);
-                            host_route_add(a, b, hint, hfrac, (uint32_t)fq, fmul(2.0f, fmul(pv, fsub(1.0f, sep))));
-                            host_route_add(a, b, hint, hfrac, (uint32_t)fq + 1, fmul(2.0f, fmul(pv, sep)));
+                            host_route_add(a, b, h, (uint32_t)fq, fmul(2.0f, fmul(pv, fsub(1.0f, sep))));
+                            host_route_add(a, b, h, (uint32_t)fq + 1, fmul(2.0f, fmul(pv, sep)));
                         }
                     } else {
                         const double val = dmul((double)A.w, (double)B.w);
                         if (INTERP == 0) {
                             const uint32_t sc = wrap_bin((uint32_t)floor(dadd((double)q, 0.5)), b.vecsize);
                             const unsigned long long w = d2u64(dmul(val, a.mult));
-                            if (w) atomicAdd(&hdev[sc], 2ull * w);
+                            if (w) shared_add_u64_split(h.dev_lo, h.dev_hi, sc, 2ull * w);
                         } else {
                             const float fq = floorf(q);
                             const double sep = (double)fsub(q, fq);
                             const unsigned long long w1 = d2u64(dmul(dmul(val, dsub(1.0, sep)), a.mult));
                             const unsigned long long w2 = d2u64(dmul(dmul(val, sep), a.mult));
-                            if (w1) atomicAdd(&hdev[wrap_bin((uint32_t)fq, b.vecsize)], 2ull * w1);
-                            if (w2) atomicAdd(&hdev[wrap_bin((uint32_t)fq + 1, b.vecsize)], 2ull * w2);
+                            if (w1) shared_add_u64_split(h.dev_lo, h.dev_hi, wrap_bin((uint32_t)fq, b.vecsize), 2ull * w1);
+                            if (w2)
+                                shared_add_u64_split(h.dev_lo, h.dev_hi, wrap_bin((uint32_t)fq + 1, b.vecsize), 2ull * w2);
                         }
                     }
                 }
@@ -638,11 +650,14 @@ __global__ void __launch_bounds__(256) ac1d_sparse_kernel(const SparseArgs a, co
         __syncthreads();
     }
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < b.vecsize; i += blockDim.x)
-        if (hdev[i]) atomicAdd(&b.dev_out[i], hdev[i]);
+    for (uint32_t i = threadIdx.x; i < b.vecsize; i += blockDim.x) {
+        const unsigned long long v = split_word(h.dev_lo, h.dev_hi, i);
+        if (v) atomicAdd(&b.dev_out[i], v);
+    }
     for (uint32_t i = threadIdx.x; i < b.size; i += blockDim.x) {
-        if (hint[i]) atomicAdd(&b.int_out[i], hint[i]);
-        if (hfrac[i] != 0.0) atomicAdd(&b.frac_out[i], hfrac[i]);
+        const unsigned long long v = split_word(h.int_lo, h.int_hi, i);
+        if (v) atomicAdd(&b.int_out[i], v);
+        if (h.frac[i] != 0.0) atomicAdd(&b.frac_out[i], h.frac[i]);
     }
 }
 

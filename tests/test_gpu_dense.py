@@ -78,6 +78,26 @@ def test_cq_small_value_paths(ctx, oracle_lib, rng, mult):
         np.testing.assert_array_equal(_u64(out), want)
 
 
+def test_cq_small_bright_pixels(ctx, oracle_lib, rng):
+    """Products at and above 2^23 (|I| up to 4096) in some tiles: those tile
+    pairs take the general integer value path, the others the packed one,
+    within one launch."""
+    o = oracle_lib
+    pm, km, mq = small_detector(48, 64, 6e-4)
+    I = _intensity(km.size // 3, rng)
+    I[5] = np.float32(4096.0)
+    I[1000] = np.float32(2896.31)
+    I[2500] = np.float32(-3000.0)
+    s = o.small_cq_mesh_shape(mq, 31)
+    for mult in (1000.0, 2.0 ** 29 - 1):
+        want = _oracle_cq_small(o, I, km, s, 0, mult)
+        for fast in (0, 64):
+            out = _zeros(want.size)
+            ctx.cq_small(_dev(I), _dev(km), I.size, to_capi_shape(s), 0, mult, out, fast_size=fast)
+            assert ctx.check() == 0
+            np.testing.assert_array_equal(_u64(out), want)
+
+
 def test_cq_small_dense_detector_region(ctx, oracle_lib):
     """The 1024x1024 radial mean-intensity map's geometry on a 128x128 crop,
     255-edge small mesh: exact against the oracle in full."""
