@@ -40,7 +40,7 @@
 namespace iac {
 
 constexpr int DTILE = 256;        // pixels per tile == threads per CTA
-constexpr int WINDOW_WORDS = 2048;  // shared-memory window (16 KB of uint64)
+constexpr int WINDOW_WORDS = 2048;  // shared-memory window: 2048 split 64-bit counters (16 KB)
 
 struct DenseArgs {
     const float *__restrict__ I;
@@ -197,14 +197,14 @@ __device__ __forceinline__ void global_put_pair(const DenseArgs &a, int fs, int 
     }
 }
 
-__device__ __forceinline__ void put(const DenseArgs &a, const Window &w, unsigned long long *win,
+__device__ __forceinline__ void put(const DenseArgs &a, const Window &w, uint32_t *win,
                                     int fs, int ms, int ss, unsigned long long v)
 {
     if (v == 0) return;
     const int x = fs - w.lo[0], y = ms - w.lo[1], z = ss - w.lo[2];
     if (w.on && (unsigned)x < (unsigned)w.dim[0] && (unsigned)y < (unsigned)w.dim[1] &&
         (unsigned)z < (unsigned)w.dim[2])
-        atomicAdd(&win[x + w.dim[0] * (y + w.dim[1] * z)], v);
+        shared_add_u64_split(win, win + WINDOW_WORDS, x + w.dim[0] * (y + w.dim[1] * z), v);
     else
         global_put_pair(a, fs, ms, ss, v);
 }
@@ -234,7 +234,7 @@ __device__ __forceinline__ float axis(float x, float y, float z, int k)
 // CHECK: apply the per-pair MaxQ test (skipped when the two tiles' bounding
 // boxes are entirely within MaxQ, where every pair passes it).
 template <int INTERP, int KA, int KB, int KC, bool CHECK>
-__device__ __forceinline__ void cq_pairs(const DenseArgs &a, const Window &w, unsigned long long *win,
+__device__ __forceinline__ void cq_pairs(const DenseArgs &a, const Window &w, uint32_t *win,
                                          const float4 *sq, int j0, float k0, float k1, float k2, float Ia)
 {
     int cur_f = 0, cur_m = 0, cur_s = 0;
@@ -320,7 +320,7 @@ __device__ __forceinline__ unsigned long long scaled_floor_normal(float p, uint3
 // key_ok guarantees for every pair inside MaxQ), the value path is chosen at
 // compile time (MINT: integer Multiplicator)
 template <int KA, int KB, int KC, bool CHECK, bool MINT>
-__device__ __forceinline__ void cq_pairs_nn(const DenseArgs &a, const Window &w, unsigned long long *win,
+__device__ __forceinline__ void cq_pairs_nn(const DenseArgs &a, const Window &w, uint32_t *win,
                                             const float4 *sq, int j0, float k0, float k1, float k2, float Ia)
 {
     constexpr int NONE = -2147483647 - 1;
@@ -354,32 +354,21 @@ __device__ __forceinline__ void cq_pairs_nn(const DenseArgs &a, const Window &w,
     if (cur != NONE) put(a, w, win, cf + a.cab, cm + a.cab, cs + a.cc, acc);
 }
 
-// shared-memory 64-bit add, issued only where p holds (no branch)
-__device__ __forceinline__ void red_shared_u64_if(bool p, uint32_t addr, unsigned long long v)
-{
-    asm volatile(
-        "{\n\t.reg .pred q;\n\t"
-        "setp.ne.b32 q, %0, 0;\n\t"
-        "@q red.shared.add.u64 [%1], %2;\n\t}\n" ::"r"((int)p),
-        "r"(addr), "l"(v)
-        : "memory");
-}
 
 // cq_pairs_nn when the window is on: every pair inside MaxQ lands in the
 // window (it spans the two tiles' q range with a voxel of margin), so the run
-// key is the voxel's window index itself and a finished run is one predicated
+// key is the voxel's window index itself and a finished run is one split 64-bit
 // shared-memory add.  Pairs that fail the intensity or MaxQ test are masked
 // rather than skipped, so a warp never diverges on them; the only branch is
 // the guard for an index outside the window (non-finite k-vectors), which
 // takes the global path of put().
 template <int KA, int KB, int KC, bool CHECK, bool MINT>
-__device__ __forceinline__ void cq_pairs_win(const DenseArgs &a, const Window &w, unsigned long long *win,
+__device__ __forceinline__ void cq_pairs_win(const DenseArgs &a, const Window &w, uint32_t *win,
                                              const float4 *sq, int j0, float k0, float k1, float k2, float Ia)
 {
     const int D0 = w.dim[0], D01 = w.dim[0] * w.dim[1];
     const int words = D01 * w.dim[2];
     const int base = (a.cab - w.lo[0]) + D0 * (a.cab - w.lo[1]) + D01 * (a.cc - w.lo[2]);
-    const uint32_t wb = (uint32_t)__cvta_generic_to_shared(win);
     const float vpdq = a.vpdq;
     int cur = 0;
     bool on = false;  // a run is pending at window index cur
@@ -400,14 +389,14 @@ __device__ __forceinline__ void cq_pairs_win(const DenseArgs &a, const Window &w
         const int key = base + f + D0 * m + D01 * sz;
         const unsigned long long v = MINT ? scaled_floor_normal(pv, a.mult_int) : d2u64(dmul((double)pv, a.mult));
         const bool brk = ok && (!on || key != cur);  // a new run starts at this pair
-        red_shared_u64_if(brk && on, wb + 8u * (uint32_t)cur, acc);
+        if (brk && on) shared_add_u64_split(win, win + WINDOW_WORDS, (uint32_t)cur, acc);
         const bool inwin = (unsigned)key < (unsigned)words;
         if (brk && !inwin) global_put_pair(a, f + a.cab, m + a.cab, sz + a.cc, v);
         acc = brk ? (inwin ? v : 0ull) : (ok ? acc + v : acc);
         cur = brk ? key : cur;
         on = brk ? inwin : on;
     }
-    red_shared_u64_if(on, wb + 8u * (uint32_t)cur, acc);
+    if (on) shared_add_u64_split(win, win + WINDOW_WORDS, (uint32_t)cur, acc);
 }
 
 // ---- two consecutive staged pixels per step, FP32 work as f32x2 pairs ----
@@ -461,7 +450,7 @@ __device__ __forceinline__ unsigned long long scaled_floor_small(float p, uint32
 
 // one pair of the packed window path: a pair that fails the intensity or
 // MaxQ test adds 0 at the pending voxel (it neither starts nor ends a run)
-__device__ __forceinline__ void win_step(const DenseArgs &a, uint32_t wb, int words, bool ok, int key, float pv,
+__device__ __forceinline__ void win_step(const DenseArgs &a, uint32_t *win, int words, bool ok, int key, float pv,
                                          int f, int m, int sz, int &cur, unsigned long long &acc)
 {
     if (ok && (unsigned)key >= (unsigned)words) {  // non-finite k-vectors only
@@ -471,7 +460,7 @@ __device__ __forceinline__ void win_step(const DenseArgs &a, uint32_t wb, int wo
     const int k = ok ? key : cur;
     const unsigned long long v = scaled_floor_small(ok ? pv : 0.0f, a.mult_int);
     const bool brk = k != cur;
-    red_shared_u64_if(brk, wb + 8u * (uint32_t)cur, acc);
+    if (brk && acc) shared_add_u64_split(win, win + WINDOW_WORDS, (uint32_t)cur, acc);
     acc = (brk ? 0ull : acc) + v;
     cur = k;
 }
@@ -483,13 +472,12 @@ __device__ __forceinline__ void win_step(const DenseArgs &a, uint32_t wb, int wo
 // then bins them in order.  j0 may be odd (diagonal tiles): the first step
 // then masks its lower lane.
 template <int KA, int KB, int KC, bool CHECK>
-__device__ __forceinline__ void cq_pairs_win2(const DenseArgs &a, const Window &w, unsigned long long *win,
+__device__ __forceinline__ void cq_pairs_win2(const DenseArgs &a, const Window &w, uint32_t *win,
                                               const float4 *sp, int j0, float k0, float k1, float k2, float Ia)
 {
     const int D0 = w.dim[0], D01 = w.dim[0] * w.dim[1];
     const int words = D01 * w.dim[2];
     const int base = (a.cab - w.lo[0]) + D0 * (a.cab - w.lo[1]) + D01 * (a.cc - w.lo[2]);
-    const uint32_t wb = (uint32_t)__cvta_generic_to_shared(win);
     const float2 vp2 = make_float2(a.vpdq, a.vpdq), K0 = make_float2(k0, k0), K1 = make_float2(k1, k1),
                  K2 = make_float2(k2, k2), IA = make_float2(Ia, Ia);
     int cur = 0;  // pending run: window index cur, value acc (0 before the first pair)
@@ -510,14 +498,14 @@ __device__ __forceinline__ void cq_pairs_win2(const DenseArgs &a, const Window &
         const int2 f = f2round_half_away(KA == 0 ? qx : KA == 1 ? qy : qz);
         const int2 m = f2round_half_away(KB == 0 ? qx : KB == 1 ? qy : qz);
         const int2 sz = f2round_half_away(KC == 0 ? qx : KC == 1 ? qy : qz);
-        win_step(a, wb, words, ok0, base + f.x + D0 * m.x + D01 * sz.x, pv.x, f.x, m.x, sz.x, cur, acc);
-        win_step(a, wb, words, ok1, base + f.y + D0 * m.y + D01 * sz.y, pv.y, f.y, m.y, sz.y, cur, acc);
+        win_step(a, win, words, ok0, base + f.x + D0 * m.x + D01 * sz.x, pv.x, f.x, m.x, sz.x, cur, acc);
+        win_step(a, win, words, ok1, base + f.y + D0 * m.y + D01 * sz.y, pv.y, f.y, m.y, sz.y, cur, acc);
     };
     int jp = j0 >> 1;
     if (j0 & 1) step(jp++, false);
 #pragma unroll 2
     for (; jp < DTILE / 2; jp++) step(jp, true);
-    red_shared_u64_if(acc != 0ull, wb + 8u * (uint32_t)cur, acc);
+    if (acc) shared_add_u64_split(win, win + WINDOW_WORDS, (uint32_t)cur, acc);
 }
 
 // upper bound of |k_a - k_b| over two boxes is below MaxQ with a margin that
@@ -543,7 +531,7 @@ template <int INTERP, int KA, int KB, int KC>
 __global__ void __launch_bounds__(DTILE, 6) cq_small_kernel(const DenseArgs a)
 {
     __shared__ float4 sq[DTILE];
-    __shared__ unsigned long long win[WINDOW_WORDS];
+    __shared__ uint32_t win[2 * WINDOW_WORDS];  // split 64-bit counters: low words, then high words
     __shared__ unsigned long long s_pair;
     __shared__ unsigned long long s_self[DTILE / 32];
     const uint32_t T = a.ntiles;
@@ -579,7 +567,7 @@ __global__ void __launch_bounds__(DTILE, 6) cq_small_kernel(const DenseArgs a)
             }
             w.on = ok && words <= WINDOW_WORDS;
             if (w.on)
-                for (int i = threadIdx.x; i < words; i += DTILE) win[i] = 0ull;
+                for (int i = threadIdx.x; i < words; i += DTILE) win[i] = win[WINDOW_WORDS + i] = 0u;
         }
         // integer Multiplicator and every product of the two tiles below 2^23
         // (the tiles' largest |I|): the packed window path
@@ -663,7 +651,7 @@ __global__ void __launch_bounds__(DTILE, 6) cq_small_kernel(const DenseArgs a)
         if (w.on) {
             const int words = w.dim[0] * w.dim[1] * w.dim[2];
             for (int i = threadIdx.x; i < words; i += DTILE) {
-                const unsigned long long v = win[i];
+                const unsigned long long v = split_word(win, win + WINDOW_WORDS, i);
                 if (!v) continue;
                 const int x = i % w.dim[0], y = (i / w.dim[0]) % w.dim[1], z = i / (w.dim[0] * w.dim[1]);
                 global_put_pair(a, x + w.lo[0], y + w.lo[1], z + w.lo[2], v);

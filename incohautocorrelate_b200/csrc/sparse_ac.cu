@@ -65,7 +65,8 @@ struct SparseArgs {
     uint64_t mesh_policy;  // set inside the kernel when cache_hints is on
     int box_r;        // half-width of the shared-memory box around q = 0 (0: none)
     int box_w;        // 2 * box_r + 1
-    uint32_t box_base;  // shared-memory address of the box (set inside the kernel)
+    uint32_t box_base;  // shared-memory address of the box's low words (set inside the kernel)
+    uint32_t box_hi;    // shared-memory address of its high words (set inside the kernel)
 };
 
 // L2 cache policies (PTX createpolicy) for the pair kernel: the half mesh is
@@ -174,6 +175,19 @@ __global__ void sparse_count_check_kernel(const float4 *__restrict__ ph, const u
 // ---------------------------------------------------------------------------
 // binning helpers (IAC/kernel.cl:349-448)
 // ---------------------------------------------------------------------------
+// v into word k of the shared-memory box, a split 64-bit counter (low words at
+// box_base, high words at box_hi): 32-bit shared atomics are native, 64-bit
+// ones are several times slower, above all where the lanes of a warp meet at
+// one voxel near q = 0
+__device__ __forceinline__ void box_add(const SparseArgs &a, uint32_t k, unsigned long long v)
+{
+    const uint32_t vl = (uint32_t)v;
+    uint32_t old;
+    asm volatile("atom.shared.add.u32 %0, [%1], %2;" : "=r"(old) : "r"(a.box_base + 4u * k), "r"(vl) : "memory");
+    const uint32_t up = (uint32_t)(v >> 32) + (old + vl < old ? 1u : 0u);
+    if (up) asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(a.box_hi + 4u * k), "r"(up) : "memory");
+}
+
 __device__ __forceinline__ void hm_put(const SparseArgs &a, int fs, int ms, int ss,
                                        unsigned long long v)
 {
@@ -187,7 +201,7 @@ __device__ __forceinline__ void hm_put(const SparseArgs &a, int fs, int ms, int 
         const uint32_t dx = (uint32_t)(fs - a.C + a.box_r), dy = (uint32_t)(ms - a.C + a.box_r);
         if (dx < (uint32_t)a.box_w && dy < (uint32_t)a.box_w && (uint32_t)ss <= (uint32_t)a.box_r) {
             const uint32_t k = ((uint32_t)ss * a.box_w + dy) * a.box_w + dx;
-            asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(a.box_base + 8u * k), "l"(v) : "memory");
+            box_add(a, k, v);
             return;
         }
     }
@@ -346,14 +360,16 @@ __global__ void __launch_bounds__(256) sparse_pairs_kernel(SparseArgs a)
     __shared__ float s_rot[9];
     __shared__ int s_small;
     __shared__ unsigned long long s_self[8];
-    extern __shared__ unsigned long long s_box[];  // (box_r + 1) x box_w x box_w, [ss][ms][fs]
+    // (box_r + 1) x box_w x box_w split 64-bit counters, [ss][ms][fs]: low words, then high words
+    extern __shared__ uint32_t s_box[];
 
     const unsigned long long ntiles = a.tile_off[a.nframes];
     const uint32_t nthr = blockDim.x;
     const uint32_t box_n = a.box_r ? (uint32_t)(a.box_r + 1) * a.box_w * a.box_w : 0u;
     a.box_base = (uint32_t)__cvta_generic_to_shared(s_box);
-    for (uint32_t k = threadIdx.x; k < box_n; k += nthr) s_box[k] = 0ull;  // visible after the
-                                                                          // loop's first barrier
+    a.box_hi = a.box_base + 4u * box_n;
+    for (uint32_t k = threadIdx.x; k < 2 * box_n; k += nthr) s_box[k] = 0u;  // visible after the
+                                                                            // loop's first barrier
     for (;;) {
         if (threadIdx.x == 0) {
             const unsigned long long t = atomicAdd(a.queue, 1ull);
@@ -430,9 +446,7 @@ __global__ void __launch_bounds__(256) sparse_pairs_kernel(SparseArgs a)
             for (uint32_t w = 0; w < (nthr + 31) / 32; w++) s += s_self[w];
             if (s) {  // q = 0: the box's centre when there is a box
                 if (a.box_r)
-                    asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(a.box_base + 8u * (uint32_t)(a.box_r * a.box_w + a.box_r)),
-                                 "l"(s)
-                                 : "memory");
+                    box_add(a, (uint32_t)(a.box_r * a.box_w + a.box_r), s);
                 else
                     atomicAdd(&a.half[(size_t)a.C + (size_t)a.C * a.S], s);
             }
@@ -440,7 +454,7 @@ __global__ void __launch_bounds__(256) sparse_pairs_kernel(SparseArgs a)
     }
     // the loop ends after a barrier: every shared-memory add is done; flush the box
     for (uint32_t k = threadIdx.x; k < box_n; k += nthr) {
-        const unsigned long long v = s_box[k];
+        const unsigned long long v = split_word(s_box, s_box + box_n, k);
         if (v == 0) continue;
         const uint32_t ss = k / (uint32_t)(a.box_w * a.box_w), r = k - ss * (uint32_t)(a.box_w * a.box_w);
         const uint32_t ms = (uint32_t)(a.C - a.box_r) + r / (uint32_t)a.box_w;
@@ -814,6 +828,7 @@ static iac_status launch_pair_batch(iac_ctx *ctx, const float *d_photons, const 
     a.box_r = pair_box_radius(a.C, tun.ctas_per_sm);
     a.box_w = 2 * a.box_r + 1;
     a.box_base = 0;
+    a.box_hi = 0;
     const size_t box_bytes = a.box_r ? sizeof(unsigned long long) * (a.box_r + 1) * a.box_w * a.box_w : 0;
     const PairKernel k = pick_kernel(p->double_map, p->interp_first, p->interp_second);
     if (box_bytes > (48u << 10))
