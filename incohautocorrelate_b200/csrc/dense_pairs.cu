@@ -528,7 +528,7 @@ __device__ __forceinline__ int own_pixel(int t)
 }
 
 template <int INTERP, int KA, int KB, int KC>
-__global__ void __launch_bounds__(DTILE, 6) cq_small_kernel(const DenseArgs a)
+__global__ void __launch_bounds__(DTILE, 5) cq_small_kernel(const DenseArgs a)
 {
     __shared__ float4 sq[DTILE];
     __shared__ uint32_t win[2 * WINDOW_WORDS];  // split 64-bit counters: low words, then high words
@@ -731,8 +731,9 @@ __global__ void __launch_bounds__(DTILE) ac1d_cq_kernel(const DenseArgs a)
                         a.mult_int ? scaled_floor(pv, a.mult_int) : (unsigned long long)(long long)dmul(val, a.mult);
                     shared_add_u64_split(hlo, hhi, sc, 2ull * v);
                 } else {
-                    const float fq = floorf(q);
-                    const uint32_t sc1 = wrap_bin((uint32_t)fq, a.hsize), sc2 = wrap_bin((uint32_t)fq + 1, a.hsize);
+                    uint32_t iq;  // q = |q| / dq <= MaxQ / dq < 2^23
+                    const float fq = floor_small(q, iq);
+                    const uint32_t sc1 = wrap_bin(iq, a.hsize), sc2 = wrap_bin(iq + 1, a.hsize);
                     const double sep = (double)fsub(q, fq);
                     const unsigned long long v1 =
                         (unsigned long long)(long long)dmul(dmul(val, dsub(1.0, sep)), a.mult);
@@ -1033,6 +1034,9 @@ iac_status iac_ac1d_cq(iac_ctx *ctx, const float *d_I, const float *d_kmap, uint
     IAC_REQUIRE(interp == 0 || interp == 1, "interpolation must be 0 or 1");
     IAC_REQUIRE(npix > 0 && npix < (1ull << 32), "iac_ac1d_cq: pixel count out of range");
     IAC_REQUIRE(sh->size >= 3 && sh->size <= 24576, "AC1D size %u out of range [3, 24576]", sh->size);
+    IAC_REQUIRE(sh->dq_per_step > 0 && (double)sh->max_q / sh->dq_per_step < 4194304.0,
+                "iac_ac1d_cq: MaxQ / dq must be below 2^22 (dq %g, MaxQ %g)", (double)sh->dq_per_step,
+                (double)sh->max_q);
     IAC_REQUIRE(mult > 0, "multiplicator must be positive");
     DeviceGuard g(ctx->device);
     DenseArgs a{};

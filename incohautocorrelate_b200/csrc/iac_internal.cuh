@@ -264,6 +264,17 @@ __device__ __forceinline__ int round_away_rz_i(float x)
     return x < 0.0f ? -r : r;
 }
 
+// floor of 0 <= q < 2^23 as a float and as an integer on the FMA and integer
+// pipes (no conversion-unit instruction): q +rz 2^23 = 2^23 + floor(q) exactly,
+// and its bits minus those of 2^23 are floor(q).  A NaN q (non-finite
+// k-vectors only) gives an index far past every histogram.
+__device__ __forceinline__ float floor_small(float q, uint32_t &iq)
+{
+    const float t = __fadd_rz(q, 8388608.0f);
+    iq = (uint32_t)(__float_as_int(t) - TWO23_BITS);
+    return fsub(t, 8388608.0f);
+}
+
 // as a float; exact for |x| < 2^23 (callers bound x), NaN stays NaN
 __device__ __forceinline__ float round_away_rz_f(float x)
 {

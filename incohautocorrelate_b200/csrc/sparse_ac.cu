@@ -631,10 +631,11 @@ __global__ void __launch_bounds__(256) ac1d_sparse_kernel(const SparseArgs a, co
                         if (INTERP == 0) {
                             host_route_add(a, b, h, (uint32_t)floor(dadd((double)q, 0.5)), fmul(2.0f, pv));
                         } else {
-                            const float fq = floorf(q);
+                            uint32_t iq;  // q = |q| / dq <= MaxQ / dq < 2^23
+                            const float fq = floor_small(q, iq);
                             const float sep = fsub(q, fq);
-                            host_route_add(a, b, h, (uint32_t)fq, fmul(2.0f, fmul(pv, fsub(1.0f, sep))));
-                            host_route_add(a, b, h, (uint32_t)fq + 1, fmul(2.0f, fmul(pv, sep)));
+                            host_route_add(a, b, h, iq, fmul(2.0f, fmul(pv, fsub(1.0f, sep))));
+                            host_route_add(a, b, h, iq + 1, fmul(2.0f, fmul(pv, sep)));
                         }
                     } else {
                         const double val = dmul((double)A.w, (double)B.w);
@@ -643,13 +644,13 @@ __global__ void __launch_bounds__(256) ac1d_sparse_kernel(const SparseArgs a, co
                             const unsigned long long w = d2u64(dmul(val, a.mult));
                             if (w) shared_add_u64_split(h.dev_lo, h.dev_hi, sc, 2ull * w);
                         } else {
-                            const float fq = floorf(q);
+                            uint32_t iq;
+                            const float fq = floor_small(q, iq);
                             const double sep = (double)fsub(q, fq);
                             const unsigned long long w1 = d2u64(dmul(dmul(val, dsub(1.0, sep)), a.mult));
                             const unsigned long long w2 = d2u64(dmul(dmul(val, sep), a.mult));
-                            if (w1) shared_add_u64_split(h.dev_lo, h.dev_hi, wrap_bin((uint32_t)fq, b.vecsize), 2ull * w1);
-                            if (w2)
-                                shared_add_u64_split(h.dev_lo, h.dev_hi, wrap_bin((uint32_t)fq + 1, b.vecsize), 2ull * w2);
+                            if (w1) shared_add_u64_split(h.dev_lo, h.dev_hi, wrap_bin(iq, b.vecsize), 2ull * w1);
+                            if (w2) shared_add_u64_split(h.dev_lo, h.dev_hi, wrap_bin(iq + 1, b.vecsize), 2ull * w2);
                         }
                     }
                 }
