@@ -248,6 +248,18 @@ iac_status iac_cq_small(iac_ctx *ctx, const float *d_intensity, const float *d_k
                         uint64_t npix, uint32_t fast_size, const iac_mesh_shape *small_shape,
                         int interp, double multiplicator, uint64_t *d_mesh, void *stream);
 
+/* One share of iac_cq_small for a run on several GPUs (the reference runs the
+ * kernel of IAC/kernel.cl:27-184 on one device): the unordered tile pairs are
+ * dealt round-robin over `nparts` shares and this call bins share `part` into
+ * d_mesh (accumulated).  The shares' meshes summed (one integer reduction,
+ * e.g. an NCCL sum of the uint64 meshes) equal iac_cq_small bit for bit, for
+ * any nparts; dealing the tile pairs round-robin spreads near and far (culled)
+ * pairs evenly.  part < nparts.  Asynchronous. */
+iac_status iac_cq_small_part(iac_ctx *ctx, const float *d_intensity, const float *d_kmap,
+                             uint64_t npix, uint32_t fast_size, const iac_mesh_shape *small_shape,
+                             int interp, double multiplicator, uint32_t part, uint32_t nparts,
+                             uint64_t *d_mesh, void *stream);
+
 /* The work items `ind` = d_rows[0 .. nrows) of AutoCorr_CQ_small
  * (IAC/kernel.cl:27-184): for each listed pixel ind and every pixel i, the
  * ordered pair (ind, i) binned exactly as that work item does, accumulated into
@@ -289,6 +301,14 @@ iac_status iac_ac1d_cq_multiplicator(const float *h_intensity, uint64_t npix, do
 iac_status iac_ac1d_cq(iac_ctx *ctx, const float *d_intensity, const float *d_kmap,
                        uint64_t npix, const iac_ac1d_shape *shape, int interp,
                        double multiplicator, uint64_t *d_hist, void *stream);
+
+/* One share of iac_ac1d_cq (kernel AutoCorr_CQ_AV, IAC/kernel.cl:656-764) for
+ * a run on several GPUs, dealt as iac_cq_small_part deals its tile pairs; the
+ * shares' histograms summed equal iac_ac1d_cq bit for bit.  Asynchronous. */
+iac_status iac_ac1d_cq_part(iac_ctx *ctx, const float *d_intensity, const float *d_kmap,
+                            uint64_t npix, const iac_ac1d_shape *shape, int interp,
+                            double multiplicator, uint32_t part, uint32_t nparts, uint64_t *d_hist,
+                            void *stream);
 
 /* The work items `ind` = d_rows[0 .. nrows) of AutoCorr_CQ_AV
  * (IAC/kernel.cl:656-764) into d_hist (uint64[shape.size], accumulated), each

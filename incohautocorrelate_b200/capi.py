@@ -132,10 +132,12 @@ def _declare(lib):
     D = C.c_double
     fn("iac_cq_small_multiplicator", [_VP, _U64, C.POINTER(D)])
     fn("iac_cq_small", [_VP, _VP, _VP, _U64, _U32, C.POINTER(MeshShape), C.c_int, D, _VP, _VP])
+    fn("iac_cq_small_part", [_VP, _VP, _VP, _U64, _U32, C.POINTER(MeshShape), C.c_int, D, _U32, _U32, _VP, _VP])
     fn("iac_cq_merge_weights", [_VP, _VP, _U32, _VP, _U64, _VP, C.POINTER(D)])
     fn("iac_cq_merge", [_VP, _VP, _VP, _U32, C.POINTER(MeshShape), C.c_int, D, _VP, _VP])
     fn("iac_ac1d_cq_multiplicator", [_VP, _U64, C.POINTER(D)])
     fn("iac_ac1d_cq", [_VP, _VP, _VP, _U64, C.POINTER(AC1DShape), C.c_int, D, _VP, _VP])
+    fn("iac_ac1d_cq_part", [_VP, _VP, _VP, _U64, C.POINTER(AC1DShape), C.c_int, D, _U32, _U32, _VP, _VP])
     fn("iac_ac1d_vecsize", [C.c_float, C.c_float], _U32)
     fn("iac_cq_small_rows", [_VP, _VP, _VP, _U64, _VP, _U32, C.POINTER(MeshShape), C.c_int, D, _VP, _VP])
     fn("iac_ac1d_cq_rows", [_VP, _VP, _VP, _U64, _VP, _U32, C.POINTER(AC1DShape), C.c_int, D, _VP, _VP])
@@ -369,10 +371,17 @@ class Context:
         return {"tile_pairs": t.tile_pairs, "block_threads": t.block_threads,
                 "ctas_per_sm": t.ctas_per_sm, "cache_hints": t.cache_hints}
 
-    def cq_small(self, d_I, d_kmap, npix, shape, interp, mult, d_mesh, stream=None, fast_size=0):
-        check(lib().iac_cq_small(self._h, _ptr(d_I), _ptr(d_kmap), int(npix), int(fast_size),
-                                 C.byref(shape), int(interp), float(mult), _ptr(d_mesh),
-                                 _ptr(stream)))
+    def cq_small(self, d_I, d_kmap, npix, shape, interp, mult, d_mesh, stream=None, fast_size=0,
+                 part=0, nparts=1):
+        """iac_cq_small, or with nparts > 1 its share `part` (iac_cq_small_part)."""
+        if nparts == 1 and part == 0:
+            check(lib().iac_cq_small(self._h, _ptr(d_I), _ptr(d_kmap), int(npix), int(fast_size),
+                                     C.byref(shape), int(interp), float(mult), _ptr(d_mesh),
+                                     _ptr(stream)))
+        else:
+            check(lib().iac_cq_small_part(self._h, _ptr(d_I), _ptr(d_kmap), int(npix), int(fast_size),
+                                          C.byref(shape), int(interp), float(mult), int(part), int(nparts),
+                                          _ptr(d_mesh), _ptr(stream)))
 
     def cq_small_rows(self, d_I, d_kmap, npix, d_rows, nrows, shape, interp, mult, d_mesh, stream=None):
         check(lib().iac_cq_small_rows(self._h, _ptr(d_I), _ptr(d_kmap), int(npix), _ptr(d_rows), int(nrows),
@@ -386,9 +395,15 @@ class Context:
         check(lib().iac_cq_merge(self._h, _ptr(d_small), _ptr(d_rw), int(nframes), C.byref(shape),
                                  int(interp), float(mult), _ptr(d_big), _ptr(stream)))
 
-    def ac1d_cq(self, d_I, d_kmap, npix, shape, interp, mult, d_hist, stream=None):
-        check(lib().iac_ac1d_cq(self._h, _ptr(d_I), _ptr(d_kmap), int(npix), C.byref(shape),
-                                int(interp), float(mult), _ptr(d_hist), _ptr(stream)))
+    def ac1d_cq(self, d_I, d_kmap, npix, shape, interp, mult, d_hist, stream=None, part=0, nparts=1):
+        """iac_ac1d_cq, or with nparts > 1 its share `part` (iac_ac1d_cq_part)."""
+        if nparts == 1 and part == 0:
+            check(lib().iac_ac1d_cq(self._h, _ptr(d_I), _ptr(d_kmap), int(npix), C.byref(shape),
+                                    int(interp), float(mult), _ptr(d_hist), _ptr(stream)))
+        else:
+            check(lib().iac_ac1d_cq_part(self._h, _ptr(d_I), _ptr(d_kmap), int(npix), C.byref(shape),
+                                         int(interp), float(mult), int(part), int(nparts), _ptr(d_hist),
+                                         _ptr(stream)))
 
     def ac1d_sparse_batch(self, d_photons, d_offsets, nframes, max_q, dqdx, interp, mult, d_hist,
                           stream=None):

@@ -52,6 +52,7 @@ struct DenseArgs {
     uint64_t npix;
     uint32_t ntiles;
     unsigned long long npairs;  // tile pairs
+    uint32_t part, nparts;      // this launch takes the tile pairs p with p % nparts == part
     uint32_t nx, ny, ptx;       // 2D patch tiling: row length, rows, patches per row (nx = 0: linear)
     uint32_t mult_int;          // Multiplicator as an integer below 2^29, else 0
     int key_ok;                 // |round(q * Voxel_per_dq)| < 512 for every pair within MaxQ
@@ -538,7 +539,7 @@ __global__ void __launch_bounds__(DTILE, 5) cq_small_kernel(const DenseArgs a)
     for (;;) {
         if (threadIdx.x == 0) s_pair = atomicAdd(a.queue, 1ull);
         __syncthreads();
-        const unsigned long long p = s_pair;
+        const unsigned long long p = s_pair * a.nparts + a.part;
         if (p >= a.npairs) break;
         uint32_t P, Q;
         decode_tile_pair(p, T, P, Q);
@@ -684,7 +685,7 @@ __global__ void __launch_bounds__(DTILE) ac1d_cq_kernel(const DenseArgs a)
     for (;;) {
         if (threadIdx.x == 0) s_pair = atomicAdd(a.queue, 1ull);
         __syncthreads();
-        const unsigned long long p = s_pair;
+        const unsigned long long p = s_pair * a.nparts + a.part;
         if (p >= a.npairs) break;
         uint32_t P, Q;
         decode_tile_pair(p, T, P, Q);
@@ -941,6 +942,8 @@ static iac_status prepare(iac_ctx *ctx, void *stream, const float *d_I, const fl
         a.ntiles = (uint32_t)((npix + DTILE - 1) / DTILE);
     }
     a.npairs = (unsigned long long)a.ntiles * (a.ntiles + 1) / 2;
+    a.part = 0;
+    a.nparts = 1;
     a.counters = ctx->d_counters;
     void *scr = nullptr;
     const size_t box_bytes = sizeof(float4) * 2 * (size_t)a.ntiles;
@@ -966,8 +969,16 @@ iac_status iac_cq_small(iac_ctx *ctx, const float *d_I, const float *d_kmap, uin
                         uint32_t fast_size, const iac_mesh_shape *sh, int interp, double mult,
                         uint64_t *d_mesh, void *stream)
 {
+    return iac_cq_small_part(ctx, d_I, d_kmap, npix, fast_size, sh, interp, mult, 0, 1, d_mesh, stream);
+}
+
+iac_status iac_cq_small_part(iac_ctx *ctx, const float *d_I, const float *d_kmap, uint64_t npix,
+                             uint32_t fast_size, const iac_mesh_shape *sh, int interp, double mult,
+                             uint32_t part, uint32_t nparts, uint64_t *d_mesh, void *stream)
+{
     IAC_TRACE();
     IAC_REQUIRE(ctx && d_I && d_kmap && sh && d_mesh, "iac_cq_small: NULL argument");
+    IAC_REQUIRE(nparts >= 1 && part < nparts, "iac_cq_small_part: part %u of %u", part, nparts);
     IAC_REQUIRE(interp == 0 || interp == 1, "interpolation must be 0 or 1");
     IAC_REQUIRE(npix > 0 && npix < (1ull << 32), "iac_cq_small: pixel count %llu out of range",
                 (unsigned long long)npix);
@@ -979,6 +990,8 @@ iac_status iac_cq_small(iac_ctx *ctx, const float *d_I, const float *d_kmap, uin
     DenseArgs a{};
     iac_status st = prepare(ctx, stream, d_I, d_kmap, npix, fast_size, mult, a);
     if (st != IAC_OK) return st;
+    a.part = part;
+    a.nparts = nparts;
     a.out = (unsigned long long *)d_mesh;
     a.maxq = sh->max_q;
     a.maxq2 = sqrt_threshold(sh->max_q);
@@ -1029,8 +1042,16 @@ iac_status iac_ac1d_cq(iac_ctx *ctx, const float *d_I, const float *d_kmap, uint
                        const iac_ac1d_shape *sh, int interp, double mult, uint64_t *d_hist,
                        void *stream)
 {
+    return iac_ac1d_cq_part(ctx, d_I, d_kmap, npix, sh, interp, mult, 0, 1, d_hist, stream);
+}
+
+iac_status iac_ac1d_cq_part(iac_ctx *ctx, const float *d_I, const float *d_kmap, uint64_t npix,
+                            const iac_ac1d_shape *sh, int interp, double mult, uint32_t part, uint32_t nparts,
+                            uint64_t *d_hist, void *stream)
+{
     IAC_TRACE();
     IAC_REQUIRE(ctx && d_I && d_kmap && sh && d_hist, "iac_ac1d_cq: NULL argument");
+    IAC_REQUIRE(nparts >= 1 && part < nparts, "iac_ac1d_cq_part: part %u of %u", part, nparts);
     IAC_REQUIRE(interp == 0 || interp == 1, "interpolation must be 0 or 1");
     IAC_REQUIRE(npix > 0 && npix < (1ull << 32), "iac_ac1d_cq: pixel count out of range");
     IAC_REQUIRE(sh->size >= 3 && sh->size <= 24576, "AC1D size %u out of range [3, 24576]", sh->size);
@@ -1044,6 +1065,8 @@ iac_status iac_ac1d_cq(iac_ctx *ctx, const float *d_I, const float *d_kmap, uint
     // a warp's shared-memory histogram atomics would collide on them
     iac_status st = prepare(ctx, stream, d_I, d_kmap, npix, 0, mult, a);
     if (st != IAC_OK) return st;
+    a.part = part;
+    a.nparts = nparts;
     a.out = (unsigned long long *)d_hist;
     a.maxq = sh->max_q;
     a.maxq2 = sqrt_threshold(sh->max_q);

@@ -117,6 +117,46 @@ def test_cq_small_dense_detector_region(ctx, oracle_lib):
 
 
 @pytest.mark.parametrize("interp", [0, 1])
+def test_dense_shares_sum_to_the_whole(ctx, oracle_lib, rng, interp):
+    """iac_cq_small_part / iac_ac1d_cq_part (the per-GPU shares of a run on
+    several GPUs): for 2, 3 and 7 shares the shares' meshes and histograms sum
+    to the single-launch result bit for bit, which is the oracle's."""
+    import torch
+    from incohautocorrelate_b200 import capi
+    o = oracle_lib
+    pm, km, mq = small_detector(48, 80, 6e-4)
+    npix = km.size // 3
+    I = _intensity(npix, rng)
+    s = o.small_cq_mesh_shape(mq, 31)
+    mult = capi.cq_small_multiplicator(I)
+    want = _oracle_cq_small(o, I, km, s, interp, mult)
+    dI, dk = _dev(I), _dev(km)
+    for fast in (0, 80):
+        for nparts in (2, 3, 7):
+            total = _zeros(want.size)
+            for part in range(nparts):
+                share = _zeros(want.size)
+                ctx.cq_small(dI, dk, npix, to_capi_shape(s), interp, mult, share, fast_size=fast, part=part,
+                             nparts=nparts)
+                total += share
+            assert ctx.check() == 0
+            np.testing.assert_array_equal(_u64(total), want)
+    sa = capi.ac1d_shape(mq, 97)
+    m1 = capi.ac1d_cq_multiplicator(I)
+    whole = _zeros(sa.size)
+    ctx.ac1d_cq(dI, dk, npix, sa, interp, m1, whole)
+    for nparts in (2, 3, 7):
+        total = _zeros(sa.size)
+        for part in range(nparts):
+            ctx.ac1d_cq(dI, dk, npix, sa, interp, m1, total, part=part, nparts=nparts)
+        assert ctx.check() == 0
+        np.testing.assert_array_equal(_u64(total), _u64(whole))
+    with pytest.raises(capi.IacError) as e:
+        ctx.cq_small(dI, dk, npix, to_capi_shape(s), interp, mult, total, part=3, nparts=3)
+    assert e.value.status == capi.IAC_ERR_INVALID_ARG
+
+
+@pytest.mark.parametrize("interp", [0, 1])
 def test_cq_merge_bit_exact(ctx, oracle_lib, rng, interp):
     from incohautocorrelate_b200 import capi, workloads as W
     o = oracle_lib

@@ -70,6 +70,50 @@ def test_two_rank_gloo_reduction_is_bit_exact(tmp_path, oracle_lib, scaling):
     np.testing.assert_array_equal(np.load(tmp_path / "reduced.npy"), want)
 
 
+def _dense_rank_main(rank, world, port, out_dir):
+    """A rank of a sharded dense C(q): its share of the pixel pairs binned into
+    its own uint64 small mesh (the oracle's work items [r0, r1) stand in for
+    the device kernel's tile-pair share), then the one integer reduction."""
+    import torch
+    import torch.distributed as dist
+
+    import oracle
+    from incohautocorrelate_b200 import shard, workloads as W
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        I = W.radial_mean_intensity(24, 32, 9.0, 0.02, 0.05, seed=3)
+        km, mq = oracle.calc_kmap(W.flat_pixel_map(24, 32, pitch=8 * 75e-6))
+        s = oracle.small_cq_mesh_shape(mq, 31)
+        npix = I.size
+        r0, r1 = npix * rank // world, npix * (rank + 1) // world
+        m = np.zeros(s.size_ab * s.size_ab * s.size_c, np.uint64)
+        oracle.lib().iaco_cq_small(oracle.p(I), oracle.p(km), npix, s, 0, 1e5, r0, r1, oracle.p(m))
+        t = torch.from_numpy(m.view(np.int64).copy())
+        shard.reduce_mesh(t, dst=0)
+        if rank == 0:
+            np.save(os.path.join(out_dir, "dense.npy"), t.numpy().view(np.uint64))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_gloo_dense_reduction_is_bit_exact(tmp_path, oracle_lib):
+    import torch.multiprocessing as mp
+
+    from incohautocorrelate_b200 import workloads as W
+    mp.start_processes(_dense_rank_main, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    I = W.radial_mean_intensity(24, 32, 9.0, 0.02, 0.05, seed=3)
+    km, mq = oracle_lib.calc_kmap(W.flat_pixel_map(24, 32, pitch=8 * 75e-6))
+    s = oracle_lib.small_cq_mesh_shape(mq, 31)
+    want = np.zeros(s.size_ab * s.size_ab * s.size_c, np.uint64)
+    oracle_lib.lib().iaco_cq_small(oracle_lib.p(I), oracle_lib.p(km), I.size, s, 0, 1e5, 0, I.size,
+                                   oracle_lib.p(want))
+    assert want.sum() > 0
+    np.testing.assert_array_equal(np.load(tmp_path / "dense.npy"), want)
+
+
 def test_balanced_ranges_cover_all_frames():
     from incohautocorrelate_b200 import shard, workloads as W
     cfg = W.rotated_config(nframes=5000, seed=3)
