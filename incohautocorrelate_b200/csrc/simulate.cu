@@ -44,6 +44,17 @@ constexpr float TWO_PI_HI = (float)TWO_PI_D;
 constexpr float TWO_PI_LO = (float)(TWO_PI_D - (double)TWO_PI_HI);
 constexpr float INV_TWO_PI = (float)(1.0 / TWO_PI_D);
 
+// the whole number of turns in a phase, rintf(arg / 2 pi) with ties to even, by
+// two FP32 adds on the FMA pipe: x + 1.5 * 2^23 rounds x to an integer in the
+// float's last place for |x| < 2^22 (phases below 2.6e7 rad; past that an FP32
+// phase has lost every fraction of a turn anyway).  rintf is a conversion-unit
+// instruction, and that unit also runs the two MUFU operations of every term,
+// which bound the simulator.
+__device__ __forceinline__ float phase_turns(float arg)
+{
+    return fsub(fadd(fmul(arg, INV_TWO_PI), ROUND_MAGIC), ROUND_MAGIC);
+}
+
 struct CrystalArgs {
     const double *__restrict__ atoms;  // 3 doubles per atom
     uint32_t natoms, nframes, nmodes;
@@ -232,7 +243,7 @@ __global__ void __launch_bounds__(SIM_THREADS) simulate_kernel(const SimArgs a)
                     if (a.accurate) {
                         sincosf(arg, &s, &c);
                     } else {
-                        const float kk = rintf(arg * INV_TWO_PI);
+                        const float kk = phase_turns(arg);
                         const float r = fmaf(-kk, TWO_PI_LO, fmaf(-kk, TWO_PI_HI, arg));
                         __sincosf(r, &s, &c);
                     }
@@ -291,7 +302,7 @@ __global__ void __launch_bounds__(SIM_THREADS) simulate_chunked_kernel(const Sim
                         if (a.accurate) {
                             sincosf(arg, &sn, &cs);
                         } else {
-                            const float kk = rintf(arg * INV_TWO_PI);
+                            const float kk = phase_turns(arg);
                             const float r = fmaf(-kk, TWO_PI_LO, fmaf(-kk, TWO_PI_HI, arg));
                             __sincosf(r, &sn, &cs);
                         }
