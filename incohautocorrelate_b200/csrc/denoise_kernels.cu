@@ -2082,6 +2082,18 @@ static bool launch_zcat(const ConvArgs &a, const TmaGeom &g0, uint32_t budget, c
                 S = st;
             }
         }
+        if (per_sm == 0) {
+            // wide rows (48 or 96 input channels with W >= 64): one CTA per SM
+            // with the stages that fit, at least one per issuer; every stage
+            // holds one input plane whose MMAs release it, so the pipeline only
+            // runs shallower (the other kernels are several times slower here)
+            const int st = g.wres_bytes < budget ? (int)std::min<uint32_t>(8u, (budget - g.wres_bytes) / g.stage_bytes)
+                                                 : 0;
+            if (st >= 2 && st >= Z::NISS) {
+                per_sm = 1;
+                S = st;
+            }
+        }
         if (per_sm == 0) return false;
         g.S = S;
         const long long grid_max = ((long long)per_sm * std::max(1, a.sms) + NG - 1) / NG;  // per channel group

@@ -64,6 +64,31 @@ def test_conv3x3_matches_oracle(ctx, rng, backend, c0, up0, c1, cout, dims):
     np.testing.assert_allclose(got, want, rtol=8e-3, atol=1e-5 * scale)
 
 
+@pytest.mark.parametrize("c1,cout,W", [(48, 16, 128), (96, 32, 64), (16, 48, 128), (32, 96, 64)])
+def test_conv3x3_wide_rows_match_oracle(ctx, rng, c1, cout, W):
+    """The decoder layers at the row widths of whole-mesh inference (128^3:
+    48 -> 16 on rows of 128, 96 -> 32 on rows of 64, and their data-gradient
+    shapes), where the dz-concatenated kernel runs one CTA per SM with the
+    stages that fit beside its weights."""
+    import torch
+    from incohautocorrelate_b200 import capi
+    from oracle import denoise_oracle as O
+    nb, D, H = 1, 5, 3
+    s1_q, s1 = _bf16(rng.normal(0, 1, (nb, D, H, W, c1)))
+    w = rng.normal(0, (2.0 / (27 * c1)) ** 0.5, (cout, 27, c1)).astype(np.float32)
+    wt_q, wq = _bf16(capi.conv_weight_tiles(w))
+    w64 = wq.reshape(27, c1 // 8, cout, 8).transpose(2, 0, 1, 3).reshape(cout, 27, c1)
+    b = rng.normal(0, 0.1, cout).astype(np.float32)
+    want = O.conv_layer(None, s1, w64, b.astype(np.float64), True, 0)
+    y = torch.zeros((nb, D, H, W, cout), dtype=torch.int16, device="cuda")
+    capi.denoise_conv3x3(ctx, 0, None, 0, 0, s1_q, c1, wt_q, torch.from_numpy(b).cuda(), cout, 1, nb, D, H, W, y)
+    torch.cuda.synchronize()
+    assert ctx.check() == 0
+    got = _from_bf16(y)
+    scale = np.abs(want).max()
+    np.testing.assert_allclose(got, want, rtol=8e-3, atol=1e-5 * scale)
+
+
 @pytest.mark.parametrize("slabs", [3, 2, 1, 0], ids=["tcgen05_dz_stacked", "tcgen05", "slabs", "per_tap"])
 @pytest.mark.parametrize("c0,up0,c1,cout", [(0, 0, 16, 16), (0, 0, 16, 32), (0, 0, 32, 32), (0, 0, 32, 64),
                                             (0, 0, 64, 64), (64, 1, 32, 32), (32, 1, 16, 16), (0, 0, 48, 16),
