@@ -438,15 +438,15 @@ __device__ __forceinline__ int2 f2round_half_away(float2 x)
     return make_int2(__float2int_rz(t.x), __float2int_rz(t.y));
 }
 
-// floor(p * M) for 0 <= p < 2^23 and an integer M < 2^29: p = m * 2^(e - 150)
-// with e >= 1 gives (m * M) >> (150 - e), a shift of at least one bit; the
-// product is below 2^53, so shifts past 63 (p below 2^-87, or p = 0 with its
-// implicit bit forced on) give 0
+// floor(p * M) for 0 <= p < 2^23 and an integer M < 2^29: p's 24-bit
+// significand times M is below 2^53, so the double product is exact and its
+// truncation is the floor.  One multiply on the (otherwise idle) FP64 pipe and
+// two conversions take fewer issue slots than the integer form (significand
+// product shifted by the exponent), which measured 1.025 s against 0.864 s at
+// 1024^2 with the run flush below.
 __device__ __forceinline__ unsigned long long scaled_floor_small(float p, uint32_t M)
 {
-    const uint32_t b = __float_as_uint(p);
-    const unsigned long long prod = (unsigned long long)((b & 0x7fffffu) | 0x800000u) * M;
-    return prod >> min(150 - (int)(b >> 23), 63);
+    return __double2ull_rz(__dmul_rn((double)p, (double)M));
 }
 
 // one pair of the packed window path: a pair that fails the intensity or
@@ -461,7 +461,7 @@ __device__ __forceinline__ void win_step(const DenseArgs &a, uint32_t *win, int 
     const int k = ok ? key : cur;
     const unsigned long long v = scaled_floor_small(ok ? pv : 0.0f, a.mult_int);
     const bool brk = k != cur;
-    if (brk && acc) shared_add_u64_split(win, win + WINDOW_WORDS, (uint32_t)cur, acc);
+    if (brk) shared_add_u64_split(win, win + WINDOW_WORDS, (uint32_t)cur, acc);  // acc may be 0: adds nothing
     acc = (brk ? 0ull : acc) + v;
     cur = k;
 }
