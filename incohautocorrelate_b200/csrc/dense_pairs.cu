@@ -725,9 +725,11 @@ __global__ void __launch_bounds__(DTILE) ac1d_cq_kernel(const DenseArgs a)
                 if (q > a.maxq) continue;
                 q = __fdiv_rn(q, a.dq);
                 if (INTERP == 0) {
-                    // sc = (uint)floor(q + 0.5) with q + 0.5 in double; for q < 2^22
-                    // the float sum is exact and gives the same bin
-                    const uint32_t sc = wrap_bin((uint32_t)floorf(fadd(q, 0.5f)), a.hsize);
+                    // sc = (uint)floor(q + 0.5) with q + 0.5 in double: floor(fl(q +
+                    // 0.49999997f)) equals it for every float 0 <= q < 2^23 (the
+                    // identity of round_half_away); fl(q + 0.5f) does not at
+                    // q = 0.5 - 2^-25, whose sum rounds up to 1
+                    const uint32_t sc = wrap_bin((uint32_t)floorf(fadd(q, 0.49999997f)), a.hsize);
                     const unsigned long long v =
                         a.mult_int ? scaled_floor(pv, a.mult_int) : (unsigned long long)(long long)dmul(val, a.mult);
                     shared_add_u64_split(hlo, hhi, sc, 2ull * v);

@@ -3,6 +3,7 @@ round() (half away from zero), checked exhaustively over every float they are
 applied to:
 
 * round_half_away (dense C(q) kernels): trunc(fl(x + copysign(0.49999997, x)));
+  the AC1D C(q) kernel's nearest bin floor(q + 1/2) is floor(fl(q + 0.49999997));
 * round_away_rz_i / round_away_rz_f (photon-pair kernel): fl(|x| + 0.49999997)
   followed by a round-toward-zero add of 2^23, i.e. floor of that sum.
 
@@ -34,3 +35,14 @@ def test_round_toward_zero_add_is_floor():
         y = np.float32(2.0 ** e) * np.linspace(1, 2, 4097, dtype=np.float32)[:-1]
         s = y.astype(np.float64) + 2.0 ** 23
         assert np.all(np.floor(s) - 2.0 ** 23 == np.floor(y.astype(np.float64)))
+
+
+def test_plain_half_add_misrounds_just_below_one_half():
+    # why the kernels add 0.49999997f and not 0.5f before a floor: for the
+    # largest float below 1/2 the float sum q + 0.5f is a tie between 1 - 2^-24
+    # and 1, rounds to the even 1, and floor gives 1 where floor(q + 1/2) is 0
+    q = np.float32(0.5) - np.float32(2.0 ** -25)
+    assert q < np.float32(0.5)
+    assert np.floor(q + np.float32(0.5)) == 1.0
+    assert np.floor(np.float64(q) + 0.5) == 0.0
+    assert np.floor(q + HALF_BELOW) == 0.0
