@@ -492,6 +492,15 @@ iac_status iac_denoise_init_params(iac_denoiser *dn, uint64_t seed);
 iac_status iac_denoise_set_params(iac_denoiser *dn, const float *h_params);
 iac_status iac_denoise_get_params(iac_denoiser *dn, float *h_params);
 iac_status iac_denoise_get_grads(iac_denoiser *dn, float *h_grads);
+/* The device gradient vector itself (float[*count], the layout of
+ * iac_denoise_get_params), which iac_denoise_backward writes and
+ * iac_denoise_adamw_step reads, for data-parallel training on several GPUs:
+ * between the two calls every rank sums the vector across ranks in place (an
+ * NCCL all-reduce) and scales it by 1 / ranks, so that all replicas take the
+ * same optimizer step on the mean gradient.  The pointer stays valid until
+ * iac_denoise_destroy.  No counterpart in the reference (its output of record
+ * is the plain mesh). */
+iac_status iac_denoise_grad_buffer(iac_denoiser *dn, float **d_grads, uint64_t *count);
 /* Training state for checkpoint/resume (no counterpart in the reference): the
  * AdamW moments (nparams floats each) and step count; set_state restores the
  * parameters, moments and step together (set_params resets the moments). */

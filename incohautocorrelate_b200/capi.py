@@ -161,6 +161,7 @@ def _declare(lib):
     fn("iac_denoise_set_params", [_VP, _VP])
     fn("iac_denoise_get_params", [_VP, _VP])
     fn("iac_denoise_get_grads", [_VP, _VP])
+    fn("iac_denoise_grad_buffer", [_VP, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)])
     fn("iac_denoise_get_state", [_VP, _VP, _VP, C.POINTER(_U64)])
     fn("iac_denoise_set_state", [_VP, _VP, _VP, _VP, _U64])
     fn("iac_denoise_forward", [_VP, _VP, _U32, _U32, _U32, _U32, _VP, _VP])
@@ -517,6 +518,19 @@ class Denoiser:
         g = np.zeros(self.nparams, np.float32)
         check(lib().iac_denoise_get_grads(self._h, g.ctypes.data))
         return g
+
+    def grad_tensor(self):
+        """The device gradient vector as a float32 torch tensor sharing its
+        memory (iac_denoise_grad_buffer): written by backward, read by
+        adamw_step; a data-parallel step all-reduces it in place."""
+        import torch
+        p, n = C.c_void_p(), C.c_uint64()
+        check(lib().iac_denoise_grad_buffer(self._h, C.byref(p), C.byref(n)))
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (int(n.value),), "typestr": "<f4",
+                                        "data": (int(p.value), False), "version": 2}
+        return torch.as_tensor(_View(), device="cuda")
 
     def get_state(self):
         """(parameters, AdamW first moments, second moments, optimizer steps)."""

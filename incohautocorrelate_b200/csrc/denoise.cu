@@ -579,6 +579,14 @@ iac_status iac_denoise_get_grads(iac_denoiser *dn, float *h_grads)
     return IAC_OK;
 }
 
+iac_status iac_denoise_grad_buffer(iac_denoiser *dn, float **d_grads, uint64_t *count)
+{
+    IAC_REQUIRE(dn && d_grads && count, "null argument");
+    *d_grads = dn->g;
+    *count = (uint64_t)dn->nparams;
+    return IAC_OK;
+}
+
 iac_status iac_denoise_forward(iac_denoiser *dn, const float *d_in, uint32_t nb, uint32_t D, uint32_t H,
                                uint32_t W, float *d_out, void *stream)
 {

@@ -254,6 +254,31 @@ def train(ctx, xin, tgt, cfg: TrainConfig, log=print, dn=None):
     return dn, hist, ms_step
 
 
+def data_parallel_step(dn, d_x, d_t, nb, D, H, W, lr, beta1=0.9, beta2=0.999, eps=1e-8, weight_decay=1e-4):
+    """One data-parallel training step on several GPUs: every rank (one process
+    per GPU, its own `Denoiser` with the same parameters) computes the
+    gradients of its own nb patches, the ranks average the gradient vector in
+    place (one all-reduce of iac_denoise_grad_buffer), and every rank then takes
+    the same AdamW step, so the replicas stay identical.  With equal local
+    batches the mean of the local mean-loss gradients is the gradient of the
+    global batch's mean loss.  Returns the global mean loss.  Without an
+    initialised process group (or with one rank) this is backward + adamw_step."""
+    import torch
+    import torch.distributed as dist
+    loss = dn.backward(d_x, d_t, nb, D, H, W)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        world = dist.get_world_size()
+        g = dn.grad_tensor()
+        dist.all_reduce(g, op=dist.ReduceOp.SUM)
+        g.div_(world)
+        t = torch.tensor([loss], dtype=torch.float64, device=g.device)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        loss = float(t.item()) / world
+        torch.cuda.synchronize()  # the reduced gradients are in place before the optimizer reads them
+    dn.adamw_step(lr, beta1, beta2, eps, weight_decay)
+    return loss
+
+
 def denoise_volume(dn, d_x, d_out, E):
     dn.forward(d_x, 1, E, E, E, d_out)
 

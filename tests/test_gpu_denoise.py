@@ -346,3 +346,48 @@ def test_graph_replayed_training_matches_eager_steps(ctx, rng):
     assert np.isfinite(losses.cpu().numpy()).all()
     eager.close()
     graph.close()
+
+
+def test_gradient_buffer_feeds_the_optimizer(ctx, rng):
+    """iac_denoise_grad_buffer (the in-place all-reduce target of data-parallel
+    training): its view holds the gradients iac_denoise_get_grads copies out,
+    and what is written into it is what AdamW uses -- zeroed gradients leave
+    only the weight decay, w <- w - lr wd w on the weights (biases keep their
+    values) -- while data_parallel_step on
+    one process is backward + AdamW."""
+    import torch
+    from incohautocorrelate_b200 import capi, denoise
+    dn = capi.Denoiser(ctx, 1, 8, 8, 8)
+    try:
+        dn.init_params(3)
+        x = torch.from_numpy(rng.gamma(2.0, 0.5, (1, 8, 8, 8)).astype(np.float32)).cuda()
+        t = (x * 1.1).contiguous()
+        dn.backward(x, t, 1, 8, 8, 8)
+        g = dn.grad_tensor()
+        assert g.numel() == dn.nparams
+        np.testing.assert_array_equal(g.cpu().numpy(), dn.get_grads())
+        assert float(g.abs().sum()) > 0
+        p0 = dn.get_params()
+        g.zero_()
+        lr, wd = 1e-2, 1e-1
+        dn.adamw_step(lr, weight_decay=wd)
+        from oracle import denoise_oracle as O
+        is_w = []
+        for ci, co in O.SPECS:
+            is_w += [True] * (co * 27 * ci) + [False] * co
+        is_w = np.array(is_w + [True] * 16 + [False])  # the head's 16 weights and its bias
+        assert is_w.size == p0.size
+        want = np.where(is_w, p0 - np.float32(lr) * (np.float32(wd) * p0), p0)
+        np.testing.assert_allclose(dn.get_params(), want, rtol=1e-6, atol=1e-9)
+        # one process: the data-parallel step is backward + AdamW, bit for bit
+        dn.set_params(p0)
+        loss = denoise.data_parallel_step(dn, x, t, 1, 8, 8, 8, 1e-3)
+        p1 = dn.get_params()
+        dn.set_params(p0)
+        loss2 = dn.backward(x, t, 1, 8, 8, 8)
+        dn.adamw_step(1e-3)
+        assert loss == loss2
+        np.testing.assert_array_equal(dn.get_params(), p1)
+    finally:
+        dn.close()
+

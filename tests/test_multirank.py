@@ -114,6 +114,63 @@ def test_two_rank_gloo_dense_reduction_is_bit_exact(tmp_path, oracle_lib):
     np.testing.assert_array_equal(np.load(tmp_path / "dense.npy"), want)
 
 
+def _dp_inputs():
+    from oracle import denoise_oracle as O
+    rng = np.random.default_rng(11)
+    parts = []
+    for ci, co in O.SPECS:
+        parts += [rng.normal(0, (2.0 / (27 * ci)) ** 0.5, co * 27 * ci), rng.normal(0, 0.05, co)]
+    parts += [rng.normal(0, 0.3, 16), [0.0]]
+    params = np.concatenate(parts)
+    x = rng.gamma(2.0, 0.5, (2, 8, 8, 8))
+    return params, x, x * 1.1 + rng.normal(0, 0.05, x.shape)
+
+
+def _dp_rank_main(rank, world, port, out_dir):
+    """A rank of data-parallel denoiser training: the gradient of its own
+    volume's mean loss (the float64 oracle stands in for the device backward),
+    summed over ranks in place and divided by the rank count, as
+    denoise.data_parallel_step does with the device gradient buffer."""
+    import torch
+    import torch.distributed as dist
+
+    from oracle import denoise_oracle as O
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        params, x, t = _dp_inputs()
+        loss, g, _ = O.loss_and_grads(params, x[rank:rank + 1], t[rank:rank + 1])
+        gt = torch.from_numpy(np.asarray(g, np.float64).copy())
+        dist.all_reduce(gt, op=dist.ReduceOp.SUM)
+        gt.div_(world)
+        lt = torch.tensor([float(loss)], dtype=torch.float64)
+        dist.all_reduce(lt, op=dist.ReduceOp.SUM)
+        if rank == 0:
+            np.save(os.path.join(out_dir, "grad.npy"), gt.numpy())
+            np.save(os.path.join(out_dir, "loss.npy"), lt.numpy() / world)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_gloo_data_parallel_gradient(tmp_path):
+    """The mean of the ranks' local mean-loss gradients is the gradient of the
+    whole batch's mean loss: the identity data-parallel denoiser training
+    relies on (equal local batches)."""
+    import torch.multiprocessing as mp
+
+    from oracle import denoise_oracle as O
+    mp.start_processes(_dp_rank_main, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    params, x, t = _dp_inputs()
+    loss, g, _ = O.loss_and_grads(params, x, t)
+    g = np.asarray(g, np.float64)
+    got = np.load(tmp_path / "grad.npy")
+    assert np.abs(g).max() > 0
+    np.testing.assert_allclose(got, g, rtol=1e-9, atol=1e-12 * np.abs(g).max())
+    np.testing.assert_allclose(np.load(tmp_path / "loss.npy")[0], float(loss), rtol=1e-12)
+
+
 def test_balanced_ranges_cover_all_frames():
     from incohautocorrelate_b200 import shard, workloads as W
     cfg = W.rotated_config(nframes=5000, seed=3)
