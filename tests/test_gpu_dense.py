@@ -156,6 +156,19 @@ def test_dense_shares_sum_to_the_whole(ctx, oracle_lib, rng, interp):
     assert e.value.status == capi.IAC_ERR_INVALID_ARG
 
 
+def test_ac1d_cq_rejects_a_bin_coordinate_past_2_22(ctx, rng):
+    """|q| / dq is floored on the FMA pipe, exact below 2^22: a shape whose
+    MaxQ / dq reaches it is refused before any launch."""
+    from incohautocorrelate_b200 import capi
+    pm, km, mq = small_detector(8, 8, 6e-4)
+    I = _intensity(64, rng)
+    sh = capi.AC1DShape(2048, 1.0, 1.0 / 5e6)
+    out = _zeros(2048)
+    with pytest.raises(capi.IacError) as e:
+        ctx.ac1d_cq(_dev(I), _dev(km), 64, sh, 1, 1e5, out)
+    assert e.value.status == capi.IAC_ERR_INVALID_ARG
+
+
 @pytest.mark.parametrize("interp", [0, 1])
 def test_cq_merge_bit_exact(ctx, oracle_lib, rng, interp):
     from incohautocorrelate_b200 import capi, workloads as W
