@@ -267,7 +267,9 @@ __device__ __forceinline__ int round_away_rz_i(float x)
 // floor of 0 <= q < 2^23 as a float and as an integer on the FMA and integer
 // pipes (no conversion-unit instruction): q +rz 2^23 = 2^23 + floor(q) exactly,
 // and its bits minus those of 2^23 are floor(q).  A NaN q (non-finite
-// k-vectors only) gives an index far past every histogram.
+// k-vectors only) gives a large index: the host-route histogram counts it as
+// out of range, the histograms that wrap their bins (as the reference's
+// sub-histogram fold does) take it modulo their size.
 __device__ __forceinline__ float floor_small(float q, uint32_t &iq)
 {
     const float t = __fadd_rz(q, 8388608.0f);
