@@ -552,6 +552,14 @@ __device__ __forceinline__ void host_route_add(const SparseArgs &a, const AC1DAr
         return;
     }
     if (v == 0.0f) return;
+    if (v > 0.0f && v < 8388608.0f) {  // the usual case, without conversion-unit instructions
+        const float t = __fadd_rz(v, 8388608.0f);  // 2^23 + floor(v)
+        if (fsub(t, 8388608.0f) == v)
+            shared_add_u64_split(h.int_lo, h.int_hi, bin, (unsigned long long)(uint32_t)(__float_as_int(t) - TWO23_BITS));
+        else
+            atomicAdd(&h.frac[bin], (double)v);
+        return;
+    }
     if (v == truncf(v) && v < 1.8e19f)
         shared_add_u64_split(h.int_lo, h.int_hi, bin, (unsigned long long)__float2ull_rz(v));
     else
@@ -629,7 +637,10 @@ __global__ void __launch_bounds__(256) ac1d_sparse_kernel(const SparseArgs a, co
                     if (host) {
                         const float pv = fmul(A.w, B.w);
                         if (INTERP == 0) {
-                            host_route_add(a, b, h, (uint32_t)floor(dadd((double)q, 0.5)), fmul(2.0f, pv));
+                            // (uint)floor(q + 0.5) in double, as floor(fl(q + 0.49999997f)) for q < 2^23
+                            uint32_t iq;
+                            floor_small(fadd(q, 0.49999997f), iq);
+                            host_route_add(a, b, h, iq, fmul(2.0f, pv));
                         } else {
                             uint32_t iq;  // q = |q| / dq <= MaxQ / dq < 2^23
                             const float fq = floor_small(q, iq);
@@ -640,7 +651,9 @@ __global__ void __launch_bounds__(256) ac1d_sparse_kernel(const SparseArgs a, co
                     } else {
                         const double val = dmul((double)A.w, (double)B.w);
                         if (INTERP == 0) {
-                            const uint32_t sc = wrap_bin((uint32_t)floor(dadd((double)q, 0.5)), b.vecsize);
+                            uint32_t iq;  // (uint)floor(q + 0.5), as above
+                            floor_small(fadd(q, 0.49999997f), iq);
+                            const uint32_t sc = wrap_bin(iq, b.vecsize);
                             const unsigned long long w = d2u64(dmul(val, a.mult));
                             if (w) shared_add_u64_split(h.dev_lo, h.dev_hi, sc, 2ull * w);
                         } else {
