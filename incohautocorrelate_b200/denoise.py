@@ -274,7 +274,8 @@ def data_parallel_step(dn, d_x, d_t, nb, D, H, W, lr, beta1=0.9, beta2=0.999, ep
         t = torch.tensor([loss], dtype=torch.float64, device=g.device)
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         loss = float(t.item()) / world
-        torch.cuda.synchronize()  # the reduced gradients are in place before the optimizer reads them
+        if g.is_cuda:
+            torch.cuda.synchronize()  # the reduced gradients are in place before the optimizer reads them
     dn.adamw_step(lr, beta1, beta2, eps, weight_decay)
     return loss
 

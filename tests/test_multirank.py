@@ -153,6 +153,68 @@ def _dp_rank_main(rank, world, port, out_dir):
         dist.destroy_process_group()
 
 
+class _OracleDenoiser:
+    """The calls data_parallel_step makes on a Denoiser, on the CPU: backward
+    puts the float64 oracle's gradient of the local mean loss into a float32
+    tensor (the device gradient buffer's stand-in), adamw_step records the
+    gradient it would apply."""
+
+    def __init__(self, params):
+        import torch
+        self.params = params
+        self.g = torch.zeros(params.size, dtype=torch.float32)
+        self.applied = None
+
+    def backward(self, x, t, nb, D, H, W):
+        import torch
+        from oracle import denoise_oracle as O
+        loss, g, _ = O.loss_and_grads(self.params, x, t)
+        self.g.copy_(torch.from_numpy(np.asarray(g, np.float32)))
+        return float(loss)
+
+    def grad_tensor(self):
+        return self.g
+
+    def adamw_step(self, lr, *args):
+        self.applied = self.g.numpy().copy()
+
+
+def _dp_step_rank_main(rank, world, port, out_dir):
+    import torch.distributed as dist
+
+    from incohautocorrelate_b200 import denoise
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        params, x, t = _dp_inputs()
+        dn = _OracleDenoiser(params)
+        loss = denoise.data_parallel_step(dn, x[rank:rank + 1], t[rank:rank + 1], 1, 8, 8, 8, 1e-3)
+        np.save(os.path.join(out_dir, f"applied{rank}.npy"), dn.applied)
+        np.save(os.path.join(out_dir, f"loss{rank}.npy"), np.array([loss]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_gloo_data_parallel_step(tmp_path):
+    """denoise.data_parallel_step itself on two gloo ranks: both ranks hand the
+    optimizer the same gradient, the whole batch's, and report the whole
+    batch's loss (float32 gradient buffer)."""
+    import torch.multiprocessing as mp
+
+    from oracle import denoise_oracle as O
+    mp.start_processes(_dp_step_rank_main, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    params, x, t = _dp_inputs()
+    loss, g, _ = O.loss_and_grads(params, x, t)
+    g = np.asarray(g, np.float64)
+    a0, a1 = np.load(tmp_path / "applied0.npy"), np.load(tmp_path / "applied1.npy")
+    np.testing.assert_array_equal(a0, a1)
+    np.testing.assert_allclose(a0, g, rtol=1e-5, atol=1e-6 * np.abs(g).max())
+    for r in range(2):
+        np.testing.assert_allclose(np.load(tmp_path / f"loss{r}.npy")[0], float(loss), rtol=1e-12)
+
+
 def test_two_rank_gloo_data_parallel_gradient(tmp_path):
     """The mean of the ranks' local mean-loss gradients is the gradient of the
     whole batch's mean loss: the identity data-parallel denoiser training
