@@ -203,11 +203,15 @@ struct SimArgs {
 constexpr int SIM_THREADS = 128;
 constexpr int SIM_MAX_EM = 1024;  // emitters per (frame, mode) staged in shared memory
 
+// pixels per thread of simulate_kernel: pixels p and p + SIM_THREADS share
+// every emitter load and the loop overhead; each pixel's sums keep their order
+constexpr int SIM_PIX = 2;
+
 __global__ void __launch_bounds__(SIM_THREADS) simulate_kernel(const SimArgs a)
 {
     extern __shared__ float4 s_em[];  // [mode][SIM_MAX_EM window]
     const uint32_t f = blockIdx.y;
-    const uint64_t p = blockIdx.x * (uint64_t)SIM_THREADS + threadIdx.x;
+    const uint64_t p0 = blockIdx.x * (uint64_t)(SIM_PIX * SIM_THREADS) + threadIdx.x;
     const uint32_t ncap = min(a.natoms, (uint32_t)SIM_MAX_EM);
     for (uint32_t m = 0; m < a.nmodes; m++) {
         const uint32_t n = min(a.em_count[(size_t)f * a.nmodes + m], ncap);
@@ -215,47 +219,75 @@ __global__ void __launch_bounds__(SIM_THREADS) simulate_kernel(const SimArgs a)
         for (uint32_t i = threadIdx.x; i < n; i += SIM_THREADS) s_em[m * ncap + i] = src[i];
     }
     __syncthreads();
-    if (p >= a.npix) return;
-    const float pc0 = a.pm[3 * p], pc1 = a.pm[3 * p + 1], pc2 = a.pm[3 * p + 2];
+    if (p0 >= a.npix) return;
+    uint64_t px[SIM_PIX];
+    float pc[SIM_PIX][3];
+#pragma unroll
+    for (int q = 0; q < SIM_PIX; q++) {
+        px[q] = p0 + (uint64_t)q * SIM_THREADS;
+        const uint64_t pp = px[q] < a.npix ? px[q] : p0;  // a pixel past the end repeats p0, unwritten
+#pragma unroll
+        for (int d = 0; d < 3; d++) pc[q][d] = a.pm[3 * pp + d];
+    }
     const float nsub = (float)((2 * a.susa + 1) * (2 * a.susa + 1));
-    float total = 0.0f;
+    float total[SIM_PIX];
+#pragma unroll
+    for (int q = 0; q < SIM_PIX; q++) total[q] = 0.0f;
     for (uint32_t m = 0; m < a.nmodes; m++) {
         const uint32_t n = min(a.em_count[(size_t)f * a.nmodes + m], ncap);
         const float4 *E = s_em + m * ncap;
-        float acc = 0.0f;
+        float acc[SIM_PIX];
+#pragma unroll
+        for (int q = 0; q < SIM_PIX; q++) acc[q] = 0.0f;
         for (int v = -a.susa; v <= a.susa; v++)
             for (int u = -a.susa; u <= a.susa; u++) {
-                // IAC/kernel.cl:823-832
-                const float c0 = fadd(fadd(pc0, fmul((float)v, a.vs[0])), fmul((float)u, a.us[0]));
-                const float c1 = fadd(fadd(pc1, fmul((float)v, a.vs[1])), fmul((float)u, a.us[1]));
-                const float c2 = fadd(fadd(pc2, fmul((float)v, a.vs[2])), fmul((float)u, a.us[2]));
-                float nk = (float)(1.0 / (double)norm3(c0, c1, c2));
-                nk = (float)((double)nk * ((2.0 * 3.1415926535897932) / (double)a.wavelength));
-                const float k0 = fmul(c0, nk), k1 = fmul(c1, nk), k2 = fmul(c2, nk);
-                float re = 0.0f, im = 0.0f;
+                float k[SIM_PIX][3], re[SIM_PIX], im[SIM_PIX];
+#pragma unroll
+                for (int q = 0; q < SIM_PIX; q++) {
+                    // IAC/kernel.cl:823-832
+                    const float c0 = fadd(fadd(pc[q][0], fmul((float)v, a.vs[0])), fmul((float)u, a.us[0]));
+                    const float c1 = fadd(fadd(pc[q][1], fmul((float)v, a.vs[1])), fmul((float)u, a.us[1]));
+                    const float c2 = fadd(fadd(pc[q][2], fmul((float)v, a.vs[2])), fmul((float)u, a.us[2]));
+                    float nk = (float)(1.0 / (double)norm3(c0, c1, c2));
+                    nk = (float)((double)nk * ((2.0 * 3.1415926535897932) / (double)a.wavelength));
+                    k[q][0] = fmul(c0, nk);
+                    k[q][1] = fmul(c1, nk);
+                    k[q][2] = fmul(c2, nk);
+                    re[q] = 0.0f;
+                    im[q] = 0.0f;
+                }
                 for (uint32_t i = 0; i < n; i++) {
                     const float4 e = E[i];
-                    float arg = fmul(k0, e.x);
-                    arg = fadd(arg, fmul(k1, e.y));
-                    arg = fadd(arg, fmul(k2, e.z));
-                    arg = fadd(arg, e.w);
-                    float s, c;
-                    if (a.accurate) {
-                        sincosf(arg, &s, &c);
-                    } else {
-                        const float kk = phase_turns(arg);
-                        const float r = fmaf(-kk, TWO_PI_LO, fmaf(-kk, TWO_PI_HI, arg));
-                        __sincosf(r, &s, &c);
+#pragma unroll
+                    for (int q = 0; q < SIM_PIX; q++) {
+                        float arg = fmul(k[q][0], e.x);
+                        arg = fadd(arg, fmul(k[q][1], e.y));
+                        arg = fadd(arg, fmul(k[q][2], e.z));
+                        arg = fadd(arg, e.w);
+                        float sn, cs;
+                        if (a.accurate) {
+                            sincosf(arg, &sn, &cs);
+                        } else {
+                            const float kk = phase_turns(arg);
+                            const float r = fmaf(-kk, TWO_PI_LO, fmaf(-kk, TWO_PI_HI, arg));
+                            __sincosf(r, &sn, &cs);
+                        }
+                        re[q] = fadd(re[q], cs);
+                        im[q] = fadd(im[q], sn);
                     }
-                    re = fadd(re, c);
-                    im = fadd(im, s);
                 }
-                const float a2 = fadd(fmul(re, re), fmul(im, im));
-                acc = fadd(acc, a.amplitude_sq ? a2 : __fsqrt_rn(a2));
+#pragma unroll
+                for (int q = 0; q < SIM_PIX; q++) {
+                    const float a2 = fadd(fmul(re[q], re[q]), fmul(im[q], im[q]));
+                    acc[q] = fadd(acc[q], a.amplitude_sq ? a2 : __fsqrt_rn(a2));
+                }
             }
-        total = fadd(total, __fdiv_rn(acc, nsub));  // per-mode image, summed as ParAdd does
+#pragma unroll
+        for (int q = 0; q < SIM_PIX; q++) total[q] = fadd(total[q], __fdiv_rn(acc[q], nsub));  // as ParAdd sums modes
     }
-    a.out[(size_t)f * a.npix + p] = total;
+#pragma unroll
+    for (int q = 0; q < SIM_PIX; q++)
+        if (px[q] < a.npix) a.out[(size_t)f * a.npix + px[q]] = total[q];
 }
 
 // simulate_kernel for crystals whose emitters do not fit the shared-memory
@@ -593,7 +625,8 @@ iac_status iac_simulate_intensity(iac_ctx *ctx, const float *d_pixel_map, uint64
         // every mode's emitters staged at once
         const size_t smem = sizeof(float4) * nmodes * natoms;
         IAC_CUDA(cudaFuncSetAttribute(simulate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        simulate_kernel<<<grid, SIM_THREADS, smem, as_stream(stream)>>>(a);
+        const dim3 grid2((unsigned)((npix + SIM_PIX * SIM_THREADS - 1) / (SIM_PIX * SIM_THREADS)), nframes);
+        simulate_kernel<<<grid2, SIM_THREADS, smem, as_stream(stream)>>>(a);
     } else {
         simulate_chunked_kernel<<<grid, SIM_THREADS, 0, as_stream(stream)>>>(a);
     }
